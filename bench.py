@@ -1,0 +1,351 @@
+#!/usr/bin/env python
+"""Benchmark: mode-solves/s of the batched 2D Helmholtz/Poisson
+diagonalisation solve (duct's helm3d hot path) on B200.
+
+Workload (one "step"): the four solves of one RK3/CN substep of the square
+duct at my = mz = 129 (n = 127 interior points), 64 Fourier modes k = 0..63
+with kx = 0.5 k (Lx = 4 pi): u, v, w Dirichlet with lambda = kx^2 + 2/(nu dt)
+(nu = 1/2000, dt = 1e-3) and the pressure Poisson problem, Neumann with
+lambda = kx^2 (kx = 0 singular, pinned as the reference does).  That is
+256 mode-solves per step on seeded synthetic complex128 right-hand sides.
+
+Arms:
+* default: the device-resident batched solve (ductgpu_solve_fields_dev) with
+  inputs in HBM; ``e2e`` times the reference-facing drop-in ductgpu_helm3d on
+  pinned host arrays (H2D + solve + D2H per field) for the same work.
+* ``--impl reference``: the reference's CPU algorithm (the oracle's
+  restatement of helm3d/solvediag with the same LAPACK/BLAS calls) on all
+  host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "mode-solves/s (batched 2D Helmholtz/Poisson diagonalisation solve)"
+UNIT = "mode-solves/s"
+WORKLOAD = "cfg1: square duct my=mz=129, 64 Fourier modes x 4 fields (u,v,w Dirichlet + pressure Neumann)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload():
+    from duct_b200 import synth
+    c = synth.config("cfg1")
+    m, nm = c["my"], c["nmodes"]
+    xalp = c["alp"] * np.arange(nm)
+    rhs = [synth.chebyshev_rhs(m, m, nm, seed=1 + i, ib=0) for i in range(len(c["fields"]))]
+    return c, m, nm, xalp, rhs
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9
+                          for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, v):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference_rate(c, m, xalp, rhs, budget_s=10.0, max_iters=None):
+    """The reference CPU algorithm (oracle restatement, same LAPACK/BLAS
+    calls) on every host core: mode-solves/s over whole cfg1 batches."""
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.set_blas_threads(1)
+    ops = O.Ops(m)
+    nm = len(xalp)
+    done, t0 = 0, time.perf_counter()
+    it = 0
+    while True:
+        for (name, bound, lam), f in zip(c["fields"], rhs):
+            O.helm3d(f, ops, bound, lam, xalp, nthreads=threads)
+            done += nm
+        it += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or (max_iters and it >= max_iters):
+            break
+    return done / el, threads, done, el
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    c, m, nm, xalp, rhs = workload()
+    per_step = nm * len(c["fields"])
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.set_blas_threads(1)
+    ops = O.Ops(m)
+
+    def step():
+        for (name, bound, lam), f in zip(c["fields"], rhs):
+            O.helm3d(f, ops, bound, lam, xalp, nthreads=threads)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    el = time.perf_counter() - t0
+    v = per_step * args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded splitmix64 Chebyshev-coefficient RHS)",
+        "config": {"workload": WORKLOAD, "mode_solves_per_step": per_step},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": "%d full cfg1 batches (%d mode-solves each)" % (args.steps, per_step)},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local, pg):
+    import duct_b200 as D
+    c, m, nm, xalp, rhs = workload()
+    n = m - 2
+    nf = len(c["fields"])
+    per_step = nm * nf
+    ctx = D.Context(local)
+    ctx.pseudomat(m)
+    prec = {"auto": D.PREC_FP64, "fp64": D.PREC_FP64, "mixed": D.PREC_MIXED}[args.precision]
+
+    # two rotating input/output sets: 2 x 4 x 2 x 17 MB = 272 MB > 126 MB L2
+    sets = []
+    for s in range(2):
+        fl = []
+        for (name, bound, lam), f in zip(c["fields"], rhs):
+            r = ctx.device_array(f.shape)
+            o = ctx.device_array(f.shape)
+            r.upload(f)
+            fl.append(dict(rhs=r, sol=o, xalp=xalp, alambda=lam, ib=0, bound=bound))
+        sets.append(fl)
+
+    for i in range(args.warmup):
+        ctx.solve_fields_dev(sets[i % 2], prec)
+    ctx.synchronize()
+    barrier(pg)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ctx.profile(True)
+    ctx.profile_reset()
+    l0 = ctx.launch_count()
+    ctx.event_record(0)
+    for i in range(args.steps):
+        ctx.solve_fields_dev(sets[i % 2], prec)
+    ctx.event_record(1)
+    ms = ctx.event_elapsed(0, 1)
+    launches = ctx.launch_count() - l0
+    kern_ms, kern_n = ctx.profile_read(D.K_PASS_FP64)
+    ctx.profile(False)
+    clk = clocks.stop()
+    ms = max_over_ranks(pg, ms)
+    barrier(pg)
+    ms_step = ms / args.steps
+    value = world * per_step / (ms_step * 1e-3)
+
+    # roofline of the dominant kernel (FP64 DMMA pass): 4 n^3 flops per
+    # complex plane per pass (an n x n operator on 2n real columns).
+    flops_launch = 4.0 * n ** 3 * per_step
+    avg_launch_s = (kern_ms / kern_n) * 1e-3 if kern_n else None
+    achieved = flops_launch / avg_launch_s / 1e12 if avg_launch_s else None
+    peak, peak_note = fp64_peak()
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": (achieved / peak) if (achieved and peak) else None,
+            "traffic": traffic_from_profile(), "kernel": "k_pass_fp64 (DMMA m16n8k8)",
+            "peak_source": peak_note,
+            "kernel_share_of_step": (kern_ms / ms) if ms else None}
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = measure_e2e(ctx, c, m, nm, xalp, rhs, prec, args, pg, world)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, threads, done, el = cpu_reference_rate(c, m, xalp, rhs, budget_s=10.0)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": "%d mode-solves (whole cfg1 batches) in %.1f s" % (done, el)}
+
+    for fl in sets:
+        for f in fl:
+            f["rhs"].free()
+            f["sol"].free()
+    ctx.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == D.PREC_FP64 else "bf16-split+f64-refine",
+            "data": "synthetic (seeded splitmix64 Chebyshev-coefficient RHS)",
+            "config": {"workload": WORKLOAD, "mode_solves_per_step": per_step,
+                       "precision": "fp64" if prec == D.PREC_FP64 else "mixed",
+                       "parallelism": "replicas" if world > 1 else "1gpu",
+                       "l2": "2 rotating input/output sets (272 MB) > 126 MB L2"},
+            "gpu_launches": launches,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def fp64_peak():
+    p = os.path.join(ROOT, "profiles", "measured_fp64_peak.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d["fp64_tflops"], "measured cuBLAS DGEMM on this pool (profiles/measured_fp64_peak.json)"
+    return None, "no measured FP64 peak available"
+
+
+def traffic_from_profile():
+    p = os.path.join(ROOT, "profiles", "k_pass_fp64_traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p)).get("bytes_per_launch")
+    return None
+
+
+def measure_e2e(ctx, c, m, nm, xalp, rhs, prec, args, pg, world):
+    """End to end through the drop-in helm3d on pinned host arrays."""
+    import ctypes as C
+    import duct_b200 as D
+    L = D.lib()
+    nbytes = rhs[0].nbytes
+    hr, hs = [], []
+    for f in rhs:
+        p = C.c_void_p()
+        ctx._check(L.ductgpu_host_alloc(ctx.h, nbytes, C.byref(p)))
+        a = np.ctypeslib.as_array((C.c_double * (nbytes // 8)).from_address(p.value))
+        a[:] = f.view(np.float64).ravel(order="F")
+        hr.append((p, a))
+        q = C.c_void_p()
+        ctx._check(L.ductgpu_host_alloc(ctx.h, nbytes, C.byref(q)))
+        hs.append(q)
+    x = np.ascontiguousarray(xalp)
+
+    def step():
+        for (name, bound, lam), (p, a), q in zip(c["fields"], hr, hs):
+            ctx._check(L.ductgpu_helm3d(ctx.h, p, q, 1, bound.encode(), float(lam), m, m, 0, nm - 1,
+                                        x.ctypes.data_as(C.c_void_p), prec))
+
+    steps = max(3, args.steps // 5)
+    for _ in range(max(3, args.warmup)):
+        step()
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    el = max_over_ranks(pg, time.perf_counter() - t0)
+    for p, a in hr:
+        L.ductgpu_host_free(ctx.h, p)
+    for q in hs:
+        L.ductgpu_host_free(ctx.h, q)
+    per_step = nm * len(rhs)
+    return {"value": world * per_step * steps / el, "unit": UNIT,
+            "h2d_bytes_per_step": nbytes * len(rhs), "d2h_bytes_per_step": nbytes * len(rhs),
+            "steps": steps, "api": "ductgpu_helm3d (host arrays, pinned)"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        # rank 0 alone times the CPU reference; other ranks exit without work
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
+    world, rank, local, pg = dist_setup(args)
+    try:
+        run_ours(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,242 @@
+"""duct_b200 -- B200 (sm_100a) implementation of the duct per-Fourier-mode
+2D Helmholtz/Poisson diagonalisation solve behind a C-ABI.
+
+The product is ``duct_b200/lib/libductgpu.so`` (C-ABI declared in
+``include/ductgpu.h``).  This module is a thin ctypes mirror of that ABI for
+Python callers, tests and the benchmark; it does no numerics of its own and
+there is no CPU fallback: if the library is missing, importing raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libductgpu.so")
+
+OK, EARG, ESTATE, ECUDA, ESOLVER, ENONFINITE, ETIMEOUT, EALLOC = range(8)
+PREC_FP64, PREC_MIXED = 0, 1
+GAUGE_POINT, GAUGE_MEAN = 0, 1
+
+EXPORTS = [
+    "ductgpu_create", "ductgpu_destroy", "ductgpu_last_error", "ductgpu_set_stream",
+    "ductgpu_get_stream", "ductgpu_synchronize", "ductgpu_pseudomat",
+    "ductgpu_get_operators", "ductgpu_set_operators", "ductgpu_set_gauge",
+    "ductgpu_helm3d", "ductgpu_solve_fields_dev", "ductgpu_device_alloc",
+    "ductgpu_device_free", "ductgpu_host_alloc", "ductgpu_host_free", "ductgpu_copy",
+    "ductgpu_event_record", "ductgpu_event_elapsed", "ductgpu_launch_count",
+    "ductgpu_profile_enable", "ductgpu_profile_reset", "ductgpu_profile_read",
+]
+K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
+
+
+class Field(C.Structure):
+    """ductgpu_field of include/ductgpu.h."""
+    _fields_ = [("rhs", C.c_void_p), ("sol", C.c_void_p), ("xalp", C.c_void_p),
+                ("alambda", C.c_double), ("ib", C.c_int), ("nmodes", C.c_int),
+                ("bound", C.c_char)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libductgpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libductgpu.so is not built (run duct_b200/build.py): %s" % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        P, I, D = C.c_void_p, C.c_int, C.c_double
+        sig = {
+            "ductgpu_create": [I, C.POINTER(P)],
+            "ductgpu_destroy": [P],
+            "ductgpu_last_error": [P, C.c_char_p, I],
+            "ductgpu_set_stream": [P, P],
+            "ductgpu_get_stream": [P],
+            "ductgpu_synchronize": [P],
+            "ductgpu_pseudomat": [P, I, I],
+            "ductgpu_get_operators": [P, C.c_char, P, P, P, C.POINTER(I)],
+            "ductgpu_set_operators": [P, C.c_char, P, P, P, I],
+            "ductgpu_set_gauge": [P, I],
+            "ductgpu_helm3d": [P, P, P, I, C.c_char, D, I, I, I, I, P, I],
+            "ductgpu_solve_fields_dev": [P, C.POINTER(Field), I, I],
+            "ductgpu_device_alloc": [P, C.c_size_t, C.POINTER(P)],
+            "ductgpu_device_free": [P, P],
+            "ductgpu_host_alloc": [P, C.c_size_t, C.POINTER(P)],
+            "ductgpu_host_free": [P, P],
+            "ductgpu_copy": [P, P, P, C.c_size_t, I],
+            "ductgpu_event_record": [P, I],
+            "ductgpu_event_elapsed": [P, I, I, C.POINTER(C.c_float)],
+            "ductgpu_launch_count": [P],
+            "ductgpu_profile_enable": [P, I],
+            "ductgpu_profile_reset": [P],
+            "ductgpu_profile_read": [P, I, C.POINTER(C.c_double), C.POINTER(C.c_longlong)],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = I
+        L.ductgpu_get_stream.restype = P
+        L.ductgpu_launch_count.restype = C.c_longlong
+        _lib = L
+    return _lib
+
+
+class DuctGPUError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("ductgpu status %d: %s" % (code, msg))
+        self.code = code
+
+
+def _ptr(a):
+    if isinstance(a, DeviceArray):
+        return C.c_void_p(a.ptr)
+    if a is None:
+        return None
+    assert a.flags.f_contiguous or a.flags.c_contiguous
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class DeviceArray:
+    """Device buffer owned through the library's allocation helpers."""
+
+    def __init__(self, ctx, shape, dtype=np.complex128):
+        self.ctx, self.shape, self.dtype = ctx, tuple(shape), np.dtype(dtype)
+        self.nbytes = int(np.prod(self.shape)) * self.dtype.itemsize
+        p = C.c_void_p()
+        ctx._check(lib().ductgpu_device_alloc(ctx.h, self.nbytes, C.byref(p)))
+        self.ptr = p.value
+
+    def upload(self, host):
+        host = np.asfortranarray(host, dtype=self.dtype)
+        assert host.nbytes == self.nbytes
+        self.ctx._check(lib().ductgpu_copy(self.ctx.h, C.c_void_p(self.ptr), _ptr(host), self.nbytes, 1))
+        self.ctx.synchronize()
+
+    def download(self):
+        out = np.empty(self.shape, dtype=self.dtype, order="F")
+        self.ctx._check(lib().ductgpu_copy(self.ctx.h, _ptr(out), C.c_void_p(self.ptr), self.nbytes, 2))
+        self.ctx.synchronize()
+        return out
+
+    def free(self):
+        if self.ptr:
+            lib().ductgpu_device_free(self.ctx.h, C.c_void_p(self.ptr))
+            self.ptr = None
+
+
+class Context:
+    """One ductgpu context (device + stream + operators)."""
+
+    def __init__(self, device=0):
+        h = C.c_void_p()
+        rc = lib().ductgpu_create(int(device), C.byref(h))
+        if rc:
+            raise DuctGPUError(rc, "ductgpu_create(device=%d) failed" % device)
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().ductgpu_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def last_error(self):
+        buf = C.create_string_buffer(512)
+        lib().ductgpu_last_error(self.h, buf, 512)
+        return buf.value.decode()
+
+    def _check(self, rc):
+        if rc:
+            raise DuctGPUError(rc, self.last_error())
+        return rc
+
+    def synchronize(self):
+        self._check(lib().ductgpu_synchronize(self.h))
+
+    def pseudomat(self, my, mz=None):
+        self._check(lib().ductgpu_pseudomat(self.h, int(my), int(mz if mz is not None else my)))
+
+    def get_operators(self, bound, n):
+        E = np.empty(n)
+        P = np.empty((n, n), order="F")
+        Q = np.empty((n, n), order="F")
+        io = C.c_int()
+        self._check(lib().ductgpu_get_operators(self.h, bound.encode(), _ptr(E), _ptr(P), _ptr(Q), C.byref(io)))
+        return E, P, Q, io.value
+
+    def set_operators(self, bound, E, P, PM1, iofzero=0):
+        E = np.ascontiguousarray(E, dtype=np.float64)
+        P = np.asfortranarray(P, dtype=np.float64)
+        PM1 = np.asfortranarray(PM1, dtype=np.float64)
+        self._check(lib().ductgpu_set_operators(self.h, bound.encode(), _ptr(E), _ptr(P), _ptr(PM1), int(iofzero)))
+
+    def set_gauge(self, gauge):
+        self._check(lib().ductgpu_set_gauge(self.h, int(gauge)))
+
+    def helm3d(self, rhs, bound, alambda, xalp, ib=0, ipro=1, precision=PREC_FP64):
+        """helm3d drop-in on host arrays: rhs (my,mz,nmodes) complex128,
+        Fortran order, modified in place like the reference (walls zeroed
+        for 'd').  Returns the solution."""
+        assert rhs.dtype == np.complex128 and rhs.flags.f_contiguous
+        my, mz, nm = rhs.shape
+        sol = np.zeros_like(rhs, order="F")
+        xalp = np.ascontiguousarray(xalp, dtype=np.float64)
+        assert xalp.shape == (nm,)
+        self._check(lib().ductgpu_helm3d(self.h, _ptr(rhs), _ptr(sol), int(ipro), bound.encode(),
+                                         float(alambda), my, mz, int(ib), int(ib) + nm - 1,
+                                         _ptr(xalp), int(precision)))
+        return sol
+
+    def solve_fields_dev(self, fields, precision=PREC_FP64):
+        """fields: list of dicts(rhs=DeviceArray, sol=DeviceArray, xalp=ndarray,
+        alambda=float, ib=int, bound='d'|'n')."""
+        arr = (Field * len(fields))()
+        keep = []
+        for i, f in enumerate(fields):
+            xalp = np.ascontiguousarray(f["xalp"], dtype=np.float64)
+            keep.append(xalp)
+            arr[i].rhs = f["rhs"].ptr if isinstance(f["rhs"], DeviceArray) else f["rhs"]
+            arr[i].sol = f["sol"].ptr if isinstance(f["sol"], DeviceArray) else f["sol"]
+            arr[i].xalp = xalp.ctypes.data
+            arr[i].alambda = float(f["alambda"])
+            arr[i].ib = int(f.get("ib", 0))
+            arr[i].nmodes = int(xalp.shape[0])
+            arr[i].bound = f["bound"].encode()
+        self._check(lib().ductgpu_solve_fields_dev(self.h, arr, len(fields), int(precision)))
+        return keep
+
+    def device_array(self, shape, dtype=np.complex128):
+        return DeviceArray(self, shape, dtype)
+
+    def event_record(self, slot):
+        self._check(lib().ductgpu_event_record(self.h, int(slot)))
+
+    def event_elapsed(self, s0, s1):
+        ms = C.c_float()
+        self._check(lib().ductgpu_event_elapsed(self.h, int(s0), int(s1), C.byref(ms)))
+        return ms.value
+
+    def launch_count(self):
+        return int(lib().ductgpu_launch_count(self.h))
+
+    def profile(self, on=True):
+        self._check(lib().ductgpu_profile_enable(self.h, int(bool(on))))
+
+    def profile_reset(self):
+        self._check(lib().ductgpu_profile_reset(self.h))
+
+    def profile_read(self, kind):
+        ms, n = C.c_double(), C.c_longlong()
+        self._check(lib().ductgpu_profile_read(self.h, int(kind), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+
+__all__ = ["Context", "DeviceArray", "DuctGPUError", "lib", "LIB_PATH", "EXPORTS",
+           "PREC_FP64", "PREC_MIXED", "GAUGE_POINT", "GAUGE_MEAN"]

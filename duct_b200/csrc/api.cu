@@ -1,0 +1,426 @@
+// api.cu -- the extern "C" entry points of libductgpu (declared in
+// include/ductgpu.h).  Host-side argument checking, buffer management and
+// the helm3d drop-in live here; the numerics are in setup.cu and
+// solve_*.cu.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "internal.h"
+
+namespace duct {
+
+int set_error(ductgpu_ctx ctx, int code, const char *fmt, ...)
+{
+    if (ctx) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(ctx->err, sizeof(ctx->err), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+int check_cuda(ductgpu_ctx ctx, cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return DUCTGPU_OK;
+    return set_error(ctx, e == cudaErrorMemoryAllocation ? DUCTGPU_EALLOC : DUCTGPU_ECUDA,
+                     "%s: %s", what, cudaGetErrorString(e));
+}
+
+int ensure(ductgpu_ctx ctx, Workspace &w, size_t bytes)
+{
+    if (w.bytes >= bytes) return DUCTGPU_OK;
+    if (w.buf) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(w.buf);
+        w.buf = nullptr;
+        w.bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&w.buf, bytes);
+    if (e != cudaSuccess) return check_cuda(ctx, e, "workspace");
+    w.bytes = bytes;
+    return DUCTGPU_OK;
+}
+
+static int ensure_lam(ductgpu_ctx ctx, int planes)
+{
+    if (ctx->lam_cap >= planes) return DUCTGPU_OK;
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->lam);
+    cudaFreeHost(ctx->lam_host);
+    ctx->lam = nullptr;
+    ctx->lam_host = nullptr;
+    ctx->lam_cap = 0;
+    const int cap = planes < 256 ? 256 : planes;
+    DUCT_CUDA(ctx, cudaMalloc(&ctx->lam, cap * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMallocHost(&ctx->lam_host, cap * sizeof(double)));
+    ctx->lam_cap = cap;
+    return DUCTGPU_OK;
+}
+
+static int validate_field(ductgpu_ctx ctx, const ductgpu_field &f)
+{
+    if (!f.rhs || !f.sol || (!f.xalp && f.nmodes > 0))
+        return set_error(ctx, DUCTGPU_EARG, "null field pointer");
+    if (f.bound != 'd' && f.bound != 'n')
+        return set_error(ctx, DUCTGPU_EARG, "bound '%c' is neither 'd' nor 'n'", f.bound);
+    if (f.nmodes < 1 || f.ib < 0)
+        return set_error(ctx, DUCTGPU_EARG, "nmodes=%d ib=%d", f.nmodes, f.ib);
+    if (((uintptr_t)f.rhs | (uintptr_t)f.sol) & 15)
+        return set_error(ctx, DUCTGPU_EARG, "field arrays must be 16-byte aligned");
+    return DUCTGPU_OK;
+}
+
+// Fill ctx->lam with lambda = alambda + xalp^2 (src/helm3d.f90:67) for every
+// plane of the fields and build the task list.
+static int prepare(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, FieldTask *tasks)
+{
+    int planes = 0;
+    for (int i = 0; i < nfields; ++i) planes += fields[i].nmodes;
+    int rc = ensure_lam(ctx, planes);
+    if (rc) return rc;
+    // the pinned staging buffer may still be read by an earlier copy
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    int p = 0;
+    for (int i = 0; i < nfields; ++i) {
+        const ductgpu_field &f = fields[i];
+        tasks[i].rhs = f.rhs;
+        tasks[i].sol = f.sol;
+        tasks[i].nmodes = f.nmodes;
+        tasks[i].mode0 = (f.ib == 0);
+        tasks[i].bound = f.bound;
+        tasks[i].plane0 = p;
+        for (int k = 0; k < f.nmodes; ++k) ctx->lam_host[p + k] = f.alambda + f.xalp[k] * f.xalp[k];
+        p += f.nmodes;
+    }
+    DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->lam, ctx->lam_host, planes * sizeof(double),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    return DUCTGPU_OK;
+}
+
+LaunchScope::LaunchScope(ductgpu_ctx ctx, int kind) : c(ctx)
+{
+    c->launches += 1;
+    if (!c->prof_on) return;
+    if (c->prof_used >= ductgpu_ctx_s::kProfSlots) profile_drain(c);
+    slot = c->prof_used++;
+    c->prof_kind[slot] = kind;
+    cudaEventRecord(c->prof_ev[2 * slot], c->stream);
+}
+
+LaunchScope::~LaunchScope()
+{
+    if (slot >= 0) cudaEventRecord(c->prof_ev[2 * slot + 1], c->stream);
+}
+
+void profile_drain(ductgpu_ctx c)
+{
+    if (!c->prof_used) return;
+    cudaEventSynchronize(c->prof_ev[2 * (c->prof_used - 1) + 1]);
+    for (int i = 0; i < c->prof_used; ++i) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, c->prof_ev[2 * i], c->prof_ev[2 * i + 1]) == cudaSuccess) {
+            c->prof_ms[c->prof_kind[i]] += ms;
+            c->prof_n[c->prof_kind[i]] += 1;
+        }
+    }
+    c->prof_used = 0;
+}
+
+}  // namespace duct
+
+using namespace duct;
+
+extern "C" {
+
+int ductgpu_create(int device, ductgpu_ctx *out)
+{
+    if (!out) return DUCTGPU_EARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return DUCTGPU_ECUDA;
+    if (cudaSetDevice(device) != cudaSuccess) return DUCTGPU_ECUDA;
+    ductgpu_ctx c = new (std::nothrow) ductgpu_ctx_s();
+    if (!c) return DUCTGPU_EALLOC;
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return DUCTGPU_ECUDA;
+    }
+    c->stream = c->own_stream;
+    if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS ||
+        cusolverDnSetStream(c->solver, c->stream) != CUSOLVER_STATUS_SUCCESS) {
+        cudaStreamDestroy(c->own_stream);
+        delete c;
+        return DUCTGPU_ESOLVER;
+    }
+    for (int i = 0; i < kNumEvents; ++i) cudaEventCreate(&c->ev[i]);
+    *out = c;
+    return DUCTGPU_OK;
+}
+
+int ductgpu_destroy(ductgpu_ctx ctx)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    free_bound(ctx->dir);
+    free_bound(ctx->neu);
+    cudaFree(ctx->xcol); cudaFree(ctx->DC); cudaFree(ctx->D2); cudaFree(ctx->AM1); cudaFree(ctx->ccw);
+    cudaFree(ctx->work.buf);
+    cudaFree(ctx->io.buf);
+    cudaFree(ctx->lam);
+    cudaFreeHost(ctx->lam_host);
+    for (int i = 0; i < kNumEvents; ++i) cudaEventDestroy(ctx->ev[i]);
+    if (ctx->prof_ev[0])
+        for (int i = 0; i < 2 * ductgpu_ctx_s::kProfSlots; ++i) cudaEventDestroy(ctx->prof_ev[i]);
+    if (ctx->solver) cusolverDnDestroy(ctx->solver);
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return DUCTGPU_OK;
+}
+
+int ductgpu_last_error(ductgpu_ctx ctx, char *buf, int len)
+{
+    if (!ctx || !buf || len < 1) return DUCTGPU_EARG;
+    strncpy(buf, ctx->err, (size_t)len - 1);
+    buf[len - 1] = 0;
+    return DUCTGPU_OK;
+}
+
+int ductgpu_set_stream(ductgpu_ctx ctx, void *cuda_stream)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    ctx->stream = cuda_stream ? (cudaStream_t)cuda_stream : ctx->own_stream;
+    if (cusolverDnSetStream(ctx->solver, ctx->stream) != CUSOLVER_STATUS_SUCCESS)
+        return set_error(ctx, DUCTGPU_ESOLVER, "cusolverDnSetStream");
+    return DUCTGPU_OK;
+}
+
+void *ductgpu_get_stream(ductgpu_ctx ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int ductgpu_synchronize(ductgpu_ctx ctx)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "synchronize");
+}
+
+int ductgpu_pseudomat(ductgpu_ctx ctx, int my, int mz)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (my != mz)
+        return set_error(ctx, DUCTGPU_EARG, "IN HELM3D: MY.NE.MZ (NOT IMPLEMENTED): my=%d mz=%d", my, mz);
+    cudaSetDevice(ctx->device);
+    return pseudomat_gpu(ctx, my);
+}
+
+int ductgpu_get_operators(ductgpu_ctx ctx, char bound, double *E, double *P, double *PM1, int *iofzero)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (!ctx->ready) return set_error(ctx, DUCTGPU_ESTATE, "operators not set up");
+    if (bound != 'd' && bound != 'n') return set_error(ctx, DUCTGPU_EARG, "bound '%c'", bound);
+    const BoundOps &b = (bound == 'n') ? ctx->neu : ctx->dir;
+    const size_t nn = (size_t)b.n * b.n;
+    if (E) DUCT_CUDA(ctx, cudaMemcpyAsync(E, b.E, b.n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (P) DUCT_CUDA(ctx, cudaMemcpyAsync(P, b.P, nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (PM1) DUCT_CUDA(ctx, cudaMemcpyAsync(PM1, b.PM1, nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (iofzero) *iofzero = b.iofzero;
+    return DUCTGPU_OK;
+}
+
+int ductgpu_set_operators(ductgpu_ctx ctx, char bound, const double *E, const double *P, const double *PM1, int iofzero)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (!ctx->ready) return set_error(ctx, DUCTGPU_ESTATE, "call ductgpu_pseudomat first");
+    if (bound != 'd' && bound != 'n') return set_error(ctx, DUCTGPU_EARG, "bound '%c'", bound);
+    if (!E || !P || !PM1) return set_error(ctx, DUCTGPU_EARG, "null operator");
+    BoundOps &b = (bound == 'n') ? ctx->neu : ctx->dir;
+    const size_t nn = (size_t)b.n * b.n;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.E, E, b.n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.P, P, nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.PM1, PM1, nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if (bound == 'n') {
+        if (iofzero <= 0) {
+            double eigmin = 1.0e6;
+            iofzero = 0;
+            for (int i = 0; i < b.n; ++i) {
+                const double e = fmin(eigmin, fabs(E[i]));
+                if (e != eigmin) { iofzero = i + 1; eigmin = e; }
+            }
+        }
+        if (iofzero > b.n) return set_error(ctx, DUCTGPU_EARG, "iofzero %d > n", iofzero);
+        b.iofzero = iofzero;
+    }
+    int rc = pack_operators(ctx, b);
+    if (rc) return rc;
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "set_operators");
+}
+
+int ductgpu_set_gauge(ductgpu_ctx ctx, int gauge)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (gauge != DUCTGPU_GAUGE_POINT && gauge != DUCTGPU_GAUGE_MEAN)
+        return set_error(ctx, DUCTGPU_EARG, "gauge %d", gauge);
+    ctx->gauge = gauge;
+    return DUCTGPU_OK;
+}
+
+int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, int precision)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (!ctx->ready) return set_error(ctx, DUCTGPU_ESTATE, "operators not set up (call ductgpu_pseudomat)");
+    if (!fields || nfields < 1 || nfields > kMaxFields)
+        return set_error(ctx, DUCTGPU_EARG, "nfields=%d (1..%d)", nfields, kMaxFields);
+    if (precision != DUCTGPU_PREC_FP64 && precision != DUCTGPU_PREC_MIXED)
+        return set_error(ctx, DUCTGPU_EARG, "precision %d", precision);
+    for (int i = 0; i < nfields; ++i) {
+        int rc = validate_field(ctx, fields[i]);
+        if (rc) return rc;
+    }
+    cudaSetDevice(ctx->device);
+    FieldTask tasks[kMaxFields];
+    int rc = prepare(ctx, fields, nfields, tasks);
+    if (rc) return rc;
+    if (precision == DUCTGPU_PREC_MIXED)
+        return set_error(ctx, DUCTGPU_EARG, "mixed precision not built yet");
+    return solve_fp64(ctx, tasks, nfields);
+}
+
+int ductgpu_helm3d(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, char bound, double alambda,
+                   int my, int mz, int ib, int ie, const double *xalp, int precision)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (ipro <= 0) {
+        int rc = ductgpu_pseudomat(ctx, my, mz);
+        if (rc) return rc;
+        if (ipro == -1) return DUCTGPU_OK;
+    }
+    if (!ctx->ready) return set_error(ctx, DUCTGPU_ESTATE, "operators not set up (call with ipro<=0)");
+    if (my != ctx->my || mz != ctx->mz)
+        return set_error(ctx, DUCTGPU_EARG, "grid %dx%d differs from the set-up %dx%d", my, mz, ctx->my, ctx->mz);
+    if (!rhs || !sol || !xalp) return set_error(ctx, DUCTGPU_EARG, "null pointer");
+    if (bound != 'd' && bound != 'n')
+        return set_error(ctx, DUCTGPU_EARG, "in solvediag error in BC: bound '%c'", bound);
+    if (ie < ib || ib < 0) return set_error(ctx, DUCTGPU_EARG, "ib=%d ie=%d", ib, ie);
+    cudaSetDevice(ctx->device);
+    const int nm = ie - ib + 1;
+    const size_t bytes = (size_t)2 * my * mz * nm * sizeof(double);
+    // helm3d zeroes the Dirichlet walls of rhs in place (src/helm3d.f90:48-60)
+    if (bound == 'd') {
+        for (int i = 0; i < nm; ++i) {
+            double *r = rhs + (size_t)2 * my * mz * i;
+            for (int j = 0; j < my; ++j) {
+                r[2 * j] = r[2 * j + 1] = 0.0;
+                r[2 * (j + (size_t)my * (mz - 1))] = r[2 * (j + (size_t)my * (mz - 1)) + 1] = 0.0;
+            }
+            for (int k = 0; k < mz; ++k) {
+                r[2 * ((size_t)my * k)] = r[2 * ((size_t)my * k) + 1] = 0.0;
+                r[2 * (my - 1 + (size_t)my * k)] = r[2 * (my - 1 + (size_t)my * k) + 1] = 0.0;
+            }
+        }
+    }
+    int rc = ensure(ctx, ctx->io, 2 * bytes);
+    if (rc) return rc;
+    double *drhs = ctx->io.buf, *dsol = ctx->io.buf + bytes / sizeof(double);
+    DUCT_CUDA(ctx, cudaMemcpyAsync(drhs, rhs, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    ductgpu_field f;
+    f.rhs = drhs;
+    f.sol = dsol;
+    f.xalp = xalp;
+    f.alambda = alambda;
+    f.ib = ib;
+    f.nmodes = nm;
+    f.bound = bound;
+    rc = ductgpu_solve_fields_dev(ctx, &f, 1, precision);
+    if (rc) return rc;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(sol, dsol, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d");
+}
+
+int ductgpu_device_alloc(ductgpu_ctx ctx, size_t bytes, void **ptr)
+{
+    if (!ctx || !ptr) return DUCTGPU_EARG;
+    cudaSetDevice(ctx->device);
+    *ptr = nullptr;
+    return check_cuda(ctx, cudaMalloc(ptr, bytes), "device_alloc");
+}
+
+int ductgpu_device_free(ductgpu_ctx ctx, void *ptr)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    cudaStreamSynchronize(ctx->stream);
+    return check_cuda(ctx, cudaFree(ptr), "device_free");
+}
+
+int ductgpu_host_alloc(ductgpu_ctx ctx, size_t bytes, void **ptr)
+{
+    if (!ctx || !ptr) return DUCTGPU_EARG;
+    *ptr = nullptr;
+    return check_cuda(ctx, cudaMallocHost(ptr, bytes), "host_alloc");
+}
+
+int ductgpu_host_free(ductgpu_ctx ctx, void *ptr)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    cudaStreamSynchronize(ctx->stream);
+    return check_cuda(ctx, cudaFreeHost(ptr), "host_free");
+}
+
+int ductgpu_copy(ductgpu_ctx ctx, void *dst, const void *src, size_t bytes, int kind)
+{
+    if (!ctx || (!dst && bytes) || (!src && bytes) || kind < 1 || kind > 3) return DUCTGPU_EARG;
+    return check_cuda(ctx, cudaMemcpyAsync(dst, src, bytes, (cudaMemcpyKind)kind, ctx->stream), "copy");
+}
+
+int ductgpu_event_record(ductgpu_ctx ctx, int slot)
+{
+    if (!ctx || slot < 0 || slot >= kNumEvents) return DUCTGPU_EARG;
+    return check_cuda(ctx, cudaEventRecord(ctx->ev[slot], ctx->stream), "event record");
+}
+
+int ductgpu_event_elapsed(ductgpu_ctx ctx, int s0, int s1, float *ms)
+{
+    if (!ctx || !ms || s0 < 0 || s1 < 0 || s0 >= kNumEvents || s1 >= kNumEvents) return DUCTGPU_EARG;
+    DUCT_CUDA(ctx, cudaEventSynchronize(ctx->ev[s1]));
+    return check_cuda(ctx, cudaEventElapsedTime(ms, ctx->ev[s0], ctx->ev[s1]), "event elapsed");
+}
+
+long long ductgpu_launch_count(ductgpu_ctx ctx) { return ctx ? ctx->launches : -1; }
+
+int ductgpu_profile_enable(ductgpu_ctx ctx, int on)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (on && !ctx->prof_ev[0])
+        for (int i = 0; i < 2 * ductgpu_ctx_s::kProfSlots; ++i)
+            DUCT_CUDA(ctx, cudaEventCreate(&ctx->prof_ev[i]));
+    if (!on) profile_drain(ctx);
+    ctx->prof_on = on != 0;
+    return DUCTGPU_OK;
+}
+
+int ductgpu_profile_reset(ductgpu_ctx ctx)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    profile_drain(ctx);
+    for (int k = 0; k < DUCTGPU_K_COUNT; ++k) {
+        ctx->prof_ms[k] = 0.0;
+        ctx->prof_n[k] = 0;
+    }
+    return DUCTGPU_OK;
+}
+
+int ductgpu_profile_read(ductgpu_ctx ctx, int kind, double *ms, long long *launches)
+{
+    if (!ctx || kind < 0 || kind >= DUCTGPU_K_COUNT) return DUCTGPU_EARG;
+    profile_drain(ctx);
+    if (ms) *ms = ctx->prof_ms[kind];
+    if (launches) *launches = ctx->prof_n[kind];
+    return DUCTGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,342 @@
+// setup.cu -- one-time FP64 operator setup on the GPU: the reference's
+// pseudomat('d',m) and pseudomat('n',m) (src/pseudomat.f90:2-312).
+//
+// Collocation nodes, the CHQZ derivative matrix, D2 = D*D, the Dirichlet
+// interior block and the Neumann-eliminated block are built by small FP64
+// kernels; the non-symmetric eigen-decomposition (the reference's dgeev) is
+// cuSOLVER's Xgeev and the inverse (dgetrf/dgetri) is getrf + getrs against
+// the identity, all on the device.  Only iofzero (an argmin over n values)
+// and the 4x4 corner matrix AM1 are finished on the host.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "internal.h"
+
+namespace duct {
+
+// src/pseudomat.f90:72-107: nodes x_j = -cos(pi j/(m-1)) and
+// DC(l,j) = dd(l)/dd(j) (-1)^(l+j) / (x_l - x_j), diagonal per CHQZ.
+__global__ void k_build_dc(int m, double *x, double *DC)
+{
+    const double pi = 3.14159265358979323846;
+    const int n = m - 1;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < m * m;
+         idx += gridDim.x * blockDim.x) {
+        const int l = idx % m, j = idx / m;
+        const double xl = -cos(pi * (double)l / (double)n);
+        const double xj = -cos(pi * (double)j / (double)n);
+        if (j == 0) x[l] = xl;
+        double v;
+        if (l == j) {
+            if (l == 0) v = -(2.0 * (double)n * (double)n + 1.0) / 6.0;
+            else if (l == m - 1) v = (2.0 * (double)n * (double)n + 1.0) / 6.0;
+            else v = -0.5 * xl / (1.0 - xl * xl);
+        } else {
+            const double ddl = (l == 0 || l == m - 1) ? 2.0 : 1.0;
+            const double ddj = (j == 0 || j == m - 1) ? 2.0 : 1.0;
+            const double sgn = ((l + j) & 1) ? -1.0 : 1.0;
+            v = ddl / ddj * sgn / (xl - xj);
+        }
+        DC[l + (size_t)m * j] = v;
+    }
+}
+
+// C = A*B, m x m column-major (src/pseudomat.f90:110, D2 = DC*DC).
+__global__ void k_matmul(int m, const double *A, const double *B, double *C)
+{
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < m * m;
+         idx += gridDim.x * blockDim.x) {
+        const int i = idx % m, j = idx / m;
+        double s = 0.0;
+        for (int k = 0; k < m; ++k) s = fma(A[i + (size_t)m * k], B[k + (size_t)m * j], s);
+        C[idx] = s;
+    }
+}
+
+// Dirichlet interior block D2(2:m-1,2:m-1) (src/pseudomat.f90:232-240) or the
+// Neumann-eliminated block (src/pseudomat.f90:116-128).
+__global__ void k_block(int m, int neumann, const double *DC, const double *D2,
+                        double *B)
+{
+    const int n = m - 2;
+    const double d11 = DC[0], d1m = DC[(size_t)m * (m - 1)];
+    const double dm1 = DC[m - 1], dmm = DC[(m - 1) + (size_t)m * (m - 1)];
+    const double det = d11 * dmm - d1m * dm1;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n;
+         idx += gridDim.x * blockDim.x) {
+        const int ii = idx % n, jj = idx / n;
+        const int i = ii + 1, j = jj + 1;
+        double v = D2[i + (size_t)m * j];
+        if (neumann) {
+            const double ter1 = D2[i] * (d1m * DC[(m - 1) + (size_t)m * j] -
+                                         dmm * DC[(size_t)m * j]) / det;
+            const double ter3 = D2[i + (size_t)m * (m - 1)] *
+                                (dm1 * DC[(size_t)m * j] -
+                                 d11 * DC[(m - 1) + (size_t)m * j]) / det;
+            v = ter1 + v + ter3;
+        }
+        B[ii + (size_t)n * jj] = v;
+    }
+}
+
+__global__ void k_identity(int n, double *I)
+{
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n;
+         idx += gridDim.x * blockDim.x)
+        I[idx] = (idx % n == idx / n) ? 1.0 : 0.0;
+}
+
+// Real parts of the complex eigenvalues W (interleaved) into E.
+__global__ void k_real_part(int n, const double *W, double *E)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        E[i] = W[2 * i];
+}
+
+// Pack an n x n column-major matrix A into the A-operand fragment order of
+// mma.sync m16n8k8 f64: element (row g + 8*(v&1), col t + 4*(v>>1)) of
+// 16x8 tile (mt, ks) goes to lane g*4+t, value v, stored at
+// ((ks*mtiles + mt)*32 + lane)*4 + v.  Outside n x n the packing is zero.
+__global__ void k_pack_a(int n, int kpad, int mtiles, const double *A, double *out)
+{
+    const int total = (kpad / 8) * mtiles * 128;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += gridDim.x * blockDim.x) {
+        const int v = idx & 3, lane = (idx >> 2) & 31, tile = idx >> 7;
+        const int mt = tile % mtiles, ks = tile / mtiles;
+        const int g = lane >> 2, t = lane & 3;
+        const int row = mt * 16 + g + 8 * (v & 1);
+        const int col = ks * 8 + t + 4 * (v >> 1);
+        out[idx] = (row < n && col < n) ? A[row + (size_t)n * col] : 0.0;
+    }
+}
+
+__global__ void k_copy_col(int n, const double *P, int col, double *out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = P[i + (size_t)n * col];
+}
+
+static int blocks_for(long n) { return (int)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184); }
+
+void free_bound(BoundOps &b)
+{
+    cudaFree(b.E); cudaFree(b.P); cudaFree(b.PM1);
+    cudaFree(b.Ppack); cudaFree(b.Qpack); cudaFree(b.pcol);
+    b = BoundOps();
+}
+
+int pack_operators(ductgpu_ctx ctx, BoundOps &b)
+{
+    const int n = b.n;
+    b.kpad = (n + 31) / 32 * 32;
+    // 4 warps along M, each owning mtiles/4 tiles of 16 rows.
+    const int mt_per_warp = (n + 63) / 64;
+    b.mtiles = 4 * mt_per_warp;
+    const size_t packed = (size_t)(b.kpad / 8) * b.mtiles * 128;
+    cudaFree(b.Ppack);
+    cudaFree(b.Qpack);
+    b.Ppack = b.Qpack = nullptr;
+    DUCT_CUDA(ctx, cudaMalloc(&b.Ppack, packed * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&b.Qpack, packed * sizeof(double)));
+    k_pack_a<<<blocks_for((long)packed), 256, 0, ctx->stream>>>(n, b.kpad, b.mtiles, b.P, b.Ppack);
+    k_pack_a<<<blocks_for((long)packed), 256, 0, ctx->stream>>>(n, b.kpad, b.mtiles, b.PM1, b.Qpack);
+    ctx->launches += 2;
+    if (b.iofzero > 0) {
+        if (!b.pcol) DUCT_CUDA(ctx, cudaMalloc(&b.pcol, n * sizeof(double)));
+        k_copy_col<<<1, 256, 0, ctx->stream>>>(n, b.P, b.iofzero - 1, b.pcol);
+        ctx->launches += 1;
+    }
+    return check_cuda(ctx, cudaGetLastError(), "pack_operators");
+}
+
+// 4x4 inverse by Gauss-Jordan with partial pivoting (the reference inverts
+// AM1 with dgetrf/dgetri, src/pseudomat.f90:177-178).
+static bool invert4(double *A)
+{
+    double a[4][8];
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) {
+            a[r][c] = A[r + 4 * c];
+            a[r][c + 4] = (r == c) ? 1.0 : 0.0;
+        }
+    for (int c = 0; c < 4; ++c) {
+        int p = c;
+        for (int r = c + 1; r < 4; ++r)
+            if (fabs(a[r][c]) > fabs(a[p][c])) p = r;
+        if (a[p][c] == 0.0) return false;
+        if (p != c)
+            for (int k = 0; k < 8; ++k) { double t = a[p][k]; a[p][k] = a[c][k]; a[c][k] = t; }
+        const double inv = 1.0 / a[c][c];
+        for (int k = 0; k < 8; ++k) a[c][k] *= inv;
+        for (int r = 0; r < 4; ++r)
+            if (r != c) {
+                const double f = a[r][c];
+                for (int k = 0; k < 8; ++k) a[r][k] -= f * a[c][k];
+            }
+    }
+    for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c) A[r + 4 * c] = a[r][c + 4];
+    return true;
+}
+
+// Eigen-decomposition of the n x n block B (destroyed) into b.E, b.P, b.PM1.
+static int eigen_gpu(ductgpu_ctx ctx, int n, double *B, BoundOps &b)
+{
+    cusolverDnHandle_t h = ctx->solver;
+    cusolverDnParams_t params = nullptr;
+    if (cusolverDnCreateParams(&params) != CUSOLVER_STATUS_SUCCESS)
+        return set_error(ctx, DUCTGPU_ESOLVER, "cusolverDnCreateParams failed");
+    double *W = nullptr, *dbuf = nullptr;
+    int *dinfo = nullptr, *ipiv = nullptr;
+    void *hbuf = nullptr;
+    size_t dws = 0, hws = 0;
+    int rc = DUCTGPU_OK;
+    std::vector<double> Wh(2 * (size_t)n);
+    int info = 0;
+    cusolverStatus_t st;
+    if ((rc = check_cuda(ctx, cudaMalloc(&W, 2 * (size_t)n * sizeof(double)), "malloc W"))) goto out;
+    if ((rc = check_cuda(ctx, cudaMalloc(&dinfo, sizeof(int)), "malloc info"))) goto out;
+    st = cusolverDnXgeev_bufferSize(h, params, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_MODE_VECTOR,
+                                    n, CUDA_R_64F, B, n, CUDA_C_64F, W, CUDA_R_64F, nullptr, 1,
+                                    CUDA_R_64F, b.P, n, CUDA_R_64F, &dws, &hws);
+    if (st != CUSOLVER_STATUS_SUCCESS) { rc = set_error(ctx, DUCTGPU_ESOLVER, "Xgeev_bufferSize status %d", (int)st); goto out; }
+    if ((rc = check_cuda(ctx, cudaMalloc(&dbuf, dws + 16), "malloc geev work"))) goto out;
+    hbuf = malloc(hws + 16);
+    if (!hbuf) { rc = set_error(ctx, DUCTGPU_EALLOC, "host workspace"); goto out; }
+    st = cusolverDnXgeev(h, params, CUSOLVER_EIG_MODE_NOVECTOR, CUSOLVER_EIG_MODE_VECTOR, n,
+                         CUDA_R_64F, B, n, CUDA_C_64F, W, CUDA_R_64F, nullptr, 1, CUDA_R_64F,
+                         b.P, n, CUDA_R_64F, dbuf, dws, hbuf, hws, dinfo);
+    if (st != CUSOLVER_STATUS_SUCCESS) { rc = set_error(ctx, DUCTGPU_ESOLVER, "Xgeev status %d", (int)st); goto out; }
+    if ((rc = check_cuda(ctx, cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "info"))) goto out;
+    if ((rc = check_cuda(ctx, cudaMemcpyAsync(Wh.data(), W, 2 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "W"))) goto out;
+    if ((rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "geev sync"))) goto out;
+    if (info != 0) { rc = set_error(ctx, DUCTGPU_ESOLVER, "Xgeev info %d", info); goto out; }
+    {
+        // The Chebyshev D2 blocks have real spectra; a complex pair would mean
+        // a packed eigenvector layout this solver does not use.
+        double emax = 0.0, imax = 0.0;
+        for (int i = 0; i < n; ++i) {
+            emax = fmax(emax, fabs(Wh[2 * i]));
+            imax = fmax(imax, fabs(Wh[2 * i + 1]));
+        }
+        if (imax > 1e-6 * emax) { rc = set_error(ctx, DUCTGPU_ESOLVER, "complex eigenvalues (|im| %.3e)", imax); goto out; }
+    }
+    k_real_part<<<blocks_for(n), 256, 0, ctx->stream>>>(n, W, b.E);
+    // inverse of P: getrf + getrs(P, I)
+    {
+        int lwork = 0;
+        if (cusolverDnDgetrf_bufferSize(h, n, n, B, n, &lwork) != CUSOLVER_STATUS_SUCCESS) {
+            rc = set_error(ctx, DUCTGPU_ESOLVER, "getrf_bufferSize"); goto out;
+        }
+        cudaFree(dbuf); dbuf = nullptr;
+        if ((rc = check_cuda(ctx, cudaMalloc(&dbuf, ((size_t)lwork + 16) * sizeof(double)), "getrf work"))) goto out;
+        if ((rc = check_cuda(ctx, cudaMalloc(&ipiv, (size_t)n * sizeof(int)), "ipiv"))) goto out;
+        if ((rc = check_cuda(ctx, cudaMemcpyAsync(B, b.P, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream), "copy P"))) goto out;
+        k_identity<<<blocks_for((long)n * n), 256, 0, ctx->stream>>>(n, b.PM1);
+        ctx->launches += 2;
+        if (cusolverDnDgetrf(h, n, n, B, n, dbuf, ipiv, dinfo) != CUSOLVER_STATUS_SUCCESS) {
+            rc = set_error(ctx, DUCTGPU_ESOLVER, "getrf"); goto out;
+        }
+        if (cusolverDnDgetrs(h, CUBLAS_OP_N, n, n, B, n, ipiv, b.PM1, n, dinfo) != CUSOLVER_STATUS_SUCCESS) {
+            rc = set_error(ctx, DUCTGPU_ESOLVER, "getrs"); goto out;
+        }
+        if ((rc = check_cuda(ctx, cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "info"))) goto out;
+        if ((rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "getrs sync"))) goto out;
+        if (info != 0) { rc = set_error(ctx, DUCTGPU_ESOLVER, "getrf/getrs info %d", info); goto out; }
+    }
+    // iofzero: first index of the smallest |E| (src/pseudomat.f90:146-152)
+    {
+        double eigmin = 1.0e6;
+        b.iofzero = 0;
+        for (int i = 0; i < n; ++i) {
+            const double e = fmin(eigmin, fabs(Wh[2 * i]));
+            if (e != eigmin) { b.iofzero = i + 1; eigmin = e; }
+        }
+    }
+out:
+    cudaFree(W); cudaFree(dbuf); cudaFree(dinfo); cudaFree(ipiv);
+    free(hbuf);
+    cusolverDnDestroyParams(params);
+    return rc;
+}
+
+int pseudomat_gpu(ductgpu_ctx ctx, int m)
+{
+    if (m < 5 || m - 2 > kMaxN)
+        return set_error(ctx, DUCTGPU_EARG, "pseudomat: my=%d outside [5,%d]", m, kMaxN + 2);
+    const int n = m - 2;
+    cudaFree(ctx->xcol); cudaFree(ctx->DC); cudaFree(ctx->D2); cudaFree(ctx->AM1); cudaFree(ctx->ccw);
+    ctx->xcol = ctx->DC = ctx->D2 = ctx->AM1 = ctx->ccw = nullptr;
+    free_bound(ctx->dir);
+    free_bound(ctx->neu);
+    ctx->ready = false;
+    DUCT_CUDA(ctx, cudaMalloc(&ctx->xcol, m * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&ctx->DC, (size_t)m * m * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&ctx->D2, (size_t)m * m * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&ctx->AM1, 16 * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&ctx->ccw, m * sizeof(double)));
+    for (BoundOps *b : {&ctx->dir, &ctx->neu}) {
+        b->n = n;
+        DUCT_CUDA(ctx, cudaMalloc(&b->E, n * sizeof(double)));
+        DUCT_CUDA(ctx, cudaMalloc(&b->P, (size_t)n * n * sizeof(double)));
+        DUCT_CUDA(ctx, cudaMalloc(&b->PM1, (size_t)n * n * sizeof(double)));
+    }
+    double *blk = nullptr;
+    DUCT_CUDA(ctx, cudaMalloc(&blk, (size_t)n * n * sizeof(double)));
+    k_build_dc<<<blocks_for((long)m * m), 256, 0, ctx->stream>>>(m, ctx->xcol, ctx->DC);
+    k_matmul<<<blocks_for((long)m * m), 256, 0, ctx->stream>>>(m, ctx->DC, ctx->DC, ctx->D2);
+    k_block<<<blocks_for((long)n * n), 256, 0, ctx->stream>>>(m, 0, ctx->DC, ctx->D2, blk);
+    ctx->launches += 3;
+    int rc = eigen_gpu(ctx, n, blk, ctx->dir);
+    if (rc == DUCTGPU_OK) {
+        k_block<<<blocks_for((long)n * n), 256, 0, ctx->stream>>>(m, 1, ctx->DC, ctx->D2, blk);
+        ctx->launches += 1;
+        rc = eigen_gpu(ctx, n, blk, ctx->neu);
+    }
+    cudaFree(blk);
+    if (rc) return rc;
+    ctx->dir.iofzero = 0;  // only the Neumann operator pins a point
+    // AM1 (src/pseudomat.f90:158-178) from the four corner entries of DC.
+    double c4[4];
+    DUCT_CUDA(ctx, cudaMemcpyAsync(&c4[0], ctx->DC, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(&c4[1], ctx->DC + (size_t)m * (m - 1), sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(&c4[2], ctx->DC + (m - 1), sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(&c4[3], ctx->DC + (m - 1) + (size_t)m * (m - 1), sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const double d11 = c4[0], d1m = c4[1], dm1 = c4[2], dmm = c4[3];
+    double A[16] = {2.0 * d11, -dm1, 0.0, -dm1,
+                    d1m, d11 - dmm, dm1, 0.0,
+                    0.0, d1m, 2.0 * dmm, d1m,
+                    d1m, 0.0, dm1, d11 - dmm};
+    if (!invert4(A)) return set_error(ctx, DUCTGPU_ESOLVER, "AM1 singular");
+    // Clenshaw-Curtis weights of the CGL nodes (for the zero-mean gauge):
+    // w_j = c_j/N (1 - sum_{k=1}^{N/2} b_k cos(2 pi k j/N)/(4k^2-1)).
+    std::vector<double> w(m);
+    {
+        const int N = m - 1;
+        const double pi = 3.14159265358979323846;
+        for (int j = 0; j <= N; ++j) {
+            double s = 0.0;
+            for (int k = 1; k <= N / 2; ++k) {
+                const double bk = (2 * k == N) ? 1.0 : 2.0;
+                s += bk * cos(2.0 * pi * (double)k * (double)j / (double)N) / (4.0 * k * k - 1.0);
+            }
+            const double cj = (j == 0 || j == N) ? 1.0 : 2.0;
+            w[j] = cj / (double)N * (1.0 - s);
+        }
+    }
+    DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->AM1, A, 16 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->ccw, w.data(), m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = pack_operators(ctx, ctx->dir))) return rc;
+    if ((rc = pack_operators(ctx, ctx->neu))) return rc;
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->my = ctx->mz = m;
+    ctx->ready = true;
+    return DUCTGPU_OK;
+}
+
+}  // namespace duct

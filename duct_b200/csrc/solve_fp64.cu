@@ -1,0 +1,541 @@
+// solve_fp64.cu -- plain FP64 diagonalisation solve on the B200 FP64 tensor
+// cores (mma.sync m16n8k8 f64, "DMMA"; tcgen05 has no f64 kind).
+//
+// The reference solves one real plane at a time with four dgemm calls, two
+// explicit transposes and a divide (src/solvediag.f90:47-80, GPU variant
+// :82-128 with cublasDgemm, transpose_gpu and mat_invdiag):
+//     U = P [ (P^-1 F P^-T) / (E_i + E_j - lambda) ] P^T .
+// Here every plane of every field goes through four batched passes, each a
+// GEMM of a fixed n x n operator against many short "lines" of the field:
+//     y-pass  out(o, z) = sum_y A(o,y) in(y, z)      (A = P^-1, then P)
+//     z-pass  out(y, o) = sum_z A(o,z) in(y, z)      (A = P^-1 with the
+//                          eigenvalue divide fused in the epilogue, then P)
+// The complex field is never de-interleaved in memory: a CTA stages 32
+// complex lines (64 real columns: re and im side by side) of one plane in
+// shared memory and multiplies the whole padded operator against them, so
+// the transposes of the reference disappear into the addressing.  The
+// operator streams through shared memory in K chunks of 32 with cp.async,
+// pre-packed in the DMMA A-fragment order (one 16-byte load per fragment
+// half, no bank conflicts).
+#include <math.h>
+
+#include "internal.h"
+
+namespace duct {
+
+constexpr int kLines = 32;   // complex lines per CTA
+constexpr int kNld = 68;     // leading dim of the staged tile (64 + 4 pad)
+constexpr int kKC = 32;      // K chunk of the streamed operator
+constexpr int kThreads = 256;
+
+struct PassField {
+    const double *src;
+    double *dst;
+    const double *A;     // packed operator
+    const double *E;     // eigenvalues for the divide
+    int nmodes;
+    int mode0;
+    int plane0;
+    int sing_io;         // 0-based iofzero of a Neumann field, else -1
+};
+
+struct PassParams {
+    PassField f[kMaxFields];
+    int cta_start[kMaxFields + 1];
+    int nf;
+    const double *lam;
+    long long plane_stride;  // doubles per complex plane
+    int n, kpad, nchunks;
+    int sk, sl;              // complex strides of (k, line)
+    int divide;
+    int zero_im_mode0;
+};
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma(double (&d)[4], const double (&a)[4], const double (&b)[2])
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 "
+        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+template <int MTW>
+__global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ PassParams p)
+{
+    extern __shared__ __align__(16) double smem[];
+    constexpr int mtiles = 4 * MTW;
+    constexpr int a_chunk = (kKC / 8) * mtiles * 128;
+    double *As = smem;
+    double *Bs = smem + 2 * a_chunk;
+
+    int fi = 0;
+    while (fi + 1 < p.nf && (int)blockIdx.x >= p.cta_start[fi + 1]) ++fi;
+    const PassField &F = p.f[fi];
+    const int local = blockIdx.x - p.cta_start[fi];
+    const int plane = local / p.nchunks;
+    const int chunk = local - plane * p.nchunks;
+    const int l0 = chunk * kLines;
+    const int L = min(kLines, p.n - l0);
+    const double *src = F.src + (long long)plane * p.plane_stride;
+    double *dst = F.dst + (long long)plane * p.plane_stride;
+    const int tid = threadIdx.x;
+    const int nkc = p.kpad / kKC;
+
+    auto load_a = [&](int c, int buf) {
+        const double *g = F.A + (size_t)c * a_chunk;
+        double *s = As + buf * a_chunk;
+        for (int i = tid * 2; i < a_chunk; i += kThreads * 2) cp_async16(s + i, g + i);
+        cp_async_commit();
+    };
+    load_a(0, 0);
+
+    // Stage the lines: Bs[k][2l + c] = in(k, l0 + l) component c, zero padded.
+    const int n = p.n, sk = p.sk, sl = p.sl;
+    if (sk == 1) {
+        for (int idx = tid; idx < p.kpad * kLines; idx += kThreads) {
+            const int k = idx % p.kpad, l = idx / p.kpad;
+            double2 v = make_double2(0.0, 0.0);
+            if (k < n && l < L)
+                v = *reinterpret_cast<const double2 *>(src + 2 * ((long long)(k + 1) * sk + (long long)(l0 + l + 1) * sl));
+            *reinterpret_cast<double2 *>(Bs + k * kNld + 2 * l) = v;
+        }
+    } else {
+        for (int idx = tid; idx < p.kpad * kLines; idx += kThreads) {
+            const int l = idx % kLines, k = idx / kLines;
+            double2 v = make_double2(0.0, 0.0);
+            if (k < n && l < L)
+                v = *reinterpret_cast<const double2 *>(src + 2 * ((long long)(k + 1) * sk + (long long)(l0 + l + 1) * sl));
+            *reinterpret_cast<double2 *>(Bs + k * kNld + 2 * l) = v;
+        }
+    }
+
+    const int lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 3, wn = warp >> 2;
+    const int g = lane >> 2, t = lane & 3;
+    double acc[MTW][4][4];
+#pragma unroll
+    for (int i = 0; i < MTW; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+
+    for (int c = 0; c < nkc; ++c) {
+        if (c + 1 < nkc) {
+            load_a(c + 1, (c + 1) & 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double *Ab = As + (c & 1) * a_chunk;
+#pragma unroll
+        for (int ks = 0; ks < kKC / 8; ++ks) {
+            double a[MTW][4];
+#pragma unroll
+            for (int mt = 0; mt < MTW; ++mt) {
+                const double2 *q = reinterpret_cast<const double2 *>(
+                    Ab + ((ks * mtiles + wm * MTW + mt) * 32 + lane) * 4);
+                const double2 q0 = q[0], q1 = q[1];
+                a[mt][0] = q0.x; a[mt][1] = q0.y; a[mt][2] = q1.x; a[mt][3] = q1.y;
+            }
+            const int kg = c * kKC + ks * 8 + t;
+            double b[4][2];
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                const int col = wn * 32 + nt * 8 + g;
+                b[nt][0] = Bs[kg * kNld + col];
+                b[nt][1] = Bs[(kg + 4) * kNld + col];
+            }
+#pragma unroll
+            for (int mt = 0; mt < MTW; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt], a[mt], b[nt]);
+        }
+        __syncthreads();
+    }
+
+    // Epilogue: rows of the accumulator are the output index o, column pairs
+    // (2t, 2t+1) are (re, im) of line l.
+    const double lam = p.lam[F.plane0 + plane];
+    const bool singular = (F.sing_io >= 0) && fabs(lam) <= 1.0e-10;
+    const bool im0 = p.zero_im_mode0 && F.mode0 && plane == 0;
+#pragma unroll
+    for (int mt = 0; mt < MTW; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const int l = wn * 16 + nt * 4 + t;
+            if (l >= L) continue;
+            const int lg = l0 + l;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int o = (wm * MTW + mt) * 16 + g + 8 * h;
+                if (o >= n) continue;
+                double re = acc[mt][nt][2 * h], im = acc[mt][nt][2 * h + 1];
+                if (p.divide) {
+                    if (singular && o == F.sing_io && lg == F.sing_io) {
+                        re = 0.0;
+                        im = 0.0;
+                    } else {
+                        const double den = (F.E[o] + F.E[lg]) - lam;
+                        re = re / den;
+                        im = im / den;
+                    }
+                }
+                if (im0) im = 0.0;
+                *reinterpret_cast<double2 *>(dst + 2 * ((long long)(o + 1) * sk + (long long)(lg + 1) * sl)) =
+                    make_double2(re, im);
+            }
+        }
+}
+
+static size_t pass_smem_bytes(int mtw, int kpad)
+{
+    const size_t a_chunk = (size_t)(kKC / 8) * (4 * mtw) * 128;
+    return (2 * a_chunk + (size_t)kpad * kNld) * sizeof(double);
+}
+
+template <int MTW>
+static cudaError_t launch_pass(ductgpu_ctx ctx, const PassParams &pp, int grid)
+{
+    const size_t smem = pass_smem_bytes(MTW, pp.kpad);
+    cudaError_t e = cudaFuncSetAttribute(k_pass_fp64<MTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    LaunchScope ls(ctx, DUCTGPU_K_PASS_FP64);
+    k_pass_fp64<MTW><<<grid, kThreads, smem, ctx->stream>>>(pp);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Walls of Dirichlet fields: helm3d zeroes the four wall lines of rhs in
+// place (src/helm3d.f90:48-60) and the solution keeps them
+// (src/solvediag.f90:131-135 writes only the interior); mode 0 has a zero
+// imaginary part everywhere (src/int2d3d.f90:91-96).
+struct WallParams {
+    double *rhs[kMaxFields];
+    double *sol[kMaxFields];
+    int cta_start[kMaxFields + 1];
+    int nf;
+    int m;
+    long long plane_stride;
+};
+
+__global__ void k_zero_walls(const __grid_constant__ WallParams p)
+{
+    int fi = 0;
+    while (fi + 1 < p.nf && (int)blockIdx.x >= p.cta_start[fi + 1]) ++fi;
+    const int plane = blockIdx.x - p.cta_start[fi];
+    const int m = p.m;
+    double *r = p.rhs[fi] + (long long)plane * p.plane_stride;
+    double *s = p.sol[fi] + (long long)plane * p.plane_stride;
+    for (int i = threadIdx.x; i < 4 * m; i += blockDim.x) {
+        const int side = i / m, q = i % m;
+        long long off;
+        if (side == 0) off = q;                           // U(q,1)
+        else if (side == 1) off = q + (long long)m * (m - 1);  // U(q,m)
+        else if (side == 2) off = (long long)m * q;       // U(1,q)
+        else off = (m - 1) + (long long)m * q;            // U(m,q)
+        const double2 z = make_double2(0.0, 0.0);
+        *reinterpret_cast<double2 *>(r + 2 * off) = z;
+        *reinterpret_cast<double2 *>(s + 2 * off) = z;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Neumann walls, corners and the singular kx=0 mode: src/solvediag.f90:
+// 161-206 (pin), 250-276 (wall lines from DC), 278-322 (corners via AM1).
+// One CTA per complex plane; the interior is already solved.
+struct FillParams {
+    double *sol[kMaxFields];
+    int mode0[kMaxFields];
+    int plane0[kMaxFields];
+    int cta_start[kMaxFields + 1];
+    int nf;
+    const double *DC, *AM1, *ccw, *pcol, *lam;
+    double wanted;
+    int m, io, gauge;
+    long long plane_stride;
+};
+
+__device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 operator*(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+
+template <int NV>
+__device__ void block_sum(double (&v)[NV], double *red)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int i = 0; i < NV; ++i)
+        for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
+    __syncthreads();
+    if (lane == 0)
+        for (int i = 0; i < NV; ++i) red[warp * NV + i] = v[i];
+    __syncthreads();
+    for (int i = 0; i < NV; ++i) {
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += red[w * NV + i];
+        v[i] = s;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_neumann_fill(const __grid_constant__ FillParams p)
+{
+    __shared__ double red[8 * 8];
+    int fi = 0;
+    while (fi + 1 < p.nf && (int)blockIdx.x >= p.cta_start[fi + 1]) ++fi;
+    const int plane = blockIdx.x - p.cta_start[fi];
+    const int m = p.m, n = m - 2;
+    double2 *U = reinterpret_cast<double2 *>(p.sol[fi] + (long long)plane * p.plane_stride);
+    const double lam = p.lam[p.plane0[fi] + plane];
+    const bool mode0 = p.mode0[fi] && plane == 0;
+    const bool singular = fabs(lam) <= 1.0e-10 && p.io >= 0;
+    const double *DC = p.DC;
+    auto u = [&](int i, int j) -> double2 & { return U[i + (long long)m * j]; };
+
+    if (singular) {
+        // U = U0 + c p p^T with c = (wanted - U0(io,io)) / p(io)^2: the value
+        // of the solution at interior point (iofzero+1, iofzero+1) becomes
+        // wanted (the reference's FT(iofzero,iofzero) choice).
+        const int io = p.io;
+        const double2 u0 = u(io + 1, io + 1);
+        __syncthreads();
+        const double pio = p.pcol[io];
+        const double2 cc = make_double2((p.wanted - u0.x) / (pio * pio), (p.wanted - u0.y) / (pio * pio));
+        for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+            const int i = idx % n, j = idx / n;
+            u(i + 1, j + 1) = u(i + 1, j + 1) + (p.pcol[i] * p.pcol[j]) * cc;
+        }
+        __syncthreads();
+    }
+    const double d11 = DC[0], d1m = DC[(long long)m * (m - 1)];
+    const double dm1 = DC[m - 1], dmm = DC[(m - 1) + (long long)m * (m - 1)];
+    const double det = d11 * dmm - d1m * dm1;
+    // z-walls U(i,1), U(i,m) of each interior row i: sums over j, one thread per i.
+    for (int i = 1 + threadIdx.x; i < m - 1; i += blockDim.x) {
+        double2 sb = make_double2(0.0, 0.0), st = sb;
+        for (int j = 1; j < m - 1; ++j) {
+            const double2 v = u(i, j);
+            sb = sb + DC[(long long)m * j] * v;
+            st = st + DC[(m - 1) + (long long)m * j] * v;
+        }
+        u(i, 0) = (-dmm) * sb + d1m * st;
+        u(i, 0) = make_double2(u(i, 0).x / det, u(i, 0).y / det);
+        double2 w = dm1 * sb + (-d11) * st;
+        u(i, m - 1) = make_double2(w.x / det, w.y / det);
+    }
+    // y-walls U(1,j), U(m,j) of each interior column j: one warp per j.
+    {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (int j = 1 + warp; j < m - 1; j += nw) {
+            double sl[4] = {0, 0, 0, 0};
+            for (int i = 1 + lane; i < m - 1; i += 32) {
+                const double2 v = u(i, j);
+                const double a = DC[(long long)m * i], b = DC[(m - 1) + (long long)m * i];
+                sl[0] += a * v.x; sl[1] += a * v.y; sl[2] += b * v.x; sl[3] += b * v.y;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                for (int o = 16; o > 0; o >>= 1) sl[q] += __shfl_xor_sync(0xffffffffu, sl[q], o);
+            if (lane == 0) {
+                u(0, j) = make_double2((-dmm * sl[0] + d1m * sl[2]) / det, (-dmm * sl[1] + d1m * sl[3]) / det);
+                u(m - 1, j) = make_double2((dm1 * sl[0] - d11 * sl[2]) / det, (dm1 * sl[1] - d11 * sl[3]) / det);
+            }
+        }
+    }
+    __syncthreads();
+    // corners
+    {
+        double f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = 1 + threadIdx.x; i < m - 1; i += blockDim.x) {
+            const double a = DC[(long long)m * i], b = DC[(m - 1) + (long long)m * i];
+            const double2 ui0 = u(i, 0), u0i = u(0, i), umi = u(m - 1, i), uim = u(i, m - 1);
+            f[0] += -a * (ui0.x + u0i.x);            f[1] += -a * (ui0.y + u0i.y);
+            f[2] += -a * umi.x + b * ui0.x;          f[3] += -a * umi.y + b * ui0.y;
+            f[4] += -b * (uim.x + umi.x);            f[5] += -b * (uim.y + umi.y);
+            f[6] += -a * uim.x + b * u0i.x;          f[7] += -a * uim.y + b * u0i.y;
+        }
+        block_sum<8>(f, red);
+        if (threadIdx.x == 0) {
+            const double *A = p.AM1;
+            double c[8];
+            for (int r = 0; r < 4; ++r) {
+                c[2 * r] = c[2 * r + 1] = 0.0;
+                for (int i = 0; i < 4; ++i) {
+                    c[2 * r] += A[r + 4 * i] * f[2 * i];
+                    c[2 * r + 1] += A[r + 4 * i] * f[2 * i + 1];
+                }
+            }
+            u(0, 0) = make_double2(c[0], c[1]);
+            u(m - 1, 0) = make_double2(c[2], c[3]);
+            u(m - 1, m - 1) = make_double2(c[4], c[5]);
+            u(0, m - 1) = make_double2(c[6], c[7]);
+        }
+        __syncthreads();
+    }
+    if (singular && p.gauge == DUCTGPU_GAUGE_MEAN) {
+        // Zero mean over [-1,1]^2 with the Clenshaw-Curtis weights of the
+        // nodes: subtract integral/4 (a constant keeps the Neumann walls).
+        double s[2] = {0.0, 0.0};
+        for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+            const int i = idx % m, j = idx / m;
+            const double w = p.ccw[i] * p.ccw[j];
+            const double2 v = u(i, j);
+            s[0] += w * v.x;
+            s[1] += w * v.y;
+        }
+        block_sum<2>(s, red);
+        for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+            const int i = idx % m, j = idx / m;
+            u(i, j) = make_double2(u(i, j).x - 0.25 * s[0], u(i, j).y - 0.25 * s[1]);
+        }
+        __syncthreads();
+    }
+    if (mode0)
+        for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+            const int i = idx % m, j = idx / m;
+            u(i, j).y = 0.0;
+        }
+}
+
+// ---------------------------------------------------------------------------
+
+static int plane_count(const FieldTask *t, int nt)
+{
+    int s = 0;
+    for (int i = 0; i < nt; ++i) s += t[i].nmodes;
+    return s;
+}
+
+int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
+{
+    if (ntasks < 1 || ntasks > kMaxFields)
+        return set_error(ctx, DUCTGPU_EARG, "solve: %d fields (1..%d)", ntasks, kMaxFields);
+    const int m = ctx->my, n = m - 2;
+    const long long ps = 2LL * m * m;
+    const int planes = plane_count(tasks, ntasks);
+    int rc = ensure(ctx, ctx->work, (size_t)2 * planes * ps * sizeof(double));
+    if (rc) return rc;
+    double *w1 = ctx->work.buf;
+    double *w2 = w1 + (size_t)planes * ps;
+
+    const int mtw = (n + 63) / 64;
+    const BoundOps &ref = ctx->dir;
+    PassParams pp{};
+    pp.nf = ntasks;
+    pp.lam = ctx->lam;
+    pp.plane_stride = ps;
+    pp.n = n;
+    pp.kpad = ref.kpad;
+    pp.nchunks = (n + kLines - 1) / kLines;
+    int cta = 0;
+    long long off = 0;
+    for (int i = 0; i < ntasks; ++i) {
+        pp.cta_start[i] = cta;
+        cta += tasks[i].nmodes * pp.nchunks;
+        pp.f[i].nmodes = tasks[i].nmodes;
+        pp.f[i].mode0 = tasks[i].mode0;
+        pp.f[i].plane0 = tasks[i].plane0;
+        pp.f[i].sing_io = (tasks[i].bound == 'n') ? ctx->neu.iofzero - 1 : -1;
+    }
+    pp.cta_start[ntasks] = cta;
+
+    // pass 1 (y, P^-1): rhs -> w1 ; pass 2 (z, P^-1, divide): w1 -> w2 ;
+    // pass 3 (z, P): w2 -> w1 ; pass 4 (y, P): w1 -> sol
+    for (int pass = 0; pass < 4; ++pass) {
+        off = 0;
+        for (int i = 0; i < ntasks; ++i) {
+            const BoundOps &b = (tasks[i].bound == 'n') ? ctx->neu : ctx->dir;
+            double *a1 = w1 + off * ps, *a2 = w2 + off * ps;
+            off += tasks[i].nmodes;
+            switch (pass) {
+            case 0: pp.f[i].src = tasks[i].rhs; pp.f[i].dst = a1; pp.f[i].A = b.Qpack; break;
+            case 1: pp.f[i].src = a1; pp.f[i].dst = a2; pp.f[i].A = b.Qpack; break;
+            case 2: pp.f[i].src = a2; pp.f[i].dst = a1; pp.f[i].A = b.Ppack; break;
+            default: pp.f[i].src = a1; pp.f[i].dst = tasks[i].sol; pp.f[i].A = b.Ppack; break;
+            }
+            pp.f[i].E = b.E;
+        }
+        const bool ypass = (pass == 0 || pass == 3);
+        pp.sk = ypass ? 1 : m;
+        pp.sl = ypass ? m : 1;
+        pp.divide = (pass == 1);
+        pp.zero_im_mode0 = (pass == 3);
+        cudaError_t e;
+        switch (mtw) {
+        case 1: e = launch_pass<1>(ctx, pp, cta); break;
+        case 2: e = launch_pass<2>(ctx, pp, cta); break;
+        default: e = launch_pass<3>(ctx, pp, cta); break;
+        }
+        if (e != cudaSuccess) return check_cuda(ctx, e, "k_pass_fp64");
+    }
+    if ((rc = zero_walls(ctx, tasks, ntasks))) return rc;
+    return neumann_fill(ctx, tasks, ntasks);
+}
+
+int zero_walls(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
+{
+    WallParams wp{};
+    int cta = 0;
+    for (int i = 0; i < ntasks; ++i) {
+        if (tasks[i].bound != 'd') continue;
+        wp.rhs[wp.nf] = tasks[i].rhs;
+        wp.sol[wp.nf] = tasks[i].sol;
+        wp.cta_start[wp.nf] = cta;
+        cta += tasks[i].nmodes;
+        wp.nf++;
+    }
+    if (!wp.nf) return DUCTGPU_OK;
+    wp.cta_start[wp.nf] = cta;
+    wp.m = ctx->my;
+    wp.plane_stride = 2LL * ctx->my * ctx->my;
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_WALLS);
+        k_zero_walls<<<cta, 128, 0, ctx->stream>>>(wp);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "k_zero_walls");
+}
+
+int neumann_fill(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
+{
+    FillParams fp{};
+    int cta = 0;
+    for (int i = 0; i < ntasks; ++i) {
+        if (tasks[i].bound != 'n') continue;
+        fp.sol[fp.nf] = tasks[i].sol;
+        fp.mode0[fp.nf] = tasks[i].mode0;
+        fp.plane0[fp.nf] = tasks[i].plane0;
+        fp.cta_start[fp.nf] = cta;
+        cta += tasks[i].nmodes;
+        fp.nf++;
+    }
+    if (!fp.nf) return DUCTGPU_OK;
+    fp.cta_start[fp.nf] = cta;
+    fp.DC = ctx->DC;
+    fp.AM1 = ctx->AM1;
+    fp.ccw = ctx->ccw;
+    fp.pcol = ctx->neu.pcol;
+    fp.lam = ctx->lam;
+    fp.wanted = ctx->wanted;
+    fp.m = ctx->my;
+    fp.io = ctx->neu.iofzero - 1;
+    fp.gauge = ctx->gauge;
+    fp.plane_stride = 2LL * ctx->my * ctx->my;
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
+        k_neumann_fill<<<cta, 256, 0, ctx->stream>>>(fp);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "k_neumann_fill");
+}
+
+}  // namespace duct

@@ -1,0 +1,155 @@
+/*
+ * ductgpu.h -- C-ABI of libductgpu, the B200 (sm_100a) implementation of the
+ * duct per-Fourier-mode 2D Helmholtz/Poisson diagonalisation solve, its
+ * Chebyshev transforms and pencil transposes.
+ *
+ * Plain C types only: pointers, sizes, doubles, chars.  Every entry returns
+ * an int status (DUCTGPU_OK = 0); the message of the last failure is read
+ * with ductgpu_last_error().  No entry aborts the process.
+ *
+ * Array conventions are the reference's: column-major (Fortran) order, y
+ * fastest; a complex field rhs(my,mz,ib:ie) is my*mz*(ie-ib+1) interleaved
+ * (re, im) doubles.  "host" entries take host arrays and copy them to and
+ * from the GPU inside the call; "_dev" entries take device pointers.
+ *
+ * A context is bound to one device and one CUDA stream; calls on one
+ * context are serialised by the caller (not re-entrant); separate contexts
+ * may be driven from separate threads.
+ */
+#ifndef DUCTGPU_H
+#define DUCTGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ductgpu_ctx_s *ductgpu_ctx;
+
+/* status codes */
+#define DUCTGPU_OK 0
+#define DUCTGPU_EARG 1       /* bad size, bound character, null pointer     */
+#define DUCTGPU_ESTATE 2     /* operators not set up (pseudomat not called)  */
+#define DUCTGPU_ECUDA 3      /* CUDA runtime error                           */
+#define DUCTGPU_ESOLVER 4    /* eigen-decomposition / inversion failure      */
+#define DUCTGPU_ENONFINITE 5 /* NaN/Inf in a result                          */
+#define DUCTGPU_ETIMEOUT 6   /* a bounded device-side wait ran out           */
+#define DUCTGPU_EALLOC 7     /* device or host allocation failure            */
+
+/* arithmetic of the solve */
+#define DUCTGPU_PREC_FP64 0  /* plain FP64 (DMMA tensor cores): the drop-in  */
+#define DUCTGPU_PREC_MIXED 1 /* BF16 split GEMMs + FP64 refinement           */
+
+/* gauge of the singular kx=0 Neumann (pressure) mode */
+#define DUCTGPU_GAUGE_POINT 0 /* reference: U(iofzero+1,iofzero+1)=wanted=0 */
+#define DUCTGPU_GAUGE_MEAN 1  /* zero mean over the duct cross-section      */
+
+/* ---- context --------------------------------------------------------- */
+/* Replaces the gpudevice module state (src/mod.f90:409-483) and the
+ * cuBLAS/cuSPARSE handle creation of src/pseudomat.f90:265-298.           */
+int ductgpu_create(int device, ductgpu_ctx *out);
+int ductgpu_destroy(ductgpu_ctx ctx);
+/* Copies the message of the last failure (NUL-terminated) into buf.       */
+int ductgpu_last_error(ductgpu_ctx ctx, char *buf, int len);
+/* Launch all work of ctx on this cudaStream_t (NULL: the context's own).  */
+int ductgpu_set_stream(ductgpu_ctx ctx, void *cuda_stream);
+/* Returns the stream work is launched on (for events around a call).      */
+void *ductgpu_get_stream(ductgpu_ctx ctx);
+int ductgpu_synchronize(ductgpu_ctx ctx);
+
+/* ---- setup (one-time) ------------------------------------------------- */
+/* pseudomat('d',my) then pseudomat('n',my) (src/pseudomat.f90:2-312, called
+ * from helm3d with ipro<=0, src/helm3d.f90:36-46), computed on the GPU in
+ * FP64: collocation nodes and derivative matrix, D2=D*D, Dirichlet interior
+ * block and Neumann-eliminated block, their eigen-decomposition, inverses,
+ * iofzero and the 4x4 corner matrix AM1.  my must equal mz (the square
+ * solver stops otherwise, src/helm3d.f90:37-41).                          */
+int ductgpu_pseudomat(ductgpu_ctx ctx, int my, int mz);
+
+/* Read back the operators of bound 'd' or 'n' (n = my-2):  E[n] eigenvalues,
+ * P[n*n] eigenvectors, PM1[n*n] inverse (column-major), iofzero (1-based,
+ * Neumann).  Any output pointer may be NULL.                              */
+int ductgpu_get_operators(ductgpu_ctx ctx, char bound, double *E, double *P,
+                          double *PM1, int *iofzero);
+
+/* Replace the eigen-decomposition of bound 'd' or 'n' with host data, e.g.
+ * the LAPACK results of the reference's own pseudomat.  Requires a prior
+ * ductgpu_pseudomat for the grid.  iofzero <= 0 recomputes it from E.     */
+int ductgpu_set_operators(ductgpu_ctx ctx, char bound, const double *E,
+                          const double *P, const double *PM1, int iofzero);
+
+/* Gauge of the singular kx=0 Neumann mode (reference default: POINT).     */
+int ductgpu_set_gauge(ductgpu_ctx ctx, int gauge);
+
+/* ---- the 2D solve ------------------------------------------------------ */
+/* helm3d(rhs,sol,work,ipro,bound,cvar,a,b,alambda), src/helm3d.f90:2-76,
+ * for one field on host arrays: solves lap(u) - (alambda + xalp(i)^2) u = f
+ * for every mode i = ib..ie (xalp[i-ib] = kx of mode i).  Same observable
+ * effects as the reference: rhs walls zeroed in place for bound 'd', mode
+ * 0 returns a real solution (src/int2d3d.f90:43,91-96), Neumann walls and
+ * corners filled (src/solvediag.f90:250-322), kx=0 Neumann mode pinned.
+ * ipro <= 0 runs the setup first; ipro == -1 only runs the setup.         */
+int ductgpu_helm3d(ductgpu_ctx ctx, double *rhs, double *sol, int ipro,
+                   char bound, double alambda, int my, int mz, int ib,
+                   int ie, const double *xalp, int precision);
+
+/* One field of a batched device-resident solve. */
+typedef struct {
+    double *rhs;         /* device, complex (my,mz,nmodes); walls zeroed in
+                            place for bound 'd' like helm3d               */
+    double *sol;         /* device, complex (my,mz,nmodes)                 */
+    const double *xalp;  /* HOST, nmodes wavenumbers                       */
+    double alambda;
+    int ib;              /* mode number of the first plane (0: real only)  */
+    int nmodes;
+    char bound;          /* 'd' or 'n'                                     */
+} ductgpu_field;
+
+/* All fields (each a helm3d call of the reference, e.g. u, v, w and the
+ * pressure of one RK substep, src/main1.f90:617-619,643) in one batched
+ * launch sequence on the context's stream.  Asynchronous: returns once the
+ * work is queued.                                                          */
+int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields,
+                             int nfields, int precision);
+
+/* ---- memory helpers (for callers without a CUDA toolchain, e.g. Fortran
+ * hosts that keep fields resident on the device between time steps) ---- */
+int ductgpu_device_alloc(ductgpu_ctx ctx, size_t bytes, void **ptr);
+int ductgpu_device_free(ductgpu_ctx ctx, void *ptr);
+/* pinned host memory: host<->device copies from it run at full link speed */
+int ductgpu_host_alloc(ductgpu_ctx ctx, size_t bytes, void **ptr);
+int ductgpu_host_free(ductgpu_ctx ctx, void *ptr);
+/* asynchronous copies on the context stream (kind: 1 = H2D, 2 = D2H,
+ * 3 = D2D, as cudaMemcpyKind)                                              */
+int ductgpu_copy(ductgpu_ctx ctx, void *dst, const void *src, size_t bytes, int kind);
+
+/* ---- timing helpers for benchmarks (CUDA events on the ctx stream) ---- */
+int ductgpu_event_record(ductgpu_ctx ctx, int slot);
+/* milliseconds between two recorded slots (synchronises on the later). */
+int ductgpu_event_elapsed(ductgpu_ctx ctx, int slot0, int slot1, float *ms);
+
+/* Count of kernels this library launched on ctx since creation.           */
+long long ductgpu_launch_count(ductgpu_ctx ctx);
+
+/* Per-kernel device time: with profiling on, every launch of the library is
+ * bracketed by CUDA events on the ctx stream.  ductgpu_profile_read
+ * synchronises and returns, for kernel class `kind` (DUCTGPU_K_*), the
+ * summed milliseconds and launch count since the last reset.               */
+#define DUCTGPU_K_PASS_FP64 0   /* FP64 DMMA GEMM pass                      */
+#define DUCTGPU_K_NEUMANN 1     /* Neumann walls/corners/pin                */
+#define DUCTGPU_K_WALLS 2       /* Dirichlet wall zeroing                   */
+#define DUCTGPU_K_MIXED_GEMM 3  /* split-precision tcgen05 GEMM pass        */
+#define DUCTGPU_K_RESIDUAL 4    /* FP64 refinement residual                 */
+#define DUCTGPU_K_TRANSFORM 5   /* Chebyshev transforms / derivatives       */
+#define DUCTGPU_K_TRANSPOSE 6   /* pencil transposes                        */
+#define DUCTGPU_K_OTHER 7
+#define DUCTGPU_K_COUNT 8
+int ductgpu_profile_enable(ductgpu_ctx ctx, int on);
+int ductgpu_profile_reset(ductgpu_ctx ctx);
+int ductgpu_profile_read(ductgpu_ctx ctx, int kind, double *ms, long long *launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,588 @@
+/*
+ * duct_oracle.c -- CPU FP64 restatement of the duct reference hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (checker and CPU baseline; see duct_oracle.h for
+ * the parity-pin statement).  Each function cites the reference routine it
+ * restates.  LAPACK/BLAS come from the OpenBLAS build bundled with SciPy
+ * (symbols scipy_dgeev_, scipy_dgetrf_, scipy_dgetri_, scipy_dgemm_), i.e.
+ * the same routines the reference calls (src/pseudomat.f90:110,131,141-142,
+ * 244,254-255; src/solvediag.f90:51-80,140-219).
+ */
+#include "duct_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ---- LAPACK / BLAS (gfortran ABI: trailing hidden string lengths) ------- */
+extern void scipy_dgeev_(const char *jobvl, const char *jobvr, const int *n,
+                         double *a, const int *lda, double *wr, double *wi,
+                         double *vl, const int *ldvl, double *vr,
+                         const int *ldvr, double *work, const int *lwork,
+                         int *info, size_t, size_t);
+extern void scipy_dgetrf_(const int *m, const int *n, double *a,
+                          const int *lda, int *ipiv, int *info);
+extern void scipy_dgetri_(const int *n, double *a, const int *lda,
+                          const int *ipiv, double *work, const int *lwork,
+                          int *info);
+extern void scipy_dgemm_(const char *ta, const char *tb, const int *m,
+                         const int *n, const int *k, const double *alpha,
+                         const double *a, const int *lda, const double *b,
+                         const int *ldb, const double *beta, double *c,
+                         const int *ldc, size_t, size_t);
+extern void scipy_openblas_set_num_threads(int);
+
+void orc_set_blas_threads(int n) { scipy_openblas_set_num_threads(n); }
+
+#define IX(i, j, ld) ((size_t)(i) + (size_t)(j) * (size_t)(ld))
+
+static void dgemm_tn(int n, const double *A, const double *B, double *C)
+{
+    /* C = A^T * B, all n x n with leading dimension n (the reference's
+     * dgemm('t','n',mm2+1,...) calls).                                      */
+    const double one = 1.0, zero = 0.0;
+    scipy_dgemm_("t", "n", &n, &n, &n, &one, A, &n, B, &n, &zero, C, &n, 1, 1);
+}
+
+static int invert(int n, double *A)
+{
+    /* dgetrf + dgetri, as src/pseudomat.f90:141-142, 254-255, 177-178.      */
+    int info = 0, lwk = 64 * (n > 4 ? n : 4);
+    int *ipiv = (int *)malloc(sizeof(int) * (size_t)n);
+    double *wk = (double *)malloc(sizeof(double) * (size_t)lwk);
+    scipy_dgetrf_(&n, &n, A, &n, ipiv, &info);
+    if (info == 0) scipy_dgetri_(&n, A, &n, ipiv, wk, &lwk, &info);
+    free(ipiv);
+    free(wk);
+    return info;
+}
+
+static int eigen(int n, double *A, double *wr, double *wi, double *vr)
+{
+    /* dgeev('n','v',...) as src/pseudomat.f90:131-132, 244-245.              */
+    int info = 0, lwk = 64 * n, one = 1;
+    double dummy = 0.0;
+    double *wk = (double *)calloc((size_t)lwk, sizeof(double));
+    scipy_dgeev_("n", "v", &n, A, &n, wr, wi, &dummy, &one, vr, &n, wk, &lwk,
+                 &info, 1, 1);
+    free(wk);
+    return info;
+}
+
+/* pseudomat, src/pseudomat.f90:2-312 (both the 'd' and the 'n' branch).   */
+int orc_pseudomat(int m, orc_ops *o)
+{
+    if (m < 4) return -1;
+    memset(o, 0, sizeof(*o));
+    const int n = m - 1, mm2 = m - 2;
+    const double pi = 4.0 * atan(1.0);
+    o->m = m;
+    o->xcol = (double *)calloc((size_t)m, sizeof(double));
+    o->DC = (double *)calloc((size_t)m * m, sizeof(double));
+    o->D2 = (double *)calloc((size_t)m * m, sizeof(double));
+    o->ED = (double *)calloc((size_t)mm2, sizeof(double));
+    o->EDim = (double *)calloc((size_t)mm2, sizeof(double));
+    o->EN = (double *)calloc((size_t)mm2, sizeof(double));
+    o->ENim = (double *)calloc((size_t)mm2, sizeof(double));
+    o->PD = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    o->PDM1 = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    o->PN = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    o->PNM1 = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    o->D2Bd = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    o->D2Bn = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    double *dd = (double *)calloc((size_t)m, sizeof(double));
+    double *D2B = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    double *x = o->xcol, *DC = o->DC, *D2 = o->D2;
+
+    /* dd and nodes: :72-85 */
+    dd[0] = 2.0;
+    for (int i = 1; i < m - 1; ++i) dd[i] = 1.0;
+    dd[m - 1] = 2.0;
+    for (int j = 0; j < m; ++j) x[j] = -cos(pi * (double)j / (double)n);
+
+    /* derivative matrix, CHQZ p.69: :90-107 (1-based l,j -> 0-based) */
+    DC[IX(0, 0, m)] = -(2.0 * (double)n * (double)n + 1.0) / 6.0;
+    DC[IX(m - 1, m - 1, m)] = -DC[IX(0, 0, m)];
+    for (int i = 1; i < n; ++i)
+        DC[IX(i, i, m)] = -0.5 * x[i] / (1.0 - x[i] * x[i]);
+    for (int l = 0; l < m; ++l) {
+        for (int j = 0; j < l; ++j) {
+            double coef = dd[l] / dd[j];
+            double sgn = ((l + j) % 2 == 0) ? 1.0 : -1.0;
+            DC[IX(l, j, m)] = coef * sgn / (x[l] - x[j]);
+        }
+        for (int j = l + 1; j < m; ++j) {
+            double coef = dd[l] / dd[j];
+            double sgn = ((l + j) % 2 == 0) ? 1.0 : -1.0;
+            DC[IX(l, j, m)] = coef * sgn / (x[l] - x[j]);
+        }
+    }
+    /* D2 = DC*DC: :110 */
+    {
+        const double one = 1.0, zero = 0.0;
+        scipy_dgemm_("n", "n", &m, &m, &m, &one, DC, &m, DC, &m, &zero, D2, &m,
+                     1, 1);
+    }
+
+    int info = 0;
+    /* ---- Dirichlet: :223-263 ---- */
+    for (int j = 0; j < mm2; ++j)
+        for (int i = 0; i < mm2; ++i)
+            D2B[IX(i, j, mm2)] = D2[IX(i + 1, j + 1, m)];
+    memcpy(o->D2Bd, D2B, sizeof(double) * (size_t)mm2 * mm2);
+    info = eigen(mm2, D2B, o->ED, o->EDim, o->PD);
+    if (info) goto done;
+    memcpy(o->PDM1, o->PD, sizeof(double) * (size_t)mm2 * mm2);
+    info = invert(mm2, o->PDM1);
+    if (info) goto done;
+
+    /* ---- Neumann: :114-186 ---- */
+    {
+        const double Det = DC[IX(0, 0, m)] * DC[IX(m - 1, m - 1, m)] -
+                           DC[IX(0, m - 1, m)] * DC[IX(m - 1, 0, m)];
+        for (int i = 1; i < n; ++i)
+            for (int j = 1; j < n; ++j) {
+                double ter1 = D2[IX(i, 0, m)] *
+                              (DC[IX(0, m - 1, m)] * DC[IX(m - 1, j, m)] -
+                               DC[IX(m - 1, m - 1, m)] * DC[IX(0, j, m)]) /
+                              Det;
+                double ter3 = D2[IX(i, m - 1, m)] *
+                              (DC[IX(m - 1, 0, m)] * DC[IX(0, j, m)] -
+                               DC[IX(0, 0, m)] * DC[IX(m - 1, j, m)]) /
+                              Det;
+                D2B[IX(i - 1, j - 1, mm2)] = ter1 + D2[IX(i, j, m)] + ter3;
+            }
+        memcpy(o->D2Bn, D2B, sizeof(double) * (size_t)mm2 * mm2);
+        info = eigen(mm2, D2B, o->EN, o->ENim, o->PN);
+        if (info) goto done;
+        memcpy(o->PNM1, o->PN, sizeof(double) * (size_t)mm2 * mm2);
+        info = invert(mm2, o->PNM1);
+        if (info) goto done;
+        /* location of the zero eigenvalue: :146-152 (strict "ne" update) */
+        double eigmin = 1.0e6;
+        o->iofzero = 0;
+        for (int i = 0; i < mm2; ++i) {
+            double eig = fmin(eigmin, fabs(o->EN[i]));
+            if (eig != eigmin) {
+                o->iofzero = i + 1;
+                eigmin = eig;
+            }
+        }
+        o->wanted = 0.0;
+        /* AM1: :158-178, Fortran AM1(r,c) -> AM1[(r-1)+(c-1)*4] */
+        double *A = o->AM1;
+        const double d11 = DC[IX(0, 0, m)], d1m = DC[IX(0, m - 1, m)];
+        const double dm1 = DC[IX(m - 1, 0, m)], dmm = DC[IX(m - 1, m - 1, m)];
+        A[0 + 0 * 4] = 2.0 * d11; A[0 + 1 * 4] = d1m;
+        A[0 + 2 * 4] = 0.0;       A[0 + 3 * 4] = d1m;
+        A[1 + 0 * 4] = -dm1;      A[1 + 1 * 4] = d11 - dmm;
+        A[1 + 2 * 4] = d1m;       A[1 + 3 * 4] = 0.0;
+        A[2 + 0 * 4] = 0.0;       A[2 + 1 * 4] = dm1;
+        A[2 + 2 * 4] = 2.0 * dmm; A[2 + 3 * 4] = dm1;
+        A[3 + 0 * 4] = -dm1;      A[3 + 1 * 4] = 0.0;
+        A[3 + 2 * 4] = d1m;       A[3 + 3 * 4] = d11 - dmm;
+        info = invert(4, A);
+    }
+done:
+    free(dd);
+    free(D2B);
+    return info;
+}
+
+void orc_ops_free(orc_ops *o)
+{
+    free(o->xcol); free(o->DC); free(o->D2);
+    free(o->ED); free(o->EDim); free(o->PD); free(o->PDM1);
+    free(o->EN); free(o->ENim); free(o->PN); free(o->PNM1);
+    free(o->D2Bd); free(o->D2Bn);
+    memset(o, 0, sizeof(*o));
+}
+
+/* Padded (m-1)^2 transposed operators exactly as the reference stores them
+ * (PDT, PDM1T, PNT, PNM1T of src/pseudomat.f90:181-186, 258-263).          */
+static void padded_transpose(int mm2, const double *P, double *PT)
+{
+    const int np1 = mm2 + 1;
+    memset(PT, 0, sizeof(double) * (size_t)np1 * np1);
+    for (int i = 0; i < mm2; ++i)
+        for (int j = 0; j < mm2; ++j) PT[IX(i, j, np1)] = P[IX(j, i, mm2)];
+}
+
+typedef struct {
+    double *F, *FT, *tmprt, *PT, *PM1T;
+} orc_work;
+
+static void work_alloc(orc_work *w, int m)
+{
+    const size_t np1 = (size_t)(m - 1);
+    w->F = (double *)calloc(np1 * np1, sizeof(double));
+    w->FT = (double *)calloc(np1 * np1, sizeof(double));
+    w->tmprt = (double *)calloc(np1 * np1, sizeof(double));
+    w->PT = (double *)calloc(np1 * np1, sizeof(double));
+    w->PM1T = (double *)calloc(np1 * np1, sizeof(double));
+}
+static void work_free(orc_work *w)
+{
+    free(w->F); free(w->FT); free(w->tmprt); free(w->PT); free(w->PM1T);
+}
+
+/* solvediag, src/solvediag.f90:2-330 (the ngpu=0 branch).                   */
+static int solvediag_w(double *U, const orc_ops *o, char bound, double xlambda,
+                       orc_work *w)
+{
+    const int m = o->m, mm2 = m - 2, np1 = m - 1;
+    const size_t nn = (size_t)np1 * np1;
+    double *F = w->F, *FT = w->FT, *tmprt = w->tmprt;
+    memset(F, 0, nn * sizeof(double));
+    memset(FT, 0, nn * sizeof(double));
+    memset(tmprt, 0, nn * sizeof(double));
+    /* interior copy: :30-34 */
+    for (int j = 1; j < m - 1; ++j)
+        for (int i = 1; i < m - 1; ++i) F[IX(i - 1, j - 1, np1)] = U[IX(i, j, m)];
+
+    if (bound == 'd') {
+        const double *D2 = o->D2;
+        /* boundary-value correction: :39-45 (D2bx = D2by = D2(:,{1,m})) */
+        for (int j = 0; j < mm2; ++j)
+            for (int i = 0; i < mm2; ++i) {
+                double bcontv = D2[IX(i + 1, 0, m)] * U[IX(0, j + 1, m)] +
+                                D2[IX(i + 1, m - 1, m)] * U[IX(m - 1, j + 1, m)];
+                double bconth = D2[IX(j + 1, 0, m)] * U[IX(i + 1, 0, m)] +
+                                D2[IX(j + 1, m - 1, m)] * U[IX(i + 1, m - 1, m)];
+                F[IX(i, j, np1)] -= bcontv + bconth;
+            }
+        padded_transpose(mm2, o->PD, w->PT);
+        padded_transpose(mm2, o->PDM1, w->PM1T);
+        /* hot loop: :51-80 */
+        dgemm_tn(np1, w->PM1T, F, FT);
+        for (int i = 0; i < np1; ++i)
+            for (int j = 0; j < np1; ++j) tmprt[IX(i, j, np1)] = FT[IX(j, i, np1)];
+        dgemm_tn(np1, tmprt, w->PM1T, F);
+        for (int j = 0; j < mm2; ++j)
+            for (int i = 0; i < mm2; ++i)
+                FT[IX(i, j, np1)] =
+                    F[IX(i, j, np1)] / ((o->ED[i] + o->ED[j]) - xlambda);
+        dgemm_tn(np1, w->PT, FT, F);
+        for (int i = 0; i < np1; ++i)
+            for (int j = 0; j < np1; ++j) tmprt[IX(i, j, np1)] = F[IX(j, i, np1)];
+        dgemm_tn(np1, tmprt, w->PT, FT);
+        /* write-back: :131-135 */
+        for (int j = 0; j < mm2; ++j)
+            for (int i = 0; i < mm2; ++i) U[IX(i + 1, j + 1, m)] = FT[IX(i, j, np1)];
+        return 0;
+    }
+    if (bound != 'n') return -1;
+
+    /* ---- Neumann: :137-322 ---- */
+    const double *EN = o->EN, *PN = o->PN, *DC = o->DC;
+    padded_transpose(mm2, o->PN, w->PT);
+    padded_transpose(mm2, o->PNM1, w->PM1T);
+    dgemm_tn(np1, w->PM1T, F, FT);
+    for (int i = 0; i < mm2; ++i)
+        for (int j = 0; j < mm2; ++j) tmprt[IX(i, j, np1)] = FT[IX(j, i, np1)];
+    dgemm_tn(np1, tmprt, w->PM1T, F);
+    if (fabs(xlambda) > 1.0e-10) {
+        for (int j = 0; j < mm2; ++j)
+            for (int i = 0; i < mm2; ++i)
+                FT[IX(i, j, np1)] = F[IX(i, j, np1)] / (EN[i] + EN[j] - xlambda);
+    } else {
+        /* singular mode: :163-206 */
+        const int io = o->iofzero - 1;
+        for (int j = 0; j < mm2; ++j)
+            for (int i = 0; i < mm2; ++i) {
+                if (i == io && j == io) continue;
+                FT[IX(i, j, np1)] = F[IX(i, j, np1)] / (EN[i] + EN[j] - xlambda);
+            }
+        FT[IX(io, io, np1)] = 0.0;
+        double valore = 0.0;
+        for (int l = 0; l < mm2; ++l) {
+            double val = 0.0;
+            for (int k = 0; k < mm2; ++k) val += PN[IX(io, k, mm2)] * FT[IX(l, k, np1)];
+            valore += PN[IX(io, l, mm2)] * val;
+        }
+        FT[IX(io, io, np1)] =
+            (o->wanted - valore) / (PN[IX(io, io, mm2)] * PN[IX(io, io, mm2)]);
+    }
+    dgemm_tn(np1, w->PT, FT, F);
+    for (int i = 0; i < mm2; ++i)
+        for (int j = 0; j < mm2; ++j) tmprt[IX(i, j, np1)] = F[IX(j, i, np1)];
+    dgemm_tn(np1, tmprt, w->PT, FT);
+    for (int j = 0; j < mm2; ++j)
+        for (int i = 0; i < mm2; ++i) U[IX(i + 1, j + 1, m)] = FT[IX(i, j, np1)];
+
+    /* Neumann wall lines: :253-276 */
+    const double d11 = DC[IX(0, 0, m)], d1m = DC[IX(0, m - 1, m)];
+    const double dm1 = DC[IX(m - 1, 0, m)], dmm = DC[IX(m - 1, m - 1, m)];
+    const double det = d11 * dmm - d1m * dm1;
+    for (int i = 1; i < m - 1; ++i) {
+        double sumb = 0.0, sumt = 0.0;
+        for (int j = 0; j < mm2; ++j) {
+            sumb += DC[IX(0, j + 1, m)] * FT[IX(i - 1, j, np1)];
+            sumt += DC[IX(m - 1, j + 1, m)] * FT[IX(i - 1, j, np1)];
+        }
+        U[IX(i, 0, m)] = (-dmm * sumb + d1m * sumt) / det;
+        U[IX(i, m - 1, m)] = (dm1 * sumb - d11 * sumt) / det;
+    }
+    for (int j = 1; j < m - 1; ++j) {
+        double suml = 0.0, sumr = 0.0;
+        for (int i = 0; i < mm2; ++i) {
+            suml += DC[IX(0, i + 1, m)] * FT[IX(i, j - 1, np1)];
+            sumr += DC[IX(m - 1, i + 1, m)] * FT[IX(i, j - 1, np1)];
+        }
+        U[IX(0, j, m)] = (-dmm * suml + d1m * sumr) / det;
+        U[IX(m - 1, j, m)] = (dm1 * suml - d11 * sumr) / det;
+    }
+    /* corners: :280-322 */
+    double ff[4] = {0, 0, 0, 0};
+    for (int i = 1; i < m - 1; ++i)
+        ff[0] = ff[0] - DC[IX(0, i, m)] * (U[IX(i, 0, m)] + U[IX(0, i, m)]);
+    for (int i = 1; i < m - 1; ++i)
+        ff[1] = ff[1] - DC[IX(0, i, m)] * U[IX(m - 1, i, m)] +
+                DC[IX(m - 1, i, m)] * U[IX(i, 0, m)];
+    for (int i = 1; i < m - 1; ++i)
+        ff[2] = ff[2] - DC[IX(m - 1, i, m)] * (U[IX(i, m - 1, m)] + U[IX(m - 1, i, m)]);
+    for (int i = 1; i < m - 1; ++i)
+        ff[3] = ff[3] - DC[IX(0, i, m)] * U[IX(i, m - 1, m)] +
+                DC[IX(m - 1, i, m)] * U[IX(0, i, m)];
+    const double *A = o->AM1;
+    double c[4];
+    for (int r = 0; r < 4; ++r) {
+        c[r] = 0.0;
+        for (int i = 0; i < 4; ++i) c[r] += A[r + 4 * i] * ff[i];
+    }
+    U[IX(0, 0, m)] = c[0];
+    U[IX(m - 1, 0, m)] = c[1];
+    U[IX(m - 1, m - 1, m)] = c[2];
+    U[IX(0, m - 1, m)] = c[3];
+    return 0;
+}
+
+int orc_solvediag(double *U, const orc_ops *o, char bound, double xlambda)
+{
+    orc_work w;
+    work_alloc(&w, o->m);
+    int r = solvediag_w(U, o, bound, xlambda, &w);
+    work_free(&w);
+    return r;
+}
+
+/* helm3d + int2d3d + com2re/re2com: src/helm3d.f90:36-72,
+ * src/int2d3d.f90:2-53, 55-109.                                            */
+int orc_helm3d(double *rhs, double *sol, int my, int mz, int ib, int ie,
+               const double *xalp, char bound, double alambda,
+               const orc_ops *o, int nthreads)
+{
+    if (my != mz || my != o->m) return -2;
+    if (bound != 'd' && bound != 'n') return -1;
+    const int nmodes = ie - ib + 1;
+    const size_t plane = (size_t)my * mz;
+    if (bound == 'd') {
+        for (int i = 0; i < nmodes; ++i) {
+            double *r = rhs + 2 * plane * (size_t)i;
+            for (int j = 0; j < my; ++j) {
+                r[2 * IX(j, 0, my)] = r[2 * IX(j, 0, my) + 1] = 0.0;
+                r[2 * IX(j, mz - 1, my)] = r[2 * IX(j, mz - 1, my) + 1] = 0.0;
+            }
+            for (int k = 0; k < mz; ++k) {
+                r[2 * IX(0, k, my)] = r[2 * IX(0, k, my) + 1] = 0.0;
+                r[2 * IX(my - 1, k, my)] = r[2 * IX(my - 1, k, my) + 1] = 0.0;
+            }
+        }
+    }
+    if (nthreads < 1) nthreads = 1;
+    int err = 0;
+#pragma omp parallel num_threads(nthreads) reduction(| : err)
+    {
+        orc_work w;
+        work_alloc(&w, my);
+        double *U = (double *)malloc(sizeof(double) * plane);
+#pragma omp for schedule(dynamic, 1)
+        for (int i = 0; i < nmodes; ++i) {
+            const int imode = ib + i;
+            const double xlambda = alambda + xalp[i] * xalp[i];
+            const double *r = rhs + 2 * plane * (size_t)i;
+            double *s = sol + 2 * plane * (size_t)i;
+            for (size_t p = 0; p < plane; ++p) U[p] = r[2 * p];
+            err |= solvediag_w(U, o, bound, xlambda, &w);
+            for (size_t p = 0; p < plane; ++p) {
+                s[2 * p] = U[p];
+                s[2 * p + 1] = 0.0;
+            }
+            if (imode == 0) continue;
+            for (size_t p = 0; p < plane; ++p) U[p] = r[2 * p + 1];
+            err |= solvediag_w(U, o, bound, xlambda, &w);
+            for (size_t p = 0; p < plane; ++p) s[2 * p + 1] += U[p];
+        }
+        free(U);
+        work_free(&w);
+    }
+    return err ? -1 : 0;
+}
+
+/* ---- Chebyshev transforms ------------------------------------------------ */
+
+/* FFTW REDFT00 of length nn: X_k = x_0 + (-1)^k x_{N} + 2 sum x_j cos(pi jk/N)
+ * with N = nn-1, evaluated directly with an exact-angle cosine table.      */
+static void redft00(const double *x, double *X, int nn, const double *ctab)
+{
+    const int N = nn - 1;
+    for (int k = 0; k < nn; ++k) {
+        double s = x[0] + ((k & 1) ? -x[N] : x[N]);
+        double acc = 0.0;
+        for (int j = 1; j < N; ++j) acc += x[j] * ctab[(size_t)((long)j * k % (2 * N))];
+        X[k] = s + 2.0 * acc;
+    }
+}
+
+static double *cos_table(int nn)
+{
+    const int N = nn - 1;
+    const double pi = 4.0 * atan(1.0);
+    double *t = (double *)malloc(sizeof(double) * (size_t)(2 * N));
+    for (int q = 0; q < 2 * N; ++q) t[q] = cos(pi * (double)q / (double)N);
+    return t;
+}
+
+/* tcheb_fftw, src/tchebw.f:62-192 (one direction; identical for y and z). */
+void orc_tcheb(double *cr, long ise, long isa, long nlines, int nn, int iopt)
+{
+    double *ctab = cos_table(nn);
+    const double dn1 = 1.0 / (double)(nn - 1), dn2 = 0.5 * dn1;
+#pragma omp parallel
+    {
+        double *buf = (double *)malloc(sizeof(double) * (size_t)nn);
+        double *out = (double *)malloc(sizeof(double) * (size_t)nn);
+#pragma omp for
+        for (long k = 0; k < nlines; ++k) {
+            double *c = cr + k * isa;
+            for (int j = 0; j < nn; ++j) buf[j] = c[j * ise];
+            if (iopt < 0) {
+                redft00(buf, out, nn, ctab);
+                for (int j = 1; j < nn - 1; ++j) c[j * ise] = dn1 * out[j];
+                c[0] = dn2 * out[0];
+                c[(long)(nn - 1) * ise] = dn2 * out[nn - 1];
+            } else {
+                buf[0] *= 2.0;
+                buf[nn - 1] *= 2.0;
+                redft00(buf, out, nn, ctab);
+                for (int j = 0; j < nn; ++j) c[j * ise] = 0.5 * out[j];
+            }
+        }
+        free(buf);
+        free(out);
+    }
+    free(ctab);
+}
+
+/* transyz, src/chebyshev.f90:458-540.                                       */
+void orc_transyz(double *cheb, int my, int mz, int nmodes, char cdir, int iopt)
+{
+    if (cdir == 'y') {
+        const long nn = (long)mz * nmodes;
+        orc_tcheb(cheb, 2, 2L * my, nn, my, iopt);
+        orc_tcheb(cheb + 1, 2, 2L * my, nn, my, iopt);
+    } else {
+        for (int i = 0; i < nmodes; ++i) {
+            double *c = cheb + (size_t)i * my * mz * 2;
+            orc_tcheb(c, 2L * my, 2, my, mz, iopt);
+            orc_tcheb(c + 1, 2L * my, 2, my, mz, iopt);
+        }
+    }
+}
+
+/* transyz_plane, src/chebyshev.f90:542-595.                                 */
+void orc_transyz_plane(double *cheb, int my, int mz, int iopt)
+{
+    orc_tcheb(cheb, 1, my, mz, my, iopt);
+    orc_tcheb(cheb, my, 1, my, mz, iopt);
+}
+
+/* One backward recurrence line (src/chebyshev.f90:44-58 pattern):
+ * out_k = -d_k for k>=1, out_0 = -d_0/2 with d_{k-1} = d_{k+1} + 2k c_k.    */
+static void deriv_line(const double *c, long st, double *out, long so, int n,
+                       double fac, int accumulate)
+{
+    double aari = 0.0, bri = 0.0, tri = 0.0, cri;
+    int ia = n;
+    for (int ii = 1; ii <= n - 1; ++ii) {
+        const int kk = n - ii;
+        cri = bri + 2.0 * (double)kk * c[(long)(ia - 1) * st];
+        if (accumulate) out[(long)(ia - 1) * so] += -tri * fac;
+        else out[(long)(ia - 1) * so] = -tri * fac;
+        bri = aari;
+        tri = cri;
+        aari = cri;
+        ia -= 1;
+    }
+    if (accumulate) out[(long)(ia - 1) * so] += -0.5 * tri * fac;
+    else out[(long)(ia - 1) * so] = -0.5 * tri * fac;
+}
+
+/* derivyz, src/chebyshev.f90:1-295.  Complex lines: real and imaginary parts
+ * follow the same real recurrence (scal is real).                           */
+void orc_derivyz(const double *u, double *du, int my, int mz, int nmodes,
+                 char cdir, int ider, double scal, char what, double aspect)
+{
+    const int acc = (what != 'n');
+    const int n = (cdir == 'y') ? my : mz;
+    const double fz = (cdir == 'y') ? 1.0 : (ider == 1 ? 1.0 / aspect : 1.0 / (aspect * aspect));
+    double *aux = (double *)malloc(sizeof(double) * (size_t)n);
+    for (int i = 0; i < nmodes; ++i) {
+        const size_t base = (size_t)i * my * mz * 2;
+        const long nlines = (cdir == 'y') ? mz : my;
+        for (long l = 0; l < nlines; ++l) {
+            for (int part = 0; part < 2; ++part) {
+                size_t off;
+                long st;
+                if (cdir == 'y') { off = base + 2 * (size_t)l * my + part; st = 2; }
+                else { off = base + 2 * (size_t)l + part; st = 2L * my; }
+                if (ider == 1) {
+                    deriv_line(u + off, st, du + off, st, n, scal * fz, acc);
+                } else {
+                    deriv_line(u + off, st, aux, 1, n, 1.0, 0);
+                    deriv_line(aux, 1, du + off, st, n, scal * fz, acc);
+                }
+            }
+        }
+    }
+    free(aux);
+}
+
+/* cheb2_integral, src/chebyshev.f90:692-723.                                */
+double orc_cheb2_integral(const double *u, int ny, int nz, double aspect)
+{
+    double sum = 0.0;
+    for (int j = 0; j < nz; j += 2)
+        for (int i = 0; i < ny; i += 2)
+            sum += u[IX(i, j, ny)] * 4.0 * aspect /
+                   ((double)(j * j - 1) * (double)(i * i - 1));
+    return sum;
+}
+
+/* cxyz2yzx / cyzx2xyz, src/parallel.F:476-529 (complex*16 elements).       */
+void orc_cxyz2yzx(const double *phys, double *phys2, int nmodes, int my, int nz)
+{
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < my; ++j)
+            for (int i = 0; i < nmodes; ++i) {
+                size_t s = (size_t)i + (size_t)nmodes * (j + (size_t)my * k);
+                size_t d = (size_t)j + (size_t)my * (k + (size_t)nz * i);
+                phys2[2 * d] = phys[2 * s];
+                phys2[2 * d + 1] = phys[2 * s + 1];
+            }
+}
+
+void orc_cyzx2xyz(double *phys, const double *phys2, int nmodes, int my, int nz)
+{
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < my; ++j)
+            for (int i = 0; i < nmodes; ++i) {
+                size_t s = (size_t)j + (size_t)my * (k + (size_t)nz * i);
+                size_t d = (size_t)i + (size_t)nmodes * (j + (size_t)my * k);
+                phys[2 * d] = phys2[2 * s];
+                phys[2 * d + 1] = phys2[2 * s + 1];
+            }
+}

@@ -1,0 +1,164 @@
+"""ctypes view of the CPU oracle (test infrastructure only).
+
+Used by tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+bench.py as the checker.  Arrays use the reference's shapes in Fortran order:
+a complex field is ``(my, mz, nmodes)`` complex128, a real plane ``(my, mz)``.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build_oracle
+
+_lib = None
+
+
+class _Ops(C.Structure):
+    _fields_ = [("m", C.c_int)] + [(n, C.POINTER(C.c_double)) for n in (
+        "xcol", "DC", "D2", "ED", "EDim", "PD", "PDM1", "EN", "ENim", "PN", "PNM1")] + [
+        ("iofzero", C.c_int), ("wanted", C.c_double), ("AM1", C.c_double * 16),
+        ("D2Bd", C.POINTER(C.c_double)), ("D2Bn", C.POINTER(C.c_double))]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = build_oracle.build()
+        L = C.CDLL(path)
+        P = C.c_void_p
+        L.orc_pseudomat.argtypes = [C.c_int, C.POINTER(_Ops)]
+        L.orc_ops_free.argtypes = [C.POINTER(_Ops)]
+        L.orc_solvediag.argtypes = [P, C.POINTER(_Ops), C.c_char, C.c_double]
+        L.orc_helm3d.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_char,
+                                 C.c_double, C.POINTER(_Ops), C.c_int]
+        L.orc_tcheb.argtypes = [P, C.c_long, C.c_long, C.c_long, C.c_int, C.c_int]
+        L.orc_transyz.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_char, C.c_int]
+        L.orc_transyz_plane.argtypes = [P, C.c_int, C.c_int, C.c_int]
+        L.orc_derivyz.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_char, C.c_int,
+                                  C.c_double, C.c_char, C.c_double]
+        L.orc_cheb2_integral.argtypes = [P, C.c_int, C.c_int, C.c_double]
+        L.orc_cheb2_integral.restype = C.c_double
+        L.orc_cxyz2yzx.argtypes = [P, P, C.c_int, C.c_int, C.c_int]
+        L.orc_cyzx2xyz.argtypes = [P, P, C.c_int, C.c_int, C.c_int]
+        L.orc_set_blas_threads.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    assert a.flags.f_contiguous or a.ndim <= 1
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Ops:
+    """Result of pseudomat('d',m) + pseudomat('n',m) (src/pseudomat.f90)."""
+
+    def __init__(self, m):
+        self._s = _Ops()
+        info = lib().orc_pseudomat(m, C.byref(self._s))
+        if info != 0:
+            raise RuntimeError("orc_pseudomat failed, info=%d" % info)
+        self.m = m
+        n = m - 2
+        s = self._s
+
+        def v(ptr, *shape):
+            return np.ctypeslib.as_array(ptr, shape=(int(np.prod(shape)),)).reshape(
+                shape, order="F").copy(order="F")
+        self.xcol = v(s.xcol, m)
+        self.DC = v(s.DC, m, m)
+        self.D2 = v(s.D2, m, m)
+        self.ED, self.EDim = v(s.ED, n), v(s.EDim, n)
+        self.PD, self.PDM1 = v(s.PD, n, n), v(s.PDM1, n, n)
+        self.EN, self.ENim = v(s.EN, n), v(s.ENim, n)
+        self.PN, self.PNM1 = v(s.PN, n, n), v(s.PNM1, n, n)
+        self.D2Bd, self.D2Bn = v(s.D2Bd, n, n), v(s.D2Bn, n, n)
+        self.iofzero = s.iofzero
+        self.wanted = s.wanted
+        self.AM1 = np.array(list(s.AM1)).reshape((4, 4), order="F")
+
+    def __del__(self):
+        try:
+            lib().orc_ops_free(C.byref(self._s))
+        except Exception:
+            pass
+
+
+def solvediag(U, ops, bound, xlambda):
+    """solvediag on one real (my,mz) plane; returns a new array."""
+    U = np.asfortranarray(U, dtype=np.float64).copy(order="F")
+    r = lib().orc_solvediag(_p(U), C.byref(ops._s), bound.encode(), float(xlambda))
+    if r:
+        raise ValueError("solvediag: bad bound")
+    return U
+
+
+def helm3d(rhs, ops, bound, alambda, xalp, ib=0, nthreads=1):
+    """helm3d on a complex (my,mz,nmodes) field.  Returns (sol, rhs_after)
+    where rhs_after carries helm3d's in-place wall zeroing for bound='d'."""
+    rhs = np.asfortranarray(rhs, dtype=np.complex128).copy(order="F")
+    my, mz, nm = rhs.shape
+    sol = np.zeros_like(rhs, order="F")
+    xalp = np.ascontiguousarray(xalp, dtype=np.float64)
+    assert xalp.shape == (nm,)
+    r = lib().orc_helm3d(_p(rhs), _p(sol), my, mz, ib, ib + nm - 1, _p(xalp),
+                         bound.encode(), float(alambda), C.byref(ops._s), int(nthreads))
+    if r:
+        raise ValueError("helm3d failed (%d)" % r)
+    return sol, rhs
+
+
+def transyz(f, cdir, iopt):
+    f = np.asfortranarray(f, dtype=np.complex128).copy(order="F")
+    my, mz, nm = f.shape
+    lib().orc_transyz(_p(f), my, mz, nm, cdir.encode(), int(iopt))
+    return f
+
+
+def transyz_plane(f, iopt):
+    f = np.asfortranarray(f, dtype=np.float64).copy(order="F")
+    my, mz = f.shape
+    lib().orc_transyz_plane(_p(f), my, mz, int(iopt))
+    return f
+
+
+def derivyz(u, cdir, ider, scal=1.0, what="n", du=None, aspect=1.0):
+    u = np.asfortranarray(u, dtype=np.complex128)
+    my, mz, nm = u.shape
+    du = np.zeros_like(u, order="F") if du is None else np.asfortranarray(du).copy(order="F")
+    lib().orc_derivyz(_p(u), _p(du), my, mz, nm, cdir.encode(), int(ider), float(scal),
+                      what.encode(), float(aspect))
+    return du
+
+
+def cheb2_integral(u, aspect=1.0):
+    u = np.asfortranarray(u, dtype=np.float64)
+    return lib().orc_cheb2_integral(_p(u), u.shape[0], u.shape[1], float(aspect))
+
+
+def cxyz2yzx(phys):
+    """phys (0:mx1, my, nz) complex -> (my, nz, 0:mx1)."""
+    phys = np.asfortranarray(phys, dtype=np.complex128)
+    nm, my, nz = phys.shape
+    out = np.zeros((my, nz, nm), dtype=np.complex128, order="F")
+    lib().orc_cxyz2yzx(_p(phys), _p(out), nm, my, nz)
+    return out
+
+
+def cyzx2xyz(phys2):
+    """phys2 (my, nz, 0:mx1) complex -> (0:mx1, my, nz)."""
+    phys2 = np.asfortranarray(phys2, dtype=np.complex128)
+    my, nz, nm = phys2.shape
+    out = np.zeros((nm, my, nz), dtype=np.complex128, order="F")
+    lib().orc_cyzx2xyz(_p(out), _p(phys2), nm, my, nz)
+    return out
+
+
+def set_blas_threads(n):
+    lib().orc_set_blas_threads(int(n))
+
+
+__all__ = ["Ops", "solvediag", "helm3d", "transyz", "transyz_plane", "derivyz",
+           "cheb2_integral", "cxyz2yzx", "cyzx2xyz", "set_blas_threads", "lib"]
+_ = os

@@ -1,0 +1,47 @@
+"""The C-ABI library loads and exports every entry declared in
+include/ductgpu.h (no GPU needed; no compute calls)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    names = set()
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if h.endswith(".h"):
+            src = open(os.path.join(ROOT, "include", h)).read()
+            src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+            names |= set(re.findall(r"\b(ductgpu_\w+)\s*\(", src))
+    return names
+
+
+def test_header_declares_entries():
+    assert {"ductgpu_create", "ductgpu_helm3d", "ductgpu_solve_fields_dev",
+            "ductgpu_pseudomat"} <= declared()
+
+
+def test_library_exports_every_declared_symbol():
+    import duct_b200 as D
+    L = D.lib()
+    missing = [n for n in sorted(declared()) if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(D.EXPORTS) <= declared()
+
+
+def test_create_without_device_returns_status():
+    import duct_b200 as D
+    h = C.c_void_p()
+    rc = D.lib().ductgpu_create(10_000, C.byref(h))
+    assert rc != 0 and not h.value
+
+
+def test_null_context_is_rejected():
+    import duct_b200 as D
+    L = D.lib()
+    assert L.ductgpu_pseudomat(None, 33, 33) == D.EARG
+    assert L.ductgpu_destroy(None) == D.EARG
+    assert L.ductgpu_launch_count(None) == -1

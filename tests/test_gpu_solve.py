@@ -1,0 +1,167 @@
+"""Parity of the CUDA solve (through the C-ABI) with the CPU oracle and the
+golden fixtures.  Tolerance: 1e-12 relative (2-norm over all points) for the
+plain FP64 path, as required of the drop-in."""
+import os
+
+import numpy as np
+import pytest
+
+import duct_b200 as D
+from duct_b200 import synth
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL = 1e-12
+
+
+def rel(a, b):
+    return np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel())
+
+
+def test_setup_spectrum_matches_lapack(gpu_ctx, oracle):
+    for m in (17, 33, 129):
+        ops = oracle.Ops(m)
+        gpu_ctx.pseudomat(m)
+        for bound, Eref in (("d", ops.ED), ("n", ops.EN)):
+            E, P, Q, io = gpu_ctx.get_operators(bound, m - 2)
+            assert rel(np.sort(E), np.sort(Eref)) < 1e-12
+            assert np.max(np.abs(P @ Q - np.eye(m - 2))) < 1e-10
+            B = ops.D2Bd if bound == "d" else ops.D2Bn
+            assert np.max(np.abs(B @ P - P * E)) < 1e-9 * np.max(np.abs(E))
+        # the singular Neumann eigenvector is constant
+        E, P, Q, io = gpu_ctx.get_operators("n", m - 2)
+        p = P[:, io - 1]
+        assert np.max(np.abs(p - p.mean())) < 1e-10 * abs(p.mean())
+
+
+def test_cfg0_dirichlet_golden(gpu_ctx):
+    g = np.load(os.path.join(GOLD, "cfg0_dirichlet.npz"))
+    rhs = synth.chebyshev_rhs(33, 33, 17, seed=0, ib=0)
+    assert np.allclose([rhs.real.sum(), rhs.imag.sum(), np.abs(rhs).sum()], g["rhs_sum"], rtol=1e-13)
+    sol = gpu_ctx.helm3d(rhs, "d", float(g["alambda"]), g["xalp"], ipro=0)
+    assert rel(sol, g["sol"]) < TOL
+    # helm3d side effects: rhs walls zeroed in place; mode 0 real
+    assert np.all(rhs[0, :, :] == 0) and np.all(rhs[-1, :, :] == 0)
+    assert np.all(rhs[:, 0, :] == 0) and np.all(rhs[:, -1, :] == 0)
+    assert np.all(sol[:, :, 0].imag == 0)
+    assert np.all(sol[0, :, :] == 0) and np.all(sol[:, -1, :] == 0)
+
+
+def _neumann_compare(sol, ref, xalp):
+    for k in range(sol.shape[2]):
+        a, b = sol[:, :, k], ref[:, :, k]
+        if abs(xalp[k]) < 1e-5:          # singular: compare modulo a constant
+            a = a - a.mean()
+            b = b - b.mean()
+        assert rel(a, b) < TOL, k
+
+
+def test_neumann_golden_modulo_gauge(gpu_ctx):
+    g = np.load(os.path.join(GOLD, "neumann17.npz"))
+    rhs = synth.chebyshev_rhs(17, 17, 5, seed=7, ib=0)
+    sol = gpu_ctx.helm3d(rhs, "n", 0.0, g["xalp"], ipro=0)
+    _neumann_compare(sol, g["sol"], g["xalp"])
+    assert np.all(sol[:, :, 0].imag == 0)
+
+
+def test_neumann_reference_gauge_with_lapack_operators(gpu_ctx, oracle):
+    """With the oracle's (LAPACK) eigen-decomposition imported, the kx=0 pin
+    lands on the same point and the whole field matches, gauge included."""
+    m, nm = 33, 6
+    ops = oracle.Ops(m)
+    gpu_ctx.pseudomat(m)
+    gpu_ctx.set_operators("d", ops.ED, ops.PD, ops.PDM1)
+    gpu_ctx.set_operators("n", ops.EN, ops.PN, ops.PNM1, ops.iofzero)
+    rhs = synth.chebyshev_rhs(m, m, nm, seed=11, ib=0)
+    xalp = 0.5 * np.arange(nm)
+    ref, _ = oracle.helm3d(rhs, ops, "n", 0.0, xalp)
+    sol = gpu_ctx.helm3d(rhs.copy(order="F"), "n", 0.0, xalp)
+    assert rel(sol, ref) < TOL
+    io = ops.iofzero
+    assert abs(sol[io, io, 0]) < 1e-12
+    refd, _ = oracle.helm3d(rhs, ops, "d", 3.0, xalp)
+    sold = gpu_ctx.helm3d(rhs.copy(order="F"), "d", 3.0, xalp)
+    assert rel(sold, refd) < TOL
+
+
+@pytest.mark.parametrize("m", [9, 17, 33, 49, 65, 97, 129, 145, 193])
+def test_sizes_against_oracle(gpu_ctx, oracle, m):
+    nm = 3
+    ops = oracle.Ops(m)
+    rhs = synth.chebyshev_rhs(m, m, nm, seed=m, ib=0)
+    xalp = np.array([0.0, 1.5, 7.0])
+    ref_d, _ = oracle.helm3d(rhs, ops, "d", 4.0e6, xalp)
+    sol_d = gpu_ctx.helm3d(rhs.copy(order="F"), "d", 4.0e6, xalp, ipro=0)
+    assert rel(sol_d, ref_d) < TOL
+    ref_n, _ = oracle.helm3d(rhs, ops, "n", 0.0, xalp)
+    sol_n = gpu_ctx.helm3d(rhs.copy(order="F"), "n", 0.0, xalp)
+    _neumann_compare(sol_n, ref_n, xalp)
+
+
+def test_offset_modes_and_single_mode(gpu_ctx, oracle):
+    m = 33
+    ops = oracle.Ops(m)
+    gpu_ctx.pseudomat(m)
+    rhs = synth.chebyshev_rhs(m, m, 2, seed=5, ib=3)
+    xalp = np.array([3.0, 4.0])
+    ref, _ = oracle.helm3d(rhs, ops, "d", 2.0, xalp, ib=3)
+    sol = gpu_ctx.helm3d(rhs.copy(order="F"), "d", 2.0, xalp, ib=3)
+    assert rel(sol, ref) < TOL
+    assert np.any(sol[:, :, 0].imag != 0)       # ib=3: no mode-0 rule
+    one = rhs[:, :, :1].copy(order="F")
+    ref1, _ = oracle.helm3d(one, ops, "n", 0.0, xalp[:1], ib=3)
+    sol1 = gpu_ctx.helm3d(one.copy(order="F"), "n", 0.0, xalp[:1], ib=3)
+    assert rel(sol1, ref1) < TOL
+
+
+def test_batched_fields_match_single_calls(gpu_ctx):
+    m, nm = 65, 5
+    gpu_ctx.pseudomat(m)
+    xalp = 0.5 * np.arange(nm)
+    specs = [("d", 4.0e6, 1), ("d", 4.0e6, 2), ("n", 0.0, 3)]
+    fields, singles = [], []
+    for bound, lam, seed in specs:
+        rhs = synth.chebyshev_rhs(m, m, nm, seed=seed, ib=0)
+        singles.append(gpu_ctx.helm3d(rhs.copy(order="F"), bound, lam, xalp))
+        r = gpu_ctx.device_array(rhs.shape)
+        s = gpu_ctx.device_array(rhs.shape)
+        r.upload(rhs)
+        fields.append(dict(rhs=r, sol=s, xalp=xalp, alambda=lam, ib=0, bound=bound))
+    gpu_ctx.solve_fields_dev(fields)
+    gpu_ctx.synchronize()
+    for f, ref in zip(fields, singles):
+        assert np.array_equal(f["sol"].download(), ref)
+        f["rhs"].free()
+        f["sol"].free()
+
+
+def test_mean_gauge(gpu_ctx, oracle):
+    m, nm = 33, 2
+    gpu_ctx.pseudomat(m)
+    rhs = synth.chebyshev_rhs(m, m, nm, seed=9, ib=0)
+    xalp = np.array([0.0, 1.0])
+    point = gpu_ctx.helm3d(rhs.copy(order="F"), "n", 0.0, xalp)
+    gpu_ctx.set_gauge(D.GAUGE_MEAN)
+    try:
+        mean = gpu_ctx.helm3d(rhs.copy(order="F"), "n", 0.0, xalp)
+    finally:
+        gpu_ctx.set_gauge(D.GAUGE_POINT)
+    integral = oracle.cheb2_integral(oracle.transyz_plane(np.asfortranarray(mean[:, :, 0].real), -1))
+    assert abs(integral) < 1e-12 * np.abs(mean).max()
+    shift = (mean[:, :, 0] - point[:, :, 0]).real
+    assert np.max(np.abs(shift - shift.mean())) < 1e-11 * np.abs(point).max()
+    assert np.array_equal(mean[:, :, 1], point[:, :, 1])
+
+
+def test_argument_errors(gpu_ctx):
+    with pytest.raises(D.DuctGPUError) as e:
+        gpu_ctx.pseudomat(33, 65)
+    assert e.value.code == D.EARG and "MY.NE.MZ" in str(e.value)
+    gpu_ctx.pseudomat(17)
+    rhs = synth.chebyshev_rhs(17, 17, 1)
+    with pytest.raises(D.DuctGPUError) as e:
+        gpu_ctx.helm3d(rhs, "x", 0.0, [0.0])
+    assert e.value.code == D.EARG
+    with pytest.raises(D.DuctGPUError) as e:
+        gpu_ctx.pseudomat(400)
+    assert e.value.code == D.EARG
