@@ -303,7 +303,7 @@ def measure_e2e(ctx, c, m, nm, xalp, rhs, prec, args, pg, world):
         p = C.c_void_p()
         ctx._check(L.ductgpu_host_alloc(ctx.h, nbytes, C.byref(p)))
         a = np.ctypeslib.as_array((C.c_double * (nbytes // 8)).from_address(p.value))
-        a[:] = f.view(np.float64).ravel(order="F")
+        a[:] = f.ravel(order="F").view(np.float64)
         hr.append((p, a))
         q = C.c_void_p()
         ctx._check(L.ductgpu_host_alloc(ctx.h, nbytes, C.byref(q)))

@@ -26,6 +26,8 @@ EXPORTS = [
     "ductgpu_device_free", "ductgpu_host_alloc", "ductgpu_host_free", "ductgpu_copy",
     "ductgpu_event_record", "ductgpu_event_elapsed", "ductgpu_launch_count",
     "ductgpu_profile_enable", "ductgpu_profile_reset", "ductgpu_profile_read",
+    "ductgpu_transyz_dev", "ductgpu_transyz", "ductgpu_derivyz_dev", "ductgpu_derivyz",
+    "ductgpu_cxyz2yzx_dev", "ductgpu_cyzx2xyz_dev", "ductgpu_chx2z_dev", "ductgpu_chz2x_dev",
 ]
 K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
 
@@ -72,6 +74,14 @@ def lib():
             "ductgpu_profile_enable": [P, I],
             "ductgpu_profile_reset": [P],
             "ductgpu_profile_read": [P, I, C.POINTER(C.c_double), C.POINTER(C.c_longlong)],
+            "ductgpu_transyz_dev": [P, P, I, I, I, C.c_char, I],
+            "ductgpu_transyz": [P, P, I, I, I, C.c_char, I],
+            "ductgpu_derivyz_dev": [P, P, P, I, I, I, C.c_char, I, D, C.c_char, D],
+            "ductgpu_derivyz": [P, P, P, I, I, I, C.c_char, I, D, C.c_char, D],
+            "ductgpu_cxyz2yzx_dev": [P, P, P, I, I, I],
+            "ductgpu_cyzx2xyz_dev": [P, P, P, I, I, I],
+            "ductgpu_chx2z_dev": [P, P, P, I, I, I],
+            "ductgpu_chz2x_dev": [P, P, P, I, I, I],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -211,6 +221,21 @@ class Context:
             arr[i].bound = f["bound"].encode()
         self._check(lib().ductgpu_solve_fields_dev(self.h, arr, len(fields), int(precision)))
         return keep
+
+    def transyz(self, f, cdir, iopt):
+        """transyz on a host complex (my,mz,nmodes) field; returns a copy."""
+        f = np.array(f, dtype=np.complex128, order="F")
+        my, mz, nm = f.shape
+        self._check(lib().ductgpu_transyz(self.h, _ptr(f), my, mz, nm, cdir.encode(), int(iopt)))
+        return f
+
+    def derivyz(self, u, cdir, ider, scal=1.0, what="n", du=None, aspect=1.0):
+        u = np.asfortranarray(u, dtype=np.complex128)
+        my, mz, nm = u.shape
+        du = np.zeros_like(u, order="F") if du is None else np.array(du, dtype=np.complex128, order="F")
+        self._check(lib().ductgpu_derivyz(self.h, _ptr(u), _ptr(du), my, mz, nm, cdir.encode(), int(ider),
+                                          float(scal), what.encode(), float(aspect)))
+        return du
 
     def device_array(self, shape, dtype=np.complex128):
         return DeviceArray(self, shape, dtype)

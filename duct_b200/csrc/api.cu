@@ -342,6 +342,120 @@ int ductgpu_helm3d(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, char bou
     return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d");
 }
 
+static int check_field(ductgpu_ctx ctx, const void *a, int my, int mz, int nmodes)
+{
+    if (!a) return set_error(ctx, DUCTGPU_EARG, "null field");
+    if (my < 2 || mz < 2 || nmodes < 1) return set_error(ctx, DUCTGPU_EARG, "my=%d mz=%d nmodes=%d", my, mz, nmodes);
+    if ((uintptr_t)a & 15) return set_error(ctx, DUCTGPU_EARG, "field must be 16-byte aligned");
+    return DUCTGPU_OK;
+}
+
+int ductgpu_transyz_dev(ductgpu_ctx ctx, double *field, int my, int mz, int nmodes, char cdir, int iopt)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_field(ctx, field, my, mz, nmodes);
+    if (rc) return rc;
+    if (cdir != 'y' && cdir != 'z') return set_error(ctx, DUCTGPU_EARG, "err in transyz: cdir '%c'", cdir);
+    cudaSetDevice(ctx->device);
+    return transyz_dev(ctx, field, my, mz, nmodes, cdir, iopt);
+}
+
+// Host-array variant: copies through the context's io workspace.
+static int host_roundtrip(ductgpu_ctx ctx, double *host, size_t bytes, double **dev)
+{
+    int rc = ensure(ctx, ctx->io, 2 * bytes);
+    if (rc) return rc;
+    *dev = ctx->io.buf;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(*dev, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    return DUCTGPU_OK;
+}
+
+int ductgpu_transyz(ductgpu_ctx ctx, double *field, int my, int mz, int nmodes, char cdir, int iopt)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_field(ctx, field, my, mz, nmodes);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    const size_t bytes = (size_t)2 * my * mz * nmodes * sizeof(double);
+    double *d = nullptr;
+    if ((rc = host_roundtrip(ctx, field, bytes, &d))) return rc;
+    if ((rc = ductgpu_transyz_dev(ctx, d, my, mz, nmodes, cdir, iopt))) return rc;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(field, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "transyz");
+}
+
+int ductgpu_derivyz_dev(ductgpu_ctx ctx, const double *u, double *du, int my, int mz, int nmodes, char cdir,
+                        int ider, double scal, char what, double aspect)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_field(ctx, u, my, mz, nmodes);
+    if (rc || (rc = check_field(ctx, du, my, mz, nmodes))) return rc;
+    if (cdir != 'y' && cdir != 'z') return set_error(ctx, DUCTGPU_EARG, "problem in derivyz: direction '%c'", cdir);
+    if (ider != 1 && ider != 2) return set_error(ctx, DUCTGPU_EARG, "this order of deriv not implemented: %d", ider);
+    if (u == du) return set_error(ctx, DUCTGPU_EARG, "derivyz: u and du must not overlap");
+    cudaSetDevice(ctx->device);
+    return derivyz_dev(ctx, u, du, my, mz, nmodes, cdir, ider, scal, what, aspect);
+}
+
+int ductgpu_derivyz(ductgpu_ctx ctx, const double *u, double *du, int my, int mz, int nmodes, char cdir,
+                    int ider, double scal, char what, double aspect)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_field(ctx, u, my, mz, nmodes);
+    if (rc || (rc = check_field(ctx, du, my, mz, nmodes))) return rc;
+    cudaSetDevice(ctx->device);
+    const size_t bytes = (size_t)2 * my * mz * nmodes * sizeof(double);
+    if ((rc = ensure(ctx, ctx->io, 2 * bytes))) return rc;
+    double *du_d = ctx->io.buf, *u_d = ctx->io.buf + bytes / sizeof(double);
+    DUCT_CUDA(ctx, cudaMemcpyAsync(u_d, u, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(du_d, du, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = ductgpu_derivyz_dev(ctx, u_d, du_d, my, mz, nmodes, cdir, ider, scal, what, aspect))) return rc;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(du, du_d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "derivyz");
+}
+
+int ductgpu_cxyz2yzx_dev(ductgpu_ctx ctx, const double *phys, double *phys2, int nmodes, int my, int nz)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_field(ctx, phys, my, nz, nmodes);
+    if (rc || (rc = check_field(ctx, phys2, my, nz, nmodes))) return rc;
+    cudaSetDevice(ctx->device);
+    return transpose_dev(ctx, phys, phys2, nmodes, (long long)my * nz);
+}
+
+int ductgpu_cyzx2xyz_dev(ductgpu_ctx ctx, double *phys, const double *phys2, int nmodes, int my, int nz)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_field(ctx, phys, my, nz, nmodes);
+    if (rc || (rc = check_field(ctx, phys2, my, nz, nmodes))) return rc;
+    cudaSetDevice(ctx->device);
+    return transpose_dev(ctx, phys2, phys, (long long)my * nz, nmodes);
+}
+
+int ductgpu_chx2z_dev(ductgpu_ctx ctx, double *xy, double *xz, int my, int mz, int nmodes)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_field(ctx, xy, my, mz, nmodes);
+    if (rc || (rc = check_field(ctx, xz, my, mz, nmodes))) return rc;
+    if (xy == xz) return set_error(ctx, DUCTGPU_EARG, "chx2z: xy and xz must differ");
+    cudaSetDevice(ctx->device);
+    const size_t bytes = (size_t)2 * my * mz * nmodes * sizeof(double);
+    DUCT_CUDA(ctx, cudaMemcpyAsync(xz, xy, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    return transpose_dev(ctx, xz, xy, (long long)my * mz, nmodes);
+}
+
+int ductgpu_chz2x_dev(ductgpu_ctx ctx, double *xz, double *xy, int my, int mz, int nmodes)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_field(ctx, xy, my, mz, nmodes);
+    if (rc || (rc = check_field(ctx, xz, my, mz, nmodes))) return rc;
+    if (xy == xz) return set_error(ctx, DUCTGPU_EARG, "chz2x: xy and xz must differ");
+    cudaSetDevice(ctx->device);
+    if ((rc = transpose_dev(ctx, xz, xy, nmodes, (long long)my * mz))) return rc;
+    const size_t bytes = (size_t)2 * my * mz * nmodes * sizeof(double);
+    return check_cuda(ctx, cudaMemcpyAsync(xz, xy, bytes, cudaMemcpyDeviceToDevice, ctx->stream), "chz2x copy");
+}
+
 int ductgpu_device_alloc(ductgpu_ctx ctx, size_t bytes, void **ptr)
 {
     if (!ctx || !ptr) return DUCTGPU_EARG;

@@ -111,6 +111,12 @@ int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
 int zero_walls(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
 int neumann_fill(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
 
+// transforms.cu
+int transyz_dev(ductgpu_ctx ctx, double *f, int my, int mz, int nmodes, char cdir, int iopt);
+int derivyz_dev(ductgpu_ctx ctx, const double *u, double *du, int my, int mz, int nmodes, char cdir,
+                int ider, double scal, char what, double aspect);
+int transpose_dev(ductgpu_ctx ctx, const double *in, double *out, long long A, long long Q);
+
 }  // namespace duct
 
 #define DUCT_CUDA(ctx, call)                                         \

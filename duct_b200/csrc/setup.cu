@@ -97,19 +97,19 @@ __global__ void k_real_part(int n, const double *W, double *E)
 }
 
 // Pack an n x n column-major matrix A into the A-operand fragment order of
-// mma.sync m16n8k8 f64: element (row g + 8*(v&1), col t + 4*(v>>1)) of
-// 16x8 tile (mt, ks) goes to lane g*4+t, value v, stored at
-// ((ks*mtiles + mt)*32 + lane)*4 + v.  Outside n x n the packing is zero.
+// mma.sync m16n8k16 f64: element (row g + 8*(v&1), col t + 4*(v>>1)) of
+// 16x16 tile (mt, ks) goes to lane g*4+t, value v (0..7), stored at
+// ((ks*mtiles + mt)*32 + lane)*8 + v.  Outside n x n the packing is zero.
 __global__ void k_pack_a(int n, int kpad, int mtiles, const double *A, double *out)
 {
-    const int total = (kpad / 8) * mtiles * 128;
+    const int total = (kpad / 16) * mtiles * 256;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += gridDim.x * blockDim.x) {
-        const int v = idx & 3, lane = (idx >> 2) & 31, tile = idx >> 7;
+        const int v = idx & 7, lane = (idx >> 3) & 31, tile = idx >> 8;
         const int mt = tile % mtiles, ks = tile / mtiles;
         const int g = lane >> 2, t = lane & 3;
         const int row = mt * 16 + g + 8 * (v & 1);
-        const int col = ks * 8 + t + 4 * (v >> 1);
+        const int col = ks * 16 + t + 4 * (v >> 1);
         out[idx] = (row < n && col < n) ? A[row + (size_t)n * col] : 0.0;
     }
 }
@@ -136,7 +136,7 @@ int pack_operators(ductgpu_ctx ctx, BoundOps &b)
     // 4 warps along M, each owning mtiles/4 tiles of 16 rows.
     const int mt_per_warp = (n + 63) / 64;
     b.mtiles = 4 * mt_per_warp;
-    const size_t packed = (size_t)(b.kpad / 8) * b.mtiles * 128;
+    const size_t packed = (size_t)(b.kpad / 16) * b.mtiles * 256;
     cudaFree(b.Ppack);
     cudaFree(b.Qpack);
     b.Ppack = b.Qpack = nullptr;

@@ -15,8 +15,10 @@
 // shared memory and multiplies the whole padded operator against them, so
 // the transposes of the reference disappear into the addressing.  The
 // operator streams through shared memory in K chunks of 32 with cp.async,
-// pre-packed in the DMMA A-fragment order (one 16-byte load per fragment
-// half, no bank conflicts).
+// pre-packed in the DMMA A-fragment order (16-byte loads, no bank
+// conflicts); with 16-wide K chunks a CTA stays under 113 KB of shared
+// memory for n <= 127, so two CTAs share an SM and hide each other's
+// staging latency.
 #include <math.h>
 
 #include "internal.h"
@@ -25,7 +27,7 @@ namespace duct {
 
 constexpr int kLines = 32;   // complex lines per CTA
 constexpr int kNld = 68;     // leading dim of the staged tile (64 + 4 pad)
-constexpr int kKC = 32;      // K chunk of the streamed operator
+constexpr int kKC = 16;      // K chunk of the streamed operator (one k16 step)
 constexpr int kThreads = 256;
 
 struct PassField {
@@ -60,13 +62,17 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-__device__ __forceinline__ void dmma(double (&d)[4], const double (&a)[4], const double (&b)[2])
+// D += A(16x16) * B(16x8), fragments as in the PTX ISA for m16n8k16 f64:
+// a[v] = A[g + 8(v&1)][t + 4(v>>1)], b[v] = B[t + 4v][g],
+// d = {D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1]}.
+__device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[8], const double (&b)[4])
 {
     asm volatile(
-        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 "
-        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 "
+        "{%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
         : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+          "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
 template <int MTW>
@@ -74,7 +80,7 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
 {
     extern __shared__ __align__(16) double smem[];
     constexpr int mtiles = 4 * MTW;
-    constexpr int a_chunk = (kKC / 8) * mtiles * 128;
+    constexpr int a_chunk = (kKC / 16) * mtiles * 256;
     double *As = smem;
     double *Bs = smem + 2 * a_chunk;
 
@@ -140,27 +146,31 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
         __syncthreads();
         const double *Ab = As + (c & 1) * a_chunk;
 #pragma unroll
-        for (int ks = 0; ks < kKC / 8; ++ks) {
-            double a[MTW][4];
+        for (int ks = 0; ks < kKC / 16; ++ks) {
+            double a[MTW][8];
 #pragma unroll
             for (int mt = 0; mt < MTW; ++mt) {
                 const double2 *q = reinterpret_cast<const double2 *>(
-                    Ab + ((ks * mtiles + wm * MTW + mt) * 32 + lane) * 4);
-                const double2 q0 = q[0], q1 = q[1];
-                a[mt][0] = q0.x; a[mt][1] = q0.y; a[mt][2] = q1.x; a[mt][3] = q1.y;
+                    Ab + ((ks * mtiles + wm * MTW + mt) * 32 + lane) * 8);
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const double2 v = q[h];
+                    a[mt][2 * h] = v.x;
+                    a[mt][2 * h + 1] = v.y;
+                }
             }
-            const int kg = c * kKC + ks * 8 + t;
-            double b[4][2];
+            const int kg = c * kKC + ks * 16 + t;
+            double b[4][4];
 #pragma unroll
             for (int nt = 0; nt < 4; ++nt) {
                 const int col = wn * 32 + nt * 8 + g;
-                b[nt][0] = Bs[kg * kNld + col];
-                b[nt][1] = Bs[(kg + 4) * kNld + col];
+#pragma unroll
+                for (int v = 0; v < 4; ++v) b[nt][v] = Bs[(kg + 4 * v) * kNld + col];
             }
 #pragma unroll
             for (int mt = 0; mt < MTW; ++mt)
 #pragma unroll
-                for (int nt = 0; nt < 4; ++nt) dmma(acc[mt][nt], a[mt], b[nt]);
+                for (int nt = 0; nt < 4; ++nt) dmma16(acc[mt][nt], a[mt], b[nt]);
         }
         __syncthreads();
     }
@@ -201,7 +211,7 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
 
 static size_t pass_smem_bytes(int mtw, int kpad)
 {
-    const size_t a_chunk = (size_t)(kKC / 8) * (4 * mtw) * 128;
+    const size_t a_chunk = (size_t)(kKC / 16) * (4 * mtw) * 256;
     return (2 * a_chunk + (size_t)kpad * kNld) * sizeof(double);
 }
 
@@ -289,58 +299,70 @@ __device__ void block_sum(double (&v)[NV], double *red)
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) k_neumann_fill(const __grid_constant__ FillParams p)
+__device__ __forceinline__ int fill_field(const FillParams &p)
 {
-    __shared__ double red[8 * 8];
     int fi = 0;
     while (fi + 1 < p.nf && (int)blockIdx.x >= p.cta_start[fi + 1]) ++fi;
-    const int plane = blockIdx.x - p.cta_start[fi];
-    const int m = p.m, n = m - 2;
-    double2 *U = reinterpret_cast<double2 *>(p.sol[fi] + (long long)plane * p.plane_stride);
-    const double lam = p.lam[p.plane0[fi] + plane];
-    const bool mode0 = p.mode0[fi] && plane == 0;
-    const bool singular = fabs(lam) <= 1.0e-10 && p.io >= 0;
-    const double *DC = p.DC;
-    auto u = [&](int i, int j) -> double2 & { return U[i + (long long)m * j]; };
+    return fi;
+}
 
-    if (singular) {
-        // U = U0 + c p p^T with c = (wanted - U0(io,io)) / p(io)^2: the value
-        // of the solution at interior point (iofzero+1, iofzero+1) becomes
-        // wanted (the reference's FT(iofzero,iofzero) choice).
-        const int io = p.io;
-        const double2 u0 = u(io + 1, io + 1);
-        __syncthreads();
-        const double pio = p.pcol[io];
-        const double2 cc = make_double2((p.wanted - u0.x) / (pio * pio), (p.wanted - u0.y) / (pio * pio));
-        for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-            const int i = idx % n, j = idx / n;
-            u(i + 1, j + 1) = u(i + 1, j + 1) + (p.pcol[i] * p.pcol[j]) * cc;
-        }
-        __syncthreads();
+// Singular kx=0 Neumann plane: U = U0 + c p p^T with
+// c = (wanted - U0(io,io)) / p(io)^2, so that the interior point
+// (iofzero+1, iofzero+1) takes the value wanted (src/solvediag.f90:195-206,
+// the reference's choice of FT(iofzero,iofzero)).  One CTA per plane: the
+// pinned value is read before any thread writes.
+__global__ void __launch_bounds__(1024) k_neumann_pin(const __grid_constant__ FillParams p)
+{
+    const int fi = fill_field(p);
+    const int plane = blockIdx.x - p.cta_start[fi];
+    const double lam = p.lam[p.plane0[fi] + plane];
+    if (!(fabs(lam) <= 1.0e-10) || p.io < 0) return;
+    const int m = p.m, n = m - 2, io = p.io;
+    double2 *U = reinterpret_cast<double2 *>(p.sol[fi] + (long long)plane * p.plane_stride);
+    const double2 u0 = U[(io + 1) + (long long)m * (io + 1)];
+    __syncthreads();
+    const double pio = p.pcol[io];
+    const double2 cc = make_double2((p.wanted - u0.x) / (pio * pio), (p.wanted - u0.y) / (pio * pio));
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int i = idx % n, j = idx / n;
+        const double w = p.pcol[i] * p.pcol[j];
+        double2 &u = U[(i + 1) + (long long)m * (j + 1)];
+        u = make_double2(u.x + w * cc.x, u.y + w * cc.y);
     }
+}
+
+// Neumann wall lines from the interior (src/solvediag.f90:253-276):
+// blockIdx.y = 0: z-walls U(i,1), U(i,m) of every interior row i (one thread
+// per row, sums over j); blockIdx.y = 1: y-walls U(1,j), U(m,j) of every
+// interior column j (one warp per column, sums over i).
+__global__ void __launch_bounds__(256) k_neumann_walls(const __grid_constant__ FillParams p)
+{
+    const int fi = fill_field(p);
+    const int plane = blockIdx.x - p.cta_start[fi];
+    const int m = p.m;
+    double2 *U = reinterpret_cast<double2 *>(p.sol[fi] + (long long)plane * p.plane_stride);
+    const double *DC = p.DC;
     const double d11 = DC[0], d1m = DC[(long long)m * (m - 1)];
     const double dm1 = DC[m - 1], dmm = DC[(m - 1) + (long long)m * (m - 1)];
     const double det = d11 * dmm - d1m * dm1;
-    // z-walls U(i,1), U(i,m) of each interior row i: sums over j, one thread per i.
-    for (int i = 1 + threadIdx.x; i < m - 1; i += blockDim.x) {
-        double2 sb = make_double2(0.0, 0.0), st = sb;
-        for (int j = 1; j < m - 1; ++j) {
-            const double2 v = u(i, j);
-            sb = sb + DC[(long long)m * j] * v;
-            st = st + DC[(m - 1) + (long long)m * j] * v;
+    if (blockIdx.y == 0) {
+        for (int i = 1 + threadIdx.x; i < m - 1; i += blockDim.x) {
+            double sb0 = 0, sb1 = 0, st0 = 0, st1 = 0;
+            for (int j = 1; j < m - 1; ++j) {
+                const double2 v = U[i + (long long)m * j];
+                const double a = DC[(long long)m * j], b = DC[(m - 1) + (long long)m * j];
+                sb0 += a * v.x; sb1 += a * v.y; st0 += b * v.x; st1 += b * v.y;
+            }
+            U[i] = make_double2((-dmm * sb0 + d1m * st0) / det, (-dmm * sb1 + d1m * st1) / det);
+            U[i + (long long)m * (m - 1)] =
+                make_double2((dm1 * sb0 - d11 * st0) / det, (dm1 * sb1 - d11 * st1) / det);
         }
-        u(i, 0) = (-dmm) * sb + d1m * st;
-        u(i, 0) = make_double2(u(i, 0).x / det, u(i, 0).y / det);
-        double2 w = dm1 * sb + (-d11) * st;
-        u(i, m - 1) = make_double2(w.x / det, w.y / det);
-    }
-    // y-walls U(1,j), U(m,j) of each interior column j: one warp per j.
-    {
+    } else {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
         for (int j = 1 + warp; j < m - 1; j += nw) {
             double sl[4] = {0, 0, 0, 0};
             for (int i = 1 + lane; i < m - 1; i += 32) {
-                const double2 v = u(i, j);
+                const double2 v = U[i + (long long)m * j];
                 const double a = DC[(long long)m * i], b = DC[(m - 1) + (long long)m * i];
                 sl[0] += a * v.x; sl[1] += a * v.y; sl[2] += b * v.x; sl[3] += b * v.y;
             }
@@ -348,42 +370,52 @@ __global__ void __launch_bounds__(256) k_neumann_fill(const __grid_constant__ Fi
             for (int q = 0; q < 4; ++q)
                 for (int o = 16; o > 0; o >>= 1) sl[q] += __shfl_xor_sync(0xffffffffu, sl[q], o);
             if (lane == 0) {
-                u(0, j) = make_double2((-dmm * sl[0] + d1m * sl[2]) / det, (-dmm * sl[1] + d1m * sl[3]) / det);
-                u(m - 1, j) = make_double2((dm1 * sl[0] - d11 * sl[2]) / det, (dm1 * sl[1] - d11 * sl[3]) / det);
+                U[(long long)m * j] = make_double2((-dmm * sl[0] + d1m * sl[2]) / det, (-dmm * sl[1] + d1m * sl[3]) / det);
+                U[(m - 1) + (long long)m * j] = make_double2((dm1 * sl[0] - d11 * sl[2]) / det, (dm1 * sl[1] - d11 * sl[3]) / det);
             }
         }
     }
-    __syncthreads();
-    // corners
-    {
-        double f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int i = 1 + threadIdx.x; i < m - 1; i += blockDim.x) {
-            const double a = DC[(long long)m * i], b = DC[(m - 1) + (long long)m * i];
-            const double2 ui0 = u(i, 0), u0i = u(0, i), umi = u(m - 1, i), uim = u(i, m - 1);
-            f[0] += -a * (ui0.x + u0i.x);            f[1] += -a * (ui0.y + u0i.y);
-            f[2] += -a * umi.x + b * ui0.x;          f[3] += -a * umi.y + b * ui0.y;
-            f[4] += -b * (uim.x + umi.x);            f[5] += -b * (uim.y + umi.y);
-            f[6] += -a * uim.x + b * u0i.x;          f[7] += -a * uim.y + b * u0i.y;
-        }
-        block_sum<8>(f, red);
-        if (threadIdx.x == 0) {
-            const double *A = p.AM1;
-            double c[8];
-            for (int r = 0; r < 4; ++r) {
-                c[2 * r] = c[2 * r + 1] = 0.0;
-                for (int i = 0; i < 4; ++i) {
-                    c[2 * r] += A[r + 4 * i] * f[2 * i];
-                    c[2 * r + 1] += A[r + 4 * i] * f[2 * i + 1];
-                }
+}
+
+// Corners from the wall lines through AM1 (src/solvediag.f90:278-322) and,
+// for the zero-mean gauge, the constant shift of the singular plane.
+__global__ void __launch_bounds__(256) k_neumann_corners(const __grid_constant__ FillParams p)
+{
+    __shared__ double red[8 * 8];
+    const int fi = fill_field(p);
+    const int plane = blockIdx.x - p.cta_start[fi];
+    const int m = p.m;
+    double2 *U = reinterpret_cast<double2 *>(p.sol[fi] + (long long)plane * p.plane_stride);
+    auto u = [&](int i, int j) -> double2 & { return U[i + (long long)m * j]; };
+    const double *DC = p.DC;
+    double f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = 1 + threadIdx.x; i < m - 1; i += blockDim.x) {
+        const double a = DC[(long long)m * i], b = DC[(m - 1) + (long long)m * i];
+        const double2 ui0 = u(i, 0), u0i = u(0, i), umi = u(m - 1, i), uim = u(i, m - 1);
+        f[0] += -a * (ui0.x + u0i.x);            f[1] += -a * (ui0.y + u0i.y);
+        f[2] += -a * umi.x + b * ui0.x;          f[3] += -a * umi.y + b * ui0.y;
+        f[4] += -b * (uim.x + umi.x);            f[5] += -b * (uim.y + umi.y);
+        f[6] += -a * uim.x + b * u0i.x;          f[7] += -a * uim.y + b * u0i.y;
+    }
+    block_sum<8>(f, red);
+    if (threadIdx.x == 0) {
+        const double *A = p.AM1;
+        double c[8];
+        for (int r = 0; r < 4; ++r) {
+            c[2 * r] = c[2 * r + 1] = 0.0;
+            for (int i = 0; i < 4; ++i) {
+                c[2 * r] += A[r + 4 * i] * f[2 * i];
+                c[2 * r + 1] += A[r + 4 * i] * f[2 * i + 1];
             }
-            u(0, 0) = make_double2(c[0], c[1]);
-            u(m - 1, 0) = make_double2(c[2], c[3]);
-            u(m - 1, m - 1) = make_double2(c[4], c[5]);
-            u(0, m - 1) = make_double2(c[6], c[7]);
         }
+        u(0, 0) = make_double2(c[0], c[1]);
+        u(m - 1, 0) = make_double2(c[2], c[3]);
+        u(m - 1, m - 1) = make_double2(c[4], c[5]);
+        u(0, m - 1) = make_double2(c[6], c[7]);
+    }
+    const double lam = p.lam[p.plane0[fi] + plane];
+    if (p.gauge == DUCTGPU_GAUGE_MEAN && fabs(lam) <= 1.0e-10) {
         __syncthreads();
-    }
-    if (singular && p.gauge == DUCTGPU_GAUGE_MEAN) {
         // Zero mean over [-1,1]^2 with the Clenshaw-Curtis weights of the
         // nodes: subtract integral/4 (a constant keeps the Neumann walls).
         double s[2] = {0.0, 0.0};
@@ -399,13 +431,7 @@ __global__ void __launch_bounds__(256) k_neumann_fill(const __grid_constant__ Fi
             const int i = idx % m, j = idx / m;
             u(i, j) = make_double2(u(i, j).x - 0.25 * s[0], u(i, j).y - 0.25 * s[1]);
         }
-        __syncthreads();
     }
-    if (mode0)
-        for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
-            const int i = idx % m, j = idx / m;
-            u(i, j).y = 0.0;
-        }
 }
 
 // ---------------------------------------------------------------------------
@@ -533,9 +559,17 @@ int neumann_fill(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
     fp.plane_stride = 2LL * ctx->my * ctx->my;
     {
         LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
-        k_neumann_fill<<<cta, 256, 0, ctx->stream>>>(fp);
+        k_neumann_pin<<<cta, 1024, 0, ctx->stream>>>(fp);
     }
-    return check_cuda(ctx, cudaGetLastError(), "k_neumann_fill");
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
+        k_neumann_walls<<<dim3(cta, 2), 256, 0, ctx->stream>>>(fp);
+    }
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
+        k_neumann_corners<<<cta, 256, 0, ctx->stream>>>(fp);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "k_neumann");
 }
 
 }  // namespace duct

@@ -113,6 +113,44 @@ typedef struct {
 int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields,
                              int nfields, int precision);
 
+/* ---- Chebyshev transforms, derivatives, pencil transposes ------------ */
+/* transyz(cheb,cdir,iopt), src/chebyshev.f90:458-540 with tcheb_fftw,
+ * src/tchebw.f:62-192: DCT-I of every line of a complex (my,mz,nmodes)
+ * field along cdir = 'y' or 'z', in place.  iopt < 0: physical ->
+ * Chebyshev (ends scaled 1/(2(n-1)), interior 1/(n-1)); iopt >= 0: the
+ * inverse.  The line length minus one must be 2^a 3^b (as the reference's
+ * FFTW plans assume, src/tchebw.f:11-12).                                 */
+int ductgpu_transyz_dev(ductgpu_ctx ctx, double *field, int my, int mz, int nmodes,
+                        char cdir, int iopt);
+int ductgpu_transyz(ductgpu_ctx ctx, double *field, int my, int mz, int nmodes,
+                    char cdir, int iopt);
+
+/* derivyz(u,du,aux,cdir,ider,scal,what), src/chebyshev.f90:1-295: first or
+ * second derivative (ider = 1, 2) of a Chebyshev-space complex field along
+ * cdir; z derivatives carry 1/aspect^ider.  what = 'n' overwrites du,
+ * anything else accumulates into it.  u and du must not overlap.         */
+int ductgpu_derivyz_dev(ductgpu_ctx ctx, const double *u, double *du, int my, int mz,
+                        int nmodes, char cdir, int ider, double scal, char what,
+                        double aspect);
+int ductgpu_derivyz(ductgpu_ctx ctx, const double *u, double *du, int my, int mz,
+                    int nmodes, char cdir, int ider, double scal, char what,
+                    double aspect);
+
+/* Local pencil transposes of one rank, src/parallel.F:476-529 (complex):
+ * cxyz2yzx: phys(0:mx1,my,nz) -> phys2(my,nz,0:mx1)
+ * cyzx2xyz: phys2(my,nz,0:mx1) -> phys(0:mx1,my,nz)                       */
+int ductgpu_cxyz2yzx_dev(ductgpu_ctx ctx, const double *phys, double *phys2,
+                         int nmodes, int my, int nz);
+int ductgpu_cyzx2xyz_dev(ductgpu_ctx ctx, double *phys, const double *phys2,
+                         int nmodes, int my, int nz);
+/* chx2z(xy,xz,wk2) and chz2x(xz,xy,wk2) on one rank, src/parallel.F:1-208:
+ * chx2z: xz <- xy (y,z,x layout), xy <- x-fastest transpose of it;
+ * chz2x: the inverse (xy <- y-fastest transpose of xz, xz <- xy).  The
+ * reference's chz2x returns before its transpose on one rank
+ * (src/parallel.F:132); this is the inverse of chx2z it documents.        */
+int ductgpu_chx2z_dev(ductgpu_ctx ctx, double *xy, double *xz, int my, int mz, int nmodes);
+int ductgpu_chz2x_dev(ductgpu_ctx ctx, double *xz, double *xy, int my, int mz, int nmodes);
+
 /* ---- memory helpers (for callers without a CUDA toolchain, e.g. Fortran
  * hosts that keep fields resident on the device between time steps) ---- */
 int ductgpu_device_alloc(ductgpu_ctx ctx, size_t bytes, void **ptr);
