@@ -28,6 +28,7 @@ EXPORTS = [
     "ductgpu_profile_enable", "ductgpu_profile_reset", "ductgpu_profile_read",
     "ductgpu_transyz_dev", "ductgpu_transyz", "ductgpu_derivyz_dev", "ductgpu_derivyz",
     "ductgpu_cxyz2yzx_dev", "ductgpu_cyzx2xyz_dev", "ductgpu_chx2z_dev", "ductgpu_chz2x_dev",
+    "ductgpu_set_refinement",
 ]
 K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
 
@@ -82,6 +83,7 @@ def lib():
             "ductgpu_cyzx2xyz_dev": [P, P, P, I, I, I],
             "ductgpu_chx2z_dev": [P, P, P, I, I, I],
             "ductgpu_chz2x_dev": [P, P, P, I, I, I],
+            "ductgpu_set_refinement": [P, I],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -186,6 +188,9 @@ class Context:
         P = np.asfortranarray(P, dtype=np.float64)
         PM1 = np.asfortranarray(PM1, dtype=np.float64)
         self._check(lib().ductgpu_set_operators(self.h, bound.encode(), _ptr(E), _ptr(P), _ptr(PM1), int(iofzero)))
+
+    def set_refinement(self, steps):
+        self._check(lib().ductgpu_set_refinement(self.h, int(steps)))
 
     def set_gauge(self, gauge):
         self._check(lib().ductgpu_set_gauge(self.h, int(gauge)))

@@ -93,7 +93,19 @@ static int prepare(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, Fi
         tasks[i].mode0 = (f.ib == 0);
         tasks[i].bound = f.bound;
         tasks[i].plane0 = p;
-        for (int k = 0; k < f.nmodes; ++k) ctx->lam_host[p + k] = f.alambda + f.xalp[k] * f.xalp[k];
+        // refinement steps from the spectral condition number of the worst
+        // plane: (2 max|E| + lam) / (2 min|E| + lam); well-conditioned
+        // fields (e.g. the implicit viscous step, lam = 2/(nu dt)) converge
+        // in one step, Poisson-like fields get the configured maximum.
+        const BoundOps &b = (f.bound == 'n') ? ctx->neu : ctx->dir;
+        double kappa = 0.0;
+        for (int k = 0; k < f.nmodes; ++k) {
+            const double lam = f.alambda + f.xalp[k] * f.xalp[k];
+            ctx->lam_host[p + k] = lam;
+            const double lo = 2.0 * b.emin + lam;
+            kappa = fmax(kappa, lo > 0.0 ? (2.0 * b.emax + lam) / lo : 1e300);
+        }
+        tasks[i].refine = (kappa <= 1.0e3 && ctx->refine_steps > 0) ? 1 : ctx->refine_steps;
         p += f.nmodes;
     }
     DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->lam, ctx->lam_host, planes * sizeof(double),
@@ -147,6 +159,8 @@ int ductgpu_create(int device, ductgpu_ctx *out)
     ductgpu_ctx c = new (std::nothrow) ductgpu_ctx_s();
     if (!c) return DUCTGPU_EALLOC;
     c->device = device;
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (c->num_sms < 1) c->num_sms = 1;
     if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
         return DUCTGPU_ECUDA;
@@ -159,6 +173,12 @@ int ductgpu_create(int device, ductgpu_ctx *out)
         return DUCTGPU_ESOLVER;
     }
     for (int i = 0; i < kNumEvents; ++i) cudaEventCreate(&c->ev[i]);
+    if (cudaMalloc(&c->dev_err, sizeof(int)) != cudaSuccess || cudaMemset(c->dev_err, 0, sizeof(int)) != cudaSuccess) {
+        cusolverDnDestroy(c->solver);
+        cudaStreamDestroy(c->own_stream);
+        delete c;
+        return DUCTGPU_EALLOC;
+    }
     *out = c;
     return DUCTGPU_OK;
 }
@@ -173,6 +193,7 @@ int ductgpu_destroy(ductgpu_ctx ctx)
     cudaFree(ctx->xcol); cudaFree(ctx->DC); cudaFree(ctx->D2); cudaFree(ctx->AM1); cudaFree(ctx->ccw);
     cudaFree(ctx->work.buf);
     cudaFree(ctx->io.buf);
+    cudaFree(ctx->dev_err);
     cudaFree(ctx->lam);
     cudaFreeHost(ctx->lam_host);
     for (int i = 0; i < kNumEvents; ++i) cudaEventDestroy(ctx->ev[i]);
@@ -203,10 +224,24 @@ int ductgpu_set_stream(ductgpu_ctx ctx, void *cuda_stream)
 
 void *ductgpu_get_stream(ductgpu_ctx ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
+// Reads and clears the device error word set by bounded waits in kernels.
+static int device_status(ductgpu_ctx ctx)
+{
+    int h = 0;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(&h, ctx->dev_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h) {
+        cudaMemsetAsync(ctx->dev_err, 0, sizeof(int), ctx->stream);
+        return set_error(ctx, DUCTGPU_ETIMEOUT, "a bounded device-side wait ran out (code %d)", h);
+    }
+    return DUCTGPU_OK;
+}
+
 int ductgpu_synchronize(ductgpu_ctx ctx)
 {
     if (!ctx) return DUCTGPU_EARG;
-    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "synchronize");
+    int rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "synchronize");
+    return rc ? rc : device_status(ctx);
 }
 
 int ductgpu_pseudomat(ductgpu_ctx ctx, int my, int mz)
@@ -244,6 +279,12 @@ int ductgpu_set_operators(ductgpu_ctx ctx, char bound, const double *E, const do
     DUCT_CUDA(ctx, cudaMemcpyAsync(b.E, E, b.n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     DUCT_CUDA(ctx, cudaMemcpyAsync(b.P, P, nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     DUCT_CUDA(ctx, cudaMemcpyAsync(b.PM1, PM1, nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    {
+        double emin = 1e300, emax = 0.0;
+        for (int i = 0; i < b.n; ++i) { emin = fmin(emin, fabs(E[i])); emax = fmax(emax, fabs(E[i])); }
+        b.emin = emin;
+        b.emax = emax;
+    }
     if (bound == 'n') {
         if (iofzero <= 0) {
             double eigmin = 1.0e6;
@@ -270,6 +311,14 @@ int ductgpu_set_gauge(ductgpu_ctx ctx, int gauge)
     return DUCTGPU_OK;
 }
 
+int ductgpu_set_refinement(ductgpu_ctx ctx, int steps)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (steps < 0 || steps > 4) return set_error(ctx, DUCTGPU_EARG, "refinement steps %d (0..4)", steps);
+    ctx->refine_steps = steps;
+    return DUCTGPU_OK;
+}
+
 int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, int precision)
 {
     if (!ctx) return DUCTGPU_EARG;
@@ -286,8 +335,7 @@ int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields, int n
     FieldTask tasks[kMaxFields];
     int rc = prepare(ctx, fields, nfields, tasks);
     if (rc) return rc;
-    if (precision == DUCTGPU_PREC_MIXED)
-        return set_error(ctx, DUCTGPU_EARG, "mixed precision not built yet");
+    if (precision == DUCTGPU_PREC_MIXED) return solve_mixed(ctx, tasks, nfields);
     return solve_fp64(ctx, tasks, nfields);
 }
 
@@ -339,7 +387,8 @@ int ductgpu_helm3d(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, char bou
     rc = ductgpu_solve_fields_dev(ctx, &f, 1, precision);
     if (rc) return rc;
     DUCT_CUDA(ctx, cudaMemcpyAsync(sol, dsol, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d");
+    rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d");
+    return rc ? rc : (precision == DUCTGPU_PREC_MIXED ? device_status(ctx) : DUCTGPU_OK);
 }
 
 static int check_field(ductgpu_ctx ctx, const void *a, int my, int mz, int nmodes)

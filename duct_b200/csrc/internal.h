@@ -30,7 +30,13 @@ struct BoundOps {
     double *Ppack = nullptr;   // P in DMMA A-fragment order, zero padded
     double *Qpack = nullptr;   // PM1 in DMMA A-fragment order
     double *pcol = nullptr;    // [n] column iofzero of P (Neumann pin)
+    double *qrow = nullptr;    // [n] row iofzero of P^-1 (null-space projection)
     int iofzero = 0;           // 1-based, Neumann only
+    double emin = 0.0, emax = 0.0;   // smallest / largest |eigenvalue| (host)
+    double *D2B = nullptr;     // [n*n] the interior operator block itself
+    double *Bpack = nullptr;   // D2B in DMMA A-fragment order (residual)
+    uint8_t *Pslices = nullptr, *Qslices = nullptr;  // BF16 slices (mixed)
+    int *Pexp = nullptr, *Qexp = nullptr;            // per-row exponents
 };
 
 struct Workspace {
@@ -42,6 +48,7 @@ struct Workspace {
 
 struct ductgpu_ctx_s {
     int device = 0;
+    int num_sms = 148;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     cusolverDnHandle_t solver = nullptr;
@@ -56,10 +63,12 @@ struct ductgpu_ctx_s {
     double *ccw = nullptr;     // [my] Clenshaw-Curtis weights on the nodes
     double wanted = 0.0;
     int gauge = DUCTGPU_GAUGE_POINT;
+    int refine_steps = 2;      // FP64 refinement steps of the split-precision path
     duct::BoundOps dir, neu;
 
     duct::Workspace work;      // pass intermediates
     duct::Workspace io;        // device copies for host entries
+    int *dev_err = nullptr;    // device error word (bounded waits)
     double *lam = nullptr;     // per-plane lambda (device)
     double *lam_host = nullptr;// pinned staging
     int lam_cap = 0;
@@ -106,8 +115,41 @@ struct FieldTask {
     int mode0;        // 1: first plane is Fourier mode 0
     char bound;
     int plane0;       // index of the first plane in ctx->lam
+    int refine;       // FP64 refinement steps for the split-precision path
 };
 int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
+
+// One batched FP64 GEMM pass (k_pass_fp64), usable by other solvers.
+struct PassField {
+    const double *src;
+    double *dst;
+    const double *A;     // packed operator
+    const double *E;     // eigenvalues for the divide
+    int nmodes;
+    int mode0;
+    int plane0;
+    int sing_io;         // 0-based iofzero of a Neumann field, else -1
+    // residual epilogue: dst = resF - resT - acc + lam * resU
+    const double *resF, *resT, *resU;
+};
+struct PassParams {
+    PassField f[kMaxFields];
+    int cta_start[kMaxFields + 1];
+    int nf;
+    const double *lam;
+    long long plane_stride;  // doubles per complex plane
+    int n, kpad, nchunks;
+    int sk, sl;              // complex strides of (k, line)
+    int divide;
+    int zero_im_mode0;
+    int residual;
+};
+constexpr int kPassLines = 32;
+int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid);
+
+// solve_mixed.cu
+int split_operator(ductgpu_ctx ctx, int n, const double *A, uint8_t **slices, int **rexp);
+int solve_mixed(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
 int zero_walls(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
 int neumann_fill(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
 

@@ -120,12 +120,20 @@ __global__ void k_copy_col(int n, const double *P, int col, double *out)
         out[i] = P[i + (size_t)n * col];
 }
 
+__global__ void k_copy_row(int n, const double *Q, int row, double *out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = Q[row + (size_t)n * i];
+}
+
 static int blocks_for(long n) { return (int)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184); }
 
 void free_bound(BoundOps &b)
 {
     cudaFree(b.E); cudaFree(b.P); cudaFree(b.PM1);
-    cudaFree(b.Ppack); cudaFree(b.Qpack); cudaFree(b.pcol);
+    cudaFree(b.Ppack); cudaFree(b.Qpack); cudaFree(b.pcol); cudaFree(b.qrow);
+    cudaFree(b.D2B); cudaFree(b.Bpack);
+    cudaFree(b.Pslices); cudaFree(b.Qslices); cudaFree(b.Pexp); cudaFree(b.Qexp);
     b = BoundOps();
 }
 
@@ -145,10 +153,23 @@ int pack_operators(ductgpu_ctx ctx, BoundOps &b)
     k_pack_a<<<blocks_for((long)packed), 256, 0, ctx->stream>>>(n, b.kpad, b.mtiles, b.P, b.Ppack);
     k_pack_a<<<blocks_for((long)packed), 256, 0, ctx->stream>>>(n, b.kpad, b.mtiles, b.PM1, b.Qpack);
     ctx->launches += 2;
+    if (b.D2B) {
+        if (!b.Bpack) DUCT_CUDA(ctx, cudaMalloc(&b.Bpack, packed * sizeof(double)));
+        k_pack_a<<<blocks_for((long)packed), 256, 0, ctx->stream>>>(n, b.kpad, b.mtiles, b.D2B, b.Bpack);
+        ctx->launches += 1;
+    }
+    // BF16 slices for the split-precision path (operators up to 128 rows)
+    if (n <= 127) {
+        int rc = split_operator(ctx, n, b.P, &b.Pslices, &b.Pexp);
+        if (rc) return rc;
+        if ((rc = split_operator(ctx, n, b.PM1, &b.Qslices, &b.Qexp))) return rc;
+    }
     if (b.iofzero > 0) {
         if (!b.pcol) DUCT_CUDA(ctx, cudaMalloc(&b.pcol, n * sizeof(double)));
         k_copy_col<<<1, 256, 0, ctx->stream>>>(n, b.P, b.iofzero - 1, b.pcol);
-        ctx->launches += 1;
+        if (!b.qrow) DUCT_CUDA(ctx, cudaMalloc(&b.qrow, n * sizeof(double)));
+        k_copy_row<<<1, 256, 0, ctx->stream>>>(n, b.PM1, b.iofzero - 1, b.qrow);
+        ctx->launches += 2;
     }
     return check_cuda(ctx, cudaGetLastError(), "pack_operators");
 }
@@ -224,6 +245,10 @@ static int eigen_gpu(ductgpu_ctx ctx, int n, double *B, BoundOps &b)
             imax = fmax(imax, fabs(Wh[2 * i + 1]));
         }
         if (imax > 1e-6 * emax) { rc = set_error(ctx, DUCTGPU_ESOLVER, "complex eigenvalues (|im| %.3e)", imax); goto out; }
+        double emin = emax;
+        for (int i = 0; i < n; ++i) emin = fmin(emin, fabs(Wh[2 * i]));
+        b.emin = emin;
+        b.emax = emax;
     }
     k_real_part<<<blocks_for(n), 256, 0, ctx->stream>>>(n, W, b.E);
     // inverse of P: getrf + getrs(P, I)
@@ -281,6 +306,7 @@ int pseudomat_gpu(ductgpu_ctx ctx, int m)
     DUCT_CUDA(ctx, cudaMalloc(&ctx->ccw, m * sizeof(double)));
     for (BoundOps *b : {&ctx->dir, &ctx->neu}) {
         b->n = n;
+        DUCT_CUDA(ctx, cudaMalloc(&b->D2B, (size_t)n * n * sizeof(double)));
         DUCT_CUDA(ctx, cudaMalloc(&b->E, n * sizeof(double)));
         DUCT_CUDA(ctx, cudaMalloc(&b->P, (size_t)n * n * sizeof(double)));
         DUCT_CUDA(ctx, cudaMalloc(&b->PM1, (size_t)n * n * sizeof(double)));
@@ -291,10 +317,12 @@ int pseudomat_gpu(ductgpu_ctx ctx, int m)
     k_matmul<<<blocks_for((long)m * m), 256, 0, ctx->stream>>>(m, ctx->DC, ctx->DC, ctx->D2);
     k_block<<<blocks_for((long)n * n), 256, 0, ctx->stream>>>(m, 0, ctx->DC, ctx->D2, blk);
     ctx->launches += 3;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->dir.D2B, blk, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     int rc = eigen_gpu(ctx, n, blk, ctx->dir);
     if (rc == DUCTGPU_OK) {
         k_block<<<blocks_for((long)n * n), 256, 0, ctx->stream>>>(m, 1, ctx->DC, ctx->D2, blk);
         ctx->launches += 1;
+        DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->neu.D2B, blk, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
         rc = eigen_gpu(ctx, n, blk, ctx->neu);
     }
     cudaFree(blk);

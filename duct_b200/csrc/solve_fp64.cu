@@ -25,33 +25,10 @@
 
 namespace duct {
 
-constexpr int kLines = 32;   // complex lines per CTA
+constexpr int kLines = kPassLines;   // complex lines per CTA
 constexpr int kNld = 68;     // leading dim of the staged tile (64 + 4 pad)
 constexpr int kKC = 16;      // K chunk of the streamed operator (one k16 step)
 constexpr int kThreads = 256;
-
-struct PassField {
-    const double *src;
-    double *dst;
-    const double *A;     // packed operator
-    const double *E;     // eigenvalues for the divide
-    int nmodes;
-    int mode0;
-    int plane0;
-    int sing_io;         // 0-based iofzero of a Neumann field, else -1
-};
-
-struct PassParams {
-    PassField f[kMaxFields];
-    int cta_start[kMaxFields + 1];
-    int nf;
-    const double *lam;
-    long long plane_stride;  // doubles per complex plane
-    int n, kpad, nchunks;
-    int sk, sl;              // complex strides of (k, line)
-    int divide;
-    int zero_im_mode0;
-};
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
 {
@@ -202,9 +179,17 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
                         im = im / den;
                     }
                 }
+                const long long off = 2 * ((long long)(o + 1) * sk + (long long)(lg + 1) * sl);
+                if (p.residual) {
+                    const long long po = (long long)plane * p.plane_stride + off;
+                    const double2 f = *reinterpret_cast<const double2 *>(F.resF + po);
+                    const double2 tt = *reinterpret_cast<const double2 *>(F.resT + po);
+                    const double2 uu = *reinterpret_cast<const double2 *>(F.resU + po);
+                    re = (f.x - tt.x) - re + lam * uu.x;
+                    im = (f.y - tt.y) - im + lam * uu.y;
+                }
                 if (im0) im = 0.0;
-                *reinterpret_cast<double2 *>(dst + 2 * ((long long)(o + 1) * sk + (long long)(lg + 1) * sl)) =
-                    make_double2(re, im);
+                *reinterpret_cast<double2 *>(dst + off) = make_double2(re, im);
             }
         }
 }
@@ -441,6 +426,18 @@ static int plane_count(const FieldTask *t, int nt)
     int s = 0;
     for (int i = 0; i < nt; ++i) s += t[i].nmodes;
     return s;
+}
+
+int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid)
+{
+    const int mtw = (pp.n + 63) / 64;
+    cudaError_t e;
+    switch (mtw) {
+    case 1: e = launch_pass<1>(ctx, pp, grid); break;
+    case 2: e = launch_pass<2>(ctx, pp, grid); break;
+    default: e = launch_pass<3>(ctx, pp, grid); break;
+    }
+    return e == cudaSuccess ? DUCTGPU_OK : check_cuda(ctx, e, "k_pass_fp64");
 }
 
 int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)

@@ -82,6 +82,11 @@ int ductgpu_set_operators(ductgpu_ctx ctx, char bound, const double *E,
 /* Gauge of the singular kx=0 Neumann mode (reference default: POINT).     */
 int ductgpu_set_gauge(ductgpu_ctx ctx, int gauge);
 
+/* FP64 iterative-refinement steps of DUCTGPU_PREC_MIXED (0..4, default 2):
+ * each step is one FP64 residual of the reference's interior operator and
+ * one more split-precision solve.                                          */
+int ductgpu_set_refinement(ductgpu_ctx ctx, int steps);
+
 /* ---- the 2D solve ------------------------------------------------------ */
 /* helm3d(rhs,sol,work,ipro,bound,cvar,a,b,alambda), src/helm3d.f90:2-76,
  * for one field on host arrays: solves lap(u) - (alambda + xalp(i)^2) u = f
