@@ -28,9 +28,17 @@ EXPORTS = [
     "ductgpu_profile_enable", "ductgpu_profile_reset", "ductgpu_profile_read",
     "ductgpu_transyz_dev", "ductgpu_transyz", "ductgpu_derivyz_dev", "ductgpu_derivyz",
     "ductgpu_cxyz2yzx_dev", "ductgpu_cyzx2xyz_dev", "ductgpu_chx2z_dev", "ductgpu_chz2x_dev",
-    "ductgpu_set_refinement",
+    "ductgpu_set_refinement", "ductgpu_pseudomat_temp", "ductgpu_helm3d_temp",
+    "ductgpu_solve_rect_fields_dev",
 ]
 K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
+
+
+class RectField(C.Structure):
+    """ductgpu_rect_field of include/ductgpu.h."""
+    _fields_ = [("rhs", C.c_void_p), ("sol", C.c_void_p), ("xalp", C.c_void_p), ("bcy", C.c_void_p),
+                ("bcz", C.c_void_p), ("alambda", C.c_double), ("ib", C.c_int), ("nmodes", C.c_int),
+                ("slot", C.c_int)]
 
 
 class Field(C.Structure):
@@ -84,6 +92,10 @@ def lib():
             "ductgpu_chx2z_dev": [P, P, P, I, I, I],
             "ductgpu_chz2x_dev": [P, P, P, I, I, I],
             "ductgpu_set_refinement": [P, I],
+            "ductgpu_pseudomat_temp": [P, I, I, I, D, D, C.c_char, C.c_char, C.c_char, C.c_char],
+            "ductgpu_helm3d_temp": [P, P, P, I, D, D, D, I, I, I, I, P, P, P, C.c_char, C.c_char,
+                                    C.c_char, C.c_char],
+            "ductgpu_solve_rect_fields_dev": [P, C.POINTER(RectField), I],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -208,6 +220,45 @@ class Context:
                                          float(alambda), my, mz, int(ib), int(ib) + nm - 1,
                                          _ptr(xalp), int(precision)))
         return sol
+
+    def pseudomat_temp(self, slot, my, mz, sy=1.0, sz=1.0, by=("d", "d"), bz=("d", "d")):
+        self._check(lib().ductgpu_pseudomat_temp(self.h, int(slot), int(my), int(mz), float(sy), float(sz),
+                                                 by[0].encode(), by[1].encode(), bz[0].encode(), bz[1].encode()))
+
+    def helm3d_temp(self, rhs, alambda, xalp, a=1.0, b=1.0, ib=0, bcy=None, bcz=None,
+                    by=("d", "d"), bz=("d", "d"), ipro=1):
+        """helm3d_temp drop-in on host arrays (operator slot 0)."""
+        assert rhs.dtype == np.complex128 and rhs.flags.f_contiguous
+        my, mz, nm = rhs.shape
+        sol = np.zeros_like(rhs, order="F")
+        xalp = np.ascontiguousarray(xalp, dtype=np.float64)
+        by_ = None if bcy is None else np.asfortranarray(bcy, dtype=np.float64)
+        bz_ = None if bcz is None else np.asfortranarray(bcz, dtype=np.float64)
+        self._check(lib().ductgpu_helm3d_temp(self.h, _ptr(rhs), _ptr(sol), int(ipro), float(a), float(b),
+                                              float(alambda), my, mz, int(ib), int(ib) + nm - 1, _ptr(xalp),
+                                              _ptr(by_), _ptr(bz_), by[0].encode(), by[1].encode(),
+                                              bz[0].encode(), bz[1].encode()))
+        return sol
+
+    def solve_rect_fields_dev(self, fields):
+        """fields: dicts(rhs, sol DeviceArray, xalp ndarray, alambda, ib, slot,
+        bcy/bcz DeviceArray or None)."""
+        arr = (RectField * len(fields))()
+        keep = []
+        for i, f in enumerate(fields):
+            xalp = np.ascontiguousarray(f["xalp"], dtype=np.float64)
+            keep.append(xalp)
+            arr[i].rhs = f["rhs"].ptr
+            arr[i].sol = f["sol"].ptr
+            arr[i].xalp = xalp.ctypes.data
+            arr[i].bcy = f["bcy"].ptr if f.get("bcy") is not None else None
+            arr[i].bcz = f["bcz"].ptr if f.get("bcz") is not None else None
+            arr[i].alambda = float(f["alambda"])
+            arr[i].ib = int(f.get("ib", 0))
+            arr[i].nmodes = int(xalp.shape[0])
+            arr[i].slot = int(f.get("slot", 0))
+        self._check(lib().ductgpu_solve_rect_fields_dev(self.h, arr, len(fields)))
+        return keep
 
     def solve_fields_dev(self, fields, precision=PREC_FP64):
         """fields: list of dicts(rhs=DeviceArray, sol=DeviceArray, xalp=ndarray,

@@ -190,6 +190,7 @@ int ductgpu_destroy(ductgpu_ctx ctx)
     cudaStreamSynchronize(ctx->stream);
     free_bound(ctx->dir);
     free_bound(ctx->neu);
+    for (int i = 0; i < kMaxRect; ++i) free_rect(ctx->rect[i]);
     cudaFree(ctx->xcol); cudaFree(ctx->DC); cudaFree(ctx->D2); cudaFree(ctx->AM1); cudaFree(ctx->ccw);
     cudaFree(ctx->work.buf);
     cudaFree(ctx->io.buf);
@@ -503,6 +504,93 @@ int ductgpu_chz2x_dev(ductgpu_ctx ctx, double *xz, double *xy, int my, int mz, i
     if ((rc = transpose_dev(ctx, xz, xy, nmodes, (long long)my * mz))) return rc;
     const size_t bytes = (size_t)2 * my * mz * nmodes * sizeof(double);
     return check_cuda(ctx, cudaMemcpyAsync(xz, xy, bytes, cudaMemcpyDeviceToDevice, ctx->stream), "chz2x copy");
+}
+
+int ductgpu_pseudomat_temp(ductgpu_ctx ctx, int slot, int my, int mz, double sy, double sz,
+                           char by1, char by2, char bz1, char bz2)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    cudaSetDevice(ctx->device);
+    return rect_setup(ctx, slot, my, mz, sy, sz, by1, by2, bz1, bz2);
+}
+
+int ductgpu_solve_rect_fields_dev(ductgpu_ctx ctx, const ductgpu_rect_field *fields, int nfields)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (!fields || nfields < 1 || nfields > kMaxFields)
+        return set_error(ctx, DUCTGPU_EARG, "nfields=%d (1..%d)", nfields, kMaxFields);
+    int planes = 0;
+    for (int i = 0; i < nfields; ++i) {
+        const ductgpu_rect_field &f = fields[i];
+        if (f.slot < 0 || f.slot >= kMaxRect || !ctx->rect[f.slot].ready)
+            return set_error(ctx, DUCTGPU_ESTATE, "rectangular slot %d not set up", f.slot);
+        if (!f.rhs || !f.sol || !f.xalp) return set_error(ctx, DUCTGPU_EARG, "null field pointer");
+        if (f.nmodes < 1 || f.ib < 0) return set_error(ctx, DUCTGPU_EARG, "nmodes=%d ib=%d", f.nmodes, f.ib);
+        if (((uintptr_t)f.rhs | (uintptr_t)f.sol) & 15) return set_error(ctx, DUCTGPU_EARG, "field arrays must be 16-byte aligned");
+        planes += f.nmodes;
+    }
+    cudaSetDevice(ctx->device);
+    int rc = ensure_lam(ctx, planes);
+    if (rc) return rc;
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    RectTask tasks[kMaxFields];
+    int p = 0;
+    for (int i = 0; i < nfields; ++i) {
+        const ductgpu_rect_field &f = fields[i];
+        tasks[i].rhs = f.rhs;
+        tasks[i].sol = f.sol;
+        tasks[i].bcy = f.bcy;
+        tasks[i].bcz = f.bcz;
+        tasks[i].nmodes = f.nmodes;
+        tasks[i].mode0 = (f.ib == 0);
+        tasks[i].plane0 = p;
+        tasks[i].slot = f.slot;
+        for (int k = 0; k < f.nmodes; ++k) ctx->lam_host[p + k] = f.alambda + f.xalp[k] * f.xalp[k];
+        p += f.nmodes;
+    }
+    DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->lam, ctx->lam_host, planes * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    return solve_rect(ctx, tasks, nfields);
+}
+
+int ductgpu_helm3d_temp(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, double a, double b, double alambda,
+                        int my, int mz, int ib, int ie, const double *xalp, const double *bcy, const double *bcz,
+                        char by1, char by2, char bz1, char bz2)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (ipro <= 0) {
+        int rc = ductgpu_pseudomat_temp(ctx, 0, my, mz, a, b, by1, by2, bz1, bz2);
+        if (rc) return rc;
+        if (ipro == -1) return DUCTGPU_OK;
+    }
+    const RectSlot &r = ctx->rect[0];
+    if (!r.ready) return set_error(ctx, DUCTGPU_ESTATE, "operators not set up (call with ipro<=0)");
+    if (my != r.my || mz != r.mz) return set_error(ctx, DUCTGPU_EARG, "grid %dx%d differs from the set-up %dx%d", my, mz, r.my, r.mz);
+    if (!rhs || !sol || !xalp) return set_error(ctx, DUCTGPU_EARG, "null pointer");
+    if (ie < ib || ib < 0) return set_error(ctx, DUCTGPU_EARG, "ib=%d ie=%d", ib, ie);
+    cudaSetDevice(ctx->device);
+    const int nm = ie - ib + 1;
+    const size_t bytes = (size_t)2 * my * mz * nm * sizeof(double);
+    const size_t by = bcy ? (size_t)2 * mz * nm * sizeof(double) : 0, bz = bcz ? (size_t)2 * my * nm * sizeof(double) : 0;
+    int rc = ensure(ctx, ctx->io, 2 * bytes + by + bz);
+    if (rc) return rc;
+    double *drhs = ctx->io.buf, *dsol = drhs + bytes / sizeof(double);
+    double *dby = dsol + bytes / sizeof(double), *dbz = dby + by / sizeof(double);
+    DUCT_CUDA(ctx, cudaMemcpyAsync(drhs, rhs, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    if (bcy) DUCT_CUDA(ctx, cudaMemcpyAsync(dby, bcy, by, cudaMemcpyHostToDevice, ctx->stream));
+    if (bcz) DUCT_CUDA(ctx, cudaMemcpyAsync(dbz, bcz, bz, cudaMemcpyHostToDevice, ctx->stream));
+    ductgpu_rect_field f;
+    f.rhs = drhs;
+    f.sol = dsol;
+    f.xalp = xalp;
+    f.bcy = bcy ? dby : nullptr;
+    f.bcz = bcz ? dbz : nullptr;
+    f.alambda = alambda;
+    f.ib = ib;
+    f.nmodes = nm;
+    f.slot = 0;
+    if ((rc = ductgpu_solve_rect_fields_dev(ctx, &f, 1))) return rc;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(sol, dsol, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d_temp");
 }
 
 int ductgpu_device_alloc(ductgpu_ctx ctx, size_t bytes, void **ptr)

@@ -18,6 +18,7 @@ namespace duct {
 constexpr int kMaxFields = 8;   // fields per batched launch
 constexpr int kMaxN = 191;      // largest interior size (my-2) supported
 constexpr int kNumEvents = 16;
+constexpr int kMaxRect = 8;     // rectangular operator slots (duct shapes)
 
 // Interior operators of one boundary condition ('d' or 'n').
 struct BoundOps {
@@ -37,6 +38,19 @@ struct BoundOps {
     double *Bpack = nullptr;   // D2B in DMMA A-fragment order (residual)
     uint8_t *Pslices = nullptr, *Qslices = nullptr;  // BF16 slices (mixed)
     int *Pexp = nullptr, *Qexp = nullptr;            // per-row exponents
+};
+
+// Operators of one rectangular duct shape (src/pseudomat_temp.f90): y and z
+// directions with their own points, half-widths and wall conditions.
+struct RectSlot {
+    bool ready = false;
+    int my = 0, mz = 0;
+    double sy = 1.0, sz = 1.0;
+    char by1 = 'd', by2 = 'd', bz1 = 'd', bz2 = 'd';
+    BoundOps y, z;
+    double *DY = nullptr, *D2Y = nullptr, *DZ = nullptr, *D2Z = nullptr;  // device
+    double *wy = nullptr, *wz = nullptr;   // Clenshaw-Curtis weights (scaled)
+    int sing_y = -1, sing_z = -1;          // argmin |E| per direction
 };
 
 struct Workspace {
@@ -66,6 +80,7 @@ struct ductgpu_ctx_s {
     int refine_steps = 2;      // FP64 refinement steps of the split-precision path
     duct::BoundOps dir, neu;
 
+    duct::RectSlot rect[duct::kMaxRect];
     duct::Workspace work;      // pass intermediates
     duct::Workspace io;        // device copies for host entries
     int *dev_err = nullptr;    // device error word (bounded waits)
@@ -123,12 +138,21 @@ int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
 struct PassField {
     const double *src;
     double *dst;
-    const double *A;     // packed operator
-    const double *E;     // eigenvalues for the divide
+    const double *A;     // packed operator (n x n, fragment order)
+    const double *E;     // eigenvalues along the pass direction (divide)
+    const double *El;    // eigenvalues along the line direction (divide)
     int nmodes;
     int mode0;
     int plane0;
-    int sing_io;         // 0-based iofzero of a Neumann field, else -1
+    int sing_io;         // 0-based singular index along the pass, else -1
+    int sing_l;          // 0-based singular index along the lines
+    // geometry of this field's planes for this pass
+    int n;               // operator size (interior points along the pass)
+    int nlines;          // interior lines (points along the other direction)
+    int nchunks;         // ceil(nlines / kPassLines)
+    int kpad, mtiles;    // padded K and 16-row tiles of the packed operator
+    int sk, sl;          // complex strides of (k, line)
+    long long plane_stride;  // doubles per complex plane
     // residual epilogue: dst = resF - resT - acc + lam * resU
     const double *resF, *resT, *resU;
 };
@@ -137,15 +161,29 @@ struct PassParams {
     int cta_start[kMaxFields + 1];
     int nf;
     const double *lam;
-    long long plane_stride;  // doubles per complex plane
-    int n, kpad, nchunks;
-    int sk, sl;              // complex strides of (k, line)
     int divide;
     int zero_im_mode0;
     int residual;
 };
 constexpr int kPassLines = 32;
 int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid);
+// Sets the geometry of one field of a pass: operator b along a direction
+// with stride sk (complex elements), nlines lines of stride sl.
+void pass_geometry(PassField &f, const BoundOps &b, const double *El, int nlines, int sk, int sl,
+                   long long plane_stride);
+
+// setup.cu (rectangular)
+int rect_setup(ductgpu_ctx ctx, int slot, int my, int mz, double sy, double sz, char by1, char by2,
+               char bz1, char bz2);
+void free_rect(RectSlot &r);
+
+// solve_rect.cu
+struct RectTask {
+    double *rhs, *sol;
+    const double *bcy, *bcz;   // device wall values (mz,2,nmodes), (my,2,nmodes) or null
+    int nmodes, mode0, plane0, slot;
+};
+int solve_rect(ductgpu_ctx ctx, const RectTask *tasks, int ntasks);
 
 // solve_mixed.cu
 int split_operator(ductgpu_ctx ctx, int n, const double *A, uint8_t **slices, int **rexp);

@@ -18,8 +18,9 @@
 namespace duct {
 
 // src/pseudomat.f90:72-107: nodes x_j = -cos(pi j/(m-1)) and
-// DC(l,j) = dd(l)/dd(j) (-1)^(l+j) / (x_l - x_j), diagonal per CHQZ.
-__global__ void k_build_dc(int m, double *x, double *DC)
+// DC(l,j) = dd(l)/dd(j) (-1)^(l+j) / (x_l - x_j), diagonal per CHQZ; every
+// entry times `scale` (1/half-width, src/pseudomat_temp.f90:77).
+__global__ void k_build_dc(int m, double *x, double *DC, double scale = 1.0)
 {
     const double pi = 3.14159265358979323846;
     const int n = m - 1;
@@ -40,7 +41,30 @@ __global__ void k_build_dc(int m, double *x, double *DC)
             const double sgn = ((l + j) & 1) ? -1.0 : 1.0;
             v = ddl / ddj * sgn / (xl - xj);
         }
-        DC[l + (size_t)m * j] = v;
+        DC[l + (size_t)m * j] = v * scale;
+    }
+}
+
+// Interior block of D2 for a wall-condition pair (b1 at -s, b2 at +s),
+// src/pseudomat_temp.f90:89-137.
+__global__ void k_block_bc(int m, char b1, char b2, const double *D, const double *D2, double *B)
+{
+    const int n = m - 2;
+    const double d11 = D[0], d1m = D[(size_t)m * (m - 1)];
+    const double dm1 = D[m - 1], dmm = D[(m - 1) + (size_t)m * (m - 1)];
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n; idx += gridDim.x * blockDim.x) {
+        const int i = idx % n + 1, j = idx / n + 1;
+        double v = D2[i + (size_t)m * j];
+        if (b1 == 'n' && b2 == 'n') {
+            const double det = d11 * dmm - d1m * dm1;
+            v = D2[i] * (d1m * D[(m - 1) + (size_t)m * j] - dmm * D[(size_t)m * j]) / det + v +
+                D2[i + (size_t)m * (m - 1)] * (dm1 * D[(size_t)m * j] - d11 * D[(m - 1) + (size_t)m * j]) / det;
+        } else if (b1 == 'd' && b2 == 'n') {
+            v = v - D2[i + (size_t)m * (m - 1)] * D[(m - 1) + (size_t)m * j] / dmm;
+        } else if (b1 == 'n' && b2 == 'd') {
+            v = v - D2[i] * D[(size_t)m * j] / d11;
+        }
+        B[(i - 1) + (size_t)n * (j - 1)] = v;
     }
 }
 
@@ -287,6 +311,93 @@ out:
     free(hbuf);
     cusolverDnDestroyParams(params);
     return rc;
+}
+
+void free_rect(RectSlot &r)
+{
+    free_bound(r.y);
+    free_bound(r.z);
+    cudaFree(r.DY); cudaFree(r.D2Y); cudaFree(r.DZ); cudaFree(r.D2Z); cudaFree(r.wy); cudaFree(r.wz);
+    r = RectSlot();
+}
+
+static void cc_weights(int m, double scale, std::vector<double> &w)
+{
+    w.assign(m, 0.0);
+    const int N = m - 1;
+    const double pi = 3.14159265358979323846;
+    for (int j = 0; j <= N; ++j) {
+        double s = 0.0;
+        for (int k = 1; k <= N / 2; ++k) {
+            const double bk = (2 * k == N) ? 1.0 : 2.0;
+            s += bk * cos(2.0 * pi * (double)k * (double)j / (double)N) / (4.0 * k * k - 1.0);
+        }
+        const double cj = (j == 0 || j == N) ? 1.0 : 2.0;
+        w[j] = scale * cj / (double)N * (1.0 - s);
+    }
+}
+
+// One direction of pseudomaty_temp / pseudomatz_temp on the GPU.
+static int rect_direction(ductgpu_ctx ctx, int m, double s, char b1, char b2, BoundOps &b, double **D,
+                          double **D2, double **w)
+{
+    const int n = m - 2;
+    double *x = nullptr, *blk = nullptr;
+    DUCT_CUDA(ctx, cudaMalloc(D, (size_t)m * m * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(D2, (size_t)m * m * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&x, m * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&blk, (size_t)n * n * sizeof(double)));
+    b.n = n;
+    DUCT_CUDA(ctx, cudaMalloc(&b.D2B, (size_t)n * n * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&b.E, n * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&b.P, (size_t)n * n * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&b.PM1, (size_t)n * n * sizeof(double)));
+    k_build_dc<<<blocks_for((long)m * m), 256, 0, ctx->stream>>>(m, x, *D, 1.0 / s);
+    k_matmul<<<blocks_for((long)m * m), 256, 0, ctx->stream>>>(m, *D, *D, *D2);
+    k_block_bc<<<blocks_for((long)n * n), 256, 0, ctx->stream>>>(m, b1, b2, *D, *D2, blk);
+    ctx->launches += 3;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.D2B, blk, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    int rc = eigen_gpu(ctx, n, blk, b);
+    cudaFree(blk);
+    cudaFree(x);
+    if (rc) return rc;
+    b.iofzero = 0;
+    if ((rc = pack_operators(ctx, b))) return rc;
+    std::vector<double> wh;
+    cc_weights(m, s, wh);
+    DUCT_CUDA(ctx, cudaMalloc(w, m * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(*w, wh.data(), m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    return DUCTGPU_OK;
+}
+
+int rect_setup(ductgpu_ctx ctx, int slot, int my, int mz, double sy, double sz, char by1, char by2,
+               char bz1, char bz2)
+{
+    if (slot < 0 || slot >= kMaxRect) return set_error(ctx, DUCTGPU_EARG, "rectangular slot %d (0..%d)", slot, kMaxRect - 1);
+    if (my < 5 || mz < 5 || my - 2 > kMaxN || mz - 2 > kMaxN)
+        return set_error(ctx, DUCTGPU_EARG, "pseudomat_temp: my=%d mz=%d outside [5,%d]", my, mz, kMaxN + 2);
+    for (char c : {by1, by2, bz1, bz2})
+        if (c != 'd' && c != 'n') return set_error(ctx, DUCTGPU_EARG, "wall condition '%c' is neither 'd' nor 'n'", c);
+    if (!(sy > 0.0) || !(sz > 0.0)) return set_error(ctx, DUCTGPU_EARG, "half-widths must be positive");
+    RectSlot &r = ctx->rect[slot];
+    cudaStreamSynchronize(ctx->stream);
+    free_rect(r);
+    r.my = my; r.mz = mz; r.sy = sy; r.sz = sz;
+    r.by1 = by1; r.by2 = by2; r.bz1 = bz1; r.bz2 = bz2;
+    int rc = rect_direction(ctx, my, sy, by1, by2, r.y, &r.DY, &r.D2Y, &r.wy);
+    if (!rc) rc = rect_direction(ctx, mz, sz, bz1, bz2, r.z, &r.DZ, &r.D2Z, &r.wz);
+    if (rc) { free_rect(r); return rc; }
+    // singular pair of the all-Neumann operator: smallest |E| per direction
+    std::vector<double> ey(r.y.n), ez(r.z.n);
+    DUCT_CUDA(ctx, cudaMemcpyAsync(ey.data(), r.y.E, r.y.n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(ez.data(), r.z.E, r.z.n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    r.sing_y = 0;
+    for (int i = 1; i < r.y.n; ++i) if (fabs(ey[i]) < fabs(ey[r.sing_y])) r.sing_y = i;
+    r.sing_z = 0;
+    for (int i = 1; i < r.z.n; ++i) if (fabs(ez[i]) < fabs(ez[r.sing_z])) r.sing_z = i;
+    r.ready = true;
+    return DUCTGPU_OK;
 }
 
 int pseudomat_gpu(ductgpu_ctx ctx, int m)

@@ -52,48 +52,51 @@ __device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[8], con
           "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
+// MTW: 16-row tiles per warp along M of the launch (fields with smaller
+// operators skip the tiles they do not have).
 template <int MTW>
 __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ PassParams p)
 {
     extern __shared__ __align__(16) double smem[];
-    constexpr int mtiles = 4 * MTW;
-    constexpr int a_chunk = (kKC / 16) * mtiles * 256;
+    constexpr int a_chunk_max = (kKC / 16) * (4 * MTW) * 256;
     double *As = smem;
-    double *Bs = smem + 2 * a_chunk;
+    double *Bs = smem + 2 * a_chunk_max;
 
     int fi = 0;
     while (fi + 1 < p.nf && (int)blockIdx.x >= p.cta_start[fi + 1]) ++fi;
     const PassField &F = p.f[fi];
     const int local = blockIdx.x - p.cta_start[fi];
-    const int plane = local / p.nchunks;
-    const int chunk = local - plane * p.nchunks;
+    const int plane = local / F.nchunks;
+    const int chunk = local - plane * F.nchunks;
     const int l0 = chunk * kLines;
-    const int L = min(kLines, p.n - l0);
-    const double *src = F.src + (long long)plane * p.plane_stride;
-    double *dst = F.dst + (long long)plane * p.plane_stride;
+    const int L = min(kLines, F.nlines - l0);
+    const double *src = F.src + (long long)plane * F.plane_stride;
+    double *dst = F.dst + (long long)plane * F.plane_stride;
     const int tid = threadIdx.x;
-    const int nkc = p.kpad / kKC;
+    const int kpad = F.kpad, mtiles = F.mtiles;
+    const int nkc = kpad / kKC;
+    const int a_chunk = (kKC / 16) * mtiles * 256;
 
     auto load_a = [&](int c, int buf) {
         const double *g = F.A + (size_t)c * a_chunk;
-        double *s = As + buf * a_chunk;
+        double *s = As + buf * a_chunk_max;
         for (int i = tid * 2; i < a_chunk; i += kThreads * 2) cp_async16(s + i, g + i);
         cp_async_commit();
     };
     load_a(0, 0);
 
     // Stage the lines: Bs[k][2l + c] = in(k, l0 + l) component c, zero padded.
-    const int n = p.n, sk = p.sk, sl = p.sl;
+    const int n = F.n, sk = F.sk, sl = F.sl;
     if (sk == 1) {
-        for (int idx = tid; idx < p.kpad * kLines; idx += kThreads) {
-            const int k = idx % p.kpad, l = idx / p.kpad;
+        for (int idx = tid; idx < kpad * kLines; idx += kThreads) {
+            const int k = idx % kpad, l = idx / kpad;
             double2 v = make_double2(0.0, 0.0);
             if (k < n && l < L)
                 v = *reinterpret_cast<const double2 *>(src + 2 * ((long long)(k + 1) * sk + (long long)(l0 + l + 1) * sl));
             *reinterpret_cast<double2 *>(Bs + k * kNld + 2 * l) = v;
         }
     } else {
-        for (int idx = tid; idx < p.kpad * kLines; idx += kThreads) {
+        for (int idx = tid; idx < kpad * kLines; idx += kThreads) {
             const int l = idx % kLines, k = idx / kLines;
             double2 v = make_double2(0.0, 0.0);
             if (k < n && l < L)
@@ -121,21 +124,9 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
             cp_async_wait<0>();
         }
         __syncthreads();
-        const double *Ab = As + (c & 1) * a_chunk;
+        const double *Ab = As + (c & 1) * a_chunk_max;
 #pragma unroll
         for (int ks = 0; ks < kKC / 16; ++ks) {
-            double a[MTW][8];
-#pragma unroll
-            for (int mt = 0; mt < MTW; ++mt) {
-                const double2 *q = reinterpret_cast<const double2 *>(
-                    Ab + ((ks * mtiles + wm * MTW + mt) * 32 + lane) * 8);
-#pragma unroll
-                for (int h = 0; h < 4; ++h) {
-                    const double2 v = q[h];
-                    a[mt][2 * h] = v.x;
-                    a[mt][2 * h + 1] = v.y;
-                }
-            }
             const int kg = c * kKC + ks * 16 + t;
             double b[4][4];
 #pragma unroll
@@ -145,9 +136,20 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
                 for (int v = 0; v < 4; ++v) b[nt][v] = Bs[(kg + 4 * v) * kNld + col];
             }
 #pragma unroll
-            for (int mt = 0; mt < MTW; ++mt)
+            for (int mt = 0; mt < MTW; ++mt) {
+                const int mtg = wm * MTW + mt;
+                if (mtg >= mtiles) continue;
+                double a[8];
+                const double2 *q = reinterpret_cast<const double2 *>(Ab + ((ks * mtiles + mtg) * 32 + lane) * 8);
 #pragma unroll
-                for (int nt = 0; nt < 4; ++nt) dmma16(acc[mt][nt], a[mt], b[nt]);
+                for (int h = 0; h < 4; ++h) {
+                    const double2 v = q[h];
+                    a[2 * h] = v.x;
+                    a[2 * h + 1] = v.y;
+                }
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) dmma16(acc[mt][nt], a, b[nt]);
+            }
         }
         __syncthreads();
     }
@@ -170,18 +172,18 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
                 if (o >= n) continue;
                 double re = acc[mt][nt][2 * h], im = acc[mt][nt][2 * h + 1];
                 if (p.divide) {
-                    if (singular && o == F.sing_io && lg == F.sing_io) {
+                    if (singular && o == F.sing_io && lg == F.sing_l) {
                         re = 0.0;
                         im = 0.0;
                     } else {
-                        const double den = (F.E[o] + F.E[lg]) - lam;
+                        const double den = (F.E[o] + F.El[lg]) - lam;
                         re = re / den;
                         im = im / den;
                     }
                 }
                 const long long off = 2 * ((long long)(o + 1) * sk + (long long)(lg + 1) * sl);
                 if (p.residual) {
-                    const long long po = (long long)plane * p.plane_stride + off;
+                    const long long po = (long long)plane * F.plane_stride + off;
                     const double2 f = *reinterpret_cast<const double2 *>(F.resF + po);
                     const double2 tt = *reinterpret_cast<const double2 *>(F.resT + po);
                     const double2 uu = *reinterpret_cast<const double2 *>(F.resU + po);
@@ -201,14 +203,29 @@ static size_t pass_smem_bytes(int mtw, int kpad)
 }
 
 template <int MTW>
-static cudaError_t launch_pass(ductgpu_ctx ctx, const PassParams &pp, int grid)
+static cudaError_t launch_pass(ductgpu_ctx ctx, const PassParams &pp, int grid, int kpad_max)
 {
-    const size_t smem = pass_smem_bytes(MTW, pp.kpad);
+    const size_t smem = pass_smem_bytes(MTW, kpad_max);
     cudaError_t e = cudaFuncSetAttribute(k_pass_fp64<MTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     LaunchScope ls(ctx, DUCTGPU_K_PASS_FP64);
     k_pass_fp64<MTW><<<grid, kThreads, smem, ctx->stream>>>(pp);
     return cudaGetLastError();
+}
+
+void pass_geometry(PassField &f, const BoundOps &b, const double *El, int nlines, int sk, int sl,
+                   long long plane_stride)
+{
+    f.n = b.n;
+    f.kpad = b.kpad;
+    f.mtiles = b.mtiles;
+    f.E = b.E;
+    f.El = El;
+    f.nlines = nlines;
+    f.nchunks = (nlines + kLines - 1) / kLines;
+    f.sk = sk;
+    f.sl = sl;
+    f.plane_stride = plane_stride;
 }
 
 // ---------------------------------------------------------------------------
@@ -430,14 +447,33 @@ static int plane_count(const FieldTask *t, int nt)
 
 int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid)
 {
-    const int mtw = (pp.n + 63) / 64;
+    int mt_max = 4, kpad_max = 32;
+    for (int i = 0; i < pp.nf; ++i) {
+        mt_max = pp.f[i].mtiles > mt_max ? pp.f[i].mtiles : mt_max;
+        kpad_max = pp.f[i].kpad > kpad_max ? pp.f[i].kpad : kpad_max;
+    }
+    const int mtw = mt_max / 4;
     cudaError_t e;
     switch (mtw) {
-    case 1: e = launch_pass<1>(ctx, pp, grid); break;
-    case 2: e = launch_pass<2>(ctx, pp, grid); break;
-    default: e = launch_pass<3>(ctx, pp, grid); break;
+    case 1: e = launch_pass<1>(ctx, pp, grid, kpad_max); break;
+    case 2: e = launch_pass<2>(ctx, pp, grid, kpad_max); break;
+    case 3: e = launch_pass<3>(ctx, pp, grid, kpad_max); break;
+    default: return set_error(ctx, DUCTGPU_EARG, "operator larger than %d", kMaxN);
     }
     return e == cudaSuccess ? DUCTGPU_OK : check_cuda(ctx, e, "k_pass_fp64");
+}
+
+// Grid of a pass: CTA ranges per field (planes x line chunks).
+static int pass_grid(PassParams &pp, const FieldTask *tasks, int ntasks)
+{
+    int cta = 0;
+    for (int i = 0; i < ntasks; ++i) {
+        pp.cta_start[i] = cta;
+        cta += tasks[i].nmodes * pp.f[i].nchunks;
+    }
+    pp.cta_start[ntasks] = cta;
+    pp.nf = ntasks;
+    return cta;
 }
 
 int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
@@ -452,31 +488,20 @@ int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
     double *w1 = ctx->work.buf;
     double *w2 = w1 + (size_t)planes * ps;
 
-    const int mtw = (n + 63) / 64;
-    const BoundOps &ref = ctx->dir;
     PassParams pp{};
-    pp.nf = ntasks;
     pp.lam = ctx->lam;
-    pp.plane_stride = ps;
-    pp.n = n;
-    pp.kpad = ref.kpad;
-    pp.nchunks = (n + kLines - 1) / kLines;
-    int cta = 0;
-    long long off = 0;
     for (int i = 0; i < ntasks; ++i) {
-        pp.cta_start[i] = cta;
-        cta += tasks[i].nmodes * pp.nchunks;
         pp.f[i].nmodes = tasks[i].nmodes;
         pp.f[i].mode0 = tasks[i].mode0;
         pp.f[i].plane0 = tasks[i].plane0;
         pp.f[i].sing_io = (tasks[i].bound == 'n') ? ctx->neu.iofzero - 1 : -1;
+        pp.f[i].sing_l = pp.f[i].sing_io;
     }
-    pp.cta_start[ntasks] = cta;
-
     // pass 1 (y, P^-1): rhs -> w1 ; pass 2 (z, P^-1, divide): w1 -> w2 ;
     // pass 3 (z, P): w2 -> w1 ; pass 4 (y, P): w1 -> sol
     for (int pass = 0; pass < 4; ++pass) {
-        off = 0;
+        long long off = 0;
+        const bool ypass = (pass == 0 || pass == 3);
         for (int i = 0; i < ntasks; ++i) {
             const BoundOps &b = (tasks[i].bound == 'n') ? ctx->neu : ctx->dir;
             double *a1 = w1 + off * ps, *a2 = w2 + off * ps;
@@ -487,20 +512,13 @@ int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
             case 2: pp.f[i].src = a2; pp.f[i].dst = a1; pp.f[i].A = b.Ppack; break;
             default: pp.f[i].src = a1; pp.f[i].dst = tasks[i].sol; pp.f[i].A = b.Ppack; break;
             }
-            pp.f[i].E = b.E;
+            pass_geometry(pp.f[i], b, b.E, n, ypass ? 1 : m, ypass ? m : 1, ps);
         }
-        const bool ypass = (pass == 0 || pass == 3);
-        pp.sk = ypass ? 1 : m;
-        pp.sl = ypass ? m : 1;
+        const int cta = pass_grid(pp, tasks, ntasks);
         pp.divide = (pass == 1);
         pp.zero_im_mode0 = (pass == 3);
-        cudaError_t e;
-        switch (mtw) {
-        case 1: e = launch_pass<1>(ctx, pp, cta); break;
-        case 2: e = launch_pass<2>(ctx, pp, cta); break;
-        default: e = launch_pass<3>(ctx, pp, cta); break;
-        }
-        if (e != cudaSuccess) return check_cuda(ctx, e, "k_pass_fp64");
+        pp.residual = 0;
+        if ((rc = fp64_pass(ctx, pp, cta))) return rc;
     }
     if ((rc = zero_walls(ctx, tasks, ntasks))) return rc;
     return neumann_fill(ctx, tasks, ntasks);

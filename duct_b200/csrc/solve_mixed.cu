@@ -561,22 +561,19 @@ int solve_mixed(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
         PassParams pp{};
         pp.nf = ns;
         pp.lam = ctx->lam;
-        pp.plane_stride = ps;
-        pp.n = n;
-        pp.kpad = ctx->dir.kpad;
-        pp.nchunks = (n + kPassLines - 1) / kPassLines;
         int cta = 0;
         for (int i = 0; i < ns; ++i) {
             const long long off = suboff[i];
             const BoundOps &b = (sub[i].bound == 'n') ? ctx->neu : ctx->dir;
-            pp.cta_start[i] = cta;
-            cta += sub[i].nmodes * pp.nchunks;
             pp.f[i].nmodes = sub[i].nmodes;
             pp.f[i].mode0 = sub[i].mode0;
             pp.f[i].plane0 = sub[i].plane0;
             pp.f[i].sing_io = -1;
+            pp.f[i].sing_l = -1;
             pp.f[i].A = b.Bpack;
-            pp.f[i].E = b.E;
+            pass_geometry(pp.f[i], b, b.E, n, 1, m, ps);
+            pp.cta_start[i] = cta;
+            cta += sub[i].nmodes * pp.f[i].nchunks;
             pp.f[i].src = sub[i].sol;
             pp.f[i].dst = w1 + off * ps;
             pp.f[i].resF = sub[i].rhs;
@@ -584,10 +581,14 @@ int solve_mixed(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
             pp.f[i].resU = sub[i].sol;
         }
         pp.cta_start[ns] = cta;
-        pp.sk = 1; pp.sl = m; pp.divide = 0; pp.zero_im_mode0 = 0; pp.residual = 0;
+        pp.divide = 0; pp.zero_im_mode0 = 0; pp.residual = 0;
         if ((rc = fp64_pass(ctx, pp, cta))) return rc;
-        for (int i = 0; i < ns; ++i) pp.f[i].dst = w3 + suboff[i] * ps;
-        pp.sk = m; pp.sl = 1; pp.residual = 1;
+        for (int i = 0; i < ns; ++i) {
+            pp.f[i].dst = w3 + suboff[i] * ps;
+            pp.f[i].sk = m;
+            pp.f[i].sl = 1;
+        }
+        pp.residual = 1;
         if ((rc = fp64_pass(ctx, pp, cta))) return rc;
         // drop the singular component of Neumann kx=0 residuals
         ProjParams pj{};

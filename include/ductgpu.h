@@ -118,6 +118,45 @@ typedef struct {
 int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields,
                              int nfields, int precision);
 
+/* ---- rectangular ducts, general wall conditions (temperature path) ---- */
+/* pseudomaty_temp + pseudomatz_temp (src/pseudomat_temp.f90:2-320) on the
+ * GPU for operator slot `slot` (0..7, one per duct shape): my x mz points on
+ * [-sy,sy] x [-sz,sz]; wall conditions by1 (y=-sy), by2 (y=+sy), bz1, bz2,
+ * each 'd' (Dirichlet) or 'n' (Neumann).                                   */
+int ductgpu_pseudomat_temp(ductgpu_ctx ctx, int slot, int my, int mz, double sy, double sz,
+                           char by1, char by2, char bz1, char bz2);
+
+/* helm3d_temp(rhs,sol,work,ipro,cvar,a,b,alambda,bcco),
+ * src/helm3d_temp.f90:2-46, on host arrays with operator slot 0: solves
+ * lap(u) - (alambda + xalp^2) u = f with wall values bcy(mz,2,nmodes) (at
+ * y = -a, +a) and bcz(my,2,nmodes) (z = -b, +b), real, the same for the
+ * real and the imaginary part as in src/int2d3d_temp.f90:71-83 (NULL: zero
+ * walls).  ipro <= 0 runs the setup first (ipro == -1: setup only).  The
+ * singular all-Neumann mode at lambda = 0, which the reference divides by
+ * zero, gets the zero-eigen-coefficient gauge (GAUGE_MEAN: zero mean).     */
+int ductgpu_helm3d_temp(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, double a,
+                        double b, double alambda, int my, int mz, int ib, int ie,
+                        const double *xalp, const double *bcy, const double *bcz,
+                        char by1, char by2, char bz1, char bz2);
+
+/* One field of a batched rectangular solve (device arrays). */
+typedef struct {
+    double *rhs;         /* device, complex (my,mz,nmodes) of the slot      */
+    double *sol;         /* device, complex (my,mz,nmodes)                  */
+    const double *xalp;  /* HOST, nmodes wavenumbers                        */
+    const double *bcy;   /* device (mz,2,nmodes) wall values, or NULL       */
+    const double *bcz;   /* device (my,2,nmodes) wall values, or NULL       */
+    double alambda;
+    int ib;
+    int nmodes;
+    int slot;            /* operator slot (duct shape)                      */
+} ductgpu_rect_field;
+
+/* Fields of several duct shapes (slots) solved together: each of the four
+ * GEMM passes is one launch over all fields, modes and shapes.           */
+int ductgpu_solve_rect_fields_dev(ductgpu_ctx ctx, const ductgpu_rect_field *fields,
+                                  int nfields);
+
 /* ---- Chebyshev transforms, derivatives, pencil transposes ------------ */
 /* transyz(cheb,cdir,iopt), src/chebyshev.f90:458-540 with tcheb_fftw,
  * src/tchebw.f:62-192: DCT-I of every line of a complex (my,mz,nmodes)

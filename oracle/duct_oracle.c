@@ -586,3 +586,225 @@ void orc_cyzx2xyz(double *phys, const double *phys2, int nmodes, int my, int nz)
                 phys[2 * d + 1] = phys2[2 * s + 1];
             }
 }
+
+
+/* ---- rectangular / general-BC solver --------------------------------- */
+
+/* pseudomaty_temp / pseudomatz_temp, src/pseudomat_temp.f90:2-320.        */
+int orc_pseudomat_temp(int m, double sc, char b1, char b2, orc_dir *d)
+{
+    if (m < 4) return -1;
+    memset(d, 0, sizeof(*d));
+    const int n = m - 1, mm2 = m - 2;
+    const double pi = 4.0 * atan(1.0);
+    d->m = m; d->s = sc; d->b1 = b1; d->b2 = b2;
+    d->D = (double *)calloc((size_t)m * m, sizeof(double));
+    d->D2 = (double *)calloc((size_t)m * m, sizeof(double));
+    d->E = (double *)calloc((size_t)mm2, sizeof(double));
+    d->P = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    d->PM1 = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    d->B = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    double *y = (double *)calloc((size_t)m, sizeof(double));
+    double *dd = (double *)calloc((size_t)m, sizeof(double));
+    double *eii = (double *)calloc((size_t)mm2, sizeof(double));
+    double *Bt = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    double *D = d->D, *D2 = d->D2;
+    dd[0] = 2.0;
+    for (int i = 1; i < m - 1; ++i) dd[i] = 1.0;
+    dd[m - 1] = 2.0;
+    for (int j = 0; j < m; ++j) y[j] = -cos(pi * (double)j / (double)n);
+    D[IX(0, 0, m)] = -(2.0 * (double)n * (double)n + 1.0) / 6.0;
+    D[IX(m - 1, m - 1, m)] = -D[IX(0, 0, m)];
+    for (int i = 1; i < n; ++i) D[IX(i, i, m)] = -0.5 * y[i] / (1.0 - y[i] * y[i]);
+    for (int l = 0; l < m; ++l)
+        for (int j = 0; j < m; ++j) {
+            if (j == l) continue;
+            const double sgn = ((l + j) % 2 == 0) ? 1.0 : -1.0;
+            D[IX(l, j, m)] = dd[l] / dd[j] * sgn / (y[l] - y[j]);
+        }
+    for (size_t i = 0; i < (size_t)m * m; ++i) D[i] *= 1.0 / sc;   /* dscal(1/s) :77 */
+    {
+        const double one = 1.0, zero = 0.0;
+        scipy_dgemm_("n", "n", &m, &m, &m, &one, D, &m, D, &m, &zero, D2, &m, 1, 1);
+    }
+    const double d11 = D[IX(0, 0, m)], d1m = D[IX(0, m - 1, m)];
+    const double dm1 = D[IX(m - 1, 0, m)], dmm = D[IX(m - 1, m - 1, m)];
+    for (int i = 1; i < n; ++i)
+        for (int j = 1; j < n; ++j) {
+            double v;
+            if (b1 == 'n' && b2 == 'n') {
+                const double Det = d11 * dmm - d1m * dm1;
+                const double ter1 = D2[IX(i, 0, m)] * (d1m * D[IX(m - 1, j, m)] - dmm * D[IX(0, j, m)]) / Det;
+                const double ter3 = D2[IX(i, m - 1, m)] * (dm1 * D[IX(0, j, m)] - d11 * D[IX(m - 1, j, m)]) / Det;
+                v = ter1 + D2[IX(i, j, m)] + ter3;
+            } else if (b1 == 'd' && b2 == 'n') {
+                v = D2[IX(i, j, m)] - D2[IX(i, m - 1, m)] * D[IX(m - 1, j, m)] / dmm;
+            } else if (b1 == 'n' && b2 == 'd') {
+                v = D2[IX(i, j, m)] - D2[IX(i, 0, m)] * D[IX(0, j, m)] / d11;
+            } else {
+                v = D2[IX(i, j, m)];
+            }
+            d->B[IX(i - 1, j - 1, mm2)] = v;
+        }
+    memcpy(Bt, d->B, sizeof(double) * (size_t)mm2 * mm2);
+    int info = eigen(mm2, Bt, d->E, eii, d->P);
+    if (!info) {
+        memcpy(d->PM1, d->P, sizeof(double) * (size_t)mm2 * mm2);
+        info = invert(mm2, d->PM1);
+    }
+    free(y); free(dd); free(eii); free(Bt);
+    return info;
+}
+
+void orc_dir_free(orc_dir *d)
+{
+    free(d->D); free(d->D2); free(d->E); free(d->P); free(d->PM1); free(d->B);
+    memset(d, 0, sizeof(*d));
+}
+
+static int argmin_abs(const double *E, int n)
+{
+    int k = 0;
+    for (int i = 1; i < n; ++i)
+        if (fabs(E[i]) < fabs(E[k])) k = i;
+    return k;
+}
+
+/* solvediag_temp + mod_term_FTy/z + edge_value_y/z.                        */
+int orc_solvediag_temp(double *U, const orc_dir *yd, const orc_dir *zd, double xlambda,
+                       const double *bcy, const double *bcz, int sing)
+{
+    const int my = yd->m, mz = zd->m, ny = my - 2, nz = mz - 2;
+    double *F = (double *)calloc((size_t)ny * nz, sizeof(double));
+    double *FT = (double *)calloc((size_t)ny * nz, sizeof(double));
+    const double *DY = yd->D, *DZ = zd->D, *D2Y = yd->D2, *D2Z = zd->D2;
+    for (int j = 1; j < mz - 1; ++j)
+        for (int i = 1; i < my - 1; ++i) F[IX(i - 1, j - 1, ny)] = U[IX(i, j, my)];
+    /* mod_term_FTy / mod_term_FTz (src/solvediag_temp.f90:86-239) */
+    for (int j = 1; j < mz - 1; ++j)
+        for (int i = 1; i < my - 1; ++i) {
+            double v = 0.0, h = 0.0;
+            if (bcy) {
+                const double c1 = bcy[j], c2 = bcy[j + mz];
+                const double a1 = D2Y[IX(i, 0, my)], a2 = D2Y[IX(i, my - 1, my)];
+                if (yd->b1 == 'd' && yd->b2 == 'd') v = -a1 * c1 - a2 * c2;
+                else if (yd->b1 == 'd' && yd->b2 == 'n')
+                    v = -a1 * c1 - a2 * (c2 - DY[IX(my - 1, 0, my)] * c1) / DY[IX(my - 1, my - 1, my)];
+                else if (yd->b1 == 'n' && yd->b2 == 'd')
+                    v = -a1 * (c1 - DY[IX(0, my - 1, my)] * c2) / DY[IX(0, 0, my)] - a2 * c2;
+                else {
+                    const double Det = DY[IX(0, 0, my)] * DY[IX(my - 1, my - 1, my)] - DY[IX(0, my - 1, my)] * DY[IX(my - 1, 0, my)];
+                    v = a1 * (DY[IX(0, my - 1, my)] * c2 - DY[IX(my - 1, my - 1, my)] * c1) / Det +
+                        a2 * (DY[IX(my - 1, 0, my)] * c1 - DY[IX(0, 0, my)] * c2) / Det;
+                }
+            }
+            if (bcz) {
+                const double c1 = bcz[i], c2 = bcz[i + my];
+                const double a1 = D2Z[IX(j, 0, mz)], a2 = D2Z[IX(j, mz - 1, mz)];
+                if (zd->b1 == 'd' && zd->b2 == 'd') h = -a1 * c1 - a2 * c2;
+                else if (zd->b1 == 'd' && zd->b2 == 'n')
+                    h = -a1 * c1 - a2 * (c2 - DZ[IX(mz - 1, 0, mz)] * c1) / DZ[IX(mz - 1, mz - 1, mz)];
+                else if (zd->b1 == 'n' && zd->b2 == 'd')
+                    h = -a1 * (c1 - DZ[IX(0, mz - 1, mz)] * c2) / DZ[IX(0, 0, mz)] - a2 * c2;
+                else {
+                    const double Det = DZ[IX(0, 0, mz)] * DZ[IX(mz - 1, mz - 1, mz)] - DZ[IX(0, mz - 1, mz)] * DZ[IX(mz - 1, 0, mz)];
+                    h = a1 * (DZ[IX(0, mz - 1, mz)] * c2 - DZ[IX(mz - 1, mz - 1, mz)] * c1) / Det +
+                        a2 * (DZ[IX(mz - 1, 0, mz)] * c1 - DZ[IX(0, 0, mz)] * c2) / Det;
+                }
+            }
+            F[IX(i - 1, j - 1, ny)] += v + h;
+        }
+    /* F = PTYM1 F PTZM1^T ; divide ; FT = PTY F PTZ^T  (:47-64) */
+    {
+        const double one = 1.0, zero = 0.0;
+        scipy_dgemm_("n", "n", &ny, &nz, &ny, &one, yd->PM1, &ny, F, &ny, &zero, FT, &ny, 1, 1);
+        scipy_dgemm_("n", "t", &ny, &nz, &nz, &one, FT, &ny, zd->PM1, &nz, &zero, F, &ny, 1, 1);
+        const int iy0 = argmin_abs(yd->E, ny), iz0 = argmin_abs(zd->E, nz);
+        for (int j = 0; j < nz; ++j)
+            for (int i = 0; i < ny; ++i) {
+                if (sing && i == iy0 && j == iz0) { FT[IX(i, j, ny)] = 0.0; continue; }
+                FT[IX(i, j, ny)] = F[IX(i, j, ny)] / (yd->E[i] + zd->E[j] - xlambda);
+            }
+        scipy_dgemm_("n", "n", &ny, &nz, &ny, &one, yd->P, &ny, FT, &ny, &zero, F, &ny, 1, 1);
+        scipy_dgemm_("n", "t", &ny, &nz, &nz, &one, F, &ny, zd->P, &nz, &zero, FT, &ny, 1, 1);
+    }
+    for (int j = 0; j < nz; ++j)
+        for (int i = 0; i < ny; ++i) U[IX(i + 1, j + 1, my)] = FT[IX(i, j, ny)];
+    /* edge_value_y (:241-300): walls y = -1, +1 for interior columns j */
+    for (int j = 1; j < mz - 1; ++j) {
+        const double c1 = bcy ? bcy[j] : 0.0, c2 = bcy ? bcy[j + mz] : 0.0;
+        double a = 0.0, b = 0.0;
+        for (int i = 1; i < my - 1; ++i) {
+            a += DY[IX(0, i, my)] * U[IX(i, j, my)];
+            b += DY[IX(my - 1, i, my)] * U[IX(i, j, my)];
+        }
+        if (yd->b1 == 'd' && yd->b2 == 'd') { U[IX(0, j, my)] = c1; U[IX(my - 1, j, my)] = c2; }
+        else if (yd->b1 == 'd' && yd->b2 == 'n') {
+            U[IX(0, j, my)] = c1;
+            U[IX(my - 1, j, my)] = (c2 - DY[IX(my - 1, 0, my)] * U[IX(0, j, my)] - b) / DY[IX(my - 1, my - 1, my)];
+        } else if (yd->b1 == 'n' && yd->b2 == 'd') {
+            U[IX(my - 1, j, my)] = c2;
+            U[IX(0, j, my)] = (c1 - DY[IX(0, my - 1, my)] * U[IX(my - 1, j, my)] - a) / DY[IX(0, 0, my)];
+        } else {
+            const double Det = DY[IX(0, 0, my)] * DY[IX(my - 1, my - 1, my)] - DY[IX(0, my - 1, my)] * DY[IX(my - 1, 0, my)];
+            U[IX(0, j, my)] = (DY[IX(my - 1, my - 1, my)] * (c1 - a) - DY[IX(0, my - 1, my)] * (c2 - b)) / Det;
+            U[IX(my - 1, j, my)] = (-DY[IX(my - 1, 0, my)] * (c1 - a) + DY[IX(0, 0, my)] * (c2 - b)) / Det;
+        }
+    }
+    /* edge_value_z (:302-351) */
+    for (int i = 1; i < my - 1; ++i) {
+        const double c1 = bcz ? bcz[i] : 0.0, c2 = bcz ? bcz[i + my] : 0.0;
+        double a = 0.0, b = 0.0;
+        for (int j = 1; j < mz - 1; ++j) {
+            a += DZ[IX(0, j, mz)] * U[IX(i, j, my)];
+            b += DZ[IX(mz - 1, j, mz)] * U[IX(i, j, my)];
+        }
+        if (zd->b1 == 'd' && zd->b2 == 'd') { U[IX(i, 0, my)] = c1; U[IX(i, mz - 1, my)] = c2; }
+        else if (zd->b1 == 'd' && zd->b2 == 'n') {
+            U[IX(i, 0, my)] = c1;
+            U[IX(i, mz - 1, my)] = (c2 - DZ[IX(mz - 1, 0, mz)] * U[IX(i, 0, my)] - b) / DZ[IX(mz - 1, mz - 1, mz)];
+        } else if (zd->b1 == 'n' && zd->b2 == 'd') {
+            U[IX(i, mz - 1, my)] = c2;
+            U[IX(i, 0, my)] = (c1 - DZ[IX(0, mz - 1, mz)] * U[IX(i, mz - 1, my)] - a) / DZ[IX(0, 0, mz)];
+        } else {
+            const double Det = DZ[IX(0, 0, mz)] * DZ[IX(mz - 1, mz - 1, mz)] - DZ[IX(0, mz - 1, mz)] * DZ[IX(mz - 1, 0, mz)];
+            U[IX(i, 0, my)] = (DZ[IX(mz - 1, mz - 1, mz)] * (c1 - a) - DZ[IX(0, mz - 1, mz)] * (c2 - b)) / Det;
+            U[IX(i, mz - 1, my)] = (-DZ[IX(mz - 1, 0, mz)] * (c1 - a) + DZ[IX(0, 0, mz)] * (c2 - b)) / Det;
+        }
+    }
+    free(F);
+    free(FT);
+    return 0;
+}
+
+int orc_helm3d_temp(const double *rhs, double *sol, int my, int mz, int ib, int ie,
+                    const double *xalp, double alambda, const orc_dir *yd, const orc_dir *zd,
+                    const double *bcy, const double *bcz, int nthreads)
+{
+    const int nmodes = ie - ib + 1;
+    const size_t plane = (size_t)my * mz;
+    if (nthreads < 1) nthreads = 1;
+#pragma omp parallel num_threads(nthreads)
+    {
+        double *U = (double *)malloc(sizeof(double) * plane);
+#pragma omp for schedule(dynamic, 1)
+        for (int i = 0; i < nmodes; ++i) {
+            const int imode = ib + i;
+            const double xl = alambda + xalp[i] * xalp[i];
+            const int sing = (yd->b1 == 'n' && yd->b2 == 'n' && zd->b1 == 'n' && zd->b2 == 'n' && fabs(xl) <= 1.0e-10);
+            const double *r = rhs + 2 * plane * (size_t)i;
+            double *s = sol + 2 * plane * (size_t)i;
+            const double *by = bcy ? bcy + (size_t)2 * mz * i : NULL;
+            const double *bz = bcz ? bcz + (size_t)2 * my * i : NULL;
+            for (size_t p = 0; p < plane; ++p) U[p] = r[2 * p];
+            orc_solvediag_temp(U, yd, zd, xl, by, bz, sing);
+            for (size_t p = 0; p < plane; ++p) { s[2 * p] = U[p]; s[2 * p + 1] = 0.0; }
+            if (imode == 0) continue;
+            for (size_t p = 0; p < plane; ++p) U[p] = r[2 * p + 1];
+            orc_solvediag_temp(U, yd, zd, xl, by, bz, sing);
+            for (size_t p = 0; p < plane; ++p) s[2 * p + 1] += U[p];
+        }
+        free(U);
+    }
+    return 0;
+}

@@ -10,10 +10,12 @@
  * built in this image (no Fortran compiler), so no output of the reference
  * itself is available.  The restatement is pinned by the reference's own
  * known-answer data -- the laminar duct table of get_dpdx
- * (src/operators.F:2496-2507, "-(dyy+dzz)U=dpval -> max(U)=1") and the
- * laminar mass flow CMASSFLOW=1.92783343620839 (utils/gen_tsd2hdf5.py:10) --
- * and by exact manufactured polynomial solutions.  Parity is therefore
- * "partially pinned": known answers, not reference outputs.
+ * (src/operators.F:2496-2507, "-(dyy+dzz)U=dpval -> max(U)=1", aspect
+ * ratios 1..10) -- by the classical series for the laminar duct flow rate
+ * and by exact manufactured polynomial solutions.  (CMASSFLOW in
+ * utils/gen_tsd2hdf5.py:10 is a run's flow rate, not the laminar integral,
+ * which is 1.9081638750 for aspect 1.)  Parity is therefore "partially
+ * pinned": known answers, not reference outputs.
  *
  * Conventions follow the reference: column-major arrays, y fastest, complex
  * fields stored as interleaved (re, im) doubles, 1-based index names in the
@@ -50,7 +52,6 @@ typedef struct {
 /* pseudomat('d',m) followed by pseudomat('n',m).  Returns LAPACK info != 0 or
  * -1 on a bad size.  */
 int  orc_pseudomat(int m, orc_ops *ops);
-/* Same, but the Neumann block/eigen solve is skipped when want_neumann=0.   */
 void orc_ops_free(orc_ops *ops);
 
 /* solvediag(U,F,FT,bound,xlambda), src/solvediag.f90:2-330, CPU branch.
@@ -91,6 +92,41 @@ double orc_cheb2_integral(const double *u, int ny, int nz, double aspect);
  * cyzx2xyz: phys2(my,nz,0:mx1) -> phys(0:mx1,my,nz)                       */
 void orc_cxyz2yzx(const double *phys, double *phys2, int nmodes, int my, int nz);
 void orc_cyzx2xyz(double *phys, const double *phys2, int nmodes, int my, int nz);
+
+/* ---- rectangular / general-BC solver (temperature path) --------------- */
+/* One direction of pseudomaty_temp / pseudomatz_temp
+ * (src/pseudomat_temp.f90:2-150, 152-320): D scaled by 1/s, D2 = D*D, the
+ * interior block for the BC pair (b1 at -s, b2 at +s; 'd' or 'n'), its
+ * eigen-decomposition and inverse.                                         */
+typedef struct {
+    int m;
+    double s;
+    char b1, b2;
+    double *D, *D2;          /* m*m                                          */
+    double *E, *P, *PM1;     /* n, n*n, n*n (n = m-2)                        */
+    double *B;               /* n*n interior block                           */
+} orc_dir;
+
+int  orc_pseudomat_temp(int m, double s, char b1, char b2, orc_dir *d);
+void orc_dir_free(orc_dir *d);
+
+/* solvediag_temp(U,F,FT,...,xlambda,bcy,bcz), src/solvediag_temp.f90:1-84
+ * with mod_term_FTy/z (:86-239) and edge_value_y/z (:241-351).  U is
+ * (my,mz) real; bcy (mz,2), bcz (my,2) wall values (NULL = zero).  The
+ * reference has no rule for the singular n/n mode at lambda = 0 (its guard
+ * abs(den).eq.1e-12 never fires, src/solvediag_temp.f90:52); this
+ * restatement zeroes the eigen-coefficient of the smallest |Ey|+|Ez| pair
+ * there (sing != 0), the gauge the CUDA path uses.                          */
+int orc_solvediag_temp(double *U, const orc_dir *y, const orc_dir *z, double xlambda,
+                       const double *bcy, const double *bcz, int sing);
+
+/* helm3d_temp over modes ib..ie (src/helm3d_temp.f90:2-46,
+ * src/int2d3d_temp.f90:51-88): the same real wall values bcy(:,:,i),
+ * bcz(:,:,i) serve the real and the imaginary solve of mode i; mode 0 is
+ * real.  bcy: (mz,2,nmodes), bcz: (my,2,nmodes), or NULL.                  */
+int orc_helm3d_temp(const double *rhs, double *sol, int my, int mz, int ib, int ie,
+                    const double *xalp, double alambda, const orc_dir *y, const orc_dir *z,
+                    const double *bcy, const double *bcz, int nthreads);
 
 void orc_set_blas_threads(int n);
 

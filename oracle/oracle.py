@@ -21,6 +21,11 @@ class _Ops(C.Structure):
         ("D2Bd", C.POINTER(C.c_double)), ("D2Bn", C.POINTER(C.c_double))]
 
 
+class _Dir(C.Structure):
+    _fields_ = [("m", C.c_int), ("s", C.c_double), ("b1", C.c_char), ("b2", C.c_char)] + [
+        (n, C.POINTER(C.c_double)) for n in ("D", "D2", "E", "P", "PM1", "B")]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -42,11 +47,18 @@ def lib():
         L.orc_cxyz2yzx.argtypes = [P, P, C.c_int, C.c_int, C.c_int]
         L.orc_cyzx2xyz.argtypes = [P, P, C.c_int, C.c_int, C.c_int]
         L.orc_set_blas_threads.argtypes = [C.c_int]
+        L.orc_pseudomat_temp.argtypes = [C.c_int, C.c_double, C.c_char, C.c_char, C.POINTER(_Dir)]
+        L.orc_dir_free.argtypes = [C.POINTER(_Dir)]
+        L.orc_solvediag_temp.argtypes = [P, C.POINTER(_Dir), C.POINTER(_Dir), C.c_double, P, P, C.c_int]
+        L.orc_helm3d_temp.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_double,
+                                      C.POINTER(_Dir), C.POINTER(_Dir), P, P, C.c_int]
         _lib = L
     return _lib
 
 
 def _p(a):
+    if a is None:
+        return None
     assert a.flags.f_contiguous or a.ndim <= 1
     return a.ctypes.data_as(C.c_void_p)
 
@@ -83,6 +95,45 @@ class Ops:
             lib().orc_ops_free(C.byref(self._s))
         except Exception:
             pass
+
+
+class Dir:
+    """One direction of pseudomaty_temp / pseudomatz_temp
+    (src/pseudomat_temp.f90): points m, half-width s, BCs b1 (at -s), b2."""
+
+    def __init__(self, m, s=1.0, b1="d", b2="d"):
+        self._s = _Dir()
+        info = lib().orc_pseudomat_temp(int(m), float(s), b1.encode(), b2.encode(), C.byref(self._s))
+        if info != 0:
+            raise RuntimeError("orc_pseudomat_temp failed, info=%d" % info)
+        self.m, self.s, self.b1, self.b2 = m, s, b1, b2
+        n = m - 2
+
+        def v(ptr, *shape):
+            return np.ctypeslib.as_array(ptr, shape=(int(np.prod(shape)),)).reshape(
+                shape, order="F").copy(order="F")
+        self.D, self.D2 = v(self._s.D, m, m), v(self._s.D2, m, m)
+        self.E, self.P, self.PM1, self.B = v(self._s.E, n), v(self._s.P, n, n), v(self._s.PM1, n, n), v(self._s.B, n, n)
+
+    def __del__(self):
+        try:
+            lib().orc_dir_free(C.byref(self._s))
+        except Exception:
+            pass
+
+
+def helm3d_temp(rhs, ydir, zdir, alambda, xalp, ib=0, bcy=None, bcz=None, nthreads=1):
+    """helm3d_temp on a complex (my,mz,nmodes) field; bcy (mz,2,nmodes),
+    bcz (my,2,nmodes) real wall values or None.  Returns the solution."""
+    rhs = np.asfortranarray(rhs, dtype=np.complex128)
+    my, mz, nm = rhs.shape
+    sol = np.zeros_like(rhs, order="F")
+    xalp = np.ascontiguousarray(xalp, dtype=np.float64)
+    by = None if bcy is None else np.asfortranarray(bcy, dtype=np.float64)
+    bz = None if bcz is None else np.asfortranarray(bcz, dtype=np.float64)
+    lib().orc_helm3d_temp(_p(rhs), _p(sol), my, mz, ib, ib + nm - 1, _p(xalp), float(alambda),
+                          C.byref(ydir._s), C.byref(zdir._s), _p(by), _p(bz), int(nthreads))
+    return sol
 
 
 def solvediag(U, ops, bound, xlambda):
@@ -159,6 +210,6 @@ def set_blas_threads(n):
     lib().orc_set_blas_threads(int(n))
 
 
-__all__ = ["Ops", "solvediag", "helm3d", "transyz", "transyz_plane", "derivyz",
+__all__ = ["Ops", "Dir", "helm3d_temp", "solvediag", "helm3d", "transyz", "transyz_plane", "derivyz",
            "cheb2_integral", "cxyz2yzx", "cyzx2xyz", "set_blas_threads", "lib"]
 _ = os

@@ -141,3 +141,53 @@ def test_helm3d_matches_planewise_solvediag(oracle):
         else:
             im = oracle.solvediag(np.asfortranarray(rhs_after[:, :, k].imag), ops, "d", 10.0 + xalp[k] ** 2)
             assert np.max(np.abs(sol[:, :, k].imag - im)) == 0.0
+
+
+# get_dpdx table for aspect ratios 1..4 (src/operators.F:2498-2501)
+DPVAL = {1.0: 3.39344926982230, 2.0: 2.19545075660646, 3.0: 2.03778220024811, 4.0: 2.00773897291851}
+
+
+@pytest.mark.parametrize("aspect,my,mz", [(2.0, 65, 129), (3.0, 49, 145), (4.0, 33, 129), (1.0, 33, 33)])
+def test_rectangular_dpval_gives_unit_max(oracle, aspect, my, mz):
+    y = oracle.Dir(my, 1.0, "d", "d")
+    z = oracle.Dir(mz, aspect, "d", "d")
+    f = np.full((my, mz, 1), -DPVAL[aspect] + 0j, order="F")
+    f[0, :] = f[-1, :] = f[:, 0] = f[:, -1] = 0.0
+    u = oracle.helm3d_temp(f, y, z, 0.0, [0.0])
+    assert abs(u.real.max() - 1.0) < 1e-12
+
+
+def test_rectangular_reduces_to_square(oracle):
+    m = 17
+    ops = oracle.Ops(m)
+    from duct_b200 import synth
+    f = synth.chebyshev_rhs(m, m, 2, seed=1)
+    f[0, :, :] = f[-1, :, :] = f[:, 0, :] = f[:, -1, :] = 0.0
+    xalp = np.array([0.0, 1.0])
+    sq, _ = oracle.helm3d(f, ops, "d", 2.0, xalp)
+    rc = oracle.helm3d_temp(f, oracle.Dir(m), oracle.Dir(m), 2.0, xalp)
+    assert np.max(np.abs(sq - rc)) < 1e-12 * np.max(np.abs(sq))
+
+
+def test_rectangular_manufactured_mixed_walls(oracle):
+    # u = y^3 + z^2 y on [-1,1]x[-2,2]: Dirichlet at y=-1 / z=+2, Neumann at
+    # y=+1 / z=-2 with the exact wall values and derivatives
+    my, mz, b = 17, 21, 2.0
+    y = oracle.Dir(my, 1.0, "d", "n")
+    z = oracle.Dir(mz, b, "n", "d")
+    yy, zz = np.meshgrid(-np.cos(np.pi * np.arange(my) / (my - 1)),
+                         -b * np.cos(np.pi * np.arange(mz) / (mz - 1)), indexing="ij")
+    u = yy ** 3 + zz ** 2 * yy
+    lam = 0.7
+    f = 6 * yy + 2 * yy - lam * u
+    bcy = np.zeros((mz, 2, 1), order="F")
+    bcy[:, 0, 0] = u[0, :]                              # u(y=-1)
+    bcy[:, 1, 0] = 3 * 1.0 + zz[0, :] ** 2              # du/dy(y=+1)
+    bcz = np.zeros((my, 2, 1), order="F")
+    bcz[:, 0, 0] = 2 * (-b) * yy[:, 0]                  # du/dz(z=-b)
+    bcz[:, 1, 0] = u[:, -1]                             # u(z=+b)
+    F = np.asfortranarray(f[:, :, None] + 0j)
+    sol = oracle.helm3d_temp(F, y, z, lam, [0.0], bcy=bcy, bcz=bcz)
+    assert np.max(np.abs(sol[1:-1, 1:-1, 0].real - u[1:-1, 1:-1])) < 1e-10
+    assert np.max(np.abs(sol[1:-1, 0, 0].real - u[1:-1, 0])) < 1e-10
+    assert np.max(np.abs(sol[-1, 1:-1, 0].real - u[-1, 1:-1])) < 1e-10
