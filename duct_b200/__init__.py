@@ -29,7 +29,8 @@ EXPORTS = [
     "ductgpu_transyz_dev", "ductgpu_transyz", "ductgpu_derivyz_dev", "ductgpu_derivyz",
     "ductgpu_cxyz2yzx_dev", "ductgpu_cyzx2xyz_dev", "ductgpu_chx2z_dev", "ductgpu_chz2x_dev",
     "ductgpu_set_refinement", "ductgpu_pseudomat_temp", "ductgpu_helm3d_temp",
-    "ductgpu_solve_rect_fields_dev",
+    "ductgpu_solve_rect_fields_dev", "ductgpu_graph_create", "ductgpu_graph_launch",
+    "ductgpu_graph_destroy", "transpose_gpu_", "mat_invdiag_gpu_",
 ]
 K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
 
@@ -96,6 +97,13 @@ def lib():
             "ductgpu_helm3d_temp": [P, P, P, I, D, D, D, I, I, I, I, P, P, P, C.c_char, C.c_char,
                                     C.c_char, C.c_char],
             "ductgpu_solve_rect_fields_dev": [P, C.POINTER(RectField), I],
+            "ductgpu_graph_create": [P, I, P, I, I, C.POINTER(I)],
+            "ductgpu_graph_launch": [P, I],
+            "ductgpu_graph_destroy": [P, I],
+            "transpose_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
+                               C.POINTER(C.c_size_t)],
+            "mat_invdiag_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
+                                 C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -259,6 +267,43 @@ class Context:
             arr[i].slot = int(f.get("slot", 0))
         self._check(lib().ductgpu_solve_rect_fields_dev(self.h, arr, len(fields)))
         return keep
+
+    def _field_array(self, fields, rect):
+        keep = []
+        if rect:
+            arr = (RectField * len(fields))()
+        else:
+            arr = (Field * len(fields))()
+        for i, f in enumerate(fields):
+            xalp = np.ascontiguousarray(f["xalp"], dtype=np.float64)
+            keep.append(xalp)
+            arr[i].rhs = f["rhs"].ptr
+            arr[i].sol = f["sol"].ptr
+            arr[i].xalp = xalp.ctypes.data
+            arr[i].alambda = float(f["alambda"])
+            arr[i].ib = int(f.get("ib", 0))
+            arr[i].nmodes = int(xalp.shape[0])
+            if rect:
+                arr[i].bcy = f["bcy"].ptr if f.get("bcy") is not None else None
+                arr[i].bcz = f["bcz"].ptr if f.get("bcz") is not None else None
+                arr[i].slot = int(f.get("slot", 0))
+            else:
+                arr[i].bound = f["bound"].encode()
+        return arr, keep
+
+    def graph_create(self, fields, rect=False, precision=PREC_FP64):
+        """Capture one batched solve as a CUDA graph; returns its id."""
+        arr, keep = self._field_array(fields, rect)
+        gid = C.c_int()
+        self._check(lib().ductgpu_graph_create(self.h, 1 if rect else 0, C.cast(arr, C.c_void_p), len(fields),
+                                               int(precision), C.byref(gid)))
+        return gid.value
+
+    def graph_launch(self, gid):
+        self._check(lib().ductgpu_graph_launch(self.h, int(gid)))
+
+    def graph_destroy(self, gid):
+        self._check(lib().ductgpu_graph_destroy(self.h, int(gid)))
 
     def solve_fields_dev(self, fields, precision=PREC_FP64):
         """fields: list of dicts(rhs=DeviceArray, sol=DeviceArray, xalp=ndarray,

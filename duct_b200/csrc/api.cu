@@ -83,7 +83,7 @@ static int prepare(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, Fi
     int rc = ensure_lam(ctx, planes);
     if (rc) return rc;
     // the pinned staging buffer may still be read by an earlier copy
-    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (!ctx->capturing) DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     int p = 0;
     for (int i = 0; i < nfields; ++i) {
         const ductgpu_field &f = fields[i];
@@ -108,15 +108,16 @@ static int prepare(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, Fi
         tasks[i].refine = (kappa <= 1.0e3 && ctx->refine_steps > 0) ? 1 : ctx->refine_steps;
         p += f.nmodes;
     }
-    DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->lam, ctx->lam_host, planes * sizeof(double),
-                                   cudaMemcpyHostToDevice, ctx->stream));
+    if (!ctx->capturing)
+        DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->lam, ctx->lam_host, planes * sizeof(double),
+                                       cudaMemcpyHostToDevice, ctx->stream));
     return DUCTGPU_OK;
 }
 
 LaunchScope::LaunchScope(ductgpu_ctx ctx, int kind) : c(ctx)
 {
     c->launches += 1;
-    if (!c->prof_on) return;
+    if (!c->prof_on || c->capturing) return;
     if (c->prof_used >= ductgpu_ctx_s::kProfSlots) profile_drain(c);
     slot = c->prof_used++;
     c->prof_kind[slot] = kind;
@@ -191,6 +192,8 @@ int ductgpu_destroy(ductgpu_ctx ctx)
     free_bound(ctx->dir);
     free_bound(ctx->neu);
     for (int i = 0; i < kMaxRect; ++i) free_rect(ctx->rect[i]);
+    for (int i = 0; i < ductgpu_ctx_s::kMaxGraphs; ++i)
+        if (ctx->graph_exec[i]) { cudaGraphExecDestroy(ctx->graph_exec[i]); cudaFree(ctx->graph_lam[i]); }
     cudaFree(ctx->xcol); cudaFree(ctx->DC); cudaFree(ctx->D2); cudaFree(ctx->AM1); cudaFree(ctx->ccw);
     cudaFree(ctx->work.buf);
     cudaFree(ctx->io.buf);
@@ -532,7 +535,7 @@ int ductgpu_solve_rect_fields_dev(ductgpu_ctx ctx, const ductgpu_rect_field *fie
     cudaSetDevice(ctx->device);
     int rc = ensure_lam(ctx, planes);
     if (rc) return rc;
-    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (!ctx->capturing) DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     RectTask tasks[kMaxFields];
     int p = 0;
     for (int i = 0; i < nfields; ++i) {
@@ -548,7 +551,8 @@ int ductgpu_solve_rect_fields_dev(ductgpu_ctx ctx, const ductgpu_rect_field *fie
         for (int k = 0; k < f.nmodes; ++k) ctx->lam_host[p + k] = f.alambda + f.xalp[k] * f.xalp[k];
         p += f.nmodes;
     }
-    DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->lam, ctx->lam_host, planes * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if (!ctx->capturing)
+        DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->lam, ctx->lam_host, planes * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     return solve_rect(ctx, tasks, nfields);
 }
 
@@ -591,6 +595,118 @@ int ductgpu_helm3d_temp(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, dou
     if ((rc = ductgpu_solve_rect_fields_dev(ctx, &f, 1))) return rc;
     DUCT_CUDA(ctx, cudaMemcpyAsync(sol, dsol, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d_temp");
+}
+
+static int run_solve(ductgpu_ctx ctx, int kind, const void *fields, int nfields, int precision)
+{
+    if (kind == 0)
+        return ductgpu_solve_fields_dev(ctx, static_cast<const ductgpu_field *>(fields), nfields, precision);
+    return ductgpu_solve_rect_fields_dev(ctx, static_cast<const ductgpu_rect_field *>(fields), nfields);
+}
+
+int ductgpu_graph_create(ductgpu_ctx ctx, int kind, const void *fields, int nfields, int precision, int *graph_id)
+{
+    if (!ctx || !fields || !graph_id || (kind != 0 && kind != 1)) return DUCTGPU_EARG;
+    int id = -1;
+    for (int i = 0; i < ductgpu_ctx_s::kMaxGraphs; ++i)
+        if (!ctx->graph_exec[i]) { id = i; break; }
+    if (id < 0) return set_error(ctx, DUCTGPU_EALLOC, "all %d graph slots in use", ductgpu_ctx_s::kMaxGraphs);
+    cudaSetDevice(ctx->device);
+    if (ctx->stream == (cudaStream_t)0)
+        return set_error(ctx, DUCTGPU_EARG, "graph capture needs a non-default stream");
+    // uncaptured run: sizes the workspaces and fills ctx->lam
+    int rc = run_solve(ctx, kind, fields, nfields, precision);
+    if (rc) return rc;
+    int planes = 0;
+    for (int i = 0; i < nfields; ++i)
+        planes += (kind == 0) ? static_cast<const ductgpu_field *>(fields)[i].nmodes
+                              : static_cast<const ductgpu_rect_field *>(fields)[i].nmodes;
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    DUCT_CUDA(ctx, cudaMalloc(&ctx->graph_lam[id], planes * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMemcpy(ctx->graph_lam[id], ctx->lam, planes * sizeof(double), cudaMemcpyDeviceToDevice));
+    double *lam_saved = ctx->lam;
+    ctx->lam = ctx->graph_lam[id];
+    ctx->capturing = true;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        rc = run_solve(ctx, kind, fields, nfields, precision);
+        cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &g);
+        if (!rc && e2 != cudaSuccess) rc = check_cuda(ctx, e2, "cudaStreamEndCapture");
+    } else {
+        rc = check_cuda(ctx, e, "cudaStreamBeginCapture");
+    }
+    ctx->capturing = false;
+    ctx->lam = lam_saved;
+    if (!rc) rc = check_cuda(ctx, cudaGraphInstantiate(&ctx->graph_exec[id], g, 0), "cudaGraphInstantiate");
+    if (g) cudaGraphDestroy(g);
+    if (rc) {
+        cudaFree(ctx->graph_lam[id]);
+        ctx->graph_lam[id] = nullptr;
+        ctx->graph_exec[id] = nullptr;
+        return rc;
+    }
+    *graph_id = id;
+    return DUCTGPU_OK;
+}
+
+int ductgpu_graph_launch(ductgpu_ctx ctx, int graph_id)
+{
+    if (!ctx || graph_id < 0 || graph_id >= ductgpu_ctx_s::kMaxGraphs || !ctx->graph_exec[graph_id])
+        return DUCTGPU_EARG;
+    ctx->launches += 1;
+    return check_cuda(ctx, cudaGraphLaunch(ctx->graph_exec[graph_id], ctx->stream), "cudaGraphLaunch");
+}
+
+int ductgpu_graph_destroy(ductgpu_ctx ctx, int graph_id)
+{
+    if (!ctx || graph_id < 0 || graph_id >= ductgpu_ctx_s::kMaxGraphs || !ctx->graph_exec[graph_id])
+        return DUCTGPU_EARG;
+    cudaStreamSynchronize(ctx->stream);
+    cudaGraphExecDestroy(ctx->graph_exec[graph_id]);
+    cudaFree(ctx->graph_lam[graph_id]);
+    ctx->graph_exec[graph_id] = nullptr;
+    ctx->graph_lam[graph_id] = nullptr;
+    return DUCTGPU_OK;
+}
+
+// ---- the reference's GPU entry points (src/mytranspose_cuda.cu:132-196) ----
+__global__ void k_real_transpose(const double *A, double *C, int nx, int ny)
+{
+    __shared__ double tile[32][33];
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int r = ty; r < 32; r += 8)
+        if (x0 + tx < nx && y0 + r < ny) tile[r][tx] = A[(x0 + tx) + (size_t)nx * (y0 + r)];
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8)
+        if (y0 + tx < ny && x0 + r < nx) C[(y0 + tx) + (size_t)ny * (x0 + r)] = tile[tx][r];
+}
+
+__global__ void k_invdiag(const double *F, const double *ED, double *C, long long n, double xlam)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        C[i] = F[i] / (ED[i] - xlam);
+}
+
+int transpose_gpu_(size_t *handle, const int *Nx, const int *Ny, const double *alpha, const size_t *devPtrA, size_t *devPtrC)
+{
+    (void)handle; (void)alpha;
+    if (!Nx || !Ny || !devPtrA || !devPtrC || *Nx < 1 || *Ny < 1) return DUCTGPU_EARG;
+    dim3 grid((*Nx + 31) / 32, (*Ny + 31) / 32);
+    k_real_transpose<<<grid, 256>>>((const double *)(*devPtrA), (double *)(*devPtrC), *Nx, *Ny);
+    return cudaGetLastError() == cudaSuccess ? DUCTGPU_OK : DUCTGPU_ECUDA;
+}
+
+int mat_invdiag_gpu_(size_t *handle, const int *Nx, const int *Ny, const double *xlam, const size_t *devPtrF,
+                     const size_t *devPtrED, size_t *devPtrC)
+{
+    (void)handle;
+    if (!Nx || !Ny || !xlam || !devPtrF || !devPtrED || !devPtrC || *Nx < 1 || *Ny < 1) return DUCTGPU_EARG;
+    const long long n = (long long)(*Nx) * (*Ny);
+    const int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+    k_invdiag<<<blocks, 256>>>((const double *)(*devPtrF), (const double *)(*devPtrED), (double *)(*devPtrC), n, *xlam);
+    return cudaGetLastError() == cudaSuccess ? DUCTGPU_OK : DUCTGPU_ECUDA;
 }
 
 int ductgpu_device_alloc(ductgpu_ctx ctx, size_t bytes, void **ptr)

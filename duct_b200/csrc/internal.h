@@ -81,6 +81,11 @@ struct ductgpu_ctx_s {
     duct::BoundOps dir, neu;
 
     duct::RectSlot rect[duct::kMaxRect];
+    // captured solves (CUDA graphs), each with its own lambda array
+    static constexpr int kMaxGraphs = 16;
+    cudaGraphExec_t graph_exec[kMaxGraphs] = {};
+    double *graph_lam[kMaxGraphs] = {};
+    bool capturing = false;
     duct::Workspace work;      // pass intermediates
     duct::Workspace io;        // device copies for host entries
     int *dev_err = nullptr;    // device error word (bounded waits)

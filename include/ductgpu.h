@@ -157,6 +157,18 @@ typedef struct {
 int ductgpu_solve_rect_fields_dev(ductgpu_ctx ctx, const ductgpu_rect_field *fields,
                                   int nfields);
 
+/* ---- captured solves (CUDA graphs) ------------------------------------ */
+/* Capture one batched solve -- kind 0: `fields` is a ductgpu_field array
+ * (square path, `precision` as in ductgpu_solve_fields_dev); kind 1: a
+ * ductgpu_rect_field array -- as a CUDA graph bound to the fields' device
+ * pointers and wavenumbers, e.g. the four solves of an RK3/CN substep.  The
+ * solve runs once uncaptured first (workspaces, checks).  Replays with
+ * ductgpu_graph_launch cost one launch.                                   */
+int ductgpu_graph_create(ductgpu_ctx ctx, int kind, const void *fields, int nfields,
+                         int precision, int *graph_id);
+int ductgpu_graph_launch(ductgpu_ctx ctx, int graph_id);
+int ductgpu_graph_destroy(ductgpu_ctx ctx, int graph_id);
+
 /* ---- Chebyshev transforms, derivatives, pencil transposes ------------ */
 /* transyz(cheb,cdir,iopt), src/chebyshev.f90:458-540 with tcheb_fftw,
  * src/tchebw.f:62-192: DCT-I of every line of a complex (my,mz,nmodes)
@@ -194,6 +206,20 @@ int ductgpu_cyzx2xyz_dev(ductgpu_ctx ctx, double *phys, const double *phys2,
  * (src/parallel.F:132); this is the inverse of chx2z it documents.        */
 int ductgpu_chx2z_dev(ductgpu_ctx ctx, double *xy, double *xz, int my, int mz, int nmodes);
 int ductgpu_chz2x_dev(ductgpu_ctx ctx, double *xz, double *xy, int my, int mz, int nmodes);
+
+/* ---- the reference's own GPU entry points (src/mytranspose_cuda.cu) --- */
+/* transpose_gpu_(handle,Nx,Ny,alpha,devPtrA,devPtrC) and
+ * mat_invdiag_gpu_(handle,Nx,Ny,xlam,devPtrF,devPtrED,devPtrC) with the
+ * reference's Fortran argument convention (pointers to integers, device
+ * addresses as size_t handles; src/mytranspose_cuda.cu:132-196).  Unlike the
+ * reference (grid(N/32,N/32), defect for N not a multiple of 32) every size
+ * is handled.  C(j,i) = A(i,j) for an Nx x Ny column-major A;
+ * C = F / (ED - xlam) elementwise.  They run on the legacy default stream;
+ * handle and alpha are accepted and unused, as in the reference.          */
+int transpose_gpu_(size_t *handle, const int *Nx, const int *Ny, const double *alpha,
+                   const size_t *devPtrA, size_t *devPtrC);
+int mat_invdiag_gpu_(size_t *handle, const int *Nx, const int *Ny, const double *xlam,
+                     const size_t *devPtrF, const size_t *devPtrED, size_t *devPtrC);
 
 /* ---- memory helpers (for callers without a CUDA toolchain, e.g. Fortran
  * hosts that keep fields resident on the device between time steps) ---- */

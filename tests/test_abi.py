@@ -15,7 +15,7 @@ def declared():
         if h.endswith(".h"):
             src = open(os.path.join(ROOT, "include", h)).read()
             src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-            names |= set(re.findall(r"\b(ductgpu_\w+)\s*\(", src))
+            names |= set(re.findall(r"\b(ductgpu_\w+|\w+_gpu_)\s*\(", src))
     return names
 
 
