@@ -31,6 +31,7 @@ EXPORTS = [
     "ductgpu_set_refinement", "ductgpu_pseudomat_temp", "ductgpu_helm3d_temp",
     "ductgpu_solve_rect_fields_dev", "ductgpu_graph_create", "ductgpu_graph_launch",
     "ductgpu_graph_destroy", "transpose_gpu_", "mat_invdiag_gpu_",
+    "ductgpu_preshen", "ductgpu_helm3d_shen", "ductgpu_solve_shen_fields_dev",
 ]
 K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
 
@@ -98,6 +99,9 @@ def lib():
                                     C.c_char, C.c_char],
             "ductgpu_solve_rect_fields_dev": [P, C.POINTER(RectField), I],
             "ductgpu_graph_create": [P, I, P, I, I, C.POINTER(I)],
+            "ductgpu_preshen": [P, I, C.c_char],
+            "ductgpu_helm3d_shen": [P, P, P, I, C.c_char, D, I, I, I, I, P],
+            "ductgpu_solve_shen_fields_dev": [P, C.POINTER(Field), I],
             "ductgpu_graph_launch": [P, I],
             "ductgpu_graph_destroy": [P, I],
             "transpose_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
@@ -229,6 +233,28 @@ class Context:
                                          _ptr(xalp), int(precision)))
         return sol
 
+    def preshen(self, my, bound):
+        self._check(lib().ductgpu_preshen(self.h, int(my), bound.encode()))
+
+    def helm3d_shen(self, rhs, bound, alambda, xalp, ib=0, ipro=1):
+        """helm3d_shen drop-in on host arrays: rhs (my,my,nmodes) complex128,
+        Fortran order, overwritten with its Chebyshev coefficients like the
+        reference.  Returns the solution."""
+        assert rhs.dtype == np.complex128 and rhs.flags.f_contiguous
+        my, mz, nm = rhs.shape
+        sol = np.zeros_like(rhs, order="F")
+        xalp = np.ascontiguousarray(xalp, dtype=np.float64)
+        assert xalp.shape == (nm,)
+        self._check(lib().ductgpu_helm3d_shen(self.h, _ptr(rhs), _ptr(sol), int(ipro), bound.encode(),
+                                              float(alambda), my, mz, int(ib), int(ib) + nm - 1, _ptr(xalp)))
+        return sol
+
+    def solve_shen_fields_dev(self, fields):
+        """Like solve_fields_dev for the Shen solver (rhs overwritten)."""
+        arr, keep = self._field_array(fields, False)
+        self._check(lib().ductgpu_solve_shen_fields_dev(self.h, arr, len(fields)))
+        return keep
+
     def pseudomat_temp(self, slot, my, mz, sy=1.0, sz=1.0, by=("d", "d"), bz=("d", "d")):
         self._check(lib().ductgpu_pseudomat_temp(self.h, int(slot), int(my), int(mz), float(sy), float(sz),
                                                  by[0].encode(), by[1].encode(), bz[0].encode(), bz[1].encode()))
@@ -291,11 +317,13 @@ class Context:
                 arr[i].bound = f["bound"].encode()
         return arr, keep
 
-    def graph_create(self, fields, rect=False, precision=PREC_FP64):
-        """Capture one batched solve as a CUDA graph; returns its id."""
+    def graph_create(self, fields, rect=False, precision=PREC_FP64, shen=False):
+        """Capture one batched solve as a CUDA graph (kind 1: rectangular,
+        2: Shen, else the square diagonalisation solve); returns its id."""
         arr, keep = self._field_array(fields, rect)
         gid = C.c_int()
-        self._check(lib().ductgpu_graph_create(self.h, 1 if rect else 0, C.cast(arr, C.c_void_p), len(fields),
+        kind = 1 if rect else (2 if shen else 0)
+        self._check(lib().ductgpu_graph_create(self.h, kind, C.cast(arr, C.c_void_p), len(fields),
                                                int(precision), C.byref(gid)))
         return gid.value
 

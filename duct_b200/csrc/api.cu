@@ -192,6 +192,8 @@ int ductgpu_destroy(ductgpu_ctx ctx)
     free_bound(ctx->dir);
     free_bound(ctx->neu);
     for (int i = 0; i < kMaxRect; ++i) free_rect(ctx->rect[i]);
+    free_shen(ctx->shen_d);
+    free_shen(ctx->shen_n);
     for (int i = 0; i < ductgpu_ctx_s::kMaxGraphs; ++i)
         if (ctx->graph_exec[i]) { cudaGraphExecDestroy(ctx->graph_exec[i]); cudaFree(ctx->graph_lam[i]); }
     cudaFree(ctx->xcol); cudaFree(ctx->DC); cudaFree(ctx->D2); cudaFree(ctx->AM1); cudaFree(ctx->ccw);
@@ -597,16 +599,103 @@ int ductgpu_helm3d_temp(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, dou
     return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d_temp");
 }
 
+int ductgpu_preshen(ductgpu_ctx ctx, int my, char bound)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (bound != 'd' && bound != 'n') return set_error(ctx, DUCTGPU_EARG, "preshen: bound '%c'", bound);
+    cudaSetDevice(ctx->device);
+    return shen_setup(ctx, my, bound);
+}
+
+int ductgpu_solve_shen_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (!fields || nfields < 1 || nfields > kMaxFields)
+        return set_error(ctx, DUCTGPU_EARG, "nfields=%d (1..%d)", nfields, kMaxFields);
+    int planes = 0, m = 0;
+    for (int i = 0; i < nfields; ++i) {
+        int rc = validate_field(ctx, fields[i]);
+        if (rc) return rc;
+        const ShenOps &s = (fields[i].bound == 'n') ? ctx->shen_n : ctx->shen_d;
+        if (!s.ready) return set_error(ctx, DUCTGPU_ESTATE, "preshen('%c') not set up", fields[i].bound);
+        if (m && s.m != m) return set_error(ctx, DUCTGPU_EARG, "fields of one call need the same grid (%d vs %d)", s.m, m);
+        m = s.m;
+        planes += fields[i].nmodes;
+    }
+    cudaSetDevice(ctx->device);
+    int rc = ensure_lam(ctx, planes);
+    if (rc) return rc;
+    // the pinned staging buffer may still be read by an earlier copy
+    if (!ctx->capturing) DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ShenTask tasks[kMaxFields];
+    int p = 0;
+    for (int i = 0; i < nfields; ++i) {
+        const ductgpu_field &f = fields[i];
+        tasks[i].rhs = f.rhs;
+        tasks[i].sol = f.sol;
+        tasks[i].nmodes = f.nmodes;
+        tasks[i].mode0 = (f.ib == 0);
+        tasks[i].plane0 = p;
+        tasks[i].bound = f.bound;
+        // xlambda = alambda + xalp(imode)^2, src/helm_shen.f90:65
+        for (int k = 0; k < f.nmodes; ++k) ctx->lam_host[p + k] = f.alambda + f.xalp[k] * f.xalp[k];
+        p += f.nmodes;
+    }
+    if (!ctx->capturing)
+        DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->lam, ctx->lam_host, planes * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    return solve_shen(ctx, tasks, nfields);
+}
+
+int ductgpu_helm3d_shen(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, char bound, double alambda,
+                        int my, int mz, int ib, int ie, const double *xalp)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (bound != 'd' && bound != 'n') return set_error(ctx, DUCTGPU_EARG, "helm3d_shen: bound '%c'", bound);
+    if (my != mz) return set_error(ctx, DUCTGPU_EARG, "helm3d_shen needs my == mz (%d, %d)", my, mz);
+    if (ipro <= 0) {
+        int rc = ductgpu_preshen(ctx, my, bound);
+        if (rc) return rc;
+        if (ipro == -1) return DUCTGPU_OK;
+    }
+    const ShenOps &s = (bound == 'n') ? ctx->shen_n : ctx->shen_d;
+    if (!s.ready) return set_error(ctx, DUCTGPU_ESTATE, "preshen not set up (call with ipro<=0)");
+    if (my != s.m) return set_error(ctx, DUCTGPU_EARG, "grid %d differs from the set-up %d", my, s.m);
+    if (!rhs || !sol || !xalp) return set_error(ctx, DUCTGPU_EARG, "null pointer");
+    if (ie < ib || ib < 0) return set_error(ctx, DUCTGPU_EARG, "ib=%d ie=%d", ib, ie);
+    cudaSetDevice(ctx->device);
+    const int nm = ie - ib + 1;
+    const size_t bytes = (size_t)2 * my * mz * nm * sizeof(double);
+    int rc = ensure(ctx, ctx->io, 2 * bytes);
+    if (rc) return rc;
+    double *drhs = ctx->io.buf, *dsol = ctx->io.buf + bytes / sizeof(double);
+    DUCT_CUDA(ctx, cudaMemcpyAsync(drhs, rhs, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    ductgpu_field f;
+    f.rhs = drhs;
+    f.sol = dsol;
+    f.xalp = xalp;
+    f.alambda = alambda;
+    f.ib = ib;
+    f.nmodes = nm;
+    f.bound = bound;
+    if ((rc = ductgpu_solve_shen_fields_dev(ctx, &f, 1))) return rc;
+    // rhs comes back as its Chebyshev coefficients, like the reference's
+    DUCT_CUDA(ctx, cudaMemcpyAsync(rhs, drhs, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(sol, dsol, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d_shen");
+}
+
 static int run_solve(ductgpu_ctx ctx, int kind, const void *fields, int nfields, int precision)
 {
     if (kind == 0)
         return ductgpu_solve_fields_dev(ctx, static_cast<const ductgpu_field *>(fields), nfields, precision);
+    if (kind == 2)
+        return ductgpu_solve_shen_fields_dev(ctx, static_cast<const ductgpu_field *>(fields), nfields);
     return ductgpu_solve_rect_fields_dev(ctx, static_cast<const ductgpu_rect_field *>(fields), nfields);
 }
 
 int ductgpu_graph_create(ductgpu_ctx ctx, int kind, const void *fields, int nfields, int precision, int *graph_id)
 {
-    if (!ctx || !fields || !graph_id || (kind != 0 && kind != 1)) return DUCTGPU_EARG;
+    if (!ctx || !fields || !graph_id || kind < 0 || kind > 2) return DUCTGPU_EARG;
     int id = -1;
     for (int i = 0; i < ductgpu_ctx_s::kMaxGraphs; ++i)
         if (!ctx->graph_exec[i]) { id = i; break; }
@@ -619,7 +708,7 @@ int ductgpu_graph_create(ductgpu_ctx ctx, int kind, const void *fields, int nfie
     if (rc) return rc;
     int planes = 0;
     for (int i = 0; i < nfields; ++i)
-        planes += (kind == 0) ? static_cast<const ductgpu_field *>(fields)[i].nmodes
+        planes += (kind != 1) ? static_cast<const ductgpu_field *>(fields)[i].nmodes
                               : static_cast<const ductgpu_rect_field *>(fields)[i].nmodes;
     DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     DUCT_CUDA(ctx, cudaMalloc(&ctx->graph_lam[id], planes * sizeof(double)));

@@ -53,6 +53,17 @@ struct RectSlot {
     int sing_y = -1, sing_z = -1;          // argmin |E| per direction
 };
 
+// Shen-Legendre operators of one wall condition (src/preshen.f90)
+struct ShenOps {
+    bool ready = false;
+    int m = 0;
+    char bound = 'd';
+    BoundOps leg;        // P = A (Chebyshev -> Legendre), PM1 = B = A^-1, n = m
+    BoundOps eig;        // P = eigenvectors, PM1 = P^-1 S^-1, E = rho, n = m-2
+    double *Md = nullptr, *Mo = nullptr, *Sm = nullptr;   // mass diag, mass (k,k+2), makeMS stiffness
+    double *bk = nullptr;   // b_k
+};
+
 struct Workspace {
     double *buf = nullptr;
     size_t bytes = 0;
@@ -81,6 +92,7 @@ struct ductgpu_ctx_s {
     duct::BoundOps dir, neu;
 
     duct::RectSlot rect[duct::kMaxRect];
+    duct::ShenOps shen_d, shen_n;
     // captured solves (CUDA graphs), each with its own lambda array
     static constexpr int kMaxGraphs = 16;
     cudaGraphExec_t graph_exec[kMaxGraphs] = {};
@@ -157,6 +169,7 @@ struct PassField {
     int nchunks;         // ceil(nlines / kPassLines)
     int kpad, mtiles;    // padded K and 16-row tiles of the packed operator
     int sk, sl;          // complex strides of (k, line)
+    int off;             // first point/line: 1 (interior) or 0 (full plane)
     long long plane_stride;  // doubles per complex plane
     // residual epilogue: dst = resF - resT - acc + lam * resU
     const double *resF, *resT, *resU;
@@ -181,6 +194,16 @@ void pass_geometry(PassField &f, const BoundOps &b, const double *El, int nlines
 int rect_setup(ductgpu_ctx ctx, int slot, int my, int mz, double sy, double sz, char by1, char by2,
                char bz1, char bz2);
 void free_rect(RectSlot &r);
+
+// shen.cu
+void free_shen(ShenOps &s);
+int shen_setup(ductgpu_ctx ctx, int m, char bound);
+struct ShenTask {
+    double *rhs, *sol;
+    int nmodes, mode0, plane0;
+    char bound;
+};
+int solve_shen(ductgpu_ctx ctx, const ShenTask *tasks, int ntasks);
 
 // solve_rect.cu
 struct RectTask {

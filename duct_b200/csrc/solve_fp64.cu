@@ -86,13 +86,13 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
     load_a(0, 0);
 
     // Stage the lines: Bs[k][2l + c] = in(k, l0 + l) component c, zero padded.
-    const int n = F.n, sk = F.sk, sl = F.sl;
+    const int n = F.n, sk = F.sk, sl = F.sl, o1 = F.off;
     if (sk == 1) {
         for (int idx = tid; idx < kpad * kLines; idx += kThreads) {
             const int k = idx % kpad, l = idx / kpad;
             double2 v = make_double2(0.0, 0.0);
             if (k < n && l < L)
-                v = *reinterpret_cast<const double2 *>(src + 2 * ((long long)(k + 1) * sk + (long long)(l0 + l + 1) * sl));
+                v = *reinterpret_cast<const double2 *>(src + 2 * ((long long)(k + o1) * sk + (long long)(l0 + l + o1) * sl));
             *reinterpret_cast<double2 *>(Bs + k * kNld + 2 * l) = v;
         }
     } else {
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
             const int l = idx % kLines, k = idx / kLines;
             double2 v = make_double2(0.0, 0.0);
             if (k < n && l < L)
-                v = *reinterpret_cast<const double2 *>(src + 2 * ((long long)(k + 1) * sk + (long long)(l0 + l + 1) * sl));
+                v = *reinterpret_cast<const double2 *>(src + 2 * ((long long)(k + o1) * sk + (long long)(l0 + l + o1) * sl));
             *reinterpret_cast<double2 *>(Bs + k * kNld + 2 * l) = v;
         }
     }
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
                         im = im / den;
                     }
                 }
-                const long long off = 2 * ((long long)(o + 1) * sk + (long long)(lg + 1) * sl);
+                const long long off = 2 * ((long long)(o + o1) * sk + (long long)(lg + o1) * sl);
                 if (p.residual) {
                     const long long po = (long long)plane * F.plane_stride + off;
                     const double2 f = *reinterpret_cast<const double2 *>(F.resF + po);
@@ -225,6 +225,7 @@ void pass_geometry(PassField &f, const BoundOps &b, const double *El, int nlines
     f.nchunks = (nlines + kLines - 1) / kLines;
     f.sk = sk;
     f.sl = sl;
+    f.off = 1;
     f.plane_stride = plane_stride;
 }
 

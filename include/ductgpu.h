@@ -157,10 +157,29 @@ typedef struct {
 int ductgpu_solve_rect_fields_dev(ductgpu_ctx ctx, const ductgpu_rect_field *fields,
                                   int nfields);
 
+/* ---- Shen-Legendre Galerkin solver (HELM_SHEN build) ----------------- */
+/* preshen(eigv,psm1,bound) + leg_cheb_mat, src/preshen.f90:2-535 and
+ * src/legendre.f90:3-110: the Legendre-Chebyshev matrices and the
+ * generalized eigen-decomposition M x = rho S x of bound 'd' or 'n' for a
+ * square my x my grid (my odd, 5..191, my-1 = 2^a 3^b for the transform). */
+int ductgpu_preshen(ductgpu_ctx ctx, int my, char bound);
+/* helm3d_shen(rhs,sol,work,ipro,bound,cvar,a,b,alambda),
+ * src/helm_shen.f90:2-85 -> int2d3d -> solveshen (src/solveshen.f90:5-94):
+ * solves -lap(u) + (alambda + xalp^2) u = rhs in the Shen basis on host
+ * arrays.  As in the reference, rhs is overwritten with its Chebyshev
+ * coefficients (transyz y and z, iopt -1); ipro <= 0 runs preshen first,
+ * ipro = -1 only that.  Mode 0 (ib = 0) has a real solution.              */
+int ductgpu_helm3d_shen(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, char bound,
+                        double alambda, int my, int mz, int ib, int ie, const double *xalp);
+/* Batched device-resident form: every field's `bound` selects its preshen
+ * operators; all fields share my (= mz).  rhs is overwritten as above.    */
+int ductgpu_solve_shen_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields);
+
 /* ---- captured solves (CUDA graphs) ------------------------------------ */
 /* Capture one batched solve -- kind 0: `fields` is a ductgpu_field array
  * (square path, `precision` as in ductgpu_solve_fields_dev); kind 1: a
- * ductgpu_rect_field array -- as a CUDA graph bound to the fields' device
+ * ductgpu_rect_field array; kind 2: a ductgpu_field array of the Shen
+ * solver (ductgpu_solve_shen_fields_dev) -- as a CUDA graph bound to the fields' device
  * pointers and wavenumbers, e.g. the four solves of an RK3/CN substep.  The
  * solve runs once uncaptured first (workspaces, checks).  Replays with
  * ductgpu_graph_launch cost one launch.                                   */

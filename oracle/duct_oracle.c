@@ -33,6 +33,12 @@ extern void scipy_dgemm_(const char *ta, const char *tb, const int *m,
                          const double *a, const int *lda, const double *b,
                          const int *ldb, const double *beta, double *c,
                          const int *ldc, size_t, size_t);
+extern void scipy_dsygv_(const int *itype, const char *jobz, const char *uplo,
+                         const int *n, double *a, const int *lda, double *b,
+                         const int *ldb, double *w, double *work,
+                         const int *lwork, int *info, size_t, size_t);
+extern void scipy_dptsv_(const int *n, const int *nrhs, double *d, double *e,
+                         double *b, const int *ldb, int *info);
 extern void scipy_openblas_set_num_threads(int);
 
 void orc_set_blas_threads(int n) { scipy_openblas_set_num_threads(n); }
@@ -806,5 +812,258 @@ int orc_helm3d_temp(const double *rhs, double *sol, int my, int mz, int ib, int 
         }
         free(U);
     }
+    return 0;
+}
+
+/* ---- Shen-Legendre Galerkin solver ------------------------------------- */
+/* generalized symmetric eigenproblem A x = w B x (itype 1), as the
+ * reference's dsygv call (src/preshen.f90:463-496).                        */
+static int sygv(int n, double *A, double *B, double *w)
+{
+    int itype = 1, info = 0, lwk = -1;
+    double q = 0.0;
+    scipy_dsygv_(&itype, "V", "U", &n, A, &n, B, &n, w, &q, &lwk, &info, 1, 1);
+    lwk = (int)q + 16;
+    double *wk = (double *)malloc(sizeof(double) * (size_t)lwk);
+    scipy_dsygv_(&itype, "V", "U", &n, A, &n, B, &n, w, wk, &lwk, &info, 1, 1);
+    free(wk);
+    return info;
+}
+
+/* preshen + makeMS + precomeigen (src/preshen.f90:2-535) and leg_cheb_mat
+ * (src/legendre.f90:3-110).                                               */
+int orc_shen_setup(int m, char bound, orc_shen *s)
+{
+    if (m < 5 || (m % 2) == 0) return -1;
+    memset(s, 0, sizeof(*s));
+    const int n = m - 2, nm1 = m - 1;
+    s->m = m;
+    s->bound = bound;
+    s->b = (double *)calloc((size_t)m, sizeof(double));
+    s->M = (double *)calloc((size_t)n * n, sizeof(double));
+    s->S = (double *)calloc((size_t)n * n, sizeof(double));
+    s->E = (double *)calloc((size_t)n, sizeof(double));
+    s->P = (double *)calloc((size_t)n * n, sizeof(double));
+    s->PSM1 = (double *)calloc((size_t)n * n, sizeof(double));
+    s->A = (double *)calloc((size_t)m * m, sizeof(double));
+    s->B = (double *)calloc((size_t)m * m, sizeof(double));
+    for (int kk = 0; kk < m; ++kk)                      /* makeMS :359-371 */
+        s->b[kk] = (bound == 'd') ? -1.0 : -(double)(kk * (kk + 1)) / (double)((kk + 2) * (kk + 3));
+    for (int k = 0; k < n; ++k) {                       /* precomeigen :450-460 */
+        s->S[IX(k, k, n)] = -s->b[k] * (double)(4 * k + 6);
+        s->M[IX(k, k, n)] = 2.0 / (double)(2 * k + 1) + 2.0 * s->b[k] * s->b[k] / (double)(2 * k + 5);
+    }
+    if (bound == 'n') s->S[0] = 2.0;
+    for (int k = 0; k < n - 2; ++k) {
+        const double v = s->b[k] * 2.0 / (double)(2 * k + 5);
+        s->M[IX(k, k + 2, n)] = v;
+        s->M[IX(k + 2, k, n)] = v;
+    }
+    int info = 0;
+    if (bound == 'd') {
+        double *Pv = (double *)malloc(sizeof(double) * (size_t)n * n);
+        double *St = (double *)malloc(sizeof(double) * (size_t)n * n);
+        memcpy(Pv, s->M, sizeof(double) * (size_t)n * n);
+        memcpy(St, s->S, sizeof(double) * (size_t)n * n);
+        info = sygv(n, Pv, St, s->E);
+        memcpy(s->P, Pv, sizeof(double) * (size_t)n * n);
+        free(Pv); free(St);
+    } else {
+        const int n1 = n - 1;                            /* :479-496 */
+        double *M1 = (double *)calloc((size_t)n1 * n1, sizeof(double));
+        double *S1 = (double *)calloc((size_t)n1 * n1, sizeof(double));
+        double *E1 = (double *)calloc((size_t)n1, sizeof(double));
+        for (int j = 0; j < n1; ++j)
+            for (int i = 0; i < n1; ++i) {
+                M1[IX(i, j, n1)] = s->M[IX(i + 1, j + 1, n)];
+                S1[IX(i, j, n1)] = s->S[IX(i + 1, j + 1, n)];
+            }
+        info = sygv(n1, M1, S1, E1);
+        s->P[0] = 1.0;
+        s->E[0] = 1.0;
+        for (int i = 0; i < n1; ++i) {
+            s->E[i + 1] = E1[i];
+            for (int j = 0; j < n1; ++j) s->P[IX(i + 1, j + 1, n)] = M1[IX(i, j, n1)];
+        }
+        free(M1); free(S1); free(E1);
+    }
+    if (info) return info;
+    memcpy(s->PSM1, s->P, sizeof(double) * (size_t)n * n);   /* :516-530 */
+    if ((info = invert(n, s->PSM1))) return info;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) s->PSM1[IX(i, j, n)] /= s->S[IX(j, j, n)];
+    /* leg_cheb_mat: A upper triangular by the recurrence :56-82 */
+    double *A = s->A;
+    A[IX(0, 0, m)] = 1.0;
+    A[IX(1, 1, m)] = 1.0;
+    for (int k = 2; k <= nm1; ++k) A[IX(k, k, m)] = 2.0 * (double)k / (double)(2 * k - 1) * A[IX(k - 1, k - 1, m)];
+    for (int k = 2; k <= nm1; k += 2) A[IX(0, k, m)] = -1.0 / (double)(k * k - 1);
+    for (int j = 2; j <= nm1 - 1; ++j) {                 /* Fortran j=2..n-1, jj=j+1 */
+        const int jj = j + 1;
+        for (int i = 1; i <= j; ++i) {
+            const int ii = i + 1;
+            const double c1 = (double)(2 * i + 2) / (double)(2 * i + 3);
+            const double c2 = (double)(2 * i) / (double)(2 * i - 1);
+            /* A(ii,jj+1)=c1*A(ii+1,jj)+c2*A(ii-1,jj)-A(ii,jj-1), 1-based */
+            A[IX(ii - 1, jj, m)] = c1 * A[IX(ii, jj - 1, m)] + c2 * A[IX(ii - 2, jj - 1, m)] - A[IX(ii - 1, jj - 2, m)];
+        }
+    }
+    memcpy(s->B, A, sizeof(double) * (size_t)m * m);
+    return invert(m, s->B);
+}
+
+void orc_shen_free(orc_shen *s)
+{
+    free(s->b); free(s->M); free(s->S); free(s->E); free(s->P); free(s->PSM1); free(s->A); free(s->B);
+    memset(s, 0, sizeof(*s));
+}
+
+/* Largest |entry| of the parity-mixing blocks of P, P^-1 S^-1 and A that
+ * the reference's even/odd split drops, relative to the largest entry.    */
+double orc_shen_parity_leak(const orc_shen *s)
+{
+    const int n = s->m - 2, m = s->m;
+    double leak = 0.0, big = 0.0;
+    /* Dirichlet pairs even rows with even (0-based) eigen-columns; the
+     * Neumann split pairs even rows with odd columns (src/preshen.f90:
+     * 203-287), except column 0 (the repaired constant mode).              */
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            const int same = ((i & 1) == (j & 1));
+            const int kept = (s->bound == 'd') ? same : (j == 0 ? (i == 0) : !same);
+            const double a = fmax(fabs(s->P[IX(i, j, n)]), fabs(s->PSM1[IX(j, i, n)]));
+            big = fmax(big, a);
+            if (!kept) leak = fmax(leak, a);
+        }
+    for (int j = 0; j < m; ++j)
+        for (int i = 0; i < m; ++i)
+            if (((i + j) & 1) && s->A[IX(i, j, m)] != 0.0) leak = fmax(leak, fabs(s->A[IX(i, j, m)]));
+    return leak / big;
+}
+
+/* DPTSV on a symmetric tridiagonal (d, e) of order k, right-hand side f.  */
+static void ptsv(int k, double *d, double *e, double *f)
+{
+    int one = 1, info = 0;
+    scipy_dptsv_(&k, &one, d, e, f, &k, &info);
+}
+
+/* solveshen, src/solveshen.f90:5-94 with chebleg2d, legshen2d,
+ * multevenodd, solV and solevenodd (src/legendre.f90:195-660,
+ * src/solveshen.f90:96-546).  The parity halves are kept together in full
+ * matrices (their coupling is round-off, orc_shen_parity_leak).           */
+int orc_solveshen(double *U, const orc_shen *s, double xlambda)
+{
+    const int m = s->m, n = m - 2;
+    const double *b = s->b;
+    double *G = (double *)calloc((size_t)m * m, sizeof(double));
+    double *T = (double *)calloc((size_t)m * m, sizeof(double));
+    double *F = (double *)calloc((size_t)n * n, sizeof(double));
+    double *W = (double *)calloc((size_t)n * n, sizeof(double));
+    const double one = 1.0, zero = 0.0;
+    /* chebleg2d(+1): G = A U A^T */
+    scipy_dgemm_("n", "n", &m, &m, &m, &one, s->A, &m, U, &m, &zero, T, &m, 1, 1);
+    scipy_dgemm_("n", "t", &m, &m, &m, &one, T, &m, s->A, &m, &zero, G, &m, 1, 1);
+    /* legshen2d(+1): leg2shen_sweep2d (src/legendre.f90:562-589) */
+    for (int jj = 0; jj < n; ++jj) {
+        const double ta = 2.0 / (double)(2 * jj + 1), tb = 2.0 * b[jj] / (double)(2 * jj + 5);
+        for (int ii = 0; ii < n; ++ii) {
+            const double tc = 2.0 / (double)(2 * ii + 1), td = 2.0 * b[ii] / (double)(2 * ii + 5);
+            F[IX(ii, jj, n)] = ta * (G[IX(ii, jj, m)] * tc + G[IX(ii + 2, jj, m)] * td) +
+                               tb * (G[IX(ii, jj + 2, m)] * tc + G[IX(ii + 2, jj + 2, m)] * td);
+        }
+    }
+    /* multevenodd(+1): W = P^-1 S^-1 F along y */
+    scipy_dgemm_("n", "n", &n, &n, &n, &one, s->PSM1, &n, F, &n, &zero, W, &n, 1, 1);
+    /* solV: per y-eigen-index ip, two SPD tridiagonal systems along z */
+    const int me = (n + 1) / 2, mo = n / 2;
+    double *de = (double *)malloc(sizeof(double) * (size_t)me), *ee = (double *)malloc(sizeof(double) * (size_t)me);
+    double *dd = (double *)malloc(sizeof(double) * (size_t)mo), *eo = (double *)malloc(sizeof(double) * (size_t)mo);
+    double *fe = (double *)malloc(sizeof(double) * (size_t)me), *fo = (double *)malloc(sizeof(double) * (size_t)mo);
+    const double *Md = s->M;
+    for (int ip = 0; ip < n; ++ip) {
+        const int neu_first = (s->bound == 'n' && ip == 0);
+        const double rho = neu_first ? 0.0 : s->E[ip];
+        const double ra1 = neu_first ? xlambda : rho * xlambda + 1.0;
+        /* solV uses makeMS's stiffness -b_k (4k+6) (src/preshen.f90:375-379),
+         * i.e. 0 for the Neumann constant mode, not precomeigen's S~ = 2.
+         * Dirichlet and Neumann ip>1: rho (alpha M + S) + M;
+         * Neumann ip=1: alpha M + S (src/solveshen.f90:410-421).           */
+        for (int q = 0; q < me; ++q) {
+            const int k = 2 * q;
+            const double Mk = Md[IX(k, k, n)], Sk = -b[k] * (double)(4 * k + 6);
+            de[q] = neu_first ? (xlambda * Mk + Sk) : (rho * (xlambda * Mk + Sk) + Mk);
+            if (q < me - 1) ee[q] = ra1 * Md[IX(k, k + 2, n)];
+            fe[q] = W[IX(ip, k, n)];
+        }
+        for (int q = 0; q < mo; ++q) {
+            const int k = 2 * q + 1;
+            const double Mk = Md[IX(k, k, n)], Sk = -b[k] * (double)(4 * k + 6);
+            dd[q] = neu_first ? (xlambda * Mk + Sk) : (rho * (xlambda * Mk + Sk) + Mk);
+            if (q < mo - 1) eo[q] = ra1 * Md[IX(k, k + 2, n)];
+            fo[q] = W[IX(ip, k, n)];
+        }
+        if (neu_first && xlambda < 1.0e-10) {            /* the intended pin :424-432 */
+            de[0] = 1.0;
+            fe[0] = 0.0;
+        }
+        ptsv(me, de, ee, fe);
+        ptsv(mo, dd, eo, fo);
+        for (int q = 0; q < me; ++q) W[IX(ip, 2 * q, n)] = fe[q];
+        for (int q = 0; q < mo; ++q) W[IX(ip, 2 * q + 1, n)] = fo[q];
+    }
+    free(de); free(ee); free(dd); free(eo); free(fe); free(fo);
+    /* multevenodd(-1): F = P W along y */
+    scipy_dgemm_("n", "n", &n, &n, &n, &one, s->P, &n, W, &n, &zero, F, &n, 1, 1);
+    /* legshen2d(-1): shen2leg_sweep2d (src/legendre.f90:627-660) */
+    for (int jj = 0; jj < m; ++jj)
+        for (int ii = 0; ii < m; ++ii) {
+            const double bi = ii >= 2 ? b[ii - 2] : 0.0, bj = jj >= 2 ? b[jj - 2] : 0.0;
+            const double s00 = (ii < n && jj < n) ? F[IX(ii, jj, n)] : 0.0;
+            const double s10 = (ii >= 2 && jj < n) ? F[IX(ii - 2, jj, n)] : 0.0;
+            const double s01 = (ii < n && jj >= 2) ? F[IX(ii, jj - 2, n)] : 0.0;
+            const double s11 = (ii >= 2 && jj >= 2) ? F[IX(ii - 2, jj - 2, n)] : 0.0;
+            G[IX(ii, jj, m)] = s00 + s01 * bj + s10 * bi + bi * bj * s11;
+        }
+    /* chebleg2d(-1): U = B G B^T */
+    scipy_dgemm_("n", "n", &m, &m, &m, &one, s->B, &m, G, &m, &zero, T, &m, 1, 1);
+    scipy_dgemm_("n", "t", &m, &m, &m, &one, T, &m, s->B, &m, &zero, U, &m, 1, 1);
+    free(G); free(T); free(F); free(W);
+    return 0;
+}
+
+/* helm3d_shen, src/helm_shen.f90:2-85: rhs -> Chebyshev coefficients in
+ * place (transyz y and z, iopt -1), int2d3d per mode (the real and the
+ * imaginary part each through solveshen; mode 0 real), solution back to
+ * physical space (transyz y and z, iopt +1).                              */
+int orc_helm3d_shen(double *rhs, double *sol, int my, int mz, int ib, int ie,
+                    const double *xalp, double alambda, const orc_shen *s, int nthreads)
+{
+    if (my != mz || my != s->m) return -2;
+    const int nmodes = ie - ib + 1;
+    const size_t plane = (size_t)my * mz;
+    orc_transyz(rhs, my, mz, nmodes, 'y', -1);
+    orc_transyz(rhs, my, mz, nmodes, 'z', -1);
+    if (nthreads < 1) nthreads = 1;
+#pragma omp parallel num_threads(nthreads)
+    {
+        double *U = (double *)malloc(sizeof(double) * plane);
+#pragma omp for schedule(dynamic, 1)
+        for (int i = 0; i < nmodes; ++i) {
+            const double xl = alambda + xalp[i] * xalp[i];
+            const double *r = rhs + 2 * plane * (size_t)i;
+            double *so = sol + 2 * plane * (size_t)i;
+            for (size_t p = 0; p < plane; ++p) U[p] = r[2 * p];
+            orc_solveshen(U, s, xl);
+            for (size_t p = 0; p < plane; ++p) { so[2 * p] = U[p]; so[2 * p + 1] = 0.0; }
+            if (ib + i == 0) continue;
+            for (size_t p = 0; p < plane; ++p) U[p] = r[2 * p + 1];
+            orc_solveshen(U, s, xl);
+            for (size_t p = 0; p < plane; ++p) so[2 * p + 1] += U[p];
+        }
+        free(U);
+    }
+    orc_transyz(sol, my, mz, nmodes, 'y', 1);
+    orc_transyz(sol, my, mz, nmodes, 'z', 1);
     return 0;
 }

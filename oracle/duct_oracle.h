@@ -128,6 +128,30 @@ int orc_helm3d_temp(const double *rhs, double *sol, int my, int mz, int ib, int 
                     const double *xalp, double alambda, const orc_dir *y, const orc_dir *z,
                     const double *bcy, const double *bcz, int nthreads);
 
+/* ---- Shen-Legendre Galerkin solver (HELM_SHEN build) ------------------ */
+/* preshen(bound) + makeMS + precomeigen (src/preshen.f90:2-535) and
+ * leg_cheb_mat (src/legendre.f90:3-110) for m (odd) points, n = m-2:
+ * b[m] basis coefficients, M, S [n*n] mass and stiffness (precomeigen),
+ * E[n], P[n*n] generalized eigen-pairs of M x = E S x, PSM1 = P^-1 S^-1,
+ * A [m*m] Chebyshev -> Legendre, B = A^-1.                                 */
+typedef struct {
+    int m;
+    char bound;
+    double *b, *M, *S, *E, *P, *PSM1, *A, *B;
+} orc_shen;
+
+int    orc_shen_setup(int m, char bound, orc_shen *s);
+void   orc_shen_free(orc_shen *s);
+/* largest parity-mixing entry the reference's even/odd split drops, relative */
+double orc_shen_parity_leak(const orc_shen *s);
+/* solveshen on one real (m,m) plane of Chebyshev coefficients, in place
+ * (src/solveshen.f90:5-94 with src/legendre.f90:195-660, :96-546).       */
+int    orc_solveshen(double *U, const orc_shen *s, double xlambda);
+/* helm3d_shen over modes ib..ie (src/helm_shen.f90:2-85): rhs (physical)
+ * is transformed to Chebyshev coefficients in place, like the reference. */
+int    orc_helm3d_shen(double *rhs, double *sol, int my, int mz, int ib, int ie,
+                       const double *xalp, double alambda, const orc_shen *s, int nthreads);
+
 void orc_set_blas_threads(int n);
 
 #ifdef __cplusplus

@@ -26,6 +26,11 @@ class _Dir(C.Structure):
         (n, C.POINTER(C.c_double)) for n in ("D", "D2", "E", "P", "PM1", "B")]
 
 
+class _Shen(C.Structure):
+    _fields_ = [("m", C.c_int), ("bound", C.c_char)] + [
+        (n, C.POINTER(C.c_double)) for n in ("b", "M", "S", "E", "P", "PSM1", "A", "B")]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -52,6 +57,13 @@ def lib():
         L.orc_solvediag_temp.argtypes = [P, C.POINTER(_Dir), C.POINTER(_Dir), C.c_double, P, P, C.c_int]
         L.orc_helm3d_temp.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_double,
                                       C.POINTER(_Dir), C.POINTER(_Dir), P, P, C.c_int]
+        L.orc_shen_setup.argtypes = [C.c_int, C.c_char, C.POINTER(_Shen)]
+        L.orc_shen_free.argtypes = [C.POINTER(_Shen)]
+        L.orc_shen_parity_leak.argtypes = [C.POINTER(_Shen)]
+        L.orc_shen_parity_leak.restype = C.c_double
+        L.orc_solveshen.argtypes = [P, C.POINTER(_Shen), C.c_double]
+        L.orc_helm3d_shen.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_double,
+                                      C.POINTER(_Shen), C.c_int]
         _lib = L
     return _lib
 
@@ -120,6 +132,56 @@ class Dir:
             lib().orc_dir_free(C.byref(self._s))
         except Exception:
             pass
+
+
+class Shen:
+    """preshen(bound) + leg_cheb_mat for m (odd) points (src/preshen.f90)."""
+
+    def __init__(self, m, bound):
+        self._s = _Shen()
+        info = lib().orc_shen_setup(int(m), bound.encode(), C.byref(self._s))
+        if info != 0:
+            raise RuntimeError("orc_shen_setup failed, info=%d" % info)
+        self.m, self.bound = m, bound
+        n = m - 2
+
+        def v(ptr, *shape):
+            return np.ctypeslib.as_array(ptr, shape=(int(np.prod(shape)),)).reshape(
+                shape, order="F").copy(order="F")
+        self.b = v(self._s.b, m)
+        self.M, self.S = v(self._s.M, n, n), v(self._s.S, n, n)
+        self.E, self.P, self.PSM1 = v(self._s.E, n), v(self._s.P, n, n), v(self._s.PSM1, n, n)
+        self.A, self.B = v(self._s.A, m, m), v(self._s.B, m, m)
+
+    def parity_leak(self):
+        return lib().orc_shen_parity_leak(C.byref(self._s))
+
+    def __del__(self):
+        try:
+            lib().orc_shen_free(C.byref(self._s))
+        except Exception:
+            pass
+
+
+def solveshen(U, shen, xlambda):
+    """solveshen on one real (m,m) plane of Chebyshev coefficients."""
+    U = np.array(U, dtype=np.float64, order="F")
+    lib().orc_solveshen(_p(U), C.byref(shen._s), float(xlambda))
+    return U
+
+
+def helm3d_shen(rhs, shen, alambda, xalp, ib=0, nthreads=1):
+    """helm3d_shen on a complex (my,mz,nmodes) field: returns (sol, rhs_after)
+    (rhs is transformed to Chebyshev space in place by the reference)."""
+    rhs = np.array(rhs, dtype=np.complex128, order="F")
+    my, mz, nm = rhs.shape
+    sol = np.zeros_like(rhs, order="F")
+    xalp = np.ascontiguousarray(xalp, dtype=np.float64)
+    rc = lib().orc_helm3d_shen(_p(rhs), _p(sol), my, mz, ib, ib + nm - 1, _p(xalp), float(alambda),
+                               C.byref(shen._s), int(nthreads))
+    if rc:
+        raise ValueError("orc_helm3d_shen: grid %dx%d does not match the set-up %d" % (my, mz, shen.m))
+    return sol, rhs
 
 
 def helm3d_temp(rhs, ydir, zdir, alambda, xalp, ib=0, bcy=None, bcz=None, nthreads=1):
@@ -210,6 +272,6 @@ def set_blas_threads(n):
     lib().orc_set_blas_threads(int(n))
 
 
-__all__ = ["Ops", "Dir", "helm3d_temp", "solvediag", "helm3d", "transyz", "transyz_plane", "derivyz",
+__all__ = ["Ops", "Dir", "Shen", "solveshen", "helm3d_shen", "helm3d_temp", "solvediag", "helm3d", "transyz", "transyz_plane", "derivyz",
            "cheb2_integral", "cxyz2yzx", "cyzx2xyz", "set_blas_threads", "lib"]
 _ = os
