@@ -32,6 +32,7 @@ EXPORTS = [
     "ductgpu_solve_rect_fields_dev", "ductgpu_graph_create", "ductgpu_graph_launch",
     "ductgpu_graph_destroy", "transpose_gpu_", "mat_invdiag_gpu_",
     "ductgpu_preshen", "ductgpu_helm3d_shen", "ductgpu_solve_shen_fields_dev",
+    "ductgpu_solve_fields_dev_noalloc",
 ]
 K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
 
@@ -102,6 +103,7 @@ def lib():
             "ductgpu_preshen": [P, I, C.c_char],
             "ductgpu_helm3d_shen": [P, P, P, I, C.c_char, D, I, I, I, I, P],
             "ductgpu_solve_shen_fields_dev": [P, C.POINTER(Field), I],
+            "ductgpu_solve_fields_dev_noalloc": [P, C.POINTER(Field), I],
             "ductgpu_graph_launch": [P, I],
             "ductgpu_graph_destroy": [P, I],
             "transpose_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),

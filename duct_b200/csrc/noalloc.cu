@@ -1,0 +1,106 @@
+// noalloc.cu -- ductgpu_solve_fields_dev_noalloc: the batched FP64 solve of
+// ductgpu_solve_fields_dev for callers that must not allocate device
+// memory.  Some host codes reserve the whole device up front with their
+// own pool allocator and have nothing left for a library's cudaMalloc;
+// others drive several streams at once and cannot afford cudaFree, which
+// waits for the whole device.  This entry point keeps its scratch (the two
+// intermediate fields of the four GEMM passes and the per-plane lambda)
+// in a fixed array that lives in this file, so it calls no cudaMalloc,
+// cudaFree or other allocating routine.
+//
+// Limits and rules for callers:
+//  * scratch is kScratchBytes (32 MiB) per GPU, held by every GPU that
+//    loads this library until the process exits; a call needs
+//    2 * planes * 2 * my * my doubles of it (planes = sum of nmodes) and at
+//    most kLamSlots planes -- larger calls are rejected with DUCTGPU_EARG;
+//  * the array is shared by every call on a GPU and keeps the last call's
+//    contents; calls whose work overlaps on one GPU (two contexts, or two
+//    streams) race on it and give wrong results -- serialise them;
+//  * nothing in it needs to start at zero: each call writes every scratch
+//    element (lambda copy, intermediate interiors) before reading it;
+//  * the first call on a GPU takes the array's device address with
+//    cudaGetSymbolAddress (which also loads this file's device code there);
+//    make that first call before any stream capture on that GPU.
+#include <mutex>
+
+#include "internal.h"
+
+static constexpr size_t kScratchBytes = 32u << 20;
+static constexpr size_t kScratchDoubles = kScratchBytes / sizeof(double);
+static constexpr int kLamSlots = 4096;        // planes per call (lambda slots)
+static constexpr int kMaxDevices = 64;
+
+// The scratch itself.  In host code this name is only a stand-in for the
+// device array: kernels get the address from cudaGetSymbolAddress.  No
+// device code here names it, so it is marked used to stay in the image.
+static __device__ __align__(256) __attribute__((used)) double g_scratch[kScratchDoubles];
+
+namespace {
+
+// Per-device address of g_scratch, filled once per device.
+double *g_scratch_dev[kMaxDevices] = {};
+std::mutex g_setup_mutex;
+// Host staging of the per-plane lambda (a plain array: no host allocation
+// either); shared like the device array.
+double g_lam_host[kMaxDevices][kLamSlots];
+
+int scratch_for_device(ductgpu_ctx ctx, double **out)
+{
+    if (ctx->device < 0 || ctx->device >= kMaxDevices)
+        return duct::set_error(ctx, DUCTGPU_EARG, "noalloc: device %d beyond %d", ctx->device, kMaxDevices);
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (!g_scratch_dev[ctx->device]) {
+        cudaError_t e = cudaSetDevice(ctx->device);
+        if (e != cudaSuccess) return duct::check_cuda(ctx, e, "noalloc: cudaSetDevice");
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_scratch);
+        if (e != cudaSuccess) return duct::check_cuda(ctx, e, "noalloc: cudaGetSymbolAddress");
+        g_scratch_dev[ctx->device] = static_cast<double *>(p);
+    }
+    *out = g_scratch_dev[ctx->device];
+    return DUCTGPU_OK;
+}
+
+}  // namespace
+
+extern "C" int ductgpu_solve_fields_dev_noalloc(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (!ctx->ready) return duct::set_error(ctx, DUCTGPU_ESTATE, "operators not set up (call ductgpu_pseudomat)");
+    if (!fields || nfields < 1 || nfields > duct::kMaxFields)
+        return duct::set_error(ctx, DUCTGPU_EARG, "nfields=%d (1..%d)", nfields, duct::kMaxFields);
+    long long planes = 0;
+    for (int i = 0; i < nfields; ++i) {
+        if (fields[i].nmodes < 1) return duct::set_error(ctx, DUCTGPU_EARG, "nmodes=%d", fields[i].nmodes);
+        planes += fields[i].nmodes;
+    }
+    const size_t ps = 2ull * ctx->my * ctx->my;   // doubles per complex plane
+    const size_t work_doubles = kScratchDoubles - kLamSlots;
+    if (planes > kLamSlots || 2ull * (size_t)planes * ps > work_doubles)
+        return duct::set_error(ctx, DUCTGPU_EARG,
+                               "noalloc: %lld planes of %dx%d need %.1f MiB of scratch; the fixed scratch "
+                               "holds %.1f MiB and %d planes (use ductgpu_solve_fields_dev)",
+                               planes, ctx->my, ctx->my, 2.0 * planes * ps * 8.0 / (1 << 20),
+                               work_doubles * 8.0 / (1 << 20), kLamSlots);
+    double *scratch = nullptr;
+    int rc = scratch_for_device(ctx, &scratch);
+    if (rc) return rc;
+
+    // Run the ordinary batched solve with the context's workspace, lambda
+    // array and its staging pointed at the fixed scratch; sized as above,
+    // nothing in that path needs to grow them, so it allocates nothing.
+    const duct::Workspace work_saved = ctx->work;
+    double *const lam_saved = ctx->lam, *const lam_host_saved = ctx->lam_host;
+    const int lam_cap_saved = ctx->lam_cap;
+    ctx->lam = scratch;                                   // [kLamSlots], 256-byte aligned
+    ctx->lam_host = g_lam_host[ctx->device];
+    ctx->lam_cap = kLamSlots;
+    ctx->work.buf = scratch + kLamSlots;                  // 32 KB in: still 256-byte aligned
+    ctx->work.bytes = work_doubles * sizeof(double);
+    rc = ductgpu_solve_fields_dev(ctx, fields, nfields, DUCTGPU_PREC_FP64);
+    ctx->work = work_saved;
+    ctx->lam = lam_saved;
+    ctx->lam_host = lam_host_saved;
+    ctx->lam_cap = lam_cap_saved;
+    return rc;
+}

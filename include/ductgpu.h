@@ -118,6 +118,21 @@ typedef struct {
 int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields,
                              int nfields, int precision);
 
+/* No counterpart in the reference.  ductgpu_solve_fields_dev (FP64) for
+ * callers that cannot allocate device memory -- a host code whose own pool
+ * allocator has reserved the device, or one that runs several streams and
+ * cannot let cudaFree wait for the whole device.  It allocates nothing: its
+ * scratch is a fixed 32 MiB array per GPU inside the library (held until
+ * the process exits).  A call may hold at most 4096 planes (sum of nmodes)
+ * and needs 2 * planes * 2 * my * my doubles of that scratch (my = 129: 62
+ * planes); larger calls return DUCTGPU_EARG.  The array is shared by all
+ * calls on a GPU: calls that overlap on one GPU race on it -- serialise
+ * them.  Nothing in it needs clearing first.  The first call on a GPU looks
+ * up the array's address (cudaGetSymbolAddress); make it before any stream
+ * capture there.  Operators must be set up (ductgpu_pseudomat) beforehand. */
+int ductgpu_solve_fields_dev_noalloc(ductgpu_ctx ctx, const ductgpu_field *fields,
+                                     int nfields);
+
 /* ---- rectangular ducts, general wall conditions (temperature path) ---- */
 /* pseudomaty_temp + pseudomatz_temp (src/pseudomat_temp.f90:2-320) on the
  * GPU for operator slot `slot` (0..7, one per duct shape): my x mz points on

@@ -1,0 +1,91 @@
+"""ductgpu_solve_fields_dev_noalloc through the C-ABI.
+
+That entry point serves callers that cannot allocate device memory (their
+own pool allocator holds the device, or cudaFree's device-wide wait would
+stall their other streams): it runs the FP64 batched solve with its scratch
+in a fixed array inside the library.  Its results must equal those of
+ductgpu_solve_fields_dev, on consecutive calls that reuse that shared
+scratch, and calls too large for the scratch must be refused.
+
+This file is named to run last, and it creates its own context, so it
+passes alone in a fresh process and after the rest of the suite."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import duct_b200 as D
+from duct_b200 import synth
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12   # the FP64 tolerance of the other solve tests
+
+
+def rel(a, b):
+    return np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel())
+
+
+def noalloc(ctx, fields):
+    L = D.lib()
+    fn = L.ductgpu_solve_fields_dev_noalloc
+    fn.argtypes = [C.c_void_p, C.POINTER(D.Field), C.c_int]
+    fn.restype = C.c_int
+    arr, keep = ctx._field_array(fields, False)
+    return fn(ctx.h, arr, len(fields)), keep
+
+
+def specs(m, nm, seed):
+    """u, v, w (Dirichlet) and p (Neumann, with the singular kx=0 mode) of one
+    substep; seeded rhs per field."""
+    xalp = 0.5 * np.arange(nm)
+    out = []
+    for k, (bound, lam) in enumerate([("d", 4.0e3), ("d", 4.0e3), ("d", 4.0e3), ("n", 0.0)]):
+        out.append((bound, lam, xalp, synth.chebyshev_rhs(m, m, nm, seed=seed + k, ib=0)))
+    return out
+
+
+def run(ctx, entry, spec):
+    fields, dev = [], []
+    for bound, lam, xalp, f in spec:
+        r, s = ctx.device_array(f.shape), ctx.device_array(f.shape)
+        r.upload(f)
+        s.upload(np.full(f.shape, np.nan + 1j * np.nan, order="F"))   # nothing stale can pass
+        dev.append((r, s))
+        fields.append(dict(rhs=r, sol=s, xalp=xalp, alambda=lam, ib=0, bound=bound))
+    if entry == "noalloc":
+        rc, _ = noalloc(ctx, fields)
+        assert rc == D.OK, ctx.last_error()
+    else:
+        ctx.solve_fields_dev(fields, precision=D.PREC_FP64)
+    ctx.synchronize()
+    out = [s.download() for r, s in dev]
+    for r, s in dev:
+        r.free()
+        s.free()
+    return out
+
+
+def test_noalloc_matches_solve_fields_dev_twice():
+    m, nm = 65, 8
+    with D.Context(0) as ctx:
+        ctx.pseudomat(m, m)
+        first, second = specs(m, nm, seed=11), specs(m, nm, seed=29)
+        ref1, ref2 = run(ctx, "plain", first), run(ctx, "plain", second)
+        got1 = run(ctx, "noalloc", first)     # first call: sets up the scratch
+        got2 = run(ctx, "noalloc", second)    # second call: reuses it
+        for got, ref in zip(got1 + got2, ref1 + ref2):
+            assert np.all(np.isfinite(got))
+            assert rel(got, ref) < TOL
+        assert np.all(got1[0][:, :, 0].imag == 0)
+
+
+def test_noalloc_rejects_calls_beyond_the_scratch():
+    m = 129
+    with D.Context(0) as ctx:
+        ctx.pseudomat(m, m)
+        f = ctx.device_array((m, m, 63))       # 63 planes of 129^2: just too many
+        fields = [dict(rhs=f, sol=f, xalp=np.zeros(63), alambda=1.0, ib=0, bound="d")]
+        rc, _ = noalloc(ctx, fields)
+        assert rc == D.EARG
+        assert "scratch" in ctx.last_error()
+        f.free()
