@@ -32,7 +32,8 @@ EXPORTS = [
     "ductgpu_solve_rect_fields_dev", "ductgpu_graph_create", "ductgpu_graph_launch",
     "ductgpu_graph_destroy", "transpose_gpu_", "mat_invdiag_gpu_",
     "ductgpu_preshen", "ductgpu_helm3d_shen", "ductgpu_solve_shen_fields_dev",
-    "ductgpu_solve_fields_dev_noalloc",
+    "ductgpu_solve_fields_dev_noalloc", "ductgpu_precomp_mass_flow",
+    "ductgpu_impose_mass_flow_dev", "ductgpu_impose_mass_flow",
 ]
 K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
 
@@ -104,6 +105,9 @@ def lib():
             "ductgpu_helm3d_shen": [P, P, P, I, C.c_char, D, I, I, I, I, P],
             "ductgpu_solve_shen_fields_dev": [P, C.POINTER(Field), I],
             "ductgpu_solve_fields_dev_noalloc": [P, C.POINTER(Field), I],
+            "ductgpu_precomp_mass_flow": [P, D, P, I, D, D, P, P],
+            "ductgpu_impose_mass_flow_dev": [P, C.POINTER(D), I, P, I],
+            "ductgpu_impose_mass_flow": [P, C.POINTER(D), I, P, I],
             "ductgpu_graph_launch": [P, I],
             "ductgpu_graph_destroy": [P, I],
             "transpose_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
@@ -200,6 +204,7 @@ class Context:
 
     def pseudomat(self, my, mz=None):
         self._check(lib().ductgpu_pseudomat(self.h, int(my), int(mz if mz is not None else my)))
+        self._my = int(my)
 
     def get_operators(self, bound, n):
         E = np.empty(n)
@@ -256,6 +261,31 @@ class Context:
         arr, keep = self._field_array(fields, False)
         self._check(lib().ductgpu_solve_shen_fields_dev(self.h, arr, len(fields)))
         return keep
+
+    def precomp_mass_flow(self, dtp, alphak, fnu, aspect=1.0):
+        """precomp_mass_flow; returns (premassfu (my,my,mrk), premassf)."""
+        alphak = np.ascontiguousarray(alphak, dtype=np.float64)
+        mrk = alphak.shape[0]
+        m = self._my
+        pf = np.zeros(mrk)
+        pu = np.zeros((m, m, mrk), order="F")
+        self._check(lib().ductgpu_precomp_mass_flow(self.h, float(dtp), _ptr(alphak), mrk, float(fnu),
+                                                    float(aspect), _ptr(pf), _ptr(pu)))
+        return pu, pf
+
+    def impose_mass_flow(self, u, csum, krk, iflag):
+        """impose_mass_flow on a host complex (my,my,...) field, modified in
+        place for iflag 1; returns csum (the measured flow for iflag 0)."""
+        assert u.dtype == np.complex128 and u.flags.f_contiguous
+        cs = C.c_double(float(csum))
+        self._check(lib().ductgpu_impose_mass_flow(self.h, C.byref(cs), int(krk), _ptr(u), int(iflag)))
+        return cs.value
+
+    def impose_mass_flow_dev(self, u, csum, krk, iflag):
+        cs = C.c_double(float(csum))
+        self._check(lib().ductgpu_impose_mass_flow_dev(self.h, C.byref(cs), int(krk), C.c_void_p(u.ptr),
+                                                       int(iflag)))
+        return cs.value
 
     def pseudomat_temp(self, slot, my, mz, sy=1.0, sz=1.0, by=("d", "d"), bz=("d", "d")):
         self._check(lib().ductgpu_pseudomat_temp(self.h, int(slot), int(my), int(mz), float(sy), float(sz),

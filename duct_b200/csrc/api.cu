@@ -194,6 +194,9 @@ int ductgpu_destroy(ductgpu_ctx ctx)
     for (int i = 0; i < kMaxRect; ++i) free_rect(ctx->rect[i]);
     free_shen(ctx->shen_d);
     free_shen(ctx->shen_n);
+    cudaFree(ctx->mf_u);
+    cudaFree(ctx->mf_f);
+    cudaFree(ctx->mf_sum);
     for (int i = 0; i < ductgpu_ctx_s::kMaxGraphs; ++i)
         if (ctx->graph_exec[i]) { cudaGraphExecDestroy(ctx->graph_exec[i]); cudaFree(ctx->graph_lam[i]); }
     cudaFree(ctx->xcol); cudaFree(ctx->DC); cudaFree(ctx->D2); cudaFree(ctx->AM1); cudaFree(ctx->ccw);

@@ -93,6 +93,11 @@ struct ductgpu_ctx_s {
 
     duct::RectSlot rect[duct::kMaxRect];
     duct::ShenOps shen_d, shen_n;
+    // constant mass-flow-rate forcing (precomp_mass_flow): premassfu
+    // (my,my,mf_mrk) real, premassf[mf_mrk], the last measured flow rate
+    double *mf_u = nullptr, *mf_f = nullptr, *mf_sum = nullptr;
+    int mf_mrk = 0, mf_my = 0;
+    double mf_aspect = 1.0;
     // captured solves (CUDA graphs), each with its own lambda array
     static constexpr int kMaxGraphs = 16;
     cudaGraphExec_t graph_exec[kMaxGraphs] = {};

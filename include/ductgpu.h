@@ -190,6 +190,24 @@ int ductgpu_helm3d_shen(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, cha
  * operators; all fields share my (= mz).  rhs is overwritten as above.    */
 int ductgpu_solve_shen_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields);
 
+/* ---- constant mass-flow-rate forcing ---------------------------------- */
+/* precomp_mass_flow(dtp,alphak,work,nwk), src/operators.F:2205-2289 (square
+ * build; needs ductgpu_pseudomat): for RK index k = 1..mrk solves
+ * (dyy+dzz)u - u/(alphak[k-1] dtp fnu) = 1 with zero walls and keeps the
+ * solution premassfu(:,:,k) and its flow rate premassf[k-1] (integral over
+ * the cross-section times aspect) in the context.  premassf (mrk) and
+ * premassfu (my*my*mrk, real) are optional host outputs (NULL: skipped).  */
+int ductgpu_precomp_mass_flow(ductgpu_ctx ctx, double dtp, const double *alphak, int mrk,
+                              double fnu, double aspect, double *premassf, double *premassfu);
+/* impose_mass_flow(csum,krk,u,work,nwk,iflag), src/operators.F:2291-2344, on
+ * the first (mode 0) plane of the device field u (complex (my,my,...)):
+ * iflag 0 stores its flow rate in *csum (synchronises); iflag 1 adds
+ * (*csum - flow)/premassf(krk) * premassfu(:,:,krk) to its real part
+ * (krk 1-based), asynchronously, in one kernel.                          */
+int ductgpu_impose_mass_flow_dev(ductgpu_ctx ctx, double *csum, int krk, double *u, int iflag);
+/* The same on a host field (only its mode 0 plane is copied).             */
+int ductgpu_impose_mass_flow(ductgpu_ctx ctx, double *csum, int krk, double *u, int iflag);
+
 /* ---- captured solves (CUDA graphs) ------------------------------------ */
 /* Capture one batched solve -- kind 0: `fields` is a ductgpu_field array
  * (square path, `precision` as in ductgpu_solve_fields_dev); kind 1: a

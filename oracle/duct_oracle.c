@@ -1067,3 +1067,55 @@ int orc_helm3d_shen(double *rhs, double *sol, int my, int mz, int ib, int ie,
     orc_transyz(sol, my, mz, nmodes, 'z', 1);
     return 0;
 }
+
+/* ---- constant mass-flow-rate forcing ----------------------------------- */
+/* precomp_mass_flow, src/operators.F:2205-2289 (square build): for each RK
+ * index krk, solve (dyy+dzz)u - u/(alphak dtp fnu) = 1 in the interior with
+ * zero walls (solvediag 'd'), store it in premassfu(:,krk) and its
+ * integral (transyz_plane -1, cheb2_integral) in premassf(krk).           */
+int orc_precomp_mass_flow(const orc_ops *o, double dtp, const double *alphak, int mrk,
+                          double fnu, double aspect, double *premassfu, double *premassf)
+{
+    const int m = o->m;
+    const size_t plane = (size_t)m * m;
+    double *w = (double *)malloc(sizeof(double) * plane);
+    for (int k = 0; k < mrk; ++k) {
+        const double flambda = -1.0 / (alphak[k] * dtp * fnu);
+        double *U = premassfu + plane * (size_t)k;
+        for (size_t p = 0; p < plane; ++p) U[p] = 1.0;
+        for (int i = 0; i < m; ++i) {
+            U[IX(i, 0, m)] = U[IX(i, m - 1, m)] = 0.0;
+            U[IX(0, i, m)] = U[IX(m - 1, i, m)] = 0.0;
+        }
+        int rc = orc_solvediag(U, o, 'd', -flambda);
+        if (rc) { free(w); return rc; }
+        memcpy(w, U, sizeof(double) * plane);
+        orc_transyz_plane(w, m, m, -1);
+        premassf[k] = orc_cheb2_integral(w, m, m, aspect);
+    }
+    free(w);
+    return 0;
+}
+
+/* impose_mass_flow, src/operators.F:2291-2344: the mass flow of the real
+ * part of mode 0 of u (complex (my,mz), first plane); iflag 0 returns it
+ * in *csum, iflag 1 adds fac premassfu(:,krk) (krk 1-based) with
+ * fac = (csum - sumg)/premassf(krk).  Returns sumg.                       */
+double orc_impose_mass_flow(double *csum, int krk, double *u, int my, int mz, double aspect,
+                            const double *premassfu, const double *premassf, int iflag)
+{
+    const size_t plane = (size_t)my * mz;
+    double *w = (double *)malloc(sizeof(double) * plane);
+    for (size_t p = 0; p < plane; ++p) w[p] = u[2 * p];
+    orc_transyz_plane(w, my, mz, -1);
+    const double sumg = orc_cheb2_integral(w, my, mz, aspect);
+    free(w);
+    if (iflag == 0) {
+        *csum = sumg;
+        return sumg;
+    }
+    const double fac = (*csum - sumg) / premassf[krk - 1];
+    const double *pu = premassfu + plane * (size_t)(krk - 1);
+    for (size_t p = 0; p < plane; ++p) u[2 * p] += fac * pu[p];
+    return sumg;
+}

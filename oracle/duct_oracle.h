@@ -152,6 +152,13 @@ int    orc_solveshen(double *U, const orc_shen *s, double xlambda);
 int    orc_helm3d_shen(double *rhs, double *sol, int my, int mz, int ib, int ie,
                        const double *xalp, double alambda, const orc_shen *s, int nthreads);
 
+/* precomp_mass_flow / impose_mass_flow, src/operators.F:2205-2344 (square
+ * build).  premassfu: (my,my,mrk) real, premassf: mrk.                     */
+int    orc_precomp_mass_flow(const orc_ops *o, double dtp, const double *alphak, int mrk,
+                             double fnu, double aspect, double *premassfu, double *premassf);
+double orc_impose_mass_flow(double *csum, int krk, double *u, int my, int mz, double aspect,
+                            const double *premassfu, const double *premassf, int iflag);
+
 void orc_set_blas_threads(int n);
 
 #ifdef __cplusplus

@@ -64,6 +64,10 @@ def lib():
         L.orc_solveshen.argtypes = [P, C.POINTER(_Shen), C.c_double]
         L.orc_helm3d_shen.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_double,
                                       C.POINTER(_Shen), C.c_int]
+        L.orc_precomp_mass_flow.argtypes = [C.POINTER(_Ops), C.c_double, P, C.c_int, C.c_double,
+                                            C.c_double, P, P]
+        L.orc_impose_mass_flow.argtypes = [P, C.c_int, P, C.c_int, C.c_int, C.c_double, P, P, C.c_int]
+        L.orc_impose_mass_flow.restype = C.c_double
         _lib = L
     return _lib
 
@@ -132,6 +136,33 @@ class Dir:
             lib().orc_dir_free(C.byref(self._s))
         except Exception:
             pass
+
+
+def precomp_mass_flow(ops, dtp, alphak, fnu, aspect=1.0):
+    """precomp_mass_flow (src/operators.F:2205-2289): returns (premassfu
+    (m,m,mrk), premassf (mrk,))."""
+    alphak = np.ascontiguousarray(alphak, dtype=np.float64)
+    m, mrk = ops.m, alphak.shape[0]
+    pu = np.zeros((m, m, mrk), order="F")
+    pf = np.zeros(mrk)
+    rc = lib().orc_precomp_mass_flow(C.byref(ops._s), float(dtp), _p(alphak), mrk, float(fnu),
+                                     float(aspect), _p(pu), _p(pf))
+    if rc:
+        raise RuntimeError("orc_precomp_mass_flow: %d" % rc)
+    return pu, pf
+
+
+def impose_mass_flow(u, csum, krk, premassfu, premassf, iflag, aspect=1.0):
+    """impose_mass_flow (src/operators.F:2291-2344) on a complex (my,mz,...)
+    field; returns (u_after, csum_after, sumg)."""
+    u = np.array(u, dtype=np.complex128, order="F")
+    my, mz = u.shape[:2]
+    cs = C.c_double(float(csum))
+    pu = np.asfortranarray(premassfu, dtype=np.float64)
+    pf = np.ascontiguousarray(premassf, dtype=np.float64)
+    sumg = lib().orc_impose_mass_flow(C.byref(cs), int(krk), _p(u), my, mz, float(aspect), _p(pu), _p(pf),
+                                      int(iflag))
+    return u, cs.value, sumg
 
 
 class Shen:
@@ -272,6 +303,6 @@ def set_blas_threads(n):
     lib().orc_set_blas_threads(int(n))
 
 
-__all__ = ["Ops", "Dir", "Shen", "solveshen", "helm3d_shen", "helm3d_temp", "solvediag", "helm3d", "transyz", "transyz_plane", "derivyz",
+__all__ = ["Ops", "Dir", "Shen", "precomp_mass_flow", "impose_mass_flow", "solveshen", "helm3d_shen", "helm3d_temp", "solvediag", "helm3d", "transyz", "transyz_plane", "derivyz",
            "cheb2_integral", "cxyz2yzx", "cyzx2xyz", "set_blas_threads", "lib"]
 _ = os
