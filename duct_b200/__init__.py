@@ -34,6 +34,7 @@ EXPORTS = [
     "ductgpu_preshen", "ductgpu_helm3d_shen", "ductgpu_solve_shen_fields_dev",
     "ductgpu_solve_fields_dev_noalloc", "ductgpu_precomp_mass_flow",
     "ductgpu_impose_mass_flow_dev", "ductgpu_impose_mass_flow",
+    "ductgpu_solve_adjoint_fields_dev", "ductgpu_helm3d_adjoint",
 ]
 K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
 
@@ -108,6 +109,8 @@ def lib():
             "ductgpu_precomp_mass_flow": [P, D, P, I, D, D, P, P],
             "ductgpu_impose_mass_flow_dev": [P, C.POINTER(D), I, P, I],
             "ductgpu_impose_mass_flow": [P, C.POINTER(D), I, P, I],
+            "ductgpu_solve_adjoint_fields_dev": [P, C.POINTER(Field), I],
+            "ductgpu_helm3d_adjoint": [P, P, P, C.c_char, D, I, I, I, I, P],
             "ductgpu_graph_launch": [P, I],
             "ductgpu_graph_destroy": [P, I],
             "transpose_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
@@ -239,6 +242,22 @@ class Context:
                                          float(alambda), my, mz, int(ib), int(ib) + nm - 1,
                                          _ptr(xalp), int(precision)))
         return sol
+
+    def helm3d_adjoint(self, gsol, bound, alambda, xalp, ib=0):
+        """Transpose of the helm3d map applied to the cotangent gsol (host,
+        complex (my,mz,nmodes)); returns grhs."""
+        gsol = np.asfortranarray(gsol, dtype=np.complex128)
+        my, mz, nm = gsol.shape
+        out = np.zeros_like(gsol, order="F")
+        xalp = np.ascontiguousarray(xalp, dtype=np.float64)
+        self._check(lib().ductgpu_helm3d_adjoint(self.h, _ptr(gsol), _ptr(out), bound.encode(), float(alambda),
+                                                 my, mz, int(ib), int(ib) + nm - 1, _ptr(xalp)))
+        return out
+
+    def solve_adjoint_fields_dev(self, fields):
+        arr, keep = self._field_array(fields, False)
+        self._check(lib().ductgpu_solve_adjoint_fields_dev(self.h, arr, len(fields)))
+        return keep
 
     def preshen(self, my, bound):
         self._check(lib().ductgpu_preshen(self.h, int(my), bound.encode()))

@@ -602,6 +602,54 @@ int ductgpu_helm3d_temp(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, dou
     return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d_temp");
 }
 
+int ductgpu_solve_adjoint_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (!ctx->ready) return set_error(ctx, DUCTGPU_ESTATE, "operators not set up (call ductgpu_pseudomat)");
+    if (!fields || nfields < 1 || nfields > kMaxFields)
+        return set_error(ctx, DUCTGPU_EARG, "nfields=%d (1..%d)", nfields, kMaxFields);
+    for (int i = 0; i < nfields; ++i) {
+        int rc = validate_field(ctx, fields[i]);
+        if (rc) return rc;
+        if (fields[i].rhs == fields[i].sol)
+            return set_error(ctx, DUCTGPU_EARG, "adjoint: input and output of field %d must differ", i);
+    }
+    cudaSetDevice(ctx->device);
+    FieldTask tasks[kMaxFields];
+    int rc = prepare(ctx, fields, nfields, tasks);
+    if (rc) return rc;
+    return solve_adjoint(ctx, tasks, nfields);
+}
+
+int ductgpu_helm3d_adjoint(ductgpu_ctx ctx, const double *gsol, double *grhs, char bound, double alambda, int my,
+                           int mz, int ib, int ie, const double *xalp)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (!ctx->ready) return set_error(ctx, DUCTGPU_ESTATE, "operators not set up (call ductgpu_pseudomat)");
+    if (my != ctx->my || mz != ctx->mz)
+        return set_error(ctx, DUCTGPU_EARG, "grid %dx%d differs from the set-up %dx%d", my, mz, ctx->my, ctx->mz);
+    if (!gsol || !grhs || !xalp) return set_error(ctx, DUCTGPU_EARG, "null pointer");
+    if (ie < ib || ib < 0) return set_error(ctx, DUCTGPU_EARG, "ib=%d ie=%d", ib, ie);
+    cudaSetDevice(ctx->device);
+    const int nm = ie - ib + 1;
+    const size_t bytes = (size_t)2 * my * mz * nm * sizeof(double);
+    int rc = ensure(ctx, ctx->io, 2 * bytes);
+    if (rc) return rc;
+    double *dg = ctx->io.buf, *dout = ctx->io.buf + bytes / sizeof(double);
+    DUCT_CUDA(ctx, cudaMemcpyAsync(dg, gsol, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    ductgpu_field f;
+    f.rhs = dg;
+    f.sol = dout;
+    f.xalp = xalp;
+    f.alambda = alambda;
+    f.ib = ib;
+    f.nmodes = nm;
+    f.bound = bound;
+    if ((rc = ductgpu_solve_adjoint_fields_dev(ctx, &f, 1))) return rc;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(grhs, dout, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d_adjoint");
+}
+
 int ductgpu_preshen(ductgpu_ctx ctx, int my, char bound)
 {
     if (!ctx) return DUCTGPU_EARG;

@@ -36,6 +36,7 @@ struct BoundOps {
     double emin = 0.0, emax = 0.0;   // smallest / largest |eigenvalue| (host)
     double *D2B = nullptr;     // [n*n] the interior operator block itself
     double *Bpack = nullptr;   // D2B in DMMA A-fragment order (residual)
+    double *PTpack = nullptr, *QTpack = nullptr;  // P^T, P^-T packed (adjoint; built on first use)
     uint8_t *Pslices = nullptr, *Qslices = nullptr;  // BF16 slices (mixed)
     int *Pexp = nullptr, *Qexp = nullptr;            // per-row exponents
 };
@@ -142,6 +143,7 @@ void profile_drain(ductgpu_ctx ctx);
 // setup.cu
 int pseudomat_gpu(ductgpu_ctx ctx, int m);
 int pack_operators(ductgpu_ctx ctx, BoundOps &b);
+int pack_transposed(ductgpu_ctx ctx, BoundOps &b);
 void free_bound(BoundOps &b);
 
 // solve_fp64.cu
@@ -155,6 +157,9 @@ struct FieldTask {
     int refine;       // FP64 refinement steps for the split-precision path
 };
 int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
+// adjoint.cu: the transpose of solve_fp64's map rhs -> sol; task.rhs is the
+// cotangent of sol (read only), task.sol receives the cotangent of rhs
+int solve_adjoint(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
 
 // One batched FP64 GEMM pass (k_pass_fp64), usable by other solvers.
 struct PassField {

@@ -152,11 +152,38 @@ __global__ void k_copy_row(int n, const double *Q, int row, double *out)
 
 static int blocks_for(long n) { return (int)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184); }
 
+// The same packing of A^T (the adjoint solve applies P^T and P^-T).
+__global__ void k_pack_at(int n, int kpad, int mtiles, const double *A, double *out)
+{
+    const int total = (kpad / 16) * mtiles * 256;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += gridDim.x * blockDim.x) {
+        const int v = idx & 7, lane = (idx >> 3) & 31, tile = idx >> 8;
+        const int mt = tile % mtiles, ks = tile / mtiles;
+        const int g = lane >> 2, t = lane & 3;
+        const int row = mt * 16 + g + 8 * (v & 1);
+        const int col = ks * 16 + t + 4 * (v >> 1);
+        out[idx] = (row < n && col < n) ? A[col + (size_t)n * row] : 0.0;
+    }
+}
+
+int pack_transposed(ductgpu_ctx ctx, BoundOps &b)
+{
+    if (b.PTpack && b.QTpack) return DUCTGPU_OK;
+    const size_t packed = (size_t)(b.kpad / 16) * b.mtiles * 256;
+    if (!b.PTpack) DUCT_CUDA(ctx, cudaMalloc(&b.PTpack, packed * sizeof(double)));
+    if (!b.QTpack) DUCT_CUDA(ctx, cudaMalloc(&b.QTpack, packed * sizeof(double)));
+    k_pack_at<<<blocks_for((long)packed), 256, 0, ctx->stream>>>(b.n, b.kpad, b.mtiles, b.P, b.PTpack);
+    k_pack_at<<<blocks_for((long)packed), 256, 0, ctx->stream>>>(b.n, b.kpad, b.mtiles, b.PM1, b.QTpack);
+    ctx->launches += 2;
+    return check_cuda(ctx, cudaGetLastError(), "pack_transposed");
+}
+
 void free_bound(BoundOps &b)
 {
     cudaFree(b.E); cudaFree(b.P); cudaFree(b.PM1);
     cudaFree(b.Ppack); cudaFree(b.Qpack); cudaFree(b.pcol); cudaFree(b.qrow);
-    cudaFree(b.D2B); cudaFree(b.Bpack);
+    cudaFree(b.D2B); cudaFree(b.Bpack); cudaFree(b.PTpack); cudaFree(b.QTpack);
     cudaFree(b.Pslices); cudaFree(b.Qslices); cudaFree(b.Pexp); cudaFree(b.Qexp);
     b = BoundOps();
 }
@@ -171,7 +198,9 @@ int pack_operators(ductgpu_ctx ctx, BoundOps &b)
     const size_t packed = (size_t)(b.kpad / 16) * b.mtiles * 256;
     cudaFree(b.Ppack);
     cudaFree(b.Qpack);
-    b.Ppack = b.Qpack = nullptr;
+    cudaFree(b.PTpack);   // the transposed packs follow the operators: rebuilt on next use
+    cudaFree(b.QTpack);
+    b.Ppack = b.Qpack = b.PTpack = b.QTpack = nullptr;
     DUCT_CUDA(ctx, cudaMalloc(&b.Ppack, packed * sizeof(double)));
     DUCT_CUDA(ctx, cudaMalloc(&b.Qpack, packed * sizeof(double)));
     k_pack_a<<<blocks_for((long)packed), 256, 0, ctx->stream>>>(n, b.kpad, b.mtiles, b.P, b.Ppack);

@@ -133,6 +133,22 @@ int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields,
 int ductgpu_solve_fields_dev_noalloc(ductgpu_ctx ctx, const ductgpu_field *fields,
                                      int nfields);
 
+/* ---- adjoint (backward) solve ------------------------------------------ */
+/* The transpose of the FP64 helm3d map rhs -> sol (of every mode and field,
+ * walls, the Neumann wall/corner fill and the kx=0 gauge included), for
+ * reverse-mode gradients through the implicit step: given the cotangent
+ * gsol of sol it returns grhs = S^T gsol, so <gsol, S f> = <grhs, f> for
+ * every f.  Computed in the transposed eigenbasis, P^-T[(P^T G P)./D]P^-1,
+ * with the same batched DMMA passes.  The reference has no adjoint; it is
+ * checked against the transpose of the oracle's dense helm3d matrix.
+ * Fields as in ductgpu_solve_fields_dev with rhs = gsol (read only) and
+ * sol = grhs (walls zero; mode 0 real).                                   */
+int ductgpu_solve_adjoint_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields,
+                                     int nfields);
+/* The same for one field on host arrays (gsol, grhs complex (my,mz,nmodes)). */
+int ductgpu_helm3d_adjoint(ductgpu_ctx ctx, const double *gsol, double *grhs, char bound,
+                           double alambda, int my, int mz, int ib, int ie, const double *xalp);
+
 /* ---- rectangular ducts, general wall conditions (temperature path) ---- */
 /* pseudomaty_temp + pseudomatz_temp (src/pseudomat_temp.f90:2-320) on the
  * GPU for operator slot `slot` (0..7, one per duct shape): my x mz points on
