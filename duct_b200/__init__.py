@@ -35,6 +35,7 @@ EXPORTS = [
     "ductgpu_solve_fields_dev_noalloc", "ductgpu_precomp_mass_flow",
     "ductgpu_impose_mass_flow_dev", "ductgpu_impose_mass_flow",
     "ductgpu_solve_adjoint_fields_dev", "ductgpu_helm3d_adjoint",
+    "ductgpu_pseudopois", "ductgpu_solvepois", "ductgpu_solve_pois_fields_dev",
 ]
 K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
 
@@ -111,6 +112,9 @@ def lib():
             "ductgpu_impose_mass_flow": [P, C.POINTER(D), I, P, I],
             "ductgpu_solve_adjoint_fields_dev": [P, C.POINTER(Field), I],
             "ductgpu_helm3d_adjoint": [P, P, P, C.c_char, D, I, I, I, I, P],
+            "ductgpu_pseudopois": [P, I],
+            "ductgpu_solvepois": [P, P, D, I],
+            "ductgpu_solve_pois_fields_dev": [P, C.POINTER(Field), I],
             "ductgpu_graph_launch": [P, I],
             "ductgpu_graph_destroy": [P, I],
             "transpose_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
@@ -257,6 +261,20 @@ class Context:
     def solve_adjoint_fields_dev(self, fields):
         arr, keep = self._field_array(fields, False)
         self._check(lib().ductgpu_solve_adjoint_fields_dev(self.h, arr, len(fields)))
+        return keep
+
+    def pseudopois(self, my):
+        self._check(lib().ductgpu_pseudopois(self.h, int(my)))
+
+    def solvepois(self, U, xlambda):
+        """solvepois on a real (my,my) plane; returns the solution."""
+        U = np.array(U, dtype=np.float64, order="F")
+        self._check(lib().ductgpu_solvepois(self.h, _ptr(U), float(xlambda), U.shape[0]))
+        return U
+
+    def solve_pois_fields_dev(self, fields):
+        arr, keep = self._field_array(fields, False)
+        self._check(lib().ductgpu_solve_pois_fields_dev(self.h, arr, len(fields)))
         return keep
 
     def preshen(self, my, bound):

@@ -194,6 +194,8 @@ int ductgpu_destroy(ductgpu_ctx ctx)
     for (int i = 0; i < kMaxRect; ++i) free_rect(ctx->rect[i]);
     free_shen(ctx->shen_d);
     free_shen(ctx->shen_n);
+    free_bound(ctx->pois);
+    cudaFree(ctx->pois_r);
     cudaFree(ctx->mf_u);
     cudaFree(ctx->mf_f);
     cudaFree(ctx->mf_sum);
@@ -265,9 +267,9 @@ int ductgpu_pseudomat(ductgpu_ctx ctx, int my, int mz)
 int ductgpu_get_operators(ductgpu_ctx ctx, char bound, double *E, double *P, double *PM1, int *iofzero)
 {
     if (!ctx) return DUCTGPU_EARG;
-    if (!ctx->ready) return set_error(ctx, DUCTGPU_ESTATE, "operators not set up");
-    if (bound != 'd' && bound != 'n') return set_error(ctx, DUCTGPU_EARG, "bound '%c'", bound);
-    const BoundOps &b = (bound == 'n') ? ctx->neu : ctx->dir;
+    if (bound == 'p' ? !ctx->pois_m : !ctx->ready) return set_error(ctx, DUCTGPU_ESTATE, "operators not set up");
+    if (bound != 'd' && bound != 'n' && bound != 'p') return set_error(ctx, DUCTGPU_EARG, "bound '%c'", bound);
+    const BoundOps &b = (bound == 'p') ? ctx->pois : (bound == 'n') ? ctx->neu : ctx->dir;
     const size_t nn = (size_t)b.n * b.n;
     if (E) DUCT_CUDA(ctx, cudaMemcpyAsync(E, b.E, b.n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (P) DUCT_CUDA(ctx, cudaMemcpyAsync(P, b.P, nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -280,10 +282,11 @@ int ductgpu_get_operators(ductgpu_ctx ctx, char bound, double *E, double *P, dou
 int ductgpu_set_operators(ductgpu_ctx ctx, char bound, const double *E, const double *P, const double *PM1, int iofzero)
 {
     if (!ctx) return DUCTGPU_EARG;
-    if (!ctx->ready) return set_error(ctx, DUCTGPU_ESTATE, "call ductgpu_pseudomat first");
-    if (bound != 'd' && bound != 'n') return set_error(ctx, DUCTGPU_EARG, "bound '%c'", bound);
+    if (bound == 'p' ? !ctx->pois_m : !ctx->ready)
+        return set_error(ctx, DUCTGPU_ESTATE, bound == 'p' ? "call ductgpu_pseudopois first" : "call ductgpu_pseudomat first");
+    if (bound != 'd' && bound != 'n' && bound != 'p') return set_error(ctx, DUCTGPU_EARG, "bound '%c'", bound);
     if (!E || !P || !PM1) return set_error(ctx, DUCTGPU_EARG, "null operator");
-    BoundOps &b = (bound == 'n') ? ctx->neu : ctx->dir;
+    BoundOps &b = (bound == 'p') ? ctx->pois : (bound == 'n') ? ctx->neu : ctx->dir;
     const size_t nn = (size_t)b.n * b.n;
     DUCT_CUDA(ctx, cudaMemcpyAsync(b.E, E, b.n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     DUCT_CUDA(ctx, cudaMemcpyAsync(b.P, P, nn * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
@@ -294,7 +297,7 @@ int ductgpu_set_operators(ductgpu_ctx ctx, char bound, const double *E, const do
         b.emin = emin;
         b.emax = emax;
     }
-    if (bound == 'n') {
+    if (bound != 'd') {
         if (iofzero <= 0) {
             double eigmin = 1.0e6;
             iofzero = 0;
@@ -648,6 +651,62 @@ int ductgpu_helm3d_adjoint(ductgpu_ctx ctx, const double *gsol, double *grhs, ch
     if ((rc = ductgpu_solve_adjoint_fields_dev(ctx, &f, 1))) return rc;
     DUCT_CUDA(ctx, cudaMemcpyAsync(grhs, dout, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d_adjoint");
+}
+
+int ductgpu_pseudopois(ductgpu_ctx ctx, int my)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    cudaSetDevice(ctx->device);
+    return pois_setup(ctx, my);
+}
+
+int ductgpu_solve_pois_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (!ctx->pois_m) return set_error(ctx, DUCTGPU_ESTATE, "pseudopois not set up");
+    if (!fields || nfields < 1 || nfields > kMaxFields)
+        return set_error(ctx, DUCTGPU_EARG, "nfields=%d (1..%d)", nfields, kMaxFields);
+    for (int i = 0; i < nfields; ++i) {
+        int rc = validate_field(ctx, fields[i]);
+        if (rc) return rc;
+        if (fields[i].bound != 'n') return set_error(ctx, DUCTGPU_EARG, "solvepois is the Neumann solver (bound 'n')");
+    }
+    cudaSetDevice(ctx->device);
+    FieldTask tasks[kMaxFields];
+    int rc = prepare(ctx, fields, nfields, tasks);
+    if (rc) return rc;
+    return solve_pois(ctx, tasks, nfields);
+}
+
+int ductgpu_solvepois(ductgpu_ctx ctx, double *U, double xlambda, int my)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (!U) return set_error(ctx, DUCTGPU_EARG, "null pointer");
+    if (!ctx->pois_m || my != ctx->pois_m)
+        return set_error(ctx, DUCTGPU_ESTATE, "pseudopois not set up for my=%d", my);
+    cudaSetDevice(ctx->device);
+    const size_t plane = (size_t)my * my;
+    std::vector<double> c(2 * plane, 0.0);
+    for (size_t p = 0; p < plane; ++p) c[2 * p] = U[p];
+    const size_t bytes = 2 * plane * sizeof(double);
+    int rc = ensure(ctx, ctx->io, 2 * bytes);
+    if (rc) return rc;
+    double *drhs = ctx->io.buf, *dsol = drhs + 2 * plane;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(drhs, c.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
+    const double zero = 0.0;
+    ductgpu_field f;
+    f.rhs = drhs;
+    f.sol = dsol;
+    f.xalp = &zero;
+    f.alambda = xlambda;
+    f.ib = 1;   // a real plane: no mode-0 rule needed, its imaginary part stays zero
+    f.nmodes = 1;
+    f.bound = 'n';
+    if ((rc = ductgpu_solve_pois_fields_dev(ctx, &f, 1))) return rc;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(c.data(), dsol, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    if ((rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "solvepois"))) return rc;
+    for (size_t p = 0; p < plane; ++p) U[p] = c[2 * p];
+    return DUCTGPU_OK;
 }
 
 int ductgpu_preshen(ductgpu_ctx ctx, int my, char bound)

@@ -94,6 +94,11 @@ struct ductgpu_ctx_s {
 
     duct::RectSlot rect[duct::kMaxRect];
     duct::ShenOps shen_d, shen_n;
+    // Galerkin-basis Neumann operators (pseudopois): EN, PN, PNM1 and the
+    // wall vectors r_-, r_+ = B^-T phi(-+1) [2 (my-2)]
+    duct::BoundOps pois;
+    double *pois_r = nullptr;
+    int pois_m = 0;
     // constant mass-flow-rate forcing (precomp_mass_flow): premassfu
     // (my,my,mf_mrk) real, premassf[mf_mrk], the last measured flow rate
     double *mf_u = nullptr, *mf_f = nullptr, *mf_sum = nullptr;
@@ -144,6 +149,11 @@ void profile_drain(ductgpu_ctx ctx);
 int pseudomat_gpu(ductgpu_ctx ctx, int m);
 int pack_operators(ductgpu_ctx ctx, BoundOps &b);
 int pack_transposed(ductgpu_ctx ctx, BoundOps &b);
+// Real eigen-decomposition of the n x n device matrix B (destroyed) into
+// b.E, b.P, b.PM1 (allocated by the caller), with emin/emax and iofzero.
+int eigen_gpu(ductgpu_ctx ctx, int n, double *B, BoundOps &b);
+// Ainv = A^-1 for an n x n device matrix (getrf/getrs; synchronises).
+int invert_dev(ductgpu_ctx ctx, int n, const double *A, double *Ainv);
 void free_bound(BoundOps &b);
 
 // solve_fp64.cu
@@ -214,6 +224,10 @@ struct ShenTask {
     char bound;
 };
 int solve_shen(ductgpu_ctx ctx, const ShenTask *tasks, int ntasks);
+
+// pois.cu
+int pois_setup(ductgpu_ctx ctx, int m);
+int solve_pois(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
 
 // solve_rect.cu
 struct RectTask {

@@ -258,7 +258,7 @@ static bool invert4(double *A)
 }
 
 // Eigen-decomposition of the n x n block B (destroyed) into b.E, b.P, b.PM1.
-static int eigen_gpu(ductgpu_ctx ctx, int n, double *B, BoundOps &b)
+int eigen_gpu(ductgpu_ctx ctx, int n, double *B, BoundOps &b)
 {
     cusolverDnHandle_t h = ctx->solver;
     cusolverDnParams_t params = nullptr;

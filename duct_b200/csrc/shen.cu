@@ -99,7 +99,7 @@ void free_shen(ShenOps &s)
 }
 
 // inverse of the n x n matrix A (device) into Ainv via getrf/getrs
-static int invert_dev(ductgpu_ctx ctx, int n, const double *A, double *Ainv)
+int invert_dev(ductgpu_ctx ctx, int n, const double *A, double *Ainv)
 {
     double *LU = nullptr, *work = nullptr;
     int *ipiv = nullptr, *dinfo = nullptr, lwork = 0, info = 0, rc = DUCTGPU_OK;

@@ -69,13 +69,15 @@ int ductgpu_pseudomat(ductgpu_ctx ctx, int my, int mz);
 
 /* Read back the operators of bound 'd' or 'n' (n = my-2):  E[n] eigenvalues,
  * P[n*n] eigenvectors, PM1[n*n] inverse (column-major), iofzero (1-based,
- * Neumann).  Any output pointer may be NULL.                              */
+ * Neumann).  Any output pointer may be NULL.  Bound 'p' reads the
+ * Galerkin-basis Neumann operators of ductgpu_pseudopois.                 */
 int ductgpu_get_operators(ductgpu_ctx ctx, char bound, double *E, double *P,
                           double *PM1, int *iofzero);
 
 /* Replace the eigen-decomposition of bound 'd' or 'n' with host data, e.g.
  * the LAPACK results of the reference's own pseudomat.  Requires a prior
- * ductgpu_pseudomat for the grid.  iofzero <= 0 recomputes it from E.     */
+ * ductgpu_pseudomat for the grid.  iofzero <= 0 recomputes it from E.
+ * Bound 'p' replaces the pseudopois operators (after ductgpu_pseudopois). */
 int ductgpu_set_operators(ductgpu_ctx ctx, char bound, const double *E,
                           const double *P, const double *PM1, int iofzero);
 
@@ -205,6 +207,18 @@ int ductgpu_helm3d_shen(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, cha
 /* Batched device-resident form: every field's `bound` selects its preshen
  * operators; all fields share my (= mz).  rhs is overwritten as above.    */
 int ductgpu_solve_shen_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields);
+
+/* ---- Galerkin-basis Neumann (pressure) solver ------------------------- */
+/* pseudopois(m), src/pseudopois.f90:2-104: the Neumann operator in the basis
+ * phi_j = T_j - j^2/(j+2)^2 T_{j+2} (B2 B^-1 on the interior nodes), its
+ * eigen-decomposition and iofzero, on the GPU; my = 5..193.               */
+int ductgpu_pseudopois(ductgpu_ctx ctx, int my);
+/* solvepois(U,F,FT,wk1,wk2,xlambda,m), src/solvepois.f90:1-170, on one real
+ * host plane U (my,my): interior = rhs in, solution (walls and corners from
+ * the basis, kx=0 point pinned to 0 when |xlambda| <= 1e-10) out.         */
+int ductgpu_solvepois(ductgpu_ctx ctx, double *U, double xlambda, int my);
+/* Batched complex fields (bound 'n'), as ductgpu_solve_fields_dev.       */
+int ductgpu_solve_pois_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields);
 
 /* ---- constant mass-flow-rate forcing ---------------------------------- */
 /* precomp_mass_flow(dtp,alphak,work,nwk), src/operators.F:2205-2289 (square

@@ -1119,3 +1119,147 @@ double orc_impose_mass_flow(double *csum, int krk, double *u, int my, int mz, do
     for (size_t p = 0; p < plane; ++p) u[2 * p] += fac * pu[p];
     return sumg;
 }
+
+/* ---- Galerkin-basis Neumann (pressure) solver -------------------------- */
+/* T_n(x) and T_n''(x) at an interior node, tch0/tch2 of
+ * src/pseudopois.f90:84-104 (theta = acos x).                              */
+static double tch0(int n, double x) { return cos((double)n * acos(x)); }
+static double tch2(int n, double x)
+{
+    const double a = (double)n * acos(x), t0 = cos(a), den = 1.0 - x * x;
+    return (x * sin(a) - (double)n * t0 * sqrt(den)) * (double)n / pow(den, 1.5);
+}
+
+/* pseudopois(m), src/pseudopois.f90:2-82: basis phi_j = T_j - j^2/(j+2)^2
+ * T_{j+2} (phi_j'(+-1) = 0), B(i,j) = phi_j(x_i) and B2 = phi_j''(x_i) on the
+ * interior nodes, PNT = B^-1, D = B2 B^-1, its eigen-decomposition (dgeev),
+ * PNM1, iofzero (smallest |EN|, strict update), wanted = 0.                */
+int orc_pseudopois(int m, orc_pois *p)
+{
+    if (m < 5) return -1;
+    memset(p, 0, sizeof(*p));
+    const int n = m - 1, mm2 = m - 2;
+    const double pi = 4.0 * atan(1.0);
+    p->m = m;
+    p->EN = (double *)calloc((size_t)mm2, sizeof(double));
+    double *ENim = (double *)calloc((size_t)mm2, sizeof(double));
+    p->PN = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    p->PNM1 = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    p->PNT = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    double *wk1 = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    double *D = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    double *x = (double *)calloc((size_t)m, sizeof(double));
+    for (int j = 0; j < m; ++j) x[j] = -cos(pi * (double)j / (double)n);
+    for (int i = 1; i < m - 1; ++i)
+        for (int j = 0; j < mm2; ++j) {
+            const double c = (double)(j * j) / (((double)j + 2.0) * ((double)j + 2.0));
+            p->PNT[IX(i - 1, j, mm2)] = tch0(j, x[i]) - c * tch0(j + 2, x[i]);
+            wk1[IX(i - 1, j, mm2)] = tch2(j, x[i]) - c * tch2(j + 2, x[i]);
+        }
+    int info = invert(mm2, p->PNT);
+    if (!info) {
+        const double one = 1.0, zero = 0.0;
+        scipy_dgemm_("n", "n", &mm2, &mm2, &mm2, &one, wk1, &mm2, p->PNT, &mm2, &zero, D, &mm2, 1, 1);
+        info = eigen(mm2, D, p->EN, ENim, p->PN);
+    }
+    if (!info) {
+        memcpy(p->PNM1, p->PN, sizeof(double) * (size_t)mm2 * mm2);
+        info = invert(mm2, p->PNM1);
+    }
+    double eigmin = 1.0e6;
+    for (int i = 0; i < mm2; ++i) {
+        const double e = fmin(eigmin, fabs(p->EN[i]));
+        if (e != eigmin) { p->iofzero = i + 1; eigmin = e; }
+    }
+    p->wanted = 0.0;
+    free(ENim); free(wk1); free(D); free(x);
+    return info;
+}
+
+void orc_pois_free(orc_pois *p)
+{
+    free(p->EN); free(p->PN); free(p->PNM1); free(p->PNT);
+    memset(p, 0, sizeof(*p));
+}
+
+/* solvepois(U,F,FT,wk1,wk2,xlambda,m), src/solvepois.f90:1-170.          */
+int orc_solvepois(double *U, const orc_pois *p, double xlambda)
+{
+    const int m = p->m, mm2 = m - 2, io = p->iofzero - 1;
+    const double one = 1.0, zero = 0.0;
+    double *F = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    double *FT = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    double *w1 = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    double *w2 = (double *)calloc((size_t)mm2 * mm2, sizeof(double));
+    for (int j = 0; j < mm2; ++j)
+        for (int i = 0; i < mm2; ++i) F[IX(i, j, mm2)] = U[IX(i + 1, j + 1, m)];
+    scipy_dgemm_("n", "n", &mm2, &mm2, &mm2, &one, p->PNM1, &mm2, F, &mm2, &zero, FT, &mm2, 1, 1);
+    scipy_dgemm_("n", "t", &mm2, &mm2, &mm2, &one, FT, &mm2, p->PNM1, &mm2, &zero, F, &mm2, 1, 1);
+    for (int j = 0; j < mm2; ++j)
+        for (int i = 0; i < mm2; ++i)
+            FT[IX(i, j, mm2)] = F[IX(i, j, mm2)] / (p->EN[i] + p->EN[j] - xlambda);
+    if (!(fabs(xlambda) > 1.0e-10)) {
+        /* :38-86: skip the zero eigen-coefficient, then choose it so that the
+         * solution takes the value wanted at (iofzero+1, iofzero+1)         */
+        FT[IX(io, io, mm2)] = 0.0;
+        double valore = 0.0;
+        for (int l = 0; l < mm2; ++l) {
+            double val = 0.0;
+            for (int k = 0; k < mm2; ++k) val += p->PN[IX(io, k, mm2)] * FT[IX(l, k, mm2)];
+            valore += p->PN[IX(io, l, mm2)] * val;
+        }
+        FT[IX(io, io, mm2)] = (p->wanted - valore) / (p->PN[IX(io, io, mm2)] * p->PN[IX(io, io, mm2)]);
+    }
+    scipy_dgemm_("n", "n", &mm2, &mm2, &mm2, &one, p->PN, &mm2, FT, &mm2, &zero, F, &mm2, 1, 1);
+    scipy_dgemm_("n", "t", &mm2, &mm2, &mm2, &one, F, &mm2, p->PN, &mm2, &zero, FT, &mm2, 1, 1);
+    for (int j = 0; j < mm2; ++j)
+        for (int i = 0; i < mm2; ++i) U[IX(i + 1, j + 1, m)] = FT[IX(i, j, mm2)];
+    /* corners :104-139: basis coefficients a = B^-1 U B^-T, phi_j(+-1) */
+    scipy_dgemm_("n", "n", &mm2, &mm2, &mm2, &one, p->PNT, &mm2, FT, &mm2, &zero, w1, &mm2, 1, 1);
+    scipy_dgemm_("n", "t", &mm2, &mm2, &mm2, &one, w1, &mm2, p->PNT, &mm2, &zero, w2, &mm2, 1, 1);
+    double vsw = 0.0, vse = 0.0, vnw = 0.0, vne = 0.0;
+    for (int i = 0; i < mm2; ++i) {
+        const double si = (i & 1) ? -1.0 : 1.0, vpol = (double)(i + 1) / (double)((i + 2) * (i + 2));
+        double isw = 0.0, ise = 0.0, inw = 0.0, ine = 0.0;
+        for (int j = 0; j < mm2; ++j) {
+            const double sj = (j & 1) ? -1.0 : 1.0, coej = (double)(j + 1) / (double)((j + 2) * (j + 2));
+            const double a = w2[IX(i, j, mm2)];
+            isw += sj * coej * a;
+            ise += sj * coej * a;
+            inw += coej * a;
+            ine += coej * a;
+        }
+        vsw += si * vpol * isw;
+        vse += vpol * ise;
+        vnw += si * vpol * inw;
+        vne += vpol * ine;
+    }
+    U[IX(0, 0, m)] = 16.0 * vsw;
+    U[IX(m - 1, 0, m)] = 16.0 * vse;
+    U[IX(0, m - 1, m)] = 16.0 * vnw;
+    U[IX(m - 1, m - 1, m)] = 16.0 * vne;
+    /* edges :141-169: w1 = B^-1 U (coefficients along y), w2 = U B^-T */
+    scipy_dgemm_("n", "t", &mm2, &mm2, &mm2, &one, FT, &mm2, p->PNT, &mm2, &zero, w2, &mm2, 1, 1);
+    for (int j = 1; j < m - 1; ++j) {
+        double vl = 0.0, vr = 0.0;
+        for (int i = 0; i < mm2; ++i) {
+            const double c = (double)(i + 1) / (double)((i + 2) * (i + 2)), s = (i & 1) ? -1.0 : 1.0;
+            vl += s * c * w1[IX(i, j - 1, mm2)];
+            vr += c * w1[IX(i, j - 1, mm2)];
+        }
+        U[IX(0, j, m)] = 4.0 * vl;
+        U[IX(m - 1, j, m)] = 4.0 * vr;
+    }
+    for (int i = 1; i < m - 1; ++i) {
+        double vl = 0.0, vr = 0.0;
+        for (int j = 0; j < mm2; ++j) {
+            const double c = (double)(j + 1) / (double)((j + 2) * (j + 2)), s = (j & 1) ? -1.0 : 1.0;
+            vl += s * c * w2[IX(i - 1, j, mm2)];
+            vr += c * w2[IX(i - 1, j, mm2)];
+        }
+        U[IX(i, 0, m)] = 4.0 * vl;
+        U[IX(i, m - 1, m)] = 4.0 * vr;
+    }
+    free(F); free(FT); free(w1); free(w2);
+    return 0;
+}

@@ -152,6 +152,21 @@ int    orc_solveshen(double *U, const orc_shen *s, double xlambda);
 int    orc_helm3d_shen(double *rhs, double *sol, int my, int mz, int ib, int ie,
                        const double *xalp, double alambda, const orc_shen *s, int nthreads);
 
+/* ---- Galerkin-basis Neumann (pressure) solver, pseudopois/solvepois --- */
+typedef struct {
+    int m;
+    double *EN, *PN, *PNM1;  /* n, n*n, n*n (n = m-2): eigen-pairs of B2 B^-1 */
+    double *PNT;             /* n*n  B^-1 (basis coefficients from interior) */
+    int iofzero;             /* 1-based, smallest |EN|                       */
+    double wanted;
+} orc_pois;
+/* pseudopois(m), src/pseudopois.f90:2-104.                                 */
+int  orc_pseudopois(int m, orc_pois *p);
+void orc_pois_free(orc_pois *p);
+/* solvepois(U,F,FT,wk1,wk2,xlambda,m), src/solvepois.f90:1-170: U real
+ * (m,m), interior in, solution with walls and corners out.                */
+int  orc_solvepois(double *U, const orc_pois *p, double xlambda);
+
 /* precomp_mass_flow / impose_mass_flow, src/operators.F:2205-2344 (square
  * build).  premassfu: (my,my,mrk) real, premassf: mrk.                     */
 int    orc_precomp_mass_flow(const orc_ops *o, double dtp, const double *alphak, int mrk,

@@ -26,6 +26,11 @@ class _Dir(C.Structure):
         (n, C.POINTER(C.c_double)) for n in ("D", "D2", "E", "P", "PM1", "B")]
 
 
+class _Pois(C.Structure):
+    _fields_ = [("m", C.c_int)] + [(n, C.POINTER(C.c_double)) for n in ("EN", "PN", "PNM1", "PNT")] + [
+        ("iofzero", C.c_int), ("wanted", C.c_double)]
+
+
 class _Shen(C.Structure):
     _fields_ = [("m", C.c_int), ("bound", C.c_char)] + [
         (n, C.POINTER(C.c_double)) for n in ("b", "M", "S", "E", "P", "PSM1", "A", "B")]
@@ -68,6 +73,9 @@ def lib():
                                             C.c_double, P, P]
         L.orc_impose_mass_flow.argtypes = [P, C.c_int, P, C.c_int, C.c_int, C.c_double, P, P, C.c_int]
         L.orc_impose_mass_flow.restype = C.c_double
+        L.orc_pseudopois.argtypes = [C.c_int, C.POINTER(_Pois)]
+        L.orc_pois_free.argtypes = [C.POINTER(_Pois)]
+        L.orc_solvepois.argtypes = [P, C.POINTER(_Pois), C.c_double]
         _lib = L
     return _lib
 
@@ -163,6 +171,38 @@ def impose_mass_flow(u, csum, krk, premassfu, premassf, iflag, aspect=1.0):
     sumg = lib().orc_impose_mass_flow(C.byref(cs), int(krk), _p(u), my, mz, float(aspect), _p(pu), _p(pf),
                                       int(iflag))
     return u, cs.value, sumg
+
+
+class Pois:
+    """pseudopois(m): the Galerkin-basis Neumann operators (src/pseudopois.f90)."""
+
+    def __init__(self, m):
+        self._s = _Pois()
+        info = lib().orc_pseudopois(int(m), C.byref(self._s))
+        if info != 0:
+            raise RuntimeError("orc_pseudopois failed, info=%d" % info)
+        self.m = m
+        n = m - 2
+
+        def v(ptr, *shape):
+            return np.ctypeslib.as_array(ptr, shape=(int(np.prod(shape)),)).reshape(
+                shape, order="F").copy(order="F")
+        self.EN, self.PN, self.PNM1, self.PNT = v(self._s.EN, n), v(self._s.PN, n, n), v(self._s.PNM1, n, n), \
+            v(self._s.PNT, n, n)
+        self.iofzero = self._s.iofzero
+
+    def __del__(self):
+        try:
+            lib().orc_pois_free(C.byref(self._s))
+        except Exception:
+            pass
+
+
+def solvepois(U, pois, xlambda):
+    """solvepois on a real (m,m) plane (interior = rhs); returns the solution."""
+    U = np.array(U, dtype=np.float64, order="F")
+    lib().orc_solvepois(_p(U), C.byref(pois._s), float(xlambda))
+    return U
 
 
 class Shen:
@@ -303,6 +343,6 @@ def set_blas_threads(n):
     lib().orc_set_blas_threads(int(n))
 
 
-__all__ = ["Ops", "Dir", "Shen", "precomp_mass_flow", "impose_mass_flow", "solveshen", "helm3d_shen", "helm3d_temp", "solvediag", "helm3d", "transyz", "transyz_plane", "derivyz",
+__all__ = ["Ops", "Dir", "Shen", "Pois", "solvepois", "precomp_mass_flow", "impose_mass_flow", "solveshen", "helm3d_shen", "helm3d_temp", "solvediag", "helm3d", "transyz", "transyz_plane", "derivyz",
            "cheb2_integral", "cxyz2yzx", "cyzx2xyz", "set_blas_threads", "lib"]
 _ = os
