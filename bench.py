@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-transforms", action="store_true")
     return ap.parse_args()
 
 
@@ -284,6 +285,8 @@ def run_ours(args, world, rank, local, pg):
         prec = D.PREC_FP64 if best == "fp64" else D.PREC_MIXED
         e2e = measure_e2e(ctx, c, m, nm, xalp, rhs, prec, args, pg, world)
 
+    hbm = transform_rates(ctx) if (rank == 0 and not args.no_transforms) else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, threads, done, el = cpu_reference_rate(c, m, xalp, rhs, budget_s=10.0)
@@ -311,6 +314,7 @@ def run_ours(args, world, rank, local, pg):
             "paths": {k: {"value": v["value"], "ms_per_step": v["ms_step"], "roofline": roofs[k],
                           "gpu_launches": v["launches"]} for k, v in res.items()},
             "mixed_rel_err_vs_fp64": acc,
+            "hbm_kernels": hbm,
         }
         print(json.dumps(line), flush=True)
 
@@ -335,6 +339,63 @@ def traffic_from_profile(kernel):
     if os.path.exists(p):
         return json.load(open(p)).get(kernel, {}).get("bytes_per_launch")
     return None
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured copy (MEASURED_PEAKS.json)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def transform_rates(ctx, reps=20):
+    """Achieved HBM bandwidth of the memory-bound kernels on a config-4 sized
+    field (my = mz = 193, 85 modes, 50.7 MB complex128): transyz along y and
+    z, derivyz, and the pencil transposes.  Four buffers rotate (203 MB > L2);
+    algorithmic bytes = read + write of one field per call."""
+    import ctypes as C
+    import duct_b200 as D
+    L = D.lib()
+    m, nm = 193, 85
+    shape = (m, m, nm)
+    rng = np.random.default_rng(0)
+    host = np.asfortranarray(rng.standard_normal(shape) + 1j * rng.standard_normal(shape))
+    bufs = [ctx.device_array(shape) for _ in range(4)]
+    for b in bufs:
+        b.upload(host)
+    fbytes = host.nbytes
+    peak, src = hbm_peak()
+    h = ctx.h
+    ops = {
+        # forward and backward alternate so the values keep their size
+        "transyz_y": lambda i: L.ductgpu_transyz_dev(h, C.c_void_p(bufs[i % 4].ptr), m, m, nm, b"y",
+                                                     -1 if (i // 4) % 2 == 0 else 1),
+        "transyz_z": lambda i: L.ductgpu_transyz_dev(h, C.c_void_p(bufs[i % 4].ptr), m, m, nm, b"z",
+                                                     -1 if (i // 4) % 2 == 0 else 1),
+        "derivyz_y": lambda i: L.ductgpu_derivyz_dev(h, C.c_void_p(bufs[i % 4].ptr), C.c_void_p(bufs[(i + 2) % 4].ptr),
+                                                     m, m, nm, b"y", 1, 1.0, b"n", 1.0),
+        "derivyz_z": lambda i: L.ductgpu_derivyz_dev(h, C.c_void_p(bufs[i % 4].ptr), C.c_void_p(bufs[(i + 2) % 4].ptr),
+                                                     m, m, nm, b"z", 1, 1.0, b"n", 1.0),
+        "cxyz2yzx": lambda i: L.ductgpu_cxyz2yzx_dev(h, C.c_void_p(bufs[i % 4].ptr), C.c_void_p(bufs[(i + 2) % 4].ptr),
+                                                     nm, m, m),
+    }
+    out = {}
+    for name, op in ops.items():
+        for i in range(3):
+            assert op(i) == 0, ctx.last_error()
+        ctx.synchronize()
+        ctx.event_record(2)
+        for i in range(reps):
+            op(i)
+        ctx.event_record(3)
+        ms = ctx.event_elapsed(2, 3) / reps
+        gbs = 2.0 * fbytes / (ms * 1e-3) / 1e9
+        out[name] = {"ms": ms, "achieved_gbs": gbs, "frac": gbs / peak}
+    for b in bufs:
+        b.free()
+    return {"field": "193x193x85 complex128 (50.7 MB), 4 rotating buffers", "peak_gbs": peak,
+            "peak_source": src, "kernels": out}
 
 
 def measure_e2e(ctx, c, m, nm, xalp, rhs, prec, args, pg, world):
