@@ -13,8 +13,7 @@
 //
 // derivyz (src/chebyshev.f90:1-295): the backward recurrence
 // d_{k-1} = d_{k+1} + 2k c_k on Chebyshev coefficients, one thread per
-// complex line, lines staged through shared memory when they are
-// contiguous in memory (y) and read directly when they are strided (z).
+// complex line on tiles of lines staged in shared memory with cp.async.
 //
 // Pencil transposes (src/parallel.F:476-529): 32x32 tiles of complex
 // elements through padded shared memory.
@@ -76,25 +75,36 @@ __device__ __forceinline__ void dft(double2 (&v)[4])
     }
 }
 
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_group 0;\n" ::);
+}
+
+// One radix-R Stockham stage over all lines of the CTA; twiddles from the
+// table tw[t] = exp(-2 pi i t / L).
 template <int R>
-__device__ __forceinline__ void stockham_stage(const double2 *x, double2 *y, int L, int Ns, int lpb)
+__device__ __forceinline__ void stockham_stage(const double2 *x, double2 *y, const double2 *tw, int L, int LS, int Ns,
+                                               int lpb)
 {
     const int nb = L / R;
+    const int tstep = L / (Ns * R);
     for (int idx = threadIdx.x; idx < nb * lpb; idx += blockDim.x) {
         const int l = idx / nb, j = idx - l * nb;
-        const double2 *xl = x + l * L;
-        double2 *yl = y + l * L;
+        const double2 *xl = x + l * LS;
+        double2 *yl = y + l * LS;
         const int k = j % Ns;
         double2 v[4];
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = xl[j + r * nb];
         if (Ns > 1) {
 #pragma unroll
-            for (int r = 1; r < R; ++r) {
-                double sn, cs;
-                sincospi(-2.0 * (double)(r * k) / (double)(Ns * R), &sn, &cs);
-                v[r] = cmul(v[r], make_double2(cs, sn));
-            }
+            for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[r * k * tstep]);
         }
         dft<R>(v);
         const int d = (j / Ns) * Ns * R + k;
@@ -103,53 +113,72 @@ __device__ __forceinline__ void stockham_stage(const double2 *x, double2 *y, int
     }
 }
 
+// Lines of a CTA: lpb consecutive lines of one plane (the launch keeps a
+// CTA inside one Fourier mode), staged with cp.async; y-lines are
+// contiguous, z-lines are read as rows of lpb consecutive y (128 B for 8).
 __global__ void __launch_bounds__(256) k_dct(const __grid_constant__ DctParams p)
 {
     extern __shared__ __align__(16) double2 buf[];
-    double2 *x = buf, *y = buf + p.lpb * p.L;
-    const int line0 = blockIdx.x * p.lpb;
-    const int nl = min(p.lpb, p.nlines - line0);
-    const int N = p.nn - 1, L = p.L;
-    auto gaddr = [&](int l, int j) -> double2 * {
-        const int line = line0 + l;
-        const int mode = line / p.lines_per_mode, q = line - mode * p.lines_per_mode;
-        return reinterpret_cast<double2 *>(p.f) + mode * p.mode_stride + q * p.line_stride + j * p.elem_stride;
-    };
-    // load + even extension; inverse: ends weighted 1, interior 1/2
+    const int L = p.L, LS = p.L + 1, N = p.nn - 1, nn = p.nn;   // LS: padded line stride
+    double2 *tw = buf;
+    double2 *x = buf + L, *y = x + p.lpb * LS;
+    const int cpm = (p.lines_per_mode + p.lpb - 1) / p.lpb;   // CTAs per mode
+    const int mode = blockIdx.x / cpm;
+    const int q0 = (blockIdx.x - mode * cpm) * p.lpb;
+    const int nl = min(p.lpb, p.lines_per_mode - q0);
+    double2 *g = reinterpret_cast<double2 *>(p.f) + mode * p.mode_stride + (long long)q0 * p.line_stride;
     const bool contiguous = (p.elem_stride == 1);
-    for (int idx = threadIdx.x; idx < p.lpb * p.nn; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < nl * nn; idx += blockDim.x) {
         int l, j;
-        if (contiguous) { l = idx / p.nn; j = idx - l * p.nn; }
-        else { j = idx / p.lpb; l = idx - j * p.lpb; }
+        if (contiguous) { l = idx / nn; j = idx - l * nn; }
+        else { j = idx / nl; l = idx - j * nl; }
+        cp_async16(x + l * LS + j, g + l * p.line_stride + (long long)j * p.elem_stride);
+    }
+    for (int t = threadIdx.x; t < L; t += blockDim.x) {
+        double sn, cs;
+        sincospi(-2.0 * (double)t / (double)L, &sn, &cs);
+        tw[t] = make_double2(cs, sn);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // even extension; the inverse weights the interior points by 1/2
+    const double si = (p.iopt >= 0) ? 0.5 : 1.0;
+    for (int idx = threadIdx.x; idx < p.lpb * (N - 1); idx += blockDim.x) {
+        const int l = idx / (N - 1), j = 1 + idx - l * (N - 1);
         double2 v = make_double2(0.0, 0.0);
-        if (l < nl) v = *gaddr(l, j);
-        if (p.iopt >= 0 && j > 0 && j < N) v = make_double2(0.5 * v.x, 0.5 * v.y);
-        x[l * L + j] = v;
-        if (j > 0 && j < N) x[l * L + (L - j)] = v;
+        if (l < nl) {
+            v = x[l * LS + j];
+            v = make_double2(si * v.x, si * v.y);
+        }
+        x[l * LS + j] = v;
+        x[l * LS + (L - j)] = v;
+    }
+    for (int l = nl + threadIdx.x; l < p.lpb; l += blockDim.x) {   // unused lines: zero ends
+        x[l * LS] = make_double2(0.0, 0.0);
+        x[l * LS + N] = make_double2(0.0, 0.0);
     }
     __syncthreads();
     int Ns = 1;
     for (int s = 0; s < p.nstages; ++s) {
         const int R = p.radix[s];
-        if (R == 4) stockham_stage<4>(x, y, L, Ns, p.lpb);
-        else if (R == 2) stockham_stage<2>(x, y, L, Ns, p.lpb);
-        else stockham_stage<3>(x, y, L, Ns, p.lpb);
+        if (R == 4) stockham_stage<4>(x, y, tw, L, LS, Ns, p.lpb);
+        else if (R == 2) stockham_stage<2>(x, y, tw, L, LS, Ns, p.lpb);
+        else stockham_stage<3>(x, y, tw, L, LS, Ns, p.lpb);
         Ns *= R;
         __syncthreads();
         double2 *t = x; x = y; y = t;
     }
     const double dn1 = 1.0 / (double)N, dn2 = 0.5 * dn1;
-    for (int idx = threadIdx.x; idx < p.lpb * p.nn; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < nl * nn; idx += blockDim.x) {
         int l, j;
-        if (contiguous) { l = idx / p.nn; j = idx - l * p.nn; }
-        else { j = idx / p.lpb; l = idx - j * p.lpb; }
-        if (l >= nl) continue;
-        double2 v = x[l * L + j];
+        if (contiguous) { l = idx / nn; j = idx - l * nn; }
+        else { j = idx / nl; l = idx - j * nl; }
+        double2 v = x[l * LS + j];
         if (p.iopt < 0) {
             const double sc = (j == 0 || j == N) ? dn2 : dn1;
             v = make_double2(sc * v.x, sc * v.y);
         }
-        *gaddr(l, j) = v;
+        g[l * p.line_stride + (long long)j * p.elem_stride] = v;
     }
 }
 
@@ -186,60 +215,47 @@ __device__ void deriv_rec(const double2 *c, long long cs, double2 *o, long long 
 
 constexpr int kDerivLines = 32;
 
+// A tile of kDerivLines lines of one mode staged with cp.async (padded odd
+// row length, conflict-free for both the y and the z access pattern), the
+// recurrence run in place by one thread per line (it reads c_k before it
+// writes out_k and then only lower indices), coalesced stores.
 __global__ void __launch_bounds__(256) k_deriv(const __grid_constant__ DerivParams p)
 {
     extern __shared__ __align__(16) double2 sm[];
-    const int line0 = blockIdx.x * kDerivLines;
-    const int nl = min(kDerivLines, p.nlines - line0);
-    auto base = [&](int l) -> long long {
-        const int line = line0 + l;
-        const int mode = line / p.lines_per_mode, q = line - mode * p.lines_per_mode;
-        return mode * p.mode_stride + q * p.line_stride;
-    };
-    const double2 *U = reinterpret_cast<const double2 *>(p.u);
-    double2 *DU = reinterpret_cast<double2 *>(p.du);
-    const int nn = p.nn;
-    if (p.elem_stride == 1) {
-        // contiguous lines: stage (in, aux) through shared memory, padded rows
-        const int ld = nn + 1;
-        double2 *cin = sm, *aux = sm + kDerivLines * ld;
-        for (int idx = threadIdx.x; idx < kDerivLines * nn; idx += blockDim.x) {
-            const int l = idx / nn, j = idx - l * nn;
-            if (l < nl) cin[l * ld + j] = U[base(l) + j];
-        }
-        __syncthreads();
-        const int l = threadIdx.x;
-        if (l < nl) {
-            if (p.ider == 1) {
-                deriv_rec(cin + l * ld, 1, aux + l * ld, 1, nn, p.fac, false);
-            } else {
-                deriv_rec(cin + l * ld, 1, aux + l * ld, 1, nn, 1.0, false);
-                deriv_rec(aux + l * ld, 1, cin + l * ld, 1, nn, p.fac, false);
-            }
-        }
-        __syncthreads();
-        const double2 *res = (p.ider == 1) ? aux : cin;
-        for (int idx = threadIdx.x; idx < kDerivLines * nn; idx += blockDim.x) {
-            const int l2 = idx / nn, j = idx - l2 * nn;
-            if (l2 >= nl) continue;
-            const long long g = base(l2) + j;
-            const double2 v = res[l2 * ld + j];
-            DU[g] = p.accumulate ? make_double2(DU[g].x + v.x, DU[g].y + v.y) : v;
-        }
-    } else {
-        // strided lines: neighbouring threads own neighbouring lines, so every
-        // step of the recurrence is a coalesced access
-        const int l = threadIdx.x;
-        if (l >= nl) return;
-        const long long b0 = base(l);
+    const int nn = p.nn, ld = nn | 1;
+    const int cpm = (p.lines_per_mode + kDerivLines - 1) / kDerivLines;
+    const int mode = blockIdx.x / cpm;
+    const int q0 = (blockIdx.x - mode * cpm) * kDerivLines;
+    const int nl = min(kDerivLines, p.lines_per_mode - q0);
+    const long long base = mode * p.mode_stride + (long long)q0 * p.line_stride;
+    const double2 *U = reinterpret_cast<const double2 *>(p.u) + base;
+    double2 *DU = reinterpret_cast<double2 *>(p.du) + base;
+    const bool contiguous = (p.elem_stride == 1);
+    for (int idx = threadIdx.x; idx < nl * nn; idx += blockDim.x) {
+        int l, k;
+        if (contiguous) { l = idx / nn; k = idx - l * nn; }
+        else { k = idx / nl; l = idx - k * nl; }
+        cp_async16(sm + l * ld + k, U + l * p.line_stride + (long long)k * p.elem_stride);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    if (threadIdx.x < nl) {
+        double2 *c = sm + threadIdx.x * ld;
         if (p.ider == 1) {
-            deriv_rec(U + b0, p.elem_stride, DU + b0, p.elem_stride, nn, p.fac, p.accumulate != 0);
+            deriv_rec(c, 1, c, 1, nn, p.fac, false);
         } else {
-            // aux line in shared memory, column l
-            double2 *aux = sm;
-            deriv_rec(U + b0, p.elem_stride, aux + l, kDerivLines, nn, 1.0, false);
-            deriv_rec(aux + l, kDerivLines, DU + b0, p.elem_stride, nn, p.fac, p.accumulate != 0);
+            deriv_rec(c, 1, c, 1, nn, 1.0, false);
+            deriv_rec(c, 1, c, 1, nn, p.fac, false);
         }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nl * nn; idx += blockDim.x) {
+        int l, k;
+        if (contiguous) { l = idx / nn; k = idx - l * nn; }
+        else { k = idx / nl; l = idx - k * nl; }
+        const long long g = l * p.line_stride + (long long)k * p.elem_stride;
+        const double2 v = sm[l * ld + k];
+        DU[g] = p.accumulate ? make_double2(DU[g].x + v.x, DU[g].y + v.y) : v;
     }
 }
 
@@ -290,13 +306,16 @@ int transyz_dev(ductgpu_ctx ctx, double *f, int my, int mz, int nmodes, char cdi
     p.nstages = plan_radices(p.L, p.radix);
     if (p.nstages < 0)
         return set_error(ctx, DUCTGPU_EARG, "transyz: line length %d - 1 must be of the form 2^a 3^b", p.nn);
-    p.lpb = 2048 / p.L;
+    // lines per CTA: two line buffers + the twiddle table in ~100 KB, so
+    // two CTAs share an SM
+    p.lpb = (int)((100 * 1024 / sizeof(double2) - p.L) / (2 * (p.L + 1)));
     if (p.lpb < 1) p.lpb = 1;
     if (p.lpb > 32) p.lpb = 32;
+    if (p.lpb > p.lines_per_mode) p.lpb = p.lines_per_mode;
     p.iopt = iopt;
-    const size_t smem = 2 * (size_t)p.lpb * p.L * sizeof(double2);
+    const size_t smem = (2 * (size_t)p.lpb * (p.L + 1) + p.L) * sizeof(double2);
     DUCT_CUDA(ctx, cudaFuncSetAttribute(k_dct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int grid = (p.nlines + p.lpb - 1) / p.lpb;
+    const int grid = nmodes * ((p.lines_per_mode + p.lpb - 1) / p.lpb);
     {
         LaunchScope ls(ctx, DUCTGPU_K_TRANSFORM);
         k_dct<<<grid, 256, smem, ctx->stream>>>(p);
@@ -316,14 +335,12 @@ int derivyz_dev(ductgpu_ctx ctx, const double *u, double *du, int my, int mz, in
     p.accumulate = (what != 'n');
     p.fac = scal;
     if (cdir == 'z') p.fac = (ider == 1) ? scal / aspect : scal / (aspect * aspect);
-    size_t smem;
-    if (p.elem_stride == 1) smem = 2 * (size_t)kDerivLines * (p.nn + 1) * sizeof(double2);
-    else smem = (size_t)kDerivLines * p.nn * sizeof(double2);
+    const size_t smem = (size_t)kDerivLines * (p.nn | 1) * sizeof(double2);
     DUCT_CUDA(ctx, cudaFuncSetAttribute(k_deriv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int grid = (p.nlines + kDerivLines - 1) / kDerivLines;
+    const int grid = nmodes * ((p.lines_per_mode + kDerivLines - 1) / kDerivLines);
     {
         LaunchScope ls(ctx, DUCTGPU_K_TRANSFORM);
-        k_deriv<<<grid, (p.elem_stride == 1) ? 256 : kDerivLines, smem, ctx->stream>>>(p);
+        k_deriv<<<grid, 256, smem, ctx->stream>>>(p);
     }
     return check_cuda(ctx, cudaGetLastError(), "k_deriv");
 }
