@@ -334,12 +334,14 @@ __global__ void __launch_bounds__(1024) k_neumann_pin(const __grid_constant__ Fi
     }
 }
 
-// Neumann wall lines from the interior (src/solvediag.f90:253-276):
-// blockIdx.y = 0: z-walls U(i,1), U(i,m) of every interior row i (one thread
-// per row, sums over j); blockIdx.y = 1: y-walls U(1,j), U(m,j) of every
-// interior column j (one warp per column, sums over i).
-__global__ void __launch_bounds__(256) k_neumann_walls(const __grid_constant__ FillParams p)
+// Neumann wall lines from the interior (src/solvediag.f90:253-276).
+// blockIdx.y < nyb: y-walls U(1,j), U(m,j), one warp per interior column j
+// (the column is contiguous: coalesced dot products with DC rows 1 and m);
+// blockIdx.y >= nyb: z-walls U(i,1), U(i,m) of 32 interior rows i per CTA,
+// the 8 thread rows splitting the sum over j (512-byte coalesced rows).
+__global__ void __launch_bounds__(256) k_neumann_walls(const __grid_constant__ FillParams p, int nyb)
 {
+    __shared__ double part[8][32][4];
     const int fi = fill_field(p);
     const int plane = blockIdx.x - p.cta_start[fi];
     const int m = p.m;
@@ -347,35 +349,43 @@ __global__ void __launch_bounds__(256) k_neumann_walls(const __grid_constant__ F
     const double *DC = p.DC;
     const double d11 = DC[0], d1m = DC[(long long)m * (m - 1)];
     const double dm1 = DC[m - 1], dmm = DC[(m - 1) + (long long)m * (m - 1)];
-    const double det = d11 * dmm - d1m * dm1;
-    if (blockIdx.y == 0) {
-        for (int i = 1 + threadIdx.x; i < m - 1; i += blockDim.x) {
-            double sb0 = 0, sb1 = 0, st0 = 0, st1 = 0;
-            for (int j = 1; j < m - 1; ++j) {
+    const double idet = 1.0 / (d11 * dmm - d1m * dm1);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if ((int)blockIdx.y < nyb) {
+        const int j = 1 + blockIdx.y * 8 + warp;
+        if (j >= m - 1) return;
+        double sl[4] = {0, 0, 0, 0};
+        for (int i = 1 + lane; i < m - 1; i += 32) {
+            const double2 v = U[i + (long long)m * j];
+            const double a = DC[(long long)m * i], b = DC[(m - 1) + (long long)m * i];
+            sl[0] += a * v.x; sl[1] += a * v.y; sl[2] += b * v.x; sl[3] += b * v.y;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            for (int o = 16; o > 0; o >>= 1) sl[q] += __shfl_xor_sync(0xffffffffu, sl[q], o);
+        if (lane == 0) {
+            U[(long long)m * j] = make_double2((-dmm * sl[0] + d1m * sl[2]) * idet, (-dmm * sl[1] + d1m * sl[3]) * idet);
+            U[(m - 1) + (long long)m * j] = make_double2((dm1 * sl[0] - d11 * sl[2]) * idet, (dm1 * sl[1] - d11 * sl[3]) * idet);
+        }
+    } else {
+        const int i = 1 + (blockIdx.y - nyb) * 32 + lane;
+        double sb0 = 0, sb1 = 0, st0 = 0, st1 = 0;
+        if (i < m - 1)
+            for (int j = 1 + warp; j < m - 1; j += 8) {
                 const double2 v = U[i + (long long)m * j];
                 const double a = DC[(long long)m * j], b = DC[(m - 1) + (long long)m * j];
                 sb0 += a * v.x; sb1 += a * v.y; st0 += b * v.x; st1 += b * v.y;
             }
-            U[i] = make_double2((-dmm * sb0 + d1m * st0) / det, (-dmm * sb1 + d1m * st1) / det);
-            U[i + (long long)m * (m - 1)] =
-                make_double2((dm1 * sb0 - d11 * st0) / det, (dm1 * sb1 - d11 * st1) / det);
-        }
-    } else {
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        for (int j = 1 + warp; j < m - 1; j += nw) {
-            double sl[4] = {0, 0, 0, 0};
-            for (int i = 1 + lane; i < m - 1; i += 32) {
-                const double2 v = U[i + (long long)m * j];
-                const double a = DC[(long long)m * i], b = DC[(m - 1) + (long long)m * i];
-                sl[0] += a * v.x; sl[1] += a * v.y; sl[2] += b * v.x; sl[3] += b * v.y;
+        part[warp][lane][0] = sb0; part[warp][lane][1] = sb1;
+        part[warp][lane][2] = st0; part[warp][lane][3] = st1;
+        __syncthreads();
+        if (warp == 0 && i < m - 1) {
+            for (int w = 1; w < 8; ++w) {
+                sb0 += part[w][lane][0]; sb1 += part[w][lane][1];
+                st0 += part[w][lane][2]; st1 += part[w][lane][3];
             }
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                for (int o = 16; o > 0; o >>= 1) sl[q] += __shfl_xor_sync(0xffffffffu, sl[q], o);
-            if (lane == 0) {
-                U[(long long)m * j] = make_double2((-dmm * sl[0] + d1m * sl[2]) / det, (-dmm * sl[1] + d1m * sl[3]) / det);
-                U[(m - 1) + (long long)m * j] = make_double2((dm1 * sl[0] - d11 * sl[2]) / det, (dm1 * sl[1] - d11 * sl[3]) / det);
-            }
+            U[i] = make_double2((-dmm * sb0 + d1m * st0) * idet, (-dmm * sb1 + d1m * st1) * idet);
+            U[i + (long long)m * (m - 1)] = make_double2((dm1 * sb0 - d11 * st0) * idet, (dm1 * sb1 - d11 * st1) * idet);
         }
     }
 }
@@ -573,13 +583,21 @@ int neumann_fill(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
     fp.io = ctx->neu.iofzero - 1;
     fp.gauge = ctx->gauge;
     fp.plane_stride = 2LL * ctx->my * ctx->my;
-    {
+    // the pin only acts on singular planes (|lambda| <= 1e-10, the kx=0
+    // pressure mode): launched only when the batch has one
+    bool any_singular = false;
+    for (int i = 0; i < ntasks && fp.io >= 0; ++i)
+        if (tasks[i].bound == 'n')
+            for (int k = 0; k < tasks[i].nmodes; ++k)
+                any_singular |= fabs(ctx->lam_host[tasks[i].plane0 + k]) <= 1.0e-10;
+    if (any_singular) {
         LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
         k_neumann_pin<<<cta, 1024, 0, ctx->stream>>>(fp);
     }
     {
+        const int n = ctx->my - 2, nyb = (n + 7) / 8, nzb = (n + 31) / 32;
         LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
-        k_neumann_walls<<<dim3(cta, 2), 256, 0, ctx->stream>>>(fp);
+        k_neumann_walls<<<dim3(cta, nyb + nzb), 256, 0, ctx->stream>>>(fp, nyb);
     }
     {
         LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
