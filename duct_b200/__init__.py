@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libductgpu.so")
 
 OK, EARG, ESTATE, ECUDA, ESOLVER, ENONFINITE, ETIMEOUT, EALLOC = range(8)
 PREC_FP64, PREC_MIXED = 0, 1
+PASS_STAGED, PASS_REGISTER, PASS_STAGED16 = 0, 1, 2
 GAUGE_POINT, GAUGE_MEAN = 0, 1
 
 EXPORTS = [
@@ -36,6 +37,7 @@ EXPORTS = [
     "ductgpu_impose_mass_flow_dev", "ductgpu_impose_mass_flow",
     "ductgpu_solve_adjoint_fields_dev", "ductgpu_helm3d_adjoint",
     "ductgpu_pseudopois", "ductgpu_solvepois", "ductgpu_solve_pois_fields_dev",
+    "ductgpu_set_pass_kernel", "ductgpu_autotune",
 ]
 K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
 
@@ -113,6 +115,8 @@ def lib():
             "ductgpu_solve_adjoint_fields_dev": [P, C.POINTER(Field), I],
             "ductgpu_helm3d_adjoint": [P, P, P, C.c_char, D, I, I, I, I, P],
             "ductgpu_pseudopois": [P, I],
+            "ductgpu_set_pass_kernel": [P, I, I],
+            "ductgpu_autotune": [P, C.POINTER(Field), I, I, C.POINTER(I)],
             "ductgpu_solvepois": [P, P, D, I],
             "ductgpu_solve_pois_fields_dev": [P, C.POINTER(Field), I],
             "ductgpu_graph_launch": [P, I],
@@ -226,6 +230,16 @@ class Context:
         P = np.asfortranarray(P, dtype=np.float64)
         PM1 = np.asfortranarray(PM1, dtype=np.float64)
         self._check(lib().ductgpu_set_operators(self.h, bound.encode(), _ptr(E), _ptr(P), _ptr(PM1), int(iofzero)))
+
+    def set_pass_kernel(self, kernel, size_class=-1):
+        self._check(lib().ductgpu_set_pass_kernel(self.h, int(size_class), int(kernel)))
+
+    def autotune(self, fields, reps=5):
+        """Pick the fastest pass kernel for these fields' size class; returns it."""
+        arr, keep = self._field_array(fields, False)
+        out = C.c_int()
+        self._check(lib().ductgpu_autotune(self.h, arr, len(fields), int(reps), C.byref(out)))
+        return out.value
 
     def set_refinement(self, steps):
         self._check(lib().ductgpu_set_refinement(self.h, int(steps)))

@@ -331,6 +331,49 @@ int ductgpu_set_refinement(ductgpu_ctx ctx, int steps)
     return DUCTGPU_OK;
 }
 
+int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (kernel != DUCTGPU_PASS_STAGED && kernel != DUCTGPU_PASS_REGISTER && kernel != DUCTGPU_PASS_STAGED16)
+        return set_error(ctx, DUCTGPU_EARG, "pass kernel %d", kernel);
+    if (size_class < -1 || size_class > 2) return set_error(ctx, DUCTGPU_EARG, "size class %d", size_class);
+    for (int c = 0; c < 3; ++c)
+        if (size_class < 0 || size_class == c) ctx->pass_variant[c] = kernel;
+    return DUCTGPU_OK;
+}
+
+int ductgpu_autotune(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, int reps, int *chosen)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (!ctx->ready) return set_error(ctx, DUCTGPU_ESTATE, "operators not set up (call ductgpu_pseudomat)");
+    if (ctx->capturing) return set_error(ctx, DUCTGPU_ESTATE, "autotune during graph capture");
+    if (reps < 1) reps = 5;
+    const int cls = (ctx->my - 2 + 63) / 64 - 1;
+    if (cls < 0 || cls > 2) return set_error(ctx, DUCTGPU_EARG, "grid %d", ctx->my);
+    const int variants[3] = {DUCTGPU_PASS_STAGED, DUCTGPU_PASS_STAGED16, DUCTGPU_PASS_REGISTER};
+    const int saved = ctx->pass_variant[cls];
+    const bool prof = ctx->prof_on;
+    ctx->prof_on = false;
+    float best_ms = 1e30f;
+    int best = saved, rc = DUCTGPU_OK;
+    for (int v : variants) {
+        ctx->pass_variant[cls] = v;
+        if ((rc = ductgpu_solve_fields_dev(ctx, fields, nfields, DUCTGPU_PREC_FP64))) break;   // warm-up
+        if ((rc = check_cuda(ctx, cudaEventRecord(ctx->ev[kNumEvents - 2], ctx->stream), "autotune"))) break;
+        for (int r = 0; r < reps && !rc; ++r) rc = ductgpu_solve_fields_dev(ctx, fields, nfields, DUCTGPU_PREC_FP64);
+        if (rc) break;
+        if ((rc = check_cuda(ctx, cudaEventRecord(ctx->ev[kNumEvents - 1], ctx->stream), "autotune"))) break;
+        if ((rc = check_cuda(ctx, cudaEventSynchronize(ctx->ev[kNumEvents - 1]), "autotune"))) break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[kNumEvents - 2], ctx->ev[kNumEvents - 1]);
+        if (ms < best_ms) { best_ms = ms; best = v; }
+    }
+    ctx->prof_on = prof;
+    ctx->pass_variant[cls] = rc ? saved : best;
+    if (chosen) *chosen = ctx->pass_variant[cls];
+    return rc;
+}
+
 int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, int precision)
 {
     if (!ctx) return DUCTGPU_EARG;

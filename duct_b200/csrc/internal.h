@@ -90,6 +90,12 @@ struct ductgpu_ctx_s {
     double wanted = 0.0;
     int gauge = DUCTGPU_GAUGE_POINT;
     int refine_steps = 2;      // FP64 refinement steps of the split-precision path
+    // GEMM-pass kernel per operator size class (n <= 63, <= 127, <= 191):
+    // DUCTGPU_PASS_STAGED or DUCTGPU_PASS_REGISTER (ductgpu_set_pass_kernel,
+    // ductgpu_autotune)
+    // defaults from measurements on B200 at n = 63, 127, 191 (cfg1 and
+    // config-4 sized batches); ductgpu_autotune re-picks them by timing
+    int pass_variant[3] = {DUCTGPU_PASS_STAGED16, DUCTGPU_PASS_STAGED, DUCTGPU_PASS_STAGED16};
     duct::BoundOps dir, neu;
 
     duct::RectSlot rect[duct::kMaxRect];

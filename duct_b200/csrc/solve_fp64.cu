@@ -54,10 +54,11 @@ __device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[8], con
 
 // MTW: 16-row tiles per warp along M of the launch (fields with smaller
 // operators skip the tiles they do not have).
-template <int MTW>
-__global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ PassParams p)
+template <int MTW, int LINES>
+__global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)) k_pass_fp64(const __grid_constant__ PassParams p)
 {
     extern __shared__ __align__(16) double smem[];
+    constexpr int NLD = 2 * LINES + 4, NTW = LINES / 8;
     constexpr int a_chunk_max = (kKC / 16) * (4 * MTW) * 256;
     double *As = smem;
     double *Bs = smem + 2 * a_chunk_max;
@@ -68,8 +69,8 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
     const int local = blockIdx.x - p.cta_start[fi];
     const int plane = local / F.nchunks;
     const int chunk = local - plane * F.nchunks;
-    const int l0 = chunk * kLines;
-    const int L = min(kLines, F.nlines - l0);
+    const int l0 = chunk * LINES;
+    const int L = min(LINES, F.nlines - l0);
     const double *src = F.src + (long long)plane * F.plane_stride;
     double *dst = F.dst + (long long)plane * F.plane_stride;
     const int tid = threadIdx.x;
@@ -88,31 +89,31 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
     // Stage the lines: Bs[k][2l + c] = in(k, l0 + l) component c, zero padded.
     const int n = F.n, sk = F.sk, sl = F.sl, o1 = F.off;
     if (sk == 1) {
-        for (int idx = tid; idx < kpad * kLines; idx += kThreads) {
+        for (int idx = tid; idx < kpad * LINES; idx += kThreads) {
             const int k = idx % kpad, l = idx / kpad;
             double2 v = make_double2(0.0, 0.0);
             if (k < n && l < L)
                 v = *reinterpret_cast<const double2 *>(src + 2 * ((long long)(k + o1) * sk + (long long)(l0 + l + o1) * sl));
-            *reinterpret_cast<double2 *>(Bs + k * kNld + 2 * l) = v;
+            *reinterpret_cast<double2 *>(Bs + k * NLD + 2 * l) = v;
         }
     } else {
-        for (int idx = tid; idx < kpad * kLines; idx += kThreads) {
-            const int l = idx % kLines, k = idx / kLines;
+        for (int idx = tid; idx < kpad * LINES; idx += kThreads) {
+            const int l = idx % LINES, k = idx / LINES;
             double2 v = make_double2(0.0, 0.0);
             if (k < n && l < L)
                 v = *reinterpret_cast<const double2 *>(src + 2 * ((long long)(k + o1) * sk + (long long)(l0 + l + o1) * sl));
-            *reinterpret_cast<double2 *>(Bs + k * kNld + 2 * l) = v;
+            *reinterpret_cast<double2 *>(Bs + k * NLD + 2 * l) = v;
         }
     }
 
     const int lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 3, wn = warp >> 2;
     const int g = lane >> 2, t = lane & 3;
-    double acc[MTW][4][4];
+    double acc[MTW][NTW][4];
 #pragma unroll
     for (int i = 0; i < MTW; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < NTW; ++j)
 #pragma unroll
             for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
 
@@ -128,12 +129,12 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
 #pragma unroll
         for (int ks = 0; ks < kKC / 16; ++ks) {
             const int kg = c * kKC + ks * 16 + t;
-            double b[4][4];
+            double b[NTW][4];
 #pragma unroll
-            for (int nt = 0; nt < 4; ++nt) {
-                const int col = wn * 32 + nt * 8 + g;
+            for (int nt = 0; nt < NTW; ++nt) {
+                const int col = wn * LINES + nt * 8 + g;
 #pragma unroll
-                for (int v = 0; v < 4; ++v) b[nt][v] = Bs[(kg + 4 * v) * kNld + col];
+                for (int v = 0; v < 4; ++v) b[nt][v] = Bs[(kg + 4 * v) * NLD + col];
             }
 #pragma unroll
             for (int mt = 0; mt < MTW; ++mt) {
@@ -148,7 +149,7 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
                     a[2 * h + 1] = v.y;
                 }
 #pragma unroll
-                for (int nt = 0; nt < 4; ++nt) dmma16(acc[mt][nt], a, b[nt]);
+                for (int nt = 0; nt < NTW; ++nt) dmma16(acc[mt][nt], a, b[nt]);
             }
         }
         __syncthreads();
@@ -162,8 +163,8 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
 #pragma unroll
     for (int mt = 0; mt < MTW; ++mt)
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-            const int l = wn * 16 + nt * 4 + t;
+        for (int nt = 0; nt < NTW; ++nt) {
+            const int l = wn * (LINES / 2) + nt * 4 + t;
             if (l >= L) continue;
             const int lg = l0 + l;
 #pragma unroll
@@ -196,20 +197,171 @@ __global__ void __launch_bounds__(kThreads) k_pass_fp64(const __grid_constant__ 
         }
 }
 
-static size_t pass_smem_bytes(int mtw, int kpad)
+// ---------------------------------------------------------------------------
+// Register-streamed variant: the CTA stages its 32 complex lines once, in
+// B-fragment order (so a lane's four k values are two contiguous 16-byte
+// words), and each warp then runs its whole K loop without a CTA barrier:
+// the operator fragments come straight from L2 (the packed operator is
+// 128 KB at n = 127 and stays resident) with a one-k-step register
+// prefetch.  WM warps along M own MT consecutive 16-row tiles each; the
+// 8 / WM warps along N own 8 / (8 / WM) of the 8 column tiles.
+// Packed B: index (((ks * 8 + nt) * 2 + half) * 32 + lane) * 2 + vv holds
+// B[ks*16 + t + 4 (2 half + vv)][nt*8 + g], lane = 4 g + t.
+template <int WM, int MT>
+__global__ void __launch_bounds__(kThreads, (MT == 1) ? 2 : 1) k_pass_fp64r(const __grid_constant__ PassParams p)
 {
-    const size_t a_chunk = (size_t)(kKC / 16) * (4 * mtw) * 256;
-    return (2 * a_chunk + (size_t)kpad * kNld) * sizeof(double);
+    extern __shared__ __align__(16) double smem[];
+    constexpr int WN = 8 / WM, NTW = 8 / WN;
+    double *Bp = smem;
+
+    int fi = 0;
+    while (fi + 1 < p.nf && (int)blockIdx.x >= p.cta_start[fi + 1]) ++fi;
+    const PassField &F = p.f[fi];
+    const int local = blockIdx.x - p.cta_start[fi];
+    const int plane = local / F.nchunks;
+    const int chunk = local - plane * F.nchunks;
+    const int l0 = chunk * kLines;
+    const int L = min(kLines, F.nlines - l0);
+    const double *src = F.src + (long long)plane * F.plane_stride;
+    double *dst = F.dst + (long long)plane * F.plane_stride;
+    const int tid = threadIdx.x;
+    const int kpad = F.kpad, mtiles = F.mtiles;
+    const int n = F.n, sk = F.sk, sl = F.sl, o1 = F.off;
+
+    // stage: element (k, line l) -> real columns 2l (re), 2l+1 (im)
+    for (int idx = tid; idx < kpad * kLines; idx += kThreads) {
+        int k, l;
+        if (sk == 1) { k = idx % kpad; l = idx / kpad; }
+        else { l = idx % kLines; k = idx / kLines; }
+        double2 v = make_double2(0.0, 0.0);
+        if (k < n && l < L)
+            v = *reinterpret_cast<const double2 *>(src + 2 * ((long long)(k + o1) * sk + (long long)(l0 + l + o1) * sl));
+        const int ks = k >> 4, kk = k & 15, t = kk & 3, vq = kk >> 2;
+        const int half = vq >> 1, vv = vq & 1;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int col = 2 * l + c, nt = col >> 3, g = col & 7;
+            Bp[((((ks * 8 + nt) * 2 + half) * 32 + (g * 4 + t)) * 2) + vv] = c ? v.y : v.x;
+        }
+    }
+    __syncthreads();
+
+    const int lane = tid & 31, warp = tid >> 5;
+    const int wm = warp % WM, wn = warp / WM;
+    const int g = lane >> 2, t = lane & 3;
+    double acc[MT][NTW][4];
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NTW; ++j)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+
+    const int nks = kpad >> 4;
+    auto load_a = [&](int ks, int mt, double (&a)[8]) {
+        const int mtg = wm * MT + mt;
+        if (mtg >= mtiles) return;
+        const double2 *q = reinterpret_cast<const double2 *>(F.A + ((size_t)(ks * mtiles + mtg) * 32 + lane) * 8);
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const double2 v = __ldg(q + h);
+            a[2 * h] = v.x;
+            a[2 * h + 1] = v.y;
+        }
+    };
+    double a_cur[MT][8], a_nxt[MT][8];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) load_a(0, mt, a_cur[mt]);
+    for (int ks = 0; ks < nks; ++ks) {
+        if (ks + 1 < nks) {
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) load_a(ks + 1, mt, a_nxt[mt]);
+        }
+#pragma unroll
+        for (int q = 0; q < NTW; ++q) {
+            const int nt = wn * NTW + q;
+            const double2 *bq = reinterpret_cast<const double2 *>(Bp + ((ks * 8 + nt) * 2) * 64) + lane;
+            const double2 b01 = bq[0], b23 = bq[32];
+            const double b[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                if (wm * MT + mt >= mtiles) continue;
+                dmma16(acc[mt][q], a_cur[mt], b);
+            }
+        }
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+            for (int v = 0; v < 8; ++v) a_cur[mt][v] = a_nxt[mt][v];
+    }
+
+    // epilogue as in k_pass_fp64: rows o of the accumulator, column pairs
+    // (2t, 2t+1) of tile nt = (re, im) of line 4 nt + t
+    const double lam = p.lam[F.plane0 + plane];
+    const bool singular = (F.sing_io >= 0) && fabs(lam) <= 1.0e-10;
+    const bool im0 = p.zero_im_mode0 && F.mode0 && plane == 0;
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+        for (int q = 0; q < NTW; ++q) {
+            const int l = (wn * NTW + q) * 4 + t;
+            if (l >= L) continue;
+            const int lg = l0 + l;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int o = (wm * MT + mt) * 16 + g + 8 * h;
+                if (o >= n) continue;
+                double re = acc[mt][q][2 * h], im = acc[mt][q][2 * h + 1];
+                if (p.divide) {
+                    if (singular && o == F.sing_io && lg == F.sing_l) {
+                        re = 0.0;
+                        im = 0.0;
+                    } else {
+                        const double den = (F.E[o] + F.El[lg]) - lam;
+                        re = re / den;
+                        im = im / den;
+                    }
+                }
+                const long long off = 2 * ((long long)(o + o1) * sk + (long long)(lg + o1) * sl);
+                if (p.residual) {
+                    const long long po = (long long)plane * F.plane_stride + off;
+                    const double2 f = *reinterpret_cast<const double2 *>(F.resF + po);
+                    const double2 tt = *reinterpret_cast<const double2 *>(F.resT + po);
+                    const double2 uu = *reinterpret_cast<const double2 *>(F.resU + po);
+                    re = (f.x - tt.x) - re + lam * uu.x;
+                    im = (f.y - tt.y) - im + lam * uu.y;
+                }
+                if (im0) im = 0.0;
+                *reinterpret_cast<double2 *>(dst + off) = make_double2(re, im);
+            }
+        }
 }
 
-template <int MTW>
-static cudaError_t launch_pass(ductgpu_ctx ctx, const PassParams &pp, int grid, int kpad_max)
+template <int WM, int MT>
+static cudaError_t launch_pass_r(ductgpu_ctx ctx, const PassParams &pp, int grid, int kpad_max)
 {
-    const size_t smem = pass_smem_bytes(MTW, kpad_max);
-    cudaError_t e = cudaFuncSetAttribute(k_pass_fp64<MTW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = (size_t)kpad_max * 64 * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(k_pass_fp64r<WM, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     LaunchScope ls(ctx, DUCTGPU_K_PASS_FP64);
-    k_pass_fp64<MTW><<<grid, kThreads, smem, ctx->stream>>>(pp);
+    k_pass_fp64r<WM, MT><<<grid, kThreads, smem, ctx->stream>>>(pp);
+    return cudaGetLastError();
+}
+
+static size_t pass_smem_bytes(int mtw, int kpad, int lines)
+{
+    const size_t a_chunk = (size_t)(kKC / 16) * (4 * mtw) * 256;
+    return (2 * a_chunk + (size_t)kpad * (2 * lines + 4)) * sizeof(double);
+}
+
+template <int MTW, int LINES>
+static cudaError_t launch_pass(ductgpu_ctx ctx, const PassParams &pp, int grid, int kpad_max)
+{
+    const size_t smem = pass_smem_bytes(MTW, kpad_max, LINES);
+    cudaError_t e = cudaFuncSetAttribute(k_pass_fp64<MTW, LINES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    LaunchScope ls(ctx, DUCTGPU_K_PASS_FP64);
+    k_pass_fp64<MTW, LINES><<<grid, kThreads, smem, ctx->stream>>>(pp);
     return cudaGetLastError();
 }
 
@@ -464,12 +616,36 @@ int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid)
         kpad_max = pp.f[i].kpad > kpad_max ? pp.f[i].kpad : kpad_max;
     }
     const int mtw = mt_max / 4;
+    if (mtw < 1 || mtw > 3) return set_error(ctx, DUCTGPU_EARG, "operator larger than %d", kMaxN);
+    const int variant = ctx->pass_variant[mtw - 1];
     cudaError_t e;
-    switch (mtw) {
-    case 1: e = launch_pass<1>(ctx, pp, grid, kpad_max); break;
-    case 2: e = launch_pass<2>(ctx, pp, grid, kpad_max); break;
-    case 3: e = launch_pass<3>(ctx, pp, grid, kpad_max); break;
-    default: return set_error(ctx, DUCTGPU_EARG, "operator larger than %d", kMaxN);
+    if (variant == DUCTGPU_PASS_REGISTER) {
+        switch (mtw) {
+        case 1: e = launch_pass_r<4, 1>(ctx, pp, grid, kpad_max); break;
+        case 2: e = launch_pass_r<8, 1>(ctx, pp, grid, kpad_max); break;
+        default: e = launch_pass_r<4, 3>(ctx, pp, grid, kpad_max); break;
+        }
+    } else if (variant == DUCTGPU_PASS_STAGED16) {
+        // 16 lines per CTA: the callers' grid is for 32; re-cut it
+        PassParams q = pp;
+        int cta = 0;
+        for (int i = 0; i < q.nf; ++i) {
+            q.f[i].nchunks = (q.f[i].nlines + 15) / 16;
+            q.cta_start[i] = cta;
+            cta += q.f[i].nmodes * q.f[i].nchunks;
+        }
+        q.cta_start[q.nf] = cta;
+        switch (mtw) {
+        case 1: e = launch_pass<1, 16>(ctx, q, cta, kpad_max); break;
+        case 2: e = launch_pass<2, 16>(ctx, q, cta, kpad_max); break;
+        default: e = launch_pass<3, 16>(ctx, q, cta, kpad_max); break;
+        }
+    } else {
+        switch (mtw) {
+        case 1: e = launch_pass<1, 32>(ctx, pp, grid, kpad_max); break;
+        case 2: e = launch_pass<2, 32>(ctx, pp, grid, kpad_max); break;
+        default: e = launch_pass<3, 32>(ctx, pp, grid, kpad_max); break;
+        }
     }
     return e == cudaSuccess ? DUCTGPU_OK : check_cuda(ctx, e, "k_pass_fp64");
 }

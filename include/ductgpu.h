@@ -120,6 +120,24 @@ typedef struct {
 int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields,
                              int nfields, int precision);
 
+/* GEMM-pass kernels of the FP64 solve (and of the residual passes):
+ * STAGED streams the operator through shared memory in 16-wide K chunks;
+ * REGISTER stages the data lines once and streams the operator from L2
+ * into registers with no CTA barrier in the K loop.  Chosen per operator
+ * size class (0: n <= 63, 1: n <= 127, 2: n <= 191); class -1 sets all.
+ * ductgpu_autotune picks them by timing.                                  */
+#define DUCTGPU_PASS_STAGED 0
+#define DUCTGPU_PASS_REGISTER 1
+#define DUCTGPU_PASS_STAGED16 2   /* STAGED with 16 lines per CTA (3 CTAs/SM) */
+int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel);
+/* Autotuner: times the FP64 batched solve of these device fields with each
+ * pass kernel (reps runs each, after one warm-up; the fields' sol arrays
+ * are overwritten and Dirichlet rhs walls zeroed, as by the solve itself)
+ * and keeps the fastest for the current grid's size class; *chosen (may be
+ * NULL) receives it.  Not during graph capture.                            */
+int ductgpu_autotune(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, int reps,
+                     int *chosen);
+
 /* No counterpart in the reference.  ductgpu_solve_fields_dev (FP64) for
  * callers that cannot allocate device memory -- a host code whose own pool
  * allocator has reserved the device, or one that runs several streams and
