@@ -46,6 +46,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-transforms", action="store_true")
+    ap.add_argument("--pass-kernel", default="auto", choices=["auto", "staged-32", "staged-16", "register"],
+                    help="GEMM-pass kernel; auto runs the library's autotuner (profiling runs fix it, since "
+                         "the autotuner's timing under a profiler is not the live one)")
+    ap.add_argument("--transforms-only", action="store_true",
+                    help="only the HBM-bound kernels (transyz, derivyz, transposes) on one GPU")
     return ap.parse_args()
 
 
@@ -210,8 +215,12 @@ def run_ours(args, world, rank, local, pg):
         sets.append(fl)
 
     # the library's autotuner picks the GEMM-pass kernel for this batch
-    pass_kernel = {D.PASS_STAGED: "staged-32", D.PASS_STAGED16: "staged-16",
-                   D.PASS_REGISTER: "register"}[ctx.autotune(sets[0], reps=5)]
+    names = {D.PASS_STAGED: "staged-32", D.PASS_STAGED16: "staged-16", D.PASS_REGISTER: "register"}
+    if args.pass_kernel == "auto":
+        pass_kernel = names[ctx.autotune(sets[0], reps=5)]
+    else:
+        pass_kernel = args.pass_kernel
+        ctx.set_pass_kernel({v: k for k, v in names.items()}[pass_kernel])
 
     def timed(prec):
         for i in range(args.warmup):
@@ -449,6 +458,11 @@ def main():
     if args.impl == "reference":
         # rank 0 alone times the CPU reference; other ranks exit without work
         run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
+    if args.transforms_only:
+        import duct_b200 as D
+        with D.Context(0) as ctx:
+            print(json.dumps(transform_rates(ctx)), flush=True)
         return
     world, rank, local, pg = dist_setup(args)
     try:
