@@ -204,6 +204,7 @@ int ductgpu_destroy(ductgpu_ctx ctx)
     cudaFree(ctx->xcol); cudaFree(ctx->DC); cudaFree(ctx->D2); cudaFree(ctx->AM1); cudaFree(ctx->ccw);
     cudaFree(ctx->work.buf);
     cudaFree(ctx->io.buf);
+    for (int i = 0; i < ductgpu_ctx_s::kTwTables; ++i) cudaFree(ctx->tw_tab[i]);
     cudaFree(ctx->dev_err);
     cudaFree(ctx->lam);
     cudaFreeHost(ctx->lam_host);

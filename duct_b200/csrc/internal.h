@@ -117,6 +117,10 @@ struct ductgpu_ctx_s {
     bool capturing = false;
     duct::Workspace work;      // pass intermediates
     duct::Workspace io;        // device copies for host entries
+    // W_L twiddle tables of the register-FFT transforms, one per length
+    static constexpr int kTwTables = 8;
+    int tw_len[kTwTables] = {};
+    void *tw_tab[kTwTables] = {};
     int *dev_err = nullptr;    // device error word (bounded waits)
     double *lam = nullptr;     // per-plane lambda (device)
     double *lam_host = nullptr;// pinned staging

@@ -183,6 +183,240 @@ __global__ void __launch_bounds__(256) k_dct(const __grid_constant__ DctParams p
 }
 
 // ---------------------------------------------------------------------------
+// Two-pass register FFT of the even extension, L = R1 * R2 (four-step):
+//   X[k1 + R1 k2] = sum_n2 W_R2^(n2 k2) W_L^(n2 k1) sum_n1 x[R2 n1 + n2] W_R1^(n1 k1)
+// Step 1: one thread per (line, n2) runs the R1-point DFT in registers and
+// applies W_L^(n2 k1); step 2: one thread per (line, k1) runs the R2-point
+// DFT.  Shared memory is touched once per step (reads and writes) instead
+// of once per radix stage.  The register DFTs are compile-time Stockham
+// sequences of radix 4, 3, 2 stages; their twiddles W_(Ns P)^(r k) come from
+// the W_L table (broadcast reads).
+template <int R>
+__host__ __device__ constexpr int reg_nstages()
+{
+    int n = 0, r = R;
+    while (r % 4 == 0) { r /= 4; ++n; }
+    while (r % 3 == 0) { r /= 3; ++n; }
+    while (r % 2 == 0) { r /= 2; ++n; }
+    return n;
+}
+template <int R>
+__host__ __device__ constexpr int reg_radix(int s)
+{
+    int r = R;
+    while (r % 4 == 0) { if (s == 0) return 4; r /= 4; --s; }
+    while (r % 3 == 0) { if (s == 0) return 3; r /= 3; --s; }
+    while (r % 2 == 0) { if (s == 0) return 2; r /= 2; --s; }
+    return 1;
+}
+
+template <int R, int S, int NS>
+__device__ __forceinline__ void reg_fft(double2 (&x)[R], const double2 *tw, int L)
+{
+    if constexpr (S < reg_nstages<R>()) {
+        constexpr int P = reg_radix<R>(S);
+        constexpr int NB = R / P;
+        double2 y[R];
+        const int tstep = L / (NS * P);
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            const int k = j % NS;
+            double2 v[4];
+#pragma unroll
+            for (int r = 0; r < P; ++r) v[r] = x[j + r * NB];
+            if (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < P; ++r) v[r] = cmul(v[r], tw[r * k * tstep]);
+            }
+            dft<P>(v);
+            const int d = (j / NS) * NS * P + k;
+#pragma unroll
+            for (int r = 0; r < P; ++r) y[d + r * NS] = v[r];
+        }
+#pragma unroll
+        for (int i = 0; i < R; ++i) x[i] = y[i];
+        reg_fft<R, S + 1, NS * P>(x, tw, L);
+    }
+}
+
+// One padded line buffer per line: point j lives at j + j / R2 (a pad word
+// after every R2 points), so the step-1 columns (stride R2) and the step-2
+// rows (R2 consecutive points) are both conflict-free, and both steps work
+// in place (step 1: each thread reads and writes its own column; step 2:
+// rows are read into registers before a barrier, then results written).
+template <int R1, int R2>
+__global__ void __launch_bounds__(256) k_dct2(const __grid_constant__ DctParams p, const double2 *__restrict__ twg)
+{
+    extern __shared__ __align__(16) double2 buf[];
+    constexpr int L = R1 * R2, LS = R1 * (R2 + 1);
+    constexpr int LPB = 256 / (R1 > R2 ? R1 : R2);   // lines per CTA (compile time: cheap index math)
+    const int N = p.nn - 1, nn = p.nn;
+    double2 *tw = buf;
+    double2 *x = buf + L;                       // [LPB][LS]
+    auto at = [](int j) { return j + j / R2; };
+    const int cpm = (p.lines_per_mode + LPB - 1) / LPB;
+    const int mode = blockIdx.x / cpm;
+    const int q0 = (blockIdx.x - mode * cpm) * LPB;
+    const int nl = min(LPB, p.lines_per_mode - q0);
+    double2 *g = reinterpret_cast<double2 *>(p.f) + mode * p.mode_stride + (long long)q0 * p.line_stride;
+    const bool contiguous = (p.elem_stride == 1);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // y-lines: a warp per line, lanes along the line; z-lines: consecutive
+    // threads on consecutive lines (l fastest), LPB a compile-time divisor
+    if (contiguous) {
+        for (int l = warp; l < nl; l += 8)
+            for (int j = lane; j < nn; j += 32) cp_async16(x + l * LS + at(j), g + l * p.line_stride + j);
+    } else {
+        for (int idx = threadIdx.x; idx < LPB * nn; idx += 256) {
+            const int j = idx / LPB, l = idx - j * LPB;
+            if (l < nl) cp_async16(x + l * LS + at(j), g + l + (long long)j * p.elem_stride);
+        }
+    }
+    for (int t = threadIdx.x; t < L; t += 256) cp_async16(tw + t, twg + t);
+    cp_async_wait_all();
+    __syncthreads();
+    const double si = (p.iopt >= 0) ? 0.5 : 1.0;
+    for (int l = warp; l < LPB; l += 8) {
+        double2 *xl = x + l * LS;
+        if (l < nl) {
+            for (int j = 1 + lane; j < N; j += 32) {
+                double2 v = xl[at(j)];
+                v = make_double2(si * v.x, si * v.y);
+                xl[at(j)] = v;
+                xl[at(L - j)] = v;
+            }
+        } else {
+            for (int j = lane; j < L; j += 32) xl[at(j)] = make_double2(0.0, 0.0);
+        }
+    }
+    __syncthreads();
+    // step 1: R1-point DFTs along n1 (column n2), twiddle W_L^(n2 k1), in place
+    {
+        const int l = threadIdx.x / R2, n2 = threadIdx.x - l * R2;
+        if (l < LPB) {
+            double2 *xl = x + l * LS;
+            double2 v[R1];
+#pragma unroll
+            for (int n1 = 0; n1 < R1; ++n1) v[n1] = xl[n1 * (R2 + 1) + n2];
+            reg_fft<R1, 0, 1>(v, tw, L);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; ++k1) xl[k1 * (R2 + 1) + n2] = (k1 == 0) ? v[0] : cmul(v[k1], tw[n2 * k1]);
+        }
+    }
+    __syncthreads();
+    // step 2: R2-point DFTs along row k1; results X[k1 + R1 k2] after a barrier
+    {
+        const int l = threadIdx.x / R1, k1 = threadIdx.x - l * R1;
+        const bool act = l < LPB;
+        double2 w[R2];
+        if (act) {
+            const double2 *xr = x + l * LS + k1 * (R2 + 1);
+#pragma unroll
+            for (int n2 = 0; n2 < R2; ++n2) w[n2] = xr[n2];
+            reg_fft<R2, 0, 1>(w, tw, L);
+        }
+        __syncthreads();
+        if (act) {
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) {
+                const int j = k1 + R1 * k2;
+                if (j <= N) x[l * LS + at(j)] = w[k2];
+            }
+        }
+    }
+    __syncthreads();
+    const double dn1 = 1.0 / (double)N, dn2 = 0.5 * dn1;
+    const bool fwd = p.iopt < 0;
+    if (contiguous) {
+        for (int l = warp; l < nl; l += 8)
+            for (int j = lane; j < nn; j += 32) {
+                double2 v = x[l * LS + at(j)];
+                if (fwd) {
+                    const double sc = (j == 0 || j == N) ? dn2 : dn1;
+                    v = make_double2(sc * v.x, sc * v.y);
+                }
+                g[l * p.line_stride + j] = v;
+            }
+    } else {
+        for (int idx = threadIdx.x; idx < LPB * nn; idx += 256) {
+            const int j = idx / LPB, l = idx - j * LPB;
+            if (l >= nl) continue;
+            double2 v = x[l * LS + at(j)];
+            if (fwd) {
+                const double sc = (j == 0 || j == N) ? dn2 : dn1;
+                v = make_double2(sc * v.x, sc * v.y);
+            }
+            g[l + (long long)j * p.elem_stride] = v;
+        }
+    }
+}
+
+__global__ void k_twiddles(int L, double2 *tw)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < L; t += gridDim.x * blockDim.x) {
+        double sn, cs;
+        sincospi(-2.0 * (double)t / (double)L, &sn, &cs);
+        tw[t] = make_double2(cs, sn);
+    }
+}
+
+// W_L table in device memory, one per length, kept in the context
+static const double2 *twiddle_table(ductgpu_ctx ctx, int L)
+{
+    for (int i = 0; i < ductgpu_ctx_s::kTwTables; ++i)
+        if (ctx->tw_len[i] == L) return reinterpret_cast<const double2 *>(ctx->tw_tab[i]);
+    for (int i = 0; i < ductgpu_ctx_s::kTwTables; ++i)
+        if (!ctx->tw_len[i]) {
+            if (ctx->capturing) return nullptr;     // no allocation inside a capture
+            if (cudaMalloc(&ctx->tw_tab[i], (size_t)L * sizeof(double2)) != cudaSuccess) return nullptr;
+            k_twiddles<<<(L + 255) / 256, 256, 0, ctx->stream>>>(L, reinterpret_cast<double2 *>(ctx->tw_tab[i]));
+            ctx->launches += 1;
+            ctx->tw_len[i] = L;
+            return reinterpret_cast<const double2 *>(ctx->tw_tab[i]);
+        }
+    return nullptr;
+}
+
+template <int R1, int R2>
+static int launch_dct2(ductgpu_ctx ctx, DctParams &p, int nmodes)
+{
+    constexpr int L = R1 * R2;
+    constexpr int RM = R1 > R2 ? R1 : R2;
+    const double2 *tw = twiddle_table(ctx, L);
+    if (!tw) return -1;                             // no table: the radix-stage kernel
+    p.lpb = 256 / RM;                               // the kernel's LPB
+    const size_t smem = ((size_t)L + (size_t)p.lpb * R1 * (R2 + 1)) * sizeof(double2);
+    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_dct2<R1, R2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int grid = nmodes * ((p.lines_per_mode + p.lpb - 1) / p.lpb);
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_TRANSFORM);
+        k_dct2<R1, R2><<<grid, 256, smem, ctx->stream>>>(p, tw);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "k_dct2");
+}
+
+// Register-FFT plans (R1 x R2 = L) for the line lengths in use; -1 if none.
+static int dct2_dispatch(ductgpu_ctx ctx, DctParams &p, int nmodes)
+{
+    switch (p.L) {
+    case 16: return launch_dct2<4, 4>(ctx, p, nmodes);
+    case 24: return launch_dct2<4, 6>(ctx, p, nmodes);
+    case 32: return launch_dct2<4, 8>(ctx, p, nmodes);
+    case 48: return launch_dct2<6, 8>(ctx, p, nmodes);
+    case 64: return launch_dct2<8, 8>(ctx, p, nmodes);
+    case 96: return launch_dct2<8, 12>(ctx, p, nmodes);
+    case 128: return launch_dct2<8, 16>(ctx, p, nmodes);
+    case 144: return launch_dct2<12, 12>(ctx, p, nmodes);
+    case 192: return launch_dct2<12, 16>(ctx, p, nmodes);
+    case 256: return launch_dct2<16, 16>(ctx, p, nmodes);
+    case 288: return launch_dct2<12, 24>(ctx, p, nmodes);
+    case 384: return launch_dct2<16, 24>(ctx, p, nmodes);
+    case 512: return launch_dct2<16, 32>(ctx, p, nmodes);
+    default: return -1;
+    }
+}
+
+// ---------------------------------------------------------------------------
 struct DerivParams {
     const double *u;
     double *du;
@@ -306,6 +540,12 @@ int transyz_dev(ductgpu_ctx ctx, double *f, int my, int mz, int nmodes, char cdi
     p.nstages = plan_radices(p.L, p.radix);
     if (p.nstages < 0)
         return set_error(ctx, DUCTGPU_EARG, "transyz: line length %d - 1 must be of the form 2^a 3^b", p.nn);
+    p.iopt = iopt;
+    // the two-pass register FFT where a plan exists, else the radix stages
+    {
+        const int rc = dct2_dispatch(ctx, p, nmodes);
+        if (rc >= 0) return rc;
+    }
     // lines per CTA: two line buffers + the twiddle table in ~100 KB, so
     // two CTAs share an SM
     p.lpb = (int)((100 * 1024 / sizeof(double2) - p.L) / (2 * (p.L + 1)));

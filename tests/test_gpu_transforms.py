@@ -17,7 +17,9 @@ def field(my, mz, nm, seed):
     return np.asfortranarray(rng.standard_normal((my, mz, nm)) + 1j * rng.standard_normal((my, mz, nm)))
 
 
-SHAPES = [(9, 17, 2), (33, 33, 3), (129, 65, 2), (193, 49, 2), (145, 33, 1), (65, 193, 1)]
+# line lengths 9..193 cover the register-FFT plans (2(n-1) = 16 ... 384);
+# 19 (2(n-1) = 36) has no plan and runs the radix-stage kernel
+SHAPES = [(9, 17, 2), (33, 33, 3), (129, 65, 2), (193, 49, 2), (145, 33, 1), (65, 193, 1), (19, 13, 2)]
 
 
 @pytest.mark.parametrize("my,mz,nm", SHAPES)
