@@ -335,7 +335,7 @@ int ductgpu_set_refinement(ductgpu_ctx ctx, int steps)
 int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel)
 {
     if (!ctx) return DUCTGPU_EARG;
-    if (kernel != DUCTGPU_PASS_STAGED && kernel != DUCTGPU_PASS_REGISTER && kernel != DUCTGPU_PASS_STAGED16)
+    if (kernel < DUCTGPU_PASS_STAGED || kernel > DUCTGPU_PASS_PERSIST)
         return set_error(ctx, DUCTGPU_EARG, "pass kernel %d", kernel);
     if (size_class < -1 || size_class > 2) return set_error(ctx, DUCTGPU_EARG, "size class %d", size_class);
     for (int c = 0; c < 3; ++c)
@@ -351,7 +351,7 @@ int ductgpu_autotune(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, 
     if (reps < 1) reps = 5;
     const int cls = (ctx->my - 2 + 63) / 64 - 1;
     if (cls < 0 || cls > 2) return set_error(ctx, DUCTGPU_EARG, "grid %d", ctx->my);
-    const int variants[3] = {DUCTGPU_PASS_STAGED, DUCTGPU_PASS_STAGED16, DUCTGPU_PASS_REGISTER};
+    const int variants[4] = {DUCTGPU_PASS_STAGED, DUCTGPU_PASS_STAGED16, DUCTGPU_PASS_REGISTER, DUCTGPU_PASS_PERSIST};
     const int saved = ctx->pass_variant[cls];
     const bool prof = ctx->prof_on;
     ctx->prof_on = false;

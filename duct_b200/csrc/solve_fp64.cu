@@ -348,6 +348,167 @@ static cudaError_t launch_pass_r(ductgpu_ctx ctx, const PassParams &pp, int grid
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Persistent variant for operators up to 128 rows (n <= 127): one CTA per
+// SM, 8 warps, each warp holding the A fragments of its 16-row tile for the
+// whole K extent in registers (KS x 8 doubles per lane, loaded once per
+// operator), looping over a contiguous range of 32-line tiles.  The next
+// tile's lines are copied into the other half of a double-buffered shared
+// memory tile with cp.async (zero-filled outside the field) while the
+// current one is multiplied, so the DMMA pipe only idles for the epilogue
+// and one barrier per tile.  MTILES 8: warp w owns rows 16w..16w+15 and all
+// 64 columns; MTILES 4: warps w and w+4 share rows 16(w&3).. and split the
+// columns.
+__device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, bool valid)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+
+template <int KS, int MTILES>
+__global__ void __launch_bounds__(kThreads, 1) k_pass_fp64p(const __grid_constant__ PassParams p, int ntiles)
+{
+    extern __shared__ __align__(16) double smem[];
+    constexpr int KPAD = 16 * KS, NTW = (MTILES == 8) ? 8 : 4;
+    constexpr int TILE = KPAD * kNld;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int mtg = (MTILES == 8) ? warp : (warp & 3);
+    const int ntb = (MTILES == 8) ? 0 : (warp >> 2) * 4;
+    // this CTA's contiguous tile range
+    const int per = ntiles / gridDim.x, extra = ntiles % gridDim.x;
+    const int t0 = blockIdx.x * per + min((int)blockIdx.x, extra);
+    const int t1 = t0 + per + ((int)blockIdx.x < extra ? 1 : 0);
+    if (t0 >= t1) return;
+
+    auto locate = [&](int tile, int &fi, int &plane, int &l0) {
+        fi = 0;
+        while (fi + 1 < p.nf && tile >= p.cta_start[fi + 1]) ++fi;
+        const int local = tile - p.cta_start[fi];
+        plane = local / p.f[fi].nchunks;
+        l0 = (local - plane * p.f[fi].nchunks) * kLines;
+    };
+    auto stage = [&](int tile, int buf) {
+        int fi, plane, l0;
+        locate(tile, fi, plane, l0);
+        const PassField &F = p.f[fi];
+        const int L = min(kLines, F.nlines - l0);
+        const double *src = F.src + (long long)plane * F.plane_stride;
+        double *Bs = smem + buf * TILE;
+        for (int idx = tid; idx < KPAD * kLines; idx += kThreads) {
+            int k, l;
+            if (F.sk == 1) { k = idx % KPAD; l = idx / KPAD; }
+            else { l = idx % kLines; k = idx / kLines; }
+            const bool ok = k < F.n && l < L;
+            const double *gp = ok ? src + 2 * ((long long)(k + F.off) * F.sk + (long long)(l0 + l + F.off) * F.sl) : src;
+            cp_async16_zfill(Bs + k * kNld + 2 * l, gp, ok);
+        }
+        cp_async_commit();
+    };
+
+    double a[KS][8];
+    const double *a_src = nullptr;
+    stage(t0, 0);
+    for (int tile = t0; tile < t1; ++tile) {
+        const int buf = (tile - t0) & 1;
+        if (tile + 1 < t1) {
+            stage(tile + 1, buf ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        int fi, plane, l0;
+        locate(tile, fi, plane, l0);
+        const PassField &F = p.f[fi];
+        if (F.A != a_src) {   // operator of this field: fragments into registers
+            a_src = F.A;
+#pragma unroll
+            for (int ks = 0; ks < KS; ++ks) {
+                const double2 *q = reinterpret_cast<const double2 *>(F.A + ((size_t)(ks * MTILES + mtg) * 32 + lane) * 8);
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const double2 v = __ldg(q + h);
+                    a[ks][2 * h] = v.x;
+                    a[ks][2 * h + 1] = v.y;
+                }
+            }
+        }
+        const double *Bs = smem + buf * TILE;
+        double acc[NTW][4];
+#pragma unroll
+        for (int q = 0; q < NTW; ++q)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[q][v] = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) {
+            const int kg = ks * 16 + t;
+#pragma unroll
+            for (int q = 0; q < NTW; ++q) {
+                const int col = (ntb + q) * 8 + g;
+                double b[4];
+#pragma unroll
+                for (int v = 0; v < 4; ++v) b[v] = Bs[(kg + 4 * v) * kNld + col];
+                dmma16(acc[q], a[ks], b);
+            }
+        }
+        // epilogue (as k_pass_fp64)
+        const int L = min(kLines, F.nlines - l0);
+        double *dst = F.dst + (long long)plane * F.plane_stride;
+        const double lam = p.lam[F.plane0 + plane];
+        const bool singular = (F.sing_io >= 0) && fabs(lam) <= 1.0e-10;
+        const bool im0 = p.zero_im_mode0 && F.mode0 && plane == 0;
+        const int n = F.n, sk = F.sk, sl = F.sl, o1 = F.off;
+#pragma unroll
+        for (int q = 0; q < NTW; ++q) {
+            const int l = (ntb + q) * 4 + t;
+            if (l >= L) continue;
+            const int lg = l0 + l;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int o = mtg * 16 + g + 8 * h;
+                if (o >= n) continue;
+                double re = acc[q][2 * h], im = acc[q][2 * h + 1];
+                if (p.divide) {
+                    if (singular && o == F.sing_io && lg == F.sing_l) {
+                        re = 0.0;
+                        im = 0.0;
+                    } else {
+                        const double den = (F.E[o] + F.El[lg]) - lam;
+                        re = re / den;
+                        im = im / den;
+                    }
+                }
+                const long long off = 2 * ((long long)(o + o1) * sk + (long long)(lg + o1) * sl);
+                if (p.residual) {
+                    const long long po = (long long)plane * F.plane_stride + off;
+                    const double2 f = *reinterpret_cast<const double2 *>(F.resF + po);
+                    const double2 tt = *reinterpret_cast<const double2 *>(F.resT + po);
+                    const double2 uu = *reinterpret_cast<const double2 *>(F.resU + po);
+                    re = (f.x - tt.x) - re + lam * uu.x;
+                    im = (f.y - tt.y) - im + lam * uu.y;
+                }
+                if (im0) im = 0.0;
+                *reinterpret_cast<double2 *>(dst + off) = make_double2(re, im);
+            }
+        }
+        __syncthreads();   // the buffer is refilled by the next iteration's stage
+    }
+}
+
+template <int KS, int MTILES>
+static cudaError_t launch_pass_p(ductgpu_ctx ctx, const PassParams &pp, int ntiles)
+{
+    const size_t smem = 2 * (size_t)16 * KS * kNld * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(k_pass_fp64p<KS, MTILES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = ntiles < ctx->num_sms ? ntiles : ctx->num_sms;
+    LaunchScope ls(ctx, DUCTGPU_K_PASS_FP64);
+    k_pass_fp64p<KS, MTILES><<<grid, kThreads, smem, ctx->stream>>>(pp, ntiles);
+    return cudaGetLastError();
+}
+
 static size_t pass_smem_bytes(int mtw, int kpad, int lines)
 {
     const size_t a_chunk = (size_t)(kKC / 16) * (4 * mtw) * 256;
@@ -619,7 +780,23 @@ int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid)
     if (mtw < 1 || mtw > 3) return set_error(ctx, DUCTGPU_EARG, "operator larger than %d", kMaxN);
     const int variant = ctx->pass_variant[mtw - 1];
     cudaError_t e;
-    if (variant == DUCTGPU_PASS_REGISTER) {
+    bool uniform = true;
+    for (int i = 1; i < pp.nf; ++i)
+        uniform = uniform && pp.f[i].kpad == pp.f[0].kpad && pp.f[i].mtiles == pp.f[0].mtiles;
+    if (variant == DUCTGPU_PASS_PERSIST && uniform && (pp.f[0].mtiles == 4 || pp.f[0].mtiles == 8)) {
+        const int ks = pp.f[0].kpad / 16;
+        if (pp.f[0].mtiles == 8) {
+            switch (ks) {
+            case 6: e = launch_pass_p<6, 8>(ctx, pp, grid); break;
+            default: e = launch_pass_p<8, 8>(ctx, pp, grid); break;
+            }
+        } else {
+            switch (ks) {
+            case 2: e = launch_pass_p<2, 4>(ctx, pp, grid); break;
+            default: e = launch_pass_p<4, 4>(ctx, pp, grid); break;
+            }
+        }
+    } else if (variant == DUCTGPU_PASS_REGISTER) {
         switch (mtw) {
         case 1: e = launch_pass_r<4, 1>(ctx, pp, grid, kpad_max); break;
         case 2: e = launch_pass_r<8, 1>(ctx, pp, grid, kpad_max); break;

@@ -129,6 +129,7 @@ int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields,
 #define DUCTGPU_PASS_STAGED 0
 #define DUCTGPU_PASS_REGISTER 1
 #define DUCTGPU_PASS_STAGED16 2   /* STAGED with 16 lines per CTA (3 CTAs/SM) */
+#define DUCTGPU_PASS_PERSIST 3    /* persistent, operator in registers (n <= 127) */
 int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel);
 /* Autotuner: times the FP64 batched solve of these device fields with each
  * pass kernel (reps runs each, after one warm-up; the fields' sol arrays

@@ -9,7 +9,7 @@ import duct_b200 as D
 from duct_b200 import synth
 
 pytestmark = pytest.mark.gpu
-VARIANTS = [D.PASS_STAGED, D.PASS_STAGED16, D.PASS_REGISTER]
+VARIANTS = [D.PASS_STAGED, D.PASS_STAGED16, D.PASS_REGISTER, D.PASS_PERSIST]
 
 
 def fields_for(ctx, m, nm):
