@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed", "int8"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-transforms", action="store_true")
@@ -246,14 +246,21 @@ def run_ours(args, world, rank, local, pg):
         barrier(pg)
         return ms / args.steps, launches, prof, clk
 
-    want = ["fp64", "mixed"] if args.precision == "auto" else [args.precision]
+    want = ["fp64", "mixed", "int8"] if args.precision == "auto" else [args.precision]
     res = {}
     for name in want:
-        prec = D.PREC_FP64 if name == "fp64" else D.PREC_MIXED
+        prec = {"fp64": D.PREC_FP64, "mixed": D.PREC_MIXED, "int8": D.PREC_INT8}[name]
         ms_step, launches, prof, clk = timed(prec)
         res[name] = dict(ms_step=ms_step, launches=launches, prof=prof, clk=clk,
                          value=world * per_step / (ms_step * 1e-3))
     # accuracy of the split path against the FP64 path on the same operators
+    acc8 = None
+    if "int8" in res and "fp64" in res:
+        ctx.solve_fields_dev(sets[0], D.PREC_FP64)
+        ref8 = [f["sol"].download() for f in sets[0]]
+        ctx.solve_fields_dev(sets[0], D.PREC_INT8)
+        acc8 = {name: float(np.linalg.norm(f["sol"].download() - r) / np.linalg.norm(r))
+                for (name, _, _), f, r in zip(c["fields"], sets[0], ref8)}
     acc = None
     if "mixed" in res and "fp64" in res:
         ctx.solve_fields_dev(sets[0], D.PREC_FP64)
@@ -282,6 +289,19 @@ def run_ours(args, world, rank, local, pg):
                            "traffic": traffic_from_profile("k_pass_fp64"),
                            "kernel": "k_pass_fp64 (FP64 DMMA m16n8k16)", "peak_source": peak64_note,
                            "kernel_share_of_step": kms / (R["ms_step"] * args.steps)}
+        elif name == "int8":
+            kms, kn = R["prof"][D.K_MIXED_GEMM]
+            # per launch: 28 slice products of the padded 128 x 128 operator
+            # against 256 real columns (128 padded lines x re/im) per plane
+            ops = 28 * 2.0 * 128 * 128 * 256 * per_step
+            ach = ops / ((kms / kn) * 1e-3) / 1e12 if kn else None
+            roofs[name] = {"bound": "tensor", "achieved": ach, "peak": 4500.0, "unit": "TOPS (int8)",
+                           "frac": (ach / 4500.0) if ach else None,
+                           "traffic": None,
+                           "kernel": "k_pass_i8 (tcgen05 kind::i8, 28 slice products, exact int32)",
+                           "peak_source": "nominal dense int8 (no measured int8 peak on this pool)",
+                           "fp64_equiv_tflops": (4.0 * n ** 3 * per_step) / ((kms / kn) * 1e-3) / 1e12 if kn else None,
+                           "kernel_share_of_step": kms / (R["ms_step"] * args.steps)}
         else:
             kms, kn = R["prof"][D.K_MIXED_GEMM]
             flops = 10 * 4.0 * n ** 3 * per_step     # 10 BF16 slice products per pass
@@ -295,7 +315,7 @@ def run_ours(args, world, rank, local, pg):
 
     e2e = None
     if not args.no_e2e:
-        prec = D.PREC_FP64 if best == "fp64" else D.PREC_MIXED
+        prec = {"fp64": D.PREC_FP64, "mixed": D.PREC_MIXED, "int8": D.PREC_INT8}[best]
         e2e = measure_e2e(ctx, c, m, nm, xalp, rhs, prec, args, pg, world)
 
     hbm = transform_rates(ctx) if (rank == 0 and not args.no_transforms) else None
@@ -316,7 +336,7 @@ def run_ours(args, world, rank, local, pg):
             "metric": METRIC, "value": B["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": B["ms_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if best == "fp64" else "bf16-split+f64-refine",
+            "dtype": {"fp64": "f64", "mixed": "bf16-split+f64-refine", "int8": "int8-split (7x7 slices, exact int32)"}[best],
             "data": "synthetic (seeded splitmix64 Chebyshev-coefficient RHS)",
             "config": {"workload": WORKLOAD, "mode_solves_per_step": per_step,
                        "precision": best,
@@ -328,6 +348,7 @@ def run_ours(args, world, rank, local, pg):
             "paths": {k: {"value": v["value"], "ms_per_step": v["ms_step"], "roofline": roofs[k],
                           "gpu_launches": v["launches"]} for k, v in res.items()},
             "mixed_rel_err_vs_fp64": acc,
+            "int8_rel_err_vs_fp64": acc8,
             "hbm_kernels": hbm,
         }
         print(json.dumps(line), flush=True)

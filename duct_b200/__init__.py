@@ -15,7 +15,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libductgpu.so")
 
 OK, EARG, ESTATE, ECUDA, ESOLVER, ENONFINITE, ETIMEOUT, EALLOC = range(8)
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_INT8 = 0, 1, 2
 PASS_STAGED, PASS_REGISTER, PASS_STAGED16, PASS_PERSIST = 0, 1, 2, 3
 GAUGE_POINT, GAUGE_MEAN = 0, 1
 

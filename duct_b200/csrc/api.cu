@@ -381,7 +381,7 @@ int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields, int n
     if (!ctx->ready) return set_error(ctx, DUCTGPU_ESTATE, "operators not set up (call ductgpu_pseudomat)");
     if (!fields || nfields < 1 || nfields > kMaxFields)
         return set_error(ctx, DUCTGPU_EARG, "nfields=%d (1..%d)", nfields, kMaxFields);
-    if (precision != DUCTGPU_PREC_FP64 && precision != DUCTGPU_PREC_MIXED)
+    if (precision != DUCTGPU_PREC_FP64 && precision != DUCTGPU_PREC_MIXED && precision != DUCTGPU_PREC_INT8)
         return set_error(ctx, DUCTGPU_EARG, "precision %d", precision);
     for (int i = 0; i < nfields; ++i) {
         int rc = validate_field(ctx, fields[i]);
@@ -392,6 +392,11 @@ int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields, int n
     int rc = prepare(ctx, fields, nfields, tasks);
     if (rc) return rc;
     if (precision == DUCTGPU_PREC_MIXED) return solve_mixed(ctx, tasks, nfields);
+    if (precision == DUCTGPU_PREC_INT8) {
+        if (ctx->my - 2 > 127)
+            return set_error(ctx, DUCTGPU_EARG, "int8-emulated solve: my=%d (at most 129)", ctx->my);
+        return solve_fp64_ex(ctx, tasks, nfields, true);
+    }
     return solve_fp64(ctx, tasks, nfields);
 }
 
@@ -444,7 +449,7 @@ int ductgpu_helm3d(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, char bou
     if (rc) return rc;
     DUCT_CUDA(ctx, cudaMemcpyAsync(sol, dsol, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d");
-    return rc ? rc : (precision == DUCTGPU_PREC_MIXED ? device_status(ctx) : DUCTGPU_OK);
+    return rc ? rc : (precision != DUCTGPU_PREC_FP64 ? device_status(ctx) : DUCTGPU_OK);
 }
 
 static int check_field(ductgpu_ctx ctx, const void *a, int my, int mz, int nmodes)

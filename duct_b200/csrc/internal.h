@@ -39,6 +39,8 @@ struct BoundOps {
     double *PTpack = nullptr, *QTpack = nullptr;  // P^T, P^-T packed (adjoint; built on first use)
     uint8_t *Pslices = nullptr, *Qslices = nullptr;  // BF16 slices (mixed)
     int *Pexp = nullptr, *Qexp = nullptr;            // per-row exponents
+    int8_t *Pi8 = nullptr, *Qi8 = nullptr;          // int8 slices (int8-emulated FP64)
+    int *Pexp8 = nullptr, *Qexp8 = nullptr;
 };
 
 // Operators of one rectangular duct shape (src/pseudomat_temp.f90): y and z
@@ -90,6 +92,7 @@ struct ductgpu_ctx_s {
     double wanted = 0.0;
     int gauge = DUCTGPU_GAUGE_POINT;
     int refine_steps = 2;      // FP64 refinement steps of the split-precision path
+    int i8_kernel = 1;         // int8-emulated passes: 0 sequential, 1 warp-specialised pipeline
     // GEMM-pass kernel per operator size class (n <= 63, <= 127, <= 191):
     // DUCTGPU_PASS_STAGED or DUCTGPU_PASS_REGISTER (ductgpu_set_pass_kernel,
     // ductgpu_autotune)
@@ -177,6 +180,8 @@ struct FieldTask {
     int refine;       // FP64 refinement steps for the split-precision path
 };
 int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
+// emulate: every GEMM pass as int8 slice products on tcgen05 (solve_i8.cu)
+int solve_fp64_ex(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks, bool emulate);
 // adjoint.cu: the transpose of solve_fp64's map rhs -> sol; task.rhs is the
 // cotangent of sol (read only), task.sol receives the cotangent of rhs
 int solve_adjoint(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
@@ -186,6 +191,8 @@ struct PassField {
     const double *src;
     double *dst;
     const double *A;     // packed operator (n x n, fragment order)
+    const int8_t *Ai8;   // int8 operator slices (int8-emulated passes), or null
+    const int *Aexp;     // per-row exponents of Ai8
     const double *E;     // eigenvalues along the pass direction (divide)
     const double *El;    // eigenvalues along the line direction (divide)
     int nmodes;
@@ -249,6 +256,9 @@ int solve_rect(ductgpu_ctx ctx, const RectTask *tasks, int ntasks);
 
 // solve_mixed.cu
 int split_operator(ductgpu_ctx ctx, int n, const double *A, uint8_t **slices, int **rexp);
+// solve_i8.cu
+int split_operator_i8(ductgpu_ctx ctx, int n, const double *A, int8_t **slices, int **rexp);
+int i8_pass(ductgpu_ctx ctx, const PassParams &pp, int grid);
 int solve_mixed(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
 int zero_walls(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
 int neumann_fill(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);

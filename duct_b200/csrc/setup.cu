@@ -185,6 +185,7 @@ void free_bound(BoundOps &b)
     cudaFree(b.Ppack); cudaFree(b.Qpack); cudaFree(b.pcol); cudaFree(b.qrow);
     cudaFree(b.D2B); cudaFree(b.Bpack); cudaFree(b.PTpack); cudaFree(b.QTpack);
     cudaFree(b.Pslices); cudaFree(b.Qslices); cudaFree(b.Pexp); cudaFree(b.Qexp);
+    cudaFree(b.Pi8); cudaFree(b.Qi8); cudaFree(b.Pexp8); cudaFree(b.Qexp8);
     b = BoundOps();
 }
 
@@ -216,6 +217,8 @@ int pack_operators(ductgpu_ctx ctx, BoundOps &b)
         int rc = split_operator(ctx, n, b.P, &b.Pslices, &b.Pexp);
         if (rc) return rc;
         if ((rc = split_operator(ctx, n, b.PM1, &b.Qslices, &b.Qexp))) return rc;
+        if ((rc = split_operator_i8(ctx, n, b.P, &b.Pi8, &b.Pexp8))) return rc;
+        if ((rc = split_operator_i8(ctx, n, b.PM1, &b.Qi8, &b.Qexp8))) return rc;
     }
     if (b.iofzero > 0) {
         if (!b.pcol) DUCT_CUDA(ctx, cudaMalloc(&b.pcol, n * sizeof(double)));

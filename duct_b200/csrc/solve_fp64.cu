@@ -840,7 +840,9 @@ static int pass_grid(PassParams &pp, const FieldTask *tasks, int ntasks)
     return cta;
 }
 
-int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
+int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks) { return solve_fp64_ex(ctx, tasks, ntasks, false); }
+
+int solve_fp64_ex(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks, bool emulate)
 {
     if (ntasks < 1 || ntasks > kMaxFields)
         return set_error(ctx, DUCTGPU_EARG, "solve: %d fields (1..%d)", ntasks, kMaxFields);
@@ -876,13 +878,15 @@ int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
             case 2: pp.f[i].src = a2; pp.f[i].dst = a1; pp.f[i].A = b.Ppack; break;
             default: pp.f[i].src = a1; pp.f[i].dst = tasks[i].sol; pp.f[i].A = b.Ppack; break;
             }
+            pp.f[i].Ai8 = (pass < 2) ? b.Qi8 : b.Pi8;
+            pp.f[i].Aexp = (pass < 2) ? b.Qexp8 : b.Pexp8;
             pass_geometry(pp.f[i], b, b.E, n, ypass ? 1 : m, ypass ? m : 1, ps);
         }
         const int cta = pass_grid(pp, tasks, ntasks);
         pp.divide = (pass == 1);
         pp.zero_im_mode0 = (pass == 3);
         pp.residual = 0;
-        if ((rc = fp64_pass(ctx, pp, cta))) return rc;
+        if ((rc = emulate ? i8_pass(ctx, pp, cta) : fp64_pass(ctx, pp, cta))) return rc;
     }
     if ((rc = zero_walls(ctx, tasks, ntasks))) return rc;
     return neumann_fill(ctx, tasks, ntasks);

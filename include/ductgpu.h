@@ -40,6 +40,8 @@ typedef struct ductgpu_ctx_s *ductgpu_ctx;
 /* arithmetic of the solve */
 #define DUCTGPU_PREC_FP64 0  /* plain FP64 (DMMA tensor cores): the drop-in  */
 #define DUCTGPU_PREC_MIXED 1 /* BF16 split GEMMs + FP64 refinement           */
+#define DUCTGPU_PREC_INT8 2  /* FP64-accurate: every GEMM pass as 7 x 7 int8   
+                                slices on tcgen05, exact int32 sums (my<=129) */
 
 /* gauge of the singular kx=0 Neumann (pressure) mode */
 #define DUCTGPU_GAUGE_POINT 0 /* reference: U(iofzero+1,iofzero+1)=wanted=0 */
