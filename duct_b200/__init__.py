@@ -37,7 +37,7 @@ EXPORTS = [
     "ductgpu_impose_mass_flow_dev", "ductgpu_impose_mass_flow",
     "ductgpu_solve_adjoint_fields_dev", "ductgpu_helm3d_adjoint",
     "ductgpu_pseudopois", "ductgpu_solvepois", "ductgpu_solve_pois_fields_dev",
-    "ductgpu_set_pass_kernel", "ductgpu_autotune",
+    "ductgpu_set_pass_kernel", "ductgpu_autotune", "ductgpu_helm3d_batch",
 ]
 K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
 
@@ -117,6 +117,7 @@ def lib():
             "ductgpu_pseudopois": [P, I],
             "ductgpu_set_pass_kernel": [P, I, I],
             "ductgpu_autotune": [P, C.POINTER(Field), I, I, C.POINTER(I)],
+            "ductgpu_helm3d_batch": [P, I, P, P, C.c_char_p, P, I, I, I, I, P, I],
             "ductgpu_solvepois": [P, P, D, I],
             "ductgpu_solve_pois_fields_dev": [P, C.POINTER(Field), I],
             "ductgpu_graph_launch": [P, I],
@@ -337,6 +338,23 @@ class Context:
         self._check(lib().ductgpu_impose_mass_flow_dev(self.h, C.byref(cs), int(krk), C.c_void_p(u.ptr),
                                                        int(iflag)))
         return cs.value
+
+    def helm3d_batch(self, rhss, bounds, alambdas, xalp, ib=0, precision=PREC_FP64):
+        """Several helm3d fields on host arrays in one pipelined call; the
+        rhs arrays are modified in place like helm3d's.  Returns the sols."""
+        sols = [np.zeros_like(r, order="F") for r in rhss]
+        for r in rhss:
+            assert r.dtype == np.complex128 and r.flags.f_contiguous and r.shape == rhss[0].shape
+        my, mz, nm = rhss[0].shape
+        n = len(rhss)
+        pr = (C.c_void_p * n)(*[r.ctypes.data for r in rhss])
+        ps = (C.c_void_p * n)(*[s_.ctypes.data for s_ in sols])
+        lam = np.ascontiguousarray(alambdas, dtype=np.float64)
+        xalp = np.ascontiguousarray(xalp, dtype=np.float64)
+        self._check(lib().ductgpu_helm3d_batch(self.h, n, C.cast(pr, C.c_void_p), C.cast(ps, C.c_void_p),
+                                               "".join(bounds).encode(), _ptr(lam), my, mz, int(ib),
+                                               int(ib) + nm - 1, _ptr(xalp), int(precision)))
+        return sols
 
     def pseudomat_temp(self, slot, my, mz, sy=1.0, sz=1.0, by=("d", "d"), bz=("d", "d")):
         self._check(lib().ductgpu_pseudomat_temp(self.h, int(slot), int(my), int(mz), float(sy), float(sz),

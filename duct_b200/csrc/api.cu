@@ -204,6 +204,16 @@ int ductgpu_destroy(ductgpu_ctx ctx)
     cudaFree(ctx->xcol); cudaFree(ctx->DC); cudaFree(ctx->D2); cudaFree(ctx->AM1); cudaFree(ctx->ccw);
     cudaFree(ctx->work.buf);
     cudaFree(ctx->io.buf);
+    if (ctx->cp_in) {
+        cudaStreamSynchronize(ctx->cp_in);
+        cudaStreamSynchronize(ctx->cp_out);
+        for (int i = 0; i < ductgpu_ctx_s::kPipeChunks; ++i) {
+            cudaEventDestroy(ctx->ev_in[i]);
+            cudaEventDestroy(ctx->ev_out[i]);
+        }
+        cudaStreamDestroy(ctx->cp_in);
+        cudaStreamDestroy(ctx->cp_out);
+    }
     for (int i = 0; i < ductgpu_ctx_s::kTwTables; ++i) cudaFree(ctx->tw_tab[i]);
     cudaFree(ctx->dev_err);
     cudaFree(ctx->lam);
@@ -436,7 +446,6 @@ int ductgpu_helm3d(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, char bou
     int rc = ensure(ctx, ctx->io, 2 * bytes);
     if (rc) return rc;
     double *drhs = ctx->io.buf, *dsol = ctx->io.buf + bytes / sizeof(double);
-    DUCT_CUDA(ctx, cudaMemcpyAsync(drhs, rhs, bytes, cudaMemcpyHostToDevice, ctx->stream));
     ductgpu_field f;
     f.rhs = drhs;
     f.sol = dsol;
@@ -445,10 +454,84 @@ int ductgpu_helm3d(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, char bou
     f.ib = ib;
     f.nmodes = nm;
     f.bound = bound;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(drhs, rhs, bytes, cudaMemcpyHostToDevice, ctx->stream));
     rc = ductgpu_solve_fields_dev(ctx, &f, 1, precision);
     if (rc) return rc;
     DUCT_CUDA(ctx, cudaMemcpyAsync(sol, dsol, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d");
+    return rc ? rc : (precision != DUCTGPU_PREC_FP64 ? device_status(ctx) : DUCTGPU_OK);
+}
+
+// Several fields of one substep on host arrays (u, v, w and p of
+// src/main1.f90:617-619, 643), with the host<->device copies overlapped:
+// field i is copied in on one stream while field i-1 is solved on the
+// context stream and field i-2 copied back on a third.  Each solve is the
+// whole field's batch.  From pinned host memory (ductgpu_host_alloc) the
+// copies run asynchronously; pageable memory gives the same results.
+int ductgpu_helm3d_batch(ductgpu_ctx ctx, int nfields, double *const *rhs, double *const *sol, const char *bounds,
+                         const double *alambdas, int my, int mz, int ib, int ie, const double *xalp, int precision)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (!ctx->ready) return set_error(ctx, DUCTGPU_ESTATE, "operators not set up (call ductgpu_pseudomat)");
+    if (nfields < 1 || nfields > kMaxFields || !rhs || !sol || !bounds || !alambdas || !xalp)
+        return set_error(ctx, DUCTGPU_EARG, "helm3d_batch: nfields=%d or null argument", nfields);
+    if (my != ctx->my || mz != ctx->mz)
+        return set_error(ctx, DUCTGPU_EARG, "grid %dx%d differs from the set-up %dx%d", my, mz, ctx->my, ctx->mz);
+    if (ie < ib || ib < 0) return set_error(ctx, DUCTGPU_EARG, "ib=%d ie=%d", ib, ie);
+    if (precision != DUCTGPU_PREC_FP64 && precision != DUCTGPU_PREC_INT8 && precision != DUCTGPU_PREC_MIXED)
+        return set_error(ctx, DUCTGPU_EARG, "precision %d", precision);
+    for (int i = 0; i < nfields; ++i) {
+        if (!rhs[i] || !sol[i]) return set_error(ctx, DUCTGPU_EARG, "null field %d", i);
+        if (bounds[i] != 'd' && bounds[i] != 'n') return set_error(ctx, DUCTGPU_EARG, "bound '%c'", bounds[i]);
+    }
+    cudaSetDevice(ctx->device);
+    if (!ctx->cp_in) {
+        DUCT_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->cp_in, cudaStreamNonBlocking));
+        DUCT_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->cp_out, cudaStreamNonBlocking));
+        for (int i = 0; i < ductgpu_ctx_s::kPipeChunks; ++i) {
+            DUCT_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_in[i], cudaEventDisableTiming));
+            DUCT_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_out[i], cudaEventDisableTiming));
+        }
+    }
+    const int nm = ie - ib + 1;
+    const size_t doubles = (size_t)2 * my * mz * nm, bytes = doubles * sizeof(double);
+    int rc = ensure(ctx, ctx->io, 2 * bytes * nfields);
+    if (rc) return rc;
+    // helm3d zeroes the Dirichlet walls of rhs in place (src/helm3d.f90:48-60)
+    for (int i = 0; i < nfields; ++i)
+        if (bounds[i] == 'd')
+            for (int k = 0; k < nm; ++k) {
+                double *r = rhs[i] + (size_t)2 * my * mz * k;
+                for (int j = 0; j < my; ++j) {
+                    r[2 * j] = r[2 * j + 1] = 0.0;
+                    r[2 * (j + (size_t)my * (mz - 1))] = r[2 * (j + (size_t)my * (mz - 1)) + 1] = 0.0;
+                }
+                for (int q = 0; q < mz; ++q) {
+                    r[2 * ((size_t)my * q)] = r[2 * ((size_t)my * q) + 1] = 0.0;
+                    r[2 * (my - 1 + (size_t)my * q)] = r[2 * (my - 1 + (size_t)my * q) + 1] = 0.0;
+                }
+            }
+    ductgpu_field f[kMaxFields];
+    for (int i = 0; i < nfields; ++i) {
+        f[i].rhs = ctx->io.buf + 2 * doubles * i;
+        f[i].sol = f[i].rhs + doubles;
+        f[i].xalp = xalp;
+        f[i].alambda = alambdas[i];
+        f[i].ib = ib;
+        f[i].nmodes = nm;
+        f[i].bound = bounds[i];
+    }
+    for (int i = 0; i < nfields; ++i) {
+        DUCT_CUDA(ctx, cudaMemcpyAsync(f[i].rhs, rhs[i], bytes, cudaMemcpyHostToDevice, ctx->cp_in));
+        DUCT_CUDA(ctx, cudaEventRecord(ctx->ev_in[i], ctx->cp_in));
+        DUCT_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_in[i], 0));
+        if ((rc = ductgpu_solve_fields_dev(ctx, &f[i], 1, precision))) return rc;
+        DUCT_CUDA(ctx, cudaEventRecord(ctx->ev_out[i], ctx->stream));
+        DUCT_CUDA(ctx, cudaStreamWaitEvent(ctx->cp_out, ctx->ev_out[i], 0));
+        DUCT_CUDA(ctx, cudaMemcpyAsync(sol[i], f[i].sol, bytes, cudaMemcpyDeviceToHost, ctx->cp_out));
+    }
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->cp_out));
+    rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d_batch");
     return rc ? rc : (precision != DUCTGPU_PREC_FP64 ? device_status(ctx) : DUCTGPU_OK);
 }
 

@@ -120,6 +120,10 @@ struct ductgpu_ctx_s {
     bool capturing = false;
     duct::Workspace work;      // pass intermediates
     duct::Workspace io;        // device copies for host entries
+    // copy streams and events of the pipelined host helm3d
+    static constexpr int kPipeChunks = 8;
+    cudaStream_t cp_in = nullptr, cp_out = nullptr;
+    cudaEvent_t ev_in[kPipeChunks] = {}, ev_out[kPipeChunks] = {};
     // W_L twiddle tables of the register-FFT transforms, one per length
     static constexpr int kTwTables = 8;
     int tw_len[kTwTables] = {};

@@ -103,6 +103,16 @@ int ductgpu_helm3d(ductgpu_ctx ctx, double *rhs, double *sol, int ipro,
                    char bound, double alambda, int my, int mz, int ib,
                    int ie, const double *xalp, int precision);
 
+/* The helm3d calls of one substep (u, v, w and p: src/main1.f90:617-619,
+ * 643) in one call on host arrays: per field the same effects as
+ * ductgpu_helm3d, with field i copied in while field i-1 is solved and
+ * field i-2 copied back (pinned host memory from ductgpu_host_alloc makes
+ * the copies asynchronous).  rhs[i], sol[i]: complex (my,mz,ie-ib+1) host
+ * arrays; bounds[i] 'd' or 'n'; alambdas[i]; one xalp for all fields.    */
+int ductgpu_helm3d_batch(ductgpu_ctx ctx, int nfields, double *const *rhs, double *const *sol,
+                         const char *bounds, const double *alambdas, int my, int mz, int ib,
+                         int ie, const double *xalp, int precision);
+
 /* One field of a batched device-resident solve. */
 typedef struct {
     double *rhs;         /* device, complex (my,mz,nmodes); walls zeroed in

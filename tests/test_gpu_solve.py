@@ -228,3 +228,20 @@ def test_argument_errors(gpu_ctx):
     with pytest.raises(D.DuctGPUError) as e:
         gpu_ctx.pseudomat(400)
     assert e.value.code == D.EARG
+
+
+def test_helm3d_batch_matches_single_calls(gpu_ctx):
+    """ductgpu_helm3d_batch (u, v, w, p on host arrays, copies overlapped)
+    gives the single-call helm3d results and the same in-place rhs effect."""
+    m, nm = 65, 6
+    gpu_ctx.pseudomat(m)
+    xalp = 0.5 * np.arange(nm)
+    specs = [("d", 4.0e3), ("d", 4.0e3), ("d", 4.0e3), ("n", 0.0)]
+    fs = [synth.chebyshev_rhs(m, m, nm, seed=60 + i, ib=0) for i in range(4)]
+    single = [gpu_ctx.helm3d(f.copy(order="F"), b, lam, xalp, ipro=1) for f, (b, lam) in zip(fs, specs)]
+    rh = [f.copy(order="F") for f in fs]
+    batch = gpu_ctx.helm3d_batch(rh, [b for b, _ in specs], [lam for _, lam in specs], xalp)
+    for a, b, r, (bd, _) in zip(batch, single, rh, specs):
+        assert np.array_equal(a, b)
+        if bd == "d":
+            assert np.all(r[0, :, :] == 0) and np.all(r[:, -1, :] == 0)
