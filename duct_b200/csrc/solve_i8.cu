@@ -563,13 +563,31 @@ __global__ void __launch_bounds__(544, 1) k_pass_i8ws(const __grid_constant__ Pa
                 const int e = ec[col] - 1022;   // column exponent: |x| < 2^e
                 uint32_t w[kI8Slices][2];
 #pragma unroll
-                for (int i = 0; i < kI8Slices; ++i) w[i][0] = w[i][1] = 0u;
+                for (int h = 0; h < 2; ++h) {
+                    // four consecutive k: digit magnitudes packed byte-wise,
+                    // then the signs applied to the four bytes at once
+                    uint32_t wd[kI8Slices], sgn = 0u;
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    int d[kI8Slices];
-                    split7_bits(c ? v[q].y : v[q].x, e, d);
+                    for (int i = 0; i < kI8Slices; ++i) wd[i] = 0u;
 #pragma unroll
-                    for (int i = 0; i < kI8Slices; ++i) w[i][q >> 2] |= ((uint32_t)d[i] & 0xFFu) << (8 * (q & 3));
+                    for (int u = 0; u < 4; ++u) {
+                        const double x = c ? v[4 * h + u].y : v[4 * h + u].x;
+                        const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+                        const int E = (int)((b >> 52) & 0x7FF);
+                        const int sh = 1026 + e - E;
+                        unsigned long long M = 0;
+                        if (E != 0 && sh < 64) M = ((b & 0x000FFFFFFFFFFFFFull) | 0x0010000000000000ull) >> sh;
+                        sgn |= (uint32_t)(b >> 63) * (0xFFu << (8 * u));
+#pragma unroll
+                        for (int i = 0; i < kI8Slices; ++i)
+                            wd[i] |= ((uint32_t)(M >> (7 * (kI8Slices - 1 - i))) & 0x7Fu) << (8 * u);
+                    }
+#pragma unroll
+                    for (int i = 0; i < kI8Slices; ++i) {
+                        // -d mod 256 = (0x80 - d) ^ 0x80 for 0 <= d <= 127, byte-parallel
+                        const uint32_t neg = (0x80808080u - wd[i]) ^ 0x80808080u;
+                        w[i][h] = (neg & sgn) | (wd[i] & ~sgn);
+                    }
                 }
 #pragma unroll
                 for (int i = 0; i < kI8Slices; ++i)
@@ -608,23 +626,24 @@ __global__ void __launch_bounds__(544, 1) k_pass_i8ws(const __grid_constant__ Pa
             if (!__all_sync(0xffffffffu, ws_wait(tempty + s, (use & 1) ^ 1, abort))) { fail(); break; }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             if (lane == 0) {
-                const unsigned a0 = i8_smem(As), b0 = i8_smem(Bs + s * kWsBStage);
+                // descriptors differ from the base ones only in the start
+                // address (16-byte units, no carry out of the 14-bit field):
+                // every offset below is a compile-time constant
+                const uint64_t da0 = i8_desc(i8_smem(As), 16, 1024);
+                const uint64_t db0 = i8_desc(i8_smem(Bs + s * kWsBStage), 16, 1024);
                 const uint32_t dacc = tbase + s * kWsAcc;
-#pragma unroll 1
-                for (int lv = 0; lv < kI8Levels; ++lv) {
-                    const int Ls = lv + 2;
-                    bool first = true;
-#pragma unroll 1
-                    for (int si = 1; si <= kI8Slices; ++si) {
-                        const int ti = Ls - si;
-                        if (ti < 1 || ti > kI8Slices) continue;
 #pragma unroll
-                        for (int ks = 0; ks < kI8K / 32; ++ks) {
-                            const uint64_t da = i8_desc(a0 + (si - 1) * kI8OpSlice + ks * 32, 16, 1024);
-                            const uint64_t db = i8_desc(b0 + (ti - 1) * kWsBSlice + ks * 32, 16, 1024);
-                            ws_mma(dacc + lv * kWsN, da, db, first ? 0u : 1u);
-                            first = false;
-                        }
+                for (int lv = 0; lv < kI8Levels; ++lv) {
+#pragma unroll
+                    for (int si = 1; si <= kI8Slices; ++si) {
+                        const int ti = lv + 2 - si;
+                        if (ti < 1 || ti > kI8Slices) continue;
+                        const bool first_pair = (si == (lv + 2 - kI8Slices > 1 ? lv + 2 - kI8Slices : 1));
+#pragma unroll
+                        for (int ks = 0; ks < kI8K / 32; ++ks)
+                            ws_mma(dacc + lv * kWsN, da0 + (uint64_t)(((si - 1) * kI8OpSlice + ks * 32) >> 4),
+                                   db0 + (uint64_t)(((ti - 1) * kWsBSlice + ks * 32) >> 4),
+                                   (first_pair && ks == 0) ? 0u : 1u);
                     }
                 }
                 ws_commit(empty + s);
