@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-transforms", action="store_true")
-    ap.add_argument("--pass-kernel", default="auto", choices=["auto", "staged-32", "staged-16", "register"],
+    ap.add_argument("--pass-kernel", default="auto", choices=["auto", "staged-32", "staged-16", "register", "persist", "parity"],
                     help="GEMM-pass kernel; auto runs the library's autotuner (profiling runs fix it, since "
                          "the autotuner's timing under a profiler is not the live one)")
     ap.add_argument("--transforms-only", action="store_true",
@@ -215,12 +215,14 @@ def run_ours(args, world, rank, local, pg):
         sets.append(fl)
 
     # the library's autotuner picks the GEMM-pass kernel for this batch
-    names = {D.PASS_STAGED: "staged-32", D.PASS_STAGED16: "staged-16", D.PASS_REGISTER: "register"}
+    names = {D.PASS_STAGED: "staged-32", D.PASS_STAGED16: "staged-16", D.PASS_REGISTER: "register",
+             D.PASS_PERSIST: "persist", D.PASS_PARITY: "parity"}
     if args.pass_kernel == "auto":
-        pass_kernel = names[ctx.autotune(sets[0], reps=5)]
+        pass_id = ctx.autotune(sets[0], reps=5)
     else:
-        pass_kernel = args.pass_kernel
-        ctx.set_pass_kernel({v: k for k, v in names.items()}[pass_kernel])
+        pass_id = {v: k for k, v in names.items()}[args.pass_kernel]
+        ctx.set_pass_kernel(pass_id)
+    pass_kernel = names[pass_id]
 
     def timed(prec):
         for i in range(args.warmup):
@@ -253,7 +255,11 @@ def run_ours(args, world, rank, local, pg):
         ms_step, launches, prof, clk = timed(prec)
         res[name] = dict(ms_step=ms_step, launches=launches, prof=prof, clk=clk,
                          value=world * per_step / (ms_step * 1e-3))
-    # accuracy of the split path against the FP64 path on the same operators
+    # accuracy of the split paths against the FP64 passes on the same (full)
+    # operators, which the split paths emulate; the flip-symmetric passes are
+    # another decomposition of the operator (checked against the oracle by
+    # tests/test_gpu_parity.py)
+    ctx.set_pass_kernel(D.PASS_STAGED)
     acc8 = None
     if "int8" in res and "fp64" in res:
         ctx.solve_fields_dev(sets[0], D.PREC_FP64)
@@ -274,6 +280,7 @@ def run_ours(args, world, rank, local, pg):
                 r = r.copy()
                 r[:, :, 0] -= r[:, :, 0].mean()
             acc[name] = float(np.linalg.norm(a - r) / np.linalg.norm(r))
+    ctx.set_pass_kernel(pass_id)
     best = max(res, key=lambda k: res[k]["value"])
     B = res[best]
     peak64, peak64_note = fp64_peak()
@@ -282,12 +289,22 @@ def run_ours(args, world, rank, local, pg):
     for name, R in res.items():
         if name == "fp64":
             kms, kn = R["prof"][D.K_PASS_FP64]
-            flops = 4.0 * n ** 3 * per_step          # n x n operator on 2n real columns per plane
+            if pass_kernel == "parity":
+                # even and odd half blocks (ceil(n/2), floor(n/2)) on 2n real
+                # columns per plane: the flops the flip-symmetric pass executes
+                he, ho = (n + 1) // 2, n // 2
+                flops = 4.0 * n * (he * he + ho * ho) * per_step
+                kname = "k_pass_fp64s (flip-symmetric half blocks, FP64 DMMA m16n8k16)"
+                traffic = traffic_from_profile("k_pass_fp64s")
+            else:
+                flops = 4.0 * n ** 3 * per_step          # n x n operator on 2n real columns per plane
+                kname = "k_pass_fp64 (FP64 DMMA m16n8k16)"
+                traffic = traffic_from_profile("k_pass_fp64")
             ach = flops / ((kms / kn) * 1e-3) / 1e12 if kn else None
             roofs[name] = {"bound": "tensor", "achieved": ach, "peak": peak64, "unit": "TFLOP/s",
                            "frac": (ach / peak64) if (ach and peak64) else None,
-                           "traffic": traffic_from_profile("k_pass_fp64"),
-                           "kernel": "k_pass_fp64 (FP64 DMMA m16n8k16)", "peak_source": peak64_note,
+                           "traffic": traffic,
+                           "kernel": kname, "peak_source": peak64_note,
                            "kernel_share_of_step": kms / (R["ms_step"] * args.steps)}
         elif name == "int8":
             kms, kn = R["prof"][D.K_MIXED_GEMM]
@@ -298,7 +315,7 @@ def run_ours(args, world, rank, local, pg):
             roofs[name] = {"bound": "tensor", "achieved": ach, "peak": 4500.0, "unit": "TOPS (int8)",
                            "frac": (ach / 4500.0) if ach else None,
                            "traffic": None,
-                           "kernel": "k_pass_i8 (tcgen05 kind::i8, 28 slice products, exact int32)",
+                           "kernel": "k_pass_i8ws (tcgen05 kind::i8, 28 slice products, exact int32)",
                            "peak_source": "nominal dense int8 (no measured int8 peak on this pool)",
                            "fp64_equiv_tflops": (4.0 * n ** 3 * per_step) / ((kms / kn) * 1e-3) / 1e12 if kn else None,
                            "kernel_share_of_step": kms / (R["ms_step"] * args.steps)}

@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libductgpu.so")
 
 OK, EARG, ESTATE, ECUDA, ESOLVER, ENONFINITE, ETIMEOUT, EALLOC = range(8)
 PREC_FP64, PREC_MIXED, PREC_INT8 = 0, 1, 2
-PASS_STAGED, PASS_REGISTER, PASS_STAGED16, PASS_PERSIST = 0, 1, 2, 3
+PASS_STAGED, PASS_REGISTER, PASS_STAGED16, PASS_PERSIST, PASS_PARITY = 0, 1, 2, 3, 4
 GAUGE_POINT, GAUGE_MEAN = 0, 1
 
 EXPORTS = [

@@ -207,7 +207,11 @@ int solve_adjoint(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
             k_neumann_fill_adj<<<cta, 1024, 4 * m * sizeof(double2), ctx->stream>>>(fp);
         }
     }
-    // L^T: y with P^T, z with P^T + divide, z with P^-T, y with P^-T
+    // L^T: y with P^T, z with P^T + divide, z with P^-T, y with P^-T.  On the
+    // flip-symmetric operators (when the forward solve uses them) the
+    // transpose of an unfolded P pass is a folded pass with the blocks
+    // transposed, and that of a folded P^-1 pass an unfolded one.
+    const bool fold = use_fold(ctx, tasks, ntasks);
     PassParams pp{};
     pp.lam = ctx->lam;
     for (int pass = 0; pass < 4; ++pass) {
@@ -231,6 +235,8 @@ int solve_adjoint(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
             case 2: f.src = a2; f.dst = a1; f.A = b.QTpack; break;
             default: f.src = a1; f.dst = tasks[i].sol; f.A = b.QTpack; break;
             }
+            if (fold)
+                fold_field(f, b, (pass < 2) ? 1 : 2, (pass < 2) ? b.PfoldT : b.QfoldT, tasks[i].bound == 'n');
             pp.cta_start[i] = cta;
             cta += tasks[i].nmodes * f.nchunks;
         }

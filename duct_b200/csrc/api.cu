@@ -322,6 +322,14 @@ int ductgpu_set_operators(ductgpu_ctx ctx, char bound, const double *E, const do
     }
     int rc = pack_operators(ctx, b);
     if (rc) return rc;
+    // imported operators are applied as given: no flip-symmetric form
+    cudaFree(b.Pfold);
+    cudaFree(b.Qfold);
+    cudaFree(b.PfoldT);
+    cudaFree(b.QfoldT);
+    cudaFree(b.Eperm);
+    b.Pfold = b.Qfold = b.PfoldT = b.QfoldT = b.Eperm = nullptr;
+    b.fold_ok = false;
     return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "set_operators");
 }
 
@@ -345,11 +353,11 @@ int ductgpu_set_refinement(ductgpu_ctx ctx, int steps)
 int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel)
 {
     if (!ctx) return DUCTGPU_EARG;
-    if (kernel < DUCTGPU_PASS_STAGED || kernel > DUCTGPU_PASS_PERSIST)
+    if (kernel < -1 || kernel > DUCTGPU_PASS_PARITY)
         return set_error(ctx, DUCTGPU_EARG, "pass kernel %d", kernel);
     if (size_class < -1 || size_class > 2) return set_error(ctx, DUCTGPU_EARG, "size class %d", size_class);
     for (int c = 0; c < 3; ++c)
-        if (size_class < 0 || size_class == c) ctx->pass_variant[c] = kernel;
+        if (size_class < 0 || size_class == c) ctx->pass_variant[c] = (kernel < 0) ? kPassDefault[c] : kernel;
     return DUCTGPU_OK;
 }
 
@@ -361,7 +369,8 @@ int ductgpu_autotune(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, 
     if (reps < 1) reps = 5;
     const int cls = (ctx->my - 2 + 63) / 64 - 1;
     if (cls < 0 || cls > 2) return set_error(ctx, DUCTGPU_EARG, "grid %d", ctx->my);
-    const int variants[4] = {DUCTGPU_PASS_STAGED, DUCTGPU_PASS_STAGED16, DUCTGPU_PASS_REGISTER, DUCTGPU_PASS_PERSIST};
+    const int variants[5] = {DUCTGPU_PASS_STAGED, DUCTGPU_PASS_STAGED16, DUCTGPU_PASS_REGISTER, DUCTGPU_PASS_PERSIST,
+                             DUCTGPU_PASS_PARITY};
     const int saved = ctx->pass_variant[cls];
     const bool prof = ctx->prof_on;
     ctx->prof_on = false;

@@ -21,6 +21,9 @@ constexpr int kNumEvents = 16;
 constexpr int kMaxRect = 8;     // rectangular operator slots (duct shapes)
 
 // Interior operators of one boundary condition ('d' or 'n').
+// default GEMM-pass kernel per operator size class (n <= 63, <= 127, <= 191)
+constexpr int kPassDefault[3] = {DUCTGPU_PASS_PARITY, DUCTGPU_PASS_PARITY, DUCTGPU_PASS_PARITY};
+
 struct BoundOps {
     int n = 0;                 // interior points, my-2
     int kpad = 0;              // n rounded up to the K chunk (32)
@@ -41,6 +44,15 @@ struct BoundOps {
     int *Pexp = nullptr, *Qexp = nullptr;            // per-row exponents
     int8_t *Pi8 = nullptr, *Qi8 = nullptr;          // int8 slices (int8-emulated FP64)
     int *Pexp8 = nullptr, *Qexp8 = nullptr;
+    // flip-symmetric form (setup.cu fold_operators): modes reordered even
+    // first (he of them) then odd (ho); Qfold / Pfold are the two half
+    // blocks stacked (2 hpad rows x hpad columns) in DMMA A-fragment order
+    bool fold_ok = false;
+    int he = 0, ho = 0, hpad = 0;
+    int sing_perm = -1;        // position of iofzero - 1 in the reordered modes
+    double *Pfold = nullptr, *Qfold = nullptr;
+    double *PfoldT = nullptr, *QfoldT = nullptr;   // the blocks transposed (adjoint)
+    double *Eperm = nullptr;   // [n] eigenvalues in the reordered mode order
 };
 
 // Operators of one rectangular duct shape (src/pseudomat_temp.f90): y and z
@@ -93,12 +105,11 @@ struct ductgpu_ctx_s {
     int gauge = DUCTGPU_GAUGE_POINT;
     int refine_steps = 2;      // FP64 refinement steps of the split-precision path
     int i8_kernel = 1;         // int8-emulated passes: 0 sequential, 1 warp-specialised pipeline
-    // GEMM-pass kernel per operator size class (n <= 63, <= 127, <= 191):
-    // DUCTGPU_PASS_STAGED or DUCTGPU_PASS_REGISTER (ductgpu_set_pass_kernel,
-    // ductgpu_autotune)
-    // defaults from measurements on B200 at n = 63, 127, 191 (cfg1 and
-    // config-4 sized batches); ductgpu_autotune re-picks them by timing
-    int pass_variant[3] = {DUCTGPU_PASS_STAGED16, DUCTGPU_PASS_STAGED, DUCTGPU_PASS_STAGED16};
+    // GEMM-pass kernel per operator size class (n <= 63, <= 127, <= 191),
+    // one of DUCTGPU_PASS_* (ductgpu_set_pass_kernel, ductgpu_autotune);
+    // defaults (kPassDefault) from measurements on B200 at n = 31, 63, 127,
+    // 191; ductgpu_autotune re-picks them by timing
+    int pass_variant[3] = {duct::kPassDefault[0], duct::kPassDefault[1], duct::kPassDefault[2]};
     duct::BoundOps dir, neu;
 
     duct::RectSlot rect[duct::kMaxRect];
@@ -165,6 +176,8 @@ void profile_drain(ductgpu_ctx ctx);
 // setup.cu
 int pseudomat_gpu(ductgpu_ctx ctx, int m);
 int pack_operators(ductgpu_ctx ctx, BoundOps &b);
+// flip-symmetric half operators of b (fold_ok false when b lacks the symmetry)
+int fold_operators(ductgpu_ctx ctx, BoundOps &b);
 int pack_transposed(ductgpu_ctx ctx, BoundOps &b);
 // Real eigen-decomposition of the n x n device matrix B (destroyed) into
 // b.E, b.P, b.PM1 (allocated by the caller), with emin/emax and iofzero.
@@ -214,6 +227,11 @@ struct PassField {
     long long plane_stride;  // doubles per complex plane
     // residual epilogue: dst = resF - resT - acc + lam * resU
     const double *resF, *resT, *resU;
+    // flip-symmetric pass (k_pass_fp64s): 1 folds a physical input into
+    // even / odd halves, 2 unfolds the two halves into a physical output;
+    // kpad is then the half extent hpad and the mode order is even first
+    int par;
+    int he, ho;
 };
 struct PassParams {
     PassField f[kMaxFields];
@@ -226,6 +244,14 @@ struct PassParams {
 };
 constexpr int kPassLines = 32;
 int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid);
+// Whether a solve (or its adjoint) over these fields runs the flip-symmetric
+// passes: DUCTGPU_PASS_PARITY selected for the size class and every field's
+// operators have the folded form.  The forward and adjoint take the same
+// decision, so the adjoint is the transpose of the map the forward applies.
+bool use_fold(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks);
+// Turns a pass field into a flip-symmetric one: par 1 folds the input,
+// par 2 unfolds the output, A is the matching folded pack of b.
+void fold_field(PassField &f, const BoundOps &b, int par, const double *A, bool neumann);
 // Sets the geometry of one field of a pass: operator b along a direction
 // with stride sk (complex elements), nlines lines of stride sl.
 void pass_geometry(PassField &f, const BoundOps &b, const double *El, int nlines, int sk, int sl,

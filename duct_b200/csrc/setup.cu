@@ -123,17 +123,26 @@ __global__ void k_real_part(int n, const double *W, double *E)
 // Pack an n x n column-major matrix A into the A-operand fragment order of
 // mma.sync m16n8k16 f64: element (row g + 8*(v&1), col t + 4*(v>>1)) of
 // 16x16 tile (mt, ks) goes to lane g*4+t, value v (0..7), stored at
-// ((ks*mtiles + mt)*32 + lane)*8 + v.  Outside n x n the packing is zero.
+// ((ks*mtiles + mt)*4 + v/2)*64 + lane*2 + v%2 -- the value pair outermost,
+// so that a warp's 16-byte loads of one pair are consecutive (no shared
+// memory bank conflicts, one 512-byte run from global memory).  Outside
+// n x n the packing is zero.
+__host__ __device__ __forceinline__ void pack_slot(int idx, int mtiles, int &row, int &col)
+{
+    const int tile = idx >> 8, h = (idx >> 6) & 3, lane = (idx >> 1) & 31, v = 2 * h + (idx & 1);
+    const int mt = tile % mtiles, ks = tile / mtiles;
+    const int g = lane >> 2, t = lane & 3;
+    row = mt * 16 + g + 8 * (v & 1);
+    col = ks * 16 + t + 4 * (v >> 1);
+}
+
 __global__ void k_pack_a(int n, int kpad, int mtiles, const double *A, double *out)
 {
     const int total = (kpad / 16) * mtiles * 256;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += gridDim.x * blockDim.x) {
-        const int v = idx & 7, lane = (idx >> 3) & 31, tile = idx >> 8;
-        const int mt = tile % mtiles, ks = tile / mtiles;
-        const int g = lane >> 2, t = lane & 3;
-        const int row = mt * 16 + g + 8 * (v & 1);
-        const int col = ks * 16 + t + 4 * (v >> 1);
+        int row, col;
+        pack_slot(idx, mtiles, row, col);
         out[idx] = (row < n && col < n) ? A[row + (size_t)n * col] : 0.0;
     }
 }
@@ -158,11 +167,8 @@ __global__ void k_pack_at(int n, int kpad, int mtiles, const double *A, double *
     const int total = (kpad / 16) * mtiles * 256;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += gridDim.x * blockDim.x) {
-        const int v = idx & 7, lane = (idx >> 3) & 31, tile = idx >> 8;
-        const int mt = tile % mtiles, ks = tile / mtiles;
-        const int g = lane >> 2, t = lane & 3;
-        const int row = mt * 16 + g + 8 * (v & 1);
-        const int col = ks * 16 + t + 4 * (v >> 1);
+        int row, col;
+        pack_slot(idx, mtiles, row, col);
         out[idx] = (row < n && col < n) ? A[col + (size_t)n * row] : 0.0;
     }
 }
@@ -186,6 +192,7 @@ void free_bound(BoundOps &b)
     cudaFree(b.D2B); cudaFree(b.Bpack); cudaFree(b.PTpack); cudaFree(b.QTpack);
     cudaFree(b.Pslices); cudaFree(b.Qslices); cudaFree(b.Pexp); cudaFree(b.Qexp);
     cudaFree(b.Pi8); cudaFree(b.Qi8); cudaFree(b.Pexp8); cudaFree(b.Qexp8);
+    cudaFree(b.Pfold); cudaFree(b.Qfold); cudaFree(b.PfoldT); cudaFree(b.QfoldT); cudaFree(b.Eperm);
     b = BoundOps();
 }
 
@@ -228,6 +235,146 @@ int pack_operators(ductgpu_ctx ctx, BoundOps &b)
         ctx->launches += 2;
     }
     return check_cuda(ctx, cudaGetLastError(), "pack_operators");
+}
+
+// Flip symmetry of the wall-normal operators.  With the same condition on
+// both walls the interior operator B commutes with the reflection J (point
+// k <-> n-1-k, the Gauss-Lobatto nodes being symmetric), so B maps even
+// vectors to even ones and odd to odd.  On the first-half values of an even
+// vector (points 0..he-1, he = ceil(n/2), the middle point included when n
+// is odd) B acts as Be(r,k) = B(r,k) + B(r,n-1-k) (B(r,mid) at the middle),
+// on those of an odd vector (0..ho-1, ho = floor(n/2)) as
+// Bo(r,k) = B(r,k) - B(r,n-1-k).  Be and Bo are decomposed on their own
+// (half-size eigen problems whose eigenvectors are exactly even / odd), and
+// with the modes ordered even first every pass becomes block diagonal:
+//   P^-1 pass: even coefficients = Ue^-1 u, u_k = (in_k + in_{n-1-k}) / 2
+//              (in_mid at the middle); odd = Uo^-1 v, v_k = (in_k - in_{n-1-k}) / 2
+//   P pass:    out_o = (Ue c_e)_o + (Uo c_o)_o, out_{n-1-o} = (Ue c_e)_o - (Uo c_o)_o
+// -- half the flops of a pass.  The result is the diagonalisation solve
+// with another, equally valid, FP64 eigen-decomposition of B (its accuracy
+// against the exact discrete solution is the same as the full one's).
+// Built only for the library's own operators (ductgpu_pseudomat): operators
+// imported with ductgpu_set_operators are applied exactly as given.  B must
+// be flip-symmetric to rounding (|B - JBJ| <= 1e-12 max|B|), both blocks'
+// spectra real, and n <= 191; otherwise fold_ok stays false and the solve
+// uses the full operators.  The (symmetric part of) B is folded on the host.
+int fold_operators(ductgpu_ctx ctx, BoundOps &b)
+{
+    b.fold_ok = false;
+    cudaFree(b.Pfold);
+    cudaFree(b.Qfold);
+    cudaFree(b.PfoldT);
+    cudaFree(b.QfoldT);
+    cudaFree(b.Eperm);
+    b.Pfold = b.Qfold = b.PfoldT = b.QfoldT = b.Eperm = nullptr;
+    const int n = b.n, he = (n + 1) / 2, ho = n / 2;
+    const int hpad = (he + 31) / 32 * 32;   // 32 rows per M warp of each half block
+    if (n < 2 || hpad > 96 || !b.D2B) return DUCTGPU_OK;
+    const size_t nn = (size_t)n * n;
+    std::vector<double> B(nn);
+    DUCT_CUDA(ctx, cudaMemcpyAsync(B.data(), b.D2B, nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    auto ba = [&](int r, int c) { return B[r + (size_t)n * c]; };
+    double bmax = 0.0, asym = 0.0;
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < n; ++r) {
+            bmax = fmax(bmax, fabs(ba(r, c)));
+            asym = fmax(asym, fabs(ba(r, c) - ba(n - 1 - r, n - 1 - c)));
+        }
+    if (!(asym <= 1.0e-12 * bmax)) return DUCTGPU_OK;
+    auto bs = [&](int r, int c) { return 0.5 * (ba(r, c) + ba(n - 1 - r, n - 1 - c)); };
+    std::vector<double> Be((size_t)he * he), Bo((size_t)ho * ho);
+    for (int c = 0; c < he; ++c)
+        for (int r = 0; r < he; ++r) Be[r + (size_t)he * c] = (c < ho) ? bs(r, c) + bs(r, n - 1 - c) : bs(r, c);
+    for (int c = 0; c < ho; ++c)
+        for (int r = 0; r < ho; ++r) Bo[r + (size_t)ho * c] = bs(r, c) - bs(r, n - 1 - c);
+
+    BoundOps be, bo;
+    be.n = he;
+    bo.n = ho;
+    double *dB = nullptr;
+    int rc = DUCTGPU_OK;
+    std::vector<double> Ue, Ie, Ee, Uo, Io, Eo;
+    auto half = [&](BoundOps &h, std::vector<double> &M, std::vector<double> &U, std::vector<double> &I,
+                    std::vector<double> &E) {
+        const int k = h.n;
+        const size_t kk = (size_t)k * k;
+        int r = DUCTGPU_OK;
+        if ((r = check_cuda(ctx, cudaMalloc(&h.E, k * sizeof(double)), "fold E"))) return r;
+        if ((r = check_cuda(ctx, cudaMalloc(&h.P, kk * sizeof(double)), "fold P"))) return r;
+        if ((r = check_cuda(ctx, cudaMalloc(&h.PM1, kk * sizeof(double)), "fold PM1"))) return r;
+        if ((r = check_cuda(ctx, cudaMemcpyAsync(dB, M.data(), kk * sizeof(double), cudaMemcpyHostToDevice, ctx->stream), "fold B"))) return r;
+        if ((r = eigen_gpu(ctx, k, dB, h))) return r;
+        U.resize(kk);
+        I.resize(kk);
+        E.resize(k);
+        if ((r = check_cuda(ctx, cudaMemcpyAsync(U.data(), h.P, kk * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "fold U"))) return r;
+        if ((r = check_cuda(ctx, cudaMemcpyAsync(I.data(), h.PM1, kk * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "fold U^-1"))) return r;
+        if ((r = check_cuda(ctx, cudaMemcpyAsync(E.data(), h.E, k * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "fold E"))) return r;
+        return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "fold sync");
+    };
+    if (!(rc = check_cuda(ctx, cudaMalloc(&dB, (size_t)he * he * sizeof(double)), "fold B")))
+        if (!(rc = half(be, Be, Ue, Ie, Ee))) rc = half(bo, Bo, Uo, Io, Eo);
+    cudaFree(dB);
+    free_bound(be);
+    free_bound(bo);
+    if (rc == DUCTGPU_ESOLVER) return DUCTGPU_OK;   // a block with a complex pair: full operators
+    if (rc) return rc;
+
+    // the two half blocks stacked, 2 hpad x hpad, in the fragment order of k_pack_a
+    const int mtiles = 2 * hpad / 16;
+    const size_t packed = (size_t)(hpad / 16) * mtiles * 256;
+    std::vector<double> Pf(packed), Qf(packed), PfT(packed), QfT(packed), Ep(n);
+    for (size_t idx = 0; idx < packed; ++idx) {
+        int row, col;
+        pack_slot((int)idx, mtiles, row, col);
+        double pv = 0.0, qv = 0.0, pt = 0.0, qt = 0.0;
+        if (row < hpad) {
+            if (row < he && col < he) {
+                pv = Ue[row + (size_t)he * col];
+                qv = Ie[row + (size_t)he * col] * ((col < ho) ? 0.5 : 1.0);
+                pt = Ue[col + (size_t)he * row];
+                qt = Ie[col + (size_t)he * row] * ((row < ho) ? 0.5 : 1.0);
+            }
+        } else if (row - hpad < ho && col < ho) {
+            const int r = row - hpad;
+            pv = Uo[r + (size_t)ho * col];
+            qv = Io[r + (size_t)ho * col] * 0.5;
+            pt = Uo[col + (size_t)ho * r];
+            qt = Io[col + (size_t)ho * r] * 0.5;
+        }
+        Pf[idx] = pv;
+        Qf[idx] = qv;
+        PfT[idx] = pt;
+        QfT[idx] = qt;
+    }
+    for (int r = 0; r < he; ++r) Ep[r] = Ee[r];
+    for (int r = 0; r < ho; ++r) Ep[he + r] = Eo[r];
+    // the pinned (singular) mode: first index of the smallest |E|, the
+    // rule of the full operators (src/pseudomat.f90:146-152)
+    int sing = -1;
+    if (b.iofzero > 0) {
+        double emin = 1.0e300;
+        for (int r = 0; r < n; ++r)
+            if (fabs(Ep[r]) < emin) { emin = fabs(Ep[r]); sing = r; }
+    }
+    DUCT_CUDA(ctx, cudaMalloc(&b.Pfold, packed * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&b.Qfold, packed * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&b.PfoldT, packed * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&b.QfoldT, packed * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&b.Eperm, n * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.Pfold, Pf.data(), packed * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.Qfold, Qf.data(), packed * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.PfoldT, PfT.data(), packed * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.QfoldT, QfT.data(), packed * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.Eperm, Ep.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    b.he = he;
+    b.ho = ho;
+    b.hpad = hpad;
+    b.sing_perm = sing;
+    b.fold_ok = true;
+    return DUCTGPU_OK;
 }
 
 // 4x4 inverse by Gauss-Jordan with partial pivoting (the reference inverts
@@ -504,6 +651,8 @@ int pseudomat_gpu(ductgpu_ctx ctx, int m)
     DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->ccw, w.data(), m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     if ((rc = pack_operators(ctx, ctx->dir))) return rc;
     if ((rc = pack_operators(ctx, ctx->neu))) return rc;
+    if ((rc = fold_operators(ctx, ctx->dir))) return rc;
+    if ((rc = fold_operators(ctx, ctx->neu))) return rc;
     DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->my = ctx->mz = m;
     ctx->ready = true;

@@ -29,11 +29,19 @@ constexpr int kLines = kPassLines;   // complex lines per CTA
 constexpr int kNld = 68;     // leading dim of the staged tile (64 + 4 pad)
 constexpr int kKC = 16;      // K chunk of the streamed operator (one k16 step)
 constexpr int kThreads = 256;
+constexpr int kParityLines = 16;   // lines per CTA of the flip-symmetric passes (3 CTAs per SM)
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
 {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+// 16-byte copy, or 16 zero bytes when !valid (gmem is then not read)
+__device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, bool valid)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
@@ -86,25 +94,21 @@ __global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)
     };
     load_a(0, 0);
 
-    // Stage the lines: Bs[k][2l + c] = in(k, l0 + l) component c, zero padded.
+    // Stage the lines: Bs[k][2l + c] = in(k, l0 + l) component c, zero
+    // padded; cp.async keeps all of a thread's copies in flight at once (the
+    // first K step's wait covers them)
     const int n = F.n, sk = F.sk, sl = F.sl, o1 = F.off;
+    auto stage = [&](int k, int l) {
+        const bool ok = k < n && l < L;
+        const double *gp = ok ? src + 2 * ((long long)(k + o1) * sk + (long long)(l0 + l + o1) * sl) : src;
+        cp_async16_zfill(Bs + k * NLD + 2 * l, gp, ok);
+    };
     if (sk == 1) {
-        for (int idx = tid; idx < kpad * LINES; idx += kThreads) {
-            const int k = idx % kpad, l = idx / kpad;
-            double2 v = make_double2(0.0, 0.0);
-            if (k < n && l < L)
-                v = *reinterpret_cast<const double2 *>(src + 2 * ((long long)(k + o1) * sk + (long long)(l0 + l + o1) * sl));
-            *reinterpret_cast<double2 *>(Bs + k * NLD + 2 * l) = v;
-        }
+        for (int idx = tid; idx < kpad * LINES; idx += kThreads) stage(idx % kpad, idx / kpad);
     } else {
-        for (int idx = tid; idx < kpad * LINES; idx += kThreads) {
-            const int l = idx % LINES, k = idx / LINES;
-            double2 v = make_double2(0.0, 0.0);
-            if (k < n && l < L)
-                v = *reinterpret_cast<const double2 *>(src + 2 * ((long long)(k + o1) * sk + (long long)(l0 + l + o1) * sl));
-            *reinterpret_cast<double2 *>(Bs + k * NLD + 2 * l) = v;
-        }
+        for (int idx = tid; idx < kpad * LINES; idx += kThreads) stage(idx / LINES, idx % LINES);
     }
+    cp_async_commit();
 
     const int lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 3, wn = warp >> 2;
@@ -141,10 +145,10 @@ __global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)
                 const int mtg = wm * MTW + mt;
                 if (mtg >= mtiles) continue;
                 double a[8];
-                const double2 *q = reinterpret_cast<const double2 *>(Ab + ((ks * mtiles + mtg) * 32 + lane) * 8);
+                const double2 *q = reinterpret_cast<const double2 *>(Ab + (ks * mtiles + mtg) * 256) + lane;
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
-                    const double2 v = q[h];
+                    const double2 v = q[32 * h];
                     a[2 * h] = v.x;
                     a[2 * h + 1] = v.y;
                 }
@@ -177,9 +181,9 @@ __global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)
                         re = 0.0;
                         im = 0.0;
                     } else {
-                        const double den = (F.E[o] + F.El[lg]) - lam;
-                        re = re / den;
-                        im = im / den;
+                        const double rden = 1.0 / ((F.E[o] + F.El[lg]) - lam);
+                        re *= rden;
+                        im *= rden;
                     }
                 }
                 const long long off = 2 * ((long long)(o + o1) * sk + (long long)(lg + o1) * sl);
@@ -195,6 +199,223 @@ __global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)
                 *reinterpret_cast<double2 *>(dst + off) = make_double2(re, im);
             }
         }
+}
+
+// ---------------------------------------------------------------------------
+// Flip-symmetric variant (fold_operators in setup.cu): the operator is the
+// two half blocks stacked, 2 H x H (H = kpad = 32 MTW), so warps 0-1 along M
+// own the even block and warps 2-3 the odd one, each over its own H rows of
+// the staged data -- half the K loop of k_pass_fp64 at the same tile shape.
+// par 1 (P^-1 passes): the physical input is folded while it is staged
+//   (rows 0..H-1: in_k + in_{n-1-k}, in_k alone at the middle point when n
+//   is odd; rows H..2H-1: in_k - in_{n-1-k}); the output is in mode order
+//   (he even modes, then ho odd ones), the eigenvalue divide as usual.
+// par 2 (P passes): the mode-ordered input is staged as the two halves; the
+//   accumulators go through shared memory, and out_o = even_o + odd_o,
+//   out_{n-1-o} = even_o - odd_o.
+template <int MTW, int LINES>
+__global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)) k_pass_fp64s(const __grid_constant__ PassParams p)
+{
+    constexpr int NLD = 2 * LINES + 4, NTW = LINES / 8;
+    constexpr int a_chunk_max = (kKC / 16) * (4 * MTW) * 256;
+    extern __shared__ __align__(16) double smem[];
+    double *As = smem;
+    double *Bs = smem + 2 * a_chunk_max;
+
+    int fi = 0;
+    while (fi + 1 < p.nf && (int)blockIdx.x >= p.cta_start[fi + 1]) ++fi;
+    const PassField &F = p.f[fi];
+    const int local = blockIdx.x - p.cta_start[fi];
+    const int plane = local / F.nchunks;
+    const int chunk = local - plane * F.nchunks;
+    const int l0 = chunk * LINES;
+    const int L = min(LINES, F.nlines - l0);
+    const double *src = F.src + (long long)plane * F.plane_stride;
+    double *dst = F.dst + (long long)plane * F.plane_stride;
+    const int tid = threadIdx.x;
+    const int H = F.kpad, mtiles = F.mtiles, rows = 2 * H;
+    const int nkc = H / kKC;
+    const int a_chunk = (kKC / 16) * mtiles * 256;
+    const int n = F.n, he = F.he, ho = F.ho, sk = F.sk, sl = F.sl, o1 = F.off;
+
+    auto load_a = [&](int c, int buf) {
+        const double *g = F.A + (size_t)c * a_chunk;
+        double *sa = As + buf * a_chunk_max;
+        for (int i = tid * 2; i < a_chunk; i += kThreads * 2) cp_async16(sa + i, g + i);
+        cp_async_commit();
+    };
+    load_a(0, 0);
+
+    // Raw rows by cp.async (all of a thread's copies in flight), placed so
+    // that the fold is in place: row r < H holds point / mode r (r < he),
+    // row H + j the partner of row j -- point n-1-j for par 1, odd mode
+    // he + j for par 2 (j < ho); the other rows are zero.
+    auto stage = [&](int r, int l) {
+        const int j = r - H;
+        const int k = (r < H) ? (r < he ? r : -1) : (j < ho ? (F.par == 1 ? n - 1 - j : he + j) : -1);
+        const bool ok = k >= 0 && l < L;
+        const double *gp = ok ? src + 2 * ((long long)(k + o1) * sk + (long long)(l0 + l + o1) * sl) : src;
+        cp_async16_zfill(Bs + r * NLD + 2 * l, gp, ok);
+    };
+    if (sk == 1) {
+        // groups of 8 threads take 4 consecutive points of 2 lines: 64-byte
+        // runs in global memory, 8 distinct bank groups in shared memory
+        const int rq = rows / 4;
+        for (int idx = tid; idx < rows * LINES; idx += kThreads) {
+            const int rest = idx >> 3;
+            stage((rest % rq) * 4 + (idx & 3), (rest / rq) * 2 + ((idx >> 2) & 1));
+        }
+    } else {
+        for (int idx = tid; idx < rows * LINES; idx += kThreads) stage(idx / LINES, idx % LINES);
+    }
+    cp_async_commit();
+    if (F.par == 1) {
+        // fold the pairs: row j <- in_j + in_{n-1-j}, row H + j <- in_j - in_{n-1-j}
+        // (the middle point of an odd n stays in row ho of the even half)
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int idx = tid; idx < ho * LINES; idx += kThreads) {
+            const int j = idx / LINES, l = idx % LINES;
+            double2 *pa = reinterpret_cast<double2 *>(Bs + j * NLD + 2 * l);
+            double2 *pb = reinterpret_cast<double2 *>(Bs + (H + j) * NLD + 2 * l);
+            const double2 a = *pa, b = *pb;
+            *pa = make_double2(a.x + b.x, a.y + b.y);
+            *pb = make_double2(a.x - b.x, a.y - b.y);
+        }
+    }
+
+    const int lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 3, wn = warp >> 2;
+    const int g = lane >> 2, t = lane & 3;
+    const int kb0 = (wm * MTW * 16 >= H) ? H : 0;   // this warp's half of the staged rows
+    double acc[MTW][NTW][4];
+#pragma unroll
+    for (int i = 0; i < MTW; ++i)
+#pragma unroll
+        for (int j = 0; j < NTW; ++j)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+
+    for (int c = 0; c < nkc; ++c) {
+        if (c + 1 < nkc) {
+            load_a(c + 1, (c + 1) & 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const double *Ab = As + (c & 1) * a_chunk_max;
+#pragma unroll
+        for (int ks = 0; ks < kKC / 16; ++ks) {
+            const int kg = kb0 + c * kKC + ks * 16 + t;
+            double b[NTW][4];
+#pragma unroll
+            for (int nt = 0; nt < NTW; ++nt) {
+                const int col = wn * LINES + nt * 8 + g;
+#pragma unroll
+                for (int v = 0; v < 4; ++v) b[nt][v] = Bs[(kg + 4 * v) * NLD + col];
+            }
+#pragma unroll
+            for (int mt = 0; mt < MTW; ++mt) {
+                const int mtg = wm * MTW + mt;
+                double a[8];
+                const double2 *q = reinterpret_cast<const double2 *>(Ab + (ks * mtiles + mtg) * 256) + lane;
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const double2 v = q[32 * h];
+                    a[2 * h] = v.x;
+                    a[2 * h + 1] = v.y;
+                }
+#pragma unroll
+                for (int nt = 0; nt < NTW; ++nt) dmma16(acc[mt][nt], a, b[nt]);
+            }
+        }
+        __syncthreads();
+    }
+
+    const double lam = p.lam[F.plane0 + plane];
+    const bool im0 = p.zero_im_mode0 && F.mode0 && plane == 0;
+    if (F.par == 1) {
+        const bool singular = (F.sing_io >= 0) && fabs(lam) <= 1.0e-10;
+#pragma unroll
+        for (int mt = 0; mt < MTW; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < NTW; ++nt) {
+                const int l = wn * (LINES / 2) + nt * 4 + t;
+                if (l >= L) continue;
+                const int lg = l0 + l;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int orow = (wm * MTW + mt) * 16 + g + 8 * h;
+                    const int o = orow < H ? (orow < he ? orow : -1) : (orow - H < ho ? he + orow - H : -1);
+                    if (o < 0) continue;
+                    double re = acc[mt][nt][2 * h], im = acc[mt][nt][2 * h + 1];
+                    if (p.divide) {
+                        if (singular && o == F.sing_io && lg == F.sing_l) {
+                            re = 0.0;
+                            im = 0.0;
+                        } else {
+                            const double rden = 1.0 / ((F.E[o] + F.El[lg]) - lam);
+                            re *= rden;
+                            im *= rden;
+                        }
+                    }
+                    if (im0) im = 0.0;
+                    const long long off = 2 * ((long long)(o + o1) * sk + (long long)(lg + o1) * sl);
+                    *reinterpret_cast<double2 *>(dst + off) = make_double2(re, im);
+                }
+            }
+        return;
+    }
+    // par 2: both halves through shared memory (the staged data is consumed).
+    // With the output points contiguous in memory (sk == 1) the halves are
+    // laid out line-major, 2H + 2 complex per line (conflict-free for the
+    // accumulator writes), so consecutive threads read consecutive 16-byte
+    // words and write consecutive points; otherwise row-major as staged.
+    auto emit = [&](const double2 *ev, const double2 *od, int rs, int o, int l) {
+        const int oh = o < he ? o : n - 1 - o;   // row of the halves (stride rs)
+        double2 v = ev[oh * rs];
+        if (oh < ho) {
+            const double2 d = od[oh * rs];
+            v = (o < he) ? make_double2(v.x + d.x, v.y + d.y) : make_double2(v.x - d.x, v.y - d.y);
+        }
+        if (im0) v.y = 0.0;
+        *reinterpret_cast<double2 *>(dst + 2 * ((long long)(o + o1) * sk + (long long)(l0 + l + o1) * sl)) = v;
+    };
+    if (sk == 1) {
+        double2 *Cs = reinterpret_cast<double2 *>(Bs);
+        const int cld = 2 * H + 2;
+#pragma unroll
+        for (int mt = 0; mt < MTW; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < NTW; ++nt)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                    Cs[(wn * (LINES / 2) + nt * 4 + t) * cld + (wm * MTW + mt) * 16 + g + 8 * h] =
+                        make_double2(acc[mt][nt][2 * h], acc[mt][nt][2 * h + 1]);
+        __syncthreads();
+        for (int idx = tid; idx < n * LINES; idx += kThreads) {
+            const int o = idx % n, l = idx / n;
+            if (l < L) emit(Cs + l * cld, Cs + l * cld + H, 1, o, l);
+        }
+    } else {
+#pragma unroll
+        for (int mt = 0; mt < MTW; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < NTW; ++nt)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int orow = (wm * MTW + mt) * 16 + g + 8 * h;
+                    *reinterpret_cast<double2 *>(Bs + orow * NLD + wn * LINES + nt * 8 + 2 * t) =
+                        make_double2(acc[mt][nt][2 * h], acc[mt][nt][2 * h + 1]);
+                }
+        __syncthreads();
+        const double2 *Rs = reinterpret_cast<const double2 *>(Bs);
+        for (int idx = tid; idx < n * LINES; idx += kThreads) {
+            const int o = idx / LINES, l = idx % LINES;
+            if (l < L) emit(Rs + l, Rs + H * (NLD / 2) + l, NLD / 2, o, l);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -261,10 +482,10 @@ __global__ void __launch_bounds__(kThreads, (MT == 1) ? 2 : 1) k_pass_fp64r(cons
     auto load_a = [&](int ks, int mt, double (&a)[8]) {
         const int mtg = wm * MT + mt;
         if (mtg >= mtiles) return;
-        const double2 *q = reinterpret_cast<const double2 *>(F.A + ((size_t)(ks * mtiles + mtg) * 32 + lane) * 8);
+        const double2 *q = reinterpret_cast<const double2 *>(F.A + (size_t)(ks * mtiles + mtg) * 256) + lane;
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
-            const double2 v = __ldg(q + h);
+            const double2 v = __ldg(q + 32 * h);
             a[2 * h] = v.x;
             a[2 * h + 1] = v.y;
         }
@@ -317,9 +538,9 @@ __global__ void __launch_bounds__(kThreads, (MT == 1) ? 2 : 1) k_pass_fp64r(cons
                         re = 0.0;
                         im = 0.0;
                     } else {
-                        const double den = (F.E[o] + F.El[lg]) - lam;
-                        re = re / den;
-                        im = im / den;
+                        const double rden = 1.0 / ((F.E[o] + F.El[lg]) - lam);
+                        re *= rden;
+                        im *= rden;
                     }
                 }
                 const long long off = 2 * ((long long)(o + o1) * sk + (long long)(lg + o1) * sl);
@@ -359,13 +580,6 @@ static cudaError_t launch_pass_r(ductgpu_ctx ctx, const PassParams &pp, int grid
 // and one barrier per tile.  MTILES 8: warp w owns rows 16w..16w+15 and all
 // 64 columns; MTILES 4: warps w and w+4 share rows 16(w&3).. and split the
 // columns.
-__device__ __forceinline__ void cp_async16_zfill(void *smem, const void *gmem, bool valid)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    const int n = valid ? 16 : 0;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
-}
-
 template <int KS, int MTILES>
 __global__ void __launch_bounds__(kThreads, 1) k_pass_fp64p(const __grid_constant__ PassParams p, int ntiles)
 {
@@ -426,10 +640,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_fp64p(const __grid_constan
             a_src = F.A;
 #pragma unroll
             for (int ks = 0; ks < KS; ++ks) {
-                const double2 *q = reinterpret_cast<const double2 *>(F.A + ((size_t)(ks * MTILES + mtg) * 32 + lane) * 8);
+                const double2 *q = reinterpret_cast<const double2 *>(F.A + (size_t)(ks * MTILES + mtg) * 256) + lane;
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
-                    const double2 v = __ldg(q + h);
+                    const double2 v = __ldg(q + 32 * h);
                     a[ks][2 * h] = v.x;
                     a[ks][2 * h + 1] = v.y;
                 }
@@ -475,9 +689,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_pass_fp64p(const __grid_constan
                         re = 0.0;
                         im = 0.0;
                     } else {
-                        const double den = (F.E[o] + F.El[lg]) - lam;
-                        re = re / den;
-                        im = im / den;
+                        const double rden = 1.0 / ((F.E[o] + F.El[lg]) - lam);
+                        re *= rden;
+                        im *= rden;
                     }
                 }
                 const long long off = 2 * ((long long)(o + o1) * sk + (long long)(lg + o1) * sl);
@@ -513,6 +727,26 @@ static size_t pass_smem_bytes(int mtw, int kpad, int lines)
 {
     const size_t a_chunk = (size_t)(kKC / 16) * (4 * mtw) * 256;
     return (2 * a_chunk + (size_t)kpad * (2 * lines + 4)) * sizeof(double);
+}
+
+template <int MTW, int LINES>
+static cudaError_t launch_pass_s(ductgpu_ctx ctx, const PassParams &pp, int hpad_max)
+{
+    // LINES-line tiles: re-cut the callers' 32-line grid
+    PassParams q = pp;
+    int grid = 0;
+    for (int i = 0; i < q.nf; ++i) {
+        q.f[i].nchunks = (q.f[i].nlines + LINES - 1) / LINES;
+        q.cta_start[i] = grid;
+        grid += q.f[i].nmodes * q.f[i].nchunks;
+    }
+    q.cta_start[q.nf] = grid;
+    const size_t smem = pass_smem_bytes(MTW, 2 * hpad_max, LINES);
+    cudaError_t e = cudaFuncSetAttribute(k_pass_fp64s<MTW, LINES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    LaunchScope ls(ctx, DUCTGPU_K_PASS_FP64);
+    k_pass_fp64s<MTW, LINES><<<grid, kThreads, smem, ctx->stream>>>(q);
+    return cudaGetLastError();
 }
 
 template <int MTW, int LINES>
@@ -780,6 +1014,19 @@ int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid)
     if (mtw < 1 || mtw > 3) return set_error(ctx, DUCTGPU_EARG, "operator larger than %d", kMaxN);
     const int variant = ctx->pass_variant[mtw - 1];
     cudaError_t e;
+    if (pp.f[0].par) {
+        // flip-symmetric half operators: solve_fp64_ex sets every field or
+        // none, kpad = hpad = 32 mtw, and uses no residual epilogue
+        for (int i = 0; i < pp.nf; ++i)
+            if (!pp.f[i].par || pp.f[i].kpad != 32 * mtw || pp.residual)
+                return set_error(ctx, DUCTGPU_EARG, "flip-symmetric pass: inconsistent field %d", i);
+        switch (mtw) {
+        case 1: e = launch_pass_s<1, kParityLines>(ctx, pp, kpad_max); break;
+        case 2: e = launch_pass_s<2, kParityLines>(ctx, pp, kpad_max); break;
+        default: e = launch_pass_s<3, kParityLines>(ctx, pp, kpad_max); break;
+        }
+        return e == cudaSuccess ? DUCTGPU_OK : check_cuda(ctx, e, "k_pass_fp64s");
+    }
     bool uniform = true;
     for (int i = 1; i < pp.nf; ++i)
         uniform = uniform && pp.f[i].kpad == pp.f[0].kpad && pp.f[i].mtiles == pp.f[0].mtiles;
@@ -842,6 +1089,26 @@ static int pass_grid(PassParams &pp, const FieldTask *tasks, int ntasks)
 
 int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks) { return solve_fp64_ex(ctx, tasks, ntasks, false); }
 
+bool use_fold(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
+{
+    if (ctx->pass_variant[(ctx->dir.mtiles / 4) - 1] != DUCTGPU_PASS_PARITY) return false;
+    for (int i = 0; i < ntasks; ++i)
+        if (!((tasks[i].bound == 'n') ? ctx->neu : ctx->dir).fold_ok) return false;
+    return true;
+}
+
+void fold_field(PassField &f, const BoundOps &b, int par, const double *A, bool neumann)
+{
+    f.par = par;
+    f.A = A;
+    f.kpad = b.hpad;
+    f.mtiles = 2 * b.hpad / 16;
+    f.he = b.he;
+    f.ho = b.ho;
+    f.E = f.El = b.Eperm;
+    f.sing_io = f.sing_l = neumann ? b.sing_perm : -1;
+}
+
 int solve_fp64_ex(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks, bool emulate)
 {
     if (ntasks < 1 || ntasks > kMaxFields)
@@ -856,6 +1123,9 @@ int solve_fp64_ex(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks, bool emul
 
     PassParams pp{};
     pp.lam = ctx->lam;
+    // flip-symmetric half operators for all four passes (the intermediate
+    // mode order differs), when selected and every field's operators have them
+    const bool fold = !emulate && use_fold(ctx, tasks, ntasks);
     for (int i = 0; i < ntasks; ++i) {
         pp.f[i].nmodes = tasks[i].nmodes;
         pp.f[i].mode0 = tasks[i].mode0;
@@ -881,6 +1151,8 @@ int solve_fp64_ex(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks, bool emul
             pp.f[i].Ai8 = (pass < 2) ? b.Qi8 : b.Pi8;
             pp.f[i].Aexp = (pass < 2) ? b.Qexp8 : b.Pexp8;
             pass_geometry(pp.f[i], b, b.E, n, ypass ? 1 : m, ypass ? m : 1, ps);
+            if (fold)
+                fold_field(pp.f[i], b, (pass < 2) ? 1 : 2, (pass < 2) ? b.Qfold : b.Pfold, tasks[i].bound == 'n');
         }
         const int cta = pass_grid(pp, tasks, ntasks);
         pp.divide = (pass == 1);

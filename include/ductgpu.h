@@ -142,6 +142,11 @@ int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields,
 #define DUCTGPU_PASS_REGISTER 1
 #define DUCTGPU_PASS_STAGED16 2   /* STAGED with 16 lines per CTA (3 CTAs/SM) */
 #define DUCTGPU_PASS_PERSIST 3    /* persistent, operator in registers (n <= 127) */
+#define DUCTGPU_PASS_PARITY 4     /* STAGED on the flip-symmetric half operators: even and
+                                     odd eigenvectors in two blocks of half size, half the
+                                     flops (n <= 191; operators without the symmetry, e.g.
+                                     from ductgpu_set_operators, run STAGED)            */
+/* kernel -1 restores the library's defaults for the size class(es).      */
 int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel);
 /* Autotuner: times the FP64 batched solve of these device fields with each
  * pass kernel (reps runs each, after one warm-up; the fields' sol arrays
