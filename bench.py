@@ -11,8 +11,12 @@ lambda = kx^2 (kx = 0 singular, pinned as the reference does).  That is
 
 Arms:
 * default: the device-resident batched solve (ductgpu_solve_fields_dev) with
-  inputs in HBM; ``e2e`` times the reference-facing drop-in ductgpu_helm3d on
-  pinned host arrays (H2D + solve + D2H per field) for the same work.
+  inputs in HBM, replayed from the library's CUDA graphs of the step (one per
+  rotating input set); the per-kernel durations behind ``roofline`` come
+  from a second run of the same steps with a CUDA event pair around every
+  launch.  ``e2e`` times the reference-facing host-array entry
+  (ductgpu_helm3d_batch: H2D + solve + D2H of the four fields, copies
+  overlapped with the solves) for the same work.
 * ``--impl reference``: the reference's CPU algorithm (the oracle's
   restatement of helm3d/solvediag with the same LAPACK/BLAS calls) on all
   host cores.
@@ -225,12 +229,39 @@ def run_ours(args, world, rank, local, pg):
     pass_kernel = names[pass_id]
 
     def timed(prec):
+        # The step is replayed from CUDA graphs of the batched solve, one per
+        # rotating input set (the library's path for a repeated substep);
+        # direct calls if the precision's solve cannot be captured.
+        try:
+            graphs = [ctx.graph_create(sets[s], precision=prec) for s in range(2)]
+        except D.DuctGPUError:
+            graphs = None
+
+        def step(i):
+            if graphs:
+                ctx.graph_launch(graphs[i % 2])
+            else:
+                ctx.solve_fields_dev(sets[i % 2], prec)
+
         for i in range(args.warmup):
-            ctx.solve_fields_dev(sets[i % 2], prec)
+            step(i)
         ctx.synchronize()
         barrier(pg)
         clocks = ClockSampler(local)
         clocks.start()
+        ctx.event_record(0)
+        for i in range(args.steps):
+            step(i)
+        ctx.event_record(1)
+        ms = ctx.event_elapsed(0, 1)
+        ctx.synchronize()
+        clk = clocks.stop()
+        ms = max_over_ranks(pg, ms)
+        barrier(pg)
+        # Kernel durations for the roofline: the same steps as direct calls
+        # with a CUDA event pair around every launch (a second timed region;
+        # the events add gaps between launches, so the step time above is
+        # taken without them).
         ctx.profile(True)
         ctx.profile_reset()
         l0 = ctx.launch_count()
@@ -238,23 +269,24 @@ def run_ours(args, world, rank, local, pg):
         for i in range(args.steps):
             ctx.solve_fields_dev(sets[i % 2], prec)
         ctx.event_record(1)
-        ms = ctx.event_elapsed(0, 1)
+        ms_prof = ctx.event_elapsed(0, 1)
         ctx.synchronize()
         launches = ctx.launch_count() - l0
         prof = {k: ctx.profile_read(k) for k in (D.K_PASS_FP64, D.K_MIXED_GEMM, D.K_NEUMANN, D.K_WALLS, D.K_RESIDUAL)}
         ctx.profile(False)
-        clk = clocks.stop()
-        ms = max_over_ranks(pg, ms)
+        if graphs:
+            for g in graphs:
+                ctx.graph_destroy(g)
         barrier(pg)
-        return ms / args.steps, launches, prof, clk
+        return ms / args.steps, launches, prof, clk, ms_prof, bool(graphs)
 
     want = ["fp64", "mixed", "int8"] if args.precision == "auto" else [args.precision]
     res = {}
     for name in want:
         prec = {"fp64": D.PREC_FP64, "mixed": D.PREC_MIXED, "int8": D.PREC_INT8}[name]
-        ms_step, launches, prof, clk = timed(prec)
-        res[name] = dict(ms_step=ms_step, launches=launches, prof=prof, clk=clk,
-                         value=world * per_step / (ms_step * 1e-3))
+        ms_step, launches, prof, clk, ms_prof, graph = timed(prec)
+        res[name] = dict(ms_step=ms_step, launches=launches, prof=prof, clk=clk, ms_prof=ms_prof,
+                         graph=graph, value=world * per_step / (ms_step * 1e-3))
     # accuracy of the split paths against the FP64 passes on the same (full)
     # operators, which the split paths emulate; the flip-symmetric passes are
     # another decomposition of the operator (checked against the oracle by
@@ -305,7 +337,7 @@ def run_ours(args, world, rank, local, pg):
                            "frac": (ach / peak64) if (ach and peak64) else None,
                            "traffic": traffic,
                            "kernel": kname, "peak_source": peak64_note,
-                           "kernel_share_of_step": kms / (R["ms_step"] * args.steps)}
+                           "kernel_share_of_step": kms / R["ms_prof"]}
         elif name == "int8":
             kms, kn = R["prof"][D.K_MIXED_GEMM]
             # per launch: 28 slice products of the padded 128 x 128 operator
@@ -318,7 +350,7 @@ def run_ours(args, world, rank, local, pg):
                            "kernel": "k_pass_i8ws (tcgen05 kind::i8, 28 slice products, exact int32)",
                            "peak_source": "nominal dense int8 (no measured int8 peak on this pool)",
                            "fp64_equiv_tflops": (4.0 * n ** 3 * per_step) / ((kms / kn) * 1e-3) / 1e12 if kn else None,
-                           "kernel_share_of_step": kms / (R["ms_step"] * args.steps)}
+                           "kernel_share_of_step": kms / R["ms_prof"]}
         else:
             kms, kn = R["prof"][D.K_MIXED_GEMM]
             flops = 10 * 4.0 * n ** 3 * per_step     # 10 BF16 slice products per pass
@@ -328,7 +360,7 @@ def run_ours(args, world, rank, local, pg):
                            "traffic": traffic_from_profile("k_pass_mixed"),
                            "kernel": "k_pass_mixed (tcgen05 kind::f16, BF16 slices)",
                            "peak_source": "measured cuBLAS bf16 burst (MEASURED_PEAKS.json)",
-                           "kernel_share_of_step": kms / (R["ms_step"] * args.steps)}
+                           "kernel_share_of_step": kms / R["ms_prof"]}
 
     e2e = None
     if not args.no_e2e:
@@ -359,11 +391,14 @@ def run_ours(args, world, rank, local, pg):
                        "precision": best,
                        "parallelism": "replicas" if world > 1 else "1gpu",
                        "l2": "2 rotating input/output sets (272 MB) > 126 MB L2",
-                       "pass_kernel": pass_kernel},
+                       "pass_kernel": pass_kernel,
+                       "step": ("CUDA-graph replay of ductgpu_solve_fields_dev (one graph per rotating set)"
+                                if B["graph"] else "ductgpu_solve_fields_dev calls"),
+                       "kernel_timing": "per-launch CUDA events in a second run of the same steps"},
             "gpu_launches": B["launches"],
             "roofline": roofs[best], "cpu_baseline": cpu, "e2e": e2e, "clocks": B["clk"],
             "paths": {k: {"value": v["value"], "ms_per_step": v["ms_step"], "roofline": roofs[k],
-                          "gpu_launches": v["launches"]} for k, v in res.items()},
+                          "gpu_launches": v["launches"], "graph": v["graph"]} for k, v in res.items()},
             "mixed_rel_err_vs_fp64": acc,
             "int8_rel_err_vs_fp64": acc8,
             "hbm_kernels": hbm,
