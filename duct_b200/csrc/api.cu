@@ -477,6 +477,10 @@ int ductgpu_helm3d(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, char bou
 // context stream and field i-2 copied back on a third.  Each solve is the
 // whole field's batch.  From pinned host memory (ductgpu_host_alloc) the
 // copies run asynchronously; pageable memory gives the same results.
+// mode ranges per field in ductgpu_helm3d_batch: 2 and 4 were measured no
+// faster at cfg1 (the host link is the limit; more pieces add launches)
+constexpr int kBatchPieces = 1;
+
 int ductgpu_helm3d_batch(ductgpu_ctx ctx, int nfields, double *const *rhs, double *const *sol, const char *bounds,
                          const double *alambdas, int my, int mz, int ib, int ie, const double *xalp, int precision)
 {
@@ -489,6 +493,8 @@ int ductgpu_helm3d_batch(ductgpu_ctx ctx, int nfields, double *const *rhs, doubl
     if (ie < ib || ib < 0) return set_error(ctx, DUCTGPU_EARG, "ib=%d ie=%d", ib, ie);
     if (precision != DUCTGPU_PREC_FP64 && precision != DUCTGPU_PREC_INT8 && precision != DUCTGPU_PREC_MIXED)
         return set_error(ctx, DUCTGPU_EARG, "precision %d", precision);
+    if (precision == DUCTGPU_PREC_INT8 && ctx->my - 2 > 127)
+        return set_error(ctx, DUCTGPU_EARG, "int8-emulated solve: my=%d (at most 129)", ctx->my);
     for (int i = 0; i < nfields; ++i) {
         if (!rhs[i] || !sol[i]) return set_error(ctx, DUCTGPU_EARG, "null field %d", i);
         if (bounds[i] != 'd' && bounds[i] != 'n') return set_error(ctx, DUCTGPU_EARG, "bound '%c'", bounds[i]);
@@ -506,7 +512,57 @@ int ductgpu_helm3d_batch(ductgpu_ctx ctx, int nfields, double *const *rhs, doubl
     const size_t doubles = (size_t)2 * my * mz * nm, bytes = doubles * sizeof(double);
     int rc = ensure(ctx, ctx->io, 2 * bytes * nfields);
     if (rc) return rc;
-    // helm3d zeroes the Dirichlet walls of rhs in place (src/helm3d.f90:48-60)
+    ductgpu_field f[kMaxFields];
+    for (int i = 0; i < nfields; ++i) {
+        f[i].rhs = ctx->io.buf + 2 * doubles * i;
+        f[i].sol = f[i].rhs + doubles;
+        f[i].xalp = xalp;
+        f[i].alambda = alambdas[i];
+        f[i].ib = ib;
+        f[i].nmodes = nm;
+        f[i].bound = bounds[i];
+    }
+    // lambda of every plane of the batch staged and uploaded once, before the
+    // first field copy is queued (a per-solve upload would wait behind the
+    // field copies on the copy engines, and the per-call staging sync would
+    // hold the host until the previous solve ended)
+    FieldTask tasks[kMaxFields];
+    if ((rc = prepare(ctx, f, nfields, tasks))) return rc;
+    // Each field goes through in kBatchPieces mode ranges: piece j is copied
+    // in while piece j-1 is solved and piece j-2 copied back, so both
+    // directions of the host link run at once for all but the first and the
+    // last piece.  Events are reused round-robin: every wait on an event is
+    // enqueued before the event is recorded again.
+    const int pieces = nm < kBatchPieces ? nm : kBatchPieces;
+    const size_t plane = (size_t)2 * my * mz;
+    int e = 0;
+    for (int i = 0; i < nfields; ++i)
+        for (int p = 0; p < pieces; ++p, ++e) {
+            const int k0 = nm * p / pieces, k1 = nm * (p + 1) / pieces;
+            FieldTask t = tasks[i];
+            t.rhs = f[i].rhs + plane * k0;
+            t.sol = f[i].sol + plane * k0;
+            t.nmodes = k1 - k0;
+            t.mode0 = (ib + k0 == 0);
+            t.plane0 = tasks[i].plane0 + k0;
+            const size_t pb = plane * (k1 - k0) * sizeof(double);
+            cudaEvent_t ein = ctx->ev_in[e % ductgpu_ctx_s::kPipeChunks];
+            cudaEvent_t eout = ctx->ev_out[e % ductgpu_ctx_s::kPipeChunks];
+            DUCT_CUDA(ctx, cudaMemcpyAsync(t.rhs, rhs[i] + plane * k0, pb, cudaMemcpyHostToDevice, ctx->cp_in));
+            DUCT_CUDA(ctx, cudaEventRecord(ein, ctx->cp_in));
+            DUCT_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ein, 0));
+            rc = (precision == DUCTGPU_PREC_MIXED) ? solve_mixed(ctx, &t, 1)
+                                                   : solve_fp64_ex(ctx, &t, 1, precision == DUCTGPU_PREC_INT8);
+            if (rc) return rc;
+            DUCT_CUDA(ctx, cudaEventRecord(eout, ctx->stream));
+            DUCT_CUDA(ctx, cudaStreamWaitEvent(ctx->cp_out, eout, 0));
+            DUCT_CUDA(ctx, cudaMemcpyAsync(sol[i] + plane * k0, t.sol, pb, cudaMemcpyDeviceToHost, ctx->cp_out));
+        }
+    // helm3d zeroes the Dirichlet walls of rhs in place (src/helm3d.f90:48-60).
+    // Done here, while the copies and solves run: the solve reads only the
+    // interior of rhs (the device copy's walls are zeroed on the device), so
+    // whether a wall value reaches the device before or after it is zeroed
+    // does not matter.
     for (int i = 0; i < nfields; ++i)
         if (bounds[i] == 'd')
             for (int k = 0; k < nm; ++k) {
@@ -520,25 +576,6 @@ int ductgpu_helm3d_batch(ductgpu_ctx ctx, int nfields, double *const *rhs, doubl
                     r[2 * (my - 1 + (size_t)my * q)] = r[2 * (my - 1 + (size_t)my * q) + 1] = 0.0;
                 }
             }
-    ductgpu_field f[kMaxFields];
-    for (int i = 0; i < nfields; ++i) {
-        f[i].rhs = ctx->io.buf + 2 * doubles * i;
-        f[i].sol = f[i].rhs + doubles;
-        f[i].xalp = xalp;
-        f[i].alambda = alambdas[i];
-        f[i].ib = ib;
-        f[i].nmodes = nm;
-        f[i].bound = bounds[i];
-    }
-    for (int i = 0; i < nfields; ++i) {
-        DUCT_CUDA(ctx, cudaMemcpyAsync(f[i].rhs, rhs[i], bytes, cudaMemcpyHostToDevice, ctx->cp_in));
-        DUCT_CUDA(ctx, cudaEventRecord(ctx->ev_in[i], ctx->cp_in));
-        DUCT_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_in[i], 0));
-        if ((rc = ductgpu_solve_fields_dev(ctx, &f[i], 1, precision))) return rc;
-        DUCT_CUDA(ctx, cudaEventRecord(ctx->ev_out[i], ctx->stream));
-        DUCT_CUDA(ctx, cudaStreamWaitEvent(ctx->cp_out, ctx->ev_out[i], 0));
-        DUCT_CUDA(ctx, cudaMemcpyAsync(sol[i], f[i].sol, bytes, cudaMemcpyDeviceToHost, ctx->cp_out));
-    }
     DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->cp_out));
     rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d_batch");
     return rc ? rc : (precision != DUCTGPU_PREC_FP64 ? device_status(ctx) : DUCTGPU_OK);
