@@ -202,6 +202,7 @@ int ductgpu_destroy(ductgpu_ctx ctx)
     for (int i = 0; i < ductgpu_ctx_s::kMaxGraphs; ++i)
         if (ctx->graph_exec[i]) { cudaGraphExecDestroy(ctx->graph_exec[i]); cudaFree(ctx->graph_lam[i]); }
     cudaFree(ctx->xcol); cudaFree(ctx->DC); cudaFree(ctx->D2); cudaFree(ctx->AM1); cudaFree(ctx->ccw);
+    cudaFree(ctx->dcr); cudaFree(ctx->pin_cc);
     cudaFree(ctx->work.buf);
     cudaFree(ctx->io.buf);
     if (ctx->cp_in) {
@@ -468,7 +469,7 @@ int ductgpu_helm3d(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, char bou
     if (rc) return rc;
     DUCT_CUDA(ctx, cudaMemcpyAsync(sol, dsol, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d");
-    return rc ? rc : (precision != DUCTGPU_PREC_FP64 ? device_status(ctx) : DUCTGPU_OK);
+    return rc ? rc : device_status(ctx);
 }
 
 // Several fields of one substep on host arrays (u, v, w and p of
@@ -578,7 +579,7 @@ int ductgpu_helm3d_batch(ductgpu_ctx ctx, int nfields, double *const *rhs, doubl
             }
     DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->cp_out));
     rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "helm3d_batch");
-    return rc ? rc : (precision != DUCTGPU_PREC_FP64 ? device_status(ctx) : DUCTGPU_OK);
+    return rc ? rc : device_status(ctx);
 }
 
 static int check_field(ductgpu_ctx ctx, const void *a, int my, int mz, int nmodes)

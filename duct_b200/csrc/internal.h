@@ -98,12 +98,15 @@ struct ductgpu_ctx_s {
     bool ready = false;
     double *xcol = nullptr;    // [my]
     double *DC = nullptr;      // [my*my]
+    double *dcr = nullptr;     // [2*my] rows 1 and my of DC, contiguous (Neumann walls)
+    double *pin_cc = nullptr;  // [2*64] point-gauge coefficients of singular planes
     double *D2 = nullptr;      // [my*my]
     double *AM1 = nullptr;     // [16] device copy
     double *ccw = nullptr;     // [my] Clenshaw-Curtis weights on the nodes
     double wanted = 0.0;
     int gauge = DUCTGPU_GAUGE_POINT;
     int refine_steps = 2;      // FP64 refinement steps of the split-precision path
+    int parity_ws = 1;         // flip-symmetric passes at hpad 32 / 64: warp-specialised persistent kernel
     int i8_kernel = 1;         // int8-emulated passes: 0 sequential, 1 warp-specialised pipeline
     // GEMM-pass kernel per operator size class (n <= 63, <= 127, <= 191),
     // one of DUCTGPU_PASS_* (ductgpu_set_pass_kernel, ductgpu_autotune);
@@ -244,6 +247,9 @@ struct PassParams {
 };
 constexpr int kPassLines = 32;
 int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid);
+// solve_fp64ws.cu: the flip-symmetric pass as a warp-specialised persistent
+// kernel (hpad 32 or 64, every field folded, no residual epilogue)
+cudaError_t fp64_pass_ws(ductgpu_ctx ctx, const PassParams &pp, int hpad);
 // Whether a solve (or its adjoint) over these fields runs the flip-symmetric
 // passes: DUCTGPU_PASS_PARITY selected for the size class and every field's
 // operators have the folded form.  The forward and adjoint take the same

@@ -585,7 +585,8 @@ int pseudomat_gpu(ductgpu_ctx ctx, int m)
         return set_error(ctx, DUCTGPU_EARG, "pseudomat: my=%d outside [5,%d]", m, kMaxN + 2);
     const int n = m - 2;
     cudaFree(ctx->xcol); cudaFree(ctx->DC); cudaFree(ctx->D2); cudaFree(ctx->AM1); cudaFree(ctx->ccw);
-    ctx->xcol = ctx->DC = ctx->D2 = ctx->AM1 = ctx->ccw = nullptr;
+    cudaFree(ctx->dcr);
+    ctx->xcol = ctx->DC = ctx->D2 = ctx->AM1 = ctx->ccw = ctx->dcr = nullptr;
     free_bound(ctx->dir);
     free_bound(ctx->neu);
     ctx->ready = false;
@@ -604,6 +605,11 @@ int pseudomat_gpu(ductgpu_ctx ctx, int m)
     double *blk = nullptr;
     DUCT_CUDA(ctx, cudaMalloc(&blk, (size_t)n * n * sizeof(double)));
     k_build_dc<<<blocks_for((long)m * m), 256, 0, ctx->stream>>>(m, ctx->xcol, ctx->DC);
+    DUCT_CUDA(ctx, cudaMalloc(&ctx->dcr, 2 * (size_t)m * sizeof(double)));
+    k_copy_row<<<1, 256, 0, ctx->stream>>>(m, ctx->DC, 0, ctx->dcr);
+    k_copy_row<<<1, 256, 0, ctx->stream>>>(m, ctx->DC, m - 1, ctx->dcr + m);
+    if (!ctx->pin_cc) DUCT_CUDA(ctx, cudaMalloc(&ctx->pin_cc, 2 * 64 * sizeof(double)));
+    ctx->launches += 2;
     k_matmul<<<blocks_for((long)m * m), 256, 0, ctx->stream>>>(m, ctx->DC, ctx->DC, ctx->D2);
     k_block<<<blocks_for((long)n * n), 256, 0, ctx->stream>>>(m, 0, ctx->DC, ctx->D2, blk);
     ctx->launches += 3;

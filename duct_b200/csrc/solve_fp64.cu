@@ -288,6 +288,13 @@ __global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)
     const int wm = warp & 3, wn = warp >> 2;
     const int g = lane >> 2, t = lane & 3;
     const int kb0 = (wm * MTW * 16 >= H) ? H : 0;   // this warp's half of the staged rows
+    // eigenvalues of the divide epilogue in shared memory (E of every row,
+    // El of the CTA's lines), staged while the operator and lines arrive
+    double *Es = Bs + rows * NLD;
+    if (F.par == 1 && p.divide) {
+        for (int i = tid; i < n; i += kThreads) Es[i] = F.E[i];
+        for (int i = tid; i < L; i += kThreads) Es[rows + i] = F.El[l0 + i];
+    }
     double acc[MTW][NTW][4];
 #pragma unroll
     for (int i = 0; i < MTW; ++i)
@@ -355,7 +362,7 @@ __global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)
                             re = 0.0;
                             im = 0.0;
                         } else {
-                            const double rden = 1.0 / ((F.E[o] + F.El[lg]) - lam);
+                            const double rden = 1.0 / ((Es[o] + Es[rows + l]) - lam);
                             re *= rden;
                             im *= rden;
                         }
@@ -741,7 +748,8 @@ static cudaError_t launch_pass_s(ductgpu_ctx ctx, const PassParams &pp, int hpad
         grid += q.f[i].nmodes * q.f[i].nchunks;
     }
     q.cta_start[q.nf] = grid;
-    const size_t smem = pass_smem_bytes(MTW, 2 * hpad_max, LINES);
+    // + the eigenvalue staging of the divide epilogue (n <= 2 hpad rows, LINES lines)
+    const size_t smem = pass_smem_bytes(MTW, 2 * hpad_max, LINES) + (size_t)(2 * hpad_max + LINES) * sizeof(double);
     cudaError_t e = cudaFuncSetAttribute(k_pass_fp64s<MTW, LINES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     LaunchScope ls(ctx, DUCTGPU_K_PASS_FP64);
@@ -815,6 +823,7 @@ __global__ void k_zero_walls(const __grid_constant__ WallParams p)
 // Neumann walls, corners and the singular kx=0 mode: src/solvediag.f90:
 // 161-206 (pin), 250-276 (wall lines from DC), 278-322 (corners via AM1).
 // One CTA per complex plane; the interior is already solved.
+constexpr int kMaxSing = 64;   // singular planes per pin launch
 struct FillParams {
     double *sol[kMaxFields];
     int mode0[kMaxFields];
@@ -822,6 +831,9 @@ struct FillParams {
     int cta_start[kMaxFields + 1];
     int nf;
     const double *DC, *AM1, *ccw, *pcol, *lam;
+    const double *dcr;          // rows 1 and m of DC, contiguous
+    double *pin_cc;             // [2 * kMaxSing] point-gauge coefficients
+    int sing_fi[kMaxSing], sing_plane[kMaxSing], nsing;
     double wanted;
     int m, io, gauge;
     long long plane_stride;
@@ -856,24 +868,32 @@ __device__ __forceinline__ int fill_field(const FillParams &p)
     return fi;
 }
 
-// Singular kx=0 Neumann plane: U = U0 + c p p^T with
-// c = (wanted - U0(io,io)) / p(io)^2, so that the interior point
-// (iofzero+1, iofzero+1) takes the value wanted (src/solvediag.f90:195-206,
-// the reference's choice of FT(iofzero,iofzero)).  One CTA per plane: the
-// pinned value is read before any thread writes.
-__global__ void __launch_bounds__(1024) k_neumann_pin(const __grid_constant__ FillParams p)
+// Point gauge of the singular planes (|lambda| <= 1e-10, the kx = 0
+// pressure mode): the field plus c P(:,io) P(:,io)^T, with c chosen so that
+// the point (iofzero+1, iofzero+1) takes the value wanted
+// (src/solvediag.f90:195-206, the reference's choice of FT(iofzero,iofzero)).
+// Two steps, so that the update can be spread over many CTAs: k_pin_coef
+// reads the point of every listed plane and stores c; k_pin_apply reads c,
+// never the point it may be changing.
+__global__ void k_pin_coef(const __grid_constant__ FillParams p)
 {
-    const int fi = fill_field(p);
-    const int plane = blockIdx.x - p.cta_start[fi];
-    const double lam = p.lam[p.plane0[fi] + plane];
-    if (!(fabs(lam) <= 1.0e-10) || p.io < 0) return;
-    const int m = p.m, n = m - 2, io = p.io;
-    double2 *U = reinterpret_cast<double2 *>(p.sol[fi] + (long long)plane * p.plane_stride);
+    const int s = threadIdx.x;
+    if (s >= p.nsing) return;
+    const int m = p.m, io = p.io;
+    const double2 *U = reinterpret_cast<const double2 *>(p.sol[p.sing_fi[s]] + (long long)p.sing_plane[s] * p.plane_stride);
     const double2 u0 = U[(io + 1) + (long long)m * (io + 1)];
-    __syncthreads();
     const double pio = p.pcol[io];
-    const double2 cc = make_double2((p.wanted - u0.x) / (pio * pio), (p.wanted - u0.y) / (pio * pio));
-    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    p.pin_cc[2 * s] = (p.wanted - u0.x) / (pio * pio);
+    p.pin_cc[2 * s + 1] = (p.wanted - u0.y) / (pio * pio);
+}
+
+// blockIdx.y: the listed plane; the CTAs along x split its n x n interior
+__global__ void __launch_bounds__(256) k_pin_apply(const __grid_constant__ FillParams p)
+{
+    const int s = blockIdx.y, m = p.m, n = m - 2;
+    double2 *U = reinterpret_cast<double2 *>(p.sol[p.sing_fi[s]] + (long long)p.sing_plane[s] * p.plane_stride);
+    const double2 cc = make_double2(p.pin_cc[2 * s], p.pin_cc[2 * s + 1]);
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n; idx += gridDim.x * blockDim.x) {
         const int i = idx % n, j = idx / n;
         const double w = p.pcol[i] * p.pcol[j];
         double2 &u = U[(i + 1) + (long long)m * (j + 1)];
@@ -902,9 +922,10 @@ __global__ void __launch_bounds__(256) k_neumann_walls(const __grid_constant__ F
         const int j = 1 + blockIdx.y * 8 + warp;
         if (j >= m - 1) return;
         double sl[4] = {0, 0, 0, 0};
+#pragma unroll 4
         for (int i = 1 + lane; i < m - 1; i += 32) {
             const double2 v = U[i + (long long)m * j];
-            const double a = DC[(long long)m * i], b = DC[(m - 1) + (long long)m * i];
+            const double a = p.dcr[i], b = p.dcr[m + i];
             sl[0] += a * v.x; sl[1] += a * v.y; sl[2] += b * v.x; sl[3] += b * v.y;
         }
 #pragma unroll
@@ -918,9 +939,10 @@ __global__ void __launch_bounds__(256) k_neumann_walls(const __grid_constant__ F
         const int i = 1 + (blockIdx.y - nyb) * 32 + lane;
         double sb0 = 0, sb1 = 0, st0 = 0, st1 = 0;
         if (i < m - 1)
+#pragma unroll 8
             for (int j = 1 + warp; j < m - 1; j += 8) {
                 const double2 v = U[i + (long long)m * j];
-                const double a = DC[(long long)m * j], b = DC[(m - 1) + (long long)m * j];
+                const double a = p.dcr[j], b = p.dcr[m + j];
                 sb0 += a * v.x; sb1 += a * v.y; st0 += b * v.x; st1 += b * v.y;
             }
         part[warp][lane][0] = sb0; part[warp][lane][1] = sb1;
@@ -947,10 +969,9 @@ __global__ void __launch_bounds__(256) k_neumann_corners(const __grid_constant__
     const int m = p.m;
     double2 *U = reinterpret_cast<double2 *>(p.sol[fi] + (long long)plane * p.plane_stride);
     auto u = [&](int i, int j) -> double2 & { return U[i + (long long)m * j]; };
-    const double *DC = p.DC;
     double f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int i = 1 + threadIdx.x; i < m - 1; i += blockDim.x) {
-        const double a = DC[(long long)m * i], b = DC[(m - 1) + (long long)m * i];
+        const double a = p.dcr[i], b = p.dcr[m + i];
         const double2 ui0 = u(i, 0), u0i = u(0, i), umi = u(m - 1, i), uim = u(i, m - 1);
         f[0] += -a * (ui0.x + u0i.x);            f[1] += -a * (ui0.y + u0i.y);
         f[2] += -a * umi.x + b * ui0.x;          f[3] += -a * umi.y + b * ui0.y;
@@ -1020,6 +1041,14 @@ int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid)
         for (int i = 0; i < pp.nf; ++i)
             if (!pp.f[i].par || pp.f[i].kpad != 32 * mtw || pp.residual)
                 return set_error(ctx, DUCTGPU_EARG, "flip-symmetric pass: inconsistent field %d", i);
+        // the persistent warp-specialised form pays one operator load per
+        // CTA: used when every SM gets several 16-line tiles
+        long long tiles = 0;
+        for (int i = 0; i < pp.nf; ++i) tiles += (long long)pp.f[i].nmodes * ((pp.f[i].nlines + 15) / 16);
+        if (ctx->parity_ws && mtw <= 2 && tiles >= 6LL * ctx->num_sms) {
+            e = fp64_pass_ws(ctx, pp, 32 * mtw);
+            return e == cudaSuccess ? DUCTGPU_OK : check_cuda(ctx, e, "k_pass_fp64w");
+        }
         switch (mtw) {
         case 1: e = launch_pass_s<1, kParityLines>(ctx, pp, kpad_max); break;
         case 2: e = launch_pass_s<2, kParityLines>(ctx, pp, kpad_max); break;
@@ -1203,6 +1232,8 @@ int neumann_fill(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
     if (!fp.nf) return DUCTGPU_OK;
     fp.cta_start[fp.nf] = cta;
     fp.DC = ctx->DC;
+    fp.dcr = ctx->dcr;
+    fp.pin_cc = ctx->pin_cc;
     fp.AM1 = ctx->AM1;
     fp.ccw = ctx->ccw;
     fp.pcol = ctx->neu.pcol;
@@ -1213,16 +1244,35 @@ int neumann_fill(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
     fp.gauge = ctx->gauge;
     fp.plane_stride = 2LL * ctx->my * ctx->my;
     // the pin only acts on singular planes (|lambda| <= 1e-10, the kx=0
-    // pressure mode): launched only when the batch has one
-    bool any_singular = false;
-    for (int i = 0; i < ntasks && fp.io >= 0; ++i)
-        if (tasks[i].bound == 'n')
-            for (int k = 0; k < tasks[i].nmodes; ++k)
-                any_singular |= fabs(ctx->lam_host[tasks[i].plane0 + k]) <= 1.0e-10;
-    if (any_singular) {
-        LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
-        k_neumann_pin<<<cta, 1024, 0, ctx->stream>>>(fp);
+    // pressure mode): listed on the host, launched only when there are any,
+    // kMaxSing planes per launch pair
+    auto pin = [&]() -> int {
+        if (!fp.nsing) return DUCTGPU_OK;
+        {
+            LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
+            k_pin_coef<<<1, kMaxSing, 0, ctx->stream>>>(fp);
+        }
+        {
+            LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
+            k_pin_apply<<<dim3(32, fp.nsing), 256, 0, ctx->stream>>>(fp);
+        }
+        fp.nsing = 0;
+        return check_cuda(ctx, cudaGetLastError(), "k_pin");
+    };
+    for (int i = 0, f = 0; i < ntasks && fp.io >= 0; ++i) {
+        if (tasks[i].bound != 'n') continue;
+        for (int k = 0; k < tasks[i].nmodes; ++k)
+            if (fabs(ctx->lam_host[tasks[i].plane0 + k]) <= 1.0e-10) {
+                fp.sing_fi[fp.nsing] = f;
+                fp.sing_plane[fp.nsing] = k;
+                if (++fp.nsing == kMaxSing) {
+                    int rc = pin();
+                    if (rc) return rc;
+                }
+            }
+        ++f;
     }
+    if (int rc = pin()) return rc;
     {
         const int n = ctx->my - 2, nyb = (n + 7) / 8, nzb = (n + 31) / 32;
         LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
