@@ -326,8 +326,15 @@ def run_ours(args, world, rank, local, pg):
                 # columns per plane: the flops the flip-symmetric pass executes
                 he, ho = (n + 1) // 2, n // 2
                 flops = 4.0 * n * (he * he + ho * ho) * per_step
-                kname = "k_pass_fp64s (flip-symmetric half blocks, FP64 DMMA m16n8k16)"
-                traffic = traffic_from_profile("k_pass_fp64s")
+                # the library's rule: the warp-specialised persistent kernel
+                # for half blocks of 32 / 64 rows and >= 6 16-line tiles per SM
+                tiles = per_step * ((n + 15) // 16)
+                if ((he + 31) // 32) * 32 <= 64 and tiles >= 6 * torch_sm_count():
+                    kname = "k_pass_fp64w (flip-symmetric half blocks, warp-specialised persistent, FP64 DMMA m16n8k16)"
+                    traffic = traffic_from_profile("k_pass_fp64w")
+                else:
+                    kname = "k_pass_fp64s (flip-symmetric half blocks, FP64 DMMA m16n8k16)"
+                    traffic = traffic_from_profile("k_pass_fp64s")
             else:
                 flops = 4.0 * n ** 3 * per_step          # n x n operator on 2n real columns per plane
                 kname = "k_pass_fp64 (FP64 DMMA m16n8k16)"
@@ -419,6 +426,11 @@ def fp64_peak():
         d = json.load(open(p))
         return d["fp64_tflops"], "measured cuBLAS DGEMM on this pool (profiles/measured_fp64_peak.json)"
     return None, "no measured FP64 peak available"
+
+
+def torch_sm_count():
+    import torch
+    return torch.cuda.get_device_properties(0).multi_processor_count
 
 
 def traffic_from_profile(kernel):
