@@ -161,3 +161,51 @@ def test_parity_batched_fields_match_single_solves(parity):
     finally:
         for x in keep:
             x.free()
+
+
+def test_warp_specialised_pass_matches_small_batches(parity, oracle):
+    """A cfg1-sized batch (4 fields x 64 modes at my = 129: 2048 tiles of 16
+    lines, >= 6 per SM) runs the warp-specialised persistent kernel; the same
+    fields in batches of 8 modes run the 3-CTA-per-SM kernel.  Same fragment
+    order, K order and epilogue arithmetic: equal bit for bit.  A few planes
+    are also checked against the oracle (bounds of the module docstring)."""
+    ctx = parity
+    m, nm, chunk = 129, 64, 8
+    ctx.pseudomat(m)
+    xalp = 0.5 * np.arange(nm)
+    specs = [("d", 4.0e6), ("d", 1.0), ("d", 4.0e6), ("n", 0.0)]
+    rhs = [synth.chebyshev_rhs(m, m, nm, seed=60 + i, ib=0) for i in range(len(specs))]
+    keep = []
+    try:
+        big = []
+        for (b, lam), f in zip(specs, rhs):
+            r, s = ctx.device_array(f.shape), ctx.device_array(f.shape)
+            r.upload(f)
+            keep += [r, s]
+            big.append(dict(rhs=r, sol=s, xalp=xalp, alambda=lam, ib=0, bound=b))
+        ctx.solve_fields_dev(big)
+        ctx.synchronize()
+        whole = [f["sol"].download() for f in big]
+        for k0 in range(0, nm, chunk):
+            small = []
+            for (b, lam), f in zip(specs, rhs):
+                part = np.asfortranarray(f[:, :, k0:k0 + chunk])
+                r, s = ctx.device_array(part.shape), ctx.device_array(part.shape)
+                r.upload(part)
+                keep += [r, s]
+                small.append(dict(rhs=r, sol=s, xalp=xalp[k0:k0 + chunk], alambda=lam, ib=k0, bound=b))
+            ctx.solve_fields_dev(small)
+            ctx.synchronize()
+            for f, w in zip(small, whole):
+                assert np.array_equal(f["sol"].download(), w[:, :, k0:k0 + chunk]), k0
+        ops = oracle.Ops(m)
+        for (b, lam), f, w in zip(specs, rhs, whole):
+            for k in (0, 1, 63):
+                ref, _ = oracle.helm3d(np.asfortranarray(f[:, :, k:k + 1]), ops, b, lam, xalp[k:k + 1], ib=k)
+                got = w[:, :, k:k + 1]
+                if b == "n" and k == 0:
+                    got, ref = got - got.mean(), ref - ref.mean()
+                assert rel(got, ref) < (TOL_D if b == "d" else TOL_NEU), (b, k)
+    finally:
+        for x in keep:
+            x.free()
