@@ -873,8 +873,8 @@ __device__ __forceinline__ int fill_field(const FillParams &p)
 // the point (iofzero+1, iofzero+1) takes the value wanted
 // (src/solvediag.f90:195-206, the reference's choice of FT(iofzero,iofzero)).
 // Two steps, so that the update can be spread over many CTAs: k_pin_coef
-// reads the point of every listed plane and stores c; k_pin_apply reads c,
-// never the point it may be changing.
+// reads the point of every listed plane and stores c; k_neumann_partials
+// applies it block by block and never reads the point it may be changing.
 __global__ void k_pin_coef(const __grid_constant__ FillParams p)
 {
     const int s = threadIdx.x;
@@ -887,88 +887,104 @@ __global__ void k_pin_coef(const __grid_constant__ FillParams p)
     p.pin_cc[2 * s + 1] = (p.wanted - u0.y) / (pio * pio);
 }
 
-// blockIdx.y: the listed plane; the CTAs along x split its n x n interior
-__global__ void __launch_bounds__(256) k_pin_apply(const __grid_constant__ FillParams p)
+// Neumann walls, corners and (for the zero-mean gauge) the constant shift,
+// in two kernels that read each interior plane once.
+// k_neumann_partials: one CTA per 32 x 32 interior block (blockIdx.y =
+// T tz + ty, T = ceil(n / 32) blocks a direction) applies the point gauge to its block (singular planes, c from
+// k_pin_coef) and writes, for each of its columns, the sums over its rows
+// of DC(1,i) U(i,j) and DC(m,i) U(i,j) (the y walls' dot products,
+// src/solvediag.f90:253-264), and for each of its rows the sums over its
+// columns of DC(1,j) U(i,j) and DC(m,j) U(i,j) (the z walls, :265-276).
+// k_neumann_finish: one CTA per plane adds the T blocks' partial sums in
+// a fixed order, writes the wall lines, then the corners through AM1
+// (:278-322) and, for the zero-mean gauge, the constant shift.
+__global__ void __launch_bounds__(256) k_neumann_partials(const __grid_constant__ FillParams p, double *part)
 {
-    const int s = blockIdx.y, m = p.m, n = m - 2;
-    double2 *U = reinterpret_cast<double2 *>(p.sol[p.sing_fi[s]] + (long long)p.sing_plane[s] * p.plane_stride);
-    const double2 cc = make_double2(p.pin_cc[2 * s], p.pin_cc[2 * s + 1]);
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n * n; idx += gridDim.x * blockDim.x) {
-        const int i = idx % n, j = idx / n;
-        const double w = p.pcol[i] * p.pcol[j];
-        double2 &u = U[(i + 1) + (long long)m * (j + 1)];
-        u = make_double2(u.x + w * cc.x, u.y + w * cc.y);
+    __shared__ double zs[8][32][4];
+    const int fi = fill_field(p);
+    const int plane = blockIdx.x - p.cta_start[fi], gp = blockIdx.x;
+    const int m = p.m, n = m - 2, np = gridDim.x, T = (n + 31) / 32;
+    const int ty = blockIdx.y % T, tz = blockIdx.y / T;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double2 *U = reinterpret_cast<double2 *>(p.sol[fi] + (long long)plane * p.plane_stride);
+    int sg = -1;
+    for (int q = 0; q < p.nsing; ++q)
+        if (p.sing_fi[q] == fi && p.sing_plane[q] == plane) sg = q;
+    const double2 cc = (sg >= 0) ? make_double2(p.pin_cc[2 * sg], p.pin_cc[2 * sg + 1]) : make_double2(0.0, 0.0);
+    const int i = 1 + ty * 32 + lane;
+    const bool iok = i <= n;
+    const double ai = iok ? p.dcr[i] : 0.0, bi = iok ? p.dcr[m + i] : 0.0;
+    const double pin_i = (sg >= 0 && iok) ? p.pcol[i - 1] : 0.0;
+    double z[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int j = 1 + tz * 32 + warp * 4 + c;
+        const bool jok = j <= n;
+        double2 v = make_double2(0.0, 0.0);
+        if (iok && jok) {
+            v = U[i + (long long)m * j];
+            if (sg >= 0) {
+                const double w = pin_i * p.pcol[j - 1];
+                v = make_double2(v.x + w * cc.x, v.y + w * cc.y);
+                U[i + (long long)m * j] = v;
+            }
+        }
+        double y[4] = {ai * v.x, ai * v.y, bi * v.x, bi * v.y};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            for (int o = 16; o > 0; o >>= 1) y[q] += __shfl_xor_sync(0xffffffffu, y[q], o);
+        if (lane == 0 && jok) {
+            double *py = part + ((long long)(gp * T + ty) * m + j) * 4;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) py[q] = y[q];
+        }
+        const double aj = jok ? p.dcr[j] : 0.0, bj = jok ? p.dcr[m + j] : 0.0;
+        z[0] += aj * v.x; z[1] += aj * v.y; z[2] += bj * v.x; z[3] += bj * v.y;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) zs[warp][lane][q] = z[q];
+    __syncthreads();
+    if (warp == 0 && iok) {
+        double *pz = part + (long long)np * T * m * 4 + ((long long)(gp * T + tz) * m + i) * 4;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            double t = zs[0][lane][q];
+            for (int w = 1; w < 8; ++w) t += zs[w][lane][q];
+            pz[q] = t;
+        }
     }
 }
 
-// Neumann wall lines from the interior (src/solvediag.f90:253-276).
-// blockIdx.y < nyb: y-walls U(1,j), U(m,j), one warp per interior column j
-// (the column is contiguous: coalesced dot products with DC rows 1 and m);
-// blockIdx.y >= nyb: z-walls U(i,1), U(i,m) of 32 interior rows i per CTA,
-// the 8 thread rows splitting the sum over j (512-byte coalesced rows).
-__global__ void __launch_bounds__(256) k_neumann_walls(const __grid_constant__ FillParams p, int nyb)
+__global__ void __launch_bounds__(256) k_neumann_finish(const __grid_constant__ FillParams p, const double *part)
 {
-    __shared__ double part[8][32][4];
+    __shared__ double red[8 * 8];
     const int fi = fill_field(p);
-    const int plane = blockIdx.x - p.cta_start[fi];
-    const int m = p.m;
+    const int plane = blockIdx.x - p.cta_start[fi], gp = blockIdx.x;
+    const int m = p.m, n = m - 2, np = gridDim.x, T = (n + 31) / 32;
     double2 *U = reinterpret_cast<double2 *>(p.sol[fi] + (long long)plane * p.plane_stride);
+    auto u = [&](int i, int j) -> double2 & { return U[i + (long long)m * j]; };
     const double *DC = p.DC;
     const double d11 = DC[0], d1m = DC[(long long)m * (m - 1)];
     const double dm1 = DC[m - 1], dmm = DC[(m - 1) + (long long)m * (m - 1)];
     const double idet = 1.0 / (d11 * dmm - d1m * dm1);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if ((int)blockIdx.y < nyb) {
-        const int j = 1 + blockIdx.y * 8 + warp;
-        if (j >= m - 1) return;
-        double sl[4] = {0, 0, 0, 0};
-#pragma unroll 4
-        for (int i = 1 + lane; i < m - 1; i += 32) {
-            const double2 v = U[i + (long long)m * j];
-            const double a = p.dcr[i], b = p.dcr[m + i];
-            sl[0] += a * v.x; sl[1] += a * v.y; sl[2] += b * v.x; sl[3] += b * v.y;
-        }
+    for (int k = 1 + threadIdx.x; k <= n; k += blockDim.x) {
+        double sy[4] = {0.0, 0.0, 0.0, 0.0}, sz[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int t = 0; t < T; ++t) {
+            const double *py = part + ((long long)(gp * T + t) * m + k) * 4;
+            const double *pz = part + (long long)np * T * m * 4 + ((long long)(gp * T + t) * m + k) * 4;
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-            for (int o = 16; o > 0; o >>= 1) sl[q] += __shfl_xor_sync(0xffffffffu, sl[q], o);
-        if (lane == 0) {
-            U[(long long)m * j] = make_double2((-dmm * sl[0] + d1m * sl[2]) * idet, (-dmm * sl[1] + d1m * sl[3]) * idet);
-            U[(m - 1) + (long long)m * j] = make_double2((dm1 * sl[0] - d11 * sl[2]) * idet, (dm1 * sl[1] - d11 * sl[3]) * idet);
-        }
-    } else {
-        const int i = 1 + (blockIdx.y - nyb) * 32 + lane;
-        double sb0 = 0, sb1 = 0, st0 = 0, st1 = 0;
-        if (i < m - 1)
-#pragma unroll 8
-            for (int j = 1 + warp; j < m - 1; j += 8) {
-                const double2 v = U[i + (long long)m * j];
-                const double a = p.dcr[j], b = p.dcr[m + j];
-                sb0 += a * v.x; sb1 += a * v.y; st0 += b * v.x; st1 += b * v.y;
+            for (int q = 0; q < 4; ++q) {
+                sy[q] += py[q];
+                sz[q] += pz[q];
             }
-        part[warp][lane][0] = sb0; part[warp][lane][1] = sb1;
-        part[warp][lane][2] = st0; part[warp][lane][3] = st1;
-        __syncthreads();
-        if (warp == 0 && i < m - 1) {
-            for (int w = 1; w < 8; ++w) {
-                sb0 += part[w][lane][0]; sb1 += part[w][lane][1];
-                st0 += part[w][lane][2]; st1 += part[w][lane][3];
-            }
-            U[i] = make_double2((-dmm * sb0 + d1m * st0) * idet, (-dmm * sb1 + d1m * st1) * idet);
-            U[i + (long long)m * (m - 1)] = make_double2((dm1 * sb0 - d11 * st0) * idet, (dm1 * sb1 - d11 * st1) * idet);
         }
+        // y walls of column k, z walls of row k
+        u(0, k) = make_double2((-dmm * sy[0] + d1m * sy[2]) * idet, (-dmm * sy[1] + d1m * sy[3]) * idet);
+        u(m - 1, k) = make_double2((dm1 * sy[0] - d11 * sy[2]) * idet, (dm1 * sy[1] - d11 * sy[3]) * idet);
+        u(k, 0) = make_double2((-dmm * sz[0] + d1m * sz[2]) * idet, (-dmm * sz[1] + d1m * sz[3]) * idet);
+        u(k, m - 1) = make_double2((dm1 * sz[0] - d11 * sz[2]) * idet, (dm1 * sz[1] - d11 * sz[3]) * idet);
     }
-}
-
-// Corners from the wall lines through AM1 (src/solvediag.f90:278-322) and,
-// for the zero-mean gauge, the constant shift of the singular plane.
-__global__ void __launch_bounds__(256) k_neumann_corners(const __grid_constant__ FillParams p)
-{
-    __shared__ double red[8 * 8];
-    const int fi = fill_field(p);
-    const int plane = blockIdx.x - p.cta_start[fi];
-    const int m = p.m;
-    double2 *U = reinterpret_cast<double2 *>(p.sol[fi] + (long long)plane * p.plane_stride);
-    auto u = [&](int i, int j) -> double2 & { return U[i + (long long)m * j]; };
+    __syncthreads();   // the wall lines of this plane, written above, feed the corners
     double f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int i = 1 + threadIdx.x; i < m - 1; i += blockDim.x) {
         const double a = p.dcr[i], b = p.dcr[m + i];
@@ -1244,43 +1260,36 @@ int neumann_fill(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
     fp.gauge = ctx->gauge;
     fp.plane_stride = 2LL * ctx->my * ctx->my;
     // the pin only acts on singular planes (|lambda| <= 1e-10, the kx=0
-    // pressure mode): listed on the host, launched only when there are any,
-    // kMaxSing planes per launch pair
-    auto pin = [&]() -> int {
-        if (!fp.nsing) return DUCTGPU_OK;
-        {
-            LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
-            k_pin_coef<<<1, kMaxSing, 0, ctx->stream>>>(fp);
-        }
-        {
-            LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
-            k_pin_apply<<<dim3(32, fp.nsing), 256, 0, ctx->stream>>>(fp);
-        }
-        fp.nsing = 0;
-        return check_cuda(ctx, cudaGetLastError(), "k_pin");
-    };
+    // pressure mode), listed on the host; the coefficient kernel is launched
+    // only when there are any
     for (int i = 0, f = 0; i < ntasks && fp.io >= 0; ++i) {
         if (tasks[i].bound != 'n') continue;
         for (int k = 0; k < tasks[i].nmodes; ++k)
             if (fabs(ctx->lam_host[tasks[i].plane0 + k]) <= 1.0e-10) {
+                if (fp.nsing == kMaxSing)
+                    return set_error(ctx, DUCTGPU_EARG, "more than %d singular (lambda = 0) Neumann planes in one call", kMaxSing);
                 fp.sing_fi[fp.nsing] = f;
                 fp.sing_plane[fp.nsing] = k;
-                if (++fp.nsing == kMaxSing) {
-                    int rc = pin();
-                    if (rc) return rc;
-                }
+                ++fp.nsing;
             }
         ++f;
     }
-    if (int rc = pin()) return rc;
-    {
-        const int n = ctx->my - 2, nyb = (n + 7) / 8, nzb = (n + 31) / 32;
+    if (fp.nsing) {
         LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
-        k_neumann_walls<<<dim3(cta, nyb + nzb), 256, 0, ctx->stream>>>(fp, nyb);
+        k_pin_coef<<<1, kMaxSing, 0, ctx->stream>>>(fp);
+    }
+    // partial sums in the pass workspace (free once the passes are done:
+    // (T = ceil(n/32)) x m x 4 doubles per plane and direction)
+    const int n = ctx->my - 2, T = (n + 31) / 32;
+    if (ctx->work.bytes < (size_t)2 * cta * T * ctx->my * 4 * sizeof(double))
+        return set_error(ctx, DUCTGPU_EARG, "Neumann fill: workspace smaller than its partial sums");
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
+        k_neumann_partials<<<dim3(cta, T * T), 256, 0, ctx->stream>>>(fp, ctx->work.buf);
     }
     {
         LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);
-        k_neumann_corners<<<cta, 256, 0, ctx->stream>>>(fp);
+        k_neumann_finish<<<cta, 256, 0, ctx->stream>>>(fp, ctx->work.buf);
     }
     return check_cuda(ctx, cudaGetLastError(), "k_neumann");
 }
