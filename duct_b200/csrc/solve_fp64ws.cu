@@ -141,11 +141,50 @@ k_pass_fp64w(const __grid_constant__ PassParams p, const __grid_constant__ WsSpl
         *abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
-    // operator and eigenvalues of the field, by every thread
+    auto tile_at = [&](int j, int &plane, int &l0) {
+        const int t = t0 + j;
+        plane = t / F.nchunks;
+        l0 = (t - plane * F.nchunks) * kWsLinesF;
+    };
+    // point pair (r, H + r) of line l per item: row r holds point / mode
+    // r (r < he), row H + r point n-1-r (P^-1 passes) or odd mode he + r
+    // (P passes), r < ho; the other rows are zero
+    auto item = [&](int idx, int &r, int &l) {
+        if (sk == 1) {   // 4 points x 2 lines per 8 threads
+            const int rest = idx >> 3;
+            r = (rest % (H / 4)) * 4 + (idx & 3);
+            l = (rest / (H / 4)) * 2 + ((idx >> 2) & 1);
+        } else {
+            r = idx / kWsLinesF;
+            l = idx % kWsLinesF;
+        }
+    };
+    auto issue = [&](int j) {
+        int plane, l0;
+        tile_at(j, plane, l0);
+        const int L = min(kWsLinesF, F.nlines - l0);
+        const double *src = F.src + (long long)plane * F.plane_stride;
+        double *S = St + (j % kWsStages) * STAGE;
+        for (int idx = tid; idx < H * kWsLinesF; idx += kWsProd) {
+            int r, l;
+            item(idx, r, l);
+            const bool lok = l < L;
+            const int kb = (F.par == 1) ? n - 1 - r : he + r;
+            const bool oka = lok && r < he, okb = lok && r < ho;
+            const long long col = (long long)(l0 + l + o1) * sl;
+            cp16z(S + r * kWsNld + 2 * l, oka ? src + 2 * ((long long)(r + o1) * sk + col) : src, oka);
+            cp16z(S + (H + r) * kWsNld + 2 * l, okb ? src + 2 * ((long long)(kb + o1) * sk + col) : src, okb);
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    // operator and eigenvalues of the field, by every thread; the producers
+    // queue the first tile with them (its stage is fresh), so the two loads
+    // overlap
     for (int i = tid * 2; i < AOP; i += kWsThreads * 2) {
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(As + i)), "l"(F.A + i));
     }
     asm volatile("cp.async.commit_group;\n" ::);
+    if (warp < 4 && ntile > 0) issue(0);
     if (p.divide) {
         for (int i = tid; i < n; i += kWsThreads) Es[i] = F.E[i];
         for (int i = tid; i < F.nlines; i += kWsThreads) Els[i] = F.El[i];
@@ -158,47 +197,10 @@ k_pass_fp64w(const __grid_constant__ PassParams p, const __grid_constant__ WsSpl
         *abort = 1;
         atomicExch(err, 2);
     };
-    auto tile_at = [&](int j, int &plane, int &l0) {
-        const int t = t0 + j;
-        plane = t / F.nchunks;
-        l0 = (t - plane * F.nchunks) * kWsLinesF;
-    };
 
     if (warp < 4) {
         // ---- producers -------------------------------------------------
-        // point pair (r, H + r) of line l per item: row r holds point / mode
-        // r (r < he), row H + r point n-1-r (P^-1 passes) or odd mode he + r
-        // (P passes), r < ho; the other rows are zero
-        auto item = [&](int idx, int &r, int &l) {
-            if (sk == 1) {   // 4 points x 2 lines per 8 threads
-                const int rest = idx >> 3;
-                r = (rest % (H / 4)) * 4 + (idx & 3);
-                l = (rest / (H / 4)) * 2 + ((idx >> 2) & 1);
-            } else {
-                r = idx / kWsLinesF;
-                l = idx % kWsLinesF;
-            }
-        };
-        auto issue = [&](int j) {
-            int plane, l0;
-            tile_at(j, plane, l0);
-            const int L = min(kWsLinesF, F.nlines - l0);
-            const double *src = F.src + (long long)plane * F.plane_stride;
-            double *S = St + (j % kWsStages) * STAGE;
-            for (int idx = tid; idx < H * kWsLinesF; idx += kWsProd) {
-                int r, l;
-                item(idx, r, l);
-                const bool lok = l < L;
-                const int kb = (F.par == 1) ? n - 1 - r : he + r;
-                const bool oka = lok && r < he, okb = lok && r < ho;
-                const long long col = (long long)(l0 + l + o1) * sl;
-                cp16z(S + r * kWsNld + 2 * l, oka ? src + 2 * ((long long)(r + o1) * sk + col) : src, oka);
-                cp16z(S + (H + r) * kWsNld + 2 * l, okb ? src + 2 * ((long long)(kb + o1) * sk + col) : src, okb);
-            }
-            asm volatile("cp.async.commit_group;\n" ::);
-        };
-        bool ok = bar_wait(empty + 0, 1u, abort);   // fresh barrier: passes
-        if (ok) issue(0);
+        bool ok = true;   // tile 0 was queued with the operator
         for (int j = 0; j < ntile && ok; ++j) {
             if (j + 1 < ntile) {
                 const int s1 = (j + 1) % kWsStages, u1 = (j + 1) / kWsStages;
