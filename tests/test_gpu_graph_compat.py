@@ -39,6 +39,47 @@ def test_graph_replay_square_substep(gpu_ctx):
         f["sol"].free()
 
 
+def test_graph_replay_cfg1_batch_matches_direct(gpu_ctx):
+    """The benchmark's step: u, v, w, p at my = 129 with 64 modes (the
+    warp-specialised flip-symmetric passes), two graphs over two buffer sets
+    replayed alternately, equal bit for bit to direct calls."""
+    m, nm = 129, 64
+    gpu_ctx.pseudomat(m)
+    xalp = 0.5 * np.arange(nm)
+    specs = (("d", 4.0e6), ("d", 4.0e6), ("d", 4.0e6), ("n", 0.0))
+    sets, keep = [], []
+    try:
+        for s in range(2):
+            fl = []
+            for i, (bound, lam) in enumerate(specs):
+                rhs = synth.chebyshev_rhs(m, m, nm, seed=100 * s + i, ib=0)
+                r, o = gpu_ctx.device_array(rhs.shape), gpu_ctx.device_array(rhs.shape)
+                r.upload(rhs)
+                keep += [r, o]
+                fl.append(dict(rhs=r, sol=o, xalp=xalp, alambda=lam, ib=0, bound=bound))
+            sets.append(fl)
+        direct = []
+        for fl in sets:
+            gpu_ctx.solve_fields_dev(fl)
+            gpu_ctx.synchronize()
+            direct.append([f["sol"].download() for f in fl])
+        gids = [gpu_ctx.graph_create(fl) for fl in sets]
+        for fl in sets:
+            for f in fl:
+                f["sol"].upload(np.zeros((m, m, nm), dtype=np.complex128, order="F"))
+        for k in range(4):
+            gpu_ctx.graph_launch(gids[k % 2])
+        gpu_ctx.synchronize()
+        for fl, d in zip(sets, direct):
+            for f, ref in zip(fl, d):
+                assert np.array_equal(f["sol"].download(), ref)
+        for g in gids:
+            gpu_ctx.graph_destroy(g)
+    finally:
+        for x in keep:
+            x.free()
+
+
 def test_graph_replay_rect(gpu_ctx):
     gpu_ctx.pseudomat_temp(0, 33, 65, 1.0, 2.0)
     gpu_ctx.pseudomat_temp(1, 49, 97, 1.0, 2.0, ("n", "n"), ("n", "n"))
