@@ -375,6 +375,7 @@ def run_ours(args, world, rank, local, pg):
         e2e = measure_e2e(ctx, c, m, nm, xalp, rhs, prec, args, pg, world)
 
     hbm = transform_rates(ctx) if (rank == 0 and not args.no_transforms) else None
+    cfg2 = uneven_rect_rate(ctx, args) if not args.no_transforms else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -409,6 +410,7 @@ def run_ours(args, world, rank, local, pg):
             "mixed_rel_err_vs_fp64": acc,
             "int8_rel_err_vs_fp64": acc8,
             "hbm_kernels": hbm,
+            "cfg2_uneven_rect_batch": cfg2,
         }
         print(json.dumps(line), flush=True)
 
@@ -426,6 +428,51 @@ def fp64_peak():
         d = json.load(open(p))
         return d["fp64_tflops"], "measured cuBLAS DGEMM on this pool (profiles/measured_fp64_peak.json)"
     return None, "no measured FP64 peak available"
+
+
+def uneven_rect_rate(ctx, args):
+    """The uneven batch of rectangular ducts (aspect 1-4 at (65,65), (65,129),
+    (49,145), (33,129) with 32, 48, 64, 96 modes; u, v, w Dirichlet with
+    lambda = kx^2 + 2/(nu dt), nu = 1/4400, dt = 5e-4, and the Neumann
+    pressure with lambda = kx^2, kx = k): 16 fields in one batched call, one
+    launch per GEMM pass, replayed from a CUDA graph; FP64 passes on the full
+    operators.  Inputs (180 MB) exceed L2."""
+    import duct_b200 as D
+    from duct_b200 import synth
+    ducts = (((65, 65), 1.0, 32), ((65, 129), 2.0, 48), ((49, 145), 3.0, 64), ((33, 129), 4.0, 96))
+    h = 2.0 / ((1.0 / 4400.0) * 5.0e-4)
+    fields, keep = [], []
+    for slot, ((my, mz), aspect, nm) in enumerate(ducts):
+        ctx.pseudomat_temp(slot, my, mz, 1.0, aspect)
+        ctx.pseudomat_temp(4 + slot, my, mz, 1.0, aspect, ("n", "n"), ("n", "n"))
+        xalp = 1.0 * np.arange(nm)
+        for fld in range(4):
+            neu = fld == 3
+            f = synth.chebyshev_rhs(my, mz, nm, seed=10 * slot + fld, ib=0)
+            r, o = ctx.device_array(f.shape), ctx.device_array(f.shape)
+            r.upload(f)
+            keep += [r, o]
+            fields.append(dict(rhs=r, sol=o, xalp=xalp, alambda=0.0 if neu else h, ib=0,
+                               slot=(4 + slot) if neu else slot))
+    gid = ctx.graph_create(fields, rect=True)
+    for _ in range(max(3, args.warmup)):
+        ctx.graph_launch(gid)
+    ctx.synchronize()
+    steps = max(10, args.steps)
+    ctx.event_record(0)
+    for _ in range(steps):
+        ctx.graph_launch(gid)
+    ctx.event_record(1)
+    ms = ctx.event_elapsed(0, 1) / steps
+    ctx.synchronize()
+    ctx.graph_destroy(gid)
+    for x in keep:
+        x.free()
+    per_step = 4 * sum(nm for _, _, nm in ducts)
+    return {"value": per_step / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "mode_solves_per_step": per_step,
+            "fields": len(fields), "steps": steps,
+            "config": "4 rectangular ducts (65x65, 65x129, 49x145, 33x129; 32/48/64/96 modes) x (u, v, w, p)",
+            "step": "CUDA-graph replay of ductgpu_solve_rect_fields_dev (16 fields, one launch per pass)"}
 
 
 def torch_sm_count():

@@ -15,7 +15,7 @@
 
 namespace duct {
 
-constexpr int kMaxFields = 8;   // fields per batched launch
+constexpr int kMaxFields = 16;  // fields per batched launch (4 ducts x u, v, w, p)
 constexpr int kMaxN = 191;      // largest interior size (my-2) supported
 constexpr int kNumEvents = 16;
 constexpr int kMaxRect = 8;     // rectangular operator slots (duct shapes)

@@ -127,8 +127,8 @@ typedef struct {
 
 /* All fields (each a helm3d call of the reference, e.g. u, v, w and the
  * pressure of one RK substep, src/main1.f90:617-619,643) in one batched
- * launch sequence on the context's stream.  Asynchronous: returns once the
- * work is queued.                                                          */
+ * launch sequence on the context's stream, 1..16 fields.  Asynchronous:
+ * returns once the work is queued.                                         */
 int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields,
                              int nfields, int precision);
 

@@ -66,8 +66,9 @@ def test_all_neumann_singular_gauge(gpu_ctx, oracle):
 
 
 def test_uneven_batch_one_launch_per_pass(gpu_ctx, oracle):
-    """The four ducts x (3 Dirichlet velocities + Neumann pressure) in one
-    batched call equal the per-duct oracle solutions."""
+    """The four ducts x (3 Dirichlet velocities + Neumann pressure) -- 16
+    fields -- in one batched call (one launch per GEMM pass) equal the
+    per-duct oracle solutions."""
     nu, dt = 1.0 / 4400.0, 5.0e-4
     h = 2.0 / (nu * dt)
     fields, refs = [], []
@@ -77,8 +78,8 @@ def test_uneven_batch_one_launch_per_pass(gpu_ctx, oracle):
         xalp = 1.0 * np.arange(nm)
         yd, zd = oracle.Dir(my, 1.0), oracle.Dir(mz, aspect)
         yn, zn = oracle.Dir(my, 1.0, "n", "n"), oracle.Dir(mz, aspect, "n", "n")
-        for fld in range(2):
-            neu = fld == 1
+        for fld in range(4):
+            neu = fld == 3
             f = synth.chebyshev_rhs(my, mz, nm, seed=10 * slot + fld, ib=0)
             lam = 0.0 if neu else h
             ref = oracle.helm3d_temp(f, yn if neu else yd, zn if neu else zd, lam, xalp)
