@@ -424,6 +424,7 @@ struct DerivParams {
     int lines_per_mode, nlines, nn;
     int ider;
     int accumulate;
+    int lpb;              // lines per CTA
     double fac;           // scal (y) or scal/aspect^ider (z)
 };
 
@@ -447,9 +448,11 @@ __device__ void deriv_rec(const double2 *c, long long cs, double2 *o, long long 
     else o[0] = val;
 }
 
-constexpr int kDerivLines = 32;
+// lines per CTA of k_deriv: y lines (contiguous) / z lines (a point of
+// consecutive lines contiguous); 16 keeps 4 CTAs on an SM at my = 193
+constexpr int kDerivLinesY = 16, kDerivLinesZ = 16;
 
-// A tile of kDerivLines lines of one mode staged with cp.async (padded odd
+// A tile of p.lpb lines of one mode staged with cp.async (padded odd
 // row length, conflict-free for both the y and the z access pattern), the
 // recurrence run in place by one thread per line (it reads c_k before it
 // writes out_k and then only lower indices), coalesced stores.
@@ -457,10 +460,10 @@ __global__ void __launch_bounds__(256) k_deriv(const __grid_constant__ DerivPara
 {
     extern __shared__ __align__(16) double2 sm[];
     const int nn = p.nn, ld = nn | 1;
-    const int cpm = (p.lines_per_mode + kDerivLines - 1) / kDerivLines;
+    const int cpm = (p.lines_per_mode + p.lpb - 1) / p.lpb;
     const int mode = blockIdx.x / cpm;
-    const int q0 = (blockIdx.x - mode * cpm) * kDerivLines;
-    const int nl = min(kDerivLines, p.lines_per_mode - q0);
+    const int q0 = (blockIdx.x - mode * cpm) * p.lpb;
+    const int nl = min(p.lpb, p.lines_per_mode - q0);
     const long long base = mode * p.mode_stride + (long long)q0 * p.line_stride;
     const double2 *U = reinterpret_cast<const double2 *>(p.u) + base;
     double2 *DU = reinterpret_cast<double2 *>(p.du) + base;
@@ -575,9 +578,10 @@ int derivyz_dev(ductgpu_ctx ctx, const double *u, double *du, int my, int mz, in
     p.accumulate = (what != 'n');
     p.fac = scal;
     if (cdir == 'z') p.fac = (ider == 1) ? scal / aspect : scal / (aspect * aspect);
-    const size_t smem = (size_t)kDerivLines * (p.nn | 1) * sizeof(double2);
+    p.lpb = (cdir == 'y') ? kDerivLinesY : kDerivLinesZ;
+    const size_t smem = (size_t)p.lpb * (p.nn | 1) * sizeof(double2);
     DUCT_CUDA(ctx, cudaFuncSetAttribute(k_deriv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int grid = nmodes * ((p.lines_per_mode + kDerivLines - 1) / kDerivLines);
+    const int grid = nmodes * ((p.lines_per_mode + p.lpb - 1) / p.lpb);
     {
         LaunchScope ls(ctx, DUCTGPU_K_TRANSFORM);
         k_deriv<<<grid, 256, smem, ctx->stream>>>(p);
