@@ -395,6 +395,212 @@ static int launch_dct2(ductgpu_ctx ctx, DctParams &p, int nmodes)
     return check_cuda(ctx, cudaGetLastError(), "k_dct2");
 }
 
+// Half-length DCT-I (N = R1 R2 even, N + 1 points a line).  With F the
+// DCT-I of a line, F_k = (x_0 + (-1)^k x_N) / 2 + sum_{j=1}^{N-1} x_j cos(pi j k / N)
+// (the 2N even-extension FFT of k_dct2 gives 2 F_k), the sequence
+//   g_0 = (x_0 + x_N) / 2,  g_{N/2} = x_{N/2},
+//   g_j = (x_j + x_{N-j}) / 2 - sin(pi j / N) (x_j - x_{N-j})   (0 < j < N, j != N/2)
+// has the length-N DFT G_k with (by the symmetric / antisymmetric split of
+// each term under j -> N - j, and 2 sin a sin b = cos(a - b) - cos(a + b))
+//   F_{2k} = (G_k + G_{N-k}) / 2,   F_{2k+1} = F_{2k-1} + i (G_k - G_{N-k}) / 2,
+//   F_1 = (x_0 - x_N) / 2 + sum_{j=1}^{N/2-1} cos(pi j / N) (x_j - x_{N-j}).
+// g is real-linear in x, so the complex line (re + i im) goes through one
+// complex FFT of length N and these formulas directly -- the half-length
+// real-data DCT of Press et al. (Numerical Recipes, sec. 12.3), here for a
+// pair of real lines at once.  Half the FFT of the even extension and half
+// its shared memory: 16 lines a CTA at N = 192 (4 CTAs per SM).
+// Shared line layout: point j at j + j / R2 (as k_dct2), x_N at R1 (R2 + 1).
+// Results: F_{2k} in slot k, F_{2k+1} in slot N - k (slot N for F_1).
+template <int R1, int R2>
+__global__ void __launch_bounds__(256) k_dcth(const __grid_constant__ DctParams p, const double2 *__restrict__ twg,
+                                             const double2 *__restrict__ tw2)
+{
+    extern __shared__ __align__(16) double2 buf[];
+    constexpr int N = R1 * R2, LS = R1 * (R2 + 1) + 1;
+    constexpr int LPB = 256 / (R1 > R2 ? R1 : R2);
+    double2 *tw = buf;                          // W_N^t, N entries
+    double2 *ha = tw + N;                       // W_2N^j, j <= N/2: (cos, -sin)(pi j / N)
+    double2 *x = ha + (N / 2 + 1);              // [LPB][LS]
+    double2 *f1 = x + LPB * LS;                 // [LPB] F_1 of each line
+    auto at = [](int j) { return j + j / R2; };
+    const int cpm = (p.lines_per_mode + LPB - 1) / LPB;
+    const int mode = blockIdx.x / cpm;
+    const int q0 = (blockIdx.x - mode * cpm) * LPB;
+    const int nl = min(LPB, p.lines_per_mode - q0);
+    double2 *g = reinterpret_cast<double2 *>(p.f) + mode * p.mode_stride + (long long)q0 * p.line_stride;
+    const bool contiguous = (p.elem_stride == 1);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (contiguous) {
+        for (int l = warp; l < nl; l += 8)
+            for (int j = lane; j <= N; j += 32) cp_async16(x + l * LS + at(j), g + l * p.line_stride + j);
+    } else {
+        for (int idx = threadIdx.x; idx < LPB * (N + 1); idx += 256) {
+            const int j = idx / LPB, l = idx - j * LPB;
+            if (l < nl) cp_async16(x + l * LS + at(j), g + l + (long long)j * p.elem_stride);
+        }
+    }
+    for (int t = threadIdx.x; t < N; t += 256) cp_async16(tw + t, twg + t);
+    for (int t = threadIdx.x; t <= N / 2; t += 256) cp_async16(ha + t, tw2 + t);
+    cp_async_wait_all();
+    __syncthreads();
+    // g in place (a warp per line); the inverse halves the interior points first
+    const double si = (p.iopt >= 0) ? 0.5 : 1.0;
+    for (int l = warp; l < LPB; l += 8) {
+        double2 *xl = x + l * LS;
+        if (l >= nl) {
+            for (int j = lane; j < LS; j += 32) xl[j] = make_double2(0.0, 0.0);
+            continue;
+        }
+        double sx = 0.0, sy = 0.0;
+        for (int j = 1 + lane; j < N / 2; j += 32) {
+            const double2 a = xl[at(j)], b = xl[at(N - j)];
+            const double2 u = make_double2(0.5 * si * (a.x + b.x), 0.5 * si * (a.y + b.y));
+            const double2 v = make_double2(si * (a.x - b.x), si * (a.y - b.y));
+            const double2 w = ha[j];   // (cos(pi j/N), -sin(pi j/N))
+            xl[at(j)] = make_double2(u.x + w.y * v.x, u.y + w.y * v.y);
+            xl[at(N - j)] = make_double2(u.x - w.y * v.x, u.y - w.y * v.y);
+            sx += w.x * v.x;
+            sy += w.x * v.y;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            sx += __shfl_xor_sync(0xffffffffu, sx, o);
+            sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        }
+        if (lane == 0) {
+            const double2 x0 = xl[at(0)], xn = xl[at(N)], xm = xl[at(N / 2)];
+            f1[l] = make_double2(0.5 * (x0.x - xn.x) + sx, 0.5 * (x0.y - xn.y) + sy);
+            xl[at(0)] = make_double2(0.5 * (x0.x + xn.x), 0.5 * (x0.y + xn.y));
+            xl[at(N / 2)] = make_double2(si * xm.x, si * xm.y);
+        }
+    }
+    __syncthreads();
+    // FFT of length N in place: R1-point DFTs along n1 (column n2) with the
+    // twiddle W_N^(n2 k1), then R2-point DFTs along each row k1
+    {
+        const int l = threadIdx.x / R2, n2 = threadIdx.x - l * R2;
+        if (l < LPB) {
+            double2 *xl = x + l * LS;
+            double2 v[R1];
+#pragma unroll
+            for (int n1 = 0; n1 < R1; ++n1) v[n1] = xl[n1 * (R2 + 1) + n2];
+            reg_fft<R1, 0, 1>(v, tw, N);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; ++k1) xl[k1 * (R2 + 1) + n2] = (k1 == 0) ? v[0] : cmul(v[k1], tw[n2 * k1]);
+        }
+    }
+    __syncthreads();
+    {
+        const int l = threadIdx.x / R1, k1 = threadIdx.x - l * R1;
+        const bool act = l < LPB;
+        double2 w[R2];
+        if (act) {
+            const double2 *xr = x + l * LS + k1 * (R2 + 1);
+#pragma unroll
+            for (int n2 = 0; n2 < R2; ++n2) w[n2] = xr[n2];
+            reg_fft<R2, 0, 1>(w, tw, N);
+        }
+        __syncthreads();
+        if (act) {
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) x[l * LS + at(k1 + R1 * k2)] = w[k2];
+        }
+    }
+    __syncthreads();
+    // From G to F, a warp per line: lane q owns the pairs (k, N - k) of a run
+    // of consecutive k <= N/2; F_{2k} = (G_k + G_{N-k}) / 2 goes to slot k and
+    // F_{2k+1} = F_1 + sum_{i=1}^{k} i (G_i - G_{N-i}) / 2 to slot N - k
+    // (the increments scanned across the warp with shuffles), F_1 to slot N.
+    for (int l = warp; l < nl; l += 8) {
+        double2 *xl = x + l * LS;
+        constexpr int CH = (N / 2 + 1 + 31) / 32;
+        const int k0 = lane * CH, k1 = min(N / 2 + 1, k0 + CH);
+        double sx = 0.0, sy = 0.0;
+        for (int k = k0; k < k1; ++k) {
+            if (k == 0 || k == N / 2) continue;
+            const double2 gk = xl[at(k)], gm = xl[at(N - k)];
+            sx -= 0.5 * (gk.y - gm.y);
+            sy += 0.5 * (gk.x - gm.x);
+        }
+        double ix = sx, iy = sy;   // inclusive prefix over lanes 0..lane
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double tx = __shfl_up_sync(0xffffffffu, ix, o), ty = __shfl_up_sync(0xffffffffu, iy, o);
+            if (lane >= o) {
+                ix += tx;
+                iy += ty;
+            }
+        }
+        const double2 b1 = f1[l];
+        double rx = b1.x + ix - sx, ry = b1.y + iy - sy;
+        for (int k = k0; k < k1; ++k) {
+            const double2 gk = xl[at(k)], gm = xl[at(k == 0 ? 0 : N - k)];
+            xl[at(k)] = make_double2(0.5 * (gk.x + gm.x), 0.5 * (gk.y + gm.y));
+            if (k > 0 && k < N / 2) {
+                rx -= 0.5 * (gk.y - gm.y);
+                ry += 0.5 * (gk.x - gm.x);
+                xl[at(N - k)] = make_double2(rx, ry);
+            }
+        }
+        if (lane == 0) xl[at(N)] = b1;
+    }
+    __syncthreads();
+    // out_j = 2 F_j, scaled by 1/(2N) at the ends and 1/N inside (forward)
+    const bool fwd = p.iopt < 0;
+    auto value = [&](int l, int j) {
+        const int slot = (j & 1) ? N - (j >> 1) : (j >> 1);
+        const double2 v = x[l * LS + at(slot)];
+        const double sc = fwd ? ((j == 0 || j == N) ? 1.0 / N : 2.0 / N) : 2.0;
+        return make_double2(sc * v.x, sc * v.y);
+    };
+    if (contiguous) {
+        for (int l = warp; l < nl; l += 8)
+            for (int j = lane; j <= N; j += 32) g[l * p.line_stride + j] = value(l, j);
+    } else {
+        for (int idx = threadIdx.x; idx < LPB * (N + 1); idx += 256) {
+            const int j = idx / LPB, l = idx - j * LPB;
+            if (l < nl) g[l + (long long)j * p.elem_stride] = value(l, j);
+        }
+    }
+}
+
+template <int R1, int R2>
+static int launch_dcth(ductgpu_ctx ctx, DctParams &p, int nmodes)
+{
+    constexpr int N = R1 * R2, LS = R1 * (R2 + 1) + 1;
+    constexpr int LPB = 256 / (R1 > R2 ? R1 : R2);
+    const double2 *tw = twiddle_table(ctx, N);
+    const double2 *tw2 = twiddle_table(ctx, 2 * N);
+    if (!tw || !tw2) return -1;
+    p.lpb = LPB;
+    const size_t smem = ((size_t)N + (N / 2 + 1) + (size_t)LPB * LS + LPB) * sizeof(double2);
+    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_dcth<R1, R2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int grid = nmodes * ((p.lines_per_mode + LPB - 1) / LPB);
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_TRANSFORM);
+        k_dcth<R1, R2><<<grid, 256, smem, ctx->stream>>>(p, tw, tw2);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "k_dcth");
+}
+
+// Half-length plans (R1 x R2 = N = nn - 1); -1 if none.
+static int dcth_dispatch(ductgpu_ctx ctx, DctParams &p, int nmodes)
+{
+    switch (p.nn - 1) {
+    case 16: return launch_dcth<4, 4>(ctx, p, nmodes);
+    case 24: return launch_dcth<4, 6>(ctx, p, nmodes);
+    case 32: return launch_dcth<4, 8>(ctx, p, nmodes);
+    case 48: return launch_dcth<6, 8>(ctx, p, nmodes);
+    case 64: return launch_dcth<8, 8>(ctx, p, nmodes);
+    case 96: return launch_dcth<8, 12>(ctx, p, nmodes);
+    case 128: return launch_dcth<8, 16>(ctx, p, nmodes);
+    case 144: return launch_dcth<12, 12>(ctx, p, nmodes);
+    case 192: return launch_dcth<12, 16>(ctx, p, nmodes);
+    case 256: return launch_dcth<16, 16>(ctx, p, nmodes);
+    default: return -1;
+    }
+}
+
 // Register-FFT plans (R1 x R2 = L) for the line lengths in use; -1 if none.
 static int dct2_dispatch(ductgpu_ctx ctx, DctParams &p, int nmodes)
 {
@@ -544,7 +750,12 @@ int transyz_dev(ductgpu_ctx ctx, double *f, int my, int mz, int nmodes, char cdi
     if (p.nstages < 0)
         return set_error(ctx, DUCTGPU_EARG, "transyz: line length %d - 1 must be of the form 2^a 3^b", p.nn);
     p.iopt = iopt;
-    // the two-pass register FFT where a plan exists, else the radix stages
+    // the half-length DCT where a plan exists, then the two-pass register
+    // FFT of the even extension, else the radix stages
+    {
+        const int rc = dcth_dispatch(ctx, p, nmodes);
+        if (rc >= 0) return rc;
+    }
     {
         const int rc = dct2_dispatch(ctx, p, nmodes);
         if (rc >= 0) return rc;
