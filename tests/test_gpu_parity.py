@@ -209,3 +209,75 @@ def test_warp_specialised_pass_matches_small_batches(parity, oracle):
     finally:
         for x in keep:
             x.free()
+
+
+def test_warp_specialised_pass_hpad32_matches_small_batches(parity):
+    """Half blocks of 32 rows (my = 65) in a batch large enough for the
+    warp-specialised kernel (4 fields x 128 modes: 2048 tiles) equal the
+    same fields in 16-mode batches (the 3-CTA-per-SM kernel) bit for bit."""
+    ctx = parity
+    m, nm, chunk = 65, 128, 16
+    ctx.pseudomat(m)
+    xalp = 0.25 * np.arange(nm)
+    specs = [("d", 2.0e4), ("d", 3.0), ("n", 0.0), ("n", 1.0)]
+    rhs = [synth.chebyshev_rhs(m, m, nm, seed=70 + i, ib=0) for i in range(len(specs))]
+    keep = []
+    try:
+        big = []
+        for (b, lam), f in zip(specs, rhs):
+            r, s = ctx.device_array(f.shape), ctx.device_array(f.shape)
+            r.upload(f)
+            keep += [r, s]
+            big.append(dict(rhs=r, sol=s, xalp=xalp, alambda=lam, ib=0, bound=b))
+        ctx.solve_fields_dev(big)
+        ctx.synchronize()
+        whole = [f["sol"].download() for f in big]
+        for k0 in range(0, nm, chunk):
+            small = []
+            for (b, lam), f in zip(specs, rhs):
+                part = np.asfortranarray(f[:, :, k0:k0 + chunk])
+                r, s = ctx.device_array(part.shape), ctx.device_array(part.shape)
+                r.upload(part)
+                keep += [r, s]
+                small.append(dict(rhs=r, sol=s, xalp=xalp[k0:k0 + chunk], alambda=lam, ib=k0, bound=b))
+            ctx.solve_fields_dev(small)
+            ctx.synchronize()
+            for f, w in zip(small, whole):
+                assert np.array_equal(f["sol"].download(), w[:, :, k0:k0 + chunk]), k0
+    finally:
+        for x in keep:
+            x.free()
+
+
+def test_adjoint_at_cfg1_size_is_the_transpose(parity):
+    """The adjoint of a cfg1-sized batch (warp-specialised kernel on the
+    transposed half blocks): <g, S f> = <S^T g, f> for u, v, w and p."""
+    ctx = parity
+    m, nm = 129, 64
+    ctx.pseudomat(m)
+    xalp = 0.5 * np.arange(nm)
+    specs = [("d", 4.0e6), ("d", 4.0e6), ("d", 4.0e6), ("n", 0.0)]
+    keep, fwd, adj, data = [], [], [], []
+    try:
+        for i, (b, lam) in enumerate(specs):
+            f = synth.chebyshev_rhs(m, m, nm, seed=90 + i, ib=0)
+            gg = synth.chebyshev_rhs(m, m, nm, seed=95 + i, ib=0)
+            a = [ctx.device_array(f.shape) for _ in range(4)]
+            a[0].upload(f)
+            a[2].upload(gg)
+            keep += a
+            fwd.append(dict(rhs=a[0], sol=a[1], xalp=xalp, alambda=lam, ib=0, bound=b))
+            adj.append(dict(rhs=a[2], sol=a[3], xalp=xalp, alambda=lam, ib=0, bound=b))
+            data.append((f, gg, a))
+        ctx.solve_fields_dev(fwd)
+        ctx.solve_adjoint_fields_dev(adj)
+        ctx.synchronize()
+        for (b, _), (f, gg, a) in zip(specs, data):
+            Sf, STg = a[1].download(), a[3].download()
+            lhs = np.vdot(gg.ravel(), Sf.ravel()).real
+            rhs_ = np.vdot(STg.ravel(), f.ravel()).real
+            scale = np.linalg.norm(gg) * np.linalg.norm(Sf) + np.linalg.norm(STg) * np.linalg.norm(f)
+            assert abs(lhs - rhs_) < 1e-13 * scale, (b, lhs, rhs_)
+    finally:
+        for x in keep:
+            x.free()
