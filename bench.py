@@ -353,7 +353,7 @@ def run_ours(args, world, rank, local, pg):
             ach = ops / ((kms / kn) * 1e-3) / 1e12 if kn else None
             roofs[name] = {"bound": "tensor", "achieved": ach, "peak": 4500.0, "unit": "TOPS (int8)",
                            "frac": (ach / 4500.0) if ach else None,
-                           "traffic": None,
+                           "traffic": traffic_from_profile("k_pass_i8ws"),
                            "kernel": "k_pass_i8ws (tcgen05 kind::i8, 28 slice products, exact int32)",
                            "peak_source": "nominal dense int8 (no measured int8 peak on this pool)",
                            "fp64_equiv_tflops": (4.0 * n ** 3 * per_step) / ((kms / kn) * 1e-3) / 1e12 if kn else None,

@@ -459,7 +459,8 @@ __global__ void __launch_bounds__(544, 1) k_pass_i8ws(const __grid_constant__ Pa
     uint8_t *As = smem;                                          // 7 x 16 KB
     uint8_t *Bs = smem + kI8Slices * kI8OpSlice;                 // 2 x 28 KB
     int *ecol = reinterpret_cast<int *>(Bs + 2 * kWsBStage);     // [4][32] exponent ring
-    uint64_t *bars = reinterpret_cast<uint64_t *>(ecol + 4 * kWsN);
+    double *elr = reinterpret_cast<double *>(ecol + 4 * kWsN);   // [4][16] line eigenvalues (divide)
+    uint64_t *bars = reinterpret_cast<uint64_t *>(elr + 4 * kWsLines);
     uint64_t *full = bars, *empty = bars + 2, *tfull = bars + 4, *tempty = bars + 6, *abar = bars + 8;
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 9);
     volatile int *abort = reinterpret_cast<volatile int *>(tslot + 1);
@@ -552,6 +553,10 @@ __global__ void __launch_bounds__(544, 1) k_pass_i8ws(const __grid_constant__ Pa
             if (anyfail) { fail(); break; }
             int *ec = ecol + (j & 3) * kWsN;
             if (tid < kWsN) ec[tid] = 0;
+            if (p.divide && tid < kWsLines) {   // the tile's line eigenvalues, for the epilogue
+                const PassField &G = p.f[fi];
+                elr[(j & 3) * kWsLines + tid] = (l0 + tid < G.nlines) ? G.El[l0 + tid] : 0.0;
+            }
             asm volatile("bar.sync 1, 256;\n" ::: "memory");
             atomicMax(&ec[2 * l], emax_re);
             atomicMax(&ec[2 * l + 1], emax_im);
@@ -661,9 +666,13 @@ __global__ void __launch_bounds__(544, 1) k_pass_i8ws(const __grid_constant__ Pa
             int fi, plane, l0;
             tile_geom(tile, fi, plane, l0);
             const PassField &F = p.f[fi];
+            // E of this row, read before the wait (the line eigenvalues come
+            // staged with the tile's exponents)
+            const double Eo = (p.divide && o < F.n) ? __ldg(F.E + o) : 0.0;
             if (!__all_sync(0xffffffffu, ws_wait(tfull + s, use & 1, abort))) { fail(); break; }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             const int L = min(kWsLines, F.nlines - l0);
+            const double *el = elr + (j & 3) * kWsLines;
             const int n = F.n, sk = F.sk, sl = F.sl, o1 = F.off;
             double *dst = F.dst + (long long)plane * F.plane_stride;
             const double lam = p.lam[F.plane0 + plane];
@@ -700,9 +709,9 @@ __global__ void __launch_bounds__(544, 1) k_pass_i8ws(const __grid_constant__ Pa
                         if (singular && o == F.sing_io && lg == F.sing_l) {
                             val[0] = val[1] = 0.0;
                         } else {
-                            const double den = (F.E[o] + F.El[lg]) - lam;
-                            val[0] /= den;
-                            val[1] /= den;
+                            const double rden = 1.0 / ((Eo + el[lq]) - lam);
+                            val[0] *= rden;
+                            val[1] *= rden;
                         }
                     }
                     const long long off = 2 * ((long long)(o + o1) * sk + (long long)(lg + o1) * sl);
@@ -744,7 +753,8 @@ int i8_pass(ductgpu_ctx ctx, const PassParams &pp, int grid)
             tiles += q.f[i].nmodes * q.f[i].nchunks;
         }
         q.cta_start[q.nf] = tiles;
-        const size_t smem = (size_t)kI8Slices * kI8OpSlice + 2 * (size_t)kWsBStage + 4 * kWsN * sizeof(int) + 128;
+        const size_t smem = (size_t)kI8Slices * kI8OpSlice + 2 * (size_t)kWsBStage + 4 * kWsN * sizeof(int) +
+                            4 * kWsLines * sizeof(double) + 128;
         DUCT_CUDA(ctx, cudaFuncSetAttribute(k_pass_i8ws, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const int ctas = tiles < ctx->num_sms ? tiles : ctx->num_sms;
         {
