@@ -395,6 +395,14 @@ static int launch_dct2(ductgpu_ctx ctx, DctParams &p, int nmodes)
     return check_cuda(ctx, cudaGetLastError(), "k_dct2");
 }
 
+// Threads per CTA of k_dcth: a CTA holds 64 / max(R1, R2) lines (4 at
+// N = 192) and runs its steps (staging, pre-step, two FFT steps, post-step,
+// store) between CTA barriers, so many small CTAs on an SM overlap the steps
+// of one another; measured at my = 193 (fraction of the HBM copy rate,
+// y / z): 256 threads 0.315 / 0.289, 128 threads 0.343 / 0.321, 64 threads
+// 0.351 / 0.324.
+constexpr int kDcthThreads = 64;
+
 // Half-length DCT-I (N = R1 R2 even, N + 1 points a line).  With F the
 // DCT-I of a line, F_k = (x_0 + (-1)^k x_N) / 2 + sum_{j=1}^{N-1} x_j cos(pi j k / N)
 // (the 2N even-extension FFT of k_dct2 gives 2 F_k), the sequence
@@ -408,16 +416,16 @@ static int launch_dct2(ductgpu_ctx ctx, DctParams &p, int nmodes)
 // complex FFT of length N and these formulas directly -- the half-length
 // real-data DCT of Press et al. (Numerical Recipes, sec. 12.3), here for a
 // pair of real lines at once.  Half the FFT of the even extension and half
-// its shared memory: 16 lines a CTA at N = 192 (4 CTAs per SM).
+// its shared memory.
 // Shared line layout: point j at j + j / R2 (as k_dct2), x_N at R1 (R2 + 1).
 // Results: F_{2k} in slot k, F_{2k+1} in slot N - k (slot N for F_1).
-template <int R1, int R2>
-__global__ void __launch_bounds__(256) k_dcth(const __grid_constant__ DctParams p, const double2 *__restrict__ twg,
+template <int R1, int R2, int NT>
+__global__ void __launch_bounds__(NT) k_dcth(const __grid_constant__ DctParams p, const double2 *__restrict__ twg,
                                              const double2 *__restrict__ tw2)
 {
     extern __shared__ __align__(16) double2 buf[];
     constexpr int N = R1 * R2, LS = R1 * (R2 + 1) + 1;
-    constexpr int LPB = 256 / (R1 > R2 ? R1 : R2);
+    constexpr int LPB = NT / (R1 > R2 ? R1 : R2), NW = NT / 32;
     double2 *tw = buf;                          // W_N^t, N entries
     double2 *ha = tw + N;                       // W_2N^j, j <= N/2: (cos, -sin)(pi j / N)
     double2 *x = ha + (N / 2 + 1);              // [LPB][LS]
@@ -431,21 +439,21 @@ __global__ void __launch_bounds__(256) k_dcth(const __grid_constant__ DctParams 
     const bool contiguous = (p.elem_stride == 1);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (contiguous) {
-        for (int l = warp; l < nl; l += 8)
+        for (int l = warp; l < nl; l += NW)
             for (int j = lane; j <= N; j += 32) cp_async16(x + l * LS + at(j), g + l * p.line_stride + j);
     } else {
-        for (int idx = threadIdx.x; idx < LPB * (N + 1); idx += 256) {
+        for (int idx = threadIdx.x; idx < LPB * (N + 1); idx += NT) {
             const int j = idx / LPB, l = idx - j * LPB;
             if (l < nl) cp_async16(x + l * LS + at(j), g + l + (long long)j * p.elem_stride);
         }
     }
-    for (int t = threadIdx.x; t < N; t += 256) cp_async16(tw + t, twg + t);
-    for (int t = threadIdx.x; t <= N / 2; t += 256) cp_async16(ha + t, tw2 + t);
+    for (int t = threadIdx.x; t < N; t += NT) cp_async16(tw + t, twg + t);
+    for (int t = threadIdx.x; t <= N / 2; t += NT) cp_async16(ha + t, tw2 + t);
     cp_async_wait_all();
     __syncthreads();
     // g in place (a warp per line); the inverse halves the interior points first
     const double si = (p.iopt >= 0) ? 0.5 : 1.0;
-    for (int l = warp; l < LPB; l += 8) {
+    for (int l = warp; l < LPB; l += NW) {
         double2 *xl = x + l * LS;
         if (l >= nl) {
             for (int j = lane; j < LS; j += 32) xl[j] = make_double2(0.0, 0.0);
@@ -511,7 +519,7 @@ __global__ void __launch_bounds__(256) k_dcth(const __grid_constant__ DctParams 
     // of consecutive k <= N/2; F_{2k} = (G_k + G_{N-k}) / 2 goes to slot k and
     // F_{2k+1} = F_1 + sum_{i=1}^{k} i (G_i - G_{N-i}) / 2 to slot N - k
     // (the increments scanned across the warp with shuffles), F_1 to slot N.
-    for (int l = warp; l < nl; l += 8) {
+    for (int l = warp; l < nl; l += NW) {
         double2 *xl = x + l * LS;
         constexpr int CH = (N / 2 + 1 + 31) / 32;
         const int k0 = lane * CH, k1 = min(N / 2 + 1, k0 + CH);
@@ -554,31 +562,31 @@ __global__ void __launch_bounds__(256) k_dcth(const __grid_constant__ DctParams 
         return make_double2(sc * v.x, sc * v.y);
     };
     if (contiguous) {
-        for (int l = warp; l < nl; l += 8)
+        for (int l = warp; l < nl; l += NW)
             for (int j = lane; j <= N; j += 32) g[l * p.line_stride + j] = value(l, j);
     } else {
-        for (int idx = threadIdx.x; idx < LPB * (N + 1); idx += 256) {
+        for (int idx = threadIdx.x; idx < LPB * (N + 1); idx += NT) {
             const int j = idx / LPB, l = idx - j * LPB;
             if (l < nl) g[l + (long long)j * p.elem_stride] = value(l, j);
         }
     }
 }
 
-template <int R1, int R2>
+template <int R1, int R2, int NT = kDcthThreads>
 static int launch_dcth(ductgpu_ctx ctx, DctParams &p, int nmodes)
 {
     constexpr int N = R1 * R2, LS = R1 * (R2 + 1) + 1;
-    constexpr int LPB = 256 / (R1 > R2 ? R1 : R2);
+    constexpr int LPB = NT / (R1 > R2 ? R1 : R2);
     const double2 *tw = twiddle_table(ctx, N);
     const double2 *tw2 = twiddle_table(ctx, 2 * N);
     if (!tw || !tw2) return -1;
     p.lpb = LPB;
     const size_t smem = ((size_t)N + (N / 2 + 1) + (size_t)LPB * LS + LPB) * sizeof(double2);
-    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_dcth<R1, R2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_dcth<R1, R2, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int grid = nmodes * ((p.lines_per_mode + LPB - 1) / LPB);
     {
         LaunchScope ls(ctx, DUCTGPU_K_TRANSFORM);
-        k_dcth<R1, R2><<<grid, 256, smem, ctx->stream>>>(p, tw, tw2);
+        k_dcth<R1, R2, NT><<<grid, NT, smem, ctx->stream>>>(p, tw, tw2);
     }
     return check_cuda(ctx, cudaGetLastError(), "k_dcth");
 }
