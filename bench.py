@@ -114,7 +114,11 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def dist_setup(args):
+def dist_setup(args, backend=None, timeout_s=120):
+    """One process per GPU from the launcher's environment (RANK, WORLD_SIZE,
+    LOCAL_RANK, MASTER_ADDR/PORT).  NCCL on GPUs, gloo without one (the
+    multi-rank host logic is tested that way on CPU); the timeout ends a
+    collective that a departed rank never joins with an error."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -123,8 +127,11 @@ def dist_setup(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
         pg = dist
     return world, rank, local, pg
 
@@ -135,10 +142,12 @@ def barrier(pg):
 
 
 def max_over_ranks(pg, v):
+    """The slowest rank's time: every multi-GPU number is the max over ranks."""
     if pg is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
