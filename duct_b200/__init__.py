@@ -21,7 +21,7 @@ GAUGE_POINT, GAUGE_MEAN = 0, 1
 
 EXPORTS = [
     "ductgpu_create", "ductgpu_destroy", "ductgpu_last_error", "ductgpu_set_stream",
-    "ductgpu_get_stream", "ductgpu_synchronize", "ductgpu_pseudomat",
+    "ductgpu_get_stream", "ductgpu_synchronize", "ductgpu_selftest_wait_timeout", "ductgpu_pseudomat",
     "ductgpu_get_operators", "ductgpu_set_operators", "ductgpu_set_gauge",
     "ductgpu_helm3d", "ductgpu_solve_fields_dev", "ductgpu_device_alloc",
     "ductgpu_device_free", "ductgpu_host_alloc", "ductgpu_host_free", "ductgpu_copy",
@@ -74,6 +74,7 @@ def lib():
             "ductgpu_set_stream": [P, P],
             "ductgpu_get_stream": [P],
             "ductgpu_synchronize": [P],
+            "ductgpu_selftest_wait_timeout": [P, C.c_uint],
             "ductgpu_pseudomat": [P, I, I],
             "ductgpu_get_operators": [P, C.c_char, P, P, P, C.POINTER(I)],
             "ductgpu_set_operators": [P, C.c_char, P, P, P, I],

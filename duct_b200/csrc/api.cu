@@ -267,6 +267,15 @@ int ductgpu_synchronize(ductgpu_ctx ctx)
     return rc ? rc : device_status(ctx);
 }
 
+int ductgpu_selftest_wait_timeout(ductgpu_ctx ctx, unsigned polls)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    cudaSetDevice(ctx->device);
+    if (polls < 1) polls = 1;
+    if (polls > (1u << 20)) polls = 1u << 20;
+    return check_cuda(ctx, wait_selftest(ctx, polls), "k_wait_selftest");
+}
+
 int ductgpu_pseudomat(ductgpu_ctx ctx, int my, int mz)
 {
     if (!ctx) return DUCTGPU_EARG;

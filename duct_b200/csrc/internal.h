@@ -250,6 +250,8 @@ int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid);
 // solve_fp64ws.cu: the flip-symmetric pass as a warp-specialised persistent
 // kernel (hpad 32 or 64, every field folded, no residual epilogue)
 cudaError_t fp64_pass_ws(ductgpu_ctx ctx, const PassParams &pp, int hpad);
+// one CTA whose bounded wait runs out after `polls` polls (failure-path self-test)
+cudaError_t wait_selftest(ductgpu_ctx ctx, unsigned polls);
 // Whether a solve (or its adjoint) over these fields runs the flip-symmetric
 // passes: DUCTGPU_PASS_PARITY selected for the size class and every field's
 // operators have the folded form.  The forward and adjoint take the same

@@ -66,9 +66,10 @@ __device__ __forceinline__ bool bar_try(uint64_t *bar, unsigned parity)
 }
 
 // bounded wait; false after the limit or once another role has failed
-__device__ __forceinline__ bool bar_wait(uint64_t *bar, unsigned parity, volatile int *abort)
+__device__ __forceinline__ bool bar_wait(uint64_t *bar, unsigned parity, volatile int *abort,
+                                         unsigned limit = kWsSpin)
 {
-    for (unsigned it = 0; it < kWsSpin; ++it) {
+    for (unsigned it = 0; it < limit; ++it) {
         if (bar_try(bar, parity)) return true;
         if ((it & 255) == 255 && *abort) return false;
         if (it > 64) __nanosleep(64);
@@ -360,6 +361,31 @@ k_pass_fp64w(const __grid_constant__ PassParams p, const __grid_constant__ WsSpl
         group_sync(g);   // the stage is free again
         if (gt == 0) bar_arrive(empty + s);
     }
+}
+
+// Self-test of the failure path: one CTA waits, with the pass kernel's
+// bounded wait, on an mbarrier that nothing arrives at.  The wait gives up
+// after `limit` polls and raises the error word, as a role of the pass
+// kernel does when its partner never hands over; nothing faults or hangs.
+__global__ void k_wait_selftest(unsigned limit, int *err)
+{
+    __shared__ uint64_t bar;
+    __shared__ int abort_flag;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&bar)), "r"(1));
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    const bool ok = bar_wait(&bar, 0, &abort_flag, limit);   // phase 0 never completes
+    if (!__all_sync(0xffffffffu, ok) && threadIdx.x == 0) atomicExch(err, 3);
+}
+
+cudaError_t wait_selftest(ductgpu_ctx ctx, unsigned polls)
+{
+    LaunchScope ls(ctx, DUCTGPU_K_OTHER);
+    k_wait_selftest<<<1, 32, 0, ctx->stream>>>(polls, ctx->dev_err);
+    return cudaGetLastError();
 }
 
 template <int H>

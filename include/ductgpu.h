@@ -59,6 +59,14 @@ int ductgpu_set_stream(ductgpu_ctx ctx, void *cuda_stream);
 /* Returns the stream work is launched on (for events around a call).      */
 void *ductgpu_get_stream(ductgpu_ctx ctx);
 int ductgpu_synchronize(ductgpu_ctx ctx);
+/* Self-test of the device-side failure path (no counterpart in the
+ * reference, whose GPU code has no bounded waits): one CTA waits, with the
+ * bounded wait of the pipelined pass kernels, on a barrier that nothing
+ * completes; after about `polls` polls (clamped to 1..1<<20, well under a
+ * second) it gives up and raises the context's error word.  The call itself
+ * returns DUCTGPU_OK; the next ductgpu_synchronize returns DUCTGPU_ETIMEOUT
+ * and clears the word, and the context stays usable.                      */
+int ductgpu_selftest_wait_timeout(ductgpu_ctx ctx, unsigned polls);
 
 /* ---- setup (one-time) ------------------------------------------------- */
 /* pseudomat('d',my) then pseudomat('n',my) (src/pseudomat.f90:2-312, called
