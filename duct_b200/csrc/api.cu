@@ -487,9 +487,16 @@ int ductgpu_helm3d(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, char bou
 // context stream and field i-2 copied back on a third.  Each solve is the
 // whole field's batch.  From pinned host memory (ductgpu_host_alloc) the
 // copies run asynchronously; pageable memory gives the same results.
-// mode ranges per field in ductgpu_helm3d_batch: 2 and 4 were measured no
-// faster at cfg1 (the host link is the limit; more pieces add launches)
-constexpr int kBatchPieces = 1;
+// Mode ranges per field in ductgpu_helm3d_batch: the first and the last
+// field go through in two, the others whole.  Only the head (the first
+// upload, before any download can start) and the tail (the last solve and
+// download, after the uploads end) use one direction of the host link, so
+// halving those two pieces is what pays; splitting every field adds solves
+// of small batches (0.06 ms of launches each) between the copies and was
+// slower.  cfg1 (4 fields of 64 modes, pinned host arrays): one piece per
+// field 1.94 ms a call, first and last in two 1.87 ms, every field in two
+// 2.08 ms, in four 2.40 ms.
+static int batch_pieces(int i, int nfields) { return (i == 0 || i == nfields - 1) ? 2 : 1; }
 
 int ductgpu_helm3d_batch(ductgpu_ctx ctx, int nfields, double *const *rhs, double *const *sol, const char *bounds,
                          const double *alambdas, int my, int mz, int ib, int ie, const double *xalp, int precision)
@@ -538,16 +545,15 @@ int ductgpu_helm3d_batch(ductgpu_ctx ctx, int nfields, double *const *rhs, doubl
     // hold the host until the previous solve ended)
     FieldTask tasks[kMaxFields];
     if ((rc = prepare(ctx, f, nfields, tasks))) return rc;
-    // Each field goes through in kBatchPieces mode ranges: piece j is copied
+    // Each field goes through in batch_pieces mode ranges: piece j is copied
     // in while piece j-1 is solved and piece j-2 copied back, so both
     // directions of the host link run at once for all but the first and the
     // last piece.  Events are reused round-robin: every wait on an event is
     // enqueued before the event is recorded again.
-    const int pieces = nm < kBatchPieces ? nm : kBatchPieces;
     const size_t plane = (size_t)2 * my * mz;
     int e = 0;
     for (int i = 0; i < nfields; ++i)
-        for (int p = 0; p < pieces; ++p, ++e) {
+        for (int p = 0, pieces = nm < batch_pieces(i, nfields) ? nm : batch_pieces(i, nfields); p < pieces; ++p, ++e) {
             const int k0 = nm * p / pieces, k1 = nm * (p + 1) / pieces;
             FieldTask t = tasks[i];
             t.rhs = f[i].rhs + plane * k0;
