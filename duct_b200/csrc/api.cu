@@ -483,10 +483,11 @@ int ductgpu_helm3d(ductgpu_ctx ctx, double *rhs, double *sol, int ipro, char bou
 
 // Several fields of one substep on host arrays (u, v, w and p of
 // src/main1.f90:617-619, 643), with the host<->device copies overlapped:
-// field i is copied in on one stream while field i-1 is solved on the
-// context stream and field i-2 copied back on a third.  Each solve is the
-// whole field's batch.  From pinned host memory (ductgpu_host_alloc) the
-// copies run asynchronously; pageable memory gives the same results.
+// a piece (a field, or a mode range of the first or last field) is copied
+// in on one stream while the previous piece is solved on the context stream
+// and the one before copied back on a third.  From pinned host memory
+// (ductgpu_host_alloc) the copies run asynchronously; pageable memory gives
+// the same results.
 // Mode ranges per field in ductgpu_helm3d_batch: the first and the last
 // field go through in two, the others whole.  Only the head (the first
 // upload, before any download can start) and the tail (the last solve and

@@ -113,9 +113,10 @@ int ductgpu_helm3d(ductgpu_ctx ctx, double *rhs, double *sol, int ipro,
 
 /* The helm3d calls of one substep (u, v, w and p: src/main1.f90:617-619,
  * 643) in one call on host arrays: per field the same effects as
- * ductgpu_helm3d, with field i copied in while field i-1 is solved and
- * field i-2 copied back (pinned host memory from ductgpu_host_alloc makes
- * the copies asynchronous).  rhs[i], sol[i]: complex (my,mz,ie-ib+1) host
+ * ductgpu_helm3d, with each field (the first and the last in two mode
+ * ranges) copied in while the previous one is solved and the one before
+ * copied back (pinned host memory from ductgpu_host_alloc makes the
+ * copies asynchronous).  rhs[i], sol[i]: complex (my,mz,ie-ib+1) host
  * arrays; bounds[i] 'd' or 'n'; alambdas[i]; one xalp for all fields.    */
 int ductgpu_helm3d_batch(ductgpu_ctx ctx, int nfields, double *const *rhs, double *const *sol,
                          const char *bounds, const double *alambdas, int my, int mz, int ib,
