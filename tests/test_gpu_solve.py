@@ -245,3 +245,22 @@ def test_helm3d_batch_matches_single_calls(gpu_ctx):
         assert np.array_equal(a, b)
         if bd == "d":
             assert np.all(r[0, :, :] == 0) and np.all(r[:, -1, :] == 0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nm", [1, 2, 3])
+@pytest.mark.parametrize("nf", [1, 2])
+def test_helm3d_batch_small_mode_counts(gpu_ctx, nm, nf):
+    """The batch splits its first and last field into two mode ranges when
+    it can: with 1-3 modes and one or two fields every range is non-empty
+    and the results equal single helm3d calls bit for bit."""
+    m = 33
+    gpu_ctx.pseudomat(m)
+    xalp = 0.5 * np.arange(nm) + 0.25
+    specs = [("d", 2.0e3), ("n", 1.0)][:nf]
+    fs = [synth.chebyshev_rhs(m, m, nm, seed=80 + i, ib=0) for i in range(nf)]
+    single = [gpu_ctx.helm3d(f.copy(order="F"), b, lam, xalp, ipro=1) for f, (b, lam) in zip(fs, specs)]
+    rh = [f.copy(order="F") for f in fs]
+    batch = gpu_ctx.helm3d_batch(rh, [b for b, _ in specs], [lam for _, lam in specs], xalp)
+    for a, b in zip(batch, single):
+        assert np.array_equal(a, b)
