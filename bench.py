@@ -19,7 +19,13 @@ Arms:
   overlapped with the solves) for the same work.
 * ``--impl reference``: the reference's CPU algorithm (the oracle's
   restatement of helm3d/solvediag with the same LAPACK/BLAS calls) on all
-  host cores.
+  host cores; under torchrun rank 0 alone runs it and prints the line.
+
+Several GPUs (``--gpus N`` under torchrun, one rank per GPU): replicas only
+-- every rank solves its own copy of the step (no exchange: Fourier modes
+are independent), ``value`` is all ranks' mode-solves over the slowest
+rank's time (max over ranks), ``scaling`` weak.  NCCL carries the barrier
+and the max on GPUs; without a GPU the same host logic runs over gloo.
 """
 import argparse
 import json
