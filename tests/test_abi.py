@@ -45,3 +45,5 @@ def test_null_context_is_rejected():
     assert L.ductgpu_pseudomat(None, 33, 33) == D.EARG
     assert L.ductgpu_destroy(None) == D.EARG
     assert L.ductgpu_launch_count(None) == -1
+    assert L.ductgpu_synchronize(None) == D.EARG
+    assert L.ductgpu_selftest_wait_timeout(None, 16) == D.EARG
