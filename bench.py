@@ -393,10 +393,12 @@ def run_ours(args, world, rank, local, pg):
     cfg2 = uneven_rect_rate(ctx, args) if not args.no_transforms else None
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, threads, done, el = cpu_reference_rate(c, m, xalp, rhs, budget_s=10.0)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": "%d mode-solves (whole cfg1 batches) in %.1f s" % (done, el)}
+        parity = parity_vs_oracle(ctx, c, m, xalp, rhs, sets, list(res), local)
 
     for fl in sets:
         for f in fl:
@@ -422,12 +424,128 @@ def run_ours(args, world, rank, local, pg):
             "roofline": roofs[best], "cpu_baseline": cpu, "e2e": e2e, "clocks": B["clk"],
             "paths": {k: {"value": v["value"], "ms_per_step": v["ms_step"], "roofline": roofs[k],
                           "gpu_launches": v["launches"], "graph": v["graph"]} for k, v in res.items()},
+            "parity": parity,
             "mixed_rel_err_vs_fp64": acc,
             "int8_rel_err_vs_fp64": acc8,
             "hbm_kernels": hbm,
             "cfg2_uneven_rect_batch": cfg2,
         }
         print(json.dumps(line), flush=True)
+
+
+def _errs(a, b):
+    """Relative error of a against b: 2-norm over all points and max-norm."""
+    d = (a - b).ravel()
+    return {"l2": float(np.linalg.norm(d) / np.linalg.norm(b.ravel())),
+            "max": float(np.abs(d).max() / np.abs(b).max())}
+
+
+def _exact_interior(F, B, P, Q, E, lam, io=None, iters=4):
+    """The solution of the FP64 discrete interior operator B(x)I + I(x)B - lam
+    by iterative refinement with long-double residuals (the FP64
+    diagonalisation as the preconditioner), pinned at interior point io
+    like the reference's kx=0 mode."""
+    Bl = B.astype(np.longdouble)
+    U = np.zeros_like(F, dtype=np.longdouble)
+    den = E[:, None] + E[None, :] - lam
+    if io is not None:
+        den[io, io] = np.inf
+    for _ in range(iters):
+        R = (F.astype(np.longdouble) - (Bl @ U + U @ Bl.T - lam * U)).astype(np.float64)
+        d = P @ ((Q @ R @ Q.T) / den) @ P.T
+        if io is not None:
+            d = d - d[io, io] * np.outer(P[:, io], P[:, io]) / P[io, io] ** 2
+        U = U + d.astype(np.longdouble)
+    return U.astype(np.float64)
+
+
+def parity_vs_oracle(ctx, c, m, xalp, rhs, sets, paths, device):
+    """The relative error of every path's result against the oracle (the
+    reference's CPU algorithm, same LAPACK calls), per field, at cfg1 and
+    cfg0.  The kx=0 pressure is compared in the reference's gauge: the
+    pinned point U(iofzero+1, iofzero+1) with iofzero from the host's
+    LAPACK order, which the caller passes (ductgpu_set_gauge_point).  Two
+    operator sources: the library's own eigen-decomposition (the default
+    drop-in) and the host's LAPACK operators imported on a grid-only set-up
+    (ductgpu_pseudomat_ex + ductgpu_set_operators).  For the Neumann field,
+    whose own-operator error is set by FP64 rounding of the eigenvectors,
+    the error of both the GPU and the oracle against an extended-precision
+    solution of the same discrete operator is given on a subset of modes."""
+    import duct_b200 as D
+    from duct_b200 import synth
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    ops = O.Ops(m)
+    refs = [O.helm3d(f, ops, bound, lam, xalp, nthreads=threads)[0] for (_, bound, lam), f in zip(c["fields"], rhs)]
+    precs = {"fp64": D.PREC_FP64, "mixed": D.PREC_MIXED, "int8": D.PREC_INT8}
+    out = {"reference": "oracle helm3d (LAPACK dgeev/dgetrf/dgetri + dgemm), same seeded inputs",
+           "gauge": "kx=0 pressure pinned at U(iofzero+1,iofzero+1)=0, iofzero=%d from the host LAPACK order "
+                    "(ductgpu_set_gauge_point)" % ops.iofzero,
+           "cfg1": {}}
+
+    def solve_all(cx, prec):
+        for f, (name, bound, lam), r in zip(sets[0], c["fields"], rhs):
+            f["rhs"].upload(r)
+        cx.solve_fields_dev(sets[0], prec)
+        cx.synchronize()
+        return [f["sol"].download() for f in sets[0]]
+
+    ctx.set_gauge_point(ops.iofzero)
+    own = {}
+    for name in paths:
+        got = solve_all(ctx, precs[name])
+        own[name] = got
+        out["cfg1"]["%s_own_operators" % name] = {fn: _errs(g, r) for (fn, _, _), g, r in zip(c["fields"], got, refs)}
+    ctx.set_gauge_point(0)
+    # the host's LAPACK operators on a grid-only set-up
+    with D.Context(device) as c2:
+        c2.pseudomat_ex(m, D.SETUP_NO_EIGEN)
+        c2.set_operators("d", ops.ED, ops.PD, ops.PDM1)
+        c2.set_operators("n", ops.EN, ops.PN, ops.PNM1, ops.iofzero)
+        got = solve_all(c2, D.PREC_FP64)
+        out["cfg1"]["fp64_lapack_operators"] = {fn: _errs(g, r) for (fn, _, _), g, r in zip(c["fields"], got, refs)}
+        out["cfg1"]["fp64_lapack_operators_folded"] = bool(c2.folded("d") and c2.folded("n"))
+    # accuracy of the Neumann field against the extended-precision solution
+    ip = [i for i, (_, b, _) in enumerate(c["fields"]) if b == "n"]
+    if ip and "fp64" in own:
+        i = ip[0]
+        lam0 = c["fields"][i][2]
+        E, P, Q = np.asarray(ops.EN), np.asarray(ops.PN), np.asarray(ops.PNM1)
+        io = ops.iofzero - 1
+        sub = [k for k in (0, 1, 2, 8, 32, len(xalp) - 1) if k < len(xalp)]
+        eg, eo, nrm = 0.0, 0.0, 0.0
+        for k in sub:
+            lam = lam0 + xalp[k] ** 2
+            F = rhs[i][1:-1, 1:-1, k]
+            for part in (np.real, np.imag):
+                Fk = np.ascontiguousarray(part(F))
+                if not np.any(Fk):
+                    continue
+                X = _exact_interior(Fk, np.asarray(ops.D2Bn), P, Q, E, lam, io if abs(lam) < 1e-10 else None)
+                eg += np.sum((part(own["fp64"][i][1:-1, 1:-1, k]) - X) ** 2)
+                eo += np.sum((part(refs[i][1:-1, 1:-1, k]) - X) ** 2)
+                nrm += np.sum(X ** 2)
+        out["cfg1"]["p_vs_extended_precision"] = {
+            "modes": sub, "gpu_fp64_own_operators_l2": float(np.sqrt(eg / nrm)),
+            "oracle_l2": float(np.sqrt(eo / nrm)),
+            "solution": "long-double-residual iterative refinement of the FP64 Neumann interior operator"}
+    # cfg0: 33^2, 17 modes, Dirichlet, lambda = kx^2 + 4e6
+    c0 = synth.config("cfg0")
+    m0, nm0 = c0["my"], c0["nmodes"]
+    x0 = c0["alp"] * np.arange(nm0)
+    ops0 = O.Ops(m0)
+    r0 = synth.chebyshev_rhs(m0, m0, nm0, seed=0, ib=0)
+    out["cfg0"] = {}
+    for (fname, bound, lam) in c0["fields"]:
+        ref0 = O.helm3d(r0, ops0, bound, lam, x0, nthreads=threads)[0]
+        with D.Context(device) as c3:
+            c3.pseudomat(m0)
+            for name in paths:
+                if name == "int8" and m0 > 129:
+                    continue
+                g = c3.helm3d(r0.copy(order="F"), bound, lam, x0, precision=precs[name])
+                out["cfg0"]["%s_own_operators_%s" % (name, fname)] = _errs(g, ref0)
+    return out
 
 
 def bf16_peak():

@@ -38,7 +38,9 @@ EXPORTS = [
     "ductgpu_solve_adjoint_fields_dev", "ductgpu_helm3d_adjoint",
     "ductgpu_pseudopois", "ductgpu_solvepois", "ductgpu_solve_pois_fields_dev",
     "ductgpu_set_pass_kernel", "ductgpu_autotune", "ductgpu_helm3d_batch",
+    "ductgpu_pseudomat_ex", "ductgpu_set_gauge_point", "ductgpu_get_fold",
 ]
+SETUP_NO_EIGEN = 1
 K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
 
 
@@ -76,6 +78,9 @@ def lib():
             "ductgpu_synchronize": [P],
             "ductgpu_selftest_wait_timeout": [P, C.c_uint],
             "ductgpu_pseudomat": [P, I, I],
+            "ductgpu_pseudomat_ex": [P, I, I, I],
+            "ductgpu_set_gauge_point": [P, I],
+            "ductgpu_get_fold": [P, C.c_char, C.POINTER(I)],
             "ductgpu_get_operators": [P, C.c_char, P, P, P, C.POINTER(I)],
             "ductgpu_set_operators": [P, C.c_char, P, P, P, I],
             "ductgpu_set_gauge": [P, I],
@@ -218,6 +223,22 @@ class Context:
     def pseudomat(self, my, mz=None):
         self._check(lib().ductgpu_pseudomat(self.h, int(my), int(mz if mz is not None else my)))
         self._my = int(my)
+
+    def pseudomat_ex(self, my, flags=SETUP_NO_EIGEN):
+        """Grid-only set-up (flags SETUP_NO_EIGEN): the eigen-decompositions
+        are imported afterwards with set_operators('d'/'n')."""
+        self._check(lib().ductgpu_pseudomat_ex(self.h, int(my), int(my), int(flags)))
+        self._my = int(my)
+
+    def set_gauge_point(self, iofzero):
+        """The kx=0 Neumann gauge point U(iofzero+1, iofzero+1) (1-based
+        interior index; 0 restores the operators' own iofzero)."""
+        self._check(lib().ductgpu_set_gauge_point(self.h, int(iofzero)))
+
+    def folded(self, bound):
+        out = C.c_int()
+        self._check(lib().ductgpu_get_fold(self.h, bound.encode(), C.byref(out)))
+        return bool(out.value)
 
     def get_operators(self, bound, n):
         E = np.empty(n)

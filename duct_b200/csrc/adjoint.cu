@@ -200,7 +200,7 @@ int solve_adjoint(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
             fp.nf = fn;
             fp.DC = ctx->DC; fp.AM1 = ctx->AM1; fp.ccw = ctx->ccw; fp.pcol = ctx->neu.pcol; fp.lam = ctx->lam;
             fp.m = m;
-            fp.io = ctx->neu.pcol ? ctx->neu.iofzero - 1 : -1;
+            fp.io = ctx->neu.pcol ? pin_index(ctx) : -1;
             fp.gauge = ctx->gauge;
             fp.plane_stride = ps;
             LaunchScope ls(ctx, DUCTGPU_K_NEUMANN);

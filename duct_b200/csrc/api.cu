@@ -180,6 +180,7 @@ int ductgpu_create(int device, ductgpu_ctx *out)
         delete c;
         return DUCTGPU_EALLOC;
     }
+    noalloc_reserve(c);
     *out = c;
     return DUCTGPU_OK;
 }
@@ -282,7 +283,27 @@ int ductgpu_pseudomat(ductgpu_ctx ctx, int my, int mz)
     if (my != mz)
         return set_error(ctx, DUCTGPU_EARG, "IN HELM3D: MY.NE.MZ (NOT IMPLEMENTED): my=%d mz=%d", my, mz);
     cudaSetDevice(ctx->device);
-    return pseudomat_gpu(ctx, my);
+    return pseudomat_gpu(ctx, my, true);
+}
+
+int ductgpu_pseudomat_ex(ductgpu_ctx ctx, int my, int mz, int flags)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (my != mz)
+        return set_error(ctx, DUCTGPU_EARG, "IN HELM3D: MY.NE.MZ (NOT IMPLEMENTED): my=%d mz=%d", my, mz);
+    if (flags & ~DUCTGPU_SETUP_NO_EIGEN) return set_error(ctx, DUCTGPU_EARG, "setup flags 0x%x", flags);
+    cudaSetDevice(ctx->device);
+    return pseudomat_gpu(ctx, my, !(flags & DUCTGPU_SETUP_NO_EIGEN));
+}
+
+int ductgpu_set_gauge_point(ductgpu_ctx ctx, int iofzero)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    if (!ctx->grid_ready) return set_error(ctx, DUCTGPU_ESTATE, "call ductgpu_pseudomat first");
+    if (iofzero < 0 || iofzero > ctx->my - 2)
+        return set_error(ctx, DUCTGPU_EARG, "gauge point %d outside 0..%d", iofzero, ctx->my - 2);
+    ctx->pin_point = iofzero;
+    return DUCTGPU_OK;
 }
 
 int ductgpu_get_operators(ductgpu_ctx ctx, char bound, double *E, double *P, double *PM1, int *iofzero)
@@ -303,7 +324,7 @@ int ductgpu_get_operators(ductgpu_ctx ctx, char bound, double *E, double *P, dou
 int ductgpu_set_operators(ductgpu_ctx ctx, char bound, const double *E, const double *P, const double *PM1, int iofzero)
 {
     if (!ctx) return DUCTGPU_EARG;
-    if (bound == 'p' ? !ctx->pois_m : !ctx->ready)
+    if (bound == 'p' ? !ctx->pois_m : !ctx->grid_ready)
         return set_error(ctx, DUCTGPU_ESTATE, bound == 'p' ? "call ductgpu_pseudopois first" : "call ductgpu_pseudomat first");
     if (bound != 'd' && bound != 'n' && bound != 'p') return set_error(ctx, DUCTGPU_EARG, "bound '%c'", bound);
     if (!E || !P || !PM1) return set_error(ctx, DUCTGPU_EARG, "null operator");
@@ -332,15 +353,23 @@ int ductgpu_set_operators(ductgpu_ctx ctx, char bound, const double *E, const do
     }
     int rc = pack_operators(ctx, b);
     if (rc) return rc;
-    // imported operators are applied as given: no flip-symmetric form
-    cudaFree(b.Pfold);
-    cudaFree(b.Qfold);
-    cudaFree(b.PfoldT);
-    cudaFree(b.QfoldT);
-    cudaFree(b.Eperm);
-    b.Pfold = b.Qfold = b.PfoldT = b.QfoldT = b.Eperm = nullptr;
-    b.fold_ok = false;
-    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "set_operators");
+    // imported operators keep the flip-symmetric passes when their
+    // eigenvectors have a clean parity (the half blocks are read off them)
+    if (bound != 'p' && (rc = fold_imported(ctx, b, E, P, PM1))) return rc;
+    if ((rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "set_operators"))) return rc;
+    if (bound != 'p') {
+        ctx->ops_set |= (bound == 'd') ? 1 : 2;
+        ctx->ready = ctx->grid_ready && ctx->ops_set == 3;
+    }
+    return DUCTGPU_OK;
+}
+
+int ductgpu_get_fold(ductgpu_ctx ctx, char bound, int *folded)
+{
+    if (!ctx || !folded) return DUCTGPU_EARG;
+    if (bound != 'd' && bound != 'n') return set_error(ctx, DUCTGPU_EARG, "bound '%c'", bound);
+    *folded = ((bound == 'n') ? ctx->neu : ctx->dir).fold_ok ? 1 : 0;
+    return DUCTGPU_OK;
 }
 
 int ductgpu_set_gauge(ductgpu_ctx ctx, int gauge)

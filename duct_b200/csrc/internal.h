@@ -95,7 +95,10 @@ struct ductgpu_ctx_s {
     char err[512] = {0};
 
     int my = 0, mz = 0;
-    bool ready = false;
+    bool ready = false;        // grid and both eigen-decompositions set up
+    bool grid_ready = false;   // grid, D, D2, blocks, AM1 (ductgpu_pseudomat[_ex])
+    int ops_set = 0;           // eigen-decompositions present: 1 Dirichlet, 2 Neumann
+    int pin_point = 0;         // kx=0 Neumann gauge point (1-based interior index; 0: iofzero)
     double *xcol = nullptr;    // [my]
     double *DC = nullptr;      // [my*my]
     double *dcr = nullptr;     // [2*my] rows 1 and my of DC, contiguous (Neumann walls)
@@ -163,8 +166,15 @@ struct ductgpu_ctx_s {
 namespace duct {
 
 int set_error(ductgpu_ctx ctx, int code, const char *fmt, ...);
+// 0-based interior index of the kx=0 Neumann gauge point: the caller's
+// (ductgpu_set_gauge_point), else the position of the smallest |eigenvalue|
+// in the operator's own order (the reference's iofzero rule)
+inline int pin_index(ductgpu_ctx c) { return (c->pin_point > 0 ? c->pin_point : c->neu.iofzero) - 1; }
 int check_cuda(ductgpu_ctx ctx, cudaError_t e, const char *what);
 int ensure(ductgpu_ctx ctx, Workspace &w, size_t bytes);
+// noalloc.cu: looks up the fixed scratch of the no-allocation entry point
+// on the context's GPU (at context creation)
+void noalloc_reserve(ductgpu_ctx ctx);
 
 // Brackets one kernel launch with profiling events when enabled and
 // counts it.  Use: { LaunchScope ls(ctx, DUCTGPU_K_...); kernel<<<>>>(); }
@@ -177,10 +187,14 @@ struct LaunchScope {
 void profile_drain(ductgpu_ctx ctx);
 
 // setup.cu
-int pseudomat_gpu(ductgpu_ctx ctx, int m);
+// eigen false: grid, D, D2, interior blocks and AM1 only; the
+// eigen-decompositions are then imported with ductgpu_set_operators
+int pseudomat_gpu(ductgpu_ctx ctx, int m, bool eigen = true);
 int pack_operators(ductgpu_ctx ctx, BoundOps &b);
 // flip-symmetric half operators of b (fold_ok false when b lacks the symmetry)
 int fold_operators(ductgpu_ctx ctx, BoundOps &b);
+// the same for imported operators (host E, P, PM1), read off their parity
+int fold_imported(ductgpu_ctx ctx, BoundOps &b, const double *E, const double *P, const double *PM1);
 int pack_transposed(ductgpu_ctx ctx, BoundOps &b);
 // Real eigen-decomposition of the n x n device matrix B (destroyed) into
 // b.E, b.P, b.PM1 (allocated by the caller), with emin/emax and iofzero.

@@ -18,9 +18,18 @@
 //    streams) race on it and give wrong results -- serialise them;
 //  * nothing in it needs to start at zero: each call writes every scratch
 //    element (lambda copy, intermediate interiors) before reading it;
-//  * the first call on a GPU takes the array's device address with
-//    cudaGetSymbolAddress (which also loads this file's device code there);
-//    make that first call before any stream capture on that GPU.
+//  * the array's device address is taken with cudaGetSymbolAddress when
+//    the first context is created on a GPU (ductgpu_create calls
+//    noalloc_reserve); under CUDA's default lazy module loading that is
+//    also when the 32 MiB is taken, under eager loading
+//    (CUDA_MODULE_LOADING=EAGER) it is taken when the library's code is
+//    loaded on the GPU.  Create the context before a pool allocator
+//    reserves the device, and before any stream capture.  If the look-up
+//    fails there it is retried by the first call, which then reports it;
+//  * the solve's own kernels are loaded on their first launch under lazy
+//    loading, which takes device memory for their code: a caller whose
+//    pool will hold the whole device sets CUDA_MODULE_LOADING=EAGER or makes
+//    one call of this entry before its pool reserves the device.
 #include <mutex>
 
 #include "internal.h"
@@ -50,10 +59,14 @@ int scratch_for_device(ductgpu_ctx ctx, double **out)
         return duct::set_error(ctx, DUCTGPU_EARG, "noalloc: device %d beyond %d", ctx->device, kMaxDevices);
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (!g_scratch_dev[ctx->device]) {
-        cudaError_t e = cudaSetDevice(ctx->device);
-        if (e != cudaSuccess) return duct::check_cuda(ctx, e, "noalloc: cudaSetDevice");
+        int prev = 0;
+        cudaError_t e = cudaGetDevice(&prev);
+        if (e != cudaSuccess) return duct::check_cuda(ctx, e, "noalloc: cudaGetDevice");
+        if ((e = cudaSetDevice(ctx->device)) != cudaSuccess)
+            return duct::check_cuda(ctx, e, "noalloc: cudaSetDevice");
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_scratch);
+        cudaSetDevice(prev);   // the caller's current device is left as it was
         if (e != cudaSuccess) return duct::check_cuda(ctx, e, "noalloc: cudaGetSymbolAddress");
         g_scratch_dev[ctx->device] = static_cast<double *>(p);
     }
@@ -62,6 +75,22 @@ int scratch_for_device(ductgpu_ctx ctx, double **out)
 }
 
 }  // namespace
+
+namespace duct {
+
+// Called by ductgpu_create: takes the scratch's address on the context's
+// GPU up front.  A failure here is not the context's: it is cleared, and
+// the first call of the entry point retries and reports it.
+void noalloc_reserve(ductgpu_ctx ctx)
+{
+    double *p = nullptr;
+    if (scratch_for_device(ctx, &p) != DUCTGPU_OK) {
+        ctx->err[0] = 0;
+        cudaGetLastError();
+    }
+}
+
+}  // namespace duct
 
 extern "C" int ductgpu_solve_fields_dev_noalloc(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields)
 {

@@ -237,6 +237,138 @@ int pack_operators(ductgpu_ctx ctx, BoundOps &b)
     return check_cuda(ctx, cudaGetLastError(), "pack_operators");
 }
 
+// Packs the two half blocks of a flip-symmetric operator b: Ue (he x he)
+// and Uo (ho x ho) are the eigenvectors of the even and odd blocks on the
+// first-half points, Ie and Io their inverses acting on the folded input
+// (in_k + in_{n-1-k} for the even block, in_k - in_{n-1-k} for the odd one,
+// in_mid alone at the middle), Ee and Eo the eigenvalues.
+static int store_fold(ductgpu_ctx ctx, BoundOps &b, const std::vector<double> &Ue, const std::vector<double> &Ie,
+                      const std::vector<double> &Ee, const std::vector<double> &Uo, const std::vector<double> &Io,
+                      const std::vector<double> &Eo)
+{
+    const int n = b.n, he = (n + 1) / 2, ho = n / 2;
+    const int hpad = (he + 31) / 32 * 32;
+    // the two half blocks stacked, 2 hpad x hpad, in the fragment order of k_pack_a
+    const int mtiles = 2 * hpad / 16;
+    const size_t packed = (size_t)(hpad / 16) * mtiles * 256;
+    std::vector<double> Pf(packed), Qf(packed), PfT(packed), QfT(packed), Ep(n);
+    for (size_t idx = 0; idx < packed; ++idx) {
+        int row, col;
+        pack_slot((int)idx, mtiles, row, col);
+        double pv = 0.0, qv = 0.0, pt = 0.0, qt = 0.0;
+        if (row < hpad) {
+            if (row < he && col < he) {
+                pv = Ue[row + (size_t)he * col];
+                qv = Ie[row + (size_t)he * col] * ((col < ho) ? 0.5 : 1.0);
+                pt = Ue[col + (size_t)he * row];
+                qt = Ie[col + (size_t)he * row] * ((row < ho) ? 0.5 : 1.0);
+            }
+        } else if (row - hpad < ho && col < ho) {
+            const int r = row - hpad;
+            pv = Uo[r + (size_t)ho * col];
+            qv = Io[r + (size_t)ho * col] * 0.5;
+            pt = Uo[col + (size_t)ho * r];
+            qt = Io[col + (size_t)ho * r] * 0.5;
+        }
+        Pf[idx] = pv;
+        Qf[idx] = qv;
+        PfT[idx] = pt;
+        QfT[idx] = qt;
+    }
+    for (int r = 0; r < he; ++r) Ep[r] = Ee[r];
+    for (int r = 0; r < ho; ++r) Ep[he + r] = Eo[r];
+    // the pinned (singular) mode: first index of the smallest |E|, the
+    // rule of the full operators (src/pseudomat.f90:146-152)
+    int sing = -1;
+    if (b.iofzero > 0) {
+        double emin = 1.0e300;
+        for (int r = 0; r < n; ++r)
+            if (fabs(Ep[r]) < emin) { emin = fabs(Ep[r]); sing = r; }
+    }
+    DUCT_CUDA(ctx, cudaMalloc(&b.Pfold, packed * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&b.Qfold, packed * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&b.PfoldT, packed * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&b.QfoldT, packed * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&b.Eperm, n * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.Pfold, Pf.data(), packed * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.Qfold, Qf.data(), packed * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.PfoldT, PfT.data(), packed * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.QfoldT, QfT.data(), packed * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(b.Eperm, Ep.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    b.he = he;
+    b.ho = ho;
+    b.hpad = hpad;
+    b.sing_perm = sing;
+    b.fold_ok = true;
+    return DUCTGPU_OK;
+}
+
+// The flip-symmetric half blocks of imported operators (host arrays E, P,
+// PM1 of ductgpu_set_operators, e.g. the reference's own LAPACK pseudomat):
+// when every eigenvector (column of P) is even or odd to rounding and the
+// matching row of P^-1 has the same parity -- true for a flip-symmetric B
+// with simple eigenvalues -- the half blocks are read off directly, with no
+// eigen-solve: Ue = the first-half rows of the even columns of P, and the
+// even rows q of P^-1 act on the folded input as
+//   q . in = sum_{k<ho} q_k (in_k + in_{n-1-k}) + q_mid in_mid,
+// i.e. Ie(r,k) = 2 q_k (k < ho), Ie(r,mid) = q_mid (the half of store_fold
+// undone); the odd ones likewise with in_k - in_{n-1-k}.  The fold then
+// applies the imported decomposition itself, its modes even first in their
+// given order.  Anything else (a column of mixed parity, counts that are
+// not ceil(n/2) / floor(n/2)) leaves fold_ok false: full passes.
+int fold_imported(ductgpu_ctx ctx, BoundOps &b, const double *E, const double *P, const double *PM1)
+{
+    b.fold_ok = false;
+    cudaFree(b.Pfold);
+    cudaFree(b.Qfold);
+    cudaFree(b.PfoldT);
+    cudaFree(b.QfoldT);
+    cudaFree(b.Eperm);
+    b.Pfold = b.Qfold = b.PfoldT = b.QfoldT = b.Eperm = nullptr;
+    const int n = b.n, he = (n + 1) / 2, ho = n / 2;
+    if (n < 2 || (he + 31) / 32 * 32 > 96) return DUCTGPU_OK;
+    // parity of column c of P and of row c of P^-1: +1 even, -1 odd, 0 mixed
+    auto parity = [&](const double *A, int c, bool row) {
+        double s = 0.0, d = 0.0;
+        for (int k = 0; k < n; ++k) {
+            const double a = row ? A[c + (size_t)n * k] : A[k + (size_t)n * c];
+            const double f = row ? A[c + (size_t)n * (n - 1 - k)] : A[(n - 1 - k) + (size_t)n * c];
+            s += (a + f) * (a + f);
+            d += (a - f) * (a - f);
+        }
+        if (d <= 1.0e-16 * s) return 1;
+        if (s <= 1.0e-16 * d) return -1;
+        return 0;
+    };
+    std::vector<int> ev, od;
+    for (int c = 0; c < n; ++c) {
+        const int pc = parity(P, c, false);
+        if (pc == 0 || parity(PM1, c, true) != pc) return DUCTGPU_OK;
+        (pc > 0 ? ev : od).push_back(c);
+    }
+    if ((int)ev.size() != he || (int)od.size() != ho) return DUCTGPU_OK;
+    std::vector<double> Ue((size_t)he * he), Ie((size_t)he * he), Ee(he), Uo((size_t)ho * ho),
+        Io((size_t)ho * ho), Eo(ho);
+    for (int r = 0; r < he; ++r) {
+        const int c = ev[r];
+        Ee[r] = E[c];
+        for (int k = 0; k < he; ++k) {
+            Ue[k + (size_t)he * r] = P[k + (size_t)n * c];
+            Ie[r + (size_t)he * k] = (k < ho ? 2.0 : 1.0) * PM1[c + (size_t)n * k];
+        }
+    }
+    for (int r = 0; r < ho; ++r) {
+        const int c = od[r];
+        Eo[r] = E[c];
+        for (int k = 0; k < ho; ++k) {
+            Uo[k + (size_t)ho * r] = P[k + (size_t)n * c];
+            Io[r + (size_t)ho * k] = 2.0 * PM1[c + (size_t)n * k];
+        }
+    }
+    return store_fold(ctx, b, Ue, Ie, Ee, Uo, Io, Eo);
+}
+
 // Flip symmetry of the wall-normal operators.  With the same condition on
 // both walls the interior operator B commutes with the reflection J (point
 // k <-> n-1-k, the Gauss-Lobatto nodes being symmetric), so B maps even
@@ -253,8 +385,8 @@ int pack_operators(ductgpu_ctx ctx, BoundOps &b)
 // -- half the flops of a pass.  The result is the diagonalisation solve
 // with another, equally valid, FP64 eigen-decomposition of B (its accuracy
 // against the exact discrete solution is the same as the full one's).
-// Built only for the library's own operators (ductgpu_pseudomat): operators
-// imported with ductgpu_set_operators are applied exactly as given.  B must
+// This decomposes the library's own operators (ductgpu_pseudomat);
+// imported ones are folded by fold_imported, without an eigen-solve.  B must
 // be flip-symmetric to rounding (|B - JBJ| <= 1e-12 max|B|), both blocks'
 // spectra real, and n <= 191; otherwise fold_ok stays false and the solve
 // uses the full operators.  The (symmetric part of) B is folded on the host.
@@ -321,60 +453,7 @@ int fold_operators(ductgpu_ctx ctx, BoundOps &b)
     if (rc == DUCTGPU_ESOLVER) return DUCTGPU_OK;   // a block with a complex pair: full operators
     if (rc) return rc;
 
-    // the two half blocks stacked, 2 hpad x hpad, in the fragment order of k_pack_a
-    const int mtiles = 2 * hpad / 16;
-    const size_t packed = (size_t)(hpad / 16) * mtiles * 256;
-    std::vector<double> Pf(packed), Qf(packed), PfT(packed), QfT(packed), Ep(n);
-    for (size_t idx = 0; idx < packed; ++idx) {
-        int row, col;
-        pack_slot((int)idx, mtiles, row, col);
-        double pv = 0.0, qv = 0.0, pt = 0.0, qt = 0.0;
-        if (row < hpad) {
-            if (row < he && col < he) {
-                pv = Ue[row + (size_t)he * col];
-                qv = Ie[row + (size_t)he * col] * ((col < ho) ? 0.5 : 1.0);
-                pt = Ue[col + (size_t)he * row];
-                qt = Ie[col + (size_t)he * row] * ((row < ho) ? 0.5 : 1.0);
-            }
-        } else if (row - hpad < ho && col < ho) {
-            const int r = row - hpad;
-            pv = Uo[r + (size_t)ho * col];
-            qv = Io[r + (size_t)ho * col] * 0.5;
-            pt = Uo[col + (size_t)ho * r];
-            qt = Io[col + (size_t)ho * r] * 0.5;
-        }
-        Pf[idx] = pv;
-        Qf[idx] = qv;
-        PfT[idx] = pt;
-        QfT[idx] = qt;
-    }
-    for (int r = 0; r < he; ++r) Ep[r] = Ee[r];
-    for (int r = 0; r < ho; ++r) Ep[he + r] = Eo[r];
-    // the pinned (singular) mode: first index of the smallest |E|, the
-    // rule of the full operators (src/pseudomat.f90:146-152)
-    int sing = -1;
-    if (b.iofzero > 0) {
-        double emin = 1.0e300;
-        for (int r = 0; r < n; ++r)
-            if (fabs(Ep[r]) < emin) { emin = fabs(Ep[r]); sing = r; }
-    }
-    DUCT_CUDA(ctx, cudaMalloc(&b.Pfold, packed * sizeof(double)));
-    DUCT_CUDA(ctx, cudaMalloc(&b.Qfold, packed * sizeof(double)));
-    DUCT_CUDA(ctx, cudaMalloc(&b.PfoldT, packed * sizeof(double)));
-    DUCT_CUDA(ctx, cudaMalloc(&b.QfoldT, packed * sizeof(double)));
-    DUCT_CUDA(ctx, cudaMalloc(&b.Eperm, n * sizeof(double)));
-    DUCT_CUDA(ctx, cudaMemcpyAsync(b.Pfold, Pf.data(), packed * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    DUCT_CUDA(ctx, cudaMemcpyAsync(b.Qfold, Qf.data(), packed * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    DUCT_CUDA(ctx, cudaMemcpyAsync(b.PfoldT, PfT.data(), packed * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    DUCT_CUDA(ctx, cudaMemcpyAsync(b.QfoldT, QfT.data(), packed * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    DUCT_CUDA(ctx, cudaMemcpyAsync(b.Eperm, Ep.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    b.he = he;
-    b.ho = ho;
-    b.hpad = hpad;
-    b.sing_perm = sing;
-    b.fold_ok = true;
-    return DUCTGPU_OK;
+    return store_fold(ctx, b, Ue, Ie, Ee, Uo, Io, Eo);
 }
 
 // 4x4 inverse by Gauss-Jordan with partial pivoting (the reference inverts
@@ -579,7 +658,7 @@ int rect_setup(ductgpu_ctx ctx, int slot, int my, int mz, double sy, double sz, 
     return DUCTGPU_OK;
 }
 
-int pseudomat_gpu(ductgpu_ctx ctx, int m)
+int pseudomat_gpu(ductgpu_ctx ctx, int m, bool eigen)
 {
     if (m < 5 || m - 2 > kMaxN)
         return set_error(ctx, DUCTGPU_EARG, "pseudomat: my=%d outside [5,%d]", m, kMaxN + 2);
@@ -590,6 +669,9 @@ int pseudomat_gpu(ductgpu_ctx ctx, int m)
     free_bound(ctx->dir);
     free_bound(ctx->neu);
     ctx->ready = false;
+    ctx->grid_ready = false;
+    ctx->ops_set = 0;
+    ctx->pin_point = 0;
     DUCT_CUDA(ctx, cudaMalloc(&ctx->xcol, m * sizeof(double)));
     DUCT_CUDA(ctx, cudaMalloc(&ctx->DC, (size_t)m * m * sizeof(double)));
     DUCT_CUDA(ctx, cudaMalloc(&ctx->D2, (size_t)m * m * sizeof(double)));
@@ -614,12 +696,12 @@ int pseudomat_gpu(ductgpu_ctx ctx, int m)
     k_block<<<blocks_for((long)n * n), 256, 0, ctx->stream>>>(m, 0, ctx->DC, ctx->D2, blk);
     ctx->launches += 3;
     DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->dir.D2B, blk, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-    int rc = eigen_gpu(ctx, n, blk, ctx->dir);
+    int rc = eigen ? eigen_gpu(ctx, n, blk, ctx->dir) : DUCTGPU_OK;
     if (rc == DUCTGPU_OK) {
         k_block<<<blocks_for((long)n * n), 256, 0, ctx->stream>>>(m, 1, ctx->DC, ctx->D2, blk);
         ctx->launches += 1;
         DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->neu.D2B, blk, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-        rc = eigen_gpu(ctx, n, blk, ctx->neu);
+        if (eigen) rc = eigen_gpu(ctx, n, blk, ctx->neu);
     }
     cudaFree(blk);
     if (rc) return rc;
@@ -655,12 +737,19 @@ int pseudomat_gpu(ductgpu_ctx ctx, int m)
     }
     DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->AM1, A, 16 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     DUCT_CUDA(ctx, cudaMemcpyAsync(ctx->ccw, w.data(), m * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->my = ctx->mz = m;
+    ctx->grid_ready = true;
+    if (!eigen) {
+        // the eigen-decompositions come from ductgpu_set_operators
+        DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        return DUCTGPU_OK;
+    }
     if ((rc = pack_operators(ctx, ctx->dir))) return rc;
     if ((rc = pack_operators(ctx, ctx->neu))) return rc;
     if ((rc = fold_operators(ctx, ctx->dir))) return rc;
     if ((rc = fold_operators(ctx, ctx->neu))) return rc;
     DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    ctx->my = ctx->mz = m;
+    ctx->ops_set = 3;
     ctx->ready = true;
     return DUCTGPU_OK;
 }

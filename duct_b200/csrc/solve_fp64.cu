@@ -1256,7 +1256,7 @@ int neumann_fill(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
     fp.lam = ctx->lam;
     fp.wanted = ctx->wanted;
     fp.m = ctx->my;
-    fp.io = ctx->neu.iofzero - 1;
+    fp.io = ctx->neu.iofzero > 0 ? pin_index(ctx) : -1;
     fp.gauge = ctx->gauge;
     fp.plane_stride = 2LL * ctx->my * ctx->my;
     // the pin only acts on singular planes (|lambda| <= 1e-10, the kx=0

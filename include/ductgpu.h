@@ -77,6 +77,15 @@ int ductgpu_selftest_wait_timeout(ductgpu_ctx ctx, unsigned polls);
  * solver stops otherwise, src/helm3d.f90:37-41).                          */
 int ductgpu_pseudomat(ductgpu_ctx ctx, int my, int mz);
 
+/* pseudomat with options.  DUCTGPU_SETUP_NO_EIGEN builds the grid, D, D2,
+ * the interior blocks, AM1 and the quadrature weights but no
+ * eigen-decomposition: both bounds' (E, P, PM1) then come from
+ * ductgpu_set_operators, e.g. from the host code's own LAPACK pseudomat
+ * (src/pseudomat.f90:131-205), and solves are accepted once 'd' and 'n'
+ * are both set.                                                            */
+#define DUCTGPU_SETUP_NO_EIGEN 1
+int ductgpu_pseudomat_ex(ductgpu_ctx ctx, int my, int mz, int flags);
+
 /* Read back the operators of bound 'd' or 'n' (n = my-2):  E[n] eigenvalues,
  * P[n*n] eigenvectors, PM1[n*n] inverse (column-major), iofzero (1-based,
  * Neumann).  Any output pointer may be NULL.  Bound 'p' reads the
@@ -86,10 +95,31 @@ int ductgpu_get_operators(ductgpu_ctx ctx, char bound, double *E, double *P,
 
 /* Replace the eigen-decomposition of bound 'd' or 'n' with host data, e.g.
  * the LAPACK results of the reference's own pseudomat.  Requires a prior
- * ductgpu_pseudomat for the grid.  iofzero <= 0 recomputes it from E.
- * Bound 'p' replaces the pseudopois operators (after ductgpu_pseudopois). */
+ * ductgpu_pseudomat[_ex] for the grid.  iofzero <= 0 recomputes it from E.
+ * When every eigenvector is even or odd under the wall-to-wall reflection
+ * (a flip-symmetric block with simple eigenvalues, as LAPACK returns for
+ * these operators) the flip-symmetric half-size passes are read off the
+ * imported matrices and the solve keeps their speed; otherwise it runs the
+ * full passes.  Bound 'p' replaces the pseudopois operators (after
+ * ductgpu_pseudopois).                                                     */
 int ductgpu_set_operators(ductgpu_ctx ctx, char bound, const double *E,
                           const double *P, const double *PM1, int iofzero);
+
+/* *folded = 1 when the solves of bound 'd' or 'n' run the flip-symmetric
+ * half-size passes, 0 when they run the full operators.                    */
+int ductgpu_get_fold(ductgpu_ctx ctx, char bound, int *folded);
+
+/* Gauge point of the singular kx=0 Neumann mode.  The reference pins
+ * U(iofzero+1, iofzero+1) = 0 (src/solvediag.f90:195-206), iofzero being the
+ * position of the smallest |eigenvalue| in the order its host LAPACK dgeev
+ * returned (src/pseudomat.f90:141-152).  That order is particular to the
+ * LAPACK build and cannot be derived from another eigen-solver, so a caller
+ * that wants the kx=0 pressure with the reference's additive constant
+ * passes its own iofzero here (1-based interior index, 1..my-2).  0
+ * restores the default: the position of the smallest |eigenvalue| in the
+ * order of the operators in use (the library's own, or imported ones).
+ * Reset by ductgpu_pseudomat.                                              */
+int ductgpu_set_gauge_point(ductgpu_ctx ctx, int iofzero);
 
 /* Gauge of the singular kx=0 Neumann mode (reference default: POINT).     */
 int ductgpu_set_gauge(ductgpu_ctx ctx, int gauge);
@@ -174,9 +204,16 @@ int ductgpu_autotune(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, 
  * and needs 2 * planes * 2 * my * my doubles of that scratch (my = 129: 62
  * planes); larger calls return DUCTGPU_EARG.  The array is shared by all
  * calls on a GPU: calls that overlap on one GPU race on it -- serialise
- * them.  Nothing in it needs clearing first.  The first call on a GPU looks
- * up the array's address (cudaGetSymbolAddress); make it before any stream
- * capture there.  Operators must be set up (ductgpu_pseudomat) beforehand. */
+ * them.  Nothing in it needs clearing first.  The array's address is looked
+ * up (cudaGetSymbolAddress) when the first context is created on a GPU,
+ * which under CUDA's default lazy module loading is also when its 32 MiB
+ * is taken (under CUDA_MODULE_LOADING=EAGER: when the library's code is
+ * loaded on the GPU, whether or not this entry is ever called); create the
+ * context before a pool allocator reserves the device and before any
+ * stream capture.  Under lazy loading the solve's kernels take device
+ * memory for their code at their first launch: set
+ * CUDA_MODULE_LOADING=EAGER, or make one call before the pool reserves the
+ * device.  Operators must be set up (ductgpu_pseudomat) beforehand.        */
 int ductgpu_solve_fields_dev_noalloc(ductgpu_ctx ctx, const ductgpu_field *fields,
                                      int nfields);
 
