@@ -504,16 +504,16 @@ def parity_vs_oracle(ctx, c, m, xalp, rhs, sets, paths, device):
         c2.set_operators("n", ops.EN, ops.PN, ops.PNM1, ops.iofzero)
         got = solve_all(c2, D.PREC_FP64)
         out["cfg1"]["fp64_lapack_operators"] = {fn: _errs(g, r) for (fn, _, _), g, r in zip(c["fields"], got, refs)}
-        out["cfg1"]["fp64_lapack_operators_folded"] = bool(c2.folded("d") and c2.folded("n"))
     # accuracy of the Neumann field against the extended-precision solution
     ip = [i for i, (_, b, _) in enumerate(c["fields"]) if b == "n"]
-    if ip and "fp64" in own:
+    if ip and own:
         i = ip[0]
         lam0 = c["fields"][i][2]
         E, P, Q = np.asarray(ops.EN), np.asarray(ops.PN), np.asarray(ops.PNM1)
         io = ops.iofzero - 1
         sub = [k for k in (0, 1, 2, 8, 32, len(xalp) - 1) if k < len(xalp)]
-        eg, eo, nrm = 0.0, 0.0, 0.0
+        err = {name: 0.0 for name in own}
+        eo, nrm = 0.0, 0.0
         for k in sub:
             lam = lam0 + xalp[k] ** 2
             F = rhs[i][1:-1, 1:-1, k]
@@ -522,13 +522,15 @@ def parity_vs_oracle(ctx, c, m, xalp, rhs, sets, paths, device):
                 if not np.any(Fk):
                     continue
                 X = _exact_interior(Fk, np.asarray(ops.D2Bn), P, Q, E, lam, io if abs(lam) < 1e-10 else None)
-                eg += np.sum((part(own["fp64"][i][1:-1, 1:-1, k]) - X) ** 2)
+                for name in own:
+                    err[name] += np.sum((part(own[name][i][1:-1, 1:-1, k]) - X) ** 2)
                 eo += np.sum((part(refs[i][1:-1, 1:-1, k]) - X) ** 2)
                 nrm += np.sum(X ** 2)
-        out["cfg1"]["p_vs_extended_precision"] = {
-            "modes": sub, "gpu_fp64_own_operators_l2": float(np.sqrt(eg / nrm)),
-            "oracle_l2": float(np.sqrt(eo / nrm)),
-            "solution": "long-double-residual iterative refinement of the FP64 Neumann interior operator"}
+        pe = {"modes": sub, "oracle_l2": float(np.sqrt(eo / nrm)),
+              "solution": "long-double-residual iterative refinement of the FP64 Neumann interior operator"}
+        for name in own:
+            pe["gpu_%s_own_operators_l2" % name] = float(np.sqrt(err[name] / nrm))
+        out["cfg1"]["p_vs_extended_precision"] = pe
     # cfg0: 33^2, 17 modes, Dirichlet, lambda = kx^2 + 4e6
     c0 = synth.config("cfg0")
     m0, nm0 = c0["my"], c0["nmodes"]

@@ -256,6 +256,9 @@ static int device_status(ductgpu_ctx ctx)
     DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (h) {
         cudaMemsetAsync(ctx->dev_err, 0, sizeof(int), ctx->stream);
+        if (h == 2)
+            return set_error(ctx, DUCTGPU_ECUDA, "a tcgen05 pass kernel found its shared memory base misaligned "
+                                                 "(not on 1024 bytes) and did nothing");
         return set_error(ctx, DUCTGPU_ETIMEOUT, "a bounded device-side wait ran out (code %d)", h);
     }
     return DUCTGPU_OK;
@@ -353,9 +356,18 @@ int ductgpu_set_operators(ductgpu_ctx ctx, char bound, const double *E, const do
     }
     int rc = pack_operators(ctx, b);
     if (rc) return rc;
-    // imported operators keep the flip-symmetric passes when their
-    // eigenvectors have a clean parity (the half blocks are read off them)
-    if (bound != 'p' && (rc = fold_imported(ctx, b, E, P, PM1))) return rc;
+    // Imported operators are applied as given, on the full passes.  Their
+    // half blocks cannot be read off them: the eigenvectors of a block built
+    // in floating point are even or odd only to the block's own asymmetry
+    // (~1e-12 relative), and dropping that part moves the solve ~1e-11 away
+    // from the imported decomposition's.
+    cudaFree(b.Pfold);
+    cudaFree(b.Qfold);
+    cudaFree(b.PfoldT);
+    cudaFree(b.QfoldT);
+    cudaFree(b.Eperm);
+    b.Pfold = b.Qfold = b.PfoldT = b.QfoldT = b.Eperm = nullptr;
+    b.fold_ok = false;
     if ((rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "set_operators"))) return rc;
     if (bound != 'p') {
         ctx->ops_set |= (bound == 'd') ? 1 : 2;

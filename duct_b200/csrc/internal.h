@@ -193,8 +193,6 @@ int pseudomat_gpu(ductgpu_ctx ctx, int m, bool eigen = true);
 int pack_operators(ductgpu_ctx ctx, BoundOps &b);
 // flip-symmetric half operators of b (fold_ok false when b lacks the symmetry)
 int fold_operators(ductgpu_ctx ctx, BoundOps &b);
-// the same for imported operators (host E, P, PM1), read off their parity
-int fold_imported(ductgpu_ctx ctx, BoundOps &b, const double *E, const double *P, const double *PM1);
 int pack_transposed(ductgpu_ctx ctx, BoundOps &b);
 // Real eigen-decomposition of the n x n device matrix B (destroyed) into
 // b.E, b.P, b.PM1 (allocated by the caller), with emin/emax and iofzero.

@@ -304,71 +304,6 @@ static int store_fold(ductgpu_ctx ctx, BoundOps &b, const std::vector<double> &U
     return DUCTGPU_OK;
 }
 
-// The flip-symmetric half blocks of imported operators (host arrays E, P,
-// PM1 of ductgpu_set_operators, e.g. the reference's own LAPACK pseudomat):
-// when every eigenvector (column of P) is even or odd to rounding and the
-// matching row of P^-1 has the same parity -- true for a flip-symmetric B
-// with simple eigenvalues -- the half blocks are read off directly, with no
-// eigen-solve: Ue = the first-half rows of the even columns of P, and the
-// even rows q of P^-1 act on the folded input as
-//   q . in = sum_{k<ho} q_k (in_k + in_{n-1-k}) + q_mid in_mid,
-// i.e. Ie(r,k) = 2 q_k (k < ho), Ie(r,mid) = q_mid (the half of store_fold
-// undone); the odd ones likewise with in_k - in_{n-1-k}.  The fold then
-// applies the imported decomposition itself, its modes even first in their
-// given order.  Anything else (a column of mixed parity, counts that are
-// not ceil(n/2) / floor(n/2)) leaves fold_ok false: full passes.
-int fold_imported(ductgpu_ctx ctx, BoundOps &b, const double *E, const double *P, const double *PM1)
-{
-    b.fold_ok = false;
-    cudaFree(b.Pfold);
-    cudaFree(b.Qfold);
-    cudaFree(b.PfoldT);
-    cudaFree(b.QfoldT);
-    cudaFree(b.Eperm);
-    b.Pfold = b.Qfold = b.PfoldT = b.QfoldT = b.Eperm = nullptr;
-    const int n = b.n, he = (n + 1) / 2, ho = n / 2;
-    if (n < 2 || (he + 31) / 32 * 32 > 96) return DUCTGPU_OK;
-    // parity of column c of P and of row c of P^-1: +1 even, -1 odd, 0 mixed
-    auto parity = [&](const double *A, int c, bool row) {
-        double s = 0.0, d = 0.0;
-        for (int k = 0; k < n; ++k) {
-            const double a = row ? A[c + (size_t)n * k] : A[k + (size_t)n * c];
-            const double f = row ? A[c + (size_t)n * (n - 1 - k)] : A[(n - 1 - k) + (size_t)n * c];
-            s += (a + f) * (a + f);
-            d += (a - f) * (a - f);
-        }
-        if (d <= 1.0e-16 * s) return 1;
-        if (s <= 1.0e-16 * d) return -1;
-        return 0;
-    };
-    std::vector<int> ev, od;
-    for (int c = 0; c < n; ++c) {
-        const int pc = parity(P, c, false);
-        if (pc == 0 || parity(PM1, c, true) != pc) return DUCTGPU_OK;
-        (pc > 0 ? ev : od).push_back(c);
-    }
-    if ((int)ev.size() != he || (int)od.size() != ho) return DUCTGPU_OK;
-    std::vector<double> Ue((size_t)he * he), Ie((size_t)he * he), Ee(he), Uo((size_t)ho * ho),
-        Io((size_t)ho * ho), Eo(ho);
-    for (int r = 0; r < he; ++r) {
-        const int c = ev[r];
-        Ee[r] = E[c];
-        for (int k = 0; k < he; ++k) {
-            Ue[k + (size_t)he * r] = P[k + (size_t)n * c];
-            Ie[r + (size_t)he * k] = (k < ho ? 2.0 : 1.0) * PM1[c + (size_t)n * k];
-        }
-    }
-    for (int r = 0; r < ho; ++r) {
-        const int c = od[r];
-        Eo[r] = E[c];
-        for (int k = 0; k < ho; ++k) {
-            Uo[k + (size_t)ho * r] = P[k + (size_t)n * c];
-            Io[r + (size_t)ho * k] = 2.0 * PM1[c + (size_t)n * k];
-        }
-    }
-    return store_fold(ctx, b, Ue, Ie, Ee, Uo, Io, Eo);
-}
-
 // Flip symmetry of the wall-normal operators.  With the same condition on
 // both walls the interior operator B commutes with the reflection J (point
 // k <-> n-1-k, the Gauss-Lobatto nodes being symmetric), so B maps even
@@ -385,8 +320,8 @@ int fold_imported(ductgpu_ctx ctx, BoundOps &b, const double *E, const double *P
 // -- half the flops of a pass.  The result is the diagonalisation solve
 // with another, equally valid, FP64 eigen-decomposition of B (its accuracy
 // against the exact discrete solution is the same as the full one's).
-// This decomposes the library's own operators (ductgpu_pseudomat);
-// imported ones are folded by fold_imported, without an eigen-solve.  B must
+// Built only for the library's own operators (ductgpu_pseudomat): operators
+// imported with ductgpu_set_operators are applied exactly as given.  B must
 // be flip-symmetric to rounding (|B - JBJ| <= 1e-12 max|B|), both blocks'
 // spectra real, and n <= 191; otherwise fold_ok stays false and the solve
 // uses the full operators.  The (symmetric part of) B is folded on the host.

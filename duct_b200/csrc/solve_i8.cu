@@ -167,6 +167,11 @@ __global__ void __launch_bounds__(256, 1) k_pass_i8(const __grid_constant__ Pass
     uint64_t *bar = reinterpret_cast<uint64_t *>(ecol + kI8N);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // 1024-byte aligned base for the swizzled buffers (see k_pass_i8ws)
+    if (i8_smem(smem) & 1023u) {
+        if (tid == 0) atomicExch(err, 2);
+        return;
+    }
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
@@ -389,6 +394,8 @@ constexpr int kWsN = 32;                            // real columns per tile
 constexpr int kWsBSlice = kWsN * kI8K;              // 4 KB
 constexpr int kWsBStage = kI8Slices * kWsBSlice;    // 28 KB
 constexpr int kWsAcc = kI8Levels * kWsN;            // 224 TMEM columns per set
+static_assert(kI8OpSlice % 1024 == 0 && kI8DataSlice % 1024 == 0 && kWsBStage % 1024 == 0,
+              "swizzle atoms of the operand buffers must stay 1024-byte aligned");
 constexpr uint32_t kWsIdesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kWsN >> 3) << 17) |
                               ((uint32_t)(kI8M >> 4) << 24);
 
@@ -466,6 +473,19 @@ __global__ void __launch_bounds__(544, 1) k_pass_i8ws(const __grid_constant__ Pa
     volatile int *abort = reinterpret_cast<volatile int *>(tslot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     constexpr int kProd = 256, kEpi = 256, kMmaWarp = 16;
+    // The carve-up above keeps every 128-byte-swizzled buffer on a 1024-byte
+    // boundary relative to the base (7 x 16 KB, then 2 x 28 KB), the
+    // mbarriers on 8 bytes and the TMEM slot on 4, provided the base itself
+    // is 1024-byte aligned.  Dynamic shared memory starts on such a boundary
+    // when the kernel declares no static shared memory; a variant that adds
+    // some (e.g. timing arrays) moves the base to a 16-byte boundary only,
+    // which misaligns the descriptors and mbarriers.  Checked before any
+    // barrier or TMEM allocation: the whole CTA returns and the host reads
+    // code 2 from the error word.
+    if (i8_smem(smem) & 1023u) {
+        if (tid == 0) atomicExch(err, 2);
+        return;
+    }
 
     if (warp == kMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"

@@ -41,6 +41,8 @@ constexpr int kLevels = 4;          // L = 2..5
 constexpr int kSliceBits = 7;
 constexpr int kOpSliceBytes = kMxM * kMxK * 2;   // 32 KB
 constexpr int kDataSliceBytes = kMxN * kMxK * 2; // 16 KB
+static_assert(kOpSliceBytes % 1024 == 0 && kDataSliceBytes % 1024 == 0,
+              "swizzle atoms of the operand buffers must stay 1024-byte aligned");
 constexpr int kTmemCols = kLevels * kMxN;        // 256
 constexpr unsigned kSpinLimit = 1u << 24;
 
@@ -166,6 +168,14 @@ __global__ void __launch_bounds__(256, 1) k_pass_mixed(const __grid_constant__ M
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int n = p.n, sk = p.sk, sl = p.sl;
+    // the 128-byte-swizzled operand buffers need a 1024-byte aligned base
+    // (dynamic shared memory starts there only when the kernel has no static
+    // shared memory); checked before any barrier or TMEM allocation, the
+    // whole CTA returns together and the host reads code 2
+    if (smem_u32(smem) & 1023u) {
+        if (tid == 0) atomicExch(p.err, 2);
+        return;
+    }
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"

@@ -96,12 +96,10 @@ int ductgpu_get_operators(ductgpu_ctx ctx, char bound, double *E, double *P,
 /* Replace the eigen-decomposition of bound 'd' or 'n' with host data, e.g.
  * the LAPACK results of the reference's own pseudomat.  Requires a prior
  * ductgpu_pseudomat[_ex] for the grid.  iofzero <= 0 recomputes it from E.
- * When every eigenvector is even or odd under the wall-to-wall reflection
- * (a flip-symmetric block with simple eigenvalues, as LAPACK returns for
- * these operators) the flip-symmetric half-size passes are read off the
- * imported matrices and the solve keeps their speed; otherwise it runs the
- * full passes.  Bound 'p' replaces the pseudopois operators (after
- * ductgpu_pseudopois).                                                     */
+ * Imported operators are applied as given, on the full (not the
+ * flip-symmetric half-size) passes: the solve then restates the reference
+ * arithmetic to rounding.  Bound 'p' replaces the pseudopois operators
+ * (after ductgpu_pseudopois).                                              */
 int ductgpu_set_operators(ductgpu_ctx ctx, char bound, const double *E,
                           const double *P, const double *PM1, int iofzero);
 

@@ -11,9 +11,7 @@ Two routes give the reference's point:
   eigen-decompositions (TOL_NEU, see test_gpu_solve.py);
 * the host's own operators imported on a grid-only set-up
   (ductgpu_pseudomat_ex + ductgpu_set_operators): the solve restates the
-  reference arithmetic (TOL_KERNEL), and the flip-symmetric half-size
-  passes are read off the imported eigenvectors, so this route keeps the
-  fast passes.
+  reference arithmetic on the full passes (TOL_KERNEL).
 """
 import numpy as np
 import pytest
@@ -49,13 +47,13 @@ def test_grid_only_setup_needs_both_bounds(gpu_ctx, oracle):
 
 
 @pytest.mark.parametrize("m", [9, 33, 64, 65, 129, 193])
-def test_imported_operators_fold_and_match(gpu_ctx, oracle, m):
+def test_imported_operators_on_grid_only_setup(gpu_ctx, oracle, m):
     nm = 4
     ops = oracle.Ops(m)
     gpu_ctx.pseudomat_ex(m)
     gpu_ctx.set_operators("d", ops.ED, ops.PD, ops.PDM1)
     gpu_ctx.set_operators("n", ops.EN, ops.PN, ops.PNM1, ops.iofzero)
-    assert gpu_ctx.folded("d") and gpu_ctx.folded("n")
+    assert not gpu_ctx.folded("d") and not gpu_ctx.folded("n")
     xalp = np.array([0.0, 0.5, 3.0, 11.0])
     rhs = synth.chebyshev_rhs(m, m, nm, seed=100 + m, ib=0)
     for bound, lam in (("d", 4.0e6), ("d", 0.0), ("n", 0.0)):
