@@ -1,6 +1,6 @@
 """Build recipe for the CPU oracle (test infrastructure only).
 
-Compiles oracle/duct_oracle.c into oracle/libduct_oracle.so, linked against
+Compiles oracle/duct_oracle.c and oracle/duct_oracle_dns.c into oracle/libduct_oracle.so, linked against
 the OpenBLAS build bundled with SciPy (LP64 LAPACK/BLAS exported with a
 ``scipy_`` prefix), with OpenMP for the mode loop of the CPU baseline.
 """
@@ -23,14 +23,14 @@ def _openblas():
 
 
 def build(force=False):
-    src = os.path.join(HERE, "duct_oracle.c")
-    hdr = os.path.join(HERE, "duct_oracle.h")
+    srcs = [os.path.join(HERE, f) for f in ("duct_oracle.c", "duct_oracle_dns.c")]
+    hdrs = [os.path.join(HERE, f) for f in ("duct_oracle.h", "orc_fft.h")]
     if (not force and os.path.exists(LIB)
-            and os.path.getmtime(LIB) >= max(os.path.getmtime(src), os.path.getmtime(hdr))):
+            and os.path.getmtime(LIB) >= max(os.path.getmtime(f) for f in srcs + hdrs)):
         return LIB
     libdir, name = _openblas()
     cmd = ["gcc", "-O2", "-fPIC", "-shared", "-fopenmp", "-std=c11", "-Wall",
-           "-o", LIB, src, "-L" + libdir, "-l:" + name, "-Wl,-rpath," + libdir, "-lm"]
+           "-o", LIB, *srcs, "-L" + libdir, "-l:" + name, "-Wl,-rpath," + libdir, "-lm"]
     subprocess.check_call(cmd)
     return LIB
 

@@ -9,6 +9,7 @@
  * 244,254-255; src/solvediag.f90:51-80,140-219).
  */
 #include "duct_oracle.h"
+#include "orc_fft.h"
 
 #include <math.h>
 #include <stdlib.h>
@@ -452,34 +453,57 @@ static double *cos_table(int nn)
     return t;
 }
 
+/* REDFT00 through the complex FFT of the even extension (length 2N):
+ * X_k = Re FFT(x_0, x_1, .., x_N, x_{N-1}, .., x_1)_k -- the O(N log N) route
+ * FFTW takes; used for the longer lines (nn >= 64), where the direct sum
+ * would dominate the oracle's time.                                         */
+static void redft00_fft(const double *x, double *X, int nn, const orc_fft_plan *p, double *wa, double *wb)
+{
+    const int N = nn - 1;
+    for (int j = 0; j <= N; ++j) { wa[2 * j] = x[j]; wa[2 * j + 1] = 0.0; }
+    for (int j = 1; j < N; ++j) { wa[2 * (2 * N - j)] = x[j]; wa[2 * (2 * N - j) + 1] = 0.0; }
+    orc_fft(p, wa, wb, 0);
+    for (int k = 0; k < nn; ++k) X[k] = wb[2 * k];
+}
+
 /* tcheb_fftw, src/tchebw.f:62-192 (one direction; identical for y and z). */
 void orc_tcheb(double *cr, long ise, long isa, long nlines, int nn, int iopt)
 {
     double *ctab = cos_table(nn);
     const double dn1 = 1.0 / (double)(nn - 1), dn2 = 0.5 * dn1;
+    const int use_fft = nn >= 64;
+    orc_fft_plan plan;
+    orc_fft_plan_init(&plan, use_fft ? 2 * (nn - 1) : 1);
 #pragma omp parallel
     {
         double *buf = (double *)malloc(sizeof(double) * (size_t)nn);
         double *out = (double *)malloc(sizeof(double) * (size_t)nn);
+        double *wa = (double *)malloc(sizeof(double) * 4 * (size_t)nn);
+        double *wb = (double *)malloc(sizeof(double) * 4 * (size_t)nn);
+#define REDFT00(x, X) (use_fft ? redft00_fft(x, X, nn, &plan, wa, wb) : redft00(x, X, nn, ctab))
 #pragma omp for
         for (long k = 0; k < nlines; ++k) {
             double *c = cr + k * isa;
             for (int j = 0; j < nn; ++j) buf[j] = c[j * ise];
             if (iopt < 0) {
-                redft00(buf, out, nn, ctab);
+                REDFT00(buf, out);
                 for (int j = 1; j < nn - 1; ++j) c[j * ise] = dn1 * out[j];
                 c[0] = dn2 * out[0];
                 c[(long)(nn - 1) * ise] = dn2 * out[nn - 1];
             } else {
                 buf[0] *= 2.0;
                 buf[nn - 1] *= 2.0;
-                redft00(buf, out, nn, ctab);
+                REDFT00(buf, out);
                 for (int j = 0; j < nn; ++j) c[j * ise] = 0.5 * out[j];
             }
         }
+#undef REDFT00
         free(buf);
         free(out);
+        free(wa);
+        free(wb);
     }
+    orc_fft_plan_free(&plan);
     free(ctab);
 }
 

@@ -179,4 +179,45 @@ void orc_set_blas_threads(int n);
 #ifdef __cplusplus
 }
 #endif
+
+/* ---- DNS time step around the solve (duct_oracle_dns.c) ---------------- */
+/* Statistics of one step (src/operators.F:1608-2004, 676-973).            */
+typedef struct {
+    double *mean;       /* 4 my mz: um, vm, wm, pm (x-means, accumulated)   */
+    double *prod;       /* 6 my mz: uub, vvb, wwb, uvb, uwb, vwb            */
+    double *ppb;        /* my mz                                            */
+    double *spec;       /* 4 x 7 x M streamwise spectra at (jinco, kinco)    */
+    double stress4[4];  /* wallstressx of the step's u                      */
+    double energy[3], energy2[3];   /* energy_fou of u, v, w               */
+    int nstat;
+} orc_dns_stats;
+
+void orc_fourx(double *fou, double *phys, int mx1, int mgalx, int my, int nz, int iopt);
+void orc_derivx(const double *u, double *du, int my, int mz, int nmodes, const double *xalp, int ider,
+                double scal, char what);
+void orc_chx2z(double *f, int my, int mz, int M);
+void orc_chz2x(double *f, int my, int mz, int M);
+void orc_advection3d(const double *u, const double *v, const double *w, double *adv1, double *adv2,
+                     double *adv3, int my, int mz, int M, int mgalx, const double *xalp, double aspect,
+                     double *stats2);
+void orc_laplacian3d(double *u, double *flap, int my, int mz, int M, const double *xalp, double aspect,
+                     double scal, char what);
+void orc_grad3d(double *u, double *dxu, double *dyu, double *dzu, int my, int mz, int M, const double *xalp,
+                double aspect, double scal, char what);
+void orc_div3d(const double *u, double *v, double *w, double *div, int my, int mz, int M, const double *xalp,
+               double aspect, double scal);
+void orc_update_uvwp(double *u, double *v, double *w, double *p, double *phi, double *rhsphi, int my, int mz,
+                     int M, const double *xalp, double aspect, double akk, double bkk, double dt, double fnu);
+double orc_max_3din(const double *u, int my, int mz, int M);
+void orc_wallstressx(const double *u, int my, int mz, double aspect, double stress4[4]);
+void orc_energy_fou(const double *u, int my, int mz, int M, double aspect, double *energy, double *energy2);
+void orc_statistics_fou(const double *u, const double *v, const double *w, const double *p, int my, int mz,
+                        int M, double *mean, double *ppb, double *spec);
+void orc_rk_coefficients(double *a, double *b, double *g, double *r);
+double orc_dns_substep(double *u, double *v, double *w, double *p, double *adv1, double *adv2, double *adv3,
+                       double *h1, double *h2, double *h3, int my, int mz, int M, int mgalx, const double *xalp,
+                       double aspect, double fnu, double dt, int krk, const orc_ops *ops, int cmassflow,
+                       double csum, const double *premassfu, const double *premassf, double dpdx,
+                       orc_dns_stats *stats, int nthreads);
+
 #endif

@@ -346,3 +346,215 @@ def set_blas_threads(n):
 __all__ = ["Ops", "Dir", "Shen", "Pois", "solvepois", "precomp_mass_flow", "impose_mass_flow", "solveshen", "helm3d_shen", "helm3d_temp", "solvediag", "helm3d", "transyz", "transyz_plane", "derivyz",
            "cheb2_integral", "cxyz2yzx", "cyzx2xyz", "set_blas_threads", "lib"]
 _ = os
+
+
+# ---- DNS time step around the solve (duct_oracle_dns.c) -------------------
+class _DnsStats(C.Structure):
+    _fields_ = [(n, C.POINTER(C.c_double)) for n in ("mean", "prod", "ppb", "spec")] + [
+        ("stress4", C.c_double * 4), ("energy", C.c_double * 3), ("energy2", C.c_double * 3),
+        ("nstat", C.c_int)]
+
+
+def _dns_sigs(L):
+    P, I, D = C.c_void_p, C.c_int, C.c_double
+    L.orc_fourx.argtypes = [P, P, I, I, I, I, I]
+    L.orc_derivx.argtypes = [P, P, I, I, I, P, I, D, C.c_char]
+    L.orc_advection3d.argtypes = [P, P, P, P, P, P, I, I, I, I, P, D, P]
+    L.orc_laplacian3d.argtypes = [P, P, I, I, I, P, D, D, C.c_char]
+    L.orc_grad3d.argtypes = [P, P, P, P, I, I, I, P, D, D, C.c_char]
+    L.orc_div3d.argtypes = [P, P, P, P, I, I, I, P, D, D]
+    L.orc_update_uvwp.argtypes = [P, P, P, P, P, P, I, I, I, P, D, D, D, D, D]
+    L.orc_max_3din.argtypes = [P, I, I, I]
+    L.orc_max_3din.restype = D
+    L.orc_wallstressx.argtypes = [P, I, I, D, P]
+    L.orc_energy_fou.argtypes = [P, I, I, I, D, C.POINTER(D), C.POINTER(D)]
+    L.orc_statistics_fou.argtypes = [P, P, P, P, I, I, I, P, P, P]
+    L.orc_rk_coefficients.argtypes = [P, P, P, P]
+    L.orc_dns_substep.argtypes = [P, P, P, P, P, P, P, P, P, P, I, I, I, I, P, D, D, D, I, C.POINTER(_Ops), I,
+                                  D, P, P, D, C.POINTER(_DnsStats), I]
+    L.orc_dns_substep.restype = D
+
+
+def _dlib():
+    L = lib()
+    if not getattr(L, "_dns_ready", False):
+        _dns_sigs(L)
+        L._dns_ready = True
+    return L
+
+
+def _cf(a):
+    return np.array(a, dtype=np.complex128, order="F")
+
+
+def fourx(fou=None, phys=None, mgalx=None, iopt=1):
+    """fourx (src/fourier.F:1-68): iopt >= 0 takes a z-cut complex
+    (M, my, nz) array and returns phys (mgalx+2, my, nz); iopt < 0 the
+    inverse (returns the z-cut (M, my, nz) array, M given by fou's shape)."""
+    L = _dlib()
+    if iopt >= 0:
+        fou = _cf(fou)
+        M, my, nz = fou.shape
+        out = np.zeros((mgalx + 2, my, nz), order="F")
+        L.orc_fourx(_p(fou), _p(out), M - 1, mgalx, my, nz, int(iopt))
+        return out
+    phys = np.asfortranarray(phys, dtype=np.float64)
+    n2, my, nz = phys.shape
+    out = np.zeros(fou.shape if fou is not None else (None,), dtype=np.complex128, order="F")
+    L.orc_fourx(_p(out), _p(phys), out.shape[0] - 1, n2 - 2, my, nz, int(iopt))
+    return out
+
+
+def derivx(u, xalp, ider, scal=1.0, what="n", du=None):
+    L = _dlib()
+    u = _cf(u)
+    my, mz, M = u.shape
+    du = np.zeros_like(u, order="F") if du is None else _cf(du)
+    L.orc_derivx(_p(u), _p(du), my, mz, M, _p(np.ascontiguousarray(xalp, dtype=np.float64)), int(ider),
+                 float(scal), what.encode())
+    return du
+
+
+def advection3d(u, v, w, mgalx, xalp, aspect=1.0, stats=False):
+    """advection3d (src/operators.F:9-276) on x-cut fields; returns
+    (adv1, adv2, adv3) and, with stats, the six product x-means
+    (uub, vvb, wwb, uvb, uwb, vwb) as a (6, my, mz) array."""
+    L = _dlib()
+    u, v, w = _cf(u), _cf(v), _cf(w)
+    my, mz, M = u.shape
+    a1, a2, a3 = (np.zeros_like(u, order="F") for _ in range(3))
+    st = np.zeros((my, mz, 6), order="F") if stats else None
+    L.orc_advection3d(_p(u), _p(v), _p(w), _p(a1), _p(a2), _p(a3), my, mz, M, int(mgalx),
+                      _p(np.ascontiguousarray(xalp, dtype=np.float64)), float(aspect), _p(st))
+    if stats:
+        return a1, a2, a3, np.moveaxis(st, 2, 0)
+    return a1, a2, a3
+
+
+def laplacian3d(u, xalp, scal, what="n", flap=None, aspect=1.0):
+    """Returns (flap, u_after): u is transformed in place and back."""
+    L = _dlib()
+    u = _cf(u)
+    my, mz, M = u.shape
+    flap = np.zeros_like(u, order="F") if flap is None else _cf(flap)
+    L.orc_laplacian3d(_p(u), _p(flap), my, mz, M, _p(np.ascontiguousarray(xalp, dtype=np.float64)),
+                      float(aspect), float(scal), what.encode())
+    return flap, u
+
+
+def grad3d(u, xalp, scal, what="n", out=None, aspect=1.0):
+    L = _dlib()
+    u = _cf(u)
+    my, mz, M = u.shape
+    dx, dy, dz = (np.zeros_like(u, order="F") for _ in range(3)) if out is None else (_cf(o) for o in out)
+    L.orc_grad3d(_p(u), _p(dx), _p(dy), _p(dz), my, mz, M, _p(np.ascontiguousarray(xalp, dtype=np.float64)),
+                 float(aspect), float(scal), what.encode())
+    return dx, dy, dz
+
+
+def div3d(u, v, w, xalp, scal, aspect=1.0):
+    L = _dlib()
+    u, v, w = _cf(u), _cf(v), _cf(w)
+    my, mz, M = u.shape
+    d = np.zeros_like(u, order="F")
+    L.orc_div3d(_p(u), _p(v), _p(w), _p(d), my, mz, M, _p(np.ascontiguousarray(xalp, dtype=np.float64)),
+                float(aspect), float(scal))
+    return d
+
+
+def update_uvwp(u, v, w, p, phi, xalp, akk, bkk, dt, fnu, aspect=1.0):
+    """Returns (u, v, w, p, phi_after, rhsphi)."""
+    L = _dlib()
+    u, v, w, p, phi = _cf(u), _cf(v), _cf(w), _cf(p), _cf(phi)
+    my, mz, M = u.shape
+    rhs = np.zeros_like(u, order="F")
+    L.orc_update_uvwp(_p(u), _p(v), _p(w), _p(p), _p(phi), _p(rhs), my, mz, M,
+                      _p(np.ascontiguousarray(xalp, dtype=np.float64)), float(aspect), float(akk), float(bkk),
+                      float(dt), float(fnu))
+    return u, v, w, p, phi, rhs
+
+
+def max_3din(u):
+    u = _cf(u)
+    return _dlib().orc_max_3din(_p(u), *u.shape)
+
+
+def wallstressx(u, aspect=1.0):
+    u = _cf(u)
+    out = np.zeros(4)
+    _dlib().orc_wallstressx(_p(u), u.shape[0], u.shape[1], float(aspect), _p(out))
+    return out
+
+
+def energy_fou(u, aspect=1.0):
+    u = _cf(u)
+    e, e2 = C.c_double(), C.c_double()
+    _dlib().orc_energy_fou(_p(u), *u.shape, float(aspect), C.byref(e), C.byref(e2))
+    return e.value, e2.value
+
+
+def rk_coefficients():
+    a, b, g, r = (np.zeros(3) for _ in range(4))
+    _dlib().orc_rk_coefficients(_p(a), _p(b), _p(g), _p(r))
+    return a, b, g, r
+
+
+class Dns:
+    """The RK3/CN time step of src/main1.f90:384-723 (square duct, no
+    temperature, DT_FIXED) on x-cut complex (my, my, M) fields, with the
+    statistics of src/operators.F gathered at the first substep of a step.
+    cmassflow True: the flow rate of the initial u is held
+    (impose_mass_flow after every substep); else the mean pressure gradient
+    dpdx drives the flow."""
+
+    def __init__(self, u, v, w, p, mgalx, alp, fnu, dt, cmassflow=True, dpdx=0.0, aspect=1.0, nthreads=1):
+        L = _dlib()
+        self.u, self.v, self.w, self.p = (_cf(f) for f in (u, v, w, p))
+        my, mz, M = self.u.shape
+        assert my == mz
+        self.my, self.M, self.mgalx = my, M, int(mgalx)
+        self.xalp = alp * np.arange(M, dtype=np.float64)
+        self.fnu, self.dt, self.aspect, self.nthreads = float(fnu), float(dt), float(aspect), int(nthreads)
+        self.adv = [np.zeros_like(self.u, order="F") for _ in range(3)]
+        self.h = [np.zeros_like(self.u, order="F") for _ in range(3)]
+        self.ops = Ops(my)
+        self.cmassflow, self.dpdx = bool(cmassflow), float(dpdx)
+        a, b, g, r = rk_coefficients()
+        self.premassfu, self.premassf = precomp_mass_flow(self.ops, self.dt, b, self.fnu, aspect)
+        _, self.csum, _ = impose_mass_flow(self.u, 0.0, 1, self.premassfu, self.premassf, 0, aspect)
+        self.stats_mean = np.zeros((my, mz, 4), order="F")
+        self.stats_prod = np.zeros((my, mz, 6), order="F")
+        self.stats_ppb = np.zeros((my, mz), order="F")
+        self.stats_spec = np.zeros((M, 7, 4), order="F")
+        self._st = _DnsStats()
+        self._st.mean = self.stats_mean.ctypes.data_as(C.POINTER(C.c_double))
+        self._st.prod = self.stats_prod.ctypes.data_as(C.POINTER(C.c_double))
+        self._st.ppb = self.stats_ppb.ctypes.data_as(C.POINTER(C.c_double))
+        self._st.spec = self.stats_spec.ctypes.data_as(C.POINTER(C.c_double))
+        self.history = []
+        self.divmax = None
+
+    def substep(self, krk, stats=False):
+        L = _dlib()
+        self.divmax = L.orc_dns_substep(
+            _p(self.u), _p(self.v), _p(self.w), _p(self.p), _p(self.adv[0]), _p(self.adv[1]), _p(self.adv[2]),
+            _p(self.h[0]), _p(self.h[1]), _p(self.h[2]), self.my, self.my, self.M, self.mgalx, _p(self.xalp),
+            self.aspect, self.fnu, self.dt, int(krk), C.byref(self.ops._s), int(self.cmassflow), float(self.csum),
+            _p(self.premassfu), _p(self.premassf), self.dpdx, C.byref(self._st) if stats else None,
+            self.nthreads)
+        if stats and krk == 1:
+            self.history.append(dict(stress4=list(self._st.stress4), energy=list(self._st.energy),
+                                     energy2=list(self._st.energy2)))
+        return self.divmax
+
+    def step(self, stats=False):
+        for krk in (1, 2, 3):
+            self.substep(krk, stats=stats)
+        return self.divmax
+
+    def statistics(self):
+        """Accumulated statistics, each summed over the recorded steps:
+        dict(nstat, mean (4,my,mz), prod (6,my,mz), ppb (my,mz), spec (4,7,M))."""
+        return dict(nstat=self._st.nstat, mean=np.moveaxis(self.stats_mean, 2, 0).copy(),
+                    prod=np.moveaxis(self.stats_prod, 2, 0).copy(), ppb=self.stats_ppb.copy(),
+                    spec=np.transpose(self.stats_spec, (2, 1, 0)).copy())
