@@ -39,9 +39,17 @@ EXPORTS = [
     "ductgpu_pseudopois", "ductgpu_solvepois", "ductgpu_solve_pois_fields_dev",
     "ductgpu_set_pass_kernel", "ductgpu_autotune", "ductgpu_helm3d_batch",
     "ductgpu_pseudomat_ex", "ductgpu_set_gauge_point", "ductgpu_get_fold",
+    "ductgpu_derivx_dev", "ductgpu_laplacian3d_dev", "ductgpu_grad3d_dev", "ductgpu_div3d_dev",
+    "ductgpu_update_uvwp_dev", "ductgpu_advection3d_dev", "ductgpu_max_3din_dev",
+    "ductgpu_wallstressx_dev", "ductgpu_energy_fou_dev", "ductgpu_statistics_fou_dev",
+    "ductgpu_dns_create", "ductgpu_dns_destroy", "ductgpu_dns_set_fields", "ductgpu_dns_get_fields",
+    "ductgpu_dns_field", "ductgpu_dns_set_graphs", "ductgpu_dns_substep", "ductgpu_dns_steps",
+    "ductgpu_dns_statistics",
 ]
 SETUP_NO_EIGEN = 1
-K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER = range(8)
+(K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER, K_LINES,
+ K_ADVECTION, K_STATS) = range(11)
+K_COUNT = 11
 
 
 class RectField(C.Structure):
@@ -127,6 +135,25 @@ def lib():
             "ductgpu_solvepois": [P, P, D, I],
             "ductgpu_solve_pois_fields_dev": [P, C.POINTER(Field), I],
             "ductgpu_graph_launch": [P, I],
+            "ductgpu_derivx_dev": [P, P, P, I, I, I, P, I, D, C.c_char],
+            "ductgpu_laplacian3d_dev": [P, P, P, I, I, I, P, D, D, C.c_char],
+            "ductgpu_grad3d_dev": [P, P, P, P, P, I, I, I, P, D, D, C.c_char],
+            "ductgpu_div3d_dev": [P, P, P, P, P, I, I, I, P, D, D],
+            "ductgpu_update_uvwp_dev": [P, P, P, P, P, P, I, I, I, P, D, D, D, D, D],
+            "ductgpu_advection3d_dev": [P, P, P, P, P, P, P, P, I, I, I, I, P, D, P],
+            "ductgpu_max_3din_dev": [P, P, I, I, I, C.POINTER(D)],
+            "ductgpu_wallstressx_dev": [P, P, I, I, D, P],
+            "ductgpu_energy_fou_dev": [P, P, I, I, I, D, C.POINTER(D), C.POINTER(D)],
+            "ductgpu_statistics_fou_dev": [P, P, P, P, P, I, I, I, P, P, P],
+            "ductgpu_dns_create": [P, I, D, D, D, D, I, D, I, I, C.POINTER(P)],
+            "ductgpu_dns_destroy": [P],
+            "ductgpu_dns_set_fields": [P, P, P, P, P],
+            "ductgpu_dns_get_fields": [P, P, P, P, P],
+            "ductgpu_dns_field": [P, I, C.POINTER(P)],
+            "ductgpu_dns_set_graphs": [P, I],
+            "ductgpu_dns_substep": [P, I, I],
+            "ductgpu_dns_steps": [P, I, I],
+            "ductgpu_dns_statistics": [P, P, P, P, P, P, C.POINTER(I), C.POINTER(I), P],
             "ductgpu_graph_destroy": [P, I],
             "transpose_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
                                C.POINTER(C.c_size_t)],
@@ -503,6 +530,65 @@ class Context:
     def launch_count(self):
         return int(lib().ductgpu_launch_count(self.h))
 
+    # ---- DNS operators on device fields (DeviceArray or int addresses) ----
+    def derivx_dev(self, u, du, xalp, ider, scal=1.0, what="n"):
+        my, mz, nm = u.shape
+        self._check(lib().ductgpu_derivx_dev(self.h, _dp(u), _dp(du), my, mz, nm, _ptr(np.ascontiguousarray(
+            xalp, dtype=np.float64)), int(ider), float(scal), what.encode()))
+
+    def laplacian3d_dev(self, u, flap, xalp, scal, what="n", aspect=1.0):
+        my, mz, nm = u.shape
+        self._check(lib().ductgpu_laplacian3d_dev(self.h, _dp(u), _dp(flap), my, mz, nm, _ptr(np.ascontiguousarray(
+            xalp, dtype=np.float64)), float(aspect), float(scal), what.encode()))
+
+    def grad3d_dev(self, u, dxu, dyu, dzu, xalp, scal, what="n", aspect=1.0):
+        my, mz, nm = u.shape
+        self._check(lib().ductgpu_grad3d_dev(self.h, _dp(u), _dp(dxu), _dp(dyu), _dp(dzu), my, mz, nm,
+                                             _ptr(np.ascontiguousarray(xalp, dtype=np.float64)), float(aspect),
+                                             float(scal), what.encode()))
+
+    def div3d_dev(self, u, v, w, div, xalp, scal, aspect=1.0):
+        my, mz, nm = u.shape
+        self._check(lib().ductgpu_div3d_dev(self.h, _dp(u), _dp(v), _dp(w), _dp(div), my, mz, nm,
+                                            _ptr(np.ascontiguousarray(xalp, dtype=np.float64)), float(aspect),
+                                            float(scal)))
+
+    def update_uvwp_dev(self, u, v, w, p, phi, xalp, akk, bkk, dt, fnu, aspect=1.0):
+        my, mz, nm = u.shape
+        self._check(lib().ductgpu_update_uvwp_dev(self.h, _dp(u), _dp(v), _dp(w), _dp(p), _dp(phi), my, mz, nm,
+                                                  _ptr(np.ascontiguousarray(xalp, dtype=np.float64)),
+                                                  float(aspect), float(akk), float(bkk), float(dt), float(fnu)))
+
+    def advection3d_dev(self, u, v, w, adv1, adv2, adv3, work, mgalx, xalp, aspect=1.0, stats2=None):
+        my, mz, nm = u.shape
+        self._check(lib().ductgpu_advection3d_dev(self.h, _dp(u), _dp(v), _dp(w), _dp(adv1), _dp(adv2), _dp(adv3),
+                                                  _dp(work), my, mz, nm, int(mgalx),
+                                                  _ptr(np.ascontiguousarray(xalp, dtype=np.float64)),
+                                                  float(aspect), None if stats2 is None else _dp(stats2)))
+
+    def max_3din_dev(self, u):
+        my, mz, nm = u.shape
+        out = C.c_double()
+        self._check(lib().ductgpu_max_3din_dev(self.h, _dp(u), my, mz, nm, C.byref(out)))
+        return out.value
+
+    def wallstressx_dev(self, u, aspect=1.0):
+        my, mz = u.shape[:2]
+        out = np.zeros(4)
+        self._check(lib().ductgpu_wallstressx_dev(self.h, _dp(u), my, mz, float(aspect), _ptr(out)))
+        return out
+
+    def energy_fou_dev(self, u, aspect=1.0):
+        my, mz, nm = u.shape
+        e, e2 = C.c_double(), C.c_double()
+        self._check(lib().ductgpu_energy_fou_dev(self.h, _dp(u), my, mz, nm, float(aspect), C.byref(e), C.byref(e2)))
+        return e.value, e2.value
+
+    def statistics_fou_dev(self, u, v, w, p, mean, ppb, spec):
+        my, mz, nm = u.shape
+        self._check(lib().ductgpu_statistics_fou_dev(self.h, _dp(u), _dp(v), _dp(w), _dp(p), my, mz, nm,
+                                                     _dp(mean), _dp(ppb), _dp(spec)))
+
     def profile(self, on=True):
         self._check(lib().ductgpu_profile_enable(self.h, int(bool(on))))
 
@@ -515,5 +601,78 @@ class Context:
         return ms.value, n.value
 
 
-__all__ = ["Context", "DeviceArray", "DuctGPUError", "lib", "LIB_PATH", "EXPORTS",
+def _dp(a):
+    """Device pointer of a DeviceArray (or an int address)."""
+    return C.c_void_p(a.ptr if isinstance(a, DeviceArray) else int(a))
+
+
+class Dns:
+    """Device-resident RK3/CN DNS of a square duct (ductgpu_dns_*): the
+    substep of src/main1.f90:384-723 with the context's solver.  Fields are
+    x-cut complex (my, my, M) with M = mgalx/3 modes (the 2/3 rule)."""
+
+    def __init__(self, ctx, mgalx, alp, fnu, dt, aspect=1.0, cmassflow=True, dpdx=0.0,
+                 precision=PREC_FP64, hist_cap=256):
+        self.ctx = ctx
+        h = C.c_void_p()
+        ctx._check(lib().ductgpu_dns_create(ctx.h, int(mgalx), float(alp), float(fnu), float(dt), float(aspect),
+                                            int(bool(cmassflow)), float(dpdx), int(precision), int(hist_cap),
+                                            C.byref(h)))
+        self.h = h
+        self.my = ctx._my
+        self.M = (2 * (int(mgalx) // 3)) // 2
+        self.hist_cap = int(hist_cap)
+
+    def close(self):
+        if self.h:
+            lib().ductgpu_dns_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_fields(self, u, v, w, p):
+        arrs = [np.asfortranarray(f, dtype=np.complex128) for f in (u, v, w, p)]
+        self.ctx._check(lib().ductgpu_dns_set_fields(self.h, *[_ptr(a) for a in arrs]))
+
+    def fields(self):
+        out = [np.empty((self.my, self.my, self.M), dtype=np.complex128, order="F") for _ in range(4)]
+        self.ctx._check(lib().ductgpu_dns_get_fields(self.h, *[_ptr(a) for a in out]))
+        return out
+
+    def field_ptr(self, which):
+        p = C.c_void_p()
+        self.ctx._check(lib().ductgpu_dns_field(self.h, int(which), C.byref(p)))
+        return p.value
+
+    def set_graphs(self, on):
+        self.ctx._check(lib().ductgpu_dns_set_graphs(self.h, int(bool(on))))
+
+    def substep(self, krk, stats=False):
+        self.ctx._check(lib().ductgpu_dns_substep(self.h, int(krk), int(bool(stats))))
+
+    def steps(self, n, stats_every=0):
+        self.ctx._check(lib().ductgpu_dns_steps(self.h, int(n), int(stats_every)))
+
+    def statistics(self):
+        """dict(nstat, mean (4,my,my), prod (6,my,my), ppb (my,my), spec
+        (4,7,M), hist (nhist,10), divmax (3,)) -- the oracle's layout."""
+        my, M = self.my, self.M
+        mean = np.zeros((my, my, 4), order="F")
+        prod = np.zeros((my, my, 6), order="F")
+        ppb = np.zeros((my, my), order="F")
+        spec = np.zeros((M, 7, 4), order="F")
+        hist = np.zeros((max(self.hist_cap, 1), 10))
+        ns, nh = C.c_int(), C.c_int()
+        dv = np.zeros(3)
+        self.ctx._check(lib().ductgpu_dns_statistics(self.h, _ptr(mean), _ptr(prod), _ptr(ppb), _ptr(spec),
+                                                     _ptr(hist), C.byref(ns), C.byref(nh), _ptr(dv)))
+        return dict(nstat=ns.value, mean=np.moveaxis(mean, 2, 0).copy(), prod=np.moveaxis(prod, 2, 0).copy(),
+                    ppb=ppb, spec=np.transpose(spec, (2, 1, 0)).copy(), hist=hist[:nh.value].copy(), divmax=dv)
+
+
+__all__ = ["Context", "Dns", "DeviceArray", "DuctGPUError", "lib", "LIB_PATH", "EXPORTS",
            "PREC_FP64", "PREC_MIXED", "GAUGE_POINT", "GAUGE_MEAN"]

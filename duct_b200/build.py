@@ -28,7 +28,8 @@ def sources():
 
 
 def _headers():
-    return glob.glob(os.path.join(SRC, "*.h")) + glob.glob(os.path.join(HERE, "..", "include", "*.h"))
+    return (glob.glob(os.path.join(SRC, "*.h")) + glob.glob(os.path.join(SRC, "*.cuh"))
+            + glob.glob(os.path.join(HERE, "..", "include", "*.h")))
 
 
 def _obj(src):

@@ -218,6 +218,7 @@ int ductgpu_destroy(ductgpu_ctx ctx)
     }
     for (int i = 0; i < ductgpu_ctx_s::kTwTables; ++i) cudaFree(ctx->tw_tab[i]);
     cudaFree(ctx->dev_err);
+    free_dns_aux(ctx);
     cudaFree(ctx->lam);
     cudaFreeHost(ctx->lam_host);
     for (int i = 0; i < kNumEvents; ++i) cudaEventDestroy(ctx->ev[i]);

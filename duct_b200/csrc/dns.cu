@@ -1,0 +1,1392 @@
+// dns.cu -- the DNS time step around the 2D solve (FP64): the x-direction
+// Fourier products of the advection term with 2/3 de-aliasing, the
+// operators of the fractional-step RK3/Crank-Nicolson substep, the
+// statistics and wall diagnostics, and a device-resident stepper whose
+// substeps are captured as CUDA graphs.
+//
+// Reference: advection3d (src/operators.F:9-276) with fourx / pack_fftw /
+// fill (src/fourier.F:1-118), mult (src/mult.F:11-45) and the pencil
+// transposes chx2z / chz2x (src/parallel.F:1-208); laplacian3d, grad3d,
+// div3d, update_uvwp (src/operators.F:278-605); wallstressx
+// (src/operators.F:676-710 -> src/chebyshev.f90:642-690), energy_fou
+// (src/operators.F:907-973), statistics_fou / statistics_fou2
+// (src/operators.F:1608-1765, 1957-2004), max_3din (src/operators.F:
+// 2524-2550); the substep of src/main1.f90:384-723 (no temperature,
+// DT_FIXED, icase 1 or CMASSFLOW).
+//
+// Layout: every field is x-cut complex (my, mz, nmodes), y fastest -- the
+// reference's u(my,mz,ib:ie).  The reference's x transform works on z-cut
+// pencils after chx2z; here the products are formed point by point straight
+// from the x-cut layout (the modes of a point are a stride-(my mz) gather
+// that is coalesced across consecutive points), so neither pencil
+// transpose exists.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <initializer_list>
+#include <new>
+#include <vector>
+
+#include "fft.cuh"
+#include "internal.h"
+
+namespace duct {
+
+static const double kPi = 3.14159265358979323846;
+
+// ---------------------------------------------------------------------------
+// Advection products.  Per (y, z) point the three velocity spectra (modes
+// 0..M-1, the rest of the mgalx-point spectrum zero: fill) go to physical
+// space along x, the six products uu, vv, ww, uv, uw, vw are formed there
+// and transformed back, modes 0..M-1 kept and scaled by 1/mgalx
+// (pack_fftw).  Two real signals share one complex FFT: u + i v (inverse),
+// w alone, and the products in pairs (uu + i vv, ww + i uv, uw + i vw),
+// separated as A_k = (X_k + conj X_{N-k})/2, B_k = -i (X_k - conj X_{N-k})/2.
+// The FFT is four-step with N = R^2: a thread per column holds R points
+// in registers; after the inverse its registers hold the physical values
+// at x = c + R k2, which are exactly the column-c inputs of the forward
+// transform, so the products never leave registers.
+// Outputs: adv1 = i kx UU, adv2 = i kx UV, adv3 = i kx UW (derivx of the
+// diagonal products, src/operators.F advection3d steps (1), (4), (5)) and
+// the five spectra uv, uw, vv, vw, ww that the y / z derivatives need.
+struct AdvParams {
+    const double2 *u, *v, *w;
+    double2 *adv1, *adv2, *adv3;
+    double2 *uv, *uw, *vv, *vw, *ww;
+    double *stats2;        // [6][P] x-means of uu, vv, ww, uv, uw, vw (added), or null
+    const double *xalp;    // device [M]
+    long long P;           // points of a plane (my mz)
+    int M;                 // Fourier modes kept (mx1 + 1)
+};
+
+// Step 2 of a four-step FFT over the CTA's points: thread (c, g) reads row
+// c of point g from wk and returns X[c + R k2] in v.
+template <int R, int TQ>
+__device__ __forceinline__ void fft_step2(const double2 *wk, double2 (&v)[R], const double2 *tw, int c, int g)
+{
+#pragma unroll
+    for (int n2 = 0; n2 < R; ++n2) v[n2] = wk[(c * R + n2) * TQ + g];
+    reg_fft<R, 0, 1>(v, tw, R * R);
+}
+
+// Step 1: the R-point DFT of column c (already in v), twiddle W_N^(c k1),
+// into wk for step 2.
+template <int R, int TQ>
+__device__ __forceinline__ void fft_step1(double2 (&v)[R], double2 *wk, const double2 *tw, int c, int g)
+{
+    reg_fft<R, 0, 1>(v, tw, R * R);
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) wk[(k1 * R + c) * TQ + g] = (k1 == 0) ? v[0] : cmul(v[k1], tw[c * k1]);
+}
+
+template <int R, int TQ>
+__global__ void __launch_bounds__(R * TQ) k_advx(const __grid_constant__ AdvParams p, const double2 *__restrict__ twg)
+{
+    constexpr int N = R * R, NT = R * TQ;
+    extern __shared__ __align__(16) double2 sm[];
+    double2 *tw = sm;                // W_N^t
+    double2 *wk = tw + N;            // [R][R][TQ] step buffer
+    double2 *xs = wk + N * TQ;       // [N][TQ] spectrum of a product pair
+    const int c = threadIdx.x / TQ, g = threadIdx.x - c * TQ;
+    const long long q0 = (long long)blockIdx.x * TQ;
+    const long long q = q0 + g;
+    const bool valid = q < p.P;
+    const int M = p.M;
+    const long long P = p.P;
+    for (int t = threadIdx.x; t < N; t += NT) cp_async16(tw + t, twg + t);
+    cp_async_wait_all();
+    __syncthreads();
+
+    // spectrum of mode k = R n1 + c of the Hermitian extension, conjugated
+    // (the inverse transform is conj(DFT(conj Z)))
+    double2 a[R];
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) {
+        const int k = R * n1 + c;
+        double2 z = make_double2(0.0, 0.0);
+        if (valid && k < M) {
+            const double2 uk = p.u[q + (long long)k * P], vk = p.v[q + (long long)k * P];
+            // Z = U + i V; mode 0: imaginary parts ignored
+            z = (k == 0) ? make_double2(uk.x, -vk.x) : make_double2(uk.x - vk.y, -(uk.y + vk.x));
+        } else if (valid && k > N - M) {
+            const long long kk = N - k;
+            const double2 uk = p.u[q + kk * P], vk = p.v[q + kk * P];
+            // Z_{N-k} = conj U_k + i conj V_k
+            z = make_double2(uk.x + vk.y, -(vk.x - uk.y));
+        }
+        a[n1] = z;
+    }
+    fft_step1<R, TQ>(a, wk, tw, c, g);
+    __syncthreads();
+    fft_step2<R, TQ>(wk, a, tw, c, g);
+    double uu[R], vv[R], ww[R];    // physical values at x = c + R k2
+#pragma unroll
+    for (int k2 = 0; k2 < R; ++k2) {
+        uu[k2] = a[k2].x;
+        vv[k2] = -a[k2].y;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int n1 = 0; n1 < R; ++n1) {
+        const int k = R * n1 + c;
+        double2 z = make_double2(0.0, 0.0);
+        if (valid && k < M) {
+            const double2 wk0 = p.w[q + (long long)k * P];
+            z = (k == 0) ? make_double2(wk0.x, 0.0) : make_double2(wk0.x, -wk0.y);
+        } else if (valid && k > N - M) {
+            const double2 wk0 = p.w[q + (long long)(N - k) * P];
+            z = make_double2(wk0.x, wk0.y);
+        }
+        a[n1] = z;
+    }
+    fft_step1<R, TQ>(a, wk, tw, c, g);
+    __syncthreads();
+    fft_step2<R, TQ>(wk, a, tw, c, g);
+#pragma unroll
+    for (int k2 = 0; k2 < R; ++k2) ww[k2] = a[k2].x;
+
+    const double sc = 1.0 / N;
+    for (int pair = 0; pair < 3; ++pair) {
+        // products at x = R k2 + c (forward input n = R n1 + n2, n2 = c, n1 = k2)
+#pragma unroll
+        for (int k2 = 0; k2 < R; ++k2) {
+            const double x = uu[k2], y = vv[k2], z = ww[k2];
+            a[k2] = (pair == 0) ? make_double2(x * x, y * y)
+                  : (pair == 1) ? make_double2(z * z, x * y)
+                                : make_double2(x * z, y * z);
+        }
+        __syncthreads();   // wk free (previous step 2 / separation done)
+        fft_step1<R, TQ>(a, wk, tw, c, g);
+        __syncthreads();
+        fft_step2<R, TQ>(wk, a, tw, c, g);
+#pragma unroll
+        for (int k2 = 0; k2 < R; ++k2) xs[(c + R * k2) * TQ + g] = a[k2];
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < M * TQ; idx += NT) {
+            const int i = idx / TQ, gg = idx - i * TQ;
+            const long long qq = q0 + gg;
+            if (qq >= P) continue;
+            const double2 X = xs[i * TQ + gg], Y = xs[(i == 0 ? 0 : N - i) * TQ + gg];
+            // A = (X + conj Y)/2, B = -i (X - conj Y)/2, both scaled by 1/N
+            const double2 A = make_double2(0.5 * sc * (X.x + Y.x), 0.5 * sc * (X.y - Y.y));
+            const double2 B = make_double2(0.5 * sc * (X.y + Y.y), -0.5 * sc * (X.x - Y.x));
+            const double kx = p.xalp[i];
+            const long long e = qq + (long long)i * P;
+            const double2 iA = make_double2(-kx * A.y, kx * A.x);
+            if (pair == 0) {            // A = uu, B = vv
+                p.adv1[e] = iA;
+                p.vv[e] = B;
+            } else if (pair == 1) {     // A = ww, B = uv
+                p.ww[e] = A;
+                p.uv[e] = B;
+                p.adv2[e] = make_double2(-kx * B.y, kx * B.x);
+            } else {                    // A = uw, B = vw
+                p.uw[e] = A;
+                p.adv3[e] = iA;
+                p.vw[e] = B;
+            }
+            if (p.stats2 && i == 0) {
+                // statistics_fou2: x-means (mode 0, real part) in the order uu, vv, ww, uv, uw, vw
+                const int sa = (pair == 0) ? 0 : (pair == 1) ? 2 : 4;
+                const int sb = (pair == 0) ? 1 : (pair == 1) ? 3 : 5;
+                p.stats2[sa * P + qq] += A.x;
+                p.stats2[sb * P + qq] += B.x;
+            }
+        }
+    }
+}
+
+template <int R, int TQ>
+static int launch_advx(ductgpu_ctx ctx, const AdvParams &p)
+{
+    constexpr int N = R * R, NT = R * TQ;
+    const double2 *tw = twiddle_table(ctx, N);
+    if (!tw) return set_error(ctx, DUCTGPU_ESTATE, "advection3d: twiddle table for mgalx=%d unavailable", N);
+    const size_t smem = ((size_t)N + 2 * (size_t)N * TQ) * sizeof(double2);
+    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_advx<R, TQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long long grid = (p.P + TQ - 1) / TQ;
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_ADVECTION);
+        k_advx<R, TQ><<<(unsigned)grid, NT, smem, ctx->stream>>>(p, tw);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "k_advx");
+}
+
+static bool advx_supported(int mgalx) { return mgalx == 16 || mgalx == 64 || mgalx == 256 || mgalx == 144; }
+
+static int advx_launch(ductgpu_ctx ctx, const AdvParams &p, int mgalx)
+{
+    switch (mgalx) {
+    case 16: return launch_advx<4, 32>(ctx, p);
+    case 64: return launch_advx<8, 16>(ctx, p);
+    case 144: return launch_advx<12, 8>(ctx, p);
+    case 256: return launch_advx<16, 8>(ctx, p);
+    default: return set_error(ctx, DUCTGPU_EARG, "advection3d: mgalx=%d (16, 64, 144 or 256)", mgalx);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Statistics.  One pass over u, v, w, p per recorded step: per point the
+// energies of energy_fou (sum over modes i >= 1 of 2 |f_i|^2, and |f_0|^2,
+// weighted by the mesh sizes dy dz), the mode-0 means and the x-mean of
+// p^2 (statistics_fou), and the wall stress of wallstressx as a dot product
+// of the mode-0 plane of u with four precomputed physical-space weight
+// planes (the reference's 2D DCT of that plane followed by the weighted
+// coefficient sums of cheb2_wallstress_circum is one linear functional per
+// wall).  Per-CTA partial sums are combined in a fixed order by a finishing
+// kernel, so the result does not depend on scheduling.
+constexpr int kStatVals = 10;    // stress4[4], energy e (u, v, w) sums, energy e0 (mode 0) sums
+constexpr int kStatThreads = 256;
+constexpr int kStatBlocksMax = 296;
+
+__device__ __forceinline__ double block_sum(double v, double *red)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x < 32) {
+        s = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    }
+    return s;   // valid in thread 0
+}
+
+struct StatParams {
+    const double2 *f[4];     // u, v, w, p (p may be null: energies / stress only)
+    const double *wcc;       // [P] dy dz
+    const double *wst;       // [4][P] wall-stress weights, or null
+    double *mean;            // [4][P] added, or null
+    double *ppb;             // [P] added, or null
+    double *partial;         // [gridDim][kStatVals]
+    long long P;
+    int M;
+    int nf;                  // fields with energies (1..3)
+};
+
+__global__ void __launch_bounds__(kStatThreads) k_stats(const __grid_constant__ StatParams p)
+{
+    __shared__ double red[32];
+    double acc[kStatVals];
+#pragma unroll
+    for (int k = 0; k < kStatVals; ++k) acc[k] = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < p.P; q += (long long)gridDim.x * blockDim.x) {
+        const double wq = p.wcc[q];
+        for (int c = 0; c < p.nf; ++c) {
+            const double2 *f = p.f[c];
+            double e = 0.0;
+            for (int i = 1; i < p.M; ++i) {
+                const double2 z = f[q + (long long)i * p.P];
+                e = e + (z.x * z.x + z.y * z.y) * 2.0;
+            }
+            const double2 z0 = f[q];
+            acc[4 + c] += e * wq;
+            acc[7 + c] += (z0.x * z0.x + z0.y * z0.y) * wq;
+            if (p.mean) p.mean[c * p.P + q] += z0.x;
+        }
+        if (p.wst) {
+            const double u0 = p.f[0][q].x;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) acc[s] += p.wst[s * p.P + q] * u0;
+        }
+        if (p.f[3]) {
+            const double2 *f = p.f[3];
+            double e = 0.0;
+            for (int i = 1; i < p.M; ++i) {
+                const double2 z = f[q + (long long)i * p.P];
+                e = e + (z.x * z.x + z.y * z.y) * 2.0;
+            }
+            const double2 z0 = f[q];
+            if (p.mean) p.mean[3 * p.P + q] += z0.x;
+            if (p.ppb) p.ppb[q] += e + (z0.x * z0.x + z0.y * z0.y);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kStatVals; ++k) {
+        const double s = block_sum(acc[k], red);
+        if (threadIdx.x == 0) p.partial[blockIdx.x * kStatVals + k] = s;
+    }
+}
+
+// out[0..3] = stress4, out[4..6] = energy (u, v, w), out[7..9] = energy2
+// (energy_fou: sqrt(e / area), sqrt((e + e0) / area)).  With a counter, the
+// values go to out + 10 * (*counter) (a history row) and the counter
+// advances; rows beyond cap are counted but not written.
+__global__ void k_stats_finish(const double *partial, int nblocks, double area, double *out, int *counter, int cap)
+{
+    __shared__ double e[kStatVals];
+    const int k = threadIdx.x;
+    if (k < kStatVals) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; ++b) s += partial[b * kStatVals + k];
+        e[k] = s;
+    }
+    __syncthreads();
+    int row = 0;
+    if (counter) {
+        row = *counter;
+        if (row >= cap) row = -1;
+    }
+    __syncthreads();
+    if (row >= 0) {
+        double *o = out + (size_t)kStatVals * row;
+        if (k < 4) o[k] = e[k];
+        else if (k < 7) {
+            o[k] = sqrt(e[k] / area);
+            o[k + 3] = sqrt((e[k] + e[k + 3]) / area);
+        }
+    }
+    if (counter && k == 0) *counter += 1;
+}
+
+// statistics_fou's streamwise spectra at seven points: spec[c][s][i] +=
+// |f_c(i, q_s)|^2 (times 2 for i >= 1).
+__global__ void k_spectra(const double2 *u, const double2 *v, const double2 *w, const double2 *p, long long P, int M,
+                          int my, int mz, double *spec)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * 7 * M) return;
+    const int i = t % M, s = (t / M) % 7, c = t / (7 * M);
+    const int jin[7] = {my / 16, my / 8, my / 4, my / 2, my / 16, my / 8, my / 4};
+    const int kin[7] = {mz / 2, mz / 2, mz / 2, mz / 2, mz / 16, mz / 8, mz / 4};
+    if (jin[s] < 1 || kin[s] < 1) return;   // grids below 16 points: no such point
+    const long long q = (long long)(jin[s] - 1) + (long long)my * (kin[s] - 1);
+    const double2 *f = (c == 0) ? u : (c == 1) ? v : (c == 2) ? w : p;
+    const double2 z = f[q + (long long)i * P];
+    const double a = z.x * z.x + z.y * z.y;
+    spec[((size_t)c * 7 + s) * M + i] += (i == 0) ? a : a * 2.0;
+}
+
+// Host: the weights.  Nodes x_j = -s cos(pi j / (n - 1)); mesh sizes of
+// src/ininewc.f90:102-112 (half the distance between the neighbours).
+static void mesh_sizes(int n, double s, std::vector<double> &d)
+{
+    std::vector<double> x(n);
+    for (int j = 0; j < n; ++j) x[j] = -s * cos(kPi * (double)j / (double)(n - 1));
+    d.assign(n, 0.0);
+    d[0] = (x[1] - x[0]) * 0.5;
+    for (int j = 1; j < n - 1; ++j) d[j] = (x[j + 1] - x[j - 1]) * 0.5;
+    d[n - 1] = (x[n - 1] - x[n - 2]) * 0.5;
+}
+
+// Forward transyz matrix C (n x n, c = C x): C[j][y] = sc_j w_y cos(pi j y / N)
+// with N = n - 1, sc_j = 2/N (1/N at j = 0, N), w_y = 1/2 at y = 0, N.
+static void dct_matrix(int n, std::vector<double> &C)
+{
+    const int N = n - 1;
+    C.assign((size_t)n * n, 0.0);
+    for (int j = 0; j < n; ++j) {
+        const double sc = (j == 0 || j == N) ? 1.0 / N : 2.0 / N;
+        for (int y = 0; y < n; ++y) {
+            const double w = (y == 0 || y == N) ? 0.5 : 1.0;
+            // cos(pi j y / N) with the argument reduced exactly (j y mod 2N)
+            const long r = ((long)j * y) % (2L * N);
+            C[(size_t)j * n + y] = sc * w * cos(kPi * (double)r / (double)N);
+        }
+    }
+}
+
+// Physical-space weight planes of wallstressx: stress_w = sum_q W_w[q] u0[q]
+// with W_w = Cy^T Wc_w Cz and Wc_w the coefficient weights of
+// cheb2_wallstress_circum (src/chebyshev.f90:642-690), divided by the
+// circumference 4 + 4 aspect.
+static void wallstress_weights(int my, int mz, double aspect, std::vector<double> &W)
+{
+    std::vector<double> Cy, Cz;
+    dct_matrix(my, Cy);
+    dct_matrix(mz, Cz);
+    std::vector<double> Wc((size_t)4 * my * mz, 0.0);
+    auto wc = [&](int s, int j, int k) -> double & { return Wc[((size_t)s * mz + k) * my + j]; };
+    const double circ = 4.0 + 4.0 * aspect;
+    for (int k = 0; k < mz; k += 2)
+        for (int j = 0; j < my; ++j) {
+            const double f = 2.0 * aspect * (double)j * j / (double)(k * k - 1);
+            wc(0, j, k) = -f / circ;
+            wc(1, j, k) = ((j & 1) ? 1.0 : -1.0) * f / circ;
+        }
+    for (int k = 0; k < mz; ++k)
+        for (int j = 0; j < my; j += 2) {
+            const double f = 2.0 / aspect * (double)k * k / (double)(j * j - 1);
+            wc(2, j, k) = -f / circ;
+            wc(3, j, k) = ((k & 1) ? 1.0 : -1.0) * f / circ;
+        }
+    W.assign((size_t)4 * my * mz, 0.0);
+    std::vector<double> T((size_t)my * mz);
+    for (int s = 0; s < 4; ++s) {
+        // T[j][z] = sum_k Wc[j][k] Cz[k][z]
+        for (int z = 0; z < mz; ++z)
+            for (int j = 0; j < my; ++j) {
+                double a = 0.0;
+                for (int k = 0; k < mz; ++k) a += wc(s, j, k) * Cz[(size_t)k * mz + z];
+                T[(size_t)z * my + j] = a;
+            }
+        // W[y][z] = sum_j Cy[j][y] T[j][z]
+        for (int z = 0; z < mz; ++z)
+            for (int y = 0; y < my; ++y) {
+                double a = 0.0;
+                for (int j = 0; j < my; ++j) a += Cy[(size_t)j * my + y] * T[(size_t)z * my + j];
+                W[((size_t)s * mz + z) * my + y] = a;
+            }
+    }
+}
+
+// max |u| over the interior points of all modes (max_3din); the per-CTA
+// maxima go through an atomic max on the bit pattern (|u| >= 0).
+__global__ void k_maxabs(const double2 *u, int my, int mz, int M, double *out)
+{
+    const long long total = (long long)(my - 2) * (mz - 2) * M;
+    double vmax = 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long j = 1 + t % (my - 2), r = t / (my - 2);
+        const long long k = 1 + r % (mz - 2), i = r / (mz - 2);
+        const double2 z = u[j + (long long)my * (k + (long long)mz * i)];
+        vmax = fmax(vmax, hypot(z.x, z.y));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+    if ((threadIdx.x & 31) == 0 && vmax > 0.0)
+        atomicMax(reinterpret_cast<unsigned long long *>(out), (unsigned long long)__double_as_longlong(vmax));
+}
+
+// ---------------------------------------------------------------------------
+// Buffers of the operator entries, owned by the context.
+struct DnsAux {
+    double *xalp = nullptr;
+    int xalp_cap = 0;
+    int w_my = 0, w_mz = 0;
+    double w_aspect = -1.0;
+    double *wcc = nullptr, *wst = nullptr;   // [P] dy dz, [4][P] wall-stress weights
+    double *partial = nullptr;               // [kStatBlocksMax][kStatVals]
+    double *out = nullptr;                   // [kStatVals + 1]: statistics, then max |u|
+};
+
+void free_dns_aux(ductgpu_ctx ctx)
+{
+    DnsAux *a = ctx->dns_aux;
+    if (!a) return;
+    cudaFree(a->xalp);
+    cudaFree(a->wcc);
+    cudaFree(a->wst);
+    cudaFree(a->partial);
+    cudaFree(a->out);
+    delete a;
+    ctx->dns_aux = nullptr;
+}
+
+static int aux_get(ductgpu_ctx ctx, DnsAux **out)
+{
+    if (!ctx->dns_aux) {
+        DnsAux *a = new (std::nothrow) DnsAux();
+        if (!a) return set_error(ctx, DUCTGPU_EALLOC, "dns: out of host memory");
+        if (cudaMalloc(&a->partial, sizeof(double) * kStatBlocksMax * kStatVals) != cudaSuccess ||
+            cudaMalloc(&a->out, sizeof(double) * (kStatVals + 1)) != cudaSuccess) {
+            cudaFree(a->partial);
+            delete a;
+            cudaGetLastError();
+            return set_error(ctx, DUCTGPU_EALLOC, "dns: device buffers");
+        }
+        ctx->dns_aux = a;
+    }
+    *out = ctx->dns_aux;
+    return DUCTGPU_OK;
+}
+
+// The wavenumbers to the device (stream-ordered after earlier launches).
+static int upload_xalp(ductgpu_ctx ctx, const double *xalp, int nmodes, const double **dev)
+{
+    DnsAux *a;
+    int rc = aux_get(ctx, &a);
+    if (rc) return rc;
+    if (!xalp) return set_error(ctx, DUCTGPU_EARG, "xalp is null");
+    if (nmodes > a->xalp_cap) {
+        DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        cudaFree(a->xalp);
+        a->xalp = nullptr;
+        a->xalp_cap = 0;
+        DUCT_CUDA(ctx, cudaMalloc(&a->xalp, sizeof(double) * nmodes));
+        a->xalp_cap = nmodes;
+    }
+    DUCT_CUDA(ctx, cudaMemcpyAsync(a->xalp, xalp, sizeof(double) * nmodes, cudaMemcpyHostToDevice, ctx->stream));
+    *dev = a->xalp;
+    return DUCTGPU_OK;
+}
+
+// Energy (mesh-size) and wall-stress weights on the device, for (my, mz, aspect).
+static int make_weights(int my, int mz, double aspect, std::vector<double> &wcc, std::vector<double> &wst)
+{
+    std::vector<double> dy, dz;
+    mesh_sizes(my, 1.0, dy);
+    mesh_sizes(mz, aspect, dz);
+    wcc.resize((size_t)my * mz);
+    for (int k = 0; k < mz; ++k)
+        for (int j = 0; j < my; ++j) wcc[(size_t)k * my + j] = dy[j] * dz[k];
+    wallstress_weights(my, mz, aspect, wst);
+    return 0;
+}
+
+static int aux_weights(ductgpu_ctx ctx, int my, int mz, double aspect, DnsAux **out)
+{
+    DnsAux *a;
+    int rc = aux_get(ctx, &a);
+    if (rc) return rc;
+    if (a->w_my != my || a->w_mz != mz || a->w_aspect != aspect) {
+        std::vector<double> wcc, wst;
+        make_weights(my, mz, aspect, wcc, wst);
+        DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        cudaFree(a->wcc);
+        cudaFree(a->wst);
+        a->wcc = a->wst = nullptr;
+        a->w_my = 0;
+        DUCT_CUDA(ctx, cudaMalloc(&a->wcc, sizeof(double) * wcc.size()));
+        DUCT_CUDA(ctx, cudaMalloc(&a->wst, sizeof(double) * wst.size()));
+        DUCT_CUDA(ctx, cudaMemcpy(a->wcc, wcc.data(), sizeof(double) * wcc.size(), cudaMemcpyHostToDevice));
+        DUCT_CUDA(ctx, cudaMemcpy(a->wst, wst.data(), sizeof(double) * wst.size(), cudaMemcpyHostToDevice));
+        a->w_my = my;
+        a->w_mz = mz;
+        a->w_aspect = aspect;
+    }
+    *out = a;
+    return DUCTGPU_OK;
+}
+
+static int check_geom(ductgpu_ctx ctx, const char *who, int my, int mz, int nmodes, bool lines)
+{
+    if (my < 3 || mz < 3 || nmodes < 1)
+        return set_error(ctx, DUCTGPU_EARG, "%s: my=%d mz=%d nmodes=%d", who, my, mz, nmodes);
+    if (lines && (!lines_supported(my) || !lines_supported(mz)))
+        return set_error(ctx, DUCTGPU_EARG, "%s: my-1=%d, mz-1=%d must be one of 16, 24, 32, 48, 64, 96, 128, 144, "
+                         "192, 256", who, my - 1, mz - 1);
+    return DUCTGPU_OK;
+}
+
+static int check_ptrs(ductgpu_ctx ctx, const char *who, std::initializer_list<const void *> ps)
+{
+    for (const void *p : ps)
+        if (!p || ((uintptr_t)p & 15))
+            return set_error(ctx, DUCTGPU_EARG, "%s: null or not 16-byte aligned field pointer", who);
+    return DUCTGPU_OK;
+}
+
+static LineOut line_out(double *out, int order, double fac, double beta, double sigma = 1.0)
+{
+    LineOut o;
+    o.out = out;
+    o.order = order;
+    o.fac = fac;
+    o.beta = beta;
+    o.sigma = sigma;
+    return o;
+}
+
+// Adds the term (c0 + c1 i kx + c2 (i kx)^2) src to an output.
+static void xterm(LineOut &o, const double *src, double c0, double c1, double c2)
+{
+    for (int t = 0; t < kLineXTerms; ++t)
+        if (!o.xs[t]) {
+            o.xs[t] = src;
+            o.xc0[t] = c0;
+            o.xc1[t] = c1;
+            o.xc2[t] = c2;
+            return;
+        }
+}
+
+static LineParams line_params(char dir, int my, int mz, int nmodes, const double *xalp_dev, int real0 = 0)
+{
+    LineParams p;
+    p.real0 = real0;
+    p.dir = dir;
+    p.my = my;
+    p.mz = mz;
+    p.nmodes = nmodes;
+    p.xalp = xalp_dev;
+    return p;
+}
+
+static void add_job(LineParams &p, const double *in, std::initializer_list<LineOut> outs)
+{
+    LineJob &J = p.job[p.njobs++];
+    J.in = in;
+    J.nout = 0;
+    for (const LineOut &o : outs) J.o[J.nout++] = o;
+}
+
+}  // namespace duct
+
+using namespace duct;
+
+// ---- the reference's operators on device fields -------------------------
+extern "C" int ductgpu_derivx_dev(ductgpu_ctx ctx, const double *u, double *du, int my, int mz, int nmodes,
+                                  const double *xalp, int ider, double scal, char what)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_geom(ctx, "derivx", my, mz, nmodes, false);
+    if (!rc) rc = check_ptrs(ctx, "derivx", {u, du});
+    if (rc) return rc;
+    if (ider != 1 && ider != 2) return set_error(ctx, DUCTGPU_EARG, "derivx: ider=%d", ider);
+    cudaSetDevice(ctx->device);
+    const double *xd;
+    if ((rc = upload_xalp(ctx, xalp, nmodes, &xd))) return rc;
+    // a line launch with an order-0 output only: du = [du +] scal (i kx)^ider u
+    LineParams p = line_params('y', my, mz, nmodes, xd);
+    LineOut o = line_out(du, 0, 0.0, what == 'n' ? 0.0 : 1.0);
+    xterm(o, u, 0.0, ider == 1 ? scal : 0.0, ider == 2 ? scal : 0.0);
+    add_job(p, u, {o});
+    if (lines_supported(my)) return lines_launch(ctx, p);
+    return set_error(ctx, DUCTGPU_EARG, "derivx: my-1=%d not a supported line length", my - 1);
+}
+
+extern "C" int ductgpu_laplacian3d_dev(ductgpu_ctx ctx, const double *u, double *flap, int my, int mz, int nmodes,
+                                       const double *xalp, double aspect, double scal, char what)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_geom(ctx, "laplacian3d", my, mz, nmodes, true);
+    if (!rc) rc = check_ptrs(ctx, "laplacian3d", {u, flap});
+    if (rc) return rc;
+    if (u == flap) return set_error(ctx, DUCTGPU_EARG, "laplacian3d: u and flap must differ");
+    cudaSetDevice(ctx->device);
+    const double *xd;
+    if ((rc = upload_xalp(ctx, xalp, nmodes, &xd))) return rc;
+    LineParams py = line_params('y', my, mz, nmodes, xd);
+    LineOut oy = line_out(flap, 2, scal, what == 'n' ? 0.0 : 1.0);
+    xterm(oy, u, 0.0, 0.0, scal);
+    add_job(py, u, {oy});
+    if ((rc = lines_launch(ctx, py))) return rc;
+    LineParams pz = line_params('z', my, mz, nmodes, xd);
+    add_job(pz, u, {line_out(flap, 2, scal / (aspect * aspect), 1.0)});
+    return lines_launch(ctx, pz);
+}
+
+extern "C" int ductgpu_grad3d_dev(ductgpu_ctx ctx, const double *u, double *dxu, double *dyu, double *dzu, int my,
+                                  int mz, int nmodes, const double *xalp, double aspect, double scal, char what)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_geom(ctx, "grad3d", my, mz, nmodes, true);
+    if (!rc) rc = check_ptrs(ctx, "grad3d", {u, dxu, dyu, dzu});
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    const double *xd;
+    if ((rc = upload_xalp(ctx, xalp, nmodes, &xd))) return rc;
+    const double beta = what == 'n' ? 0.0 : 1.0;
+    LineParams py = line_params('y', my, mz, nmodes, xd);
+    LineOut ox = line_out(dxu, 0, 0.0, beta);
+    xterm(ox, u, 0.0, scal, 0.0);
+    add_job(py, u, {line_out(dyu, 1, scal, beta), ox});
+    if ((rc = lines_launch(ctx, py))) return rc;
+    LineParams pz = line_params('z', my, mz, nmodes, xd);
+    add_job(pz, u, {line_out(dzu, 1, scal / aspect, beta)});
+    return lines_launch(ctx, pz);
+}
+
+extern "C" int ductgpu_div3d_dev(ductgpu_ctx ctx, const double *u, const double *v, const double *w, double *div,
+                                 int my, int mz, int nmodes, const double *xalp, double aspect, double scal)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_geom(ctx, "div3d", my, mz, nmodes, true);
+    if (!rc) rc = check_ptrs(ctx, "div3d", {u, v, w, div});
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    const double *xd;
+    if ((rc = upload_xalp(ctx, xalp, nmodes, &xd))) return rc;
+    LineParams py = line_params('y', my, mz, nmodes, xd);
+    LineOut o = line_out(div, 1, scal, 0.0);
+    xterm(o, u, 0.0, scal, 0.0);
+    add_job(py, v, {o});
+    if ((rc = lines_launch(ctx, py))) return rc;
+    LineParams pz = line_params('z', my, mz, nmodes, xd);
+    add_job(pz, w, {line_out(div, 1, scal / aspect, 1.0)});
+    return lines_launch(ctx, pz);
+}
+
+namespace duct {
+// update_uvwp (no FILTER): p += phi - f1 lap(phi), u += s2 i kx phi,
+// v += s2 phi_y, w += s2 phi_z, with f1 = (akk + bkk) dt nu, s2 = -dt (akk + bkk).
+static int update_lines(ductgpu_ctx ctx, double *u, double *v, double *w, double *p, const double *phi, int my, int mz,
+                        int nmodes, const double *xd, double aspect, double akk, double bkk, double dt, double fnu,
+                        int real0 = 0)
+{
+    const double f1 = (akk + bkk) * dt * fnu, s2 = -dt * (akk + bkk);
+    LineParams py = line_params('y', my, mz, nmodes, xd, real0);
+    LineOut op = line_out(p, 2, -f1, 1.0);
+    xterm(op, phi, 1.0, 0.0, -f1);
+    LineOut ou = line_out(u, 0, 0.0, 1.0);
+    xterm(ou, phi, 0.0, s2, 0.0);
+    add_job(py, phi, {op, line_out(v, 1, s2, 1.0), ou});
+    int rc = lines_launch(ctx, py);
+    if (rc) return rc;
+    LineParams pz = line_params('z', my, mz, nmodes, xd, real0);
+    add_job(pz, phi, {line_out(p, 2, -f1 / (aspect * aspect), 1.0), line_out(w, 1, s2 / aspect, 1.0)});
+    return lines_launch(ctx, pz);
+}
+}  // namespace duct
+
+extern "C" int ductgpu_update_uvwp_dev(ductgpu_ctx ctx, double *u, double *v, double *w, double *p, const double *phi,
+                                       int my, int mz, int nmodes, const double *xalp, double aspect, double akk,
+                                       double bkk, double dt, double fnu)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_geom(ctx, "update_uvwp", my, mz, nmodes, true);
+    if (!rc) rc = check_ptrs(ctx, "update_uvwp", {u, v, w, p, phi});
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    const double *xd;
+    if ((rc = upload_xalp(ctx, xalp, nmodes, &xd))) return rc;
+    return update_lines(ctx, u, v, w, p, phi, my, mz, nmodes, xd, aspect, akk, bkk, dt, fnu);
+}
+
+namespace duct {
+// advection3d on x-cut fields: the x-FFT products (k_advx) and the y / z
+// derivatives of the off-diagonal and diagonal products (two line launches).
+static int advection_issue(ductgpu_ctx ctx, const double *u, const double *v, const double *w, double *a1, double *a2,
+                           double *a3, double *const prod[5], int my, int mz, int M, int mgalx, const double *xd,
+                           double aspect, double *stats2, int real0 = 0)
+{
+    AdvParams ap{};
+    ap.u = reinterpret_cast<const double2 *>(u);
+    ap.v = reinterpret_cast<const double2 *>(v);
+    ap.w = reinterpret_cast<const double2 *>(w);
+    ap.adv1 = reinterpret_cast<double2 *>(a1);
+    ap.adv2 = reinterpret_cast<double2 *>(a2);
+    ap.adv3 = reinterpret_cast<double2 *>(a3);
+    ap.uv = reinterpret_cast<double2 *>(prod[0]);
+    ap.uw = reinterpret_cast<double2 *>(prod[1]);
+    ap.vv = reinterpret_cast<double2 *>(prod[2]);
+    ap.vw = reinterpret_cast<double2 *>(prod[3]);
+    ap.ww = reinterpret_cast<double2 *>(prod[4]);
+    ap.stats2 = stats2;
+    ap.xalp = xd;
+    ap.P = (long long)my * mz;
+    ap.M = M;
+    int rc = advx_launch(ctx, ap, mgalx);
+    if (rc) return rc;
+    // adv1 += d(uv)/dy + d(uw)/dz; adv2 += d(vv)/dy + d(vw)/dz; adv3 += d(vw)/dy + d(ww)/dz
+    LineParams py = line_params('y', my, mz, M, xd, real0);
+    add_job(py, prod[0], {line_out(a1, 1, 1.0, 1.0)});
+    add_job(py, prod[2], {line_out(a2, 1, 1.0, 1.0)});
+    add_job(py, prod[3], {line_out(a3, 1, 1.0, 1.0)});
+    if ((rc = lines_launch(ctx, py))) return rc;
+    LineParams pz = line_params('z', my, mz, M, xd, real0);
+    add_job(pz, prod[1], {line_out(a1, 1, 1.0 / aspect, 1.0)});
+    add_job(pz, prod[3], {line_out(a2, 1, 1.0 / aspect, 1.0)});
+    add_job(pz, prod[4], {line_out(a3, 1, 1.0 / aspect, 1.0)});
+    return lines_launch(ctx, pz);
+}
+
+static int mgalx_modes(int mgalx) { return (2 * (mgalx / 3)) / 2; }
+}  // namespace duct
+
+extern "C" int ductgpu_advection3d_dev(ductgpu_ctx ctx, const double *u, const double *v, const double *w,
+                                       double *adv1, double *adv2, double *adv3, double *work, int my, int mz,
+                                       int nmodes, int mgalx, const double *xalp, double aspect, double *stats2)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_geom(ctx, "advection3d", my, mz, nmodes, true);
+    if (!rc) rc = check_ptrs(ctx, "advection3d", {u, v, w, adv1, adv2, adv3, work});
+    if (rc) return rc;
+    if (!advx_supported(mgalx)) return set_error(ctx, DUCTGPU_EARG, "advection3d: mgalx=%d (16, 64, 144, 256)", mgalx);
+    if (nmodes != mgalx_modes(mgalx))
+        return set_error(ctx, DUCTGPU_EARG, "advection3d: nmodes=%d, mgalx=%d keeps %d modes (mx = 2 (mgalx/3))",
+                         nmodes, mgalx, mgalx_modes(mgalx));
+    cudaSetDevice(ctx->device);
+    const double *xd;
+    if ((rc = upload_xalp(ctx, xalp, nmodes, &xd))) return rc;
+    const size_t fd = 2ull * my * mz * nmodes;
+    double *prod[5] = {work, work + fd, work + 2 * fd, work + 3 * fd, work + 4 * fd};
+    return advection_issue(ctx, u, v, w, adv1, adv2, adv3, prod, my, mz, nmodes, mgalx, xd, aspect, stats2);
+}
+
+extern "C" int ductgpu_max_3din_dev(ductgpu_ctx ctx, const double *u, int my, int mz, int nmodes, double *divmax)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_geom(ctx, "max_3din", my, mz, nmodes, false);
+    if (!rc) rc = check_ptrs(ctx, "max_3din", {u});
+    if (rc) return rc;
+    if (!divmax) return set_error(ctx, DUCTGPU_EARG, "max_3din: null output");
+    cudaSetDevice(ctx->device);
+    DnsAux *a;
+    if ((rc = aux_get(ctx, &a))) return rc;
+    DUCT_CUDA(ctx, cudaMemsetAsync(a->out + kStatVals, 0, sizeof(double), ctx->stream));
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_STATS);
+        k_maxabs<<<2 * ctx->num_sms, 256, 0, ctx->stream>>>(reinterpret_cast<const double2 *>(u), my, mz, nmodes,
+                                                            a->out + kStatVals);
+    }
+    DUCT_CUDA(ctx, cudaGetLastError());
+    DUCT_CUDA(ctx, cudaMemcpyAsync(divmax, a->out + kStatVals, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "max_3din");
+}
+
+namespace duct {
+static int stats_issue(ductgpu_ctx ctx, const double *const f[4], int nf, const double *wcc, const double *wst,
+                       double *mean, double *ppb, double *partial, double *out, int *counter, int cap, long long P,
+                       int M, double aspect)
+{
+    StatParams sp{};
+    for (int c = 0; c < 4; ++c) sp.f[c] = reinterpret_cast<const double2 *>(f[c]);
+    sp.wcc = wcc;
+    sp.wst = wst;
+    sp.mean = mean;
+    sp.ppb = ppb;
+    sp.partial = partial;
+    sp.P = P;
+    sp.M = M;
+    sp.nf = nf;
+    int blocks = (int)((P + kStatThreads - 1) / kStatThreads);
+    if (blocks > kStatBlocksMax) blocks = kStatBlocksMax;
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_STATS);
+        k_stats<<<blocks, kStatThreads, 0, ctx->stream>>>(sp);
+    }
+    DUCT_CUDA(ctx, cudaGetLastError());
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_STATS);
+        k_stats_finish<<<1, 32, 0, ctx->stream>>>(partial, blocks, 4.0 * aspect, out, counter, cap);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "k_stats");
+}
+}  // namespace duct
+
+extern "C" int ductgpu_wallstressx_dev(ductgpu_ctx ctx, const double *u, int my, int mz, double aspect,
+                                       double *stress4)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_geom(ctx, "wallstressx", my, mz, 1, false);
+    if (!rc) rc = check_ptrs(ctx, "wallstressx", {u});
+    if (rc) return rc;
+    if (!stress4) return set_error(ctx, DUCTGPU_EARG, "wallstressx: null output");
+    cudaSetDevice(ctx->device);
+    DnsAux *a;
+    if ((rc = aux_weights(ctx, my, mz, aspect, &a))) return rc;
+    const double *f[4] = {u, nullptr, nullptr, nullptr};
+    if ((rc = stats_issue(ctx, f, 1, a->wcc, a->wst, nullptr, nullptr, a->partial, a->out, nullptr, 0,
+                          (long long)my * mz, 1, aspect)))
+        return rc;
+    DUCT_CUDA(ctx, cudaMemcpyAsync(stress4, a->out, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "wallstressx");
+}
+
+extern "C" int ductgpu_energy_fou_dev(ductgpu_ctx ctx, const double *u, int my, int mz, int nmodes, double aspect,
+                                      double *energy, double *energy2)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_geom(ctx, "energy_fou", my, mz, nmodes, false);
+    if (!rc) rc = check_ptrs(ctx, "energy_fou", {u});
+    if (rc) return rc;
+    if (!energy || !energy2) return set_error(ctx, DUCTGPU_EARG, "energy_fou: null output");
+    cudaSetDevice(ctx->device);
+    DnsAux *a;
+    if ((rc = aux_weights(ctx, my, mz, aspect, &a))) return rc;
+    const double *f[4] = {u, nullptr, nullptr, nullptr};
+    if ((rc = stats_issue(ctx, f, 1, a->wcc, nullptr, nullptr, nullptr, a->partial, a->out, nullptr, 0,
+                          (long long)my * mz, nmodes, aspect)))
+        return rc;
+    double o[kStatVals];
+    DUCT_CUDA(ctx, cudaMemcpyAsync(o, a->out, sizeof(o), cudaMemcpyDeviceToHost, ctx->stream));
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *energy = o[4];
+    *energy2 = o[7];
+    return DUCTGPU_OK;
+}
+
+extern "C" int ductgpu_statistics_fou_dev(ductgpu_ctx ctx, const double *u, const double *v, const double *w,
+                                          const double *p, int my, int mz, int nmodes, double *mean, double *ppb,
+                                          double *spec)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_geom(ctx, "statistics_fou", my, mz, nmodes, false);
+    if (!rc) rc = check_ptrs(ctx, "statistics_fou", {u, v, w, p});
+    if (rc) return rc;
+    if (!mean || !ppb || !spec) return set_error(ctx, DUCTGPU_EARG, "statistics_fou: null accumulator");
+    if (my < 16 || mz < 16)
+        return set_error(ctx, DUCTGPU_EARG, "statistics_fou: my=%d mz=%d (the spectra points need 16 or more)", my, mz);
+    cudaSetDevice(ctx->device);
+    DnsAux *a;
+    if ((rc = aux_weights(ctx, my, mz, 1.0, &a))) return rc;
+    const double *f[4] = {u, v, w, p};
+    if ((rc = stats_issue(ctx, f, 3, a->wcc, nullptr, mean, ppb, a->partial, a->out, nullptr, 0, (long long)my * mz,
+                          nmodes, 1.0)))
+        return rc;
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_STATS);
+        k_spectra<<<(4 * 7 * nmodes + 127) / 128, 128, 0, ctx->stream>>>(
+            reinterpret_cast<const double2 *>(u), reinterpret_cast<const double2 *>(v),
+            reinterpret_cast<const double2 *>(w), reinterpret_cast<const double2 *>(p), (long long)my * mz, nmodes,
+            my, mz, spec);
+    }
+    DUCT_CUDA(ctx, cudaGetLastError());
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "statistics_fou");
+}
+
+// ---------------------------------------------------------------------------
+// The RK3/CN stepper (src/main1.f90:384-723) on device-resident fields.
+namespace duct {
+// Runge-Kutta coefficients, src/mod.f90:52-55
+static const double kAkk[3] = {29.0 / 96.0, -3.0 / 40.0, 1.0 / 6.0};
+static const double kBkk[3] = {37.0 / 160.0, 5.0 / 24.0, 1.0 / 6.0};
+static const double kGkk[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+static const double kRkk[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+}  // namespace duct
+
+struct ductgpu_dns_s {
+    ductgpu_ctx ctx = nullptr;
+    int my = 0, M = 0, mgalx = 0, precision = DUCTGPU_PREC_FP64;
+    double alp = 1.0, fnu = 0.0, dt = 0.0, aspect = 1.0, dpdx = 0.0;
+    int cmassflow = 1;
+    double csum = 0.0;
+    long long P = 0;
+    size_t fdoubles = 0;         // doubles of a field
+    double *mem = nullptr;       // all fields in one allocation
+    double *vel[3] = {}, *p = nullptr;
+    double *adv[2][3] = {};      // advection terms: substep k writes adv[k % 2], reads adv[(k - 1) % 2]
+    double *h[3] = {};
+    double *prod[5] = {};        // uv, uw, vv, vw, ww
+    double *xalp = nullptr;      // device [M]
+    double *lam_d[3] = {}, *lam_n = nullptr;
+    // host copies: the Neumann fill finds the singular (kx = 0) planes on the host
+    std::vector<double> lamh_d[3], lamh_n;
+    // statistics accumulators and per-step history
+    double *st_mean = nullptr, *st_prod = nullptr, *st_ppb = nullptr, *st_spec = nullptr;
+    double *wcc = nullptr, *wst = nullptr, *partial = nullptr;
+    double *hist = nullptr;
+    int *hist_n = nullptr;
+    int hist_cap = 0;
+    int nstat = 0;
+    double *divmax = nullptr;    // [3], one per substep
+    bool use_graphs = true;
+    bool warm[3] = {};
+    cudaGraphExec_t graph[3][2] = {};
+};
+
+namespace duct {
+
+// The solves read the per-plane lambda from ctx->lam (device) and, for the
+// Neumann fill's singular planes, from ctx->lam_host: both point at the
+// stepper's own copies for the call.
+static int dns_solve(ductgpu_dns d, FieldTask *t, int n, const double *lam, std::vector<double> &lamh)
+{
+    ductgpu_ctx ctx = d->ctx;
+    double *saved = ctx->lam, *saved_h = ctx->lam_host;
+    ctx->lam = const_cast<double *>(lam);
+    ctx->lam_host = lamh.data();
+    int rc;
+    if (d->precision == DUCTGPU_PREC_MIXED) rc = solve_mixed(ctx, t, n);
+    else rc = solve_fp64_ex(ctx, t, n, d->precision == DUCTGPU_PREC_INT8);
+    ctx->lam = saved;
+    ctx->lam_host = saved_h;
+    return rc;
+}
+
+// One substep krk (1..3); stats: gather the statistics of the step (the
+// reference does so at krk = 1).
+static int dns_issue(ductgpu_dns d, int krk, bool stats)
+{
+    ductgpu_ctx ctx = d->ctx;
+    const int k = krk - 1, my = d->my, M = d->M;
+    const double a = kAkk[k], b = kBkk[k], gm = kGkk[k], rho = kRkk[k];
+    const double nu = d->fnu, dt = d->dt, asp = d->aspect;
+    double **an = d->adv[krk % 2], **ao = d->adv[(krk - 1) % 2];
+    double *u = d->vel[0], *v = d->vel[1], *w = d->vel[2], *p = d->p;
+    const double *xd = d->xalp;
+    int rc;
+    // (ii) adv(u^{k-1}); statistics_fou2 of the products with the statistics
+    if ((rc = advection_issue(ctx, u, v, w, an[0], an[1], an[2], d->prod, my, my, M, d->mgalx, xd, asp,
+                              stats ? d->st_prod : nullptr, 1)))
+        return rc;
+    if (stats) {
+        // wallstressx, energy_fou (u, v, w), statistics_fou (u, v, w, p)
+        const double *f[4] = {u, v, w, p};
+        if ((rc = stats_issue(ctx, f, 3, d->wcc, d->wst, d->st_mean, d->st_ppb, d->partial, d->hist, d->hist_n,
+                              d->hist_cap, d->P, M, asp)))
+            return rc;
+        {
+            LaunchScope ls(ctx, DUCTGPU_K_STATS);
+            k_spectra<<<(4 * 7 * M + 127) / 128, 128, 0, ctx->stream>>>(
+                reinterpret_cast<const double2 *>(u), reinterpret_cast<const double2 *>(v),
+                reinterpret_cast<const double2 *>(w), reinterpret_cast<const double2 *>(p), d->P, M, my, my,
+                d->st_spec);
+        }
+        DUCT_CUDA(ctx, cudaGetLastError());
+    }
+    // (i), (iii)-(v), the x-part of (vi), (vi-b): along y,
+    //   h = -rho adv_old - gamma adv + u/dt + a nu lap_x,y(u) [- (a+b) (i kx p + dpdx)]
+    {
+        LineParams py = line_params('y', my, my, M, xd, 1);
+        for (int c = 0; c < 3; ++c) {
+            LineOut o = line_out(d->h[c], 2, nu * a, 0.0);
+            xterm(o, d->vel[c], 1.0 / dt, 0.0, nu * a);
+            xterm(o, an[c], -gm, 0.0, 0.0);
+            if (krk > 1) xterm(o, ao[c], -rho, 0.0, 0.0);
+            if (c == 0) {
+                xterm(o, p, 0.0, -(a + b), 0.0);
+                if (!d->cmassflow) o.m0 = -(a + b) * d->dpdx;
+            }
+            add_job(py, d->vel[c], {o});
+        }
+        if ((rc = lines_launch(ctx, py))) return rc;
+    }
+    // (vi) y and z parts of -(a+b) grad p
+    {
+        LineParams py = line_params('y', my, my, M, xd, 1);
+        add_job(py, p, {line_out(d->h[1], 1, -(a + b), 1.0)});
+        if ((rc = lines_launch(ctx, py))) return rc;
+        LineParams pz = line_params('z', my, my, M, xd, 1);
+        add_job(pz, p, {line_out(d->h[2], 1, -(a + b) / asp, 1.0)});
+        if ((rc = lines_launch(ctx, pz))) return rc;
+    }
+    // (iv) z part of the laplacian, then (vii) h *= -1/(nu beta)
+    {
+        LineParams pz = line_params('z', my, my, M, xd, 1);
+        for (int c = 0; c < 3; ++c)
+            add_job(pz, d->vel[c], {line_out(d->h[c], 2, nu * a / (asp * asp), 1.0, -1.0 / (nu * b))});
+        if ((rc = lines_launch(ctx, pz))) return rc;
+    }
+    // (viii) predictor: helm3d 'd', helco = 1/(beta nu dt)
+    {
+        FieldTask t[3];
+        for (int c = 0; c < 3; ++c) {
+            t[c].rhs = d->h[c];
+            t[c].sol = d->vel[c];
+            t[c].nmodes = M;
+            t[c].mode0 = 1;
+            t[c].bound = 'd';
+            t[c].plane0 = c * M;
+            t[c].refine = 1;
+        }
+        if ((rc = dns_solve(d, t, 3, d->lam_d[k], d->lamh_d[k]))) return rc;
+    }
+    // (ix) rhs of the pseudo-pressure: div(u) / ((a+b) dt) -> h1
+    const double sdiv = 1.0 / ((a + b) * dt);
+    {
+        LineParams py = line_params('y', my, my, M, xd, 1);
+        LineOut o = line_out(d->h[0], 1, sdiv, 0.0);
+        xterm(o, u, 0.0, sdiv, 0.0);
+        add_job(py, v, {o});
+        if ((rc = lines_launch(ctx, py))) return rc;
+        LineParams pz = line_params('z', my, my, M, xd, 1);
+        add_job(pz, w, {line_out(d->h[0], 1, sdiv / asp, 1.0)});
+        if ((rc = lines_launch(ctx, pz))) return rc;
+    }
+    // (x) Poisson 'n' -> phi in h2
+    {
+        FieldTask t;
+        t.rhs = d->h[0];
+        t.sol = d->h[1];
+        t.nmodes = M;
+        t.mode0 = 1;
+        t.bound = 'n';
+        t.plane0 = 0;
+        t.refine = ctx->refine_steps;
+        if ((rc = dns_solve(d, &t, 1, d->lam_n, d->lamh_n))) return rc;
+    }
+    // (xi) update u, v, w, p
+    if ((rc = update_lines(ctx, u, v, w, p, d->h[1], my, my, M, xd, asp, a, b, dt, nu, 1))) return rc;
+    if (d->cmassflow) {
+        double cs = d->csum;
+        if ((rc = ductgpu_impose_mass_flow_dev(ctx, &cs, krk, u, 1))) return rc;
+    }
+    // divergence check: max |div u| over the interior (max_3din) -> divmax[k]
+    DUCT_CUDA(ctx, cudaMemsetAsync(d->divmax + k, 0, sizeof(double), ctx->stream));
+    {
+        LineParams py = line_params('y', my, my, M, xd, 1);
+        LineOut o = line_out(d->h[2], 1, 1.0, 0.0);
+        xterm(o, u, 0.0, 1.0, 0.0);
+        add_job(py, v, {o});
+        if ((rc = lines_launch(ctx, py))) return rc;
+        LineParams pz = line_params('z', my, my, M, xd, 1);
+        LineOut oz = line_out(d->h[2], 1, 1.0 / asp, 1.0);
+        oz.maxabs = d->divmax + k;
+        add_job(pz, w, {oz});
+        if ((rc = lines_launch(ctx, pz))) return rc;
+    }
+    return DUCTGPU_OK;
+}
+
+static void dns_free(ductgpu_dns d)
+{
+    if (!d) return;
+    if (d->ctx) {
+        cudaSetDevice(d->ctx->device);
+        cudaStreamSynchronize(d->ctx->stream);
+    }
+    for (int k = 0; k < 3; ++k)
+        for (int s = 0; s < 2; ++s)
+            if (d->graph[k][s]) cudaGraphExecDestroy(d->graph[k][s]);
+    cudaFree(d->mem);
+    cudaFree(d->xalp);
+    for (int k = 0; k < 3; ++k) cudaFree(d->lam_d[k]);
+    cudaFree(d->lam_n);
+    cudaFree(d->st_mean);
+    cudaFree(d->wcc);
+    cudaFree(d->hist);
+    cudaFree(d->hist_n);
+    delete d;
+}
+
+}  // namespace duct
+
+extern "C" int ductgpu_dns_create(ductgpu_ctx ctx, int mgalx, double alp, double fnu, double dt, double aspect,
+                                  int cmassflow, double dpdx, int precision, int hist_cap, ductgpu_dns *out)
+{
+    if (!ctx || !out) return DUCTGPU_EARG;
+    *out = nullptr;
+    if (!ctx->ready) return set_error(ctx, DUCTGPU_ESTATE, "dns: operators not set up (call ductgpu_pseudomat)");
+    const int my = ctx->my;
+    if (ctx->mz != my) return set_error(ctx, DUCTGPU_EARG, "dns: square duct only (my=%d mz=%d)", my, ctx->mz);
+    int rc = check_geom(ctx, "dns", my, my, 1, true);
+    if (rc) return rc;
+    if (!advx_supported(mgalx)) return set_error(ctx, DUCTGPU_EARG, "dns: mgalx=%d (16, 64, 144, 256)", mgalx);
+    if (!(fnu > 0.0) || !(dt > 0.0) || !(aspect > 0.0))
+        return set_error(ctx, DUCTGPU_EARG, "dns: nu=%g dt=%g aspect=%g", fnu, dt, aspect);
+    if (precision != DUCTGPU_PREC_FP64 && precision != DUCTGPU_PREC_INT8 && precision != DUCTGPU_PREC_MIXED)
+        return set_error(ctx, DUCTGPU_EARG, "dns: precision %d", precision);
+    if (precision == DUCTGPU_PREC_INT8 && my - 2 > 127)
+        return set_error(ctx, DUCTGPU_EARG, "dns: int8-emulated solve needs my <= 129 (my=%d)", my);
+    if (hist_cap < 0) hist_cap = 0;
+    cudaSetDevice(ctx->device);
+    ductgpu_dns d = new (std::nothrow) ductgpu_dns_s();
+    if (!d) return set_error(ctx, DUCTGPU_EALLOC, "dns: out of host memory");
+    d->ctx = ctx;
+    d->my = my;
+    d->mgalx = mgalx;
+    d->M = mgalx_modes(mgalx);
+    d->alp = alp;
+    d->fnu = fnu;
+    d->dt = dt;
+    d->aspect = aspect;
+    d->cmassflow = cmassflow ? 1 : 0;
+    d->dpdx = dpdx;
+    d->precision = precision;
+    d->P = (long long)my * my;
+    d->fdoubles = 2ull * d->P * d->M;
+    const int M = d->M;
+    auto fail = [&](int code) {
+        dns_free(d);
+        return code;
+    };
+    // fields: u v w p, adv 2x3, h 3, prod 5 = 18
+    if (cudaMalloc(&d->mem, sizeof(double) * d->fdoubles * 18) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(set_error(ctx, DUCTGPU_EALLOC, "dns: %.1f MB of fields", 18.0 * d->fdoubles * 8 / 1e6));
+    }
+    double *f = d->mem;
+    for (int c = 0; c < 3; ++c) d->vel[c] = f, f += d->fdoubles;
+    d->p = f, f += d->fdoubles;
+    for (int s = 0; s < 2; ++s)
+        for (int c = 0; c < 3; ++c) d->adv[s][c] = f, f += d->fdoubles;
+    for (int c = 0; c < 3; ++c) d->h[c] = f, f += d->fdoubles;
+    for (int c = 0; c < 5; ++c) d->prod[c] = f, f += d->fdoubles;
+    if (cudaMemsetAsync(d->mem, 0, sizeof(double) * d->fdoubles * 18, ctx->stream) != cudaSuccess)
+        return fail(check_cuda(ctx, cudaGetLastError(), "dns: memset"));
+    // wavenumbers and the lambda of every solve (per RK index)
+    std::vector<double> xa(M), lam(3 * M);
+    for (int i = 0; i < M; ++i) xa[i] = alp * i;
+    if (cudaMalloc(&d->xalp, sizeof(double) * M) != cudaSuccess ||
+        cudaMemcpy(d->xalp, xa.data(), sizeof(double) * M, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(check_cuda(ctx, cudaGetLastError(), "dns: xalp"));
+    for (int k = 0; k < 3; ++k) {
+        const double helco = 1.0 / (kBkk[k] * fnu * dt);
+        for (int c = 0; c < 3; ++c)
+            for (int i = 0; i < M; ++i) lam[c * M + i] = helco + xa[i] * xa[i];
+        d->lamh_d[k] = lam;
+        if (cudaMalloc(&d->lam_d[k], sizeof(double) * 3 * M) != cudaSuccess ||
+            cudaMemcpy(d->lam_d[k], lam.data(), sizeof(double) * 3 * M, cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(check_cuda(ctx, cudaGetLastError(), "dns: lambda"));
+    }
+    for (int i = 0; i < M; ++i) lam[i] = xa[i] * xa[i];
+    d->lamh_n.assign(lam.begin(), lam.begin() + M);
+    if (cudaMalloc(&d->lam_n, sizeof(double) * M) != cudaSuccess ||
+        cudaMemcpy(d->lam_n, lam.data(), sizeof(double) * M, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(check_cuda(ctx, cudaGetLastError(), "dns: lambda"));
+    // statistics: mean [4][P], prod [6][P], ppb [P], spec [4][7][M] in one block; weights
+    const size_t nst = 4 * d->P + 6 * d->P + d->P + 4 * 7 * (size_t)M;
+    if (cudaMalloc(&d->st_mean, sizeof(double) * nst) != cudaSuccess)
+        return fail(check_cuda(ctx, cudaGetLastError(), "dns: statistics"));
+    d->st_prod = d->st_mean + 4 * d->P;
+    d->st_ppb = d->st_prod + 6 * d->P;
+    d->st_spec = d->st_ppb + d->P;
+    cudaMemset(d->st_mean, 0, sizeof(double) * nst);
+    {
+        std::vector<double> wcc, wst;
+        make_weights(my, my, aspect, wcc, wst);
+        const size_t nw = wcc.size() + wst.size() + (size_t)kStatBlocksMax * kStatVals;
+        if (cudaMalloc(&d->wcc, sizeof(double) * nw) != cudaSuccess)
+            return fail(check_cuda(ctx, cudaGetLastError(), "dns: weights"));
+        d->wst = d->wcc + wcc.size();
+        d->partial = d->wst + wst.size();
+        cudaMemcpy(d->wcc, wcc.data(), sizeof(double) * wcc.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(d->wst, wst.data(), sizeof(double) * wst.size(), cudaMemcpyHostToDevice);
+    }
+    d->hist_cap = hist_cap;
+    if (cudaMalloc(&d->hist, sizeof(double) * kStatVals * (hist_cap > 0 ? hist_cap : 1)) != cudaSuccess ||
+        cudaMalloc(&d->hist_n, sizeof(int)) != cudaSuccess || cudaMemset(d->hist_n, 0, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&d->divmax, sizeof(double) * 3) != cudaSuccess)
+        return fail(check_cuda(ctx, cudaGetLastError(), "dns: history"));
+    // the flow-rate forcing of CMASSFLOW: premassfu / premassf with alphak = beta_k
+    if (d->cmassflow && (rc = ductgpu_precomp_mass_flow(ctx, dt, kBkk, 3, fnu, aspect, nullptr, nullptr)))
+        return fail(rc);
+    if ((rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "dns_create"))) return fail(rc);
+    *out = d;
+    return DUCTGPU_OK;
+}
+
+extern "C" int ductgpu_dns_destroy(ductgpu_dns d)
+{
+    if (!d) return DUCTGPU_EARG;
+    dns_free(d);
+    return DUCTGPU_OK;
+}
+
+// which: 0 u, 1 v, 2 w, 3 p
+extern "C" int ductgpu_dns_field(ductgpu_dns d, int which, double **dev)
+{
+    if (!d || !dev || which < 0 || which > 3) return DUCTGPU_EARG;
+    *dev = which < 3 ? d->vel[which] : d->p;
+    return DUCTGPU_OK;
+}
+
+extern "C" int ductgpu_dns_set_fields(ductgpu_dns d, const double *u, const double *v, const double *w,
+                                      const double *p)
+{
+    if (!d) return DUCTGPU_EARG;
+    ductgpu_ctx ctx = d->ctx;
+    if (!u || !v || !w || !p) return set_error(ctx, DUCTGPU_EARG, "dns_set_fields: null field");
+    cudaSetDevice(ctx->device);
+    const double *src[4] = {u, v, w, p};
+    double *dst[4] = {d->vel[0], d->vel[1], d->vel[2], d->p};
+    for (int c = 0; c < 4; ++c)
+        DUCT_CUDA(ctx, cudaMemcpyAsync(dst[c], src[c], sizeof(double) * d->fdoubles, cudaMemcpyDefault, ctx->stream));
+    // CMASSFLOW: the flow rate to hold is that of the initial u
+    if (d->cmassflow) {
+        int rc = ductgpu_impose_mass_flow_dev(ctx, &d->csum, 1, d->vel[0], 0);
+        if (rc) return rc;
+        // the captured substeps bake the flow rate in: re-capture
+        for (int k = 0; k < 3; ++k)
+            for (int s = 0; s < 2; ++s)
+                if (d->graph[k][s]) {
+                    cudaGraphExecDestroy(d->graph[k][s]);
+                    d->graph[k][s] = nullptr;
+                }
+    }
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "dns_set_fields");
+}
+
+extern "C" int ductgpu_dns_get_fields(ductgpu_dns d, double *u, double *v, double *w, double *p)
+{
+    if (!d) return DUCTGPU_EARG;
+    ductgpu_ctx ctx = d->ctx;
+    cudaSetDevice(ctx->device);
+    double *dst[4] = {u, v, w, p};
+    const double *src[4] = {d->vel[0], d->vel[1], d->vel[2], d->p};
+    for (int c = 0; c < 4; ++c)
+        if (dst[c])
+            DUCT_CUDA(ctx, cudaMemcpyAsync(dst[c], src[c], sizeof(double) * d->fdoubles, cudaMemcpyDefault, ctx->stream));
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "dns_get_fields");
+}
+
+extern "C" int ductgpu_dns_set_graphs(ductgpu_dns d, int on)
+{
+    if (!d) return DUCTGPU_EARG;
+    d->use_graphs = on != 0;
+    return DUCTGPU_OK;
+}
+
+namespace duct {
+static int dns_run_substep(ductgpu_dns d, int krk, bool stats)
+{
+    ductgpu_ctx ctx = d->ctx;
+    const int k = krk - 1, s = stats ? 1 : 0;
+    if (!d->use_graphs || ctx->prof_on) return dns_issue(d, krk, stats);
+    if (!d->graph[k][s]) {
+        // the first run of each RK index is uncaptured: it sizes the
+        // workspaces and builds the twiddle tables; later runs capture
+        // the substep once (without executing it) and replay the graph
+        if (!d->warm[k]) {
+            int rc = dns_issue(d, krk, stats);
+            if (rc) return rc;
+            DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            d->warm[k] = true;
+            return DUCTGPU_OK;
+        }
+        ctx->capturing = true;
+        cudaGraph_t g = nullptr;
+        int rc = DUCTGPU_OK;
+        cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            rc = dns_issue(d, krk, stats);
+            cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &g);
+            if (!rc && e2 != cudaSuccess) rc = check_cuda(ctx, e2, "cudaStreamEndCapture");
+        } else {
+            rc = check_cuda(ctx, e, "cudaStreamBeginCapture");
+        }
+        ctx->capturing = false;
+        if (!rc) rc = check_cuda(ctx, cudaGraphInstantiate(&d->graph[k][s], g, 0), "cudaGraphInstantiate");
+        if (g) cudaGraphDestroy(g);
+        if (rc) return rc;
+    }
+    ctx->launches += 1;
+    return check_cuda(ctx, cudaGraphLaunch(d->graph[k][s], ctx->stream), "cudaGraphLaunch");
+}
+}  // namespace duct
+
+extern "C" int ductgpu_dns_substep(ductgpu_dns d, int krk, int stats)
+{
+    if (!d) return DUCTGPU_EARG;
+    if (krk < 1 || krk > 3) return set_error(d->ctx, DUCTGPU_EARG, "dns_substep: krk=%d (1..3)", krk);
+    cudaSetDevice(d->ctx->device);
+    const bool st = stats && krk == 1;
+    int rc = dns_run_substep(d, krk, st);
+    if (!rc && st) d->nstat += 1;
+    return rc;
+}
+
+// nsteps full RK3 steps; statistics gathered at every stats_every-th step
+// (0: none), counting from the first step of this call.  Asynchronous.
+extern "C" int ductgpu_dns_steps(ductgpu_dns d, int nsteps, int stats_every)
+{
+    if (!d) return DUCTGPU_EARG;
+    if (nsteps < 0) return set_error(d->ctx, DUCTGPU_EARG, "dns_steps: nsteps=%d", nsteps);
+    cudaSetDevice(d->ctx->device);
+    for (int s = 0; s < nsteps; ++s) {
+        const int st = (stats_every > 0 && s % stats_every == 0) ? 1 : 0;
+        for (int krk = 1; krk <= 3; ++krk) {
+            int rc = ductgpu_dns_substep(d, krk, st);
+            if (rc) return rc;
+        }
+    }
+    return DUCTGPU_OK;
+}
+
+// Accumulated statistics (device -> host; null outputs skipped): mean
+// [4][my][my] (u, v, w, p mode-0 real parts, summed over the recorded
+// steps), prod [6][my][my] (uu, vv, ww, uv, uw, vw), ppb [my][my], spec
+// [4][7][M]; hist [nrows][10] rows of stress4[4], energy[3], energy2[3];
+// nstat recorded steps, nhist rows written (at most the capacity given to
+// ductgpu_dns_create).  divmax3: max |div u| after each substep of the last
+// step.  Synchronises.
+extern "C" int ductgpu_dns_statistics(ductgpu_dns d, double *mean, double *prod, double *ppb, double *spec,
+                                      double *hist, int *nstat, int *nhist, double *divmax3)
+{
+    if (!d) return DUCTGPU_EARG;
+    ductgpu_ctx ctx = d->ctx;
+    cudaSetDevice(ctx->device);
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const size_t P = d->P;
+    if (mean) DUCT_CUDA(ctx, cudaMemcpy(mean, d->st_mean, sizeof(double) * 4 * P, cudaMemcpyDeviceToHost));
+    if (prod) DUCT_CUDA(ctx, cudaMemcpy(prod, d->st_prod, sizeof(double) * 6 * P, cudaMemcpyDeviceToHost));
+    if (ppb) DUCT_CUDA(ctx, cudaMemcpy(ppb, d->st_ppb, sizeof(double) * P, cudaMemcpyDeviceToHost));
+    if (spec) DUCT_CUDA(ctx, cudaMemcpy(spec, d->st_spec, sizeof(double) * 4 * 7 * d->M, cudaMemcpyDeviceToHost));
+    int nh = 0;
+    DUCT_CUDA(ctx, cudaMemcpy(&nh, d->hist_n, sizeof(int), cudaMemcpyDeviceToHost));
+    if (nh > d->hist_cap) nh = d->hist_cap;
+    if (hist && nh > 0) DUCT_CUDA(ctx, cudaMemcpy(hist, d->hist, sizeof(double) * kStatVals * nh, cudaMemcpyDeviceToHost));
+    if (nstat) *nstat = d->nstat;
+    if (nhist) *nhist = nh;
+    if (divmax3) DUCT_CUDA(ctx, cudaMemcpy(divmax3, d->divmax, sizeof(double) * 3, cudaMemcpyDeviceToHost));
+    return DUCTGPU_OK;
+}

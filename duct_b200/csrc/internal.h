@@ -86,6 +86,8 @@ struct Workspace {
 
 }  // namespace duct
 
+namespace duct { struct DnsAux; }
+
 struct ductgpu_ctx_s {
     int device = 0;
     int num_sms = 148;
@@ -146,6 +148,7 @@ struct ductgpu_ctx_s {
     int tw_len[kTwTables] = {};
     void *tw_tab[kTwTables] = {};
     int *dev_err = nullptr;    // device error word (bounded waits)
+    duct::DnsAux *dns_aux = nullptr;   // buffers of the DNS operator entries (dns.cu)
     double *lam = nullptr;     // per-plane lambda (device)
     double *lam_host = nullptr;// pinned staging
     int lam_cap = 0;
@@ -318,6 +321,44 @@ int transyz_dev(ductgpu_ctx ctx, double *f, int my, int mz, int nmodes, char cdi
 int derivyz_dev(ductgpu_ctx ctx, const double *u, double *du, int my, int mz, int nmodes, char cdir,
                 int ider, double scal, char what, double aspect);
 int transpose_dev(ductgpu_ctx ctx, const double *in, double *out, long long A, long long Q);
+
+// cheb_lines.cu: fused Chebyshev derivative lines with a pointwise epilogue
+// (see the file's header).  One output:
+//   out = sigma * (beta * out + fac * D^order(in) + sum_t (xc0_t + xc1_t i kx
+//                  + xc2_t (i kx)^2) xs_t + [mode 0] m0)
+// with D the reference's derivyz between transyz -1 / +1 along the launch's
+// direction (fac already divided by aspect^order for z).  maxabs (device,
+// or null): atomic max of |out| over the interior points.
+constexpr int kLineXTerms = 4;
+constexpr int kMaxLineOut = 3;
+constexpr int kMaxLineJobs = 4;
+struct LineOut {
+    double *out = nullptr;
+    const double *xs[kLineXTerms] = {};
+    double xc0[kLineXTerms] = {}, xc1[kLineXTerms] = {}, xc2[kLineXTerms] = {};
+    double fac = 1.0, beta = 0.0, sigma = 1.0, m0 = 0.0;
+    double *maxabs = nullptr;
+    int order = 0;
+};
+struct LineJob {
+    const double *in = nullptr;
+    int nout = 0;
+    LineOut o[kMaxLineOut];
+};
+struct LineParams {
+    LineJob job[kMaxLineJobs];
+    int njobs = 0;
+    int my = 0, mz = 0, nmodes = 0;
+    char dir = 'y';
+    const double *xalp = nullptr;   // device [nmodes]
+    int real0 = 0;                  // 1: mode 0 of every input is real -> derivative terms of mode 0 real
+    int ctas_per_job = 0;           // set by lines_launch
+};
+int lines_launch(ductgpu_ctx ctx, const LineParams &p);
+// dns.cu
+void free_dns_aux(ductgpu_ctx ctx);
+bool lines_supported(int nn);
+const double2 *twiddle_table(ductgpu_ctx ctx, int L);
 
 }  // namespace duct
 

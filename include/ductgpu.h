@@ -369,6 +369,105 @@ int ductgpu_cyzx2xyz_dev(ductgpu_ctx ctx, double *phys, const double *phys2,
 int ductgpu_chx2z_dev(ductgpu_ctx ctx, double *xy, double *xz, int my, int mz, int nmodes);
 int ductgpu_chz2x_dev(ductgpu_ctx ctx, double *xz, double *xy, int my, int mz, int nmodes);
 
+/* ---- operators of the DNS time step (x-cut complex (my,mz,nmodes) device
+ * fields, wavenumbers xalp[nmodes] on the host) ------------------------
+ * The y / z derivatives are the reference's transyz(-1) -> derivyz ->
+ * transyz(+1) round trip, computed per line in one pass (my-1 and mz-1 one
+ * of 16, 24, 32, 48, 64, 96, 128, 144, 192, 256); x derivatives are i kx.
+ * The reference transforms some inputs in place and back (changing them by
+ * rounding); here inputs are left untouched.  Asynchronous on the context
+ * stream unless stated.                                                   */
+/* derivx(u,du,ider,scal,what), src/fourier.F:120-188:
+ * du = [du +] scal (i kx)^ider u (what = 'n' overwrites).                 */
+int ductgpu_derivx_dev(ductgpu_ctx ctx, const double *u, double *du, int my, int mz, int nmodes,
+                       const double *xalp, int ider, double scal, char what);
+/* laplacian3d(u,flap,tmp,tmpyz,scal,what), src/operators.F:278-347:
+ * flap = [flap +] scal (-kx^2 u + u_yy + u_zz / aspect^2).               */
+int ductgpu_laplacian3d_dev(ductgpu_ctx ctx, const double *u, double *flap, int my, int mz,
+                            int nmodes, const double *xalp, double aspect, double scal, char what);
+/* grad3d(u,dxu,dyu,dzu,tmp,tmpyz,scal,what), src/operators.F:349-425.     */
+int ductgpu_grad3d_dev(ductgpu_ctx ctx, const double *u, double *dxu, double *dyu, double *dzu,
+                       int my, int mz, int nmodes, const double *xalp, double aspect, double scal,
+                       char what);
+/* div3d(u,v,w,div,tmp,tmpyz,scal), src/operators.F:427-501:
+ * div = scal (i kx u + v_y + w_z / aspect).                               */
+int ductgpu_div3d_dev(ductgpu_ctx ctx, const double *u, const double *v, const double *w, double *div,
+                      int my, int mz, int nmodes, const double *xalp, double aspect, double scal);
+/* update_uvwp(u,v,w,p,phi,rhsphi,tmp,tmpyz,akk,bkk), src/operators.F:503-605
+ * (no FILTER): p += phi - (akk+bkk) dt fnu lap(phi); (u,v,w) -= dt
+ * (akk+bkk) grad(phi).  The reference's rhsphi work array is not produced. */
+int ductgpu_update_uvwp_dev(ductgpu_ctx ctx, double *u, double *v, double *w, double *p,
+                            const double *phi, int my, int mz, int nmodes, const double *xalp,
+                            double aspect, double akk, double bkk, double dt, double fnu);
+/* advection3d(u,v,w,adv1,adv2,adv3,...), src/operators.F:9-276, with the
+ * x transforms of fourx/pack_fftw/fill (src/fourier.F:1-118, 2/3 rule:
+ * nmodes = mx/2, mx = 2 (mgalx/3); mgalx one of 16, 64, 144, 256) and the
+ * pencil transposes folded into the addressing.  work: 5 fields of the same
+ * size (the products uv, uw, vv, vw, ww).  stats2 (device (my,mz,6) or
+ * NULL): statistics_fou2 (src/operators.F:1957-2004) -- the x-means of uu,
+ * vv, ww, uv, uw, vw added.                                              */
+int ductgpu_advection3d_dev(ductgpu_ctx ctx, const double *u, const double *v, const double *w,
+                            double *adv1, double *adv2, double *adv3, double *work, int my, int mz,
+                            int nmodes, int mgalx, const double *xalp, double aspect, double *stats2);
+/* max_3din(u,divmax), src/operators.F:2524-2550: max |u| over the interior
+ * points of every mode (synchronises).                                    */
+int ductgpu_max_3din_dev(ductgpu_ctx ctx, const double *u, int my, int mz, int nmodes, double *divmax);
+/* wallstressx(u,tmpyz,stress4), src/operators.F:676-710 with
+ * cheb2_wallstress_circum (src/chebyshev.f90:642-690): the wall stress of
+ * the x-mean of u per wall (host stress4[4]; synchronises).               */
+int ductgpu_wallstressx_dev(ductgpu_ctx ctx, const double *u, int my, int mz, double aspect,
+                            double *stress4);
+/* energy_fou(u,energy,energy2), src/operators.F:907-973 (one rank):
+ * sqrt(sum_{i>=1} 2|u_i|^2 dy dz / area) and the same with mode 0
+ * (synchronises).                                                         */
+int ductgpu_energy_fou_dev(ductgpu_ctx ctx, const double *u, int my, int mz, int nmodes, double aspect,
+                           double *energy, double *energy2);
+/* statistics_fou(u,v,w,p,1), src/operators.F:1608-1765 (one rank): adds
+ * to the device accumulators mean (my,mz,4) the mode-0 real parts of u, v,
+ * w, p, ppb (my,mz) the x-mean of p^2, spec (nmodes,7,4) the streamwise
+ * spectra at the reference's seven points (synchronises).                 */
+int ductgpu_statistics_fou_dev(ductgpu_ctx ctx, const double *u, const double *v, const double *w,
+                               const double *p, int my, int mz, int nmodes, double *mean, double *ppb,
+                               double *spec);
+
+/* ---- the RK3/Crank-Nicolson DNS step, device resident ------------------
+ * The substep of src/main1.f90:384-723 (square duct, no temperature,
+ * DT_FIXED): advection (i), (ii); statistics at the first substep of a
+ * recorded step; the explicit right-hand side (iii)-(vii); the implicit
+ * helm3d 'd' solves of u, v, w (viii); the pseudo-pressure Poisson solve
+ * (ix), (x); update_uvwp (xi); impose_mass_flow with CMASSFLOW; the
+ * divergence check max_3din.  Needs a context set up with
+ * ductgpu_pseudomat at my = mz.  cmassflow 1 holds the flow rate of the
+ * initial u (set by ductgpu_dns_set_fields); 0 drives the flow with the
+ * mean pressure gradient dpdx.  precision: DUCTGPU_PREC_* of the solves.
+ * hist_cap: rows of the per-step diagnostics history kept on the device.
+ * After the first use of each RK index, a substep runs as one CUDA graph
+ * launch.                                                                 */
+typedef struct ductgpu_dns_s *ductgpu_dns;
+int ductgpu_dns_create(ductgpu_ctx ctx, int mgalx, double alp, double fnu, double dt, double aspect,
+                       int cmassflow, double dpdx, int precision, int hist_cap, ductgpu_dns *out);
+int ductgpu_dns_destroy(ductgpu_dns dns);
+/* u, v, w, p: complex (my,my,nmodes) host or device arrays (copied).      */
+int ductgpu_dns_set_fields(ductgpu_dns dns, const double *u, const double *v, const double *w,
+                           const double *p);
+/* NULL outputs are skipped; host or device destinations.  Synchronises.   */
+int ductgpu_dns_get_fields(ductgpu_dns dns, double *u, double *v, double *w, double *p);
+/* Device pointer of the resident field which = 0 u, 1 v, 2 w, 3 p.        */
+int ductgpu_dns_field(ductgpu_dns dns, int which, double **dev);
+/* Graph replay of substeps on (1, the default) or off.                    */
+int ductgpu_dns_set_graphs(ductgpu_dns dns, int on);
+/* One substep krk = 1..3 (stats: gather the step's statistics, krk 1).    */
+int ductgpu_dns_substep(ductgpu_dns dns, int krk, int stats);
+/* nsteps RK3 steps, statistics every stats_every-th step (0: none).       */
+int ductgpu_dns_steps(ductgpu_dns dns, int nsteps, int stats_every);
+/* Accumulated statistics to the host (NULL outputs skipped): mean
+ * (my,my,4), prod (my,my,6) (uu, vv, ww, uv, uw, vw), ppb (my,my), spec
+ * (nmodes,7,4); hist rows (10 doubles: stress4[4], energy[3] of u, v, w,
+ * energy2[3]); nstat recorded steps; nhist rows; divmax3 the divergence
+ * after each substep of the last step.  Synchronises.                    */
+int ductgpu_dns_statistics(ductgpu_dns dns, double *mean, double *prod, double *ppb, double *spec,
+                           double *hist, int *nstat, int *nhist, double *divmax3);
+
 /* ---- the reference's own GPU entry points (src/mytranspose_cuda.cu) --- */
 /* transpose_gpu_(handle,Nx,Ny,alpha,devPtrA,devPtrC) and
  * mat_invdiag_gpu_(handle,Nx,Ny,xlam,devPtrF,devPtrED,devPtrC) with the
@@ -414,7 +513,10 @@ long long ductgpu_launch_count(ductgpu_ctx ctx);
 #define DUCTGPU_K_TRANSFORM 5   /* Chebyshev transforms / derivatives       */
 #define DUCTGPU_K_TRANSPOSE 6   /* pencil transposes                        */
 #define DUCTGPU_K_OTHER 7
-#define DUCTGPU_K_COUNT 8
+#define DUCTGPU_K_LINES 8      /* fused Chebyshev line derivative + epilogue */
+#define DUCTGPU_K_ADVECTION 9  /* x-direction Fourier products (advection)  */
+#define DUCTGPU_K_STATS 10     /* statistics / diagnostics reductions     */
+#define DUCTGPU_K_COUNT 11
 int ductgpu_profile_enable(ductgpu_ctx ctx, int on);
 int ductgpu_profile_reset(ductgpu_ctx ctx);
 int ductgpu_profile_read(ductgpu_ctx ctx, int kind, double *ms, long long *launches);
