@@ -21,125 +21,135 @@
 // times, then transyz +1.  The DCT-I is the half-length form (one complex
 // FFT of N points for the real and imaginary lines at once, Press et al.,
 // Numerical Recipes sec. 12.3; the same transform as transforms.cu's k_dcth),
-// and both scans of the recurrence (one per parity class) run across a warp
-// with shuffles.  A job may produce two outputs from one input line (e.g.
-// phi_y and phi_yy of update_uvwp): one forward transform, both recurrences,
-// one inverse per output.
+// and both scans of the recurrence (one per parity class) run across the
+// lanes that own the line with shuffles.  A job may produce up to three
+// outputs from one input line (e.g. p, v and u of update_uvwp): one forward
+// transform, the recurrences, one inverse per derivative output.
+//
+// Work split: a line belongs to a segment of LPL consecutive lanes (16 for
+// N = 96..256, 8 or 4 below), so a warp carries 32 / LPL lines through the
+// whole chain on its own -- warp-synchronous, with no CTA barrier after the
+// twiddle tables are loaded -- and many independent warps per SM hide the
+// FP64 and shared-memory latencies of the short dependent phases (pre-step,
+// two FFT steps, scans).  The two lines of a warp are neighbours (z and
+// z + 1 for y lines, y and y + 1 for z lines), so the strided accesses of
+// z lines still move whole 32-byte sectors.
 #include "fft.cuh"
 #include "internal.h"
 
 namespace duct {
 
-// Scans of the forward / inverse post-step and of the recurrence, and the
-// forward / inverse pre-step, one warp per line.  Layout of a line in the
-// FFT buffer: point j at j + j / R2 (a pad word every R2 points), point N
-// last.
+// Shuffles within a segment of W lanes.
+template <int W>
+__device__ __forceinline__ double seg_sum(double v)
+{
+#pragma unroll
+    for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, W);
+    return v;
+}
 
-// Forward pre-step on the staged line in x (in place):
+// Chunk of a scan over n values on W lanes, rounded up to an odd count:
+// lanes then start their chunks on distinct 16-byte banks of a quarter warp.
+__host__ __device__ constexpr int odd_chunk(int n, int w) { return ((n + w - 1) / w) | 1; }
+
+// Layout of a line in its FFT buffer: point j at j + j / R2 (a pad word every
+// R2 points), point N last.
+template <int R2>
+__device__ __forceinline__ int at(int j) { return j + j / R2; }
+
+// Pre-step, in place on the staged line (src null) or from a natural-order
+// line src -- the staged physical line, or (DOUBLE_ENDS) a coefficient line
+// whose two ends count twice (y_0 = 2 c_0, y_N = 2 c_N):
 //   g_0 = (x_0 + x_N)/2, g_{N/2} = x_{N/2},
 //   g_j = (x_j + x_{N-j})/2 - sin(pi j/N)(x_j - x_{N-j}),
-//   F_1 = (x_0 - x_N)/2 + sum_{j=1}^{N/2-1} cos(pi j/N)(x_j - x_{N-j}).
-// src (natural order, or null for x itself) gives the inverse's input,
-// whose two ends count twice (y_0 = 2 c_0, y_N = 2 c_N).
-template <int R2, int N>
-__device__ __forceinline__ void pre_step(double2 *xl, const double2 *src, const double2 *ha, double2 &f1, int lane)
+//   F_1 = (x_0 - x_N)/2 + sum_{j=1}^{N/2-1} cos(pi j/N)(x_j - x_{N-j}) -> *f1.
+template <int R2, int N, int W, bool DOUBLE_ENDS>
+__device__ __forceinline__ void pre_seg(double2 *xl, const double2 *src, const double2 *ha, double2 *f1, int s)
 {
-    auto at = [](int j) { return j + j / R2; };
     double sx = 0.0, sy = 0.0;
-    for (int j = 1 + lane; j < N / 2; j += 32) {
-        const double2 a = src ? src[j] : xl[at(j)], b = src ? src[N - j] : xl[at(N - j)];
+    for (int j = 1 + s; j < N / 2; j += W) {
+        const double2 a = src ? src[j] : xl[at<R2>(j)], b = src ? src[N - j] : xl[at<R2>(N - j)];
         const double2 u = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y + b.y));
         const double2 v = make_double2(a.x - b.x, a.y - b.y);
         const double2 w = ha[j];   // (cos(pi j/N), -sin(pi j/N))
-        xl[at(j)] = make_double2(u.x + w.y * v.x, u.y + w.y * v.y);
-        xl[at(N - j)] = make_double2(u.x - w.y * v.x, u.y - w.y * v.y);
+        xl[at<R2>(j)] = make_double2(u.x + w.y * v.x, u.y + w.y * v.y);
+        xl[at<R2>(N - j)] = make_double2(u.x - w.y * v.x, u.y - w.y * v.y);
         sx += w.x * v.x;
         sy += w.x * v.y;
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        sx += __shfl_xor_sync(0xffffffffu, sx, o);
-        sy += __shfl_xor_sync(0xffffffffu, sy, o);
-    }
-    if (lane == 0) {
+    sx = seg_sum<W>(sx);
+    sy = seg_sum<W>(sy);
+    if (s == 0) {
         double2 x0, xn, xm;
         if (src) {
-            x0 = make_double2(2.0 * src[0].x, 2.0 * src[0].y);
-            xn = make_double2(2.0 * src[N].x, 2.0 * src[N].y);
+            const double e = DOUBLE_ENDS ? 2.0 : 1.0;
+            x0 = make_double2(e * src[0].x, e * src[0].y);
+            xn = make_double2(e * src[N].x, e * src[N].y);
             xm = src[N / 2];
         } else {
-            x0 = xl[at(0)];
-            xn = xl[at(N)];
-            xm = xl[at(N / 2)];
+            x0 = xl[at<R2>(0)];
+            xn = xl[at<R2>(N)];
+            xm = xl[at<R2>(N / 2)];
         }
-        f1 = make_double2(0.5 * (x0.x - xn.x) + sx, 0.5 * (x0.y - xn.y) + sy);
-        xl[at(0)] = make_double2(0.5 * (x0.x + xn.x), 0.5 * (x0.y + xn.y));
-        xl[at(N / 2)] = xm;
+        *f1 = make_double2(0.5 * (x0.x - xn.x) + sx, 0.5 * (x0.y - xn.y) + sy);
+        xl[at<R2>(0)] = make_double2(0.5 * (x0.x + xn.x), 0.5 * (x0.y + xn.y));
+        xl[at<R2>(N / 2)] = xm;
     }
+    __syncwarp();
 }
 
-// Length-N FFT of every line in place: R1-point DFTs along n1 (column n2)
-// with the twiddle W_N^(n2 k1), then R2-point DFTs along each row k1.
-template <int R1, int R2, int NT, int LPB, int LS>
-__device__ __forceinline__ void fft_lines(double2 *x, const double2 *tw)
+// Length-N FFT of a line in place (N = R1 R2, R1, R2 <= W): lane n2 runs the
+// R1-point DFT of column n2 and applies W_N^(n2 k1), then lane k1 the
+// R2-point DFT of row k1.
+template <int R1, int R2, int W>
+__device__ __forceinline__ void fft_seg(double2 *xl, const double2 *tw, int s)
 {
     constexpr int N = R1 * R2;
-    auto at = [](int j) { return j + j / R2; };
-    {
-        const int l = threadIdx.x / R2, n2 = threadIdx.x - l * R2;
-        if (l < LPB) {
-            double2 *xl = x + l * LS;
-            double2 v[R1];
+    if (s < R2) {
+        double2 v[R1];
 #pragma unroll
-            for (int n1 = 0; n1 < R1; ++n1) v[n1] = xl[n1 * (R2 + 1) + n2];
-            reg_fft<R1, 0, 1>(v, tw, N);
+        for (int n1 = 0; n1 < R1; ++n1) v[n1] = xl[n1 * (R2 + 1) + s];
+        reg_fft<R1, 0, 1>(v, tw, N);
 #pragma unroll
-            for (int k1 = 0; k1 < R1; ++k1) xl[k1 * (R2 + 1) + n2] = (k1 == 0) ? v[0] : cmul(v[k1], tw[n2 * k1]);
-        }
+        for (int k1 = 0; k1 < R1; ++k1) xl[k1 * (R2 + 1) + s] = (k1 == 0) ? v[0] : cmul(v[k1], tw[s * k1]);
     }
-    __syncthreads();
-    {
-        const int l = threadIdx.x / R1, k1 = threadIdx.x - l * R1;
-        const bool act = l < LPB;
-        double2 w[R2];
-        if (act) {
-            const double2 *xr = x + l * LS + k1 * (R2 + 1);
+    __syncwarp();
+    double2 w[R2];
+    if (s < R1) {
 #pragma unroll
-            for (int n2 = 0; n2 < R2; ++n2) w[n2] = xr[n2];
-            reg_fft<R2, 0, 1>(w, tw, N);
-        }
-        __syncthreads();
-        if (act) {
-#pragma unroll
-            for (int k2 = 0; k2 < R2; ++k2) x[l * LS + at(k1 + R1 * k2)] = w[k2];
-        }
+        for (int n2 = 0; n2 < R2; ++n2) w[n2] = xl[s * (R2 + 1) + n2];
+        reg_fft<R2, 0, 1>(w, tw, N);
     }
-    __syncthreads();
+    __syncwarp();
+    if (s < R1) {
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) xl[at<R2>(s + R1 * k2)] = w[k2];
+    }
+    __syncwarp();
 }
 
 // Post-step: F_{2k} = (G_k + G_{N-k})/2, F_{2k+1} = F_1 + sum_{m=1}^{k}
-// i (G_m - G_{N-m})/2 (a warp scan of the increments).  nat != null: the
-// coefficients c = scale F (ends 1/N, interior 2/N: transyz -1) in natural
-// order into nat; else F in place in slot order (F_{2k} in slot k,
-// F_{2k+1} in slot N - k, F_1 in slot N).
-template <int R2, int N>
-__device__ __forceinline__ void post_step(double2 *xl, double2 *nat, double2 f1, int lane)
+// i (G_m - G_{N-m})/2 (a scan of the increments over the segment).  nat !=
+// null: the coefficients c = scale F (ends 1/N, interior 2/N: transyz -1)
+// in natural order into nat; else F in place in slot order (F_{2k} in slot
+// k, F_{2k+1} in slot N - k, F_1 in slot N).
+template <int R2, int N, int W>
+__device__ __forceinline__ void post_seg(double2 *xl, double2 *nat, double2 f1, int s)
 {
-    auto at = [](int j) { return j + j / R2; };
-    constexpr int CH = (N / 2 + 1 + 31) / 32;
-    const int k0 = lane * CH, k1 = min(N / 2 + 1, k0 + CH);
+    constexpr int CH = odd_chunk(N / 2 + 1, W);
+    const int k0 = s * CH, k1 = min(N / 2 + 1, k0 + CH);
     double sx = 0.0, sy = 0.0;
     for (int k = k0; k < k1; ++k) {
         if (k == 0 || k == N / 2) continue;
-        const double2 gk = xl[at(k)], gm = xl[at(N - k)];
+        const double2 gk = xl[at<R2>(k)], gm = xl[at<R2>(N - k)];
         sx -= 0.5 * (gk.y - gm.y);
         sy += 0.5 * (gk.x - gm.x);
     }
     double ix = sx, iy = sy;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const double tx = __shfl_up_sync(0xffffffffu, ix, o), ty = __shfl_up_sync(0xffffffffu, iy, o);
-        if (lane >= o) {
+    for (int o = 1; o < W; o <<= 1) {
+        const double tx = __shfl_up_sync(0xffffffffu, ix, o, W), ty = __shfl_up_sync(0xffffffffu, iy, o, W);
+        if (s >= o) {
             ix += tx;
             iy += ty;
         }
@@ -147,7 +157,7 @@ __device__ __forceinline__ void post_step(double2 *xl, double2 *nat, double2 f1,
     double rx = f1.x + ix - sx, ry = f1.y + iy - sy;
     constexpr double s_in = 2.0 / N, s_end = 1.0 / N;
     for (int k = k0; k < k1; ++k) {
-        const double2 gk = xl[at(k)], gm = xl[at(k == 0 ? 0 : N - k)];
+        const double2 gk = xl[at<R2>(k)], gm = xl[at<R2>(k == 0 ? 0 : N - k)];
         const double2 fe = make_double2(0.5 * (gk.x + gm.x), 0.5 * (gk.y + gm.y));
         if (k > 0 && k < N / 2) {
             rx -= 0.5 * (gk.y - gm.y);
@@ -158,58 +168,62 @@ __device__ __forceinline__ void post_step(double2 *xl, double2 *nat, double2 f1,
             nat[2 * k] = make_double2(se * fe.x, se * fe.y);
             if (k < N / 2) nat[2 * k + 1] = make_double2(s_in * rx, s_in * ry);
         } else {
-            xl[at(k)] = fe;
-            if (k > 0 && k < N / 2) xl[at(N - k)] = make_double2(rx, ry);
+            xl[at<R2>(k)] = fe;
+            if (k > 0 && k < N / 2) xl[at<R2>(N - k)] = make_double2(rx, ry);
         }
     }
-    if (!nat && lane == 0) xl[at(N)] = f1;
+    if (!nat && s == 0) xl[at<R2>(N)] = f1;
+    __syncwarp();
 }
 
-// Derivative recurrence on a natural-order coefficient line s -> t:
-//   e_k = sum_{j >= k, j = k mod 2} 2 j s_j,  t_m = -e_{m+1} (m >= 1),
-//   t_0 = -e_1 / 2, t_N = 0
+// Derivative recurrence in place on a natural-order coefficient line:
+//   e_k = sum_{j >= k, j = k mod 2} 2 j c_j,  c_m <- -e_{m+1} (m >= 1),
+//   c_0 <- -e_1 / 2, c_N <- 0
 // (src/chebyshev.f90:44-58; e_k is the reference's running value cri).
-// Lane q owns k in [1 + q CH, 1 + (q + 1) CH); the two parity classes are
-// suffix-scanned across the warp.
-template <int N>
-__device__ __forceinline__ void recurrence(const double2 *s, double2 *t, int lane)
+// Lane s owns k in [1 + s CH, 1 + (s + 1) CH): a first pass sums its chunk
+// per parity class, the sums are suffix-scanned over the segment, and a
+// backward pass writes c[k-1], reading c[k-1] just before.  The only
+// element a lane overwrites in another lane's chunk is that lane's top one,
+// which every lane keeps in a register before the warp barrier.
+template <int N, int W>
+__device__ __forceinline__ void rec_seg(double2 *c, int s)
 {
-    constexpr int CH = (N + 31) / 32;
-    const int k0 = 1 + lane * CH, k1 = min(N + 1, k0 + CH);
-    double2 se = make_double2(0.0, 0.0), so = se;
+    constexpr int CH = odd_chunk(N, W);
+    const int k0 = 1 + s * CH, k1 = min(N + 1, k0 + CH);
+    double2 se = make_double2(0.0, 0.0), so = se, top = se;
     for (int k = k0; k < k1; ++k) {
-        const double2 v = s[k];
+        const double2 v = c[k];
         const double f = 2.0 * k;
         if (k & 1) { so.x += f * v.x; so.y += f * v.y; }
         else { se.x += f * v.x; se.y += f * v.y; }
+        top = v;
     }
-    double2 ie = se, io = so;   // inclusive suffix sums over lanes >= lane
+    double2 ie = se, io = so;   // inclusive suffix sums over lanes >= s
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const double ax = __shfl_down_sync(0xffffffffu, ie.x, o), ay = __shfl_down_sync(0xffffffffu, ie.y, o);
-        const double bx = __shfl_down_sync(0xffffffffu, io.x, o), by = __shfl_down_sync(0xffffffffu, io.y, o);
-        if (lane + o < 32) {
+    for (int o = 1; o < W; o <<= 1) {
+        const double ax = __shfl_down_sync(0xffffffffu, ie.x, o, W), ay = __shfl_down_sync(0xffffffffu, ie.y, o, W);
+        const double bx = __shfl_down_sync(0xffffffffu, io.x, o, W), by = __shfl_down_sync(0xffffffffu, io.y, o, W);
+        if (s + o < W) {
             ie.x += ax; ie.y += ay;
             io.x += bx; io.y += by;
         }
     }
     double2 re = make_double2(ie.x - se.x, ie.y - se.y), ro = make_double2(io.x - so.x, io.y - so.y);
+    __syncwarp();
+    double2 cur = top;
     for (int k = k1 - 1; k >= k0; --k) {
-        const double2 v = s[k];
+        const double2 v = cur;
+        if (k > k0) cur = c[k - 1];   // read before this iteration overwrites it
         const double f = 2.0 * k;
         double2 e;
         if (k & 1) { ro.x += f * v.x; ro.y += f * v.y; e = ro; }
         else { re.x += f * v.x; re.y += f * v.y; e = re; }
         const double h = (k == 1) ? -0.5 : -1.0;
-        t[k - 1] = make_double2(h * e.x, h * e.y);
+        c[k - 1] = make_double2(h * e.x, h * e.y);
     }
-    if (lane == 0) t[N] = make_double2(0.0, 0.0);
+    if (s == 0) c[N] = make_double2(0.0, 0.0);
+    __syncwarp();
 }
-
-struct LineGeom {
-    long long ls, es, ms;   // complex strides: line, element, mode
-    int lpm;                // lines per mode
-};
 
 __device__ __forceinline__ double2 xterm_coef(const LineOut &o, int t, double kx)
 {
@@ -217,171 +231,187 @@ __device__ __forceinline__ double2 xterm_coef(const LineOut &o, int t, double kx
     return make_double2(o.xc0[t] - o.xc2[t] * kx * kx, o.xc1[t] * kx);
 }
 
-__device__ __forceinline__ void atomic_max_nonneg(double *a, double v)
+// Stores one output of a line.  deriv: the transform's result in slot order
+// in xl.  maxabs: the interior points' max |out|, reduced over the warp.
+template <int R2, int N, int W>
+__device__ __forceinline__ void store_seg(const LineOut &o, const double2 *xl, bool deriv, long long lbase,
+                                          long long es, bool act, bool interior_line, int mode, double kx, bool real0,
+                                          int s)
 {
-    atomicMax(reinterpret_cast<unsigned long long *>(a), (unsigned long long)__double_as_longlong(v));
-}
-
-// Stores one output of a CTA's lines.  slotted: the transform's result in
-// slot order in x (null for an order-0 output).
-template <int R2, int N, int NT, int LPB, int LS>
-__device__ __forceinline__ void store_output(const LineOut &o, const double2 *x, bool contiguous, const LineGeom &g,
-                                             long long base, int nl, int q0, int mode, double kx, bool real0)
-{
-    auto at = [](int j) { return j + j / R2; };
-    double2 *out = reinterpret_cast<double2 *>(o.out) + base;
-    double2 cf[kLineXTerms];
-    const double2 *xs[kLineXTerms];
-#pragma unroll
-    for (int t = 0; t < kLineXTerms; ++t) {
-        cf[t] = xterm_coef(o, t, kx);
-        xs[t] = o.xs[t] ? reinterpret_cast<const double2 *>(o.xs[t]) + base : nullptr;
-    }
-    const double m0 = (mode == 0) ? o.m0 : 0.0;
-    const bool deriv = o.order > 0;
     double vmax = 0.0;
-    auto one = [&](int l, int j) {
-        const long long gi = l * g.ls + (long long)j * g.es;
-        double2 v = make_double2(m0, 0.0);
-        if (deriv) {
-            const int slot = (j & 1) ? N - (j >> 1) : (j >> 1);
-            const double2 f = x[l * LS + at(slot)];
-            v.x += o.fac * f.x;
-            // the real and imaginary lines share one FFT; a real mode-0
-            // line keeps an exactly real derivative, as with real DCTs
-            if (!real0) v.y += o.fac * f.y;
-        }
+    if (act) {
+        double2 *out = reinterpret_cast<double2 *>(o.out) + lbase;
+        double2 cf[kLineXTerms];
+        const double2 *xs[kLineXTerms];
 #pragma unroll
-        for (int t = 0; t < kLineXTerms; ++t)
-            if (xs[t]) {
-                const double2 s = xs[t][gi];
-                v.x += cf[t].x * s.x - cf[t].y * s.y;
-                v.y += cf[t].x * s.y + cf[t].y * s.x;
-            }
-        if (o.beta != 0.0) {
-            const double2 w = out[gi];
-            v.x += o.beta * w.x;
-            v.y += o.beta * w.y;
+        for (int t = 0; t < kLineXTerms; ++t) {
+            cf[t] = xterm_coef(o, t, kx);
+            xs[t] = o.xs[t] ? reinterpret_cast<const double2 *>(o.xs[t]) + lbase : nullptr;
         }
-        v.x *= o.sigma;
-        v.y *= o.sigma;
-        out[gi] = v;
-        if (o.maxabs && j > 0 && j < N && q0 + l > 0 && q0 + l < g.lpm - 1) vmax = fmax(vmax, hypot(v.x, v.y));
-    };
-    if (contiguous) {
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        for (int l = warp; l < nl; l += NT / 32)
-            for (int j = lane; j <= N; j += 32) one(l, j);
-    } else {
-        for (int idx = threadIdx.x; idx < LPB * (N + 1); idx += NT) {
-            const int j = idx / LPB, l = idx - j * LPB;
-            if (l < nl) one(l, j);
+        const double m0 = (mode == 0) ? o.m0 : 0.0;
+        for (int j = s; j <= N; j += W) {
+            const long long gi = (long long)j * es;
+            double2 v = make_double2(m0, 0.0);
+            if (deriv) {
+                const int slot = (j & 1) ? N - (j >> 1) : (j >> 1);
+                const double2 f = xl[at<R2>(slot)];
+                v.x += o.fac * f.x;
+                // the real and imaginary lines share one FFT; a real mode-0
+                // line keeps an exactly real derivative, as with real DCTs
+                if (!real0) v.y += o.fac * f.y;
+            }
+#pragma unroll
+            for (int t = 0; t < kLineXTerms; ++t)
+                if (xs[t]) {
+                    const double2 sv = xs[t][gi];
+                    v.x += cf[t].x * sv.x - cf[t].y * sv.y;
+                    v.y += cf[t].x * sv.y + cf[t].y * sv.x;
+                }
+            if (o.beta != 0.0) {
+                const double2 w = out[gi];
+                v.x += o.beta * w.x;
+                v.y += o.beta * w.y;
+            }
+            v.x *= o.sigma;
+            v.y *= o.sigma;
+            out[gi] = v;
+            if (interior_line && j > 0 && j < N) vmax = fmax(vmax, hypot(v.x, v.y));
         }
     }
     if (o.maxabs) {
 #pragma unroll
-        for (int s = 16; s > 0; s >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, s));
-        if ((threadIdx.x & 31) == 0 && vmax > 0.0) atomic_max_nonneg(o.maxabs, vmax);
+        for (int t = 16; t > 0; t >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, t));
+        if ((threadIdx.x & 31) == 0 && vmax > 0.0)
+            atomicMax(reinterpret_cast<unsigned long long *>(o.maxabs), (unsigned long long)__double_as_longlong(vmax));
     }
 }
 
-template <int R1, int R2, int NT>
-__global__ void __launch_bounds__(NT) k_lines(const __grid_constant__ LineParams p, const double2 *__restrict__ twg,
-                                              const double2 *__restrict__ tw2g)
+// Shared memory per line: the FFT buffer (LS), the coefficients (N + 1; also
+// the landing place of the next line's prefetch) and F_1.
+template <int R1, int R2>
+struct LineShape {
+    static constexpr int N = R1 * R2, NN = N + 1, LS = R1 * (R2 + 1) + 1, PL = LS + NN + 1;
+};
+
+template <int R1, int R2, int W, int WPB>
+__global__ void __launch_bounds__(32 * WPB, 16 / WPB) k_lines(const __grid_constant__ LineParams p,
+                                                              const double2 *__restrict__ twg,
+                                                              const double2 *__restrict__ tw2g)
 {
-    constexpr int N = R1 * R2, NN = N + 1, LS = R1 * (R2 + 1) + 1;
-    constexpr int LPB = NT / (R1 > R2 ? R1 : R2), NW = NT / 32;
+    using S = LineShape<R1, R2>;
+    constexpr int N = S::N, LS = S::LS, PL = S::PL, LPW = 32 / W, NT = 32 * WPB;
     extern __shared__ __align__(16) double2 sm[];
     double2 *tw = sm;                   // W_N^t, N entries
     double2 *ha = tw + N;               // (cos, -sin)(pi j / N), j <= N/2
-    double2 *x = ha + (N / 2 + 1);      // [LPB][LS] FFT buffer
-    double2 *c = x + LPB * LS;          // [LPB][NN] coefficients, then order-2 coefficients
-    double2 *d = c + LPB * NN;          // [LPB][NN] order-1 coefficients
-    double2 *f1 = d + LPB * NN;         // [LPB]
-    auto at = [](int j) { return j + j / R2; };
+    double2 *lines = ha + (N / 2 + 1);  // [WPB * LPW][PL]
+    for (int t = threadIdx.x; t < N; t += NT) tw[t] = twg[t];
+    for (int t = threadIdx.x; t <= N / 2; t += NT) ha[t] = tw2g[t];
+    __syncthreads();
 
-    const int job = blockIdx.x / p.ctas_per_job;
-    const int r = blockIdx.x - job * p.ctas_per_job;
-    const LineJob &J = p.job[job];
-    LineGeom g;
-    const bool contiguous = (p.dir == 'y');
-    g.ms = (long long)p.my * p.mz;
-    if (contiguous) { g.ls = p.my; g.es = 1; g.lpm = p.mz; }
-    else { g.ls = 1; g.es = p.my; g.lpm = p.my; }
-    const int cpm = (g.lpm + LPB - 1) / LPB;
-    const int mode = r / cpm;
-    const int q0 = (r - mode * cpm) * LPB;
-    const int nl = min(LPB, g.lpm - q0);
-    const long long base = mode * g.ms + (long long)q0 * g.ls;
-    const double kx = p.xalp[mode];
+    // persistent warps over work items = (job, mode, pair of neighbouring lines)
+    const bool ydir = (p.dir == 'y');
+    const long long ms = (long long)p.my * p.mz;
+    const long long ls = ydir ? p.my : 1, es = ydir ? 1 : p.my;
+    const int lpm = ydir ? p.mz : p.my;
+    const int gpm = (lpm + LPW - 1) / LPW;              // line groups per mode
+    const long long per_job = (long long)gpm * p.nmodes;
+    const long long items = per_job * p.njobs;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int s = lane % W, seg = lane / W;
+    const long long wstep = (long long)gridDim.x * WPB;
+    double2 *xl = lines + (warp * LPW + seg) * PL, *cl = xl + LS, *f1 = cl + S::NN;
 
-    bool any_deriv = false, need2 = false;
-    for (int k = 0; k < J.nout; ++k) {
-        any_deriv |= J.o[k].order > 0;
-        need2 |= J.o[k].order == 2;
-    }
-    if (any_deriv) {
-        const double2 *in = reinterpret_cast<const double2 *>(J.in) + base;
-        if (contiguous) {
-            for (int l = warp; l < nl; l += NW)
-                for (int j = lane; j <= N; j += 32) cp_async16(x + l * LS + at(j), in + l * g.ls + j);
-        } else {
-            for (int idx = threadIdx.x; idx < LPB * NN; idx += NT) {
-                const int j = idx / LPB, l = idx - j * LPB;
-                if (l < nl) cp_async16(x + l * LS + at(j), in + l + (long long)j * g.es);
-            }
+    struct Item {
+        int job, mode, q;
+        bool act;
+        long long lbase;
+    };
+    auto item_of = [&](long long it) {
+        Item I;
+        I.job = (int)(it / per_job);
+        const long long r = it - (long long)I.job * per_job;
+        I.mode = (int)(r / gpm);
+        I.q = (int)(r - (long long)I.mode * gpm) * LPW + seg;
+        I.act = I.q < lpm;
+        I.lbase = I.mode * ms + (long long)(I.act ? I.q : 0) * ls;
+        return I;
+    };
+    auto needs_input = [&](int job) {
+        const LineJob &J = p.job[job];
+        for (int k = 0; k < J.nout; ++k)
+            if (J.o[k].order > 0) return true;
+        return false;
+    };
+    // the physical line of an item into cl (natural order), asynchronously
+    auto prefetch = [&](const Item &I) {
+        if (I.act && needs_input(I.job)) {
+            const double2 *in = reinterpret_cast<const double2 *>(p.job[I.job].in) + I.lbase;
+            for (int j = s; j <= N; j += W) cp_async16(cl + j, in + (long long)j * es);
         }
-        for (int t = threadIdx.x; t < N; t += NT) cp_async16(tw + t, twg + t);
-        for (int t = threadIdx.x; t <= N / 2; t += NT) cp_async16(ha + t, tw2g + t);
-        cp_async_wait_all();
-        __syncthreads();
-        // forward transform -> c (natural order, transyz -1 scaling)
-        for (int l = warp; l < LPB; l += NW) {
-            double2 *xl = x + l * LS;
-            if (l >= nl) {
-                for (int j = lane; j < LS; j += 32) xl[j] = make_double2(0.0, 0.0);
-                continue;
-            }
-            pre_step<R2, N>(xl, nullptr, ha, f1[l], lane);
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+
+    long long it = (long long)blockIdx.x * WPB + warp;
+    Item I = item_of(it);
+    if (it < items) prefetch(I);
+    for (; it < items; it += wstep) {
+        const LineJob &J = p.job[I.job];
+        const double kx = p.xalp[I.mode];
+        const bool real0 = p.real0 && I.mode == 0;
+        const bool interior_line = I.q > 0 && I.q < lpm - 1;
+        const Item next = item_of(it + wstep);
+        const bool has_next = it + wstep < items;
+        int maxord = 0, last = -1;
+        for (int k = 0; k < J.nout; ++k) {
+            maxord = max(maxord, J.o[k].order);
+            if (J.o[k].order > 0) last = k;
         }
-        __syncthreads();
-        fft_lines<R1, R2, NT, LPB, LS>(x, tw);
-        for (int l = warp; l < nl; l += NW) post_step<R2, N>(x + l * LS, c + l * NN, f1[l], lane);
-        __syncthreads();
-        // order 1 -> d; order 2 -> c (over the coefficients, no longer needed)
-        for (int l = warp; l < nl; l += NW) {
-            recurrence<N>(c + l * NN, d + l * NN, lane);
+        asm volatile("cp.async.wait_group 0;\n" ::);
+        __syncwarp();
+        if (maxord > 0) {
+            if (!I.act)
+                for (int j = s; j <= N; j += W) cl[j] = make_double2(0.0, 0.0);
             __syncwarp();
-            if (need2) recurrence<N>(d + l * NN, c + l * NN, lane);
-        }
-        __syncthreads();
-    }
-    for (int oi = 0; oi < J.nout; ++oi) {
-        const LineOut &o = J.o[oi];
-        if (o.order > 0) {
-            const double2 *y = (o.order == 1) ? d : c;
-            for (int l = warp; l < LPB; l += NW) {
-                if (l >= nl) continue;   // zeroed above; the FFT of zeros stays zero
-                pre_step<R2, N>(x + l * LS, y + l * NN, ha, f1[l], lane);
+            pre_seg<R2, N, W, false>(xl, cl, ha, f1, s);
+            fft_seg<R1, R2, W>(xl, tw, s);
+            post_seg<R2, N, W>(xl, cl, *f1, s);
+            // order 1 outputs, then (one more recurrence) order 2 outputs;
+            // the next item's line is fetched into cl once its last read is done
+            bool fetched = false;
+            for (int ord = 1; ord <= maxord; ++ord) {
+                rec_seg<N, W>(cl, s);
+                for (int k = 0; k < J.nout; ++k) {
+                    const LineOut &o = J.o[k];
+                    if (o.order != ord) continue;
+                    pre_seg<R2, N, W, true>(xl, cl, ha, f1, s);
+                    if (k == last && ord == maxord && has_next) {
+                        prefetch(next);
+                        fetched = true;
+                    }
+                    fft_seg<R1, R2, W>(xl, tw, s);
+                    post_seg<R2, N, W>(xl, nullptr, *f1, s);
+                    store_seg<R2, N, W>(o, xl, true, I.lbase, es, I.act, interior_line, I.mode, kx, real0, s);
+                    __syncwarp();
+                }
             }
-            __syncthreads();
-            fft_lines<R1, R2, NT, LPB, LS>(x, tw);
-            for (int l = warp; l < nl; l += NW) post_step<R2, N>(x + l * LS, nullptr, f1[l], lane);
-            __syncthreads();
+            if (!fetched && has_next) prefetch(next);
+        } else if (has_next) {
+            prefetch(next);
         }
-        store_output<R2, N, NT, LPB, LS>(o, x, contiguous, g, base, nl, q0, mode, kx, p.real0 && mode == 0);
-        __syncthreads();
+        for (int k = 0; k < J.nout; ++k)
+            if (J.o[k].order == 0)
+                store_seg<R2, N, W>(J.o[k], xl, false, I.lbase, es, I.act, interior_line, I.mode, kx, real0, s);
+        I = next;
     }
+    asm volatile("cp.async.wait_group 0;\n" ::);
 }
 
-const double2 *twiddle_table(ductgpu_ctx ctx, int L);
-
-template <int R1, int R2, int NT>
+template <int R1, int R2, int W, int WPB>
 static int launch_lines(ductgpu_ctx ctx, const LineParams &p0)
 {
-    constexpr int N = R1 * R2, NN = N + 1, LS = R1 * (R2 + 1) + 1;
-    constexpr int LPB = NT / (R1 > R2 ? R1 : R2);
+    using S = LineShape<R1, R2>;
+    constexpr int N = S::N, LPB = (32 / W) * WPB;
+    static_assert(R1 <= W && R2 <= W && 32 % W == 0, "a line's FFT columns and rows fit its lane segment");
     const double2 *tw = twiddle_table(ctx, N);
     const double2 *tw2 = twiddle_table(ctx, 2 * N);
     if (!tw || !tw2)
@@ -389,14 +419,19 @@ static int launch_lines(ductgpu_ctx ctx, const LineParams &p0)
                          ctx->capturing ? " (first use inside a capture)" : "");
     LineParams p = p0;
     const int lpm = (p.dir == 'y') ? p.mz : p.my;
-    p.ctas_per_job = p.nmodes * ((lpm + LPB - 1) / LPB);
-    const size_t smem = ((size_t)N + (N / 2 + 1) + (size_t)LPB * LS + 2 * (size_t)LPB * NN + LPB) * sizeof(double2);
-    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_lines<R1, R2, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const long long grid = (long long)p.ctas_per_job * p.njobs;
+    // one work item (job, mode, line pair) per warp: measured at my = 193
+    // (a cfg4 DNS step) this beats persistent warps that prefetch their next
+    // item (16 / WPB CTAs per SM; 10.4 against 9.6 ms of line kernels a step)
+    const long long items = (long long)p.njobs * p.nmodes * ((lpm + 32 / W - 1) / (32 / W));
+    const long long grid = (items + WPB - 1) / WPB;
     if (grid > 0x7fffffffLL) return set_error(ctx, DUCTGPU_EARG, "lines: grid too large");
+    p.ctas_per_job = 0;
+    const size_t smem = ((size_t)N + (N / 2 + 1) + (size_t)LPB * S::PL) * sizeof(double2);
+    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_lines<R1, R2, W, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
     {
         LaunchScope ls(ctx, DUCTGPU_K_LINES);
-        k_lines<R1, R2, NT><<<(unsigned)grid, NT, smem, ctx->stream>>>(p, tw, tw2);
+        k_lines<R1, R2, W, WPB><<<(unsigned)grid, 32 * WPB, smem, ctx->stream>>>(p, tw, tw2);
     }
     return check_cuda(ctx, cudaGetLastError(), "k_lines");
 }
@@ -425,16 +460,16 @@ int lines_launch(ductgpu_ctx ctx, const LineParams &p)
     }
     const int nn = (p.dir == 'y') ? p.my : p.mz;
     switch (nn - 1) {
-    case 16: return launch_lines<4, 4, 64>(ctx, p);
-    case 24: return launch_lines<4, 6, 64>(ctx, p);
-    case 32: return launch_lines<4, 8, 64>(ctx, p);
-    case 48: return launch_lines<6, 8, 64>(ctx, p);
-    case 64: return launch_lines<8, 8, 64>(ctx, p);
-    case 96: return launch_lines<8, 12, 64>(ctx, p);
-    case 128: return launch_lines<8, 16, 64>(ctx, p);
-    case 144: return launch_lines<12, 12, 64>(ctx, p);
-    case 192: return launch_lines<12, 16, 64>(ctx, p);
-    case 256: return launch_lines<16, 16, 64>(ctx, p);
+    case 16: return launch_lines<4, 4, 4, 4>(ctx, p);
+    case 24: return launch_lines<4, 6, 8, 4>(ctx, p);
+    case 32: return launch_lines<4, 8, 8, 4>(ctx, p);
+    case 48: return launch_lines<6, 8, 8, 4>(ctx, p);
+    case 64: return launch_lines<8, 8, 8, 4>(ctx, p);
+    case 96: return launch_lines<8, 12, 16, 4>(ctx, p);
+    case 128: return launch_lines<8, 16, 16, 4>(ctx, p);
+    case 144: return launch_lines<12, 12, 16, 4>(ctx, p);
+    case 192: return launch_lines<12, 16, 16, 4>(ctx, p);
+    case 256: return launch_lines<16, 16, 16, 4>(ctx, p);
     default:
         return set_error(ctx, DUCTGPU_EARG, "lines: line length %d - 1 is not one of 16, 24, 32, 48, 64, 96, 128, "
                          "144, 192, 256", nn);
