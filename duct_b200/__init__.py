@@ -44,7 +44,7 @@ EXPORTS = [
     "ductgpu_wallstressx_dev", "ductgpu_energy_fou_dev", "ductgpu_statistics_fou_dev",
     "ductgpu_dns_create", "ductgpu_dns_destroy", "ductgpu_dns_set_fields", "ductgpu_dns_get_fields",
     "ductgpu_dns_field", "ductgpu_dns_set_graphs", "ductgpu_dns_substep", "ductgpu_dns_steps",
-    "ductgpu_dns_statistics",
+    "ductgpu_dns_statistics", "ductgpu_profile_bytes",
 ]
 SETUP_NO_EIGEN = 1
 (K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER, K_LINES,
@@ -154,6 +154,7 @@ def lib():
             "ductgpu_dns_substep": [P, I, I],
             "ductgpu_dns_steps": [P, I, I],
             "ductgpu_dns_statistics": [P, P, P, P, P, P, C.POINTER(I), C.POINTER(I), P],
+            "ductgpu_profile_bytes": [P, I, C.POINTER(D)],
             "ductgpu_graph_destroy": [P, I],
             "transpose_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
                                C.POINTER(C.c_size_t)],
@@ -599,6 +600,11 @@ class Context:
         ms, n = C.c_double(), C.c_longlong()
         self._check(lib().ductgpu_profile_read(self.h, int(kind), C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    def profile_bytes(self, kind):
+        b = C.c_double()
+        self._check(lib().ductgpu_profile_bytes(self.h, int(kind), C.byref(b)))
+        return b.value
 
 
 def _dp(a):

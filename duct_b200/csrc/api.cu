@@ -1222,6 +1222,7 @@ int ductgpu_profile_reset(ductgpu_ctx ctx)
     for (int k = 0; k < DUCTGPU_K_COUNT; ++k) {
         ctx->prof_ms[k] = 0.0;
         ctx->prof_n[k] = 0;
+        ctx->prof_bytes[k] = 0.0;
     }
     return DUCTGPU_OK;
 }
@@ -1232,6 +1233,13 @@ int ductgpu_profile_read(ductgpu_ctx ctx, int kind, double *ms, long long *launc
     profile_drain(ctx);
     if (ms) *ms = ctx->prof_ms[kind];
     if (launches) *launches = ctx->prof_n[kind];
+    return DUCTGPU_OK;
+}
+
+int ductgpu_profile_bytes(ductgpu_ctx ctx, int kind, double *bytes)
+{
+    if (!ctx || kind < 0 || kind >= DUCTGPU_K_COUNT || !bytes) return DUCTGPU_EARG;
+    *bytes = ctx->prof_bytes[kind];
     return DUCTGPU_OK;
 }
 

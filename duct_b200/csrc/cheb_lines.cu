@@ -429,6 +429,23 @@ static int launch_lines(ductgpu_ctx ctx, const LineParams &p0)
     const size_t smem = ((size_t)N + (N / 2 + 1) + (size_t)LPB * S::PL) * sizeof(double2);
     DUCT_CUDA(ctx, cudaFuncSetAttribute(k_lines<R1, R2, W, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
+    if (ctx->prof_on && !ctx->capturing) {
+        // algorithmic bytes: the input once (if transformed), every output
+        // written once and read once more if accumulated, every x-term source
+        double fields = 0.0;
+        for (int i = 0; i < p.njobs; ++i) {
+            const LineJob &J = p.job[i];
+            bool in = false;
+            for (int k = 0; k < J.nout; ++k) {
+                const LineOut &o = J.o[k];
+                in |= o.order > 0;
+                fields += 1.0 + (o.beta != 0.0 ? 1.0 : 0.0);
+                for (int t = 0; t < kLineXTerms; ++t) fields += o.xs[t] ? 1.0 : 0.0;
+            }
+            fields += in ? 1.0 : 0.0;
+        }
+        ctx->prof_bytes[DUCTGPU_K_LINES] += fields * 16.0 * p.my * p.mz * p.nmodes;
+    }
     {
         LaunchScope ls(ctx, DUCTGPU_K_LINES);
         k_lines<R1, R2, W, WPB><<<(unsigned)grid, 32 * WPB, smem, ctx->stream>>>(p, tw, tw2);

@@ -206,6 +206,8 @@ static int launch_advx(ductgpu_ctx ctx, const AdvParams &p)
     const size_t smem = ((size_t)N + 2 * (size_t)N * TQ) * sizeof(double2);
     DUCT_CUDA(ctx, cudaFuncSetAttribute(k_advx<R, TQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long long grid = (p.P + TQ - 1) / TQ;
+    // algorithmic bytes: u, v, w read, eight product fields written
+    if (ctx->prof_on && !ctx->capturing) ctx->prof_bytes[DUCTGPU_K_ADVECTION] += 11.0 * 16.0 * p.P * p.M;
     {
         LaunchScope ls(ctx, DUCTGPU_K_ADVECTION);
         k_advx<R, TQ><<<(unsigned)grid, NT, smem, ctx->stream>>>(p, tw);

@@ -164,6 +164,7 @@ struct ductgpu_ctx_s {
     int prof_used = 0;
     double prof_ms[DUCTGPU_K_COUNT] = {};
     long long prof_n[DUCTGPU_K_COUNT] = {};
+    double prof_bytes[DUCTGPU_K_COUNT] = {};   // algorithmic bytes of the launches (kernels that count them)
 };
 
 namespace duct {

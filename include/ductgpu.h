@@ -520,6 +520,11 @@ long long ductgpu_launch_count(ductgpu_ctx ctx);
 int ductgpu_profile_enable(ductgpu_ctx ctx, int on);
 int ductgpu_profile_reset(ductgpu_ctx ctx);
 int ductgpu_profile_read(ductgpu_ctx ctx, int kind, double *ms, long long *launches);
+/* Algorithmic bytes (each field element read or written once) of the
+ * launches of class `kind` since the last reset, counted on the host for
+ * the kernels that report them (DUCTGPU_K_LINES, DUCTGPU_K_ADVECTION);
+ * with profiling on only.                                                 */
+int ductgpu_profile_bytes(ductgpu_ctx ctx, int kind, double *bytes);
 
 #ifdef __cplusplus
 }
