@@ -44,7 +44,8 @@ EXPORTS = [
     "ductgpu_wallstressx_dev", "ductgpu_energy_fou_dev", "ductgpu_statistics_fou_dev",
     "ductgpu_dns_create", "ductgpu_dns_destroy", "ductgpu_dns_set_fields", "ductgpu_dns_get_fields",
     "ductgpu_dns_field", "ductgpu_dns_set_graphs", "ductgpu_dns_substep", "ductgpu_dns_steps",
-    "ductgpu_dns_statistics", "ductgpu_profile_bytes",
+    "ductgpu_dns_statistics", "ductgpu_profile_bytes", "ductgpu_dns_set_forcing",
+    "ductgpu_dns_wallstress_after", "ductgpu_dns_grad_wallstress",
 ]
 SETUP_NO_EIGEN = 1
 (K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER, K_LINES,
@@ -155,6 +156,9 @@ def lib():
             "ductgpu_dns_steps": [P, I, I],
             "ductgpu_dns_statistics": [P, P, P, P, P, P, C.POINTER(I), C.POINTER(I), P],
             "ductgpu_profile_bytes": [P, I, C.POINTER(D)],
+            "ductgpu_dns_set_forcing": [P, P, P, P],
+            "ductgpu_dns_wallstress_after": [P, I, C.POINTER(D)],
+            "ductgpu_dns_grad_wallstress": [P, C.POINTER(D), P],
             "ductgpu_graph_destroy": [P, I],
             "transpose_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
                                C.POINTER(C.c_size_t)],
@@ -662,6 +666,26 @@ class Dns:
 
     def steps(self, n, stats_every=0):
         self.ctx._check(lib().ductgpu_dns_steps(self.h, int(n), int(stats_every)))
+
+    def set_forcing(self, f=None):
+        """Body force (f1, f2, f3) of complex (my, my, M) arrays, or None."""
+        if f is None:
+            self.ctx._check(lib().ductgpu_dns_set_forcing(self.h, None, None, None))
+            return
+        arrs = [np.asfortranarray(x, dtype=np.complex128) for x in f]
+        self.ctx._check(lib().ductgpu_dns_set_forcing(self.h, *[_ptr(a) for a in arrs]))
+
+    def wallstress_after(self, nsteps=1):
+        J = C.c_double()
+        self.ctx._check(lib().ductgpu_dns_wallstress_after(self.h, int(nsteps), C.byref(J)))
+        return J.value
+
+    def grad_wallstress(self):
+        """(J, dJ/df as a (3, my, my, M) complex array) through one step."""
+        g = np.zeros((3, self.M, self.my, self.my), dtype=np.complex128)   # C order = 3 Fortran fields
+        J = C.c_double()
+        self.ctx._check(lib().ductgpu_dns_grad_wallstress(self.h, C.byref(J), g.ctypes.data_as(C.c_void_p)))
+        return J.value, np.stack([np.asfortranarray(np.transpose(g[c], (2, 1, 0))) for c in range(3)])
 
     def statistics(self):
         """dict(nstat, mean (4,my,my), prod (6,my,my), ppb (my,my), spec

@@ -960,6 +960,12 @@ struct ductgpu_dns_s {
     int hist_cap = 0;
     int nstat = 0;
     double *divmax = nullptr;    // [3], one per substep
+    // body force (src/main1.f90 (vi-b): forcings enter h like -grad p, h += (a + b) f)
+    double *force = nullptr;     // 3 fields, owned
+    bool forced = false;
+    // reverse sweep: transposed derivative matrices, checkpoints, cotangents
+    double *dmat = nullptr;      // [2][my][my] D1, D2 (real, column-major)
+    double *adj = nullptr;       // adjoint work fields
     bool use_graphs = true;
     bool warm[3] = {};
     cudaGraphExec_t graph[3][2] = {};
@@ -1028,6 +1034,7 @@ static int dns_issue(ductgpu_dns d, int krk, bool stats)
                 xterm(o, p, 0.0, -(a + b), 0.0);
                 if (!d->cmassflow) o.m0 = -(a + b) * d->dpdx;
             }
+            if (d->forced) xterm(o, d->force + c * d->fdoubles, a + b, 0.0, 0.0);
             add_job(py, d->vel[c], {o});
         }
         if ((rc = lines_launch(ctx, py))) return rc;
@@ -1127,6 +1134,9 @@ static void dns_free(ductgpu_dns d)
     cudaFree(d->wcc);
     cudaFree(d->hist);
     cudaFree(d->hist_n);
+    cudaFree(d->force);
+    cudaFree(d->dmat);
+    cudaFree(d->adj);
     delete d;
 }
 
@@ -1216,7 +1226,8 @@ extern "C" int ductgpu_dns_create(ductgpu_ctx ctx, int mgalx, double alp, double
     {
         std::vector<double> wcc, wst;
         make_weights(my, my, aspect, wcc, wst);
-        const size_t nw = wcc.size() + wst.size() + (size_t)kStatBlocksMax * kStatVals;
+        // the partial sums of the statistics kernel, and one row of scratch results after them
+        const size_t nw = wcc.size() + wst.size() + (size_t)(kStatBlocksMax + 1) * kStatVals;
         if (cudaMalloc(&d->wcc, sizeof(double) * nw) != cudaSuccess)
             return fail(check_cuda(ctx, cudaGetLastError(), "dns: weights"));
         d->wst = d->wcc + wcc.size();
@@ -1390,5 +1401,515 @@ extern "C" int ductgpu_dns_statistics(ductgpu_dns d, double *mean, double *prod,
     if (nstat) *nstat = d->nstat;
     if (nhist) *nhist = nh;
     if (divmax3) DUCT_CUDA(ctx, cudaMemcpy(divmax3, d->divmax, sizeof(double) * 3, cudaMemcpyDeviceToHost));
+    return DUCTGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Body force and the gradient of the four-wall shear functional through one
+// RK3/CN step by reverse mode (the discrete adjoint of the step above).
+//
+// Forward step: three substeps S_k mapping (u, v, w, p, A_{k-1}) to
+// (u', v', w', p', A_k), linear in everything but the advection A_k =
+// adv(u, v, w).  J = sum over the four walls of wallstressx(u) after the
+// step, a linear functional of the mode-0 real part of u.  The reverse
+// sweep applies, substep by substep from the last, the transpose of every
+// linear map in the coefficient inner product <a, b> = Re sum conj(a) b:
+//   mass flow   u += pu (csum - Q u)/pf         ->  u_ -= Q^T <pu, u_> / pf
+//   update      p' = p + phi - f1 Lap phi, u' = u* + s2 grad phi
+//   pressure    phi = S_n(div u* / ((a+b) dt))  ->  the adjoint Neumann solve
+//   predictor   u* = S_d(sigma h)               ->  the adjoint Dirichlet solve
+//   rhs         h = a nu Lap u + u/dt - gamma A_k - rho A_{k-1} - (a+b) grad p + (a+b) f
+//   advection   A_i = sum_j d_j P(u_i u_j)      ->  linearised at the substep's
+//               entry velocities (kept as in-memory checkpoints):
+//               u_m += sum_j W Spec(u_j Phys(W^-1 (Q_mj + Q_jm))), Q_ij = d_j^T A_i,
+//               W = diag(1, 2, 2, ...) the weights of the Hermitian modes.
+// Derivative transposes: i kx -> -i kx along x; along y and z the real
+// collocation matrices D1, D2 of the line kernel (built by applying it to
+// the unit vectors) transposed.
+namespace duct {
+
+static void dns_drop_graphs(ductgpu_dns d)
+{
+    for (int k = 0; k < 3; ++k)
+        for (int s = 0; s < 2; ++s)
+            if (d->graph[k][s]) {
+                cudaGraphExecDestroy(d->graph[k][s]);
+                d->graph[k][s] = nullptr;
+            }
+}
+
+// out = beta out + fac A^T in along lines (A nn x nn column-major real);
+// mode 0 keeps a zero imaginary part with real0 (the forward derivative
+// terms of a real mode-0 line are real).
+__global__ void k_lines_mat_t(const double *A, int nn, const double2 *in, double2 *out, int my, int mz, int M,
+                              int ydir, double fac, double beta, int real0)
+{
+    const long long P = (long long)my * mz, total = P * M;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long mode = t / P, q = t - mode * P;
+        const int y = (int)(q % my), z = (int)(q / my);
+        const int j = ydir ? y : z;
+        const double2 *line = in + mode * P + (ydir ? (long long)my * z : (long long)y);
+        const long long es = ydir ? 1 : my;
+        const double *col = A + (long long)nn * j;
+        double ax = 0.0, ay = 0.0;
+        for (int k = 0; k < nn; ++k) {
+            const double2 v = line[k * es];
+            ax += col[k] * v.x;
+            ay += col[k] * v.y;
+        }
+        if (real0 && mode == 0) ay = 0.0;
+        double2 o = make_double2(fac * ax, fac * ay);
+        if (beta != 0.0) {
+            const double2 w = out[t];
+            o.x += beta * w.x;
+            o.y += beta * w.y;
+        }
+        out[t] = o;
+    }
+}
+
+__global__ void k_real_part(const double2 *in, double *out, long long n)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        out[t] = in[t].x;
+}
+
+__global__ void k_unit_plane(double2 *e, int nn)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)nn * nn;
+         t += (long long)gridDim.x * blockDim.x)
+        e[t] = make_double2((t % nn) == (t / nn) ? 1.0 : 0.0, 0.0);
+}
+
+// dJ/du: the mode-0 real part gets the sum of the four wall-stress weights.
+__global__ void k_seed_wall(double2 *ub, const double *wst, long long P)
+{
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P; q += (long long)gridDim.x * blockDim.x)
+        ub[q].x += wst[q] + wst[P + q] + wst[2 * P + q] + wst[3 * P + q];
+}
+
+// Transpose of impose_mass_flow's correction u0 += pu (csum - Q u0) / pf,
+// Q u0 = aspect sum w_j w_k Re u0: u0_ -= aspect w_j w_k <pu, Re u0_> / pf.
+__global__ void __launch_bounds__(1024) k_mf_adj(double2 *u, const double *w, int m, double aspect, const double *pu,
+                                                 const double *pf)
+{
+    __shared__ double red[33];
+    const long long plane = (long long)m * m;
+    double acc = 0.0;
+    for (long long i = threadIdx.x; i < plane; i += blockDim.x) acc += pu[i] * u[i].x;
+    const double s = block_sum(acc, red);
+    __shared__ double sh;
+    if (threadIdx.x == 0) sh = s;
+    __syncthreads();
+    const double f = aspect * sh / *pf;
+    for (long long i = threadIdx.x; i < plane; i += blockDim.x) u[i].x -= f * w[i % m] * w[i / m];
+}
+
+struct AdjAdvParams {
+    const double2 *u, *v, *w;    // entry velocities of the substep
+    const double2 *S[6];         // Q_mj + Q_jm for (m, j) = 11, 22, 33, 12, 13, 23
+    double2 *ub[3];              // cotangents of u, v, w (added)
+    long long P;
+    int M;
+};
+
+// Transposed advection products per (y, z) point (see the block comment):
+// r_m = sum_j u_j Phys(W^-1 S_mj), u_m += W Spec(r_m).
+template <int R, int TQ>
+__global__ void __launch_bounds__(R * TQ) k_advx_adj(const __grid_constant__ AdjAdvParams p,
+                                                     const double2 *__restrict__ twg)
+{
+    constexpr int N = R * R, NT = R * TQ;
+    extern __shared__ __align__(16) double2 sm[];
+    double2 *tw = sm, *wk = tw + N, *xs = wk + N * TQ;
+    const int c = threadIdx.x / TQ, g = threadIdx.x - c * TQ;
+    const long long q0 = (long long)blockIdx.x * TQ, q = q0 + g;
+    const bool valid = q < p.P;
+    const int M = p.M;
+    const long long P = p.P;
+    for (int t = threadIdx.x; t < N; t += NT) cp_async16(tw + t, twg + t);
+    cp_async_wait_all();
+    __syncthreads();
+    double2 a[R];
+    // physical values of X + i Y along x (each a Hermitian spectrum, modes
+    // >= 1 scaled by sc): re into xr, im into yr
+    auto ifft_pair = [&](const double2 *X, const double2 *Y, double sc, double (&xr)[R], double (&yr)[R]) {
+#pragma unroll
+        for (int n1 = 0; n1 < R; ++n1) {
+            const int k = R * n1 + c;
+            double2 z = make_double2(0.0, 0.0);
+            if (valid && k < M) {
+                const double2 x = X[q + (long long)k * P], y = Y ? Y[q + (long long)k * P] : make_double2(0.0, 0.0);
+                z = (k == 0) ? make_double2(x.x, -y.x) : make_double2(sc * (x.x - y.y), -sc * (x.y + y.x));
+            } else if (valid && k > N - M) {
+                const long long kk = N - k;
+                const double2 x = X[q + kk * P], y = Y ? Y[q + kk * P] : make_double2(0.0, 0.0);
+                z = make_double2(sc * (x.x + y.y), -sc * (y.x - x.y));
+            }
+            a[n1] = z;
+        }
+        __syncthreads();
+        fft_step1<R, TQ>(a, wk, tw, c, g);
+        __syncthreads();
+        fft_step2<R, TQ>(wk, a, tw, c, g);
+#pragma unroll
+        for (int k2 = 0; k2 < R; ++k2) {
+            xr[k2] = a[k2].x;
+            yr[k2] = -a[k2].y;
+        }
+    };
+    double uu[R], vv[R], ww[R], r1[R], r2[R], r3[R], s1[R], s2[R];
+    ifft_pair(p.u, p.v, 1.0, uu, vv);
+    ifft_pair(p.w, nullptr, 1.0, ww, s1);
+    ifft_pair(p.S[0], p.S[1], 0.5, s1, s2);          // S11, S22
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        r1[k] = uu[k] * s1[k];
+        r2[k] = vv[k] * s2[k];
+    }
+    ifft_pair(p.S[2], p.S[3], 0.5, s1, s2);          // S33, S12
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        r3[k] = ww[k] * s1[k];
+        r1[k] += vv[k] * s2[k];
+        r2[k] += uu[k] * s2[k];
+    }
+    ifft_pair(p.S[4], p.S[5], 0.5, s1, s2);          // S13, S23
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        r1[k] += ww[k] * s1[k];
+        r3[k] += uu[k] * s1[k] + vv[k] * s2[k];
+        r2[k] += ww[k] * s2[k];
+    }
+    const double sc = 1.0 / N;
+    for (int pair = 0; pair < 2; ++pair) {
+#pragma unroll
+        for (int k2 = 0; k2 < R; ++k2) a[k2] = pair == 0 ? make_double2(r1[k2], r2[k2]) : make_double2(r3[k2], 0.0);
+        __syncthreads();
+        fft_step1<R, TQ>(a, wk, tw, c, g);
+        __syncthreads();
+        fft_step2<R, TQ>(wk, a, tw, c, g);
+#pragma unroll
+        for (int k2 = 0; k2 < R; ++k2) xs[(c + R * k2) * TQ + g] = a[k2];
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < M * TQ; idx += NT) {
+            const int i = idx / TQ, gg = idx - i * TQ;
+            const long long qq = q0 + gg;
+            if (qq >= P) continue;
+            const double2 X = xs[i * TQ + gg], Y = xs[(i == 0 ? 0 : N - i) * TQ + gg];
+            const double wgt = (i == 0) ? sc : 2.0 * sc;   // W Spec
+            const double2 A = make_double2(0.5 * wgt * (X.x + Y.x), 0.5 * wgt * (X.y - Y.y));
+            const double2 B = make_double2(0.5 * wgt * (X.y + Y.y), -0.5 * wgt * (X.x - Y.x));
+            const long long e = qq + (long long)i * P;
+            double2 *o0 = p.ub[pair == 0 ? 0 : 2];
+            double2 t0 = o0[e];
+            o0[e] = make_double2(t0.x + A.x, t0.y + A.y);
+            if (pair == 0) {
+                double2 t1 = p.ub[1][e];
+                p.ub[1][e] = make_double2(t1.x + B.x, t1.y + B.y);
+            }
+        }
+    }
+}
+
+template <int R, int TQ>
+static int launch_advx_adj(ductgpu_ctx ctx, const AdjAdvParams &p)
+{
+    constexpr int N = R * R, NT = R * TQ;
+    const double2 *tw = twiddle_table(ctx, N);
+    if (!tw) return set_error(ctx, DUCTGPU_ESTATE, "adjoint advection: twiddle table unavailable");
+    const size_t smem = ((size_t)N + 2 * (size_t)N * TQ) * sizeof(double2);
+    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_advx_adj<R, TQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_ADVECTION);
+        k_advx_adj<R, TQ><<<(unsigned)((p.P + TQ - 1) / TQ), NT, smem, ctx->stream>>>(p, tw);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "k_advx_adj");
+}
+
+static int advx_adj_launch(ductgpu_ctx ctx, const AdjAdvParams &p, int mgalx)
+{
+    switch (mgalx) {
+    case 16: return launch_advx_adj<4, 32>(ctx, p);
+    case 64: return launch_advx_adj<8, 16>(ctx, p);
+    case 144: return launch_advx_adj<12, 8>(ctx, p);
+    case 256: return launch_advx_adj<16, 8>(ctx, p);
+    default: return set_error(ctx, DUCTGPU_EARG, "adjoint advection: mgalx=%d", mgalx);
+    }
+}
+
+// Work fields of the reverse sweep (offsets in fields of fdoubles).
+enum AdjSlot {
+    kSave = 0,          // u, v, w, p at the start (restored after the sweep)
+    kCk = 4,            // 3 substeps x (u, v, w) entry velocities
+    kUb = 13,           // u_, v_, w_, p_
+    kAnext = 17,        // 3: cotangent of A_{k} from substep k + 1
+    kAcur = 20,         // 3: total cotangent of this substep's A_k
+    kHb = 23,           // 3: cotangents of the solves' right-hand sides
+    kPhib = 26, kRb = 27,
+    kS = 28,            // 6: Q_mj + Q_jm
+    kFb = 34,           // 3: dJ/df
+    kE = 37,            // 2 planes: unit vectors, operator (set-up of D1, D2)
+    kAdjFields = 38
+};
+
+static int dns_adj_ensure(ductgpu_dns d)
+{
+    ductgpu_ctx ctx = d->ctx;
+    if (d->adj) return DUCTGPU_OK;
+    if (cudaMalloc(&d->adj, sizeof(double) * d->fdoubles * kAdjFields) != cudaSuccess ||
+        cudaMalloc(&d->dmat, sizeof(double) * 2 * d->my * d->my) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(ctx, DUCTGPU_EALLOC, "dns gradient: work fields");
+    }
+    // D1, D2: the line kernel applied to the unit vectors of one plane
+    const int m = d->my;
+    double *E = d->adj + kE * d->fdoubles, *O = E + 2ull * m * m;
+    k_unit_plane<<<(m * m + 255) / 256, 256, 0, ctx->stream>>>(reinterpret_cast<double2 *>(E), m);
+    for (int ord = 1; ord <= 2; ++ord) {
+        LineParams py = line_params('y', m, m, 1, d->xalp);
+        add_job(py, E, {line_out(O, ord, 1.0, 0.0)});
+        int rc = lines_launch(ctx, py);
+        if (rc) return rc;
+        k_real_part<<<(m * m + 255) / 256, 256, 0, ctx->stream>>>(reinterpret_cast<const double2 *>(O),
+                                                                  d->dmat + (size_t)(ord - 1) * m * m, (long long)m * m);
+    }
+    ctx->launches += 3;
+    return check_cuda(ctx, cudaGetLastError(), "dns gradient set-up");
+}
+
+// out = beta out + fac D_ord^T in along dir
+static int mat_t(ductgpu_dns d, int ord, char dir, const double *in, double *out, double fac, double beta)
+{
+    ductgpu_ctx ctx = d->ctx;
+    const long long total = d->P * d->M;
+    int blocks = (int)((total + 255) / 256);
+    if (blocks > 8 * ctx->num_sms) blocks = 8 * ctx->num_sms;
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_LINES);
+        k_lines_mat_t<<<blocks, 256, 0, ctx->stream>>>(d->dmat + (size_t)(ord - 1) * d->my * d->my, d->my,
+                                                       reinterpret_cast<const double2 *>(in),
+                                                       reinterpret_cast<double2 *>(out), d->my, d->my, d->M,
+                                                       dir == 'y', fac, beta, 1);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "k_lines_mat_t");
+}
+
+// out = sigma (beta out + sum_t (c0 + c1 i kx + c2 (i kx)^2) src_t) (pointwise)
+struct PTerm {
+    const double *src;
+    double c0, c1, c2;
+};
+static int pointwise(ductgpu_dns d, double *out, double beta, std::initializer_list<PTerm> terms)
+{
+    LineParams p = line_params('y', d->my, d->my, d->M, d->xalp, 1);
+    LineOut o = line_out(out, 0, 0.0, beta);
+    for (const PTerm &t : terms) xterm(o, t.src, t.c0, t.c1, t.c2);
+    add_job(p, nullptr, {o});
+    return lines_launch(d->ctx, p);
+}
+
+static int dns_adj_solve(ductgpu_dns d, char bound, const double *const *g, double *const *out, int n, int k)
+{
+    ductgpu_ctx ctx = d->ctx;
+    FieldTask t[3];
+    for (int c = 0; c < n; ++c) {
+        t[c].rhs = const_cast<double *>(g[c]);
+        t[c].sol = out[c];
+        t[c].nmodes = d->M;
+        t[c].mode0 = 1;
+        t[c].bound = bound;
+        t[c].plane0 = c * d->M;
+        t[c].refine = 1;
+    }
+    double *saved = ctx->lam, *saved_h = ctx->lam_host;
+    ctx->lam = bound == 'n' ? d->lam_n : d->lam_d[k];
+    ctx->lam_host = bound == 'n' ? d->lamh_n.data() : d->lamh_d[k].data();
+    const int rc = solve_adjoint(ctx, t, n);
+    ctx->lam = saved;
+    ctx->lam_host = saved_h;
+    return rc;
+}
+
+static int dns_gradient(ductgpu_dns d, double *J)
+{
+    ductgpu_ctx ctx = d->ctx;
+    int rc = dns_adj_ensure(d);
+    if (rc) return rc;
+    const size_t F = d->fdoubles, fb = sizeof(double) * F;
+    const int m = d->my, M = d->M;
+    const double nu = d->fnu, dt = d->dt, asp = d->aspect;
+    double *W = d->adj;
+    auto slot = [&](int s) { return W + (size_t)s * F; };
+    double *vel[4] = {d->vel[0], d->vel[1], d->vel[2], d->p};
+    for (int c = 0; c < 4; ++c) DUCT_CUDA(ctx, cudaMemcpyAsync(slot(kSave + c), vel[c], fb, cudaMemcpyDeviceToDevice, ctx->stream));
+    // forward step with the substeps' entry velocities kept
+    for (int krk = 1; krk <= 3; ++krk) {
+        for (int c = 0; c < 3; ++c)
+            DUCT_CUDA(ctx, cudaMemcpyAsync(slot(kCk + 3 * (krk - 1) + c), d->vel[c], fb, cudaMemcpyDeviceToDevice,
+                                           ctx->stream));
+        if ((rc = dns_issue(d, krk, false))) return rc;
+    }
+    // J = sum of the four wall stresses of the final u
+    {
+        const double *f[4] = {d->vel[0], nullptr, nullptr, nullptr};
+        double *out = d->partial + (size_t)kStatBlocksMax * kStatVals;   // the scratch row
+        if ((rc = stats_issue(ctx, f, 1, d->wcc, d->wst, nullptr, nullptr, d->partial, out, nullptr, 0, d->P, 1,
+                              asp)))
+            return rc;
+        double s4[4];
+        DUCT_CUDA(ctx, cudaMemcpyAsync(s4, out, sizeof(s4), cudaMemcpyDeviceToHost, ctx->stream));
+        DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        *J = s4[0] + s4[1] + s4[2] + s4[3];
+    }
+    // reverse sweep
+    DUCT_CUDA(ctx, cudaMemsetAsync(slot(kUb), 0, 4 * fb, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemsetAsync(slot(kAnext), 0, 3 * fb, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemsetAsync(slot(kFb), 0, 3 * fb, ctx->stream));
+    k_seed_wall<<<(unsigned)((d->P + 255) / 256), 256, 0, ctx->stream>>>(reinterpret_cast<double2 *>(slot(kUb)), d->wst,
+                                                                         d->P);
+    ctx->launches += 1;
+    double *ub[3] = {slot(kUb), slot(kUb + 1), slot(kUb + 2)}, *pb = slot(kUb + 3);
+    double *an[3] = {slot(kAnext), slot(kAnext + 1), slot(kAnext + 2)};
+    double *ac[3] = {slot(kAcur), slot(kAcur + 1), slot(kAcur + 2)};
+    double *hb[3] = {slot(kHb), slot(kHb + 1), slot(kHb + 2)};
+    double *phib = slot(kPhib), *rb = slot(kRb), *fbar[3] = {slot(kFb), slot(kFb + 1), slot(kFb + 2)};
+    double *S[6];
+    for (int i = 0; i < 6; ++i) S[i] = slot(kS + i);
+    for (int krk = 3; krk >= 1; --krk) {
+        const int k = krk - 1;
+        const double a = kAkk[k], b = kBkk[k], gm = kGkk[k], rho = kRkk[k];
+        const double f1 = (a + b) * dt * nu, s2 = -dt * (a + b), sdiv = 1.0 / ((a + b) * dt), sig = -1.0 / (nu * b);
+        // (mass flow)
+        if (d->cmassflow) {
+            LaunchScope ls(ctx, DUCTGPU_K_OTHER);
+            k_mf_adj<<<1, 1024, 0, ctx->stream>>>(reinterpret_cast<double2 *>(ub[0]), ctx->ccw, m, ctx->mf_aspect,
+                                                   ctx->mf_u + (size_t)m * m * k, ctx->mf_f + k);
+        }
+        // (update) phi_ = (I - f1 Lap)^T p_ + s2 grad^T u_
+        if ((rc = pointwise(d, phib, 0.0, {{pb, 1.0, 0.0, -f1}, {ub[0], 0.0, -s2, 0.0}}))) return rc;
+        if ((rc = mat_t(d, 2, 'y', pb, phib, -f1, 1.0))) return rc;
+        if ((rc = mat_t(d, 2, 'z', pb, phib, -f1 / (asp * asp), 1.0))) return rc;
+        if ((rc = mat_t(d, 1, 'y', ub[1], phib, s2, 1.0))) return rc;
+        if ((rc = mat_t(d, 1, 'z', ub[2], phib, s2 / asp, 1.0))) return rc;
+        // (pressure) r_ = S_n^T phi_ ; u*_ += sdiv grad^T r_
+        {
+            const double *g[1] = {phib};
+            double *o[1] = {rb};
+            if ((rc = dns_adj_solve(d, 'n', g, o, 1, k))) return rc;
+        }
+        if ((rc = pointwise(d, ub[0], 1.0, {{rb, 0.0, -sdiv, 0.0}}))) return rc;
+        if ((rc = mat_t(d, 1, 'y', rb, ub[1], sdiv, 1.0))) return rc;
+        if ((rc = mat_t(d, 1, 'z', rb, ub[2], sdiv / asp, 1.0))) return rc;
+        // (predictor) h_ = S_d^T u*_ ; the right-hand side's cotangent is sig h_
+        {
+            const double *g[3] = {ub[0], ub[1], ub[2]};
+            if ((rc = dns_adj_solve(d, 'd', g, hb, 3, k))) return rc;
+        }
+        // p_ -= (a+b) sig grad^T h_
+        if ((rc = pointwise(d, pb, 1.0, {{hb[0], 0.0, (a + b) * sig, 0.0}}))) return rc;
+        if ((rc = mat_t(d, 1, 'y', hb[1], pb, -(a + b) * sig, 1.0))) return rc;
+        if ((rc = mat_t(d, 1, 'z', hb[2], pb, -(a + b) * sig / asp, 1.0))) return rc;
+        for (int c = 0; c < 3; ++c) {
+            // A_k's cotangent; the previous substep's; f_; u_ entering the substep
+            if ((rc = pointwise(d, ac[c], 0.0, {{an[c], 1.0, 0.0, 0.0}, {hb[c], -gm * sig, 0.0, 0.0}}))) return rc;
+            if ((rc = pointwise(d, an[c], 0.0, {{hb[c], -rho * sig, 0.0, 0.0}}))) return rc;
+            if ((rc = pointwise(d, fbar[c], 1.0, {{hb[c], (a + b) * sig, 0.0, 0.0}}))) return rc;
+            if ((rc = pointwise(d, ub[c], 0.0, {{hb[c], sig / dt, 0.0, sig * a * nu}}))) return rc;
+            if ((rc = mat_t(d, 2, 'y', hb[c], ub[c], sig * a * nu, 1.0))) return rc;
+            if ((rc = mat_t(d, 2, 'z', hb[c], ub[c], sig * a * nu / (asp * asp), 1.0))) return rc;
+        }
+        // (advection) S_mj = Q_mj + Q_jm, Q_ij = d_j^T A_i
+        if ((rc = pointwise(d, S[0], 0.0, {{ac[0], 0.0, -2.0, 0.0}}))) return rc;          // 2 Q11
+        if ((rc = mat_t(d, 1, 'y', ac[1], S[1], 2.0, 0.0))) return rc;                       // 2 Q22
+        if ((rc = mat_t(d, 1, 'z', ac[2], S[2], 2.0 / asp, 0.0))) return rc;                 // 2 Q33
+        if ((rc = pointwise(d, S[3], 0.0, {{ac[1], 0.0, -1.0, 0.0}}))) return rc;          // Q21
+        if ((rc = mat_t(d, 1, 'y', ac[0], S[3], 1.0, 1.0))) return rc;                       // + Q12
+        if ((rc = pointwise(d, S[4], 0.0, {{ac[2], 0.0, -1.0, 0.0}}))) return rc;          // Q31
+        if ((rc = mat_t(d, 1, 'z', ac[0], S[4], 1.0 / asp, 1.0))) return rc;                 // + Q13
+        if ((rc = mat_t(d, 1, 'y', ac[2], S[5], 1.0, 0.0))) return rc;                       // Q32
+        if ((rc = mat_t(d, 1, 'z', ac[1], S[5], 1.0 / asp, 1.0))) return rc;                 // + Q23
+        AdjAdvParams ap{};
+        ap.u = reinterpret_cast<const double2 *>(slot(kCk + 3 * k));
+        ap.v = reinterpret_cast<const double2 *>(slot(kCk + 3 * k + 1));
+        ap.w = reinterpret_cast<const double2 *>(slot(kCk + 3 * k + 2));
+        for (int i = 0; i < 6; ++i) ap.S[i] = reinterpret_cast<const double2 *>(S[i]);
+        for (int c = 0; c < 3; ++c) ap.ub[c] = reinterpret_cast<double2 *>(ub[c]);
+        ap.P = d->P;
+        ap.M = M;
+        if ((rc = advx_adj_launch(ctx, ap, d->mgalx))) return rc;
+    }
+    // the state as it was
+    for (int c = 0; c < 4; ++c) DUCT_CUDA(ctx, cudaMemcpyAsync(vel[c], slot(kSave + c), fb, cudaMemcpyDeviceToDevice, ctx->stream));
+    return check_cuda(ctx, cudaGetLastError(), "dns gradient");
+}
+
+}  // namespace duct
+
+extern "C" int ductgpu_dns_set_forcing(ductgpu_dns d, const double *f1, const double *f2, const double *f3)
+{
+    if (!d) return DUCTGPU_EARG;
+    ductgpu_ctx ctx = d->ctx;
+    cudaSetDevice(ctx->device);
+    const bool on = f1 || f2 || f3;
+    if (on && !d->force && cudaMalloc(&d->force, sizeof(double) * 3 * d->fdoubles) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(ctx, DUCTGPU_EALLOC, "dns_set_forcing: 3 fields");
+    }
+    const double *src[3] = {f1, f2, f3};
+    for (int c = 0; c < 3 && on; ++c) {
+        double *dst = d->force + c * d->fdoubles;
+        if (src[c]) DUCT_CUDA(ctx, cudaMemcpyAsync(dst, src[c], sizeof(double) * d->fdoubles, cudaMemcpyDefault, ctx->stream));
+        else DUCT_CUDA(ctx, cudaMemsetAsync(dst, 0, sizeof(double) * d->fdoubles, ctx->stream));
+    }
+    if (on != d->forced) dns_drop_graphs(d);   // the substep graphs were captured with the other choice
+    d->forced = on;
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "dns_set_forcing");
+}
+
+extern "C" int ductgpu_dns_grad_wallstress(ductgpu_dns d, double *J, double *fbar)
+{
+    if (!d || !J) return DUCTGPU_EARG;
+    ductgpu_ctx ctx = d->ctx;
+    cudaSetDevice(ctx->device);
+    int rc = dns_gradient(d, J);
+    if (rc) return rc;
+    if (fbar)
+        DUCT_CUDA(ctx, cudaMemcpyAsync(fbar, d->adj + (size_t)kFb * d->fdoubles, sizeof(double) * 3 * d->fdoubles,
+                                       cudaMemcpyDefault, ctx->stream));
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "dns_grad_wallstress");
+}
+
+// J = the four-wall stress of u after nsteps RK3 steps from the current
+// state (left unchanged): the functional the gradient differentiates.
+extern "C" int ductgpu_dns_wallstress_after(ductgpu_dns d, int nsteps, double *J)
+{
+    if (!d || !J || nsteps < 0) return DUCTGPU_EARG;
+    ductgpu_ctx ctx = d->ctx;
+    cudaSetDevice(ctx->device);
+    int rc = dns_adj_ensure(d);
+    if (rc) return rc;
+    const size_t fb = sizeof(double) * d->fdoubles;
+    double *vel[4] = {d->vel[0], d->vel[1], d->vel[2], d->p};
+    for (int c = 0; c < 4; ++c)
+        DUCT_CUDA(ctx, cudaMemcpyAsync(d->adj + (size_t)(kSave + c) * d->fdoubles, vel[c], fb, cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
+    for (int s = 0; s < nsteps; ++s)
+        for (int krk = 1; krk <= 3; ++krk)
+            if ((rc = dns_issue(d, krk, false))) return rc;
+    const double *f[4] = {d->vel[0], nullptr, nullptr, nullptr};
+    double *out = d->partial + (size_t)kStatBlocksMax * kStatVals;
+    if ((rc = stats_issue(ctx, f, 1, d->wcc, d->wst, nullptr, nullptr, d->partial, out, nullptr, 0, d->P, 1,
+                          d->aspect)))
+        return rc;
+    double s4[4];
+    DUCT_CUDA(ctx, cudaMemcpyAsync(s4, out, sizeof(s4), cudaMemcpyDeviceToHost, ctx->stream));
+    for (int c = 0; c < 4; ++c)
+        DUCT_CUDA(ctx, cudaMemcpyAsync(vel[c], d->adj + (size_t)(kSave + c) * d->fdoubles, fb, cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *J = s4[0] + s4[1] + s4[2] + s4[3];
     return DUCTGPU_OK;
 }

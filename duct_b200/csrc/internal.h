@@ -330,7 +330,7 @@ int transpose_dev(ductgpu_ctx ctx, const double *in, double *out, long long A, l
 // with D the reference's derivyz between transyz -1 / +1 along the launch's
 // direction (fac already divided by aspect^order for z).  maxabs (device,
 // or null): atomic max of |out| over the interior points.
-constexpr int kLineXTerms = 4;
+constexpr int kLineXTerms = 5;
 constexpr int kMaxLineOut = 3;
 constexpr int kMaxLineJobs = 4;
 struct LineOut {

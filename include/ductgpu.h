@@ -467,6 +467,26 @@ int ductgpu_dns_steps(ductgpu_dns dns, int nsteps, int stats_every);
  * after each substep of the last step.  Synchronises.                    */
 int ductgpu_dns_statistics(ductgpu_dns dns, double *mean, double *prod, double *ppb, double *spec,
                            double *hist, int *nstat, int *nhist, double *divmax3);
+/* Body force f = (f1, f2, f3) (complex (my,my,nmodes) fields, host or
+ * device; copied): it enters the substep's right-hand side like the
+ * pressure gradient and the reference's forcings (src/main1.f90 (vi-b),
+ * force_global / add_puff_forcing with -(akk+bkk)): h += (akk+bkk) f.
+ * All NULL removes it.                                                    */
+int ductgpu_dns_set_forcing(ductgpu_dns dns, const double *f1, const double *f2, const double *f3);
+/* J = the wall stress of u summed over the four walls (wallstressx,
+ * src/operators.F:676-710) after nsteps RK3 steps from the current state;
+ * the state is left as it was.                                            */
+int ductgpu_dns_wallstress_after(ductgpu_dns dns, int nsteps, double *J);
+/* Reverse mode through one RK3/CN step from the current state (left as it
+ * was): J as above after one step, and fbar = dJ/df (3 complex fields,
+ * host or device; the gradient in the coefficient inner product
+ * Re sum conj(a) b, i.e. dJ/dRe f + i dJ/dIm f per coefficient).  The
+ * discrete adjoint of the GPU step: adjoint solves (transposed eigenbasis),
+ * transposed derivative matrices, the transposed advection products
+ * linearised at the substeps' entry velocities (in-memory checkpoints of
+ * the forward sweep), the mass-flow correction transposed.  Synchronises.
+ * No counterpart in the reference (it has no adjoint).                    */
+int ductgpu_dns_grad_wallstress(ductgpu_dns dns, double *J, double *fbar);
 
 /* ---- the reference's own GPU entry points (src/mytranspose_cuda.cu) --- */
 /* transpose_gpu_(handle,Nx,Ny,alpha,devPtrA,devPtrC) and

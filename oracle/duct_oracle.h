@@ -218,6 +218,6 @@ double orc_dns_substep(double *u, double *v, double *w, double *p, double *adv1,
                        double *h1, double *h2, double *h3, int my, int mz, int M, int mgalx, const double *xalp,
                        double aspect, double fnu, double dt, int krk, const orc_ops *ops, int cmassflow,
                        double csum, const double *premassfu, const double *premassf, double dpdx,
-                       orc_dns_stats *stats, int nthreads);
+                       orc_dns_stats *stats, int nthreads, const double *force);
 
 #endif

@@ -434,7 +434,7 @@ double orc_dns_substep(double *u, double *v, double *w, double *p, double *adv1,
                        double *h1, double *h2, double *h3, int my, int mz, int M, int mgalx, const double *xalp,
                        double aspect, double fnu, double dt, int krk, const orc_ops *ops, int cmassflow,
                        double csum, const double *premassfu, const double *premassf, double dpdx,
-                       orc_dns_stats *stats, int nthreads)
+                       orc_dns_stats *stats, int nthreads, const double *force)
 {
     const size_t nf = 2 * (size_t)my * mz * M;
     const int k = krk - 1;
@@ -467,6 +467,11 @@ double orc_dns_substep(double *u, double *v, double *w, double *p, double *adv1,
     for (int c = 0; c < 3; ++c) daxpy_((long)nf, 1.0 / dt, vel[c], h[c]);
     /* (vi) h += -(alpha_k + beta_k) grad p */
     orc_grad3d(p, h1, h2, h3, my, mz, M, xalp, aspect, -(akkc[k] + bkkc[k]), '+');
+    /* (vi-b) a body force f (3 fields, or NULL) enters like the pressure
+     * gradient and the reference's forcings (force_global / add_puff_forcing
+     * with scale -(akk+bkk)): h += (akk+bkk) f */
+    if (force)
+        for (int c = 0; c < 3; ++c) daxpy_((long)nf, akkc[k] + bkkc[k], force + (size_t)c * nf, h[c]);
     /* (vi-b) mean pressure gradient on mode 0 of x-momentum (not CMASSFLOW) */
     if (!cmassflow) {
         const double t = -(akkc[k] + bkkc[k]) * dpdx;

@@ -371,7 +371,7 @@ def _dns_sigs(L):
     L.orc_statistics_fou.argtypes = [P, P, P, P, I, I, I, P, P, P]
     L.orc_rk_coefficients.argtypes = [P, P, P, P]
     L.orc_dns_substep.argtypes = [P, P, P, P, P, P, P, P, P, P, I, I, I, I, P, D, D, D, I, C.POINTER(_Ops), I,
-                                  D, P, P, D, C.POINTER(_DnsStats), I]
+                                  D, P, P, D, C.POINTER(_DnsStats), I, P]
     L.orc_dns_substep.restype = D
 
 
@@ -533,6 +533,11 @@ class Dns:
         self._st.spec = self.stats_spec.ctypes.data_as(C.POINTER(C.c_double))
         self.history = []
         self.divmax = None
+        self.force = None
+
+    def set_forcing(self, f=None):
+        """Body force (f1, f2, f3), h += (akk+bkk) f in every substep; None removes it."""
+        self.force = None if f is None else np.asfortranarray(np.stack([_cf(x) for x in f], axis=3))
 
     def substep(self, krk, stats=False):
         L = _dlib()
@@ -541,7 +546,7 @@ class Dns:
             _p(self.h[0]), _p(self.h[1]), _p(self.h[2]), self.my, self.my, self.M, self.mgalx, _p(self.xalp),
             self.aspect, self.fnu, self.dt, int(krk), C.byref(self.ops._s), int(self.cmassflow), float(self.csum),
             _p(self.premassfu), _p(self.premassf), self.dpdx, C.byref(self._st) if stats else None,
-            self.nthreads)
+            self.nthreads, None if self.force is None else _p(self.force))
         if stats and krk == 1:
             self.history.append(dict(stress4=list(self._st.stress4), energy=list(self._st.energy),
                                      energy2=list(self._st.energy2)))
