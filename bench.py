@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-transforms", action="store_true")
     ap.add_argument("--no-dns", action="store_true", help="skip the config-4 DNS steps/s block")
+    ap.add_argument("--dns-only", action="store_true",
+                    help="only the config-4 DNS block (one GPU; with --dns-steps for short profiling runs)")
+    ap.add_argument("--dns-steps", type=int, default=None, help="timed DNS steps (default: the config's 200)")
     ap.add_argument("--pass-kernel", default="auto", choices=["auto", "staged-32", "staged-16", "register", "persist", "parity"],
                     help="GEMM-pass kernel; auto runs the library's autotuner (profiling runs fix it, since "
                          "the autotuner's timing under a profiler is not the live one)")
@@ -592,7 +595,7 @@ def dns_cfg4(args, local, with_cpu):
     cfg = synth.dns_config("cfg4")
     m, mg, alp, dt = cfg["my"], cfg["mgalx"], cfg["alp"], cfg["dt"]
     fnu = Q_LAMINAR / (4.0 * cfg["re_b"])
-    nsteps = cfg["steps"]
+    nsteps = cfg["steps"] if args.dns_steps is None else args.dns_steps
     u, v, w, p, _ = synth.dns_initial(mg, m, alp, cfg["amp"], seed=4)
     out = {"config": "cfg4: mgalx=256 (85 modes) x 193 x 193, Lx=4pi, Re_b=4400, dt=2e-4, 10%% perturbation, "
                      "CMASSFLOW, statistics every step, FP64 solves", "steps": nsteps, "warmup": 3}
@@ -847,6 +850,9 @@ def main():
         import duct_b200 as D
         with D.Context(0) as ctx:
             print(json.dumps(transform_rates(ctx)), flush=True)
+        return
+    if args.dns_only:
+        print(json.dumps({"cfg4_dns": dns_cfg4(args, 0, not args.no_cpu)}), flush=True)
         return
     world, rank, local, pg = dist_setup(args)
     try:

@@ -67,7 +67,11 @@ template <int R2, int N, int W, bool DOUBLE_ENDS>
 __device__ __forceinline__ void pre_seg(double2 *xl, const double2 *src, const double2 *ha, double2 *f1, int s)
 {
     double sx = 0.0, sy = 0.0;
-    for (int j = 1 + s; j < N / 2; j += W) {
+    constexpr int IT = (N / 2 - 1 + W - 1) / W;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int j = 1 + s + it * W;
+        if (j >= N / 2) break;
         const double2 a = src ? src[j] : xl[at<R2>(j)], b = src ? src[N - j] : xl[at<R2>(N - j)];
         const double2 u = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y + b.y));
         const double2 v = make_double2(a.x - b.x, a.y - b.y);
@@ -139,7 +143,10 @@ __device__ __forceinline__ void post_seg(double2 *xl, double2 *nat, double2 f1, 
     constexpr int CH = odd_chunk(N / 2 + 1, W);
     const int k0 = s * CH, k1 = min(N / 2 + 1, k0 + CH);
     double sx = 0.0, sy = 0.0;
-    for (int k = k0; k < k1; ++k) {
+#pragma unroll
+    for (int i = 0; i < CH; ++i) {
+        const int k = k0 + i;
+        if (k >= k1) break;
         if (k == 0 || k == N / 2) continue;
         const double2 gk = xl[at<R2>(k)], gm = xl[at<R2>(N - k)];
         sx -= 0.5 * (gk.y - gm.y);
@@ -156,7 +163,10 @@ __device__ __forceinline__ void post_seg(double2 *xl, double2 *nat, double2 f1, 
     }
     double rx = f1.x + ix - sx, ry = f1.y + iy - sy;
     constexpr double s_in = 2.0 / N, s_end = 1.0 / N;
-    for (int k = k0; k < k1; ++k) {
+#pragma unroll
+    for (int i = 0; i < CH; ++i) {
+        const int k = k0 + i;
+        if (k >= k1) break;
         const double2 gk = xl[at<R2>(k)], gm = xl[at<R2>(k == 0 ? 0 : N - k)];
         const double2 fe = make_double2(0.5 * (gk.x + gm.x), 0.5 * (gk.y + gm.y));
         if (k > 0 && k < N / 2) {
@@ -191,7 +201,10 @@ __device__ __forceinline__ void rec_seg(double2 *c, int s)
     constexpr int CH = odd_chunk(N, W);
     const int k0 = 1 + s * CH, k1 = min(N + 1, k0 + CH);
     double2 se = make_double2(0.0, 0.0), so = se, top = se;
-    for (int k = k0; k < k1; ++k) {
+#pragma unroll
+    for (int i = 0; i < CH; ++i) {
+        const int k = k0 + i;
+        if (k >= k1) break;
         const double2 v = c[k];
         const double f = 2.0 * k;
         if (k & 1) { so.x += f * v.x; so.y += f * v.y; }
@@ -211,7 +224,10 @@ __device__ __forceinline__ void rec_seg(double2 *c, int s)
     double2 re = make_double2(ie.x - se.x, ie.y - se.y), ro = make_double2(io.x - so.x, io.y - so.y);
     __syncwarp();
     double2 cur = top;
-    for (int k = k1 - 1; k >= k0; --k) {
+#pragma unroll
+    for (int i = CH - 1; i >= 0; --i) {
+        const int k = k0 + i;
+        if (k >= k1) continue;
         const double2 v = cur;
         if (k > k0) cur = c[k - 1];   // read before this iteration overwrites it
         const double f = 2.0 * k;
@@ -249,6 +265,7 @@ __device__ __forceinline__ void store_seg(const LineOut &o, const double2 *xl, b
             xs[t] = o.xs[t] ? reinterpret_cast<const double2 *>(o.xs[t]) + lbase : nullptr;
         }
         const double m0 = (mode == 0) ? o.m0 : 0.0;
+#pragma unroll 4
         for (int j = s; j <= N; j += W) {
             const long long gi = (long long)j * es;
             double2 v = make_double2(m0, 0.0);
@@ -346,6 +363,7 @@ __global__ void __launch_bounds__(32 * WPB, 16 / WPB) k_lines(const __grid_const
     auto prefetch = [&](const Item &I) {
         if (I.act && needs_input(I.job)) {
             const double2 *in = reinterpret_cast<const double2 *>(p.job[I.job].in) + I.lbase;
+#pragma unroll
             for (int j = s; j <= N; j += W) cp_async16(cl + j, in + (long long)j * es);
         }
         asm volatile("cp.async.commit_group;\n" ::);
