@@ -682,9 +682,10 @@ def uneven_rect_rate(ctx, args):
     """The uneven batch of rectangular ducts (aspect 1-4 at (65,65), (65,129),
     (49,145), (33,129) with 32, 48, 64, 96 modes; u, v, w Dirichlet with
     lambda = kx^2 + 2/(nu dt), nu = 1/4400, dt = 5e-4, and the Neumann
-    pressure with lambda = kx^2, kx = k): 16 fields in one batched call, one
-    launch per GEMM pass, replayed from a CUDA graph; FP64 passes on the full
-    operators.  Inputs (180 MB) exceed L2."""
+    pressure with lambda = kx^2, kx = k): 16 fields in one batched call,
+    replayed from a CUDA graph; FP64 passes on the flip-symmetric half blocks
+    (every duct has matching walls per direction), and on the full operators
+    for comparison.  Inputs (180 MB) exceed L2."""
     import duct_b200 as D
     from duct_b200 import synth
     ducts = (((65, 65), 1.0, 32), ((65, 129), 2.0, 48), ((49, 145), 3.0, 64), ((33, 129), 4.0, 96))
@@ -702,25 +703,35 @@ def uneven_rect_rate(ctx, args):
             keep += [r, o]
             fields.append(dict(rhs=r, sol=o, xalp=xalp, alambda=0.0 if neu else h, ib=0,
                                slot=(4 + slot) if neu else slot))
-    gid = ctx.graph_create(fields, rect=True)
-    for _ in range(max(3, args.warmup)):
-        ctx.graph_launch(gid)
-    ctx.synchronize()
-    steps = max(10, args.steps)
-    ctx.event_record(0)
-    for _ in range(steps):
-        ctx.graph_launch(gid)
-    ctx.event_record(1)
-    ms = ctx.event_elapsed(0, 1) / steps
-    ctx.synchronize()
-    ctx.graph_destroy(gid)
+    def timed(fold):
+        ctx.set_rect_fold(fold)
+        gid = ctx.graph_create(fields, rect=True)
+        for _ in range(max(3, args.warmup)):
+            ctx.graph_launch(gid)
+        ctx.synchronize()
+        steps = max(10, args.steps)
+        ctx.event_record(0)
+        for _ in range(steps):
+            ctx.graph_launch(gid)
+        ctx.event_record(1)
+        ms = ctx.event_elapsed(0, 1) / steps
+        ctx.synchronize()
+        ctx.graph_destroy(gid)
+        return ms, steps
+
+    ms_full, _ = timed(False)
+    ms, steps = timed(True)
+    ctx.set_rect_fold(True)
     for x in keep:
         x.free()
     per_step = 4 * sum(nm for _, _, nm in ducts)
     return {"value": per_step / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "mode_solves_per_step": per_step,
             "fields": len(fields), "steps": steps,
             "config": "4 rectangular ducts (65x65, 65x129, 49x145, 33x129; 32/48/64/96 modes) x (u, v, w, p)",
-            "step": "CUDA-graph replay of ductgpu_solve_rect_fields_dev (16 fields, one launch per pass)"}
+            "step": "CUDA-graph replay of ductgpu_solve_rect_fields_dev (16 fields): flip-symmetric half blocks, "
+                    "one launch per pass and half-block size (8 GEMM-pass launches)",
+            "full_operators": {"value": per_step / (ms_full * 1e-3), "ms_per_step": ms_full,
+                               "step": "the same on the full operators, one launch per GEMM pass"}}
 
 
 def torch_sm_count():

@@ -45,7 +45,7 @@ EXPORTS = [
     "ductgpu_dns_create", "ductgpu_dns_destroy", "ductgpu_dns_set_fields", "ductgpu_dns_get_fields",
     "ductgpu_dns_field", "ductgpu_dns_set_graphs", "ductgpu_dns_substep", "ductgpu_dns_steps",
     "ductgpu_dns_statistics", "ductgpu_profile_bytes", "ductgpu_dns_set_forcing",
-    "ductgpu_dns_wallstress_after", "ductgpu_dns_grad_wallstress",
+    "ductgpu_dns_wallstress_after", "ductgpu_dns_grad_wallstress", "ductgpu_set_rect_fold",
 ]
 SETUP_NO_EIGEN = 1
 (K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER, K_LINES,
@@ -157,6 +157,7 @@ def lib():
             "ductgpu_dns_statistics": [P, P, P, P, P, P, C.POINTER(I), C.POINTER(I), P],
             "ductgpu_profile_bytes": [P, I, C.POINTER(D)],
             "ductgpu_dns_set_forcing": [P, P, P, P],
+            "ductgpu_set_rect_fold": [P, I],
             "ductgpu_dns_wallstress_after": [P, I, C.POINTER(D)],
             "ductgpu_dns_grad_wallstress": [P, C.POINTER(D), P],
             "ductgpu_graph_destroy": [P, I],
@@ -295,6 +296,9 @@ class Context:
         out = C.c_int()
         self._check(lib().ductgpu_autotune(self.h, arr, len(fields), int(reps), C.byref(out)))
         return out.value
+
+    def set_rect_fold(self, on):
+        self._check(lib().ductgpu_set_rect_fold(self.h, int(bool(on))))
 
     def set_refinement(self, steps):
         self._check(lib().ductgpu_set_refinement(self.h, int(steps)))

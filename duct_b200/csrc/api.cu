@@ -413,6 +413,13 @@ int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel)
     return DUCTGPU_OK;
 }
 
+int ductgpu_set_rect_fold(ductgpu_ctx ctx, int on)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    ctx->rect_fold = on ? 1 : 0;
+    return DUCTGPU_OK;
+}
+
 int ductgpu_autotune(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, int reps, int *chosen)
 {
     if (!ctx) return DUCTGPU_EARG;

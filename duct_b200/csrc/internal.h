@@ -66,6 +66,7 @@ struct RectSlot {
     double *DY = nullptr, *D2Y = nullptr, *DZ = nullptr, *D2Z = nullptr;  // device
     double *wy = nullptr, *wz = nullptr;   // Clenshaw-Curtis weights (scaled)
     int sing_y = -1, sing_z = -1;          // argmin |E| per direction
+    int sing_yp = -1, sing_zp = -1;        // the same in the flip-symmetric (even-first) mode order
 };
 
 // Shen-Legendre operators of one wall condition (src/preshen.f90)
@@ -113,6 +114,7 @@ struct ductgpu_ctx_s {
     int refine_steps = 2;      // FP64 refinement steps of the split-precision path
     int parity_ws = 1;         // flip-symmetric passes at hpad 32 / 64: warp-specialised persistent kernel
     int i8_kernel = 1;         // int8-emulated passes: 0 sequential, 1 warp-specialised pipeline
+    int rect_fold = 1;         // rectangular solves on the flip-symmetric half blocks where both walls match
     // GEMM-pass kernel per operator size class (n <= 63, <= 127, <= 191),
     // one of DUCTGPU_PASS_* (ductgpu_set_pass_kernel, ductgpu_autotune);
     // defaults (kPassDefault) from measurements on B200 at n = 31, 63, 127,

@@ -589,6 +589,24 @@ int rect_setup(ductgpu_ctx ctx, int slot, int my, int mz, double sy, double sz, 
     for (int i = 1; i < r.y.n; ++i) if (fabs(ey[i]) < fabs(ey[r.sing_y])) r.sing_y = i;
     r.sing_z = 0;
     for (int i = 1; i < r.z.n; ++i) if (fabs(ez[i]) < fabs(ez[r.sing_z])) r.sing_z = i;
+    // flip-symmetric half blocks of a direction whose two walls match (the
+    // operator then commutes with the reflection of the nodes; fold_operators
+    // checks it), and the singular mode's place in their even-first order
+    auto fold_dir = [&](BoundOps &b, char w1, char w2, int &sing) -> int {
+        sing = -1;
+        if (w1 != w2) return DUCTGPU_OK;
+        int rc2 = fold_operators(ctx, b);
+        if (rc2 || !b.fold_ok) return rc2;
+        std::vector<double> ep(b.n);
+        DUCT_CUDA(ctx, cudaMemcpy(ep.data(), b.Eperm, b.n * sizeof(double), cudaMemcpyDeviceToHost));
+        sing = 0;
+        for (int i = 1; i < b.n; ++i) if (fabs(ep[i]) < fabs(ep[sing])) sing = i;
+        return DUCTGPU_OK;
+    };
+    if ((rc = fold_dir(r.y, by1, by2, r.sing_yp)) || (rc = fold_dir(r.z, bz1, bz2, r.sing_zp))) {
+        free_rect(r);
+        return rc;
+    }
     r.ready = true;
     return DUCTGPU_OK;
 }

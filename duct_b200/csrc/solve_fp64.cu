@@ -1060,8 +1060,12 @@ int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid)
         // the persistent warp-specialised form pays one operator load per
         // CTA: used when every SM gets several 16-line tiles
         long long tiles = 0;
-        for (int i = 0; i < pp.nf; ++i) tiles += (long long)pp.f[i].nmodes * ((pp.f[i].nlines + 15) / 16);
-        if (ctx->parity_ws && mtw <= 2 && tiles >= 6LL * ctx->num_sms) {
+        bool lines_fit = true;   // the persistent form stages the line eigenvalues in 2 hpad slots
+        for (int i = 0; i < pp.nf; ++i) {
+            tiles += (long long)pp.f[i].nmodes * ((pp.f[i].nlines + 15) / 16);
+            lines_fit = lines_fit && pp.f[i].nlines <= 2 * pp.f[i].kpad;
+        }
+        if (ctx->parity_ws && mtw <= 2 && lines_fit && tiles >= 6LL * ctx->num_sms) {
             e = fp64_pass_ws(ctx, pp, 32 * mtw);
             return e == cudaSuccess ? DUCTGPU_OK : check_cuda(ctx, e, "k_pass_fp64w");
         }

@@ -185,6 +185,11 @@ int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields,
                                      from ductgpu_set_operators, run STAGED)            */
 /* kernel -1 restores the library's defaults for the size class(es).      */
 int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel);
+/* Rectangular solves (ductgpu_helm3d_temp, ductgpu_solve_rect_fields_dev)
+ * on the flip-symmetric half blocks wherever both walls of each direction
+ * match (1, the default) or on the full operators (0).  Folded passes run
+ * one launch per half-block size of the pass direction.                  */
+int ductgpu_set_rect_fold(ductgpu_ctx ctx, int on);
 /* Autotuner: times the FP64 batched solve of these device fields with each
  * pass kernel (reps runs each, after one warm-up; the fields' sol arrays
  * are overwritten and Dirichlet rhs walls zeroed, as by the solve itself)

@@ -65,10 +65,14 @@ def test_all_neumann_singular_gauge(gpu_ctx, oracle):
     assert abs(oracle.cheb2_integral(c, aspect=b)) < 1e-11 * np.abs(gm).max()
 
 
-def test_uneven_batch_one_launch_per_pass(gpu_ctx, oracle):
+@pytest.mark.parametrize("fold", [False, True])
+def test_uneven_batch_one_launch_per_pass(gpu_ctx, oracle, fold):
     """The four ducts x (3 Dirichlet velocities + Neumann pressure) -- 16
-    fields -- in one batched call (one launch per GEMM pass) equal the
-    per-duct oracle solutions."""
+    fields -- in one batched call equal the per-duct oracle solutions: on
+    the full operators one launch per GEMM pass; on the flip-symmetric half
+    blocks one launch per pass and half-block size (y: all 32 rows; z: 32,
+    64 and 96 rows for mz = 65, 129, 145), 8 in all."""
+    gpu_ctx.set_rect_fold(fold)
     nu, dt = 1.0 / 4400.0, 5.0e-4
     h = 2.0 / (nu * dt)
     fields, refs = [], []
@@ -93,7 +97,8 @@ def test_uneven_batch_one_launch_per_pass(gpu_ctx, oracle):
     gpu_ctx.synchronize()
     ms, npass = gpu_ctx.profile_read(D.K_PASS_FP64)
     gpu_ctx.profile(False)
-    assert npass == 4            # one launch per GEMM pass for all ducts and fields
+    gpu_ctx.set_rect_fold(True)
+    assert npass == (8 if fold else 4)
     for f, (ref, neu) in zip(fields, refs):
         got = f["sol"].download()
         if neu:
