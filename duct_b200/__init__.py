@@ -297,6 +297,13 @@ class Context:
         self._check(lib().ductgpu_autotune(self.h, arr, len(fields), int(reps), C.byref(out)))
         return out.value
 
+    def apply_tuning(self, my, mz=None, path=None):
+        """The offline tuning table's settings for this grid (duct_b200/tune.py):
+        pass kernel of the size class, folded or full rectangular passes.
+        Returns the table entry, or None (library defaults kept)."""
+        from duct_b200 import tune
+        return tune.apply(self, int(my), int(mz if mz is not None else my), path or tune.TABLE)
+
     def set_rect_fold(self, on):
         self._check(lib().ductgpu_set_rect_fold(self.h, int(bool(on))))
 

@@ -105,8 +105,10 @@ __device__ __forceinline__ void pre_seg(double2 *xl, const double2 *src, const d
 // Length-N FFT of a line in place (N = R1 R2, R1, R2 <= W): lane n2 runs the
 // R1-point DFT of column n2 and applies W_N^(n2 k1), then lane k1 the
 // R2-point DFT of row k1.
+// twT[k1 R2 + n2] = W_N^(n2 k1): the inter-step twiddles laid out so that
+// the lanes of a segment (n2) read consecutive words.
 template <int R1, int R2, int W>
-__device__ __forceinline__ void fft_seg(double2 *xl, const double2 *tw, int s)
+__device__ __forceinline__ void fft_seg(double2 *xl, const double2 *tw, const double2 *twT, int s)
 {
     constexpr int N = R1 * R2;
     if (s < R2) {
@@ -115,7 +117,7 @@ __device__ __forceinline__ void fft_seg(double2 *xl, const double2 *tw, int s)
         for (int n1 = 0; n1 < R1; ++n1) v[n1] = xl[n1 * (R2 + 1) + s];
         reg_fft<R1, 0, 1>(v, tw, N);
 #pragma unroll
-        for (int k1 = 0; k1 < R1; ++k1) xl[k1 * (R2 + 1) + s] = (k1 == 0) ? v[0] : cmul(v[k1], tw[s * k1]);
+        for (int k1 = 0; k1 < R1; ++k1) xl[k1 * (R2 + 1) + s] = (k1 == 0) ? v[0] : cmul(v[k1], twT[k1 * R2 + s]);
     }
     __syncwarp();
     double2 w[R2];
@@ -319,9 +321,14 @@ __global__ void __launch_bounds__(32 * WPB, 16 / WPB) k_lines(const __grid_const
     constexpr int N = S::N, LS = S::LS, PL = S::PL, LPW = 32 / W, NT = 32 * WPB;
     extern __shared__ __align__(16) double2 sm[];
     double2 *tw = sm;                   // W_N^t, N entries
-    double2 *ha = tw + N;               // (cos, -sin)(pi j / N), j <= N/2
+    double2 *twT = tw + N;              // W_N^(n2 k1) at k1 R2 + n2, N entries
+    double2 *ha = twT + N;              // (cos, -sin)(pi j / N), j <= N/2
     double2 *lines = ha + (N / 2 + 1);  // [WPB * LPW][PL]
-    for (int t = threadIdx.x; t < N; t += NT) tw[t] = twg[t];
+    for (int t = threadIdx.x; t < N; t += NT) {
+        tw[t] = twg[t];
+        const int k1 = t / R2, n2 = t - k1 * R2;
+        twT[t] = twg[(n2 * k1) % N];
+    }
     for (int t = threadIdx.x; t <= N / 2; t += NT) ha[t] = tw2g[t];
     __syncthreads();
 
@@ -391,7 +398,7 @@ __global__ void __launch_bounds__(32 * WPB, 16 / WPB) k_lines(const __grid_const
                 for (int j = s; j <= N; j += W) cl[j] = make_double2(0.0, 0.0);
             __syncwarp();
             pre_seg<R2, N, W, false>(xl, cl, ha, f1, s);
-            fft_seg<R1, R2, W>(xl, tw, s);
+            fft_seg<R1, R2, W>(xl, tw, twT, s);
             post_seg<R2, N, W>(xl, cl, *f1, s);
             // order 1 outputs, then (one more recurrence) order 2 outputs;
             // the next item's line is fetched into cl once its last read is done
@@ -406,7 +413,7 @@ __global__ void __launch_bounds__(32 * WPB, 16 / WPB) k_lines(const __grid_const
                         prefetch(next);
                         fetched = true;
                     }
-                    fft_seg<R1, R2, W>(xl, tw, s);
+                    fft_seg<R1, R2, W>(xl, tw, twT, s);
                     post_seg<R2, N, W>(xl, nullptr, *f1, s);
                     store_seg<R2, N, W>(o, xl, true, I.lbase, es, I.act, interior_line, I.mode, kx, real0, s);
                     __syncwarp();
@@ -444,7 +451,7 @@ static int launch_lines(ductgpu_ctx ctx, const LineParams &p0)
     const long long grid = (items + WPB - 1) / WPB;
     if (grid > 0x7fffffffLL) return set_error(ctx, DUCTGPU_EARG, "lines: grid too large");
     p.ctas_per_job = 0;
-    const size_t smem = ((size_t)N + (N / 2 + 1) + (size_t)LPB * S::PL) * sizeof(double2);
+    const size_t smem = (2 * (size_t)N + (N / 2 + 1) + (size_t)LPB * S::PL) * sizeof(double2);
     DUCT_CUDA(ctx, cudaFuncSetAttribute(k_lines<R1, R2, W, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
     if (ctx->prof_on && !ctx->capturing) {
@@ -500,11 +507,11 @@ int lines_launch(ductgpu_ctx ctx, const LineParams &p)
     case 32: return launch_lines<4, 8, 8, 4>(ctx, p);
     case 48: return launch_lines<6, 8, 8, 4>(ctx, p);
     case 64: return launch_lines<8, 8, 8, 4>(ctx, p);
-    case 96: return launch_lines<8, 12, 16, 4>(ctx, p);
-    case 128: return launch_lines<8, 16, 16, 4>(ctx, p);
-    case 144: return launch_lines<12, 12, 16, 4>(ctx, p);
-    case 192: return launch_lines<12, 16, 16, 4>(ctx, p);
-    case 256: return launch_lines<16, 16, 16, 4>(ctx, p);
+    case 96: return launch_lines<8, 12, 16, 8>(ctx, p);
+    case 128: return launch_lines<8, 16, 16, 8>(ctx, p);
+    case 144: return launch_lines<12, 12, 16, 8>(ctx, p);
+    case 192: return launch_lines<12, 16, 16, 8>(ctx, p);
+    case 256: return launch_lines<16, 16, 16, 8>(ctx, p);
     default:
         return set_error(ctx, DUCTGPU_EARG, "lines: line length %d - 1 is not one of 16, 24, 32, 48, 64, 96, 128, "
                          "144, 192, 256", nn);
