@@ -46,6 +46,7 @@ EXPORTS = [
     "ductgpu_dns_field", "ductgpu_dns_set_graphs", "ductgpu_dns_substep", "ductgpu_dns_steps",
     "ductgpu_dns_statistics", "ductgpu_profile_bytes", "ductgpu_dns_set_forcing",
     "ductgpu_dns_wallstress_after", "ductgpu_dns_grad_wallstress", "ductgpu_set_rect_fold",
+    "ductgpu_set_line_kernel",
 ]
 SETUP_NO_EIGEN = 1
 (K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER, K_LINES,
@@ -158,6 +159,7 @@ def lib():
             "ductgpu_profile_bytes": [P, I, C.POINTER(D)],
             "ductgpu_dns_set_forcing": [P, P, P, P],
             "ductgpu_set_rect_fold": [P, I],
+            "ductgpu_set_line_kernel": [P, I],
             "ductgpu_dns_wallstress_after": [P, I, C.POINTER(D)],
             "ductgpu_dns_grad_wallstress": [P, C.POINTER(D), P],
             "ductgpu_graph_destroy": [P, I],
@@ -303,6 +305,11 @@ class Context:
         Returns the table entry, or None (library defaults kept)."""
         from duct_b200 import tune
         return tune.apply(self, int(my), int(mz if mz is not None else my), path or tune.TABLE)
+
+    def set_line_kernel(self, kernel):
+        """1 (default), 2: derivative lines on the FP64 tensor cores (2: the
+        operator fragments fetched a step ahead), 0: the FFT kernel."""
+        self._check(lib().ductgpu_set_line_kernel(self.h, int(kernel)))
 
     def set_rect_fold(self, on):
         self._check(lib().ductgpu_set_rect_fold(self.h, int(bool(on))))

@@ -219,6 +219,7 @@ int ductgpu_destroy(ductgpu_ctx ctx)
     for (int i = 0; i < ductgpu_ctx_s::kTwTables; ++i) cudaFree(ctx->tw_tab[i]);
     cudaFree(ctx->dev_err);
     free_dns_aux(ctx);
+    free_dlines(ctx);
     cudaFree(ctx->lam);
     cudaFreeHost(ctx->lam_host);
     for (int i = 0; i < kNumEvents; ++i) cudaEventDestroy(ctx->ev[i]);
@@ -410,6 +411,13 @@ int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel)
     if (size_class < -1 || size_class > 2) return set_error(ctx, DUCTGPU_EARG, "size class %d", size_class);
     for (int c = 0; c < 3; ++c)
         if (size_class < 0 || size_class == c) ctx->pass_variant[c] = (kernel < 0) ? kPassDefault[c] : kernel;
+    return DUCTGPU_OK;
+}
+
+int ductgpu_set_line_kernel(ductgpu_ctx ctx, int kernel)
+{
+    if (!ctx || kernel < 0 || kernel > 2) return DUCTGPU_EARG;
+    ctx->dlines = kernel;
     return DUCTGPU_OK;
 }
 

@@ -501,6 +501,7 @@ int lines_launch(ductgpu_ctx ctx, const LineParams &p)
         }
     }
     const int nn = (p.dir == 'y') ? p.my : p.mz;
+    if (ctx->dlines && dlines_supported(nn)) return dlines_launch(ctx, p);
     switch (nn - 1) {
     case 16: return launch_lines<4, 4, 4, 4>(ctx, p);
     case 24: return launch_lines<4, 6, 8, 4>(ctx, p);

@@ -1,0 +1,422 @@
+// dlines.cu -- the Chebyshev derivative lines of cheb_lines.cu on the FP64
+// tensor cores (mma.sync m16n8k16 f64, "DMMA").
+//
+// For one line length nn the reference's derivative (transyz -1, the
+// recurrence once or twice, transyz +1) is a fixed real nn x nn matrix D
+// (D1 or D2), built on the host in long double from that same chain.
+// On the symmetric Gauss-Lobatto nodes D1 anticommutes with the reflection
+// J (point k <-> nn-1-k) and D2 commutes with it, so with the line split
+// into u_c = x_c + x_{nn-1-c} (c < ho; u_mid = x_mid, nn = 2 ho + 1) and
+// v_c = x_c - x_{nn-1-c} (c < ho) the derivative is two half-size GEMMs
+//   P_r = sum_c Ap(r,c) u_c,  Ap(r,c) = (D(r,c) + D(r,nn-1-c)) / 2, Ap(r,mid) = D(r,mid)
+//   M_r = sum_c Am(r,c) v_c,  Am(r,c) = (D(r,c) - D(r,nn-1-c)) / 2
+// for the rows r < he = ho + 1, and
+//   y_r = P_r + M_r,  y_{nn-1-r} = s (P_r - M_r)   (s = -1 for D1, +1 for D2)
+// -- half the flops of the full matrix, 2 (he^2 + he ho) per real column.
+// The store is k_lines' epilogue (out = sigma (beta out + fac y + x-terms +
+// [mode 0] m0), the max |out| reduction), so lines_launch hands a launch
+// either to k_lines (the FFT form) or to this kernel.
+//
+// A CTA takes 16 complex lines (32 real columns) of one mode of one job,
+// staged once with cp.async and folded in place (u_k to row k, v_k to row
+// nn-1-k); a warp per 16 output rows (MT = ceil(he/16) warps) runs the two
+// GEMMs of every derivative output of the job over them, reading its A
+// fragments straight from L2 (the operators are 0.2 MB) -- no CTA barrier
+// inside the K loop.
+#include <math.h>
+
+#include <type_traits>
+#include <vector>
+
+#include "internal.h"
+
+namespace duct {
+
+constexpr int kDlLines = 16;                 // complex lines per CTA
+constexpr int kDlCols = 2 * kDlLines;        // real columns
+constexpr int kDlNld = kDlCols + 8;          // row stride of U, V: B fragments conflict free
+
+struct DLineParams {
+    LineParams lp;
+    const double *A[2][2];   // [order - 1][0: Ap, 1: Am], HR x HR each, DMMA A-fragment order
+    int nn, he, ho;
+    int ctas_per_job;
+};
+
+__device__ __forceinline__ void dl_cp16(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+
+// D += A(16x16) B(16x8), m16n8k16 f64 fragments (PTX ISA):
+// a[v] = A[g + 8(v&1)][t + 4(v>>1)], b[v] = B[t + 4v][g],
+// d = {D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1]}.
+__device__ __forceinline__ void dl_mma(double (&d)[4], const double (&a)[8], const double (&b)[4])
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 "
+        "{%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+          "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
+__device__ __forceinline__ double2 dl_xcoef(const LineOut &o, int t, double kx)
+{
+    return make_double2(o.xc0[t] - o.xc2[t] * kx * kx, o.xc1[t] * kx);
+}
+
+// One output element: out[gi] = sigma (beta out + fac y + x-terms + m0).
+// Returns |out| for the interior max (0 where it does not count).
+__device__ __forceinline__ double dl_store(const LineOut &o, long long gi, double2 y, bool deriv, double kx,
+                                           double m0, bool real0, bool interior)
+{
+    double2 *out = reinterpret_cast<double2 *>(o.out);
+    double2 v = make_double2(m0, 0.0);
+    if (deriv) {
+        v.x += o.fac * y.x;
+        if (!real0) v.y += o.fac * y.y;
+    }
+#pragma unroll
+    for (int t = 0; t < kLineXTerms; ++t)
+        if (o.xs[t]) {
+            const double2 c = dl_xcoef(o, t, kx);
+            const double2 s = reinterpret_cast<const double2 *>(o.xs[t])[gi];
+            v.x += c.x * s.x - c.y * s.y;
+            v.y += c.x * s.y + c.y * s.x;
+        }
+    if (o.beta != 0.0) {
+        const double2 w = out[gi];
+        v.x += o.beta * w.x;
+        v.y += o.beta * w.y;
+    }
+    v.x *= o.sigma;
+    v.y *= o.sigma;
+    out[gi] = v;
+    return interior ? hypot(v.x, v.y) : 0.0;
+}
+
+// Without the prefetch, registers for about 16 resident warps per SM
+// (two CTAs at least).
+template <int MT, bool PF>
+__global__ void __launch_bounds__(32 * MT, PF ? 1 : (16 / MT > 2 ? 16 / MT : 2))
+    k_dlines(const __grid_constant__ DLineParams q)
+{
+    constexpr int NT = 4;                    // n-tiles of 8 real columns: 16 complex lines
+    extern __shared__ __align__(16) double Xs[];   // [nn][kDlNld]: the raw lines, (re, im) column pairs
+
+    const LineParams &p = q.lp;
+    const int job = blockIdx.x / q.ctas_per_job;
+    const int rr = blockIdx.x - job * q.ctas_per_job;
+    const LineJob &J = p.job[job];
+    const bool ydir = (p.dir == 'y');
+    const long long ms = (long long)p.my * p.mz;
+    const long long ls = ydir ? p.my : 1, es = ydir ? 1 : p.my;
+    const int lpm = ydir ? p.mz : p.my;
+    const int cpm = (lpm + kDlLines - 1) / kDlLines;
+    const int mode = rr / cpm;
+    const int q0 = (rr - mode * cpm) * kDlLines;
+    const int L = min(kDlLines, lpm - q0);
+    const long long base = mode * ms + (long long)q0 * ls;
+    const double kx = p.xalp[mode];
+    const bool real0 = p.real0 && mode == 0;
+    const int nn = q.nn, he = q.he, ho = q.ho;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const double m0 = (mode == 0) ? 1.0 : 0.0;
+
+    int maxord = 0;
+    for (int k = 0; k < J.nout; ++k) maxord = max(maxord, J.o[k].order);
+    if (maxord > 0) {
+        const double2 *in = reinterpret_cast<const double2 *>(J.in) + base;
+        for (int idx = tid; idx < nn * kDlLines; idx += 32 * MT) {
+            int j, l;
+            if (ydir) { j = idx % nn; l = idx / nn; }
+            else { l = idx % kDlLines; j = idx / kDlLines; }
+            double *dst = Xs + j * kDlNld + 2 * l;
+            if (l < L) dl_cp16(dst, in + (long long)l * ls + (long long)j * es);
+            else { dst[0] = 0.0; dst[1] = 0.0; }
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+        asm volatile("cp.async.wait_group 0;\n" ::);
+        __syncthreads();
+        // fold in place: u_k = x_k + x_{nn-1-k} to row k, v_k = x_k - x_{nn-1-k}
+        // to row nn-1-k (k < ho; the middle row is u_ho = x_ho)
+        for (int idx = tid; idx < ho * kDlCols; idx += 32 * MT) {
+            const int k = idx / kDlCols, c = idx - k * kDlCols;
+            const double a = Xs[k * kDlNld + c], b = Xs[(nn - 1 - k) * kDlNld + c];
+            Xs[k * kDlNld + c] = a + b;
+            Xs[(nn - 1 - k) * kDlNld + c] = a - b;
+        }
+        __syncthreads();
+    }
+    double vmax = 0.0;
+    const double *maxabs_out = nullptr;
+    const int mt = warp;                     // this warp's 16 output rows
+    for (int oi = 0; oi < J.nout; ++oi) {
+        const LineOut &o = J.o[oi];
+        if (o.maxabs) maxabs_out = o.maxabs;
+        if (o.order == 0) {
+            for (int idx = tid; idx < nn * kDlLines; idx += 32 * MT) {
+                int j, l;
+                if (ydir) { j = idx % nn; l = idx / nn; }
+                else { l = idx % kDlLines; j = idx / kDlLines; }
+                if (l >= L) continue;
+                const long long gi = base + (long long)l * ls + (long long)j * es;
+                const bool in_int = o.maxabs && j > 0 && j < nn - 1 && q0 + l > 0 && q0 + l < lpm - 1;
+                vmax = fmax(vmax, dl_store(o, gi, make_double2(0.0, 0.0), false, kx, m0 * o.m0, real0, in_int));
+            }
+            continue;
+        }
+        // A fragments of tile (ks, mt) at (ks MT + mt) 256, read from L2 a step ahead
+        const double2 *Ap = reinterpret_cast<const double2 *>(q.A[o.order - 1][0] + (size_t)mt * 256) + lane;
+        const double2 *Am = reinterpret_cast<const double2 *>(q.A[o.order - 1][1] + (size_t)mt * 256) + lane;
+        auto load_a = [&](const double2 *src, int ks, double (&a)[8]) {
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const double2 v = __ldg(src + (size_t)ks * MT * 128 + 32 * h);
+                a[2 * h] = v.x;
+                a[2 * h + 1] = v.y;
+            }
+        };
+        double acc[2][NT][4];
+#pragma unroll
+        for (int pm = 0; pm < 2; ++pm)
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) acc[pm][nt][v] = 0.0;
+        // P = Ap u, then M = Am v (one GEMM at a time: fewer live registers).
+        // B fragments of K step ks: u_k from row k, v_k from row nn-1-k; only
+        // the last step reaches k >= ho (u_ho the middle, zero beyond)
+#pragma unroll
+        for (int pm = 0; pm < 2; ++pm) {
+            const double2 *Asrc = pm ? Am : Ap;
+            auto step = [&](int ks, const double (&a)[8], auto last) {
+#pragma unroll
+                for (int nt = 0; nt < NT; ++nt) {
+                    const int col = nt * 8 + g;
+                    double b[4];
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) {
+                        const int k = ks * 16 + t + 4 * v;
+                        const int row = pm ? nn - 1 - k : k;
+                        if (decltype(last)::value)
+                            b[v] = (pm ? k < ho : k <= ho) ? Xs[row * kDlNld + col] : 0.0;
+                        else
+                            b[v] = Xs[row * kDlNld + col];
+                    }
+                    dl_mma(acc[pm][nt], a, b);
+                }
+            };
+            double a[8], an[8];
+            if (PF) load_a(Asrc, 0, a);
+#pragma unroll 1
+            for (int ks = 0; ks < MT; ++ks) {
+                if (!PF) load_a(Asrc, ks, a);
+                else if (ks + 1 < MT) load_a(Asrc, ks + 1, an);
+                if (ks + 1 < MT) step(ks, a, std::false_type());
+                else step(ks, a, std::true_type());
+                if (PF && ks + 1 < MT) {
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) a[i] = an[i];
+                }
+            }
+        }
+        // y_r = P_r + M_r, y_{nn-1-r} = s (P_r - M_r); columns (2t, 2t+1) of
+        // n-tile nt are (re, im) of line 4 nt + t
+        const double s = (o.order == 1) ? -1.0 : 1.0;
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+            const int l = nt * 4 + t;
+            if (l >= L) continue;
+            const bool chk = o.maxabs && q0 + l > 0 && q0 + l < lpm - 1;
+            const long long lb = base + (long long)l * ls;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = mt * 16 + g + 8 * h;
+                if (r >= he) continue;
+                const double pr = acc[0][nt][2 * h], pi = acc[0][nt][2 * h + 1];
+                const double mr = acc[1][nt][2 * h], mi = acc[1][nt][2 * h + 1];
+                vmax = fmax(vmax, dl_store(o, lb + (long long)r * es, make_double2(pr + mr, pi + mi), true, kx,
+                                           m0 * o.m0, real0, chk && r > 0));
+                if (r < ho)
+                    vmax = fmax(vmax, dl_store(o, lb + (long long)(nn - 1 - r) * es,
+                                               make_double2(s * (pr - mr), s * (pi - mi)), true, kx, m0 * o.m0,
+                                               real0, chk && r > 0));
+            }
+        }
+    }
+    if (maxabs_out) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+        if (lane == 0 && vmax > 0.0)
+            atomicMax(reinterpret_cast<unsigned long long *>(const_cast<double *>(maxabs_out)),
+                      (unsigned long long)__double_as_longlong(vmax));
+    }
+}
+
+// the odd line lengths of the FFT kernel with half blocks up to 112 rows
+bool dlines_supported(int nn) { return (nn & 1) && lines_supported(nn) && (nn + 1) / 2 <= 16 * 7; }
+
+void free_dlines(ductgpu_ctx ctx)
+{
+    for (int i = 0; i < ductgpu_ctx_s::kDlineSlots; ++i) {
+        cudaFree(ctx->dl_ops[i]);
+        ctx->dl_ops[i] = nullptr;
+        ctx->dl_nn[i] = 0;
+    }
+}
+
+// The derivative matrix D = B R^ord F of one line of nn = N + 1 points,
+// column-major, in long double: F the forward tcheb (src/tchebw.f:62-192:
+// c_k = w_k (x_0 + (-1)^k x_N + 2 sum_{0<j<N} x_j cos(pi j k / N)), w_k =
+// 1/N inside, 1/(2N) at k = 0, N), R the derivative recurrence of derivyz
+// (src/chebyshev.f90:44-58: d_N = 0, d_{k-1} = d_{k+1} + 2 k c_k, out_k =
+// -d_k for k >= 1, out_0 = -d_0 / 2), B the inverse tcheb (x_j = sum_k c_k
+// cos(pi j k / N)).  The 64-bit significand keeps the entries' own error
+// (~ 2^-64 N^4 at the corners of D2) below their FP64 rounding; the same
+// chain run in FP64 on unit vectors leaves errors ~ 2^-53 N^3 on entries
+// of size N^2 that a whole line then sums.
+static void cheb_deriv_matrix(int nn, int ord, std::vector<long double> &D)
+{
+    const int N = nn - 1;
+    const long double pi = 3.141592653589793238462643383279502884L;
+    std::vector<long double> ct(2 * (size_t)N), c(nn), d(nn);
+    for (int q = 0; q < 2 * N; ++q) ct[q] = cosl(pi * (long double)q / (long double)N);
+    D.assign((size_t)nn * nn, 0.0L);
+    for (int col = 0; col < nn; ++col) {
+        const long double sc = (col == 0 || col == N) ? 1.0L : 2.0L;
+        for (int k = 0; k < nn; ++k) {
+            const long double w = (k == 0 || k == N) ? 0.5L / N : 1.0L / N;
+            c[k] = w * sc * ct[(size_t)((long)col * k % (2 * N))];
+        }
+        for (int o = 0; o < ord; ++o) {
+            long double dk1 = 0.0L, dk = 0.0L;     // d_{k+1}, d_k, walking k down from N
+            d[N] = 0.0L;
+            for (int k = N; k >= 1; --k) {
+                const long double dm = dk1 + 2.0L * k * c[k];   // d_{k-1}
+                d[k] = -dk;
+                dk1 = dk;
+                dk = dm;
+            }
+            d[0] = -0.5L * dk;
+            c.swap(d);
+        }
+        for (int j = 0; j < nn; ++j) {
+            long double x = 0.0L;
+            for (int k = 0; k < nn; ++k) x += c[k] * ct[(size_t)((long)j * k % (2 * N))];
+            D[(size_t)j + (size_t)nn * col] = x;
+        }
+    }
+}
+
+// The folded, packed operators of line length nn (built on first use:
+// not inside a stream capture).
+static int dlines_ops(ductgpu_ctx ctx, int nn, const double **ops, int *hr)
+{
+    const int he = (nn + 1) / 2, ho = nn / 2, MT = (he + 15) / 16, HR = 16 * MT;
+    const size_t blk = (size_t)HR * HR;
+    *hr = HR;
+    int slot = -1;
+    for (int i = 0; i < ductgpu_ctx_s::kDlineSlots; ++i)
+        if (ctx->dl_nn[i] == nn) { *ops = ctx->dl_ops[i]; return DUCTGPU_OK; }
+    for (int i = 0; i < ductgpu_ctx_s::kDlineSlots && slot < 0; ++i)
+        if (!ctx->dl_nn[i]) slot = i;
+    if (slot < 0) return set_error(ctx, DUCTGPU_ESTATE, "derivative lines: more than %d line lengths",
+                                   ductgpu_ctx_s::kDlineSlots);
+    if (ctx->capturing)
+        return set_error(ctx, DUCTGPU_ESTATE, "derivative lines: operators for nn=%d first built inside a capture", nn);
+    // fold and pack: [ord][Ap, Am]
+    std::vector<double> packed(4 * blk, 0.0);
+    std::vector<long double> M;
+    for (int ord = 0; ord < 2; ++ord) {
+        cheb_deriv_matrix(nn, ord + 1, M);
+        auto d = [&](int r, int c) { return M[(size_t)r + (size_t)nn * c]; };
+        for (int pm = 0; pm < 2; ++pm)
+            for (size_t idx = 0; idx < blk; ++idx) {
+                int row, col;
+                pack_slot((int)idx, MT, row, col);
+                long double v = 0.0L;
+                if (row < he) {
+                    if (pm == 0) {
+                        if (col < ho) v = 0.5L * (d(row, col) + d(row, nn - 1 - col));
+                        else if (col == ho) v = d(row, ho);   // the middle point
+                    } else if (col < ho) {
+                        v = 0.5L * (d(row, col) - d(row, nn - 1 - col));
+                    }
+                }
+                packed[(size_t)(2 * ord + pm) * blk + idx] = (double)v;
+            }
+    }
+    double *dev = nullptr;
+    DUCT_CUDA(ctx, cudaMalloc(&dev, packed.size() * sizeof(double)));
+    DUCT_CUDA(ctx, cudaMemcpy(dev, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice));
+    ctx->dl_ops[slot] = dev;
+    ctx->dl_nn[slot] = nn;
+    *ops = dev;
+    return DUCTGPU_OK;
+}
+
+template <int MT, bool PF>
+static int launch_dlines(ductgpu_ctx ctx, DLineParams &q)
+{
+    const size_t smem = (size_t)q.nn * kDlNld * sizeof(double);
+    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_dlines<MT, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long long grid = (long long)q.ctas_per_job * q.lp.njobs;
+    if (grid > 0x7fffffffLL) return set_error(ctx, DUCTGPU_EARG, "derivative lines: grid too large");
+    if (ctx->prof_on && !ctx->capturing) {
+        double fields = 0.0;
+        for (int i = 0; i < q.lp.njobs; ++i) {
+            const LineJob &J = q.lp.job[i];
+            bool in = false;
+            for (int k = 0; k < J.nout; ++k) {
+                const LineOut &o = J.o[k];
+                in |= o.order > 0;
+                fields += 1.0 + (o.beta != 0.0 ? 1.0 : 0.0);
+                for (int t = 0; t < kLineXTerms; ++t) fields += o.xs[t] ? 1.0 : 0.0;
+            }
+            fields += in ? 1.0 : 0.0;
+        }
+        ctx->prof_bytes[DUCTGPU_K_LINES] += fields * 16.0 * q.lp.my * q.lp.mz * q.lp.nmodes;
+    }
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_LINES);
+        k_dlines<MT, PF><<<(unsigned)grid, 32 * MT, smem, ctx->stream>>>(q);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "k_dlines");
+}
+
+int dlines_launch(ductgpu_ctx ctx, const LineParams &p)
+{
+    const int nn = (p.dir == 'y') ? p.my : p.mz;
+    DLineParams q;
+    q.lp = p;
+    q.nn = nn;
+    q.he = (nn + 1) / 2;
+    q.ho = nn / 2;
+    const double *ops = nullptr;
+    int HR = 0;
+    int rc = dlines_ops(ctx, nn, &ops, &HR);
+    if (rc) return rc;
+    const size_t blk = (size_t)HR * HR;
+    for (int ord = 0; ord < 2; ++ord)
+        for (int pm = 0; pm < 2; ++pm) q.A[ord][pm] = ops + (size_t)(2 * ord + pm) * blk;
+    const int lpm = (p.dir == 'y') ? p.mz : p.my;
+    q.ctas_per_job = p.nmodes * ((lpm + kDlLines - 1) / kDlLines);
+    // dlines 1: A fragments loaded at each K step, two CTAs of the longest
+    // lines per SM (measured on the 193 x 193, 85-mode laplacian: 0.265 ms
+    // against 0.313 ms for the FFT kernel); 2: fetched a step ahead, more
+    // registers, one CTA per SM (0.345 ms)
+    const bool pf = ctx->dlines == 2;
+#define DL_CASE(mt) \
+    case mt: return pf ? launch_dlines<mt, true>(ctx, q) : launch_dlines<mt, false>(ctx, q);
+    switch (HR / 16) {
+        DL_CASE(1) DL_CASE(2) DL_CASE(3) DL_CASE(4) DL_CASE(5) DL_CASE(6) DL_CASE(7)
+    default: return set_error(ctx, DUCTGPU_EARG, "derivative lines: line length %d", nn);
+    }
+#undef DL_CASE
+}
+
+}  // namespace duct

@@ -146,11 +146,17 @@ struct ductgpu_ctx_s {
     cudaStream_t cp_in = nullptr, cp_out = nullptr;
     cudaEvent_t ev_in[kPipeChunks] = {}, ev_out[kPipeChunks] = {};
     // W_L twiddle tables of the register-FFT transforms, one per length
-    static constexpr int kTwTables = 8;
+    static constexpr int kTwTables = 24;
     int tw_len[kTwTables] = {};
     void *tw_tab[kTwTables] = {};
     int *dev_err = nullptr;    // device error word (bounded waits)
     duct::DnsAux *dns_aux = nullptr;   // buffers of the DNS operator entries (dns.cu)
+    // derivative lines on the FP64 tensor cores (dlines.cu): the folded,
+    // packed collocation matrices per line length
+    static constexpr int kDlineSlots = 12;
+    int dl_nn[kDlineSlots] = {};
+    double *dl_ops[kDlineSlots] = {};
+    int dlines = 1;            // 1: derivative lines by DMMA where supported, 0: the FFT kernel
     double *lam = nullptr;     // per-plane lambda (device)
     double *lam_host = nullptr;// pinned staging
     int lam_cap = 0;
@@ -360,6 +366,25 @@ struct LineParams {
 int lines_launch(ductgpu_ctx ctx, const LineParams &p);
 // dns.cu
 void free_dns_aux(ductgpu_ctx ctx);
+
+// Position (row, col) of element idx of an operator packed in the DMMA
+// A-fragment order used by every FP64 pass (m16n8k16: tiles of 16 x 16,
+// m-tile fastest; inside a tile the value pair outermost, then the lane,
+// so that a warp's 16-byte loads are consecutive).
+__host__ __device__ __forceinline__ void pack_slot(int idx, int mtiles, int &row, int &col)
+{
+    const int tile = idx >> 8, h = (idx >> 6) & 3, lane = (idx >> 1) & 31, v = 2 * h + (idx & 1);
+    const int mt = tile % mtiles, ks = tile / mtiles;
+    const int g = lane >> 2, t = lane & 3;
+    row = mt * 16 + g + 8 * (v & 1);
+    col = ks * 16 + t + 4 * (v >> 1);
+}
+
+// dlines.cu: the derivative lines on the FP64 tensor cores (flip-symmetric
+// half blocks of the collocation matrices of k_lines)
+bool dlines_supported(int nn);
+int dlines_launch(ductgpu_ctx ctx, const LineParams &p);
+void free_dlines(ductgpu_ctx ctx);
 bool lines_supported(int nn);
 const double2 *twiddle_table(ductgpu_ctx ctx, int L);
 

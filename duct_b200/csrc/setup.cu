@@ -127,15 +127,6 @@ __global__ void k_real_part(int n, const double *W, double *E)
 // so that a warp's 16-byte loads of one pair are consecutive (no shared
 // memory bank conflicts, one 512-byte run from global memory).  Outside
 // n x n the packing is zero.
-__host__ __device__ __forceinline__ void pack_slot(int idx, int mtiles, int &row, int &col)
-{
-    const int tile = idx >> 8, h = (idx >> 6) & 3, lane = (idx >> 1) & 31, v = 2 * h + (idx & 1);
-    const int mt = tile % mtiles, ks = tile / mtiles;
-    const int g = lane >> 2, t = lane & 3;
-    row = mt * 16 + g + 8 * (v & 1);
-    col = ks * 16 + t + 4 * (v >> 1);
-}
-
 __global__ void k_pack_a(int n, int kpad, int mtiles, const double *A, double *out)
 {
     const int total = (kpad / 16) * mtiles * 256;
