@@ -500,6 +500,22 @@ int lines_launch(ductgpu_ctx ctx, const LineParams &p)
             if (J.o[k].order > 0 && !J.in) return set_error(ctx, DUCTGPU_EARG, "lines: job %d has no input", i);
         }
     }
+    // an output's destination and sources against the other outputs' destinations
+    for (int i = 0; i < p.njobs; ++i)
+        for (int k = 0; k < p.job[i].nout; ++k) {
+            const LineOut &o = p.job[i].o[k];
+            for (int i2 = 0; i2 < p.njobs; ++i2)
+                for (int k2 = 0; k2 < p.job[i2].nout; ++k2) {
+                    if (i2 == i && k2 == k) continue;
+                    const double *w = p.job[i2].o[k2].out;
+                    bool hit = (o.out == w);       // two writers of one field, or beta reading the other's
+
+                    for (int t = 0; t < kLineXTerms; ++t) hit |= (o.xs[t] == w);
+                    if (hit)
+                        return set_error(ctx, DUCTGPU_EARG, "lines: job %d output %d reads or writes what job %d output %d writes",
+                                         i, k, i2, k2);
+                }
+        }
     const int nn = (p.dir == 'y') ? p.my : p.mz;
     if (ctx->dlines && dlines_supported(nn)) return dlines_launch(ctx, p);
     switch (nn - 1) {

@@ -1,28 +1,30 @@
 // dlines.cu -- the Chebyshev derivative lines of cheb_lines.cu on the FP64
 // tensor cores (mma.sync m16n8k16 f64, "DMMA").
 //
-// For one line length nn the reference's derivative (transyz -1, the
-// recurrence once or twice, transyz +1) is a fixed real nn x nn matrix D
-// (D1 or D2), built on the host in long double from that same chain.
-// On the symmetric Gauss-Lobatto nodes D1 anticommutes with the reflection
-// J (point k <-> nn-1-k) and D2 commutes with it, so with the line split
-// into u_c = x_c + x_{nn-1-c} (c < ho; u_mid = x_mid, nn = 2 ho + 1) and
-// v_c = x_c - x_{nn-1-c} (c < ho) the derivative is two half-size GEMMs
-//   P_r = sum_c Ap(r,c) u_c,  Ap(r,c) = (D(r,c) + D(r,nn-1-c)) / 2, Ap(r,mid) = D(r,mid)
-//   M_r = sum_c Am(r,c) v_c,  Am(r,c) = (D(r,c) - D(r,nn-1-c)) / 2
-// for the rows r < he = ho + 1, and
+// For one line length nn = 2 ho + 1 the reference's derivative (transyz -1,
+// the recurrence once or twice, transyz +1) is a fixed real nn x nn matrix
+// D (D1 or D2), built on the host in long double from that same chain.  On
+// the symmetric Gauss-Lobatto nodes D1 anticommutes with the reflection J
+// (point k <-> nn-1-k) and D2 commutes with it, so with the line split into
+// u_c = x_c + x_{nn-1-c} and v_c = x_c - x_{nn-1-c} (c < ho) and the middle
+// point x_ho the derivative is, for the rows r < ho,
+//   P_r = sum_{c<ho} Ap(r,c) u_c + D(r,ho) x_ho,  Ap(r,c) = (D(r,c) + D(r,nn-1-c)) / 2
+//   M_r = sum_{c<ho} Am(r,c) v_c,                Am(r,c) = (D(r,c) - D(r,nn-1-c)) / 2
 //   y_r = P_r + M_r,  y_{nn-1-r} = s (P_r - M_r)   (s = -1 for D1, +1 for D2)
-// -- half the flops of the full matrix, 2 (he^2 + he ho) per real column.
-// The store is k_lines' epilogue (out = sigma (beta out + fac y + x-terms +
-// [mode 0] m0), the max |out| reduction), so lines_launch hands a launch
-// either to k_lines (the FFT form) or to this kernel.
+// and for the middle row y_ho = sum_{c<ho} (Ap(ho,c) u_c + Am(ho,c) v_c) +
+// D(ho,ho) x_ho: two ho x ho GEMMs on the tensor cores (half the flops of
+// the full matrix), the middle column a rank-1 update of P and the middle
+// row a dot product in FP64 FMAs, so that ho = 16 MT (nn = 2^k + 1) pads
+// nothing.  The store is k_lines' epilogue (out = sigma (beta out + fac y +
+// x-terms + [mode 0] m0), the max |out| reduction), so lines_launch hands a
+// launch either to k_lines (the FFT form) or to this kernel.
 //
 // A CTA takes 16 complex lines (32 real columns) of one mode of one job,
 // staged once with cp.async and folded in place (u_k to row k, v_k to row
-// nn-1-k); a warp per 16 output rows (MT = ceil(he/16) warps) runs the two
-// GEMMs of every derivative output of the job over them, reading its A
-// fragments straight from L2 (the operators are 0.2 MB) -- no CTA barrier
-// inside the K loop.
+// nn-1-k, x_ho stays); a warp per 16 rows r < ho (MT = ceil(ho / 16) warps)
+// runs the two GEMMs of every derivative output of the job over them,
+// reading its A fragments straight from L2 (the operators are at most
+// 0.5 MB), with no CTA barrier inside the K loop.
 #include <math.h>
 
 #include <type_traits>
@@ -34,12 +36,18 @@ namespace duct {
 
 constexpr int kDlLines = 16;                 // complex lines per CTA
 constexpr int kDlCols = 2 * kDlLines;        // real columns
-constexpr int kDlNld = kDlCols + 8;          // row stride of U, V: B fragments conflict free
+constexpr int kDlNld = kDlCols + 8;          // row stride of the staged lines: B fragments conflict free
+constexpr int kDlMaxMT = 8;                  // ho <= 128: line lengths up to 257
+
+// Operators of one order, HR = 16 MT: Ap and Am (HR x HR each, rows and
+// columns >= ho zero, DMMA A-fragment order), then the vectors D(r, ho)
+// (r < ho), Ap(ho, c), Am(ho, c) (c < ho) and D(ho, ho), HR doubles each.
+inline size_t dl_chunk(int HR) { return 2 * (size_t)HR * HR + 4 * (size_t)HR; }
 
 struct DLineParams {
     LineParams lp;
-    const double *A[2][2];   // [order - 1][0: Ap, 1: Am], HR x HR each, DMMA A-fragment order
-    int nn, he, ho;
+    const double *op[2];     // [order - 1]
+    int nn, ho;
     int ctas_per_job;
 };
 
@@ -97,14 +105,15 @@ __device__ __forceinline__ double dl_store(const LineOut &o, long long gi, doubl
     return interior ? hypot(v.x, v.y) : 0.0;
 }
 
-// Without the prefetch, registers for about 16 resident warps per SM
-// (two CTAs at least).
-template <int MT, bool PF>
-__global__ void __launch_bounds__(32 * MT, PF ? 1 : (16 / MT > 2 ? 16 / MT : 2))
+// Registers for about 16 resident warps per SM (two CTAs at least).
+template <int MT>
+__global__ void __launch_bounds__(32 * MT, 16 / MT > 2 ? 16 / MT : 2)
     k_dlines(const __grid_constant__ DLineParams q)
 {
     constexpr int NT = 4;                    // n-tiles of 8 real columns: 16 complex lines
-    extern __shared__ __align__(16) double Xs[];   // [nn][kDlNld]: the raw lines, (re, im) column pairs
+    constexpr int HR = 16 * MT;
+    constexpr size_t blk = (size_t)HR * HR;
+    extern __shared__ __align__(16) double Xs[];   // [nn][kDlNld] lines ((re, im) column pairs), then red
 
     const LineParams &p = q.lp;
     const int job = blockIdx.x / q.ctas_per_job;
@@ -121,19 +130,21 @@ __global__ void __launch_bounds__(32 * MT, PF ? 1 : (16 / MT > 2 ? 16 / MT : 2))
     const long long base = mode * ms + (long long)q0 * ls;
     const double kx = p.xalp[mode];
     const bool real0 = p.real0 && mode == 0;
-    const int nn = q.nn, he = q.he, ho = q.ho;
+    const int nn = q.nn, ho = q.ho;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
     const double m0 = (mode == 0) ? 1.0 : 0.0;
+    double *red = Xs + (size_t)nn * kDlNld;  // [2][MT][32]: the middle row's partial sums
 
+    // element idx of the CTA's lines: line idx % 16, point idx / 16 (a warp
+    // touches two points of 16 lines: whole 32-byte sectors along y, 512
+    // contiguous bytes along z; 16-byte shared stores without conflicts)
     int maxord = 0;
     for (int k = 0; k < J.nout; ++k) maxord = max(maxord, J.o[k].order);
     if (maxord > 0) {
         const double2 *in = reinterpret_cast<const double2 *>(J.in) + base;
         for (int idx = tid; idx < nn * kDlLines; idx += 32 * MT) {
-            int j, l;
-            if (ydir) { j = idx % nn; l = idx / nn; }
-            else { l = idx % kDlLines; j = idx / kDlLines; }
+            const int l = idx % kDlLines, j = idx / kDlLines;
             double *dst = Xs + j * kDlNld + 2 * l;
             if (l < L) dl_cp16(dst, in + (long long)l * ls + (long long)j * es);
             else { dst[0] = 0.0; dst[1] = 0.0; }
@@ -142,7 +153,7 @@ __global__ void __launch_bounds__(32 * MT, PF ? 1 : (16 / MT > 2 ? 16 / MT : 2))
         asm volatile("cp.async.wait_group 0;\n" ::);
         __syncthreads();
         // fold in place: u_k = x_k + x_{nn-1-k} to row k, v_k = x_k - x_{nn-1-k}
-        // to row nn-1-k (k < ho; the middle row is u_ho = x_ho)
+        // to row nn-1-k (k < ho); row ho keeps x_ho
         for (int idx = tid; idx < ho * kDlCols; idx += 32 * MT) {
             const int k = idx / kDlCols, c = idx - k * kDlCols;
             const double a = Xs[k * kDlNld + c], b = Xs[(nn - 1 - k) * kDlNld + c];
@@ -153,33 +164,72 @@ __global__ void __launch_bounds__(32 * MT, PF ? 1 : (16 / MT > 2 ? 16 / MT : 2))
     }
     double vmax = 0.0;
     const double *maxabs_out = nullptr;
-    const int mt = warp;                     // this warp's 16 output rows
+    const int mt = warp;                     // this warp's 16 rows and 16-column slice of the middle row
     for (int oi = 0; oi < J.nout; ++oi) {
         const LineOut &o = J.o[oi];
         if (o.maxabs) maxabs_out = o.maxabs;
         if (o.order == 0) {
-            for (int idx = tid; idx < nn * kDlLines; idx += 32 * MT) {
-                int j, l;
-                if (ydir) { j = idx % nn; l = idx / nn; }
-                else { l = idx % kDlLines; j = idx / kDlLines; }
-                if (l >= L) continue;
-                const long long gi = base + (long long)l * ls + (long long)j * es;
-                const bool in_int = o.maxabs && j > 0 && j < nn - 1 && q0 + l > 0 && q0 + l < lpm - 1;
-                vmax = fmax(vmax, dl_store(o, gi, make_double2(0.0, 0.0), false, kx, m0 * o.m0, real0, in_int));
+            // four elements at a time, their loads before their stores
+            constexpr int B = 4;
+            for (int i0 = tid; i0 < nn * kDlLines; i0 += B * 32 * MT) {
+                double2 v[B];
+                long long gi[B];
+                bool ok[B];
+#pragma unroll
+                for (int e = 0; e < B; ++e) {
+                    const int idx = i0 + e * 32 * MT, l = idx % kDlLines, j = idx / kDlLines;
+                    ok[e] = idx < nn * kDlLines && l < L;
+                    gi[e] = base + (long long)l * ls + (long long)j * es;
+                    v[e] = make_double2(m0 * o.m0, 0.0);
+                }
+#pragma unroll
+                for (int tt = 0; tt < kLineXTerms; ++tt)
+                    if (o.xs[tt]) {
+                        const double2 c = dl_xcoef(o, tt, kx);
+#pragma unroll
+                        for (int e = 0; e < B; ++e)
+                            if (ok[e]) {
+                                const double2 x = reinterpret_cast<const double2 *>(o.xs[tt])[gi[e]];
+                                v[e].x += c.x * x.x - c.y * x.y;
+                                v[e].y += c.x * x.y + c.y * x.x;
+                            }
+                    }
+                double2 *out = reinterpret_cast<double2 *>(o.out);
+                if (o.beta != 0.0) {
+#pragma unroll
+                    for (int e = 0; e < B; ++e)
+                        if (ok[e]) {
+                            const double2 w = out[gi[e]];
+                            v[e].x += o.beta * w.x;
+                            v[e].y += o.beta * w.y;
+                        }
+                }
+#pragma unroll
+                for (int e = 0; e < B; ++e)
+                    if (ok[e]) {
+                        const int idx = i0 + e * 32 * MT, l = idx % kDlLines, j = idx / kDlLines;
+                        const double2 w = make_double2(o.sigma * v[e].x, o.sigma * v[e].y);
+                        out[gi[e]] = w;
+                        if (o.maxabs && j > 0 && j < nn - 1 && q0 + l > 0 && q0 + l < lpm - 1)
+                            vmax = fmax(vmax, hypot(w.x, w.y));
+                    }
             }
             continue;
         }
-        // A fragments of tile (ks, mt) at (ks MT + mt) 256, read from L2 a step ahead
-        const double2 *Ap = reinterpret_cast<const double2 *>(q.A[o.order - 1][0] + (size_t)mt * 256) + lane;
-        const double2 *Am = reinterpret_cast<const double2 *>(q.A[o.order - 1][1] + (size_t)mt * 256) + lane;
-        auto load_a = [&](const double2 *src, int ks, double (&a)[8]) {
-#pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                const double2 v = __ldg(src + (size_t)ks * MT * 128 + 32 * h);
-                a[2 * h] = v.x;
-                a[2 * h + 1] = v.y;
+        const double *opb = q.op[o.order - 1];
+        // the middle row: this warp's 16 columns of it for real column `lane`
+        {
+            const double *rowP = opb + 2 * blk + HR, *rowM = opb + 2 * blk + 2 * HR;
+            double part = (mt == 0) ? __ldg(opb + 2 * blk + 3 * HR) * Xs[ho * kDlNld + lane] : 0.0;
+#pragma unroll 4
+            for (int i = 0; i < 16; ++i) {
+                const int c = mt * 16 + i;
+                if (c < ho)
+                    part = fma(__ldg(rowP + c), Xs[c * kDlNld + lane],
+                               fma(__ldg(rowM + c), Xs[(nn - 1 - c) * kDlNld + lane], part));
             }
-        };
+            red[((oi & 1) * MT + mt) * 32 + lane] = part;
+        }
         double acc[2][NT][4];
 #pragma unroll
         for (int pm = 0; pm < 2; ++pm)
@@ -189,10 +239,10 @@ __global__ void __launch_bounds__(32 * MT, PF ? 1 : (16 / MT > 2 ? 16 / MT : 2))
                 for (int v = 0; v < 4; ++v) acc[pm][nt][v] = 0.0;
         // P = Ap u, then M = Am v (one GEMM at a time: fewer live registers).
         // B fragments of K step ks: u_k from row k, v_k from row nn-1-k; only
-        // the last step reaches k >= ho (u_ho the middle, zero beyond)
+        // the last step can reach k >= ho (zero there)
 #pragma unroll
         for (int pm = 0; pm < 2; ++pm) {
-            const double2 *Asrc = pm ? Am : Ap;
+            const double2 *Asrc = reinterpret_cast<const double2 *>(opb + pm * blk + (size_t)mt * 256) + lane;
             auto step = [&](int ks, const double (&a)[8], auto last) {
 #pragma unroll
                 for (int nt = 0; nt < NT; ++nt) {
@@ -202,49 +252,116 @@ __global__ void __launch_bounds__(32 * MT, PF ? 1 : (16 / MT > 2 ? 16 / MT : 2))
                     for (int v = 0; v < 4; ++v) {
                         const int k = ks * 16 + t + 4 * v;
                         const int row = pm ? nn - 1 - k : k;
-                        if (decltype(last)::value)
-                            b[v] = (pm ? k < ho : k <= ho) ? Xs[row * kDlNld + col] : 0.0;
-                        else
-                            b[v] = Xs[row * kDlNld + col];
+                        if (decltype(last)::value) b[v] = (k < ho) ? Xs[row * kDlNld + col] : 0.0;
+                        else b[v] = Xs[row * kDlNld + col];
                     }
                     dl_mma(acc[pm][nt], a, b);
                 }
             };
-            double a[8], an[8];
-            if (PF) load_a(Asrc, 0, a);
 #pragma unroll 1
             for (int ks = 0; ks < MT; ++ks) {
-                if (!PF) load_a(Asrc, ks, a);
-                else if (ks + 1 < MT) load_a(Asrc, ks + 1, an);
+                double a[8];
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const double2 v = __ldg(Asrc + (size_t)ks * MT * 128 + 32 * h);
+                    a[2 * h] = v.x;
+                    a[2 * h + 1] = v.y;
+                }
                 if (ks + 1 < MT) step(ks, a, std::false_type());
                 else step(ks, a, std::true_type());
-                if (PF && ks + 1 < MT) {
+            }
+            if (pm == 0) {
+                // the middle column: P_r += D(r, ho) x_ho
+                const double d0 = __ldg(opb + 2 * blk + mt * 16 + g), d1 = __ldg(opb + 2 * blk + mt * 16 + g + 8);
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) a[i] = an[i];
+                for (int nt = 0; nt < NT; ++nt) {
+                    const double xr = Xs[ho * kDlNld + nt * 8 + 2 * t], xi = Xs[ho * kDlNld + nt * 8 + 2 * t + 1];
+                    acc[0][nt][0] = fma(d0, xr, acc[0][nt][0]);
+                    acc[0][nt][1] = fma(d0, xi, acc[0][nt][1]);
+                    acc[0][nt][2] = fma(d1, xr, acc[0][nt][2]);
+                    acc[0][nt][3] = fma(d1, xi, acc[0][nt][3]);
                 }
             }
         }
         // y_r = P_r + M_r, y_{nn-1-r} = s (P_r - M_r); columns (2t, 2t+1) of
-        // n-tile nt are (re, im) of line 4 nt + t
-        const double s = (o.order == 1) ? -1.0 : 1.0;
+        // n-tile nt are (re, im) of line 4 nt + t.  Every load of the
+        // epilogue comes before its first store, so the loads of the 16
+        // elements need not wait for stores the compiler cannot prove
+        // disjoint from them.
+        {
+            const double s = (o.order == 1) ? -1.0 : 1.0;
+            double2 v[NT][2][2];
 #pragma unroll
-        for (int nt = 0; nt < NT; ++nt) {
-            const int l = nt * 4 + t;
-            if (l >= L) continue;
-            const bool chk = o.maxabs && q0 + l > 0 && q0 + l < lpm - 1;
-            const long long lb = base + (long long)l * ls;
+            for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
+                for (int h = 0; h < 2; ++h) {
+                    const double pr = acc[0][nt][2 * h], pi = acc[0][nt][2 * h + 1];
+                    const double mr = acc[1][nt][2 * h], mi = acc[1][nt][2 * h + 1];
+                    v[nt][h][0] = make_double2(m0 * o.m0 + o.fac * (pr + mr), real0 ? 0.0 : o.fac * (pi + mi));
+                    v[nt][h][1] = make_double2(m0 * o.m0 + o.fac * s * (pr - mr), real0 ? 0.0 : o.fac * s * (pi - mi));
+                }
+            auto valid = [&](int nt, int h) { return nt * 4 + t < L && mt * 16 + g + 8 * h < ho; };
+            auto gidx = [&](int nt, int h, int m) {
                 const int r = mt * 16 + g + 8 * h;
-                if (r >= he) continue;
-                const double pr = acc[0][nt][2 * h], pi = acc[0][nt][2 * h + 1];
-                const double mr = acc[1][nt][2 * h], mi = acc[1][nt][2 * h + 1];
-                vmax = fmax(vmax, dl_store(o, lb + (long long)r * es, make_double2(pr + mr, pi + mi), true, kx,
-                                           m0 * o.m0, real0, chk && r > 0));
-                if (r < ho)
-                    vmax = fmax(vmax, dl_store(o, lb + (long long)(nn - 1 - r) * es,
-                                               make_double2(s * (pr - mr), s * (pi - mi)), true, kx, m0 * o.m0,
-                                               real0, chk && r > 0));
+                return base + (long long)(nt * 4 + t) * ls + (long long)(m ? nn - 1 - r : r) * es;
+            };
+#pragma unroll
+            for (int tt = 0; tt < kLineXTerms; ++tt)
+                if (o.xs[tt]) {
+                    const double2 c = dl_xcoef(o, tt, kx);
+                    const double2 *src = reinterpret_cast<const double2 *>(o.xs[tt]);
+#pragma unroll
+                    for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h)
+#pragma unroll
+                            for (int m = 0; m < 2; ++m)
+                                if (valid(nt, h)) {
+                                    const double2 x = src[gidx(nt, h, m)];
+                                    v[nt][h][m].x += c.x * x.x - c.y * x.y;
+                                    v[nt][h][m].y += c.x * x.y + c.y * x.x;
+                                }
+                }
+            double2 *out = reinterpret_cast<double2 *>(o.out);
+            if (o.beta != 0.0) {
+#pragma unroll
+                for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+#pragma unroll
+                        for (int m = 0; m < 2; ++m)
+                            if (valid(nt, h)) {
+                                const double2 w = out[gidx(nt, h, m)];
+                                v[nt][h][m].x += o.beta * w.x;
+                                v[nt][h][m].y += o.beta * w.y;
+                            }
+            }
+#pragma unroll
+            for (int nt = 0; nt < NT; ++nt) {
+                const int l = nt * 4 + t;
+                const bool chk = o.maxabs && q0 + l > 0 && q0 + l < lpm - 1;
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+#pragma unroll
+                    for (int m = 0; m < 2; ++m)
+                        if (valid(nt, h)) {
+                            const double2 w = make_double2(o.sigma * v[nt][h][m].x, o.sigma * v[nt][h][m].y);
+                            out[gidx(nt, h, m)] = w;
+                            if (chk && mt * 16 + g + 8 * h > 0) vmax = fmax(vmax, hypot(w.x, w.y));
+                        }
+            }
+        }
+        __syncthreads();                     // the partial sums of the middle row
+        if (warp == 0) {
+            double y = 0.0;
+#pragma unroll
+            for (int w = 0; w < MT; ++w) y += red[((oi & 1) * MT + w) * 32 + lane];
+            const double yi = __shfl_down_sync(0xffffffffu, y, 1);
+            const int l = lane >> 1;
+            if (!(lane & 1) && l < L) {
+                const bool chk = o.maxabs && q0 + l > 0 && q0 + l < lpm - 1;
+                vmax = fmax(vmax, dl_store(o, base + (long long)l * ls + (long long)ho * es, make_double2(y, yi), true,
+                                           kx, m0 * o.m0, real0, chk));
             }
         }
     }
@@ -257,8 +374,8 @@ __global__ void __launch_bounds__(32 * MT, PF ? 1 : (16 / MT > 2 ? 16 / MT : 2))
     }
 }
 
-// the odd line lengths of the FFT kernel with half blocks up to 112 rows
-bool dlines_supported(int nn) { return (nn & 1) && lines_supported(nn) && (nn + 1) / 2 <= 16 * 7; }
+// odd line lengths of the FFT kernel with ho <= 128 (17 .. 257)
+bool dlines_supported(int nn) { return (nn & 1) && nn >= 17 && lines_supported(nn) && nn / 2 <= 16 * kDlMaxMT; }
 
 void free_dlines(ductgpu_ctx ctx)
 {
@@ -313,11 +430,11 @@ static void cheb_deriv_matrix(int nn, int ord, std::vector<long double> &D)
 }
 
 // The folded, packed operators of line length nn (built on first use:
-// not inside a stream capture).
+// not inside a stream capture): [order 1 chunk][order 2 chunk].
 static int dlines_ops(ductgpu_ctx ctx, int nn, const double **ops, int *hr)
 {
-    const int he = (nn + 1) / 2, ho = nn / 2, MT = (he + 15) / 16, HR = 16 * MT;
-    const size_t blk = (size_t)HR * HR;
+    const int ho = nn / 2, MT = (ho + 15) / 16, HR = 16 * MT;
+    const size_t blk = (size_t)HR * HR, chunk = dl_chunk(HR);
     *hr = HR;
     int slot = -1;
     for (int i = 0; i < ductgpu_ctx_s::kDlineSlots; ++i)
@@ -328,27 +445,26 @@ static int dlines_ops(ductgpu_ctx ctx, int nn, const double **ops, int *hr)
                                    ductgpu_ctx_s::kDlineSlots);
     if (ctx->capturing)
         return set_error(ctx, DUCTGPU_ESTATE, "derivative lines: operators for nn=%d first built inside a capture", nn);
-    // fold and pack: [ord][Ap, Am]
-    std::vector<double> packed(4 * blk, 0.0);
+    std::vector<double> packed(2 * chunk, 0.0);
     std::vector<long double> M;
     for (int ord = 0; ord < 2; ++ord) {
         cheb_deriv_matrix(nn, ord + 1, M);
         auto d = [&](int r, int c) { return M[(size_t)r + (size_t)nn * c]; };
-        for (int pm = 0; pm < 2; ++pm)
-            for (size_t idx = 0; idx < blk; ++idx) {
-                int row, col;
-                pack_slot((int)idx, MT, row, col);
-                long double v = 0.0L;
-                if (row < he) {
-                    if (pm == 0) {
-                        if (col < ho) v = 0.5L * (d(row, col) + d(row, nn - 1 - col));
-                        else if (col == ho) v = d(row, ho);   // the middle point
-                    } else if (col < ho) {
-                        v = 0.5L * (d(row, col) - d(row, nn - 1 - col));
-                    }
-                }
-                packed[(size_t)(2 * ord + pm) * blk + idx] = (double)v;
+        double *dst = packed.data() + ord * chunk;
+        for (size_t idx = 0; idx < blk; ++idx) {
+            int row, col;
+            pack_slot((int)idx, MT, row, col);
+            if (row < ho && col < ho) {
+                dst[idx] = (double)(0.5L * (d(row, col) + d(row, nn - 1 - col)));
+                dst[blk + idx] = (double)(0.5L * (d(row, col) - d(row, nn - 1 - col)));
             }
+        }
+        for (int r = 0; r < ho; ++r) {
+            dst[2 * blk + r] = (double)d(r, ho);
+            dst[2 * blk + HR + r] = (double)(0.5L * (d(ho, r) + d(ho, nn - 1 - r)));
+            dst[2 * blk + 2 * HR + r] = (double)(0.5L * (d(ho, r) - d(ho, nn - 1 - r)));
+        }
+        dst[2 * blk + 3 * HR] = (double)d(ho, ho);
     }
     double *dev = nullptr;
     DUCT_CUDA(ctx, cudaMalloc(&dev, packed.size() * sizeof(double)));
@@ -359,11 +475,11 @@ static int dlines_ops(ductgpu_ctx ctx, int nn, const double **ops, int *hr)
     return DUCTGPU_OK;
 }
 
-template <int MT, bool PF>
+template <int MT>
 static int launch_dlines(ductgpu_ctx ctx, DLineParams &q)
 {
-    const size_t smem = (size_t)q.nn * kDlNld * sizeof(double);
-    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_dlines<MT, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t smem = ((size_t)q.nn * kDlNld + 2 * (size_t)MT * 32) * sizeof(double);
+    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_dlines<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long long grid = (long long)q.ctas_per_job * q.lp.njobs;
     if (grid > 0x7fffffffLL) return set_error(ctx, DUCTGPU_EARG, "derivative lines: grid too large");
     if (ctx->prof_on && !ctx->capturing) {
@@ -383,7 +499,7 @@ static int launch_dlines(ductgpu_ctx ctx, DLineParams &q)
     }
     {
         LaunchScope ls(ctx, DUCTGPU_K_LINES);
-        k_dlines<MT, PF><<<(unsigned)grid, 32 * MT, smem, ctx->stream>>>(q);
+        k_dlines<MT><<<(unsigned)grid, 32 * MT, smem, ctx->stream>>>(q);
     }
     return check_cuda(ctx, cudaGetLastError(), "k_dlines");
 }
@@ -394,29 +510,26 @@ int dlines_launch(ductgpu_ctx ctx, const LineParams &p)
     DLineParams q;
     q.lp = p;
     q.nn = nn;
-    q.he = (nn + 1) / 2;
     q.ho = nn / 2;
     const double *ops = nullptr;
     int HR = 0;
     int rc = dlines_ops(ctx, nn, &ops, &HR);
     if (rc) return rc;
-    const size_t blk = (size_t)HR * HR;
-    for (int ord = 0; ord < 2; ++ord)
-        for (int pm = 0; pm < 2; ++pm) q.A[ord][pm] = ops + (size_t)(2 * ord + pm) * blk;
+    q.op[0] = ops;
+    q.op[1] = ops + dl_chunk(HR);
     const int lpm = (p.dir == 'y') ? p.mz : p.my;
     q.ctas_per_job = p.nmodes * ((lpm + kDlLines - 1) / kDlLines);
-    // dlines 1: A fragments loaded at each K step, two CTAs of the longest
-    // lines per SM (measured on the 193 x 193, 85-mode laplacian: 0.265 ms
-    // against 0.313 ms for the FFT kernel); 2: fetched a step ahead, more
-    // registers, one CTA per SM (0.345 ms)
-    const bool pf = ctx->dlines == 2;
-#define DL_CASE(mt) \
-    case mt: return pf ? launch_dlines<mt, true>(ctx, q) : launch_dlines<mt, false>(ctx, q);
     switch (HR / 16) {
-        DL_CASE(1) DL_CASE(2) DL_CASE(3) DL_CASE(4) DL_CASE(5) DL_CASE(6) DL_CASE(7)
+    case 1: return launch_dlines<1>(ctx, q);
+    case 2: return launch_dlines<2>(ctx, q);
+    case 3: return launch_dlines<3>(ctx, q);
+    case 4: return launch_dlines<4>(ctx, q);
+    case 5: return launch_dlines<5>(ctx, q);
+    case 6: return launch_dlines<6>(ctx, q);
+    case 7: return launch_dlines<7>(ctx, q);
+    case 8: return launch_dlines<8>(ctx, q);
     default: return set_error(ctx, DUCTGPU_EARG, "derivative lines: line length %d", nn);
     }
-#undef DL_CASE
 }
 
 }  // namespace duct

@@ -337,7 +337,10 @@ int transpose_dev(ductgpu_ctx ctx, const double *in, double *out, long long A, l
 //                  + xc2_t (i kx)^2) xs_t + [mode 0] m0)
 // with D the reference's derivyz between transyz -1 / +1 along the launch's
 // direction (fac already divided by aspect^order for z).  maxabs (device,
-// or null): atomic max of |out| over the interior points.
+// or null): atomic max of |out| over the interior points.  No output of a
+// launch may write, or read (as an x-term), the field that another output
+// of the launch writes: the kernels order an element's loads only before
+// its own store (lines_launch checks).
 constexpr int kLineXTerms = 5;
 constexpr int kMaxLineOut = 3;
 constexpr int kMaxLineJobs = 4;

@@ -192,12 +192,10 @@ int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel);
 int ductgpu_set_rect_fold(ductgpu_ctx ctx, int on);
 /* Kernel of the y / z derivative lines of the DNS operators: 1 (default)
  * the collocation matrices' flip-symmetric half blocks on the FP64 tensor
- * cores (odd line lengths 17..193; operators built in long double), 2 the
- * same with the operator fragments fetched a K step ahead (more registers,
- * one CTA of the longest lines per SM), 0 the FFT-based transyz + derivyz
- * + transyz chain in one kernel (every supported length; its half-length
- * DCT-I carries a few 1e-12 of relative error at 129 and 193 points, the
- * tensor-core form a few 1e-13).                                          */
+ * cores (odd line lengths 17..257; operators built in long double), 0 the
+ * FFT-based transyz + derivyz + transyz chain in one kernel (its half-
+ * length DCT-I carries a few 1e-12 of relative error at 129 and 193
+ * points, the tensor-core form a few 1e-13).                              */
 int ductgpu_set_line_kernel(ductgpu_ctx ctx, int kernel);
 /* Autotuner: times the FP64 batched solve of these device fields with each
  * pass kernel (reps runs each, after one warm-up; the fields' sol arrays
