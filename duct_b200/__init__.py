@@ -307,8 +307,8 @@ class Context:
         return tune.apply(self, int(my), int(mz if mz is not None else my), path or tune.TABLE)
 
     def set_line_kernel(self, kernel):
-        """1 (default): derivative lines on the FP64 tensor cores, 0: the FFT
-        kernel."""
+        """1 (default), 2: derivative lines on the FP64 tensor cores with 8 or
+        16 lines per CTA, 0: the FFT kernel."""
         self._check(lib().ductgpu_set_line_kernel(self.h, int(kernel)))
 
     def set_rect_fold(self, on):

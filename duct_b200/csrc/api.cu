@@ -416,7 +416,7 @@ int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel)
 
 int ductgpu_set_line_kernel(ductgpu_ctx ctx, int kernel)
 {
-    if (!ctx || kernel < 0 || kernel > 1) return DUCTGPU_EARG;
+    if (!ctx || kernel < 0 || kernel > 2) return DUCTGPU_EARG;
     ctx->dlines = kernel;
     return DUCTGPU_OK;
 }

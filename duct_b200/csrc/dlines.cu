@@ -34,9 +34,13 @@
 
 namespace duct {
 
-constexpr int kDlLines = 16;                 // complex lines per CTA
-constexpr int kDlCols = 2 * kDlLines;        // real columns
-constexpr int kDlNld = kDlCols + 8;          // row stride of the staged lines: B fragments conflict free
+// A CTA of NT n-tiles takes 4 NT complex lines (8 NT real columns); the
+// staged rows are 8 NT + 4 doubles apart, a stride of 4 mod 16 doubles, so
+// that the B-fragment loads of a half-warp (rows t, columns g < 4) meet 16
+// distinct bank pairs.
+template <int NT> struct DlShape {
+    static constexpr int lines = 4 * NT, cols = 8 * NT, nld = 8 * NT + 4;
+};
 constexpr int kDlMaxMT = 8;                  // ho <= 128: line lengths up to 257
 
 // Operators of one order, HR = 16 MT: Ap and Am (HR x HR each, rows and
@@ -105,12 +109,14 @@ __device__ __forceinline__ double dl_store(const LineOut &o, long long gi, doubl
     return interior ? hypot(v.x, v.y) : 0.0;
 }
 
-// Registers for about 16 resident warps per SM (two CTAs at least).
-template <int MT>
-__global__ void __launch_bounds__(32 * MT, 16 / MT > 2 ? 16 / MT : 2)
+// Registers for about WARPS resident warps per SM, two CTAs at least (a
+// latency-bound kernel: the staging, the L2 operator loads and the
+// epilogue's loads are hidden by other warps rather than by prefetching).
+template <int MT, int NT, int WARPS>
+__global__ void __launch_bounds__(32 * MT, WARPS / MT > 2 ? WARPS / MT : 2)
     k_dlines(const __grid_constant__ DLineParams q)
 {
-    constexpr int NT = 4;                    // n-tiles of 8 real columns: 16 complex lines
+    constexpr int kDlLines = DlShape<NT>::lines, kDlCols = DlShape<NT>::cols, kDlNld = DlShape<NT>::nld;
     constexpr int HR = 16 * MT;
     constexpr size_t blk = (size_t)HR * HR;
     extern __shared__ __align__(16) double Xs[];   // [nn][kDlNld] lines ((re, im) column pairs), then red
@@ -220,16 +226,19 @@ __global__ void __launch_bounds__(32 * MT, 16 / MT > 2 ? 16 / MT : 2)
         // the middle row: this warp's 16 columns of it for real column `lane`
         {
             const double *rowP = opb + 2 * blk + HR, *rowM = opb + 2 * blk + 2 * HR;
-            double part = (mt == 0) ? __ldg(opb + 2 * blk + 3 * HR) * Xs[ho * kDlNld + lane] : 0.0;
-#pragma unroll 4
+            const int cl = lane < kDlCols ? lane : 0;     // lanes beyond the columns repeat column 0
+            double part = (mt == 0) ? __ldg(opb + 2 * blk + 3 * HR) * Xs[ho * kDlNld + cl] : 0.0;
+#pragma unroll
             for (int i = 0; i < 16; ++i) {
                 const int c = mt * 16 + i;
                 if (c < ho)
-                    part = fma(__ldg(rowP + c), Xs[c * kDlNld + lane],
-                               fma(__ldg(rowM + c), Xs[(nn - 1 - c) * kDlNld + lane], part));
+                    part = fma(__ldg(rowP + c), Xs[c * kDlNld + cl],
+                               fma(__ldg(rowM + c), Xs[(nn - 1 - c) * kDlNld + cl], part));
             }
             red[((oi & 1) * MT + mt) * 32 + lane] = part;
         }
+        // the middle column's coefficients D(r, ho) of this thread's rows
+        const double d0 = __ldg(opb + 2 * blk + mt * 16 + g), d1 = __ldg(opb + 2 * blk + mt * 16 + g + 8);
         double acc[2][NT][4];
 #pragma unroll
         for (int pm = 0; pm < 2; ++pm)
@@ -272,7 +281,6 @@ __global__ void __launch_bounds__(32 * MT, 16 / MT > 2 ? 16 / MT : 2)
             }
             if (pm == 0) {
                 // the middle column: P_r += D(r, ho) x_ho
-                const double d0 = __ldg(opb + 2 * blk + mt * 16 + g), d1 = __ldg(opb + 2 * blk + mt * 16 + g + 8);
 #pragma unroll
                 for (int nt = 0; nt < NT; ++nt) {
                     const double xr = Xs[ho * kDlNld + nt * 8 + 2 * t], xi = Xs[ho * kDlNld + nt * 8 + 2 * t + 1];
@@ -475,11 +483,11 @@ static int dlines_ops(ductgpu_ctx ctx, int nn, const double **ops, int *hr)
     return DUCTGPU_OK;
 }
 
-template <int MT>
+template <int MT, int NT, int WARPS>
 static int launch_dlines(ductgpu_ctx ctx, DLineParams &q)
 {
-    const size_t smem = ((size_t)q.nn * kDlNld + 2 * (size_t)MT * 32) * sizeof(double);
-    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_dlines<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t smem = ((size_t)q.nn * DlShape<NT>::nld + 2 * (size_t)MT * 32) * sizeof(double);
+    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_dlines<MT, NT, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long long grid = (long long)q.ctas_per_job * q.lp.njobs;
     if (grid > 0x7fffffffLL) return set_error(ctx, DUCTGPU_EARG, "derivative lines: grid too large");
     if (ctx->prof_on && !ctx->capturing) {
@@ -499,7 +507,7 @@ static int launch_dlines(ductgpu_ctx ctx, DLineParams &q)
     }
     {
         LaunchScope ls(ctx, DUCTGPU_K_LINES);
-        k_dlines<MT><<<(unsigned)grid, 32 * MT, smem, ctx->stream>>>(q);
+        k_dlines<MT, NT, WARPS><<<(unsigned)grid, 32 * MT, smem, ctx->stream>>>(q);
     }
     return check_cuda(ctx, cudaGetLastError(), "k_dlines");
 }
@@ -518,18 +526,21 @@ int dlines_launch(ductgpu_ctx ctx, const LineParams &p)
     q.op[0] = ops;
     q.op[1] = ops + dl_chunk(HR);
     const int lpm = (p.dir == 'y') ? p.mz : p.my;
-    q.ctas_per_job = p.nmodes * ((lpm + kDlLines - 1) / kDlLines);
+    // dlines 1: 8 lines per CTA with registers for 32 resident warps per SM
+    // (the fastest measured on the 193 x 193, 85-mode DNS step: 9.56 ms a
+    // step, against 9.97 ms with 24 warps, 10.8 ms with 16 and 10.9 ms for
+    // 16 lines per CTA with 16 warps; 4 lines per CTA: 10.1 ms); 2: 16
+    // lines per CTA, 16 warps (each operator fragment feeds twice the MMAs)
+    const bool wide = ctx->dlines == 2;
+    const int lines = wide ? DlShape<4>::lines : DlShape<2>::lines;
+    q.ctas_per_job = p.nmodes * ((lpm + lines - 1) / lines);
+#define DL_CASE(mt) \
+    case mt: return wide ? launch_dlines<mt, 4, 16>(ctx, q) : launch_dlines<mt, 2, 32>(ctx, q);
     switch (HR / 16) {
-    case 1: return launch_dlines<1>(ctx, q);
-    case 2: return launch_dlines<2>(ctx, q);
-    case 3: return launch_dlines<3>(ctx, q);
-    case 4: return launch_dlines<4>(ctx, q);
-    case 5: return launch_dlines<5>(ctx, q);
-    case 6: return launch_dlines<6>(ctx, q);
-    case 7: return launch_dlines<7>(ctx, q);
-    case 8: return launch_dlines<8>(ctx, q);
+        DL_CASE(1) DL_CASE(2) DL_CASE(3) DL_CASE(4) DL_CASE(5) DL_CASE(6) DL_CASE(7) DL_CASE(8)
     default: return set_error(ctx, DUCTGPU_EARG, "derivative lines: line length %d", nn);
     }
+#undef DL_CASE
 }
 
 }  // namespace duct

@@ -192,10 +192,11 @@ int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel);
 int ductgpu_set_rect_fold(ductgpu_ctx ctx, int on);
 /* Kernel of the y / z derivative lines of the DNS operators: 1 (default)
  * the collocation matrices' flip-symmetric half blocks on the FP64 tensor
- * cores (odd line lengths 17..257; operators built in long double), 0 the
- * FFT-based transyz + derivyz + transyz chain in one kernel (its half-
- * length DCT-I carries a few 1e-12 of relative error at 129 and 193
- * points, the tensor-core form a few 1e-13).                              */
+ * cores, 8 lines per CTA (odd line lengths 17..257; operators built in
+ * long double), 2 the same with 16 lines per CTA, 0 the FFT-based transyz
+ * + derivyz + transyz chain in one kernel (its half-length DCT-I carries a
+ * few 1e-12 of relative error at 129 and 193 points, the tensor-core form
+ * a few 1e-13).                                                           */
 int ductgpu_set_line_kernel(ductgpu_ctx ctx, int kernel);
 /* Autotuner: times the FP64 batched solve of these device fields with each
  * pass kernel (reps runs each, after one warm-up; the fields' sol arrays

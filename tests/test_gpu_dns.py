@@ -63,12 +63,12 @@ def dev(ctx, a):
     return d
 
 
-@pytest.mark.parametrize("kernel", [1, 0])
+@pytest.mark.parametrize("kernel", [1, 2, 0])
 @pytest.mark.parametrize("my,mz,aspect", [(33, 33, 1.0), (17, 33, 2.0), (65, 49, 0.5), (193, 129, 1.5),
                                           (145, 257, 2.0)])
 def test_line_operators_match_oracle(ctx, oracle, my, mz, aspect, kernel):
-    """Both line kernels: the collocation matrices' half blocks on the FP64
-    tensor cores (1) and the FFT chain (0)."""
+    """Every line kernel: the collocation matrices' half blocks on the FP64
+    tensor cores (1: 8 lines per CTA, 2: 16) and the FFT chain (0)."""
     ctx.set_line_kernel(kernel)
     tol = 4e-11 if kernel == 0 and max(my, mz) >= 129 else 1e-12
     nm = 6
@@ -103,7 +103,7 @@ def test_line_operators_match_oracle(ctx, oracle, my, mz, aspect, kernel):
     ctx.set_line_kernel(1)
 
 
-@pytest.mark.parametrize("kernel", [1, 0])
+@pytest.mark.parametrize("kernel", [1, 2, 0])
 def test_update_uvwp_matches_oracle(ctx, oracle, kernel):
     ctx.set_line_kernel(kernel)
     my, nm, aspect = 33, 5, 1.5
