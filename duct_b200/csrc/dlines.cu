@@ -134,6 +134,7 @@ __global__ void __launch_bounds__(32 * MT, WARPS / MT > 2 ? WARPS / MT : 2)
     const int q0 = (rr - mode * cpm) * kDlLines;
     const int L = min(kDlLines, lpm - q0);
     const long long base = mode * ms + (long long)q0 * ls;
+    const int lsi = (int)ls, esi = (int)es;  // strides within a mode (a plane holds < 2^31 points)
     const double kx = p.xalp[mode];
     const bool real0 = p.real0 && mode == 0;
     const int nn = q.nn, ho = q.ho;
@@ -152,7 +153,7 @@ __global__ void __launch_bounds__(32 * MT, WARPS / MT > 2 ? WARPS / MT : 2)
         for (int idx = tid; idx < nn * kDlLines; idx += 32 * MT) {
             const int l = idx % kDlLines, j = idx / kDlLines;
             double *dst = Xs + j * kDlNld + 2 * l;
-            if (l < L) dl_cp16(dst, in + (long long)l * ls + (long long)j * es);
+            if (l < L) dl_cp16(dst, in + (l * lsi + j * esi));
             else { dst[0] = 0.0; dst[1] = 0.0; }
         }
         asm volatile("cp.async.commit_group;\n" ::);
@@ -179,13 +180,13 @@ __global__ void __launch_bounds__(32 * MT, WARPS / MT > 2 ? WARPS / MT : 2)
             constexpr int B = 4;
             for (int i0 = tid; i0 < nn * kDlLines; i0 += B * 32 * MT) {
                 double2 v[B];
-                long long gi[B];
+                int gi[B];
                 bool ok[B];
 #pragma unroll
                 for (int e = 0; e < B; ++e) {
                     const int idx = i0 + e * 32 * MT, l = idx % kDlLines, j = idx / kDlLines;
                     ok[e] = idx < nn * kDlLines && l < L;
-                    gi[e] = base + (long long)l * ls + (long long)j * es;
+                    gi[e] = l * lsi + j * esi;
                     v[e] = make_double2(m0 * o.m0, 0.0);
                 }
 #pragma unroll
@@ -195,12 +196,12 @@ __global__ void __launch_bounds__(32 * MT, WARPS / MT > 2 ? WARPS / MT : 2)
 #pragma unroll
                         for (int e = 0; e < B; ++e)
                             if (ok[e]) {
-                                const double2 x = reinterpret_cast<const double2 *>(o.xs[tt])[gi[e]];
+                                const double2 x = (reinterpret_cast<const double2 *>(o.xs[tt]) + base)[gi[e]];
                                 v[e].x += c.x * x.x - c.y * x.y;
                                 v[e].y += c.x * x.y + c.y * x.x;
                             }
                     }
-                double2 *out = reinterpret_cast<double2 *>(o.out);
+                double2 *out = reinterpret_cast<double2 *>(o.out) + base;
                 if (o.beta != 0.0) {
 #pragma unroll
                     for (int e = 0; e < B; ++e)
@@ -309,15 +310,16 @@ __global__ void __launch_bounds__(32 * MT, WARPS / MT > 2 ? WARPS / MT : 2)
                     v[nt][h][1] = make_double2(m0 * o.m0 + o.fac * s * (pr - mr), real0 ? 0.0 : o.fac * s * (pi - mi));
                 }
             auto valid = [&](int nt, int h) { return nt * 4 + t < L && mt * 16 + g + 8 * h < ho; };
+            // offsets from the CTA's first element: within one mode, 32 bits
             auto gidx = [&](int nt, int h, int m) {
                 const int r = mt * 16 + g + 8 * h;
-                return base + (long long)(nt * 4 + t) * ls + (long long)(m ? nn - 1 - r : r) * es;
+                return (nt * 4 + t) * lsi + (m ? nn - 1 - r : r) * esi;
             };
 #pragma unroll
             for (int tt = 0; tt < kLineXTerms; ++tt)
                 if (o.xs[tt]) {
                     const double2 c = dl_xcoef(o, tt, kx);
-                    const double2 *src = reinterpret_cast<const double2 *>(o.xs[tt]);
+                    const double2 *src = reinterpret_cast<const double2 *>(o.xs[tt]) + base;
 #pragma unroll
                     for (int nt = 0; nt < NT; ++nt)
 #pragma unroll
@@ -330,7 +332,7 @@ __global__ void __launch_bounds__(32 * MT, WARPS / MT > 2 ? WARPS / MT : 2)
                                     v[nt][h][m].y += c.x * x.y + c.y * x.x;
                                 }
                 }
-            double2 *out = reinterpret_cast<double2 *>(o.out);
+            double2 *out = reinterpret_cast<double2 *>(o.out) + base;
             if (o.beta != 0.0) {
 #pragma unroll
                 for (int nt = 0; nt < NT; ++nt)
