@@ -6,8 +6,8 @@
 //   (dyy + dzz) u - u / (alphak(k) dt nu) = 1,  u = 0 on the walls,
 // and its flow rate, all RK indices in one batched solve.  impose: the flow
 // rate of the real part of mode 0 and the correction u0 += fac premassfu(k),
-// fac = (csum - flow)/premassf(k), in ONE single-CTA kernel, so the step
-// needs no host round trip (iflag 1).
+// fac = (csum - flow)/premassf(k), on the device (a partial-sum kernel and
+// an apply kernel), so the step needs no host round trip (iflag 1).
 //
 // The flow rate is the Clenshaw-Curtis quadrature of the physical values,
 // sum_pq w_p w_q u_pq * aspect, which integrates the same Chebyshev
@@ -65,21 +65,42 @@ __global__ void __launch_bounds__(1024) k_mf_store(const double *sol, double *pu
     if (threadIdx.x == 0) pf[k] = acc * aspect;
 }
 
-// impose_mass_flow on the first (mode 0) plane of u: sum -> *sum_out; with
-// iflag 1, u0.re += (csum - sum) / pf * pu.
-__global__ void __launch_bounds__(1024) k_mf_impose(double *u, const double *w, int m, double aspect,
-                                                    const double *pu, const double *pf, double csum, int iflag,
-                                                    double *sum_out)
+// impose_mass_flow on the first (mode 0) plane of u in two kernels over
+// kMfBlocks CTAs: per-CTA partial sums of the quadrature, then every CTA
+// adds the partials in the same fixed order (so the result does not depend
+// on scheduling), CTA 0 stores the flow rate, and with iflag 1 every CTA
+// corrects its slice, u0.re += (csum - sum) / pf * pu.
+constexpr int kMfBlocks = 64;
+constexpr int kMfThreads = 256;
+
+__global__ void __launch_bounds__(kMfThreads) k_mf_partial(const double *u, const double *w, int m, double *part)
 {
     __shared__ double red[33];
-    const long plane = (long)m * m;
+    const long plane = (long)m * m, chunk = (plane + kMfBlocks - 1) / kMfBlocks;
+    const long i0 = blockIdx.x * chunk, i1 = min(plane, i0 + chunk);
     double acc = 0.0;
-    for (long i = threadIdx.x; i < plane; i += blockDim.x) acc += w[i % m] * w[i / m] * u[2 * i];
-    const double sumg = block_sum(acc, red) * aspect;
-    if (threadIdx.x == 0) *sum_out = sumg;
+    for (long i = i0 + threadIdx.x; i < i1; i += kMfThreads) acc += w[i % m] * w[i / m] * u[2 * i];
+    acc = block_sum(acc, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+__global__ void __launch_bounds__(kMfThreads) k_mf_apply(double *u, double aspect, const double *pu,
+                                                        const double *pf, double csum, int iflag, const double *part,
+                                                        int m, double *sum_out)
+{
+    __shared__ double tot;
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int b = 0; b < kMfBlocks; ++b) s += part[b];
+        tot = s * aspect;
+        if (blockIdx.x == 0) *sum_out = tot;
+    }
+    __syncthreads();
     if (!iflag) return;
-    const double fac = (csum - sumg) / *pf;
-    for (long i = threadIdx.x; i < plane; i += blockDim.x) u[2 * i] += fac * pu[i];
+    const double fac = (csum - tot) / *pf;
+    const long plane = (long)m * m, chunk = (plane + kMfBlocks - 1) / kMfBlocks;
+    const long i0 = blockIdx.x * chunk, i1 = min(plane, i0 + chunk);
+    for (long i = i0 + threadIdx.x; i < i1; i += kMfThreads) u[2 * i] += fac * pu[i];
 }
 
 }  // namespace duct
@@ -107,7 +128,7 @@ extern "C" int ductgpu_precomp_mass_flow(ductgpu_ctx ctx, double dtp, const doub
     ctx->mf_mrk = 0;
     DUCT_CUDA(ctx, cudaMalloc(&ctx->mf_u, plane * mrk * sizeof(double)));
     DUCT_CUDA(ctx, cudaMalloc(&ctx->mf_f, mrk * sizeof(double)));
-    DUCT_CUDA(ctx, cudaMalloc(&ctx->mf_sum, sizeof(double)));
+    DUCT_CUDA(ctx, cudaMalloc(&ctx->mf_sum, (1 + kMfBlocks) * sizeof(double)));   // the sum, then the partials
     int rc = ensure(ctx, ctx->io, 2 * 2 * plane * mrk * sizeof(double));
     if (rc) return rc;
     double *rhs = ctx->io.buf, *sol = rhs + 2 * plane * mrk;
@@ -159,8 +180,11 @@ extern "C" int ductgpu_impose_mass_flow_dev(ductgpu_ctx ctx, double *csum, int k
     const int k = iflag ? krk - 1 : 0;
     {
         LaunchScope ls(ctx, DUCTGPU_K_OTHER);
-        k_mf_impose<<<1, 1024, 0, ctx->stream>>>(u, ctx->ccw, m, ctx->mf_aspect, ctx->mf_u + (size_t)m * m * k,
-                                                 ctx->mf_f + k, *csum, iflag, ctx->mf_sum);
+        double *part = ctx->mf_sum + 1;
+        k_mf_partial<<<kMfBlocks, kMfThreads, 0, ctx->stream>>>(u, ctx->ccw, m, part);
+        k_mf_apply<<<kMfBlocks, kMfThreads, 0, ctx->stream>>>(u, ctx->mf_aspect, ctx->mf_u + (size_t)m * m * k,
+                                                              ctx->mf_f + k, *csum, iflag, part, m, ctx->mf_sum);
+        ctx->launches += 1;     // the scope counted the first of the two
     }
     DUCT_CUDA(ctx, cudaGetLastError());
     if (iflag) return DUCTGPU_OK;
