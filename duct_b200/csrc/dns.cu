@@ -80,8 +80,8 @@ __device__ __forceinline__ void fft_step1(double2 (&v)[R], double2 *wk, const do
     for (int k1 = 0; k1 < R; ++k1) wk[(k1 * R + c) * TQ + g] = (k1 == 0) ? v[0] : cmul(v[k1], tw[c * k1]);
 }
 
-template <int R, int TQ>
-__global__ void __launch_bounds__(R * TQ) k_advx(const __grid_constant__ AdvParams p, const double2 *__restrict__ twg)
+template <int R, int TQ, int MINB = 1>
+__global__ void __launch_bounds__(R * TQ, MINB) k_advx(const __grid_constant__ AdvParams p, const double2 *__restrict__ twg)
 {
     constexpr int N = R * R, NT = R * TQ;
     extern __shared__ __align__(16) double2 sm[];
@@ -197,20 +197,20 @@ __global__ void __launch_bounds__(R * TQ) k_advx(const __grid_constant__ AdvPara
     }
 }
 
-template <int R, int TQ>
+template <int R, int TQ, int MINB = 1>
 static int launch_advx(ductgpu_ctx ctx, const AdvParams &p)
 {
     constexpr int N = R * R, NT = R * TQ;
     const double2 *tw = twiddle_table(ctx, N);
     if (!tw) return set_error(ctx, DUCTGPU_ESTATE, "advection3d: twiddle table for mgalx=%d unavailable", N);
     const size_t smem = ((size_t)N + 2 * (size_t)N * TQ) * sizeof(double2);
-    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_advx<R, TQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_advx<R, TQ, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long long grid = (p.P + TQ - 1) / TQ;
     // algorithmic bytes: u, v, w read, eight product fields written
     if (ctx->prof_on && !ctx->capturing) ctx->prof_bytes[DUCTGPU_K_ADVECTION] += 11.0 * 16.0 * p.P * p.M;
     {
         LaunchScope ls(ctx, DUCTGPU_K_ADVECTION);
-        k_advx<R, TQ><<<(unsigned)grid, NT, smem, ctx->stream>>>(p, tw);
+        k_advx<R, TQ, MINB><<<(unsigned)grid, NT, smem, ctx->stream>>>(p, tw);
     }
     return check_cuda(ctx, cudaGetLastError(), "k_advx");
 }
@@ -223,7 +223,10 @@ static int advx_launch(ductgpu_ctx ctx, const AdvParams &p, int mgalx)
     case 16: return launch_advx<4, 32>(ctx, p);
     case 64: return launch_advx<8, 16>(ctx, p);
     case 144: return launch_advx<12, 8>(ctx, p);
-    case 256: return launch_advx<16, 8>(ctx, p);
+    // mgalx = 256: registers for three CTAs per SM (168; some spilling), 1.13
+    // against 1.21 ms a config-4 step with the compiler's 255 at two CTAs;
+    // 64-thread CTAs (4 points) at 4 or 6 per SM measured 1.27 / 1.19 ms
+    case 256: return launch_advx<16, 8, 3>(ctx, p);
     default: return set_error(ctx, DUCTGPU_EARG, "advection3d: mgalx=%d (16, 64, 144 or 256)", mgalx);
     }
 }
