@@ -44,7 +44,7 @@ EXPORTS = [
     "ductgpu_wallstressx_dev", "ductgpu_energy_fou_dev", "ductgpu_statistics_fou_dev",
     "ductgpu_dns_create", "ductgpu_dns_destroy", "ductgpu_dns_set_fields", "ductgpu_dns_get_fields",
     "ductgpu_dns_field", "ductgpu_dns_set_graphs", "ductgpu_dns_substep", "ductgpu_dns_steps",
-    "ductgpu_dns_statistics", "ductgpu_profile_bytes", "ductgpu_dns_set_forcing",
+    "ductgpu_dns_statistics", "ductgpu_profile_bytes", "ductgpu_profile_flops", "ductgpu_dns_set_forcing",
     "ductgpu_dns_wallstress_after", "ductgpu_dns_grad_wallstress", "ductgpu_set_rect_fold",
     "ductgpu_set_line_kernel",
 ]
@@ -157,6 +157,7 @@ def lib():
             "ductgpu_dns_steps": [P, I, I],
             "ductgpu_dns_statistics": [P, P, P, P, P, P, C.POINTER(I), C.POINTER(I), P],
             "ductgpu_profile_bytes": [P, I, C.POINTER(D)],
+            "ductgpu_profile_flops": [P, I, C.POINTER(D)],
             "ductgpu_dns_set_forcing": [P, P, P, P],
             "ductgpu_set_rect_fold": [P, I],
             "ductgpu_set_line_kernel": [P, I],
@@ -627,6 +628,11 @@ class Context:
         b = C.c_double()
         self._check(lib().ductgpu_profile_bytes(self.h, int(kind), C.byref(b)))
         return b.value
+
+    def profile_flops(self, kind):
+        f = C.c_double()
+        self._check(lib().ductgpu_profile_flops(self.h, int(kind), C.byref(f)))
+        return f.value
 
 
 def _dp(a):

@@ -1238,6 +1238,7 @@ int ductgpu_profile_reset(ductgpu_ctx ctx)
         ctx->prof_ms[k] = 0.0;
         ctx->prof_n[k] = 0;
         ctx->prof_bytes[k] = 0.0;
+        ctx->prof_flops[k] = 0.0;
     }
     return DUCTGPU_OK;
 }
@@ -1255,6 +1256,13 @@ int ductgpu_profile_bytes(ductgpu_ctx ctx, int kind, double *bytes)
 {
     if (!ctx || kind < 0 || kind >= DUCTGPU_K_COUNT || !bytes) return DUCTGPU_EARG;
     *bytes = ctx->prof_bytes[kind];
+    return DUCTGPU_OK;
+}
+
+int ductgpu_profile_flops(ductgpu_ctx ctx, int kind, double *flops)
+{
+    if (!ctx || kind < 0 || kind >= DUCTGPU_K_COUNT || !flops) return DUCTGPU_EARG;
+    *flops = ctx->prof_flops[kind];
     return DUCTGPU_OK;
 }
 

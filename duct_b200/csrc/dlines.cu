@@ -506,6 +506,12 @@ static int launch_dlines(ductgpu_ctx ctx, DLineParams &q)
             fields += in ? 1.0 : 0.0;
         }
         ctx->prof_bytes[DUCTGPU_K_LINES] += fields * 16.0 * q.lp.my * q.lp.mz * q.lp.nmodes;
+        // per CTA and derivative output: 2 GEMMs x MT warps x MT K steps x NT
+        // m16n8k16 MMAs of 2 x 16 x 8 x 16 flops
+        int nderiv = 0;
+        for (int i = 0; i < q.lp.njobs; ++i)
+            for (int k = 0; k < q.lp.job[i].nout; ++k) nderiv += q.lp.job[i].o[k].order > 0;
+        ctx->prof_flops[DUCTGPU_K_LINES] += (double)q.ctas_per_job * nderiv * 2.0 * MT * MT * NT * 4096.0;
     }
     {
         LaunchScope ls(ctx, DUCTGPU_K_LINES);

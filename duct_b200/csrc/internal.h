@@ -173,6 +173,7 @@ struct ductgpu_ctx_s {
     double prof_ms[DUCTGPU_K_COUNT] = {};
     long long prof_n[DUCTGPU_K_COUNT] = {};
     double prof_bytes[DUCTGPU_K_COUNT] = {};   // algorithmic bytes of the launches (kernels that count them)
+    double prof_flops[DUCTGPU_K_COUNT] = {};   // executed tensor-core flops (kernels that count them)
 };
 
 namespace duct {

@@ -558,6 +558,10 @@ int ductgpu_profile_read(ductgpu_ctx ctx, int kind, double *ms, long long *launc
  * the kernels that report them (DUCTGPU_K_LINES, DUCTGPU_K_ADVECTION);
  * with profiling on only.                                                 */
 int ductgpu_profile_bytes(ductgpu_ctx ctx, int kind, double *bytes);
+/* Tensor-core flops executed (padded tiles included) by the launches of
+ * class `kind` since the last reset, for the kernels that report them
+ * (DUCTGPU_K_LINES on the FP64 tensor cores); with profiling on only.     */
+int ductgpu_profile_flops(ductgpu_ctx ctx, int kind, double *flops);
 
 #ifdef __cplusplus
 }
