@@ -516,6 +516,12 @@ int lines_launch(ductgpu_ctx ctx, const LineParams &p)
                                          i, k, i2, k2);
                 }
         }
+    // a job's input against the other jobs' destinations (its own may be in place)
+    for (int i = 0; i < p.njobs; ++i)
+        for (int i2 = 0; i2 < p.njobs; ++i2)
+            for (int k2 = 0; k2 < p.job[i2].nout && i2 != i; ++k2)
+                if (p.job[i].in && p.job[i].in == p.job[i2].o[k2].out)
+                    return set_error(ctx, DUCTGPU_EARG, "lines: job %d reads what job %d output %d writes", i, i2, k2);
     const int nn = (p.dir == 'y') ? p.my : p.mz;
     if (ctx->dlines && dlines_supported(nn)) return dlines_launch(ctx, p);
     switch (nn - 1) {

@@ -121,6 +121,22 @@ def test_update_uvwp_matches_oracle(ctx, oracle, kernel):
     ctx.set_line_kernel(1)
 
 
+def test_update_uvwp_rejects_aliased_outputs(ctx):
+    """update_uvwp writes p, v and u from one line launch; passing the same
+    array as u and v would make two outputs of the launch write one field,
+    which the kernels cannot order: the call is refused before any launch."""
+    my, nm = 33, 3
+    xalp = 0.5 * np.arange(nm)
+    d = [dev(ctx, smooth(my, my, nm, s)) for s in (41, 42, 43, 44)]
+    before = [a.download() for a in d]
+    with pytest.raises(D.DuctGPUError) as e:
+        ctx.update_uvwp_dev(d[0], d[0], d[1], d[2], d[3], xalp, 29 / 96, 37 / 160, 1e-3, 1 / 2000)
+    assert e.value.code == D.EARG and "writes" in str(e.value)
+    for a, b in zip(d, before):
+        assert np.array_equal(a.download(), b)
+        a.free()
+
+
 @pytest.mark.parametrize("mgalx,my", [(16, 17), (64, 33), (64, 65)])
 def test_advection3d_matches_oracle(ctx, oracle, mgalx, my):
     M = (2 * (mgalx // 3)) // 2
