@@ -728,9 +728,10 @@ def uneven_rect_rate(ctx, args):
         ctx.graph_destroy(gid)
         return ms, steps
 
-    ms_full, _ = timed(False)
-    ms, steps = timed(True)
-    ctx.set_rect_fold(True)
+    ms_full, _ = timed(0)
+    ms_queue, _ = timed(2)
+    ms, steps = timed(1)
+    ctx.set_rect_fold(1)
     for x in keep:
         x.free()
     per_step = 4 * sum(nm for _, _, nm in ducts)
@@ -739,6 +740,9 @@ def uneven_rect_rate(ctx, args):
             "config": "4 rectangular ducts (65x65, 65x129, 49x145, 33x129; 32/48/64/96 modes) x (u, v, w, p)",
             "step": "CUDA-graph replay of ductgpu_solve_rect_fields_dev (16 fields): flip-symmetric half blocks, "
                     "one launch per pass and half-block size (8 GEMM-pass launches)",
+            "single_launch": {"value": per_step / (ms_queue * 1e-3), "ms_per_step": ms_queue,
+                              "step": "the same, the four passes of all 16 fields as ONE persistent launch "
+                                      "(tiles in pass order, per-plane counters between the passes)"},
             "full_operators": {"value": per_step / (ms_full * 1e-3), "ms_per_step": ms_full,
                                "step": "the same on the full operators, one launch per GEMM pass"}}
 

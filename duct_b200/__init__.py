@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libductgpu.so")
 
 OK, EARG, ESTATE, ECUDA, ESOLVER, ENONFINITE, ETIMEOUT, EALLOC = range(8)
 PREC_FP64, PREC_MIXED, PREC_INT8 = 0, 1, 2
-PASS_STAGED, PASS_REGISTER, PASS_STAGED16, PASS_PERSIST, PASS_PARITY = 0, 1, 2, 3, 4
+PASS_STAGED, PASS_REGISTER, PASS_STAGED16, PASS_PERSIST, PASS_PARITY, PASS_PARITY_QUEUE = 0, 1, 2, 3, 4, 5
 GAUGE_POINT, GAUGE_MEAN = 0, 1
 
 EXPORTS = [
@@ -313,7 +313,10 @@ class Context:
         self._check(lib().ductgpu_set_line_kernel(self.h, int(kernel)))
 
     def set_rect_fold(self, on):
-        self._check(lib().ductgpu_set_rect_fold(self.h, int(bool(on))))
+        """Rectangular solves: 1 (True) the flip-symmetric half blocks, one
+        launch per pass and half-block size; 2 the same in one persistent
+        launch per solve; 0 (False) the full operators."""
+        self._check(lib().ductgpu_set_rect_fold(self.h, int(on)))
 
     def set_refinement(self, steps):
         self._check(lib().ductgpu_set_refinement(self.h, int(steps)))

@@ -218,6 +218,7 @@ int ductgpu_destroy(ductgpu_ctx ctx)
     }
     for (int i = 0; i < ductgpu_ctx_s::kTwTables; ++i) cudaFree(ctx->tw_tab[i]);
     cudaFree(ctx->dev_err);
+    cudaFree(ctx->pq_ctr);
     free_dns_aux(ctx);
     free_dlines(ctx);
     cudaFree(ctx->lam);
@@ -406,7 +407,7 @@ int ductgpu_set_refinement(ductgpu_ctx ctx, int steps)
 int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel)
 {
     if (!ctx) return DUCTGPU_EARG;
-    if (kernel < -1 || kernel > DUCTGPU_PASS_PARITY)
+    if (kernel < -1 || kernel > DUCTGPU_PASS_PARITY_QUEUE)
         return set_error(ctx, DUCTGPU_EARG, "pass kernel %d", kernel);
     if (size_class < -1 || size_class > 2) return set_error(ctx, DUCTGPU_EARG, "size class %d", size_class);
     for (int c = 0; c < 3; ++c)
@@ -424,7 +425,8 @@ int ductgpu_set_line_kernel(ductgpu_ctx ctx, int kernel)
 int ductgpu_set_rect_fold(ductgpu_ctx ctx, int on)
 {
     if (!ctx) return DUCTGPU_EARG;
-    ctx->rect_fold = on ? 1 : 0;
+    if (on < 0 || on > 2) return set_error(ctx, DUCTGPU_EARG, "rect fold %d (0, 1, 2)", on);
+    ctx->rect_fold = on;
     return DUCTGPU_OK;
 }
 
@@ -436,8 +438,8 @@ int ductgpu_autotune(ductgpu_ctx ctx, const ductgpu_field *fields, int nfields, 
     if (reps < 1) reps = 5;
     const int cls = (ctx->my - 2 + 63) / 64 - 1;
     if (cls < 0 || cls > 2) return set_error(ctx, DUCTGPU_EARG, "grid %d", ctx->my);
-    const int variants[5] = {DUCTGPU_PASS_STAGED, DUCTGPU_PASS_STAGED16, DUCTGPU_PASS_REGISTER, DUCTGPU_PASS_PERSIST,
-                             DUCTGPU_PASS_PARITY};
+    const int variants[6] = {DUCTGPU_PASS_STAGED, DUCTGPU_PASS_STAGED16, DUCTGPU_PASS_REGISTER, DUCTGPU_PASS_PERSIST,
+                             DUCTGPU_PASS_PARITY, DUCTGPU_PASS_PARITY_QUEUE};
     const int saved = ctx->pass_variant[cls];
     const bool prof = ctx->prof_on;
     ctx->prof_on = false;

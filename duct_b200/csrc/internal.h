@@ -150,6 +150,8 @@ struct ductgpu_ctx_s {
     int tw_len[kTwTables] = {};
     void *tw_tab[kTwTables] = {};
     int *dev_err = nullptr;    // device error word (bounded waits)
+    int *pq_ctr = nullptr;     // counters of the queued flip-symmetric passes
+    size_t pq_cap = 0;
     duct::DnsAux *dns_aux = nullptr;   // buffers of the DNS operator entries (dns.cu)
     // derivative lines on the FP64 tensor cores (dlines.cu): the folded,
     // packed collocation matrices per line length
@@ -272,6 +274,8 @@ struct PassParams {
 };
 constexpr int kPassLines = 32;
 int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid);
+// the four flip-symmetric passes of a batched solve in one persistent launch
+int fp64_pass_queue(ductgpu_ctx ctx, const PassParams *pp);
 // solve_fp64ws.cu: the flip-symmetric pass as a warp-specialised persistent
 // kernel (hpad 32 or 64, every field folded, no residual epilogue)
 cudaError_t fp64_pass_ws(ductgpu_ctx ctx, const PassParams &pp, int hpad);

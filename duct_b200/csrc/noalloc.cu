@@ -126,7 +126,15 @@ extern "C" int ductgpu_solve_fields_dev_noalloc(ductgpu_ctx ctx, const ductgpu_f
     ctx->lam_cap = kLamSlots;
     ctx->work.buf = scratch + kLamSlots;                  // 32 KB in: still 256-byte aligned
     ctx->work.bytes = work_doubles * sizeof(double);
+    // the queued flip-symmetric passes keep device counters: the same
+    // passes one launch each instead
+    int variant_saved[3];
+    for (int c = 0; c < 3; ++c) {
+        variant_saved[c] = ctx->pass_variant[c];
+        if (ctx->pass_variant[c] == DUCTGPU_PASS_PARITY_QUEUE) ctx->pass_variant[c] = DUCTGPU_PASS_PARITY;
+    }
     rc = ductgpu_solve_fields_dev(ctx, fields, nfields, DUCTGPU_PREC_FP64);
+    for (int c = 0; c < 3; ++c) ctx->pass_variant[c] = variant_saved[c];
     ctx->work = work_saved;
     ctx->lam = lam_saved;
     ctx->lam_host = lam_host_saved;

@@ -213,19 +213,18 @@ __global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)
 // par 2 (P passes): the mode-ordered input is staged as the two halves; the
 //   accumulators go through shared memory, and out_o = even_o + odd_o,
 //   out_{n-1-o} = even_o - odd_o.
+// One tile (field fi, the field's tile `local` = plane * nchunks + chunk)
+// of a flip-symmetric pass, by every thread of the CTA; smem as sized by
+// pass_smem_bytes for this MTW (with the eigenvalue staging).
 template <int MTW, int LINES>
-__global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)) k_pass_fp64s(const __grid_constant__ PassParams p)
+__device__ __forceinline__ void pass_s_tile(const PassParams &p, int fi, int local, double *smem)
 {
     constexpr int NLD = 2 * LINES + 4, NTW = LINES / 8;
     constexpr int a_chunk_max = (kKC / 16) * (4 * MTW) * 256;
-    extern __shared__ __align__(16) double smem[];
     double *As = smem;
     double *Bs = smem + 2 * a_chunk_max;
 
-    int fi = 0;
-    while (fi + 1 < p.nf && (int)blockIdx.x >= p.cta_start[fi + 1]) ++fi;
     const PassField &F = p.f[fi];
-    const int local = blockIdx.x - p.cta_start[fi];
     const int plane = local / F.nchunks;
     const int chunk = local - plane * F.nchunks;
     const int l0 = chunk * LINES;
@@ -422,6 +421,111 @@ __global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)
             const int o = idx / LINES, l = idx % LINES;
             if (l < L) emit(Rs + l, Rs + H * (NLD / 2) + l, NLD / 2, o, l);
         }
+    }
+}
+
+template <int MTW, int LINES>
+__global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)) k_pass_fp64s(const __grid_constant__ PassParams p)
+{
+    extern __shared__ __align__(16) double smem[];
+    int fi = 0;
+    while (fi + 1 < p.nf && (int)blockIdx.x >= p.cta_start[fi + 1]) ++fi;
+    pass_s_tile<MTW, LINES>(p, fi, (int)blockIdx.x - p.cta_start[fi], smem);
+}
+
+// ---------------------------------------------------------------------------
+// The four flip-symmetric passes of a batched solve in ONE persistent launch.
+// CTAs take tiles from a global counter in pass order -- (pass, field,
+// plane, chunk) -- and a tile of pass k > 0 first waits until every tile of
+// the earlier passes of its plane is done (per-plane completion counters,
+// released with a fence and an atomic add), so passes of different planes
+// overlap and no launch boundary separates them.  Tiles are dequeued in
+// dependency order by CTAs that are running, so every wait ends; each is
+// still bounded: a wait that runs out raises the error word (code 1) and
+// an abort flag that ends the other CTAs' waits and their dequeue loops.
+struct PassQueue {
+    PassParams pass[4];
+    int items[5];                  // first tile of each pass; items[4]: all tiles
+    int need[4][kMaxFields];       // tiles per plane of field i in the passes before k
+    int plane_base[kMaxFields];    // field i's first per-plane counter
+};
+constexpr unsigned kQueueSpin = 1u << 22;
+
+// ctr[0]: dequeue counter, ctr[1]: abort flag, ctr[2 + plane_base[i] + plane]:
+// tiles done of that plane (all zero at launch)
+__device__ __forceinline__ void queue_release(int *cnt)
+{
+    asm volatile("red.release.gpu.global.add.s32 [%0], 1;\n" ::"l"(cnt) : "memory");
+}
+
+// Thread 0 takes the next tile while the current one runs (the atomic's
+// result is used only after it) and polls the new tile's dependency; warp 1
+// releases the finished tile's count (one release after the CTA barrier
+// that follows the tile's stores) in parallel with that poll.
+template <int MTWMAX>
+__global__ void __launch_bounds__(kThreads, MTWMAX == 3 ? 2 : 3)
+    k_pass_fp64q(const __grid_constant__ PassQueue q, int *ctr, int *err)
+{
+    extern __shared__ __align__(16) double smem[];
+    __shared__ int s_cur, s_stop;
+    volatile int *abort = ctr + 1;
+    const int tid = threadIdx.x, total = q.items[4];
+    if (tid == 0) s_cur = atomicAdd(ctr, 1);
+    __syncthreads();
+    int *pending = nullptr;     // warp 1's lane 0: the count of the tile to release
+    for (;;) {
+        const int item = s_cur;
+        if (item >= total) {
+            if (tid == 32 && pending) queue_release(pending);
+            return;
+        }
+        int k = 0;
+        while (item >= q.items[k + 1]) ++k;
+        const PassParams &p = q.pass[k];
+        const int idx = item - q.items[k];
+        int fi = 0;
+        while (fi + 1 < p.nf && idx >= p.cta_start[fi + 1]) ++fi;
+        const int local = idx - p.cta_start[fi];
+        int *cnt = ctr + 2 + q.plane_base[fi] + local / p.f[fi].nchunks;
+        int next = total;
+        if (tid == 0) {
+            next = *abort ? total : atomicAdd(ctr, 1);
+            int stop = 0;
+            if (k > 0) {
+                const int need = q.need[k][fi];
+                for (unsigned it = 0;; ++it) {
+                    int v;
+                    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(cnt) : "memory");
+                    if (v >= need) break;
+                    if ((it & 63) == 63 && *abort) {
+                        stop = 1;
+                        break;
+                    }
+                    if (it >= kQueueSpin) {
+                        stop = 1;
+                        atomicExch(err, 1);
+                        atomicExch(ctr + 1, 1);
+                        break;
+                    }
+                    __nanosleep(it < 64 ? 32 : 256);
+                }
+            }
+            s_stop = stop;
+        }
+        if (tid == 32 && pending) {
+            queue_release(pending);
+            pending = nullptr;
+        }
+        __syncthreads();    // s_stop; every thread has read s_cur
+        if (s_stop) return;
+        const int mtw = p.f[fi].kpad / 32;
+        if (mtw == 1) pass_s_tile<1, kParityLines>(p, fi, local, smem);
+        else if (mtw == 2 && MTWMAX >= 2) pass_s_tile<MTWMAX >= 2 ? 2 : 1, kParityLines>(p, fi, local, smem);
+        else if (MTWMAX >= 3) pass_s_tile<MTWMAX >= 3 ? 3 : 1, kParityLines>(p, fi, local, smem);
+        if (tid == 32) pending = cnt;
+        __syncthreads();    // the tile's stores issued, its shared memory consumed
+        if (tid == 0) s_cur = next;
+        __syncthreads();
     }
 }
 
@@ -755,6 +859,79 @@ static cudaError_t launch_pass_s(ductgpu_ctx ctx, const PassParams &pp, int hpad
     LaunchScope ls(ctx, DUCTGPU_K_PASS_FP64);
     k_pass_fp64s<MTW, LINES><<<grid, kThreads, smem, ctx->stream>>>(q);
     return cudaGetLastError();
+}
+
+template <int MTWMAX>
+static int launch_pass_q(ductgpu_ctx ctx, const PassQueue &q, int *ctr, int tiles)
+{
+    const int hmax = 32 * MTWMAX;
+    const size_t smem = pass_smem_bytes(MTWMAX, 2 * hmax, kParityLines) + (size_t)(2 * hmax + kParityLines) * sizeof(double);
+    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_pass_fp64q<MTWMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    DUCT_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pass_fp64q<MTWMAX>, kThreads, smem));
+    if (per_sm < 1) return set_error(ctx, DUCTGPU_ECUDA, "queued passes: no CTA fits an SM");
+    const int grid = tiles < per_sm * ctx->num_sms ? tiles : per_sm * ctx->num_sms;
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_PASS_FP64);
+        k_pass_fp64q<MTWMAX><<<grid, kThreads, smem, ctx->stream>>>(q, ctr, ctx->dev_err);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "k_pass_fp64q");
+}
+
+// The four flip-symmetric passes pp[0..3] of a batched solve (every field
+// folded, the same fields in each pass) as one persistent launch.
+int fp64_pass_queue(ductgpu_ctx ctx, const PassParams *pp)
+{
+    PassQueue q{};
+    const int nf = pp[0].nf;
+    int tiles = 0, mtw = 1, planes = 0;
+    for (int k = 0; k < 4; ++k) {
+        PassParams &p = q.pass[k];
+        p = pp[k];
+        if (p.nf != nf || p.residual) return set_error(ctx, DUCTGPU_EARG, "queued passes: pass %d", k);
+        int grid = 0;
+        for (int i = 0; i < nf; ++i) {
+            PassField &f = p.f[i];
+            if (!f.par || (f.kpad != 32 && f.kpad != 64 && f.kpad != 96) || f.nmodes != pp[0].f[i].nmodes)
+                return set_error(ctx, DUCTGPU_EARG, "queued passes: pass %d field %d", k, i);
+            f.nchunks = (f.nlines + kParityLines - 1) / kParityLines;
+            p.cta_start[i] = grid;
+            grid += f.nmodes * f.nchunks;
+            mtw = f.kpad / 32 > mtw ? f.kpad / 32 : mtw;
+        }
+        p.cta_start[nf] = grid;
+        q.items[k] = tiles;
+        tiles += grid;
+    }
+    q.items[4] = tiles;
+    for (int i = 0; i < nf; ++i) {
+        q.plane_base[i] = planes;
+        planes += q.pass[0].f[i].nmodes;
+        int acc = 0;
+        for (int k = 0; k < 4; ++k) {
+            q.need[k][i] = acc;
+            acc += q.pass[k].f[i].nchunks;
+        }
+    }
+    if (tiles <= 0) return DUCTGPU_OK;
+    const size_t cbytes = (size_t)(2 + planes) * sizeof(int);
+    // sized once for 16 fields x 256 modes: a captured graph keeps the pointer
+    const size_t cap = cbytes > (2 + 16 * 256) * sizeof(int) ? cbytes : (2 + 16 * 256) * sizeof(int);
+    if (ctx->pq_cap < cbytes) {
+        if (ctx->capturing)
+            return set_error(ctx, DUCTGPU_ESTATE, "queued passes: counters first sized inside a capture");
+        cudaFree(ctx->pq_ctr);
+        ctx->pq_ctr = nullptr;
+        ctx->pq_cap = 0;
+        DUCT_CUDA(ctx, cudaMalloc(&ctx->pq_ctr, cap));
+        ctx->pq_cap = cap;
+    }
+    DUCT_CUDA(ctx, cudaMemsetAsync(ctx->pq_ctr, 0, cbytes, ctx->stream));
+    switch (mtw) {
+    case 1: return launch_pass_q<1>(ctx, q, ctx->pq_ctr, tiles);
+    case 2: return launch_pass_q<2>(ctx, q, ctx->pq_ctr, tiles);
+    default: return launch_pass_q<3>(ctx, q, ctx->pq_ctr, tiles);
+    }
 }
 
 template <int MTW, int LINES>
@@ -1140,7 +1317,8 @@ int solve_fp64(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks) { return sol
 
 bool use_fold(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks)
 {
-    if (ctx->pass_variant[(ctx->dir.mtiles / 4) - 1] != DUCTGPU_PASS_PARITY) return false;
+    const int v = ctx->pass_variant[(ctx->dir.mtiles / 4) - 1];
+    if (v != DUCTGPU_PASS_PARITY && v != DUCTGPU_PASS_PARITY_QUEUE) return false;
     for (int i = 0; i < ntasks; ++i)
         if (!((tasks[i].bound == 'n') ? ctx->neu : ctx->dir).fold_ok) return false;
     return true;
@@ -1182,6 +1360,9 @@ int solve_fp64_ex(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks, bool emul
         pp.f[i].sing_io = (tasks[i].bound == 'n') ? ctx->neu.iofzero - 1 : -1;
         pp.f[i].sing_l = pp.f[i].sing_io;
     }
+    // the four folded passes as one persistent launch
+    const bool queue = fold && ctx->pass_variant[(ctx->dir.mtiles / 4) - 1] == DUCTGPU_PASS_PARITY_QUEUE;
+    PassParams qp[4];
     // pass 1 (y, P^-1): rhs -> w1 ; pass 2 (z, P^-1, divide): w1 -> w2 ;
     // pass 3 (z, P): w2 -> w1 ; pass 4 (y, P): w1 -> sol
     for (int pass = 0; pass < 4; ++pass) {
@@ -1207,8 +1388,10 @@ int solve_fp64_ex(ductgpu_ctx ctx, const FieldTask *tasks, int ntasks, bool emul
         pp.divide = (pass == 1);
         pp.zero_im_mode0 = (pass == 3);
         pp.residual = 0;
-        if ((rc = emulate ? i8_pass(ctx, pp, cta) : fp64_pass(ctx, pp, cta))) return rc;
+        if (queue) qp[pass] = pp;
+        else if ((rc = emulate ? i8_pass(ctx, pp, cta) : fp64_pass(ctx, pp, cta))) return rc;
     }
+    if (queue && (rc = fp64_pass_queue(ctx, qp))) return rc;
     if ((rc = zero_walls(ctx, tasks, ntasks))) return rc;
     return neumann_fill(ctx, tasks, ntasks);
 }

@@ -196,7 +196,7 @@ k_pass_fp64w(const __grid_constant__ PassParams p, const __grid_constant__ WsSpl
 
     auto fail = [&]() {
         *abort = 1;
-        atomicExch(err, 2);
+        atomicExch(err, 1);     // a wait ran out (code 2 is the tcgen05 kernels' misaligned base)
     };
 
     if (warp < 4) {

@@ -255,54 +255,76 @@ int solve_rect(ductgpu_ctx ctx, const RectTask *tasks, int ntasks)
         fold = r.y.fold_ok && r.z.fold_ok;
     }
     if (fold) {
-        // a launch per half-block size of the pass direction (the folded
-        // kernels take one operator size per launch)
-        for (int pass = 0; pass < 4; ++pass) {
+        // field i of pass `pass` on the half blocks
+        auto folded_field = [&](PassField &f, int pass, int i) {
+            const RectSlot &r = ctx->rect[tasks[i].slot];
             const bool ypass = (pass == 0 || pass == 3);
-            bool done[kMaxFields] = {};
-            for (int lead = 0; lead < ntasks; ++lead) {
-                if (done[lead]) continue;
-                const int hp = ypass ? ctx->rect[tasks[lead].slot].y.hpad : ctx->rect[tasks[lead].slot].z.hpad;
-                PassParams pp{};
-                pp.lam = ctx->lam;
-                int cta = 0, nf = 0;
-                for (int i = lead; i < ntasks; ++i) {
-                    const RectSlot &r = ctx->rect[tasks[i].slot];
-                    const BoundOps &b = ypass ? r.y : r.z;
-                    if (done[i] || b.hpad != hp) continue;
-                    done[i] = true;
-                    PassField &f = pp.f[nf];
-                    const long long ps = 2LL * r.my * r.mz;
-                    pass_geometry(f, b, ypass ? r.z.E : r.y.E, ypass ? r.z.n : r.y.n, ypass ? 1 : r.my,
-                                  ypass ? r.my : 1, ps);
-                    f.nmodes = tasks[i].nmodes;
-                    f.mode0 = tasks[i].mode0;
-                    f.plane0 = tasks[i].plane0;
-                    const double *src0 = (tasks[i].bcy || tasks[i].bcz) ? w3 + offs[i] : tasks[i].rhs;
-                    switch (pass) {
-                    case 0: f.src = src0; f.dst = w1 + offs[i]; break;
-                    case 1: f.src = w1 + offs[i]; f.dst = w2 + offs[i]; break;
-                    case 2: f.src = w2 + offs[i]; f.dst = w1 + offs[i]; break;
-                    default: f.src = w1 + offs[i]; f.dst = tasks[i].sol; break;
+            const BoundOps &b = ypass ? r.y : r.z;
+            const long long ps = 2LL * r.my * r.mz;
+            pass_geometry(f, b, ypass ? r.z.E : r.y.E, ypass ? r.z.n : r.y.n, ypass ? 1 : r.my, ypass ? r.my : 1,
+                          ps);
+            f.nmodes = tasks[i].nmodes;
+            f.mode0 = tasks[i].mode0;
+            f.plane0 = tasks[i].plane0;
+            const double *src0 = (tasks[i].bcy || tasks[i].bcz) ? w3 + offs[i] : tasks[i].rhs;
+            switch (pass) {
+            case 0: f.src = src0; f.dst = w1 + offs[i]; break;
+            case 1: f.src = w1 + offs[i]; f.dst = w2 + offs[i]; break;
+            case 2: f.src = w2 + offs[i]; f.dst = w1 + offs[i]; break;
+            default: f.src = w1 + offs[i]; f.dst = tasks[i].sol; break;
+            }
+            fold_field(f, b, (pass < 2) ? 1 : 2, (pass < 2) ? b.Qfold : b.Pfold, false);
+            // eigenvalues along the pass and along the lines, both in the
+            // even-first order; the all-Neumann singular pair in it
+            f.E = b.Eperm;
+            f.El = ypass ? r.z.Eperm : r.y.Eperm;
+            const bool allneu = kp.f[i].allneu;
+            f.sing_io = allneu ? (ypass ? r.sing_yp : r.sing_zp) : -1;
+            f.sing_l = allneu ? (ypass ? r.sing_zp : r.sing_yp) : -1;
+        };
+        auto pass_flags = [](PassParams &pp, int pass) {
+            pp.divide = (pass == 1);
+            pp.zero_im_mode0 = (pass == 3);
+            pp.residual = 0;
+        };
+        if (ctx->rect_fold == 2) {
+            // one persistent launch for the four passes of every field, any
+            // mix of half-block sizes
+            PassParams pp[4] = {};
+            for (int pass = 0; pass < 4; ++pass) {
+                pp[pass].lam = ctx->lam;
+                pp[pass].nf = ntasks;
+                pass_flags(pp[pass], pass);
+                for (int i = 0; i < ntasks; ++i) folded_field(pp[pass].f[i], pass, i);
+            }
+            if ((rc = fp64_pass_queue(ctx, pp))) return rc;
+        } else {
+            // a launch per pass and half-block size of the pass direction
+            for (int pass = 0; pass < 4; ++pass) {
+                const bool ypass = (pass == 0 || pass == 3);
+                bool done[kMaxFields] = {};
+                for (int lead = 0; lead < ntasks; ++lead) {
+                    if (done[lead]) continue;
+                    const int hp = ypass ? ctx->rect[tasks[lead].slot].y.hpad : ctx->rect[tasks[lead].slot].z.hpad;
+                    PassParams pp{};
+                    pp.lam = ctx->lam;
+                    int cta = 0, nf = 0;
+                    for (int i = lead; i < ntasks; ++i) {
+                        const RectSlot &r = ctx->rect[tasks[i].slot];
+                        const BoundOps &b = ypass ? r.y : r.z;
+                        if (done[i] || b.hpad != hp) continue;
+                        done[i] = true;
+                        PassField &f = pp.f[nf];
+                        folded_field(f, pass, i);
+                        pp.cta_start[nf] = cta;
+                        cta += tasks[i].nmodes * f.nchunks;
+                        ++nf;
                     }
-                    fold_field(f, b, (pass < 2) ? 1 : 2, (pass < 2) ? b.Qfold : b.Pfold, false);
-                    // eigenvalues along the pass and along the lines, both in the
-                    // even-first order; the all-Neumann singular pair in it
-                    f.E = b.Eperm;
-                    f.El = ypass ? r.z.Eperm : r.y.Eperm;
-                    const bool allneu = kp.f[i].allneu;
-                    f.sing_io = allneu ? (ypass ? r.sing_yp : r.sing_zp) : -1;
-                    f.sing_l = allneu ? (ypass ? r.sing_zp : r.sing_yp) : -1;
                     pp.cta_start[nf] = cta;
-                    cta += tasks[i].nmodes * f.nchunks;
-                    ++nf;
+                    pp.nf = nf;
+                    pass_flags(pp, pass);
+                    if ((rc = fp64_pass(ctx, pp, cta))) return rc;
                 }
-                pp.cta_start[nf] = cta;
-                pp.nf = nf;
-                pp.divide = (pass == 1);
-                pp.zero_im_mode0 = (pass == 3);
-                pp.residual = 0;
-                if ((rc = fp64_pass(ctx, pp, cta))) return rc;
             }
         }
         {

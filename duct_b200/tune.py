@@ -4,7 +4,8 @@ and persistent forms, the flip-symmetric half-block passes) for a batch of
 fields at each grid size and writes the fastest per size to a JSON table
 keyed by (ny, nz).  `Context.apply_tuning()` reads the table back and sets
 the pass kernel of the context's size class (ductgpu_set_pass_kernel) and,
-for rectangular grids, the folded / full choice (ductgpu_set_rect_fold).
+for rectangular grids, the folded (one persistent launch, or one launch per
+pass and half-block size) / full choice (ductgpu_set_rect_fold).
 
     python -m duct_b200.tune --square 33,65,129,193 --rect 65x129,49x145,33x129 \\
         --out duct_b200/tuning.json
@@ -12,8 +13,9 @@ for rectangular grids, the folded / full choice (ductgpu_set_rect_fold).
 Square grids: a substep's u, v, w (Dirichlet, lambda = kx^2 + 2/(nu dt))
 and p (Neumann, lambda = kx^2) with `--modes` Fourier modes, every variant
 timed over CUDA-graph replays.  Rectangular grids (my x mz, aspect mz/my):
-the same four fields through ductgpu_solve_rect_fields_dev, folded against
-full operators.  Needs a GPU.
+the same four fields through ductgpu_solve_rect_fields_dev: folded, one
+launch per pass and size, folded in one launch, and full operators.
+Needs a GPU.
 """
 import argparse
 import json
@@ -24,7 +26,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuning.json")
 
-VARIANTS = {"staged-32": 0, "register": 1, "staged-16": 2, "persist": 3, "parity": 4}
+VARIANTS = {"staged-32": 0, "register": 1, "staged-16": 2, "persist": 3, "parity": 4, "parity-queue": 5}
 
 
 def _time_graph(ctx, gid, reps):
@@ -83,15 +85,16 @@ def tune_rect(ctx, my, mz, nmodes, reps=20):
         keep += [r, s]
         fields.append(dict(rhs=r, sol=s, xalp=xalp, alambda=0.0 if neu else lam, ib=0, slot=1 if neu else 0))
     ms = {}
-    for name, fold in (("full", False), ("fold", True)):
+    modes = {"full": 0, "fold": 1, "fold-one-launch": 2}
+    for name, fold in modes.items():
         ctx.set_rect_fold(fold)
         gid = ctx.graph_create(fields, rect=True)
         ms[name] = _time_graph(ctx, gid, reps)
         ctx.graph_destroy(gid)
-    ctx.set_rect_fold(True)
+    ctx.set_rect_fold(1)
     for x in keep:
         x.free()
-    return {"ny": my, "nz": mz, "nmodes": nmodes, "fields": 4, "rect_fold": ms["fold"] <= ms["full"],
+    return {"ny": my, "nz": mz, "nmodes": nmodes, "fields": 4, "rect_fold": modes[min(ms, key=ms.get)],
             "ms_per_batch": ms}
 
 

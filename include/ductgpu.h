@@ -183,12 +183,19 @@ int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields,
                                      odd eigenvectors in two blocks of half size, half the
                                      flops (n <= 191; operators without the symmetry, e.g.
                                      from ductgpu_set_operators, run STAGED)            */
+#define DUCTGPU_PASS_PARITY_QUEUE 5 /* PARITY with the four passes of a solve in ONE
+                                     persistent launch: tiles taken in pass order, a
+                                     plane's pass waiting on per-plane counters of its
+                                     earlier passes (bounded waits)                     */
 /* kernel -1 restores the library's defaults for the size class(es).      */
 int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel);
 /* Rectangular solves (ductgpu_helm3d_temp, ductgpu_solve_rect_fields_dev)
  * on the flip-symmetric half blocks wherever both walls of each direction
- * match (1, the default) or on the full operators (0).  Folded passes run
- * one launch per half-block size of the pass direction.                  */
+ * match: 1 (the default) one launch per pass and half-block size; 2 the
+ * four passes of every field as ONE persistent launch (tiles taken in pass
+ * order, a plane's pass waiting on per-plane counters of its earlier
+ * passes, any mix of half-block sizes; measured slower on the config-2
+ * batch, 0.59 against 0.46 ms); 0 the full operators.                    */
 int ductgpu_set_rect_fold(ductgpu_ctx ctx, int on);
 /* Kernel of the y / z derivative lines of the DNS operators: 1 (default)
  * the collocation matrices' flip-symmetric half blocks on the FP64 tensor
