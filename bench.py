@@ -60,7 +60,8 @@ def parse():
     ap.add_argument("--dns-only", action="store_true",
                     help="only the config-4 DNS block (one GPU; with --dns-steps for short profiling runs)")
     ap.add_argument("--dns-steps", type=int, default=None, help="timed DNS steps (default: the config's 200)")
-    ap.add_argument("--pass-kernel", default="auto", choices=["auto", "staged-32", "staged-16", "register", "persist", "parity"],
+    ap.add_argument("--pass-kernel", default="auto",
+                    choices=["auto", "staged-32", "staged-16", "register", "persist", "parity", "parity-queue"],
                     help="GEMM-pass kernel; auto runs the library's autotuner (profiling runs fix it, since "
                          "the autotuner's timing under a profiler is not the live one)")
     ap.add_argument("--transforms-only", action="store_true",
@@ -239,7 +240,7 @@ def run_ours(args, world, rank, local, pg):
 
     # the library's autotuner picks the GEMM-pass kernel for this batch
     names = {D.PASS_STAGED: "staged-32", D.PASS_STAGED16: "staged-16", D.PASS_REGISTER: "register",
-             D.PASS_PERSIST: "persist", D.PASS_PARITY: "parity"}
+             D.PASS_PERSIST: "persist", D.PASS_PARITY: "parity", D.PASS_PARITY_QUEUE: "parity-queue"}
     if args.pass_kernel == "auto":
         pass_id = ctx.autotune(sets[0], reps=5)
     else:
@@ -340,7 +341,13 @@ def run_ours(args, world, rank, local, pg):
     for name, R in res.items():
         if name == "fp64":
             kms, kn = R["prof"][D.K_PASS_FP64]
-            if pass_kernel == "parity":
+            if pass_kernel == "parity-queue":
+                # one launch runs the four flip-symmetric passes of the step
+                he, ho = (n + 1) // 2, n // 2
+                flops = 4 * 4.0 * n * (he * he + ho * ho) * per_step
+                kname = "k_pass_fp64q (the four flip-symmetric passes in one persistent launch, FP64 DMMA m16n8k16)"
+                traffic = None
+            elif pass_kernel == "parity":
                 # even and odd half blocks (ceil(n/2), floor(n/2)) on 2n real
                 # columns per plane: the flops the flip-symmetric pass executes
                 he, ho = (n + 1) // 2, n // 2
