@@ -44,7 +44,7 @@ EXPORTS = [
     "ductgpu_wallstressx_dev", "ductgpu_energy_fou_dev", "ductgpu_statistics_fou_dev",
     "ductgpu_dns_create", "ductgpu_dns_destroy", "ductgpu_dns_set_fields", "ductgpu_dns_get_fields",
     "ductgpu_dns_field", "ductgpu_dns_set_graphs", "ductgpu_dns_substep", "ductgpu_dns_steps",
-    "ductgpu_dns_statistics", "ductgpu_profile_bytes", "ductgpu_profile_flops", "ductgpu_dns_set_forcing",
+    "ductgpu_dns_statistics", "ductgpu_profile_bytes", "ductgpu_profile_flops", "ductgpu_cheb_deriv_matrix", "ductgpu_dns_set_forcing",
     "ductgpu_dns_wallstress_after", "ductgpu_dns_grad_wallstress", "ductgpu_set_rect_fold",
     "ductgpu_set_line_kernel",
 ]
@@ -158,6 +158,7 @@ def lib():
             "ductgpu_dns_statistics": [P, P, P, P, P, P, C.POINTER(I), C.POINTER(I), P],
             "ductgpu_profile_bytes": [P, I, C.POINTER(D)],
             "ductgpu_profile_flops": [P, I, C.POINTER(D)],
+            "ductgpu_cheb_deriv_matrix": [I, I, C.POINTER(D)],
             "ductgpu_dns_set_forcing": [P, P, P, P],
             "ductgpu_set_rect_fold": [P, I],
             "ductgpu_set_line_kernel": [P, I],
@@ -177,6 +178,17 @@ def lib():
         L.ductgpu_launch_count.restype = C.c_longlong
         _lib = L
     return _lib
+
+
+def cheb_deriv_matrix(n, order):
+    """The n x n real matrix of the reference's derivative chain along one
+    Chebyshev direction (transyz -1, derivyz of this order, transyz +1), as
+    the tensor-core line kernel applies it; host only (no GPU needed)."""
+    out = np.zeros((n, n), dtype=np.float64, order="F")
+    rc = lib().ductgpu_cheb_deriv_matrix(int(n), int(order), out.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc:
+        raise DuctGPUError(rc, "cheb_deriv_matrix: n=%d order=%d" % (n, order))
+    return out
 
 
 class DuctGPUError(RuntimeError):

@@ -552,3 +552,14 @@ int dlines_launch(ductgpu_ctx ctx, const LineParams &p)
 }
 
 }  // namespace duct
+
+// The derivative matrix of one Chebyshev line, for callers and tests on the
+// host: no context, no GPU.
+extern "C" int ductgpu_cheb_deriv_matrix(int n, int order, double *D)
+{
+    if (n < 3 || n > 1025 || order < 1 || order > 2 || !D) return DUCTGPU_EARG;
+    std::vector<long double> M;
+    duct::cheb_deriv_matrix(n, order, M);
+    for (size_t i = 0; i < M.size(); ++i) D[i] = (double)M[i];
+    return DUCTGPU_OK;
+}

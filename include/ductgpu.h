@@ -205,6 +205,16 @@ int ductgpu_set_rect_fold(ductgpu_ctx ctx, int on);
  * few 1e-12 of relative error at 129 and 193 points, the tensor-core form
  * a few 1e-13).                                                           */
 int ductgpu_set_line_kernel(ductgpu_ctx ctx, int kernel);
+/* The real n x n matrix (column-major, 3 <= n <= 1025 points, order 1 or
+ * 2) of the reference's derivative along one Chebyshev direction --
+ * transyz -1, derivyz, transyz +1 (src/tchebw.f:62-192,
+ * src/chebyshev.f90:1-295) -- computed in long double and rounded to FP64;
+ * the operators the tensor-core line kernel applies (as flip-symmetric half
+ * blocks).  For order 1 it is -cheb_colloc_deriv1 of
+ * src/cheb_collocation.F (the chain differentiates along the ascending
+ * coordinate), for order 2 the square of that.  Host only: no context, no
+ * GPU; O(n^3) work.                                                      */
+int ductgpu_cheb_deriv_matrix(int n, int order, double *D);
 /* Autotuner: times the FP64 batched solve of these device fields with each
  * pass kernel (reps runs each, after one warm-up; the fields' sol arrays
  * are overwritten and Dirichlet rhs walls zeroed, as by the solve itself)
