@@ -81,6 +81,7 @@ __device__ __forceinline__ double2 dl_xcoef(const LineOut &o, int t, double kx)
 
 // One output element: out[gi] = sigma (beta out + fac y + x-terms + m0).
 // Returns |out| for the interior max (0 where it does not count).
+template <int NXM>
 __device__ __forceinline__ double dl_store(const LineOut &o, long long gi, double2 y, bool deriv, double kx,
                                            double m0, bool real0, bool interior)
 {
@@ -91,7 +92,7 @@ __device__ __forceinline__ double dl_store(const LineOut &o, long long gi, doubl
         if (!real0) v.y += o.fac * y.y;
     }
 #pragma unroll
-    for (int t = 0; t < kLineXTerms; ++t)
+    for (int t = 0; t < NXM; ++t)
         if (o.xs[t]) {
             const double2 c = dl_xcoef(o, t, kx);
             const double2 s = reinterpret_cast<const double2 *>(o.xs[t])[gi];
@@ -112,7 +113,9 @@ __device__ __forceinline__ double dl_store(const LineOut &o, long long gi, doubl
 // Registers for about WARPS resident warps per SM, two CTAs at least (a
 // latency-bound kernel: the staging, the L2 operator loads and the
 // epilogue's loads are hidden by other warps rather than by prefetching).
-template <int MT, int NT, int WARPS>
+// NXM: the x-terms an output of the launch may have (1, or all
+// kLineXTerms): fewer registers where the launch's outputs have at most one
+template <int MT, int NT, int WARPS, int NXM>
 __global__ void __launch_bounds__(32 * MT, WARPS / MT > 2 ? WARPS / MT : 2)
     k_dlines(const __grid_constant__ DLineParams q)
 {
@@ -190,7 +193,7 @@ __global__ void __launch_bounds__(32 * MT, WARPS / MT > 2 ? WARPS / MT : 2)
                     v[e] = make_double2(m0 * o.m0, 0.0);
                 }
 #pragma unroll
-                for (int tt = 0; tt < kLineXTerms; ++tt)
+                for (int tt = 0; tt < NXM; ++tt)
                     if (o.xs[tt]) {
                         const double2 c = dl_xcoef(o, tt, kx);
 #pragma unroll
@@ -316,7 +319,7 @@ __global__ void __launch_bounds__(32 * MT, WARPS / MT > 2 ? WARPS / MT : 2)
                 return (nt * 4 + t) * lsi + (m ? nn - 1 - r : r) * esi;
             };
 #pragma unroll
-            for (int tt = 0; tt < kLineXTerms; ++tt)
+            for (int tt = 0; tt < NXM; ++tt)
                 if (o.xs[tt]) {
                     const double2 c = dl_xcoef(o, tt, kx);
                     const double2 *src = reinterpret_cast<const double2 *>(o.xs[tt]) + base;
@@ -370,7 +373,7 @@ __global__ void __launch_bounds__(32 * MT, WARPS / MT > 2 ? WARPS / MT : 2)
             const int l = lane >> 1;
             if (!(lane & 1) && l < L) {
                 const bool chk = o.maxabs && q0 + l > 0 && q0 + l < lpm - 1;
-                vmax = fmax(vmax, dl_store(o, base + (long long)l * ls + (long long)ho * es, make_double2(y, yi), true,
+                vmax = fmax(vmax, dl_store<NXM>(o, base + (long long)l * ls + (long long)ho * es, make_double2(y, yi), true,
                                            kx, m0 * o.m0, real0, chk));
             }
         }
@@ -485,11 +488,11 @@ static int dlines_ops(ductgpu_ctx ctx, int nn, const double **ops, int *hr)
     return DUCTGPU_OK;
 }
 
-template <int MT, int NT, int WARPS>
+template <int MT, int NT, int WARPS, int NXM>
 static int launch_dlines(ductgpu_ctx ctx, DLineParams &q)
 {
     const size_t smem = ((size_t)q.nn * DlShape<NT>::nld + 2 * (size_t)MT * 32) * sizeof(double);
-    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_dlines<MT, NT, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_dlines<MT, NT, WARPS, NXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long long grid = (long long)q.ctas_per_job * q.lp.njobs;
     if (grid > 0x7fffffffLL) return set_error(ctx, DUCTGPU_EARG, "derivative lines: grid too large");
     if (ctx->prof_on && !ctx->capturing) {
@@ -515,7 +518,7 @@ static int launch_dlines(ductgpu_ctx ctx, DLineParams &q)
     }
     {
         LaunchScope ls(ctx, DUCTGPU_K_LINES);
-        k_dlines<MT, NT, WARPS><<<(unsigned)grid, 32 * MT, smem, ctx->stream>>>(q);
+        k_dlines<MT, NT, WARPS, NXM><<<(unsigned)grid, 32 * MT, smem, ctx->stream>>>(q);
     }
     return check_cuda(ctx, cudaGetLastError(), "k_dlines");
 }
@@ -540,10 +543,17 @@ int dlines_launch(ductgpu_ctx ctx, const LineParams &p)
     // 16 lines per CTA with 16 warps; 4 lines per CTA: 10.1 ms); 2: 16
     // lines per CTA, 16 warps (each operator fragment feeds twice the MMAs)
     const bool wide = ctx->dlines == 2;
+    // at most one x-term per output (xterm() fills the slots in order)
+    bool one_x = true;
+    for (int i = 0; i < p.njobs; ++i)
+        for (int k = 0; k < p.job[i].nout; ++k)
+            for (int t = 1; t < kLineXTerms; ++t) one_x = one_x && !p.job[i].o[k].xs[t];
     const int lines = wide ? DlShape<4>::lines : DlShape<2>::lines;
     q.ctas_per_job = p.nmodes * ((lpm + lines - 1) / lines);
 #define DL_CASE(mt) \
-    case mt: return wide ? launch_dlines<mt, 4, 16>(ctx, q) : launch_dlines<mt, 2, 32>(ctx, q);
+    case mt:                                                                                      \
+        return wide ? (one_x ? launch_dlines<mt, 4, 16, 1>(ctx, q) : launch_dlines<mt, 4, 16, kLineXTerms>(ctx, q)) \
+                    : (one_x ? launch_dlines<mt, 2, 32, 1>(ctx, q) : launch_dlines<mt, 2, 32, kLineXTerms>(ctx, q));
     switch (HR / 16) {
         DL_CASE(1) DL_CASE(2) DL_CASE(3) DL_CASE(4) DL_CASE(5) DL_CASE(6) DL_CASE(7) DL_CASE(8)
     default: return set_error(ctx, DUCTGPU_EARG, "derivative lines: line length %d", nn);
