@@ -713,8 +713,9 @@ def uneven_rect_rate(ctx, args):
     lambda = kx^2 + 2/(nu dt), nu = 1/4400, dt = 5e-4, and the Neumann
     pressure with lambda = kx^2, kx = k): 16 fields in one batched call,
     replayed from a CUDA graph; FP64 passes on the flip-symmetric half blocks
-    (every duct has matching walls per direction), and on the full operators
-    for comparison.  Inputs (180 MB) exceed L2."""
+    (every duct has matching walls per direction; the fields' groups of
+    equal half-block sizes on concurrent streams), as one persistent launch,
+    and on the full operators for comparison.  Inputs (180 MB) exceed L2."""
     import duct_b200 as D
     from duct_b200 import synth
     ducts = (((65, 65), 1.0, 32), ((65, 129), 2.0, 48), ((49, 145), 3.0, 64), ((33, 129), 4.0, 96))
@@ -759,7 +760,8 @@ def uneven_rect_rate(ctx, args):
             "fields": len(fields), "steps": steps,
             "config": "4 rectangular ducts (65x65, 65x129, 49x145, 33x129; 32/48/64/96 modes) x (u, v, w, p)",
             "step": "CUDA-graph replay of ductgpu_solve_rect_fields_dev (16 fields): flip-symmetric half blocks, "
-                    "one launch per pass and half-block size (8 GEMM-pass launches)",
+                    "fields grouped by half-block sizes (3 groups), each group's four passes on a stream of "
+                    "its own (12 GEMM-pass launches, parallel graph branches)",
             "single_launch": {"value": per_step / (ms_queue * 1e-3), "ms_per_step": ms_queue,
                               "step": "the same, the four passes of all 16 fields as ONE persistent launch "
                                       "(tiles in pass order, per-plane counters between the passes)"},

@@ -325,9 +325,10 @@ class Context:
         self._check(lib().ductgpu_set_line_kernel(self.h, int(kernel)))
 
     def set_rect_fold(self, on):
-        """Rectangular solves: 1 (True) the flip-symmetric half blocks, one
-        launch per pass and half-block size; 2 the same in one persistent
-        launch per solve; 0 (False) the full operators."""
+        """Rectangular solves: 1 (True) the flip-symmetric half blocks, the
+        fields' groups of equal half-block sizes on concurrent streams; 2 the
+        same in one persistent launch per solve; 0 (False) the full
+        operators."""
         self._check(lib().ductgpu_set_rect_fold(self.h, int(on)))
 
     def set_refinement(self, steps):

@@ -219,6 +219,14 @@ int ductgpu_destroy(ductgpu_ctx ctx)
     for (int i = 0; i < ductgpu_ctx_s::kTwTables; ++i) cudaFree(ctx->tw_tab[i]);
     cudaFree(ctx->dev_err);
     cudaFree(ctx->pq_ctr);
+    for (int i = 0; i < ductgpu_ctx_s::kSideStreams; ++i) {
+        if (ctx->side[i]) {
+            cudaStreamSynchronize(ctx->side[i]);
+            cudaStreamDestroy(ctx->side[i]);
+        }
+        if (ctx->side_join[i]) cudaEventDestroy(ctx->side_join[i]);
+    }
+    if (ctx->side_fork) cudaEventDestroy(ctx->side_fork);
     free_dns_aux(ctx);
     free_dlines(ctx);
     cudaFree(ctx->lam);

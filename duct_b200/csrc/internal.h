@@ -152,6 +152,10 @@ struct ductgpu_ctx_s {
     int *dev_err = nullptr;    // device error word (bounded waits)
     int *pq_ctr = nullptr;     // counters of the queued flip-symmetric passes
     size_t pq_cap = 0;
+    // side streams of a rectangular batch's independent field groups
+    static constexpr int kSideStreams = 4;
+    cudaStream_t side[kSideStreams] = {};
+    cudaEvent_t side_fork = nullptr, side_join[kSideStreams] = {};
     duct::DnsAux *dns_aux = nullptr;   // buffers of the DNS operator entries (dns.cu)
     // derivative lines on the FP64 tensor cores (dlines.cu): the folded,
     // packed collocation matrices per line length

@@ -287,7 +287,69 @@ int solve_rect(ductgpu_ctx ctx, const RectTask *tasks, int ntasks)
             pp.zero_im_mode0 = (pass == 3);
             pp.residual = 0;
         };
-        if (ctx->rect_fold == 2) {
+        // fields grouped by the half-block sizes of their two directions:
+        // groups are independent, so with several of them each group's four
+        // passes run on a stream of its own (forked from and joined to the
+        // context's stream; a captured graph gets parallel branches), and
+        // the small launches of one group fill the tails of the others'
+        int grp[kMaxFields], ng = 0, gy[kMaxFields], gz[kMaxFields];
+        for (int i = 0; i < ntasks; ++i) {
+            const RectSlot &r = ctx->rect[tasks[i].slot];
+            int g = 0;
+            while (g < ng && !(gy[g] == r.y.hpad && gz[g] == r.z.hpad)) ++g;
+            if (g == ng) {
+                gy[ng] = r.y.hpad;
+                gz[ng] = r.z.hpad;
+                ++ng;
+            }
+            grp[i] = g;
+        }
+        bool streams = ctx->rect_fold == 1 && ng > 1 && ng <= 1 + ductgpu_ctx_s::kSideStreams;
+        if (streams && !ctx->side[ng - 2]) {
+            if (ctx->capturing) {
+                streams = false;        // created outside a capture only: one stream then
+            } else {
+                if (!ctx->side_fork) DUCT_CUDA(ctx, cudaEventCreateWithFlags(&ctx->side_fork, cudaEventDisableTiming));
+                for (int k = 0; k < ng - 1; ++k)
+                    if (!ctx->side[k]) {
+                        DUCT_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking));
+                        DUCT_CUDA(ctx, cudaEventCreateWithFlags(&ctx->side_join[k], cudaEventDisableTiming));
+                    }
+            }
+        }
+        if (streams) {
+            cudaStream_t main = ctx->stream;
+            DUCT_CUDA(ctx, cudaEventRecord(ctx->side_fork, main));
+            int rcg = DUCTGPU_OK;
+            for (int g = 0; g < ng; ++g) {
+                cudaStream_t st = g ? ctx->side[g - 1] : main;
+                if (g) DUCT_CUDA(ctx, cudaStreamWaitEvent(st, ctx->side_fork, 0));
+                ctx->stream = st;
+                for (int pass = 0; pass < 4 && !rcg; ++pass) {
+                    PassParams pp{};
+                    pp.lam = ctx->lam;
+                    int cta = 0, nf = 0;
+                    for (int i = 0; i < ntasks; ++i) {
+                        if (grp[i] != g) continue;
+                        folded_field(pp.f[nf], pass, i);
+                        pp.cta_start[nf] = cta;
+                        cta += tasks[i].nmodes * pp.f[nf].nchunks;
+                        ++nf;
+                    }
+                    pp.cta_start[nf] = cta;
+                    pp.nf = nf;
+                    pass_flags(pp, pass);
+                    rcg = fp64_pass(ctx, pp, cta);
+                }
+                ctx->stream = main;
+                if (g) {
+                    // joined even after an error, so that a capture stays whole
+                    cudaEventRecord(ctx->side_join[g - 1], st);
+                    cudaStreamWaitEvent(main, ctx->side_join[g - 1], 0);
+                }
+            }
+            if (rcg) return rcg;
+        } else if (ctx->rect_fold == 2) {
             // one persistent launch for the four passes of every field, any
             // mix of half-block sizes
             PassParams pp[4] = {};

@@ -191,11 +191,13 @@ int ductgpu_solve_fields_dev(ductgpu_ctx ctx, const ductgpu_field *fields,
 int ductgpu_set_pass_kernel(ductgpu_ctx ctx, int size_class, int kernel);
 /* Rectangular solves (ductgpu_helm3d_temp, ductgpu_solve_rect_fields_dev)
  * on the flip-symmetric half blocks wherever both walls of each direction
- * match: 1 (the default) one launch per pass and half-block size; 2 the
+ * match: 1 (the default) the fields grouped by their half-block sizes, each
+ * group's four passes on a stream of its own (forked from and joined to
+ * the context's stream; parallel branches in a captured graph); 2 the
  * four passes of every field as ONE persistent launch (tiles taken in pass
  * order, a plane's pass waiting on per-plane counters of its earlier
  * passes, any mix of half-block sizes; measured slower on the config-2
- * batch, 0.59 against 0.46 ms); 0 the full operators.                    */
+ * batch, 0.59 against 0.42 ms); 0 the full operators.                    */
 int ductgpu_set_rect_fold(ductgpu_ctx ctx, int on);
 /* Kernel of the y / z derivative lines of the DNS operators: 1 (default)
  * the collocation matrices' flip-symmetric half blocks on the FP64 tensor
