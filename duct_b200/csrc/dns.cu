@@ -995,6 +995,39 @@ static int dns_solve(ductgpu_dns d, FieldTask *t, int n, const double *lam, std:
 
 // One substep krk (1..3); stats: gather the statistics of the step (the
 // reference does so at krk = 1).
+// Work issued between side_fork and side_join runs on the context's first
+// side stream, after everything issued before on its stream and concurrent
+// with what is issued on it meanwhile.  Without the side stream (first needed
+// inside a capture), and while launches are profiled one by one (whose
+// event times would overlap), everything stays on one stream.
+static bool side_fork(ductgpu_ctx ctx, cudaStream_t *main)
+{
+    *main = ctx->stream;
+    if (ctx->prof_on) return false;
+    if (!ctx->side[0]) {
+        if (ctx->capturing) return false;
+        if (!ctx->side_fork && cudaEventCreateWithFlags(&ctx->side_fork, cudaEventDisableTiming) != cudaSuccess)
+            return false;
+        if (cudaStreamCreateWithFlags(&ctx->side[0], cudaStreamNonBlocking) != cudaSuccess) return false;
+        if (cudaEventCreateWithFlags(&ctx->side_join[0], cudaEventDisableTiming) != cudaSuccess) {
+            cudaStreamDestroy(ctx->side[0]);
+            ctx->side[0] = nullptr;
+            return false;
+        }
+    }
+    if (cudaEventRecord(ctx->side_fork, *main) != cudaSuccess ||
+        cudaStreamWaitEvent(ctx->side[0], ctx->side_fork, 0) != cudaSuccess)
+        return false;
+    return true;
+}
+
+static int side_join(ductgpu_ctx ctx, cudaStream_t main)
+{
+    int rc = check_cuda(ctx, cudaEventRecord(ctx->side_join[0], ctx->side[0]), "side stream join");
+    int rc2 = check_cuda(ctx, cudaStreamWaitEvent(main, ctx->side_join[0], 0), "side stream join");
+    return rc ? rc : rc2;
+}
+
 static int dns_issue(ductgpu_dns d, int krk, bool stats)
 {
     ductgpu_ctx ctx = d->ctx;
@@ -1005,25 +1038,35 @@ static int dns_issue(ductgpu_dns d, int krk, bool stats)
     double *u = d->vel[0], *v = d->vel[1], *w = d->vel[2], *p = d->p;
     const double *xd = d->xalp;
     int rc;
-    // (ii) adv(u^{k-1}); statistics_fou2 of the products with the statistics
-    if ((rc = advection_issue(ctx, u, v, w, an[0], an[1], an[2], d->prod, my, my, M, d->mgalx, xd, asp,
-                              stats ? d->st_prod : nullptr, 1)))
-        return rc;
+    // (ii) adv(u^{k-1}); statistics_fou2 of the products with the statistics.
+    // The statistics kernels only read u, v, w, p: on the side stream,
+    // concurrent with the advection
+    cudaStream_t mainst = ctx->stream;
+    const bool fork_stats = stats && side_fork(ctx, &mainst);
     if (stats) {
+        if (fork_stats) ctx->stream = ctx->side[0];
         // wallstressx, energy_fou (u, v, w), statistics_fou (u, v, w, p)
         const double *f[4] = {u, v, w, p};
-        if ((rc = stats_issue(ctx, f, 3, d->wcc, d->wst, d->st_mean, d->st_ppb, d->partial, d->hist, d->hist_n,
-                              d->hist_cap, d->P, M, asp)))
-            return rc;
-        {
+        rc = stats_issue(ctx, f, 3, d->wcc, d->wst, d->st_mean, d->st_ppb, d->partial, d->hist, d->hist_n,
+                         d->hist_cap, d->P, M, asp);
+        if (!rc) {
             LaunchScope ls(ctx, DUCTGPU_K_STATS);
             k_spectra<<<(4 * 7 * M + 127) / 128, 128, 0, ctx->stream>>>(
                 reinterpret_cast<const double2 *>(u), reinterpret_cast<const double2 *>(v),
                 reinterpret_cast<const double2 *>(w), reinterpret_cast<const double2 *>(p), d->P, M, my, my,
                 d->st_spec);
         }
-        DUCT_CUDA(ctx, cudaGetLastError());
+        if (!rc) rc = check_cuda(ctx, cudaGetLastError(), "k_spectra");
+        ctx->stream = mainst;
     }
+    if (!rc)
+        rc = advection_issue(ctx, u, v, w, an[0], an[1], an[2], d->prod, my, my, M, d->mgalx, xd, asp,
+                             stats ? d->st_prod : nullptr, 1);
+    if (fork_stats) {
+        const int rj = side_join(ctx, mainst);
+        if (!rc) rc = rj;
+    }
+    if (rc) return rc;
     // (i), (iii)-(v), the x-part of (vi), (vi-b): along y,
     //   h = -rho adv_old - gamma adv + u/dt + a nu lap_x,y(u) [- (a+b) (i kx p + dpdx)]
     {
@@ -1042,14 +1085,25 @@ static int dns_issue(ductgpu_dns d, int krk, bool stats)
         }
         if ((rc = lines_launch(ctx, py))) return rc;
     }
-    // (vi) y and z parts of -(a+b) grad p
+    // (vi) y and z parts of -(a+b) grad p: different outputs, the z part on
+    // the side stream concurrent with the y part
     {
         LineParams py = line_params('y', my, my, M, xd, 1);
         add_job(py, p, {line_out(d->h[1], 1, -(a + b), 1.0)});
-        if ((rc = lines_launch(ctx, py))) return rc;
         LineParams pz = line_params('z', my, my, M, xd, 1);
         add_job(pz, p, {line_out(d->h[2], 1, -(a + b) / asp, 1.0)});
-        if ((rc = lines_launch(ctx, pz))) return rc;
+        const bool fork = side_fork(ctx, &mainst);
+        rc = lines_launch(ctx, py);
+        if (!rc) {
+            if (fork) ctx->stream = ctx->side[0];
+            rc = lines_launch(ctx, pz);
+            ctx->stream = mainst;
+        }
+        if (fork) {
+            const int rj = side_join(ctx, mainst);
+            if (!rc) rc = rj;
+        }
+        if (rc) return rc;
     }
     // (iv) z part of the laplacian, then (vii) h *= -1/(nu beta)
     {
