@@ -80,14 +80,16 @@ __device__ __forceinline__ void fft_step1(double2 (&v)[R], double2 *wk, const do
     for (int k1 = 0; k1 < R; ++k1) wk[(k1 * R + c) * TQ + g] = (k1 == 0) ? v[0] : cmul(v[k1], tw[c * k1]);
 }
 
-template <int R, int TQ, int MINB = 1>
+template <int R, int TQ, int MINB = 1, bool ALIAS = false>
 __global__ void __launch_bounds__(R * TQ, MINB) k_advx(const __grid_constant__ AdvParams p, const double2 *__restrict__ twg)
 {
     constexpr int N = R * R, NT = R * TQ;
     extern __shared__ __align__(16) double2 sm[];
     double2 *tw = sm;                // W_N^t
     double2 *wk = tw + N;            // [R][R][TQ] step buffer
-    double2 *xs = wk + N * TQ;       // [N][TQ] spectrum of a product pair
+    // [N][TQ] spectrum of a product pair; ALIAS: in the step buffer, once
+    // every thread has read its step-2 column out of it
+    double2 *xs = ALIAS ? wk : wk + N * TQ;
     const int c = threadIdx.x / TQ, g = threadIdx.x - c * TQ;
     const long long q0 = (long long)blockIdx.x * TQ;
     const long long q = q0 + g;
@@ -160,6 +162,7 @@ __global__ void __launch_bounds__(R * TQ, MINB) k_advx(const __grid_constant__ A
         fft_step1<R, TQ>(a, wk, tw, c, g);
         __syncthreads();
         fft_step2<R, TQ>(wk, a, tw, c, g);
+        if (ALIAS) __syncthreads();
 #pragma unroll
         for (int k2 = 0; k2 < R; ++k2) xs[(c + R * k2) * TQ + g] = a[k2];
         __syncthreads();
@@ -197,20 +200,20 @@ __global__ void __launch_bounds__(R * TQ, MINB) k_advx(const __grid_constant__ A
     }
 }
 
-template <int R, int TQ, int MINB = 1>
+template <int R, int TQ, int MINB = 1, bool ALIAS = false>
 static int launch_advx(ductgpu_ctx ctx, const AdvParams &p)
 {
     constexpr int N = R * R, NT = R * TQ;
     const double2 *tw = twiddle_table(ctx, N);
     if (!tw) return set_error(ctx, DUCTGPU_ESTATE, "advection3d: twiddle table for mgalx=%d unavailable", N);
-    const size_t smem = ((size_t)N + 2 * (size_t)N * TQ) * sizeof(double2);
-    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_advx<R, TQ, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t smem = ((size_t)N + (ALIAS ? 1 : 2) * (size_t)N * TQ) * sizeof(double2);
+    DUCT_CUDA(ctx, cudaFuncSetAttribute(k_advx<R, TQ, MINB, ALIAS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long long grid = (p.P + TQ - 1) / TQ;
     // algorithmic bytes: u, v, w read, eight product fields written
     if (ctx->prof_on && !ctx->capturing) ctx->prof_bytes[DUCTGPU_K_ADVECTION] += 11.0 * 16.0 * p.P * p.M;
     {
         LaunchScope ls(ctx, DUCTGPU_K_ADVECTION);
-        k_advx<R, TQ, MINB><<<(unsigned)grid, NT, smem, ctx->stream>>>(p, tw);
+        k_advx<R, TQ, MINB, ALIAS><<<(unsigned)grid, NT, smem, ctx->stream>>>(p, tw);
     }
     return check_cuda(ctx, cudaGetLastError(), "k_advx");
 }
@@ -223,10 +226,13 @@ static int advx_launch(ductgpu_ctx ctx, const AdvParams &p, int mgalx)
     case 16: return launch_advx<4, 32>(ctx, p);
     case 64: return launch_advx<8, 16>(ctx, p);
     case 144: return launch_advx<12, 8>(ctx, p);
-    // mgalx = 256: registers for three CTAs per SM (168; some spilling), 1.13
-    // against 1.21 ms a config-4 step with the compiler's 255 at two CTAs;
-    // 64-thread CTAs (4 points) at 4 or 6 per SM measured 1.27 / 1.19 ms
-    case 256: return launch_advx<16, 8, 3>(ctx, p);
+    // mgalx = 256: the pair spectrum aliased onto the step buffer (36 KB of
+    // shared memory a CTA) and registers for four CTAs per SM (128, spilling):
+    // 1.075 ms a config-4 step, against 1.096 for three CTAs aliased, 1.126
+    // for three with separate buffers (168 registers), 1.21 for two (255)
+    // and 1.21 for five (96); 64-thread CTAs (4 points) at 4 or 6 per SM
+    // measured 1.27 / 1.19 ms
+    case 256: return launch_advx<16, 8, 4, true>(ctx, p);
     default: return set_error(ctx, DUCTGPU_EARG, "advection3d: mgalx=%d (16, 64, 144 or 256)", mgalx);
     }
 }
