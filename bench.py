@@ -674,6 +674,7 @@ def dns_cfg4(args, local, with_cpu):
                 "x_fft_products": {"bound": "hbm", "achieved": abytes / (ams * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                                    "frac": abytes / (ams * 1e-3) / 1e9 / peak},
                 "peak_source": peak_src}
+            out["checkpoint"] = dns_checkpoint(ctx, d)
     if with_cpu:
         from oracle import oracle as O
         threads = os.cpu_count() or 1
@@ -705,6 +706,39 @@ def dns_cfg4(args, local, with_cpu):
             "statistics": {k: _errs(st[k], ref[k]) for k in ("mean", "prod", "ppb", "spec")},
             "stress_energy_history": _errs(st["hist"], hist)}
     return out
+
+
+def dns_checkpoint(ctx, d):
+    """The stepper's state written as the reference's uvwp_NNNN.h5
+    (save_4fields_fou_hdf5 + writeheader_hdf5) to a temporary directory and
+    read back as a restart (read_4fields_fou_hdf5): wall-clock times of the
+    calls (to the page cache, no fsync), the swap kernels' event time, and
+    whether the restart restored the fields bit for bit."""
+    import tempfile
+    import duct_b200 as D
+    before = d.fields()
+    with tempfile.TemporaryDirectory() as tdir:
+        path = D.uvwp_filename(tdir + "/", 1)
+        ctx.profile(True)
+        ctx.profile_reset()
+        t0 = time.perf_counter()
+        d.save_hdf5(path, time=0.0)
+        t_save = time.perf_counter() - t0
+        kms, kn = ctx.profile_read(D.K_OTHER)
+        ctx.profile(False)
+        nbytes = os.path.getsize(path)
+        t0 = time.perf_counter()
+        d.load_hdf5(path)
+        t_load = time.perf_counter() - t0
+    after = d.fields()
+    field_bytes = 4 * before[0].nbytes
+    return {"file_bytes": nbytes, "field_bytes": field_bytes,
+            "save_ms": 1e3 * t_save, "save_GBps": field_bytes / t_save / 1e9,
+            "load_ms": 1e3 * t_load, "load_GBps": field_bytes / t_load / 1e9,
+            "swap_kernels": {"launches": kn, "ms": kms, "GBps": field_bytes / (kms * 1e-3) / 1e9 if kms else None,
+                             "note": "HBM -> big-endian -> mapped pinned host chunks (the host link bounds it)"},
+            "restart_bit_exact": all(np.array_equal(a, b) for a, b in zip(before, after)),
+            "note": "wall clock of ductgpu_dns_save_hdf5 / _load_hdf5 (file in the page cache, no fsync)"}
 
 
 def uneven_rect_rate(ctx, args):

@@ -46,7 +46,9 @@ EXPORTS = [
     "ductgpu_dns_field", "ductgpu_dns_set_graphs", "ductgpu_dns_substep", "ductgpu_dns_steps",
     "ductgpu_dns_statistics", "ductgpu_profile_bytes", "ductgpu_profile_flops", "ductgpu_cheb_deriv_matrix", "ductgpu_dns_set_forcing",
     "ductgpu_dns_wallstress_after", "ductgpu_dns_grad_wallstress", "ductgpu_set_rect_fold",
-    "ductgpu_set_line_kernel",
+    "ductgpu_set_line_kernel", "ductgpu_uvwp_filename", "ductgpu_save_4fields_fou_hdf5_dev",
+    "ductgpu_read_hdf5_header", "ductgpu_read_4fields_fou_hdf5_dev", "ductgpu_dns_save_hdf5",
+    "ductgpu_dns_load_hdf5",
 ]
 SETUP_NO_EIGEN = 1
 (K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER, K_LINES,
@@ -66,6 +68,25 @@ class Field(C.Structure):
     _fields_ = [("rhs", C.c_void_p), ("sol", C.c_void_p), ("xalp", C.c_void_p),
                 ("alambda", C.c_double), ("ib", C.c_int), ("nmodes", C.c_int),
                 ("bound", C.c_char)]
+
+
+class H5Header(C.Structure):
+    """ductgpu_h5_header of include/ductgpu.h (writeheader_hdf5's scalars)."""
+    _fields_ = [("nparams", C.c_int), ("numerop", C.c_int), ("mgalx", C.c_int), ("my", C.c_int),
+                ("mz", C.c_int), ("mx1", C.c_int), ("alp", C.c_double), ("aspect", C.c_double),
+                ("time", C.c_double), ("fnu", C.c_double), ("cfl", C.c_double), ("dtfixed", C.c_double),
+                ("cmassflow", C.c_double), ("slip", C.c_double), ("divergence", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+    @classmethod
+    def from_dict(cls, d):
+        h = cls()
+        for k, _ in cls._fields_:
+            if k in d:
+                setattr(h, k, d[k])
+        return h
 
 
 _lib = None
@@ -165,6 +186,12 @@ def lib():
             "ductgpu_dns_wallstress_after": [P, I, C.POINTER(D)],
             "ductgpu_dns_grad_wallstress": [P, C.POINTER(D), P],
             "ductgpu_graph_destroy": [P, I],
+            "ductgpu_uvwp_filename": [C.c_char_p, I, C.c_char_p, I],
+            "ductgpu_save_4fields_fou_hdf5_dev": [P, C.c_char_p, P, P, P, P, C.POINTER(H5Header)],
+            "ductgpu_read_hdf5_header": [P, C.c_char_p, C.POINTER(H5Header)],
+            "ductgpu_read_4fields_fou_hdf5_dev": [P, C.c_char_p, P, P, P, P, I, I, I, C.POINTER(H5Header)],
+            "ductgpu_dns_save_hdf5": [P, C.c_char_p, D, D, D],
+            "ductgpu_dns_load_hdf5": [P, C.c_char_p, C.POINTER(D)],
             "transpose_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
                                C.POINTER(C.c_size_t)],
             "mat_invdiag_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
@@ -189,6 +216,25 @@ def cheb_deriv_matrix(n, order):
     if rc:
         raise DuctGPUError(rc, "cheb_deriv_matrix: n=%d order=%d" % (n, order))
     return out
+
+
+def uvwp_filename(fuvwpout, iimag):
+    """The reference's field file name: prefix (up to its first blank) +
+    'uvwp_' + iimag as i4.4 + '.h5' (ductgpu_uvwp_filename)."""
+    buf = C.create_string_buffer(4096)
+    rc = lib().ductgpu_uvwp_filename(os.fsencode(fuvwpout), int(iimag), buf, 4096)
+    if rc:
+        raise DuctGPUError(rc, "uvwp_filename")
+    return buf.value.decode()
+
+
+def read_hdf5_header(filename):
+    """readheader_hdf5 of a uvwp_NNNN.h5 file, as a dict (no GPU needed)."""
+    h = H5Header()
+    rc = lib().ductgpu_read_hdf5_header(None, os.fsencode(filename), C.byref(h))
+    if rc:
+        raise DuctGPUError(rc, "read_hdf5_header(%s) failed" % filename)
+    return h.as_dict()
 
 
 class DuctGPUError(RuntimeError):
@@ -629,6 +675,27 @@ class Context:
         self._check(lib().ductgpu_statistics_fou_dev(self.h, _dp(u), _dp(v), _dp(w), _dp(p), my, mz, nm,
                                                      _dp(mean), _dp(ppb), _dp(spec)))
 
+    def save_4fields_fou_hdf5_dev(self, filename, u, v, w, p, header):
+        """save_4fields_fou_hdf5 of device complex (my, mz, mx1+1) fields;
+        header: a dict of ductgpu_h5_header fields (sizes and scalars)."""
+        h = H5Header.from_dict(header)
+        self._check(lib().ductgpu_save_4fields_fou_hdf5_dev(self.h, os.fsencode(filename), _dp(u), _dp(v), _dp(w),
+                                                            _dp(p), C.byref(h)))
+
+    def read_hdf5_header(self, filename):
+        h = H5Header()
+        self._check(lib().ductgpu_read_hdf5_header(self.h, os.fsencode(filename), C.byref(h)))
+        return h.as_dict()
+
+    def read_4fields_fou_hdf5_dev(self, filename, u, v, w, p):
+        """read_4fields_fou_hdf5 into device complex (my, mz, nmodes) fields
+        (the shape of u); returns the file's header as a dict."""
+        my, mz, nm = u.shape
+        h = H5Header()
+        self._check(lib().ductgpu_read_4fields_fou_hdf5_dev(self.h, os.fsencode(filename), _dp(u), _dp(v), _dp(w),
+                                                            _dp(p), my, mz, nm, C.byref(h)))
+        return h.as_dict()
+
     def profile(self, on=True):
         self._check(lib().ductgpu_profile_enable(self.h, int(bool(on))))
 
@@ -701,6 +768,17 @@ class Dns:
     def set_graphs(self, on):
         self.ctx._check(lib().ductgpu_dns_set_graphs(self.h, int(bool(on))))
 
+    def save_hdf5(self, filename, time=0.0, cfl=0.0, slip=0.0):
+        """The state as a uvwp_NNNN.h5 file (ductgpu_dns_save_hdf5)."""
+        self.ctx._check(lib().ductgpu_dns_save_hdf5(self.h, os.fsencode(filename), float(time), float(cfl),
+                                                    float(slip)))
+
+    def load_hdf5(self, filename):
+        """Restart from a uvwp_NNNN.h5 file; returns the file's time."""
+        t = C.c_double()
+        self.ctx._check(lib().ductgpu_dns_load_hdf5(self.h, os.fsencode(filename), C.byref(t)))
+        return t.value
+
     def substep(self, krk, stats=False):
         self.ctx._check(lib().ductgpu_dns_substep(self.h, int(krk), int(bool(stats))))
 
@@ -744,5 +822,6 @@ class Dns:
                     ppb=ppb, spec=np.transpose(spec, (2, 1, 0)).copy(), hist=hist[:nh.value].copy(), divmax=dv)
 
 
-__all__ = ["Context", "Dns", "DeviceArray", "DuctGPUError", "lib", "LIB_PATH", "EXPORTS",
+__all__ = ["Context", "Dns", "DeviceArray", "DuctGPUError", "H5Header", "lib", "LIB_PATH", "EXPORTS",
+           "uvwp_filename", "read_hdf5_header",
            "PREC_FP64", "PREC_MIXED", "GAUGE_POINT", "GAUGE_MEAN"]

@@ -1326,6 +1326,25 @@ extern "C" int ductgpu_dns_field(ductgpu_dns d, int which, double **dev)
     return DUCTGPU_OK;
 }
 
+// After the fields were replaced: with CMASSFLOW the flow rate to hold is
+// that of the new u, and the captured substeps (which bake it in) are
+// re-captured.  Synchronises.
+static int dns_fields_changed(ductgpu_dns d)
+{
+    ductgpu_ctx ctx = d->ctx;
+    if (d->cmassflow) {
+        int rc = ductgpu_impose_mass_flow_dev(ctx, &d->csum, 1, d->vel[0], 0);
+        if (rc) return rc;
+        for (int k = 0; k < 3; ++k)
+            for (int s = 0; s < 2; ++s)
+                if (d->graph[k][s]) {
+                    cudaGraphExecDestroy(d->graph[k][s]);
+                    d->graph[k][s] = nullptr;
+                }
+    }
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "dns_set_fields");
+}
+
 extern "C" int ductgpu_dns_set_fields(ductgpu_dns d, const double *u, const double *v, const double *w,
                                       const double *p)
 {
@@ -1337,19 +1356,48 @@ extern "C" int ductgpu_dns_set_fields(ductgpu_dns d, const double *u, const doub
     double *dst[4] = {d->vel[0], d->vel[1], d->vel[2], d->p};
     for (int c = 0; c < 4; ++c)
         DUCT_CUDA(ctx, cudaMemcpyAsync(dst[c], src[c], sizeof(double) * d->fdoubles, cudaMemcpyDefault, ctx->stream));
-    // CMASSFLOW: the flow rate to hold is that of the initial u
-    if (d->cmassflow) {
-        int rc = ductgpu_impose_mass_flow_dev(ctx, &d->csum, 1, d->vel[0], 0);
-        if (rc) return rc;
-        // the captured substeps bake the flow rate in: re-capture
-        for (int k = 0; k < 3; ++k)
-            for (int s = 0; s < 2; ++s)
-                if (d->graph[k][s]) {
-                    cudaGraphExecDestroy(d->graph[k][s]);
-                    d->graph[k][s] = nullptr;
-                }
-    }
-    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "dns_set_fields");
+    return dns_fields_changed(d);
+}
+
+// The stepper's state as a uvwp_NNNN.h5 file (src/main1.f90:735-752 with
+// save_4fields_fou_hdf5) and back (the irestart read).
+extern "C" int ductgpu_dns_save_hdf5(ductgpu_dns d, const char *filename, double time, double cfl, double slip)
+{
+    if (!d) return DUCTGPU_EARG;
+    ductgpu_ctx ctx = d->ctx;
+    cudaSetDevice(ctx->device);
+    ductgpu_h5_header h{};
+    h.nparams = 7;
+    h.numerop = 1;
+    h.mgalx = d->mgalx;
+    h.my = h.mz = d->my;
+    h.mx1 = d->M - 1;
+    h.alp = d->alp;
+    h.aspect = d->aspect;
+    h.time = time;
+    h.fnu = d->fnu;
+    h.cfl = cfl;
+    h.dtfixed = d->dt;
+    h.cmassflow = d->cmassflow ? d->csum : 0.0;
+    h.slip = slip;
+    double dv[3];
+    DUCT_CUDA(ctx, cudaMemcpyAsync(dv, d->divmax, sizeof dv, cudaMemcpyDeviceToHost, ctx->stream));
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    h.divergence = dv[2];
+    return ductgpu_save_4fields_fou_hdf5_dev(ctx, filename, d->vel[0], d->vel[1], d->vel[2], d->p, &h);
+}
+
+extern "C" int ductgpu_dns_load_hdf5(ductgpu_dns d, const char *filename, double *time)
+{
+    if (!d) return DUCTGPU_EARG;
+    ductgpu_ctx ctx = d->ctx;
+    cudaSetDevice(ctx->device);
+    ductgpu_h5_header h{};
+    int rc = ductgpu_read_4fields_fou_hdf5_dev(ctx, filename, d->vel[0], d->vel[1], d->vel[2], d->p, d->my, d->my,
+                                              d->M, &h);
+    if (rc) return rc;
+    if (time) *time = h.time;
+    return dns_fields_changed(d);
 }
 
 extern "C" int ductgpu_dns_get_fields(ductgpu_dns d, double *u, double *v, double *w, double *p)

@@ -10,6 +10,7 @@
 #include <stdio.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "../../include/ductgpu.h"
 
@@ -194,6 +195,13 @@ int ensure(ductgpu_ctx ctx, Workspace &w, size_t bytes);
 // noalloc.cu: looks up the fixed scratch of the no-allocation entry point
 // on the context's GPU (at context creation)
 void noalloc_reserve(ductgpu_ctx ctx);
+// h5io.cu: the metadata of a uvwp_NNNN.h5 file (everything before the four
+// fields' data), the fields' file offsets and the end-of-file address
+struct H5Layout {
+    std::vector<uint8_t> meta;
+    uint64_t field_off[4] = {}, field_bytes = 0, eof = 0;
+};
+void h5_layout(const ductgpu_h5_header *hdr, H5Layout &L);
 
 // Brackets one kernel launch with profiling events when enabled and
 // counts it.  Use: { LaunchScope ls(ctx, DUCTGPU_K_...); kernel<<<>>>(); }

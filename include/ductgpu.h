@@ -520,6 +520,58 @@ int ductgpu_dns_wallstress_after(ductgpu_dns dns, int nsteps, double *J);
  * No counterpart in the reference (it has no adjoint).                    */
 int ductgpu_dns_grad_wallstress(ductgpu_dns dns, double *J, double *fbar);
 
+/* ---- field checkpoint files uvwp_NNNN.h5 --------------------------------
+ * The reference's restart / output file (src/readwrite_hdf5.f90): datasets
+ * u, v, w, p of HDF5 shape (mx1+1, mz, my, 2), big-endian doubles (the
+ * Fortran (2, my, mz, mx1+1) view of a complex (my, mz, mx1+1) field), and
+ * writeheader_hdf5's scalars in the root group.  Written in the HDF5 file
+ * format without an HDF5 library (version 0 superblock, symbol-table root
+ * group, contiguous storage: what libhdf5 writes with its default format
+ * bounds); read back from that subset.  File errors return DUCTGPU_EARG
+ * with the reason in ductgpu_last_error.                                  */
+typedef struct {
+    int nparams;        /* 7: no temperature fields (read back; written as 7) */
+    int numerop;        /* ranks of the run (written as given, 1 if <= 0)      */
+    int mgalx, my, mz, mx1;
+    double alp, aspect, time, fnu, cfl, dtfixed, cmassflow;
+    double slip;        /* dataset SLIP-VELOCITY                               */
+    double divergence;  /* dataset DIVERGENCE                                  */
+} ductgpu_h5_header;
+/* concat5b(fuvwpout,'uvwp_',5,ext,4,'.',1,'h5',2,filename) with ext the
+ * i4.4 of iimag (src/readwrite_hdf5.f90:326-330, src/concat.F:74-87): the
+ * prefix up to its first blank + "uvwp_NNNN.h5".  cap: bytes of out.     */
+int ductgpu_uvwp_filename(const char *fuvwpout, int iimag, char *out, int cap);
+/* save_4fields_fou_hdf5(u,v,w,p,iimag,'r8') on one rank
+ * (src/readwrite_hdf5.f90:276-386, h5dump_parallel :650-722,
+ * writeheader_hdf5 :851-920): u, v, w, p are DEVICE complex
+ * (my, mz, mx1+1) fields; the header gives the sizes and the scalars.
+ * The fields are converted to big-endian on the GPU (in stream order after
+ * the work already on the context's stream).  Synchronises.               */
+int ductgpu_save_4fields_fou_hdf5_dev(ductgpu_ctx ctx, const char *filename, const double *u,
+                                      const double *v, const double *w, const double *p,
+                                      const ductgpu_h5_header *hdr);
+/* readheader_hdf5 (src/readwrite_hdf5.f90:799-849); without mx1 in the file
+ * mx1 = 2 (mgalx/3)/2 - 1 as there.  ctx may be NULL (no error text).     */
+int ductgpu_read_hdf5_header(ductgpu_ctx ctx, const char *filename, ductgpu_h5_header *hdr);
+/* read_4fields_fou_hdf5(u,v,w,p,filename,'r8') (src/readwrite_hdf5.f90:5-197
+ * with h5load_parallel :199-273) into DEVICE complex (my, mz, nmodes)
+ * fields: the file's modes beyond nmodes are dropped and missing ones are
+ * zero, as there; a file of another my or mz is refused (the reference
+ * re-interpolates with cheb_interp, which is not built).  hdr_out (may be
+ * NULL) receives the file's header.  Synchronises.                        */
+int ductgpu_read_4fields_fou_hdf5_dev(ductgpu_ctx ctx, const char *filename, double *u, double *v,
+                                      double *w, double *p, int my, int mz, int nmodes,
+                                      ductgpu_h5_header *hdr_out);
+/* The stepper's state to / from such a file (src/main1.f90:735-752 saves
+ * every nimag steps; irestart reads it back at start-up).  save: header
+ * from the stepper (mgalx, my = mz, mx1 = modes - 1, alp, aspect, fnu,
+ * dtfixed = dt, cmassflow = the held flow rate, DIVERGENCE = the last
+ * substep's max_3din) plus the caller's time, cfl and slip.  load: the
+ * fields as ductgpu_dns_set_fields takes them (with cmassflow the flow rate
+ * of the loaded u is held), the file's time to *time (may be NULL).       */
+int ductgpu_dns_save_hdf5(ductgpu_dns dns, const char *filename, double time, double cfl, double slip);
+int ductgpu_dns_load_hdf5(ductgpu_dns dns, const char *filename, double *time);
+
 /* ---- the reference's own GPU entry points (src/mytranspose_cuda.cu) --- */
 /* transpose_gpu_(handle,Nx,Ny,alpha,devPtrA,devPtrC) and
  * mat_invdiag_gpu_(handle,Nx,Ny,xlam,devPtrF,devPtrED,devPtrC) with the

@@ -1,0 +1,158 @@
+"""The field checkpoint file uvwp_NNNN.h5 through the library on the GPU.
+
+save_4fields_fou_hdf5 (src/readwrite_hdf5.f90:276-386 with h5dump_parallel
+:650-722 and writeheader_hdf5 :851-920): the library's file must equal the
+oracle's restatement byte for byte, and the oracle's independent reader must
+decode it to the device fields bit for bit.  read_4fields_fou_hdf5 (:5-197):
+the library reads its own and the oracle's files back bit for bit, drops or
+zero-fills modes as the reference does and refuses another y-z resolution.
+The stepper writes its state and restarts from it (src/main1.f90:735-752):
+a restarted run repeats the original to rounding.
+"""
+import numpy as np
+import pytest
+
+import duct_b200 as D
+from duct_b200 import synth
+from oracle import h5file as H
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    with D.Context(0) as c:
+        yield c
+
+
+def fields(my, mz, nm, seed):
+    rng = np.random.default_rng(seed)
+    return [np.asfortranarray(rng.standard_normal((my, mz, nm)) + 1j * rng.standard_normal((my, mz, nm)))
+            for _ in range(4)]
+
+
+def dev(ctx, a):
+    d = ctx.device_array(a.shape)
+    d.upload(a)
+    return d
+
+
+def header(my, mz, nm, **kw):
+    h = dict(numerop=1, mgalx=3 * nm, my=my, mz=mz, mx1=nm - 1, alp=0.5, aspect=1.0, time=1.25, fnu=1 / 4400.0,
+             cfl=0.0, dtfixed=2e-4, cmassflow=1.9, slip=0.0, divergence=1e-13)
+    h.update(kw)
+    return h
+
+
+# (33, 33, 11): one chunk per field; (129, 129, 43): 11.4 MB fields, two
+# 8 MiB staging chunks each (the double-buffered path); (17, 9, 3): my != mz
+@pytest.mark.parametrize("my,mz,nm", [(33, 33, 11), (129, 129, 43), (17, 9, 3)])
+def test_save_equals_oracle_file_and_decodes(ctx, tmp_path, my, mz, nm):
+    host = fields(my, mz, nm, my + nm)
+    d = [dev(ctx, f) for f in host]
+    hdr = header(my, mz, nm)
+    path = tmp_path / "uvwp_0003.h5"
+    try:
+        ctx.save_4fields_fou_hdf5_dev(str(path), *d, hdr)
+        buf = path.read_bytes()
+        ref = H.write_4fields(host, hdr)
+        assert len(buf) == len(ref)
+        diff = np.flatnonzero(np.frombuffer(buf, np.uint8) != np.frombuffer(ref, np.uint8))
+        assert diff.size == 0, "first differing byte at %d of %d" % (diff[0], len(buf))
+        ds = H.read(buf)
+        for a, b in zip(H.fields_of(ds), host):
+            assert np.array_equal(a, b)
+        h = H.header_of(ds)
+        for k, v in hdr.items():
+            assert h[k] == v, k
+        # read back through the library into fresh device fields
+        back = [ctx.device_array((my, mz, nm)) for _ in range(4)]
+        got_hdr = ctx.read_4fields_fou_hdf5_dev(str(path), *back)
+        for a, b in zip(back, host):
+            assert np.array_equal(a.download(), b)
+            a.free()
+        for k, v in hdr.items():
+            assert got_hdr[k] == v, k
+    finally:
+        for a in d:
+            a.free()
+
+
+def test_read_oracle_file_with_fewer_and_more_modes(ctx, tmp_path):
+    """h5load_parallel + the copy of read_4fields_fou_hdf5: modes beyond the
+    run's are dropped, missing ones are zero."""
+    my, nm = 33, 11
+    host = fields(my, my, nm, 5)
+    path = tmp_path / "f.h5"
+    path.write_bytes(H.write_4fields(host, header(my, my, nm)))
+    for want in (7, 11, 15):
+        out = [ctx.device_array((my, my, want)) for _ in range(4)]
+        try:
+            for a in out:
+                a.upload(np.full((my, my, want), 7.0 + 7.0j))
+            ctx.read_4fields_fou_hdf5_dev(str(path), *out)
+            for a, b in zip(out, host):
+                g = a.download()
+                k = min(want, nm)
+                assert np.array_equal(g[:, :, :k], b[:, :, :k])
+                assert not np.any(g[:, :, k:])
+        finally:
+            for a in out:
+                a.free()
+
+
+def test_read_refuses_other_resolution_and_host_fields(ctx, tmp_path):
+    my, nm = 33, 5
+    host = fields(my, my, nm, 6)
+    path = tmp_path / "f.h5"
+    path.write_bytes(H.write_4fields(host, header(my, my, nm)))
+    out = [ctx.device_array((65, 65, nm)) for _ in range(4)]
+    try:
+        before = out[0].download()
+        with pytest.raises(D.DuctGPUError, match="re-interpolation"):
+            ctx.read_4fields_fou_hdf5_dev(str(path), *out)
+        assert np.array_equal(out[0].download(), before)    # nothing written
+    finally:
+        for a in out:
+            a.free()
+    d = [dev(ctx, f) for f in host]
+    try:
+        with pytest.raises(D.DuctGPUError, match="device memory"):
+            ctx.save_4fields_fou_hdf5_dev(str(tmp_path / "g.h5"), host[0].ctypes.data, *d[1:], header(my, my, nm))
+        with pytest.raises(D.DuctGPUError):
+            ctx.save_4fields_fou_hdf5_dev(str(tmp_path / "no/such/dir/g.h5"), *d, header(my, my, nm))
+    finally:
+        for a in d:
+            a.free()
+
+
+def test_dns_save_and_restart_repeat_the_run(ctx, tmp_path):
+    m, mgalx, alp, fnu, dt = 33, 64, 1.0, 1.0 / 2000.0, 1e-3
+    u, v, w, p, dpval = synth.dns_initial(mgalx, m, alp, 0.1, seed=11)
+    ctx.pseudomat(m, m)
+    path = str(tmp_path / D.uvwp_filename("", 1))
+    with D.Dns(ctx, mgalx, alp, fnu, dt, cmassflow=True) as dns:
+        dns.set_fields(u, v, w, p)
+        dns.steps(2)
+        dns.save_hdf5(path, time=2 * dt, cfl=0.25, slip=0.0)
+        saved = dns.fields()
+        divmax = dns.statistics()["divmax"]
+        dns.steps(2)
+        after = dns.fields()
+    ds = H.read(open(path, "rb").read())
+    for a, b in zip(H.fields_of(ds), saved):
+        assert np.array_equal(a, b)
+    h = H.header_of(ds)
+    assert (h["mgalx"], h["my"], h["mz"], h["mx1"]) == (mgalx, m, m, saved[0].shape[2] - 1)
+    assert h["dtfixed"] == dt and h["time"] == 2 * dt and h["cfl"] == 0.25 and h["alp"] == alp
+    assert h["divergence"] == divmax[2]
+    # the restart holds the flow rate of the loaded u, which the mass-flow
+    # correction kept at the original's to rounding: the run repeats to
+    # rounding
+    with D.Dns(ctx, mgalx, alp, fnu, dt, cmassflow=True) as dns:
+        assert dns.load_hdf5(path) == 2 * dt
+        for a, b in zip(dns.fields(), saved):
+            assert np.array_equal(a, b)
+        dns.steps(2)
+        for a, b in zip(dns.fields(), after):
+            assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()

@@ -1,0 +1,121 @@
+"""The field checkpoint file uvwp_NNNN.h5 on the CPU: the oracle's writer
+against its independent reader, the library's header reader and file name
+rule against the oracle (no GPU: the library's HDF5 reader of the header is
+host code), and the reader's refusals of damaged files.
+
+Reference: save_4fields_fou_hdf5 / writeheader_hdf5 / readheader_hdf5
+(src/readwrite_hdf5.f90:276-386, 799-920), concat5b (src/concat.F:74-87).
+"""
+import numpy as np
+import pytest
+
+import duct_b200 as D
+from oracle import h5file as H
+
+
+def fields(my, mz, nm, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(4):
+        f = rng.standard_normal((my, mz, nm)) + 1j * rng.standard_normal((my, mz, nm))
+        out.append(np.asfortranarray(f))
+    return out
+
+
+HDR = dict(numerop=1, mgalx=16, my=9, mz=7, mx1=4, alp=0.5, aspect=1.25, time=3.75, fnu=1 / 4400.0,
+           cfl=0.3, dtfixed=2e-4, cmassflow=1.92783343620839, slip=1e-17, divergence=3.5e-13)
+
+
+def test_oracle_writer_reader_roundtrip():
+    f = fields(9, 7, 5, 1)
+    buf = H.write_4fields(f, HDR)
+    ds = H.read(buf)
+    assert ds["u"].shape == (5, 7, 9, 2) and ds["u"].dtype == np.float64
+    for a, b in zip(H.fields_of(ds), f):
+        assert np.array_equal(a, b)
+    h = H.header_of(ds)
+    assert h["nparams"] == 7
+    for k, v in HDR.items():
+        assert h[k] == v, k
+
+
+def test_oracle_file_layout_facts():
+    """Big-endian doubles in (mx1+1, mz, my, 2) order at a 4 KiB-aligned
+    offset; the file ends at the superblock's end-of-file address."""
+    f = fields(9, 7, 5, 2)
+    buf = H.write_4fields(f, HDR)
+    eof = int.from_bytes(buf[40:48], "little")
+    assert eof == len(buf)
+    raw = f[0].reshape(-1, order="F").view(np.float64).astype(">f8").tobytes()
+    at = buf.find(raw)
+    assert at > 0 and at % 4096 == 0
+
+
+def test_library_reads_oracle_header(tmp_path):
+    path = tmp_path / "uvwp_0003.h5"
+    path.write_bytes(H.write_4fields(fields(9, 7, 5, 3), HDR))
+    h = D.read_hdf5_header(str(path))
+    assert h["nparams"] == 7
+    for k, v in HDR.items():
+        assert h[k] == v, k
+
+
+def test_library_header_without_mx1(tmp_path):
+    """readheader_hdf5 (src/readwrite_hdf5.f90:822-825): a file without mx1
+    holds the 2/3-rule modes of mgalx."""
+    hdr = dict(HDR, mgalx=64, mx1=20)
+    path = tmp_path / "old.h5"
+    path.write_bytes(H.write_4fields(fields(9, 7, 21, 4), hdr, omit=("mx1", "numerop")))
+    h = D.read_hdf5_header(str(path))
+    assert h["mx1"] == 2 * (64 // 3) // 2 - 1 == 20
+    assert h["numerop"] == 1
+
+
+def test_library_reads_file_behind_a_user_block(tmp_path):
+    """A superblock after a 512-byte user block: addresses count from it."""
+    buf = H.write_4fields(fields(9, 7, 5, 5), HDR)
+    path = tmp_path / "ub.h5"
+    path.write_bytes(b"\0" * 512 + buf)
+    assert D.read_hdf5_header(str(path))["time"] == HDR["time"]
+    assert H.header_of(H.read(path.read_bytes()))["time"] == HDR["time"]
+
+
+@pytest.mark.parametrize("cut", ["truncated", "signature", "snod", "heap", "empty"])
+def test_library_refuses_damaged_files(tmp_path, cut):
+    buf = bytearray(H.write_4fields(fields(9, 7, 5, 6), HDR))
+    if cut == "truncated":
+        buf = buf[:len(buf) // 2]
+    elif cut == "signature":
+        buf[1:4] = b"XYZ"
+    elif cut == "snod":
+        at = buf.find(b"SNOD")
+        buf[at:at + 4] = b"SNOX"
+    elif cut == "heap":
+        at = buf.find(b"HEAP")
+        buf[at + 8:at + 16] = (1 << 40).to_bytes(8, "little")   # heap larger than the file
+    else:
+        buf = bytearray()
+    path = tmp_path / "bad.h5"
+    path.write_bytes(bytes(buf))
+    with pytest.raises(D.DuctGPUError):
+        D.read_hdf5_header(str(path))
+    if cut != "empty":
+        with pytest.raises(H.FormatError):
+            H.read(bytes(buf))
+
+
+def test_library_refuses_missing_file(tmp_path):
+    with pytest.raises(D.DuctGPUError):
+        D.read_hdf5_header(str(tmp_path / "nothing.h5"))
+
+
+@pytest.mark.parametrize("prefix,iimag", [("run/", 0), ("run/", 7), ("/data/duct_", 123), ("out ", 9999),
+                                          ("a b c", 42), ("x/", 10000), ("x/", -1)])
+def test_uvwp_filename_matches_concat5b(prefix, iimag):
+    assert D.uvwp_filename(prefix, iimag) == H.uvwp_filename(prefix, iimag)
+
+
+def test_uvwp_filename_examples():
+    assert D.uvwp_filename("run/", 12) == "run/uvwp_0012.h5"
+    assert D.uvwp_filename("out   ", 3) == "outuvwp_0003.h5"
+    assert D.uvwp_filename("x/", 12345) == "x/uvwp_****.h5"
