@@ -1327,14 +1327,18 @@ extern "C" int ductgpu_dns_field(ductgpu_dns d, int which, double **dev)
 }
 
 // After the fields were replaced: with CMASSFLOW the flow rate to hold is
-// that of the new u, and the captured substeps (which bake it in) are
-// re-captured.  Synchronises.
-static int dns_fields_changed(ductgpu_dns d)
+// `csum` when given (> 0), else that of the new u, and the captured
+// substeps (which bake it in) are re-captured.  Synchronises.
+static int dns_fields_changed(ductgpu_dns d, double csum = 0.0)
 {
     ductgpu_ctx ctx = d->ctx;
     if (d->cmassflow) {
-        int rc = ductgpu_impose_mass_flow_dev(ctx, &d->csum, 1, d->vel[0], 0);
-        if (rc) return rc;
+        if (csum > 0.0) {
+            d->csum = csum;
+        } else {
+            int rc = ductgpu_impose_mass_flow_dev(ctx, &d->csum, 1, d->vel[0], 0);
+            if (rc) return rc;
+        }
         for (int k = 0; k < 3; ++k)
             for (int s = 0; s < 2; ++s)
                 if (d->graph[k][s]) {
@@ -1397,7 +1401,9 @@ extern "C" int ductgpu_dns_load_hdf5(ductgpu_dns d, const char *filename, double
                                               d->M, &h);
     if (rc) return rc;
     if (time) *time = h.time;
-    return dns_fields_changed(d);
+    // the run's constant flow rate travels in the file (writeheader_hdf5's
+    // cmassflow), so a restart holds exactly the saved run's
+    return dns_fields_changed(d, h.cmassflow);
 }
 
 extern "C" int ductgpu_dns_get_fields(ductgpu_dns d, double *u, double *v, double *w, double *p)

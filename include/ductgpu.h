@@ -567,8 +567,10 @@ int ductgpu_read_4fields_fou_hdf5_dev(ductgpu_ctx ctx, const char *filename, dou
  * from the stepper (mgalx, my = mz, mx1 = modes - 1, alp, aspect, fnu,
  * dtfixed = dt, cmassflow = the held flow rate, DIVERGENCE = the last
  * substep's max_3din) plus the caller's time, cfl and slip.  load: the
- * fields as ductgpu_dns_set_fields takes them (with cmassflow the flow rate
- * of the loaded u is held), the file's time to *time (may be NULL).       */
+ * fields as ductgpu_dns_set_fields takes them, the file's time to *time
+ * (may be NULL); with cmassflow the file's cmassflow is the flow rate held
+ * (that of the loaded u when the file's is 0), so a restart repeats the
+ * saved run bit for bit.                                                   */
 int ductgpu_dns_save_hdf5(ductgpu_dns dns, const char *filename, double time, double cfl, double slip);
 int ductgpu_dns_load_hdf5(ductgpu_dns dns, const char *filename, double *time);
 

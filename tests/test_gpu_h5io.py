@@ -7,7 +7,7 @@ decode it to the device fields bit for bit.  read_4fields_fou_hdf5 (:5-197):
 the library reads its own and the oracle's files back bit for bit, drops or
 zero-fills modes as the reference does and refuses another y-z resolution.
 The stepper writes its state and restarts from it (src/main1.f90:735-752):
-a restarted run repeats the original to rounding.
+a restarted run repeats the original bit for bit.
 """
 import numpy as np
 import pytest
@@ -146,13 +146,12 @@ def test_dns_save_and_restart_repeat_the_run(ctx, tmp_path):
     assert (h["mgalx"], h["my"], h["mz"], h["mx1"]) == (mgalx, m, m, saved[0].shape[2] - 1)
     assert h["dtfixed"] == dt and h["time"] == 2 * dt and h["cfl"] == 0.25 and h["alp"] == alp
     assert h["divergence"] == divmax[2]
-    # the restart holds the flow rate of the loaded u, which the mass-flow
-    # correction kept at the original's to rounding: the run repeats to
-    # rounding
+    # the restart holds the file's cmassflow, the run's own flow rate: the
+    # run repeats bit for bit
     with D.Dns(ctx, mgalx, alp, fnu, dt, cmassflow=True) as dns:
         assert dns.load_hdf5(path) == 2 * dt
         for a, b in zip(dns.fields(), saved):
             assert np.array_equal(a, b)
         dns.steps(2)
         for a, b in zip(dns.fields(), after):
-            assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
+            assert np.array_equal(a, b)
