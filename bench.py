@@ -708,6 +708,24 @@ def dns_cfg4(args, local, with_cpu):
     return out
 
 
+def _fs_rates(directory, nbytes):
+    """Plain write / read rates of the file system under `directory` for a
+    file of nbytes (numpy tofile / fromfile, no fsync): the bound the
+    checkpoint calls run against."""
+    import tempfile
+    buf = np.random.default_rng(0).integers(0, 255, nbytes, dtype=np.uint8)
+    with tempfile.TemporaryDirectory(dir=directory) as tdir:
+        path = os.path.join(tdir, "plain.bin")
+        t0 = time.perf_counter()
+        buf.tofile(path)
+        tw = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        back = np.fromfile(path, dtype=np.uint8)
+        tr = time.perf_counter() - t0
+    assert back.size == nbytes
+    return {"write_GBps": nbytes / tw / 1e9, "read_GBps": nbytes / tr / 1e9}
+
+
 def dns_checkpoint(ctx, d):
     """The stepper's state written as the reference's uvwp_NNNN.h5
     (save_4fields_fou_hdf5 + writeheader_hdf5) to a temporary directory and
@@ -732,7 +750,23 @@ def dns_checkpoint(ctx, d):
         t_load = time.perf_counter() - t0
     after = d.fields()
     field_bytes = 4 * before[0].nbytes
-    return {"file_bytes": nbytes, "field_bytes": field_bytes,
+    fs = _fs_rates(tempfile.gettempdir(), nbytes)
+    shm = None
+    if os.path.isdir("/dev/shm"):
+        st = os.statvfs("/dev/shm")
+        if st.f_bavail * st.f_frsize > 3 * nbytes:
+            with tempfile.TemporaryDirectory(dir="/dev/shm") as tdir:
+                path = D.uvwp_filename(tdir + "/", 1)
+                t0 = time.perf_counter()
+                d.save_hdf5(path, time=0.0)
+                ts = time.perf_counter() - t0
+                t0 = time.perf_counter()
+                d.load_hdf5(path)
+                tl = time.perf_counter() - t0
+            shm = {"save_ms": 1e3 * ts, "save_GBps": field_bytes / ts / 1e9, "load_ms": 1e3 * tl,
+                   "load_GBps": field_bytes / tl / 1e9, "file_system": _fs_rates("/dev/shm", nbytes)}
+    return {"file_bytes": nbytes, "field_bytes": field_bytes, "tmpdir": tempfile.gettempdir(),
+            "tmpdir_plain_io": fs, "dev_shm": shm,
             "save_ms": 1e3 * t_save, "save_GBps": field_bytes / t_save / 1e9,
             "load_ms": 1e3 * t_load, "load_GBps": field_bytes / t_load / 1e9,
             "swap_kernels": {"launches": kn, "ms": kms, "GBps": field_bytes / (kms * 1e-3) / 1e9 if kms else None,
