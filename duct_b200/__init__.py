@@ -48,7 +48,7 @@ EXPORTS = [
     "ductgpu_dns_wallstress_after", "ductgpu_dns_grad_wallstress", "ductgpu_set_rect_fold",
     "ductgpu_set_line_kernel", "ductgpu_uvwp_filename", "ductgpu_save_4fields_fou_hdf5_dev",
     "ductgpu_read_hdf5_header", "ductgpu_read_4fields_fou_hdf5_dev", "ductgpu_dns_save_hdf5",
-    "ductgpu_dns_load_hdf5",
+    "ductgpu_dns_load_hdf5", "ductgpu_vorticity_dev", "ductgpu_dns_statistics_omg",
 ]
 SETUP_NO_EIGEN = 1
 (K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER, K_LINES,
@@ -192,6 +192,8 @@ def lib():
             "ductgpu_read_4fields_fou_hdf5_dev": [P, C.c_char_p, P, P, P, P, I, I, I, C.POINTER(H5Header)],
             "ductgpu_dns_save_hdf5": [P, C.c_char_p, D, D, D],
             "ductgpu_dns_load_hdf5": [P, C.c_char_p, C.POINTER(D)],
+            "ductgpu_vorticity_dev": [P, P, P, P, P, I, I, I, P, D, I],
+            "ductgpu_dns_statistics_omg": [P, P, P, C.POINTER(I)],
             "transpose_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
                                C.POINTER(C.c_size_t)],
             "mat_invdiag_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
@@ -652,6 +654,12 @@ class Context:
                                                   _ptr(np.ascontiguousarray(xalp, dtype=np.float64)),
                                                   float(aspect), None if stats2 is None else _dp(stats2)))
 
+    def vorticity_dev(self, u, v, w, vort, xalp, iflag, aspect=1.0):
+        my, mz, nm = u.shape
+        self._check(lib().ductgpu_vorticity_dev(self.h, _dp(u), _dp(v), _dp(w), _dp(vort), my, mz, nm,
+                                                _ptr(np.ascontiguousarray(xalp, dtype=np.float64)), float(aspect),
+                                                int(iflag)))
+
     def max_3din_dev(self, u):
         my, mz, nm = u.shape
         out = C.c_double()
@@ -804,6 +812,17 @@ class Dns:
         J = C.c_double()
         self.ctx._check(lib().ductgpu_dns_grad_wallstress(self.h, C.byref(J), g.ctypes.data_as(C.c_void_p)))
         return J.value, np.stack([np.asfortranarray(np.transpose(g[c], (2, 1, 0))) for c in range(3)])
+
+    def statistics_omg(self):
+        """dict(om2 (3,my,my): omx2, omy2, omz2; hist (nhist,16): sector
+        energies [5] and |Re| integrals [5] of om_x, energy_fou of om_x,
+        om_y, om_z, the same with mode 0) -- ductgpu_dns_statistics_omg."""
+        my = self.my
+        om2 = np.zeros((my, my, 3), order="F")
+        hist = np.zeros((max(self.hist_cap, 1), 16))
+        nh = C.c_int()
+        self.ctx._check(lib().ductgpu_dns_statistics_omg(self.h, _ptr(om2), _ptr(hist), C.byref(nh)))
+        return dict(om2=np.moveaxis(om2, 2, 0).copy(), hist=hist[:nh.value].copy())
 
     def statistics(self):
         """dict(nstat, mean (4,my,my), prod (6,my,my), ppb (my,my), spec

@@ -373,6 +373,87 @@ __global__ void k_spectra(const double2 *u, const double2 *v, const double2 *w, 
     spec[((size_t)c * 7 + s) * M + i] += (i == 0) ? a : a * 2.0;
 }
 
+// Vorticity statistics of a recorded step (src/main1.f90:453-466): per
+// component c of omega, statistics_omg2_fou (src/operators.F:1859-1955)
+// om2[c] += |w_0|^2 + sum_{i>=1} 2 |w_i|^2 per point, and energy_fou's sums
+// (907-973); for omega_x also energy_fou_zero_sector (1018-1099, |w_0|^2 dy
+// dz per sector) and integral_abs_zero_sector (1462-1541, |Re w_0| dy dz).
+// Sectors of point (j, k), 1-based: 1 j<k, j<mz+1-k; 2 j<k, j>mz+1-k;
+// 3 j>k, j>mz+1-k; 4 j>k, j<mz+1-k; 5 on a diagonal.
+constexpr int kOmgVals = 16;   // e (x, y, z), e0 (x, y, z), sector |w0|^2 [5], sector |Re w0| [5]
+
+struct OmgParams {
+    const double2 *f[3];     // omega_x, omega_y, omega_z
+    const double *wcc;       // [P] dy dz
+    double *om2;             // [3][P] added
+    double *partial;         // [gridDim][kOmgVals]
+    long long P;
+    int M, my, mz;
+};
+
+__global__ void __launch_bounds__(kStatThreads) k_omg_stats(const __grid_constant__ OmgParams p)
+{
+    __shared__ double red[32];
+    double acc[kOmgVals];
+#pragma unroll
+    for (int k = 0; k < kOmgVals; ++k) acc[k] = 0.0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < p.P; q += (long long)gridDim.x * blockDim.x) {
+        const double wq = p.wcc[q];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double2 *f = p.f[c];
+            double e = 0.0;
+            for (int i = 1; i < p.M; ++i) {
+                const double2 z = f[q + (long long)i * p.P];
+                e = e + (z.x * z.x + z.y * z.y) * 2.0;
+            }
+            const double2 z0 = f[q];
+            const double a0 = z0.x * z0.x + z0.y * z0.y;
+            p.om2[c * p.P + q] += e + a0;
+            acc[c] += e * wq;
+            acc[3 + c] += a0 * wq;
+        }
+        const int j = (int)(q % p.my) + 1, k = (int)(q / p.my) + 1, kr = p.mz + 1 - k;
+        const int s = (j < k && j < kr) ? 0 : (j < k && j > kr) ? 1 : (j > k && j > kr) ? 2 : (j > k && j < kr) ? 3 : 4;
+        const double2 z0 = p.f[0][q];
+#pragma unroll
+        for (int t = 0; t < 5; ++t) {
+            acc[6 + t] += (t == s) ? (z0.x * z0.x + z0.y * z0.y) * wq : 0.0;
+            acc[11 + t] += (t == s) ? fabs(z0.x) * wq : 0.0;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kOmgVals; ++k) {
+        const double sum = block_sum(acc[k], red);
+        if (threadIdx.x == 0) p.partial[blockIdx.x * kOmgVals + k] = sum;
+    }
+}
+
+// The row of the step just recorded by k_stats_finish (*counter - 1):
+// out[0..4] energomx4 (sector energies / area), out[5..9] energomxb4
+// (sector |Re w0| integrals / area), out[10..12] energy_fou of omega_x,
+// omega_y, omega_z (sqrt(e / area)), out[13..15] the same with mode 0.
+__global__ void k_omg_finish(const double *partial, int nblocks, double area, double *out, const int *counter, int cap)
+{
+    __shared__ double e[kOmgVals];
+    const int k = threadIdx.x;
+    if (k < kOmgVals) {
+        double sum = 0.0;
+        for (int b = 0; b < nblocks; ++b) sum += partial[b * kOmgVals + k];
+        e[k] = sum;
+    }
+    __syncthreads();
+    const int row = *counter - 1;
+    if (row < 0 || row >= cap) return;
+    double *o = out + (size_t)kOmgVals * row;
+    if (k < 3) {
+        o[10 + k] = sqrt(e[k] / area);
+        o[13 + k] = sqrt((e[k] + e[3 + k]) / area);
+    } else if (k >= 6 && k < 16) {
+        o[k - 6] = e[k] / area;
+    }
+}
+
 // Host: the weights.  Nodes x_j = -s cos(pi j / (n - 1)); mesh sizes of
 // src/ininewc.f90:102-112 (half the distance between the neighbours).
 static void mesh_sizes(int n, double s, std::vector<double> &d)
@@ -628,6 +709,13 @@ static void add_job(LineParams &p, const double *in, std::initializer_list<LineO
     for (const LineOut &o : outs) J.o[J.nout++] = o;
 }
 
+// One more output of job `job` (from the same staged lines).
+static void add_out(LineParams &p, int job, const LineOut &o)
+{
+    LineJob &J = p.job[job];
+    if (J.nout < kMaxLineOut) J.o[J.nout++] = o;
+}
+
 }  // namespace duct
 
 using namespace duct;
@@ -672,6 +760,40 @@ extern "C" int ductgpu_laplacian3d_dev(ductgpu_ctx ctx, const double *u, double 
     LineParams pz = line_params('z', my, mz, nmodes, xd);
     add_job(pz, u, {line_out(flap, 2, scal / (aspect * aspect), 1.0)});
     return lines_launch(ctx, pz);
+}
+
+extern "C" int ductgpu_vorticity_dev(ductgpu_ctx ctx, const double *u, const double *v, const double *w, double *vort,
+                                     int my, int mz, int nmodes, const double *xalp, double aspect, int iflag)
+{
+    if (!ctx) return DUCTGPU_EARG;
+    int rc = check_geom(ctx, "vorticity", my, mz, nmodes, true);
+    if (!rc) rc = check_ptrs(ctx, "vorticity", {u, v, w, vort});
+    if (rc) return rc;
+    if (iflag < 1 || iflag > 3) return set_error(ctx, DUCTGPU_EARG, "vorticity: component %d (1, 2, 3)", iflag);
+    if (vort == u || vort == v || vort == w) return set_error(ctx, DUCTGPU_EARG, "vorticity: vort must differ from u, v, w");
+    cudaSetDevice(ctx->device);
+    const double *xd;
+    if ((rc = upload_xalp(ctx, xalp, nmodes, &xd))) return rc;
+    if (iflag == 1) {                       // om_x = w,y - v,z
+        LineParams py = line_params('y', my, mz, nmodes, xd);
+        add_job(py, w, {line_out(vort, 1, 1.0, 0.0)});
+        if ((rc = lines_launch(ctx, py))) return rc;
+        LineParams pz = line_params('z', my, mz, nmodes, xd);
+        add_job(pz, v, {line_out(vort, 1, -1.0 / aspect, 1.0)});
+        return lines_launch(ctx, pz);
+    }
+    if (iflag == 2) {                       // om_y = u,z - w,x
+        LineParams pz = line_params('z', my, mz, nmodes, xd);
+        LineOut o = line_out(vort, 1, 1.0 / aspect, 0.0);
+        xterm(o, w, 0.0, -1.0, 0.0);
+        add_job(pz, u, {o});
+        return lines_launch(ctx, pz);
+    }
+    LineParams py = line_params('y', my, mz, nmodes, xd);   // om_z = v,x - u,y
+    LineOut o = line_out(vort, 1, -1.0, 0.0);
+    xterm(o, v, 0.0, 1.0, 0.0);
+    add_job(py, u, {o});
+    return lines_launch(ctx, py);
 }
 
 extern "C" int ductgpu_grad3d_dev(ductgpu_ctx ctx, const double *u, double *dxu, double *dyu, double *dzu, int my,
@@ -861,6 +983,34 @@ static int stats_issue(ductgpu_ctx ctx, const double *const f[4], int nf, const 
     }
     return check_cuda(ctx, cudaGetLastError(), "k_stats");
 }
+
+// The vorticity statistics of one recorded step from omega (om) into the
+// accumulators om2 and the history row the step's k_stats_finish opened.
+static int omg_issue(ductgpu_ctx ctx, double *const om[3], const double *wcc, double *om2, double *partial,
+                     double *out, const int *counter, int cap, int my, int mz, int M, double aspect)
+{
+    OmgParams op{};
+    for (int c = 0; c < 3; ++c) op.f[c] = reinterpret_cast<const double2 *>(om[c]);
+    op.wcc = wcc;
+    op.om2 = om2;
+    op.partial = partial;
+    op.P = (long long)my * mz;
+    op.M = M;
+    op.my = my;
+    op.mz = mz;
+    int blocks = (int)((op.P + kStatThreads - 1) / kStatThreads);
+    if (blocks > kStatBlocksMax) blocks = kStatBlocksMax;
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_STATS);
+        k_omg_stats<<<blocks, kStatThreads, 0, ctx->stream>>>(op);
+    }
+    DUCT_CUDA(ctx, cudaGetLastError());
+    {
+        LaunchScope ls(ctx, DUCTGPU_K_STATS);
+        k_omg_finish<<<1, 32, 0, ctx->stream>>>(partial, blocks, 4.0 * aspect, out, counter, cap);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "k_omg_stats");
+}
 }  // namespace duct
 
 extern "C" int ductgpu_wallstressx_dev(ductgpu_ctx ctx, const double *u, int my, int mz, double aspect,
@@ -963,6 +1113,8 @@ struct ductgpu_dns_s {
     std::vector<double> lamh_d[3], lamh_n;
     // statistics accumulators and per-step history
     double *st_mean = nullptr, *st_prod = nullptr, *st_ppb = nullptr, *st_spec = nullptr;
+    double *st_om2 = nullptr;    // [3][P] omx2, omy2, omz2 (statistics_omg2_fou)
+    double *hist_om = nullptr;   // per recorded step: kOmgVals vorticity diagnostics
     double *wcc = nullptr, *wst = nullptr, *partial = nullptr;
     double *hist = nullptr;
     int *hist_n = nullptr;
@@ -1089,6 +1241,15 @@ static int dns_issue(ductgpu_dns d, int krk, bool stats)
             if (d->forced) xterm(o, d->force + c * d->fdoubles, a + b, 0.0, 0.0);
             add_job(py, d->vel[c], {o});
         }
+        if (stats) {
+            // the vorticity diagnostics of src/main1.f90:453-466 from the
+            // same staged lines, into the product fields (free once the
+            // advection is done): omega_z = i kx v - du/dy, omega_x = dw/dy
+            LineOut oz = line_out(d->prod[2], 1, -1.0, 0.0);
+            xterm(oz, v, 0.0, 1.0, 0.0);
+            add_out(py, 0, oz);
+            add_out(py, 2, line_out(d->prod[0], 1, 1.0, 0.0));
+        }
         if ((rc = lines_launch(ctx, py))) return rc;
     }
     // (vi) y and z parts of -(a+b) grad p: different outputs, the z part on
@@ -1116,7 +1277,27 @@ static int dns_issue(ductgpu_dns d, int krk, bool stats)
         LineParams pz = line_params('z', my, my, M, xd, 1);
         for (int c = 0; c < 3; ++c)
             add_job(pz, d->vel[c], {line_out(d->h[c], 2, nu * a / (asp * asp), 1.0, -1.0 / (nu * b))});
+        if (stats) {
+            // omega_x -= dv/dz, omega_y = du/dz - i kx w
+            add_out(pz, 1, line_out(d->prod[0], 1, -1.0 / asp, 1.0));
+            LineOut oy = line_out(d->prod[1], 1, 1.0 / asp, 0.0);
+            xterm(oy, w, 0.0, -1.0, 0.0);
+            add_out(pz, 0, oy);
+        }
         if ((rc = lines_launch(ctx, pz))) return rc;
+    }
+    // the vorticity statistics on the side stream, concurrent with the
+    // predictor solves (they read only the product fields)
+    const bool fork_omg = stats && side_fork(ctx, &mainst);
+    if (stats) {
+        if (fork_omg) ctx->stream = ctx->side[0];
+        rc = omg_issue(ctx, d->prod, d->wcc, d->st_om2, d->partial, d->hist_om, d->hist_n, d->hist_cap, my, my, M,
+                       asp);
+        ctx->stream = mainst;
+        if (rc) {
+            if (fork_omg) side_join(ctx, mainst);
+            return rc;
+        }
     }
     // (viii) predictor: helm3d 'd', helco = 1/(beta nu dt)
     {
@@ -1130,7 +1311,12 @@ static int dns_issue(ductgpu_dns d, int krk, bool stats)
             t[c].plane0 = c * M;
             t[c].refine = 1;
         }
-        if ((rc = dns_solve(d, t, 3, d->lam_d[k], d->lamh_d[k]))) return rc;
+        rc = dns_solve(d, t, 3, d->lam_d[k], d->lamh_d[k]);
+        if (fork_omg) {
+            const int rj = side_join(ctx, mainst);
+            if (!rc) rc = rj;
+        }
+        if (rc) return rc;
     }
     // (ix) rhs of the pseudo-pressure: div(u) / ((a+b) dt) -> h1
     const double sdiv = 1.0 / ((a + b) * dt);
@@ -1196,7 +1382,9 @@ static void dns_free(ductgpu_dns d)
     cudaFree(d->st_mean);
     cudaFree(d->wcc);
     cudaFree(d->hist);
+    cudaFree(d->hist_om);
     cudaFree(d->hist_n);
+    cudaFree(d->divmax);
     cudaFree(d->force);
     cudaFree(d->dmat);
     cudaFree(d->adj);
@@ -1278,19 +1466,20 @@ extern "C" int ductgpu_dns_create(ductgpu_ctx ctx, int mgalx, double alp, double
     if (cudaMalloc(&d->lam_n, sizeof(double) * M) != cudaSuccess ||
         cudaMemcpy(d->lam_n, lam.data(), sizeof(double) * M, cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(check_cuda(ctx, cudaGetLastError(), "dns: lambda"));
-    // statistics: mean [4][P], prod [6][P], ppb [P], spec [4][7][M] in one block; weights
-    const size_t nst = 4 * d->P + 6 * d->P + d->P + 4 * 7 * (size_t)M;
+    // statistics: mean [4][P], prod [6][P], ppb [P], spec [4][7][M], om2 [3][P] in one block; weights
+    const size_t nst = 4 * d->P + 6 * d->P + d->P + 4 * 7 * (size_t)M + 3 * d->P;
     if (cudaMalloc(&d->st_mean, sizeof(double) * nst) != cudaSuccess)
         return fail(check_cuda(ctx, cudaGetLastError(), "dns: statistics"));
     d->st_prod = d->st_mean + 4 * d->P;
     d->st_ppb = d->st_prod + 6 * d->P;
     d->st_spec = d->st_ppb + d->P;
+    d->st_om2 = d->st_spec + 4 * 7 * (size_t)M;
     cudaMemset(d->st_mean, 0, sizeof(double) * nst);
     {
         std::vector<double> wcc, wst;
         make_weights(my, my, aspect, wcc, wst);
         // the partial sums of the statistics kernel, and one row of scratch results after them
-        const size_t nw = wcc.size() + wst.size() + (size_t)(kStatBlocksMax + 1) * kStatVals;
+        const size_t nw = wcc.size() + wst.size() + (size_t)(kStatBlocksMax + 1) * (kOmgVals > kStatVals ? kOmgVals : kStatVals);
         if (cudaMalloc(&d->wcc, sizeof(double) * nw) != cudaSuccess)
             return fail(check_cuda(ctx, cudaGetLastError(), "dns: weights"));
         d->wst = d->wcc + wcc.size();
@@ -1300,6 +1489,7 @@ extern "C" int ductgpu_dns_create(ductgpu_ctx ctx, int mgalx, double alp, double
     }
     d->hist_cap = hist_cap;
     if (cudaMalloc(&d->hist, sizeof(double) * kStatVals * (hist_cap > 0 ? hist_cap : 1)) != cudaSuccess ||
+        cudaMalloc(&d->hist_om, sizeof(double) * kOmgVals * (hist_cap > 0 ? hist_cap : 1)) != cudaSuccess ||
         cudaMalloc(&d->hist_n, sizeof(int)) != cudaSuccess || cudaMemset(d->hist_n, 0, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&d->divmax, sizeof(double) * 3) != cudaSuccess)
         return fail(check_cuda(ctx, cudaGetLastError(), "dns: history"));
@@ -1518,6 +1708,22 @@ extern "C" int ductgpu_dns_statistics(ductgpu_dns d, double *mean, double *prod,
     if (nstat) *nstat = d->nstat;
     if (nhist) *nhist = nh;
     if (divmax3) DUCT_CUDA(ctx, cudaMemcpy(divmax3, d->divmax, sizeof(double) * 3, cudaMemcpyDeviceToHost));
+    return DUCTGPU_OK;
+}
+
+extern "C" int ductgpu_dns_statistics_omg(ductgpu_dns d, double *om2, double *hist, int *nhist)
+{
+    if (!d) return DUCTGPU_EARG;
+    ductgpu_ctx ctx = d->ctx;
+    cudaSetDevice(ctx->device);
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (om2) DUCT_CUDA(ctx, cudaMemcpy(om2, d->st_om2, sizeof(double) * 3 * d->P, cudaMemcpyDeviceToHost));
+    int nh = 0;
+    DUCT_CUDA(ctx, cudaMemcpy(&nh, d->hist_n, sizeof(int), cudaMemcpyDeviceToHost));
+    if (nh > d->hist_cap) nh = d->hist_cap;
+    if (hist && nh > 0)
+        DUCT_CUDA(ctx, cudaMemcpy(hist, d->hist_om, sizeof(double) * kOmgVals * nh, cudaMemcpyDeviceToHost));
+    if (nhist) *nhist = nh;
     return DUCTGPU_OK;
 }
 

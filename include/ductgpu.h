@@ -454,6 +454,12 @@ int ductgpu_wallstressx_dev(ductgpu_ctx ctx, const double *u, int my, int mz, do
  * (synchronises).                                                         */
 int ductgpu_energy_fou_dev(ductgpu_ctx ctx, const double *u, int my, int mz, int nmodes, double aspect,
                            double *energy, double *energy2);
+/* vorticity(u,v,w,vort,tmp,iflag), src/operators.F:810-905: component
+ * iflag of the vorticity, 1 om_x = dw/dy - dv/dz, 2 om_y = du/dz - dw/dx,
+ * 3 om_z = dv/dx - du/dy, of device x-cut fields (vort distinct from u, v,
+ * w; xalp on the host).                                                   */
+int ductgpu_vorticity_dev(ductgpu_ctx ctx, const double *u, const double *v, const double *w, double *vort,
+                          int my, int mz, int nmodes, const double *xalp, double aspect, int iflag);
 /* statistics_fou(u,v,w,p,1), src/operators.F:1608-1765 (one rank): adds
  * to the device accumulators mean (my,mz,4) the mode-0 real parts of u, v,
  * w, p, ppb (my,mz) the x-mean of p^2, spec (nmodes,7,4) the streamwise
@@ -499,6 +505,15 @@ int ductgpu_dns_steps(ductgpu_dns dns, int nsteps, int stats_every);
  * after each substep of the last step.  Synchronises.                    */
 int ductgpu_dns_statistics(ductgpu_dns dns, double *mean, double *prod, double *ppb, double *spec,
                            double *hist, int *nstat, int *nhist, double *divmax3);
+/* The vorticity diagnostics of the recorded steps (src/main1.f90:453-466):
+ * om2 (my,my,3) the accumulators omx2, omy2, omz2 of statistics_omg2_fou
+ * (src/operators.F:1859-1955); hist rows of 16 doubles per recorded step,
+ * in the order of ductgpu_dns_statistics' rows: energy_fou_zero_sector of
+ * om_x (energomx4[5], :1018-1099), integral_abs_zero_sector of om_x
+ * (energomxb4[5], :1462-1541), energy_fou of om_x, om_y, om_z (energomx,
+ * energomy, energomz) and the same with mode 0 (energomxb, energomyb,
+ * energomzb).  NULL outputs are skipped.  Synchronises.                   */
+int ductgpu_dns_statistics_omg(ductgpu_dns dns, double *om2, double *hist, int *nhist);
 /* Body force f = (f1, f2, f3) (complex (my,my,nmodes) fields, host or
  * device; copied): it enters the substep's right-hand side like the
  * pressure gradient and the reference's forcings (src/main1.f90 (vi-b),

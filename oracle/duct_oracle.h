@@ -190,6 +190,10 @@ typedef struct {
     double stress4[4];  /* wallstressx of the step's u                      */
     double energy[3], energy2[3];   /* energy_fou of u, v, w               */
     int nstat;
+    /* vorticity diagnostics (src/main1.f90:453-466); om2 NULL: not gathered */
+    double *om2;        /* 3 my mz: omx2, omy2, omz2 (statistics_omg2_fou)   */
+    double omg[16];     /* the step's energomx4[5], energomxb4[5], energy_fou
+                           of om_x, om_y, om_z, the same with mode 0         */
 } orc_dns_stats;
 
 void orc_fourx(double *fou, double *phys, int mx1, int mgalx, int my, int nz, int iopt);
@@ -200,6 +204,11 @@ void orc_chz2x(double *f, int my, int mz, int M);
 void orc_advection3d(const double *u, const double *v, const double *w, double *adv1, double *adv2,
                      double *adv3, int my, int mz, int M, int mgalx, const double *xalp, double aspect,
                      double *stats2);
+void orc_vorticity(double *u, double *v, double *w, double *vort, double *tmp, int my, int mz, int M,
+                   const double *xalp, double aspect, int iflag);
+void orc_statistics_omg2_fou(const double *fou, int my, int mz, int M, double *om2);
+void orc_energy_fou_zero_sector(const double *u, int my, int mz, double aspect, double energy[5]);
+void orc_integral_abs_zero_sector(const double *u, int my, int mz, double aspect, double energy[5]);
 void orc_laplacian3d(double *u, double *flap, int my, int mz, int M, const double *xalp, double aspect,
                      double scal, char what);
 void orc_grad3d(double *u, double *dxu, double *dyu, double *dzu, int my, int mz, int M, const double *xalp,

@@ -381,6 +381,94 @@ void orc_energy_fou(const double *u, int my, int mz, int M, double aspect, doubl
     free(y); free(z); free(dy); free(dz);
 }
 
+/* vorticity(u,v,w,vort,tmp,iflag), src/operators.F:810-905: om_x = w,y -
+ * v,z (1), om_y = u,z - w,x (2), om_z = v,x - u,y (3), with the reference's
+ * transyz / derivyz / transyz sequence (u, v, w go through its in-place
+ * round trips, so they come back to rounding, as there). */
+void orc_vorticity(double *u, double *v, double *w, double *vort, double *tmp, int my, int mz, int M,
+                   const double *xalp, double aspect, int iflag)
+{
+    const long n = 2L * my * mz * M;
+    if (iflag == 1) {
+        dphys(w, vort, my, mz, M, 'y', 1, 1.0, aspect, 1);
+        dphys(v, tmp, my, mz, M, 'z', 1, 1.0, aspect, 1);
+    } else if (iflag == 2) {
+        dphys(u, vort, my, mz, M, 'z', 1, 1.0, aspect, 1);
+        orc_derivx(w, tmp, my, mz, M, xalp, 1, 1.0, 'n');
+    } else {
+        orc_derivx(v, vort, my, mz, M, xalp, 1, 1.0, 'n');
+        dphys(u, tmp, my, mz, M, 'y', 1, 1.0, aspect, 1);
+    }
+    daxpy_(n, -1.0, tmp, vort);
+}
+
+/* statistics_omg2_fou(fou,iflag), src/operators.F:1859-1955 (one rank):
+ * om2[my mz] += |fou_0|^2 + sum_{i>=1} 2 |fou_i|^2 (mode 0 first, as there). */
+void orc_statistics_omg2_fou(const double *fou, int my, int mz, int M, double *om2)
+{
+    const long pl = (long)my * mz;
+    for (long q = 0; q < pl; ++q) om2[q] = om2[q] + (CPLX(fou, q) * CPLX(fou, q) + CPLXI(fou, q) * CPLXI(fou, q));
+    for (int i = 1; i < M; ++i)
+        for (long q = 0; q < pl; ++q) {
+            const size_t e = (size_t)i * pl + q;
+            om2[q] = om2[q] + (CPLX(fou, e) * CPLX(fou, e) + CPLXI(fou, e) * CPLXI(fou, e)) * 2.0;
+        }
+}
+
+/* The sector of point (j, k), 1-based, of energy_fou_zero_sector and
+ * integral_abs_zero_sector (0-based sector index; 4 = on a diagonal). */
+static int zero_sector(int j, int k, int mz)
+{
+    if (j < k && j < mz + 1 - k) return 0;
+    if (j < k && j > mz + 1 - k) return 1;
+    if (j > k && j > mz + 1 - k) return 2;
+    if (j > k && j < mz + 1 - k) return 3;
+    return 4;
+}
+
+/* energy_fou_zero_sector(u,energy), src/operators.F:1018-1099 (one rank):
+ * energy[s] = sum over sector s of |u_0|^2 dy dz / area. */
+void orc_energy_fou_zero_sector(const double *u, int my, int mz, double aspect, double energy[5])
+{
+    double *y = (double *)malloc(sizeof(double) * my), *z = (double *)malloc(sizeof(double) * mz);
+    double *dy = (double *)malloc(sizeof(double) * my), *dz = (double *)malloc(sizeof(double) * mz);
+    cgl_nodes(my, 1.0, y);
+    cgl_nodes(mz, aspect, z);
+    mesh_weights(y, my, dy);
+    mesh_weights(z, mz, dz);
+    for (int s = 0; s < 5; ++s) energy[s] = 0.0;
+    for (int k = 1; k <= mz; ++k)
+        for (int j = 1; j <= my; ++j) {
+            const size_t q = (size_t)(j - 1) + (size_t)my * (k - 1);
+            const double ue = CPLX(u, q) * CPLX(u, q) + CPLXI(u, q) * CPLXI(u, q);
+            const int s = zero_sector(j, k, mz);
+            energy[s] = energy[s] + ue * dy[j - 1] * dz[k - 1];
+        }
+    for (int s = 0; s < 5; ++s) energy[s] = energy[s] / (4.0 * aspect);
+    free(y); free(z); free(dy); free(dz);
+}
+
+/* integral_abs_zero_sector(u,energy), src/operators.F:1462-1541 (one rank):
+ * energy[s] = sum over sector s of |Re u_0| dy dz / area. */
+void orc_integral_abs_zero_sector(const double *u, int my, int mz, double aspect, double energy[5])
+{
+    double *y = (double *)malloc(sizeof(double) * my), *z = (double *)malloc(sizeof(double) * mz);
+    double *dy = (double *)malloc(sizeof(double) * my), *dz = (double *)malloc(sizeof(double) * mz);
+    cgl_nodes(my, 1.0, y);
+    cgl_nodes(mz, aspect, z);
+    mesh_weights(y, my, dy);
+    mesh_weights(z, mz, dz);
+    for (int s = 0; s < 5; ++s) energy[s] = 0.0;
+    for (int k = 1; k <= mz; ++k)
+        for (int j = 1; j <= my; ++j) {
+            const size_t q = (size_t)(j - 1) + (size_t)my * (k - 1);
+            const int s = zero_sector(j, k, mz);
+            energy[s] = energy[s] + fabs(CPLX(u, q)) * dy[j - 1] * dz[k - 1];
+        }
+    for (int s = 0; s < 5; ++s) energy[s] = energy[s] / (4.0 * aspect);
+    free(y); free(z); free(dy); free(dz);
+}
+
 /* statistics_fou(u,v,w,p,1), src/operators.F:1608-1765 (one rank):
  * mean[4 my mz] += mode-0 real parts of u, v, w, p; ppb[my mz] += the
  * x-mean of p^2 (|p_0|^2 + sum 2|p_i|^2); spec[4][7][M] += the streamwise
@@ -456,6 +544,23 @@ double orc_dns_substep(double *u, double *v, double *w, double *p, double *adv1,
         orc_energy_fou(u, my, mz, M, aspect, &stats->energy[0], &stats->energy2[0]);
         orc_energy_fou(v, my, mz, M, aspect, &stats->energy[1], &stats->energy2[1]);
         orc_energy_fou(w, my, mz, M, aspect, &stats->energy[2], &stats->energy2[2]);
+        if (stats->om2) {
+            /* src/main1.f90:453-466: each vorticity component, its second
+             * moments and energies; the zero-mode sectors of om_x */
+            double *vort = (double *)malloc(sizeof(double) * nf), *tmp = (double *)malloc(sizeof(double) * nf);
+            const size_t pl = (size_t)my * mz;
+            for (int c = 0; c < 3; ++c) {
+                orc_vorticity(u, v, w, vort, tmp, my, mz, M, xalp, aspect, c + 1);
+                orc_statistics_omg2_fou(vort, my, mz, M, stats->om2 + c * pl);
+                orc_energy_fou(vort, my, mz, M, aspect, &stats->omg[10 + c], &stats->omg[13 + c]);
+                if (c == 0) {
+                    orc_energy_fou_zero_sector(vort, my, mz, aspect, stats->omg);
+                    orc_integral_abs_zero_sector(vort, my, mz, aspect, stats->omg + 5);
+                }
+            }
+            free(vort);
+            free(tmp);
+        }
         orc_statistics_fou(u, v, w, p, my, mz, M, stats->mean, stats->ppb, stats->spec);
         stats->nstat += 1;
     }

@@ -352,7 +352,7 @@ _ = os
 class _DnsStats(C.Structure):
     _fields_ = [(n, C.POINTER(C.c_double)) for n in ("mean", "prod", "ppb", "spec")] + [
         ("stress4", C.c_double * 4), ("energy", C.c_double * 3), ("energy2", C.c_double * 3),
-        ("nstat", C.c_int)]
+        ("nstat", C.c_int), ("om2", C.POINTER(C.c_double)), ("omg", C.c_double * 16)]
 
 
 def _dns_sigs(L):
@@ -361,6 +361,7 @@ def _dns_sigs(L):
     L.orc_derivx.argtypes = [P, P, I, I, I, P, I, D, C.c_char]
     L.orc_advection3d.argtypes = [P, P, P, P, P, P, I, I, I, I, P, D, P]
     L.orc_laplacian3d.argtypes = [P, P, I, I, I, P, D, D, C.c_char]
+    L.orc_vorticity.argtypes = [P, P, P, P, P, I, I, I, P, D, I]
     L.orc_grad3d.argtypes = [P, P, P, P, I, I, I, P, D, D, C.c_char]
     L.orc_div3d.argtypes = [P, P, P, P, I, I, I, P, D, D]
     L.orc_update_uvwp.argtypes = [P, P, P, P, P, P, I, I, I, P, D, D, D, D, D]
@@ -429,6 +430,18 @@ def advection3d(u, v, w, mgalx, xalp, aspect=1.0, stats=False):
     if stats:
         return a1, a2, a3, np.moveaxis(st, 2, 0)
     return a1, a2, a3
+
+
+def vorticity(u, v, w, xalp, iflag, aspect=1.0):
+    """vorticity (src/operators.F:810-905), component iflag (1, 2, 3); the
+    inputs are copied (the reference's round trips change them in place)."""
+    L = _dlib()
+    u, v, w = (np.array(_cf(f), order="F") for f in (u, v, w))
+    my, mz, M = u.shape
+    vort, tmp = np.zeros_like(u, order="F"), np.zeros_like(u, order="F")
+    L.orc_vorticity(_p(u), _p(v), _p(w), _p(vort), _p(tmp), my, mz, M,
+                    _p(np.ascontiguousarray(xalp, dtype=np.float64)), float(aspect), int(iflag))
+    return vort
 
 
 def laplacian3d(u, xalp, scal, what="n", flap=None, aspect=1.0):
@@ -531,6 +544,8 @@ class Dns:
         self._st.prod = self.stats_prod.ctypes.data_as(C.POINTER(C.c_double))
         self._st.ppb = self.stats_ppb.ctypes.data_as(C.POINTER(C.c_double))
         self._st.spec = self.stats_spec.ctypes.data_as(C.POINTER(C.c_double))
+        self.stats_om2 = np.zeros((my, mz, 3), order="F")
+        self._st.om2 = self.stats_om2.ctypes.data_as(C.POINTER(C.c_double))
         self.history = []
         self.divmax = None
         self.force = None
@@ -549,13 +564,19 @@ class Dns:
             self.nthreads, None if self.force is None else _p(self.force))
         if stats and krk == 1:
             self.history.append(dict(stress4=list(self._st.stress4), energy=list(self._st.energy),
-                                     energy2=list(self._st.energy2)))
+                                     energy2=list(self._st.energy2), omg=list(self._st.omg)))
         return self.divmax
 
     def step(self, stats=False):
         for krk in (1, 2, 3):
             self.substep(krk, stats=stats)
         return self.divmax
+
+    def statistics_omg(self):
+        """The vorticity diagnostics (src/main1.f90:453-466): om2 (3,my,mz)
+        summed over the recorded steps, hist (nstep,16) one row per step."""
+        return dict(om2=np.moveaxis(self.stats_om2, 2, 0).copy(),
+                    hist=np.array([h["omg"] for h in self.history]).reshape(-1, 16))
 
     def statistics(self):
         """Accumulated statistics, each summed over the recorded steps:

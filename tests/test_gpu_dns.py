@@ -98,6 +98,11 @@ def test_line_operators_match_oracle(ctx, oracle, my, mz, aspect, kernel):
     ref = oracle.derivx(u, xalp, 2, scal=0.3)
     ctx.derivx_dev(du, out[0], xalp, 2, 0.3, "n")
     assert rel(out[0].download(), ref) < 1e-14
+    # vorticity, the three components
+    for c in (1, 2, 3):
+        ref = oracle.vorticity(u, v, w, xalp, c, aspect=aspect)
+        ctx.vorticity_dev(du, dv, dw, out[c - 1], xalp, c, aspect=aspect)
+        assert rel(out[c - 1].download(), ref) < tol, c
     for a in (du, dv, dw, dp, *out):
         a.free()
     ctx.set_line_kernel(1)
@@ -251,6 +256,12 @@ def test_dns_steps_match_oracle(oracle, cmassflow):
             assert np.abs(st["hist"] - hist).max() < 1e-10 * np.abs(hist).max()
             assert st["divmax"][2] == pytest.approx(orc.divmax, rel=1e-6, abs=1e-13)
             assert st["divmax"].max() < 1e-11
+            # the vorticity diagnostics of the recorded steps
+            om, oref = gpu.statistics_omg(), orc.statistics_omg()
+            assert rel(om["om2"], oref["om2"]) < 1e-10
+            assert om["hist"].shape == oref["hist"].shape == (3, 16)
+            assert np.abs(om["hist"] - oref["hist"]).max() < 1e-10 * np.abs(oref["hist"]).max()
+            assert np.all(oref["hist"][:, 10:] > 0)
 
 
 def test_dns_graph_replay_equals_direct_launches(oracle):

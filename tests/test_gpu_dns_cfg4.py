@@ -8,8 +8,9 @@ oracle's (LAPACK-order) point.
 
 Tolerances: u, v, w 1e-12 relative (measured 2e-14 after two steps); p
 1e-10 (measured 2.9e-11: the Neumann solve's conditioning, as in
-test_gpu_dns.py); the statistics (means, products, x-mean of p^2, spectra)
-and the wall-stress / energy history 1e-10, the north star's bar for the
+test_gpu_dns.py); the statistics (means, products, x-mean of p^2, spectra),
+the wall-stress / energy history and the vorticity diagnostics (second
+moments, enstrophies, zero-mode sectors) 1e-10, the north star's bar for the
 flow statistics (measured at most 1.4e-11 and 3.9e-11).
 """
 import os
@@ -39,6 +40,7 @@ def test_cfg4_step_matches_oracle(oracle):
     orc = oracle.Dns(u, v, w, p, mg, alp, fnu, dt, cmassflow=True, nthreads=os.cpu_count() or 1)
     orc.step(stats=True)
     ref = orc.statistics()
+    oref = orc.statistics_omg()
     hist = np.array([h["stress4"] + h["energy"] + h["energy2"] for h in orc.history])
     with D.Context(0) as ctx:
         ctx.pseudomat(m)
@@ -48,12 +50,16 @@ def test_cfg4_step_matches_oracle(oracle):
             d.steps(1, stats_every=1)
             got = d.fields()
             st = d.statistics()
+            om = d.statistics_omg()
     for g, r in zip(got[:3], (orc.u, orc.v, orc.w)):
         assert rel(g, r) < 1e-12
     assert rel(got[3], orc.p) < 1e-10
     for k in ("mean", "prod", "ppb", "spec"):
         assert rel(st[k], ref[k]) < 1e-10, k
     assert rel(st["hist"], hist) < 1e-10
+    # the vorticity diagnostics of the step (src/main1.f90:453-466)
+    assert rel(om["om2"], oref["om2"]) < 1e-10
+    assert rel(om["hist"], oref["hist"]) < 1e-10
     # max |div u| over the interior after each substep: the first starts from
     # the seeded state (measured 2.4e-12), the projection then keeps it at
     # rounding (4e-16..5e-16 after the second and third)
