@@ -48,7 +48,7 @@ EXPORTS = [
     "ductgpu_dns_wallstress_after", "ductgpu_dns_grad_wallstress", "ductgpu_set_rect_fold",
     "ductgpu_set_line_kernel", "ductgpu_uvwp_filename", "ductgpu_save_4fields_fou_hdf5_dev",
     "ductgpu_read_hdf5_header", "ductgpu_read_4fields_fou_hdf5_dev", "ductgpu_dns_save_hdf5",
-    "ductgpu_dns_load_hdf5", "ductgpu_vorticity_dev", "ductgpu_dns_statistics_omg",
+    "ductgpu_dns_load_hdf5", "ductgpu_vorticity_dev", "ductgpu_dns_statistics_omg", "ductgpu_dns_cfl",
 ]
 SETUP_NO_EIGEN = 1
 (K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER, K_LINES,
@@ -194,6 +194,7 @@ def lib():
             "ductgpu_dns_load_hdf5": [P, C.c_char_p, C.POINTER(D)],
             "ductgpu_vorticity_dev": [P, P, P, P, P, I, I, I, P, D, I],
             "ductgpu_dns_statistics_omg": [P, P, P, C.POINTER(I)],
+            "ductgpu_dns_cfl": [P, C.POINTER(D), C.POINTER(D), C.POINTER(D)],
             "transpose_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
                                C.POINTER(C.c_size_t)],
             "mat_invdiag_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
@@ -812,6 +813,12 @@ class Dns:
         J = C.c_double()
         self.ctx._check(lib().ductgpu_dns_grad_wallstress(self.h, C.byref(J), g.ctypes.data_as(C.c_void_p)))
         return J.value, np.stack([np.asfortranarray(np.transpose(g[c], (2, 1, 0))) for c in range(3)])
+
+    def cfl(self):
+        """dict(cfl, slip, cfl_max) of ductgpu_dns_cfl (cfl_max is reset)."""
+        c, s, m = C.c_double(), C.c_double(), C.c_double()
+        self.ctx._check(lib().ductgpu_dns_cfl(self.h, C.byref(c), C.byref(s), C.byref(m)))
+        return dict(cfl=c.value, slip=s.value, cfl_max=m.value)
 
     def statistics_omg(self):
         """dict(om2 (3,my,my): omx2, omy2, omz2; hist (nhist,16): sector

@@ -58,7 +58,31 @@ struct AdvParams {
     const double *xalp;    // device [M]
     long long P;           // points of a plane (my mz)
     int M;                 // Fourier modes kept (mx1 + 1)
+    // determine_step / slip_velocity_3d (src/operators.F:608-672, 2552-2608)
+    // on the physical velocities, or null: atomic maxima (order_key) of
+    // max(|u| hx, |v|/dy, |w|/dz) into cfl[0] and cfl[2], of the velocity
+    // components on the walls into cfl[1]
+    unsigned long long *cfl;
+    const double *rdyz;    // [my + mz]: 1/dy, 1/dz
+    double hx;             // alp mgalx / (2 pi)
+    int my, mz;
 };
+
+// A monotone map of doubles to unsigned integers (x < y <=> key(x) <
+// key(y)), so that an integer atomic max keeps the largest double; key 0
+// lies below every number.
+__device__ __forceinline__ unsigned long long order_key(double x)
+{
+    const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+static double order_key_value(unsigned long long k)
+{
+    const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    double x;
+    memcpy(&x, &b, sizeof x);
+    return x;
+}
 
 // Step 2 of a four-step FFT over the CTA's points: thread (c, g) reads row
 // c of point g from wk and returns X[c + R k2] in v.
@@ -128,6 +152,20 @@ __global__ void __launch_bounds__(R * TQ, MINB) k_advx(const __grid_constant__ A
         uu[k2] = a[k2].x;
         vv[k2] = -a[k2].y;
     }
+    // the time-step and slip checks of the step's first substep
+    double eig = 0.0, slip = -1.0e308, rdz = 0.0;
+    bool wall = false;
+    if (p.cfl && valid) {
+        const int j = (int)(q % p.my), kz = (int)(q / p.my);
+        const double rdy = p.rdyz[j];
+        rdz = p.rdyz[p.my + kz];
+        wall = j == 0 || j == p.my - 1 || kz == 0 || kz == p.mz - 1;
+#pragma unroll
+        for (int k2 = 0; k2 < R; ++k2) {
+            eig = fmax(eig, fmax(fabs(uu[k2]) * p.hx, fabs(vv[k2]) * rdy));
+            if (wall) slip = fmax(slip, fmax(uu[k2], vv[k2]));
+        }
+    }
     __syncthreads();
 #pragma unroll
     for (int n1 = 0; n1 < R; ++n1) {
@@ -147,6 +185,25 @@ __global__ void __launch_bounds__(R * TQ, MINB) k_advx(const __grid_constant__ A
     fft_step2<R, TQ>(wk, a, tw, c, g);
 #pragma unroll
     for (int k2 = 0; k2 < R; ++k2) ww[k2] = a[k2].x;
+    if (p.cfl) {
+        if (valid) {
+#pragma unroll
+            for (int k2 = 0; k2 < R; ++k2) {
+                eig = fmax(eig, fabs(ww[k2]) * rdz);
+                if (wall) slip = fmax(slip, ww[k2]);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            eig = fmax(eig, __shfl_xor_sync(0xffffffffu, eig, o));
+            slip = fmax(slip, __shfl_xor_sync(0xffffffffu, slip, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMax(p.cfl, order_key(eig));
+            atomicMax(p.cfl + 1, order_key(slip));
+            atomicMax(p.cfl + 2, order_key(eig));
+        }
+    }
 
     const double sc = 1.0 / N;
     for (int pair = 0; pair < 3; ++pair) {
@@ -592,7 +649,7 @@ static int aux_get(ductgpu_ctx ctx, DnsAux **out)
 // The wavenumbers to the device (stream-ordered after earlier launches).
 static int upload_xalp(ductgpu_ctx ctx, const double *xalp, int nmodes, const double **dev)
 {
-    DnsAux *a;
+    DnsAux *a = nullptr;
     int rc = aux_get(ctx, &a);
     if (rc) return rc;
     if (!xalp) return set_error(ctx, DUCTGPU_EARG, "xalp is null");
@@ -624,7 +681,7 @@ static int make_weights(int my, int mz, double aspect, std::vector<double> &wcc,
 
 static int aux_weights(ductgpu_ctx ctx, int my, int mz, double aspect, DnsAux **out)
 {
-    DnsAux *a;
+    DnsAux *a = nullptr;
     int rc = aux_get(ctx, &a);
     if (rc) return rc;
     if (a->w_my != my || a->w_mz != mz || a->w_aspect != aspect) {
@@ -878,7 +935,8 @@ namespace duct {
 // derivatives of the off-diagonal and diagonal products (two line launches).
 static int advection_issue(ductgpu_ctx ctx, const double *u, const double *v, const double *w, double *a1, double *a2,
                            double *a3, double *const prod[5], int my, int mz, int M, int mgalx, const double *xd,
-                           double aspect, double *stats2, int real0 = 0)
+                           double aspect, double *stats2, int real0 = 0, unsigned long long *cfl = nullptr,
+                           const double *rdyz = nullptr, double hx = 0.0)
 {
     AdvParams ap{};
     ap.u = reinterpret_cast<const double2 *>(u);
@@ -896,6 +954,11 @@ static int advection_issue(ductgpu_ctx ctx, const double *u, const double *v, co
     ap.xalp = xd;
     ap.P = (long long)my * mz;
     ap.M = M;
+    ap.cfl = cfl;
+    ap.rdyz = rdyz;
+    ap.hx = hx;
+    ap.my = my;
+    ap.mz = mz;
     int rc = advx_launch(ctx, ap, mgalx);
     if (rc) return rc;
     // adv1 += d(uv)/dy + d(uw)/dz; adv2 += d(vv)/dy + d(vw)/dz; adv3 += d(vw)/dy + d(ww)/dz
@@ -942,7 +1005,7 @@ extern "C" int ductgpu_max_3din_dev(ductgpu_ctx ctx, const double *u, int my, in
     if (rc) return rc;
     if (!divmax) return set_error(ctx, DUCTGPU_EARG, "max_3din: null output");
     cudaSetDevice(ctx->device);
-    DnsAux *a;
+    DnsAux *a = nullptr;
     if ((rc = aux_get(ctx, &a))) return rc;
     DUCT_CUDA(ctx, cudaMemsetAsync(a->out + kStatVals, 0, sizeof(double), ctx->stream));
     {
@@ -1022,7 +1085,7 @@ extern "C" int ductgpu_wallstressx_dev(ductgpu_ctx ctx, const double *u, int my,
     if (rc) return rc;
     if (!stress4) return set_error(ctx, DUCTGPU_EARG, "wallstressx: null output");
     cudaSetDevice(ctx->device);
-    DnsAux *a;
+    DnsAux *a = nullptr;
     if ((rc = aux_weights(ctx, my, mz, aspect, &a))) return rc;
     const double *f[4] = {u, nullptr, nullptr, nullptr};
     if ((rc = stats_issue(ctx, f, 1, a->wcc, a->wst, nullptr, nullptr, a->partial, a->out, nullptr, 0,
@@ -1041,7 +1104,7 @@ extern "C" int ductgpu_energy_fou_dev(ductgpu_ctx ctx, const double *u, int my, 
     if (rc) return rc;
     if (!energy || !energy2) return set_error(ctx, DUCTGPU_EARG, "energy_fou: null output");
     cudaSetDevice(ctx->device);
-    DnsAux *a;
+    DnsAux *a = nullptr;
     if ((rc = aux_weights(ctx, my, mz, aspect, &a))) return rc;
     const double *f[4] = {u, nullptr, nullptr, nullptr};
     if ((rc = stats_issue(ctx, f, 1, a->wcc, nullptr, nullptr, nullptr, a->partial, a->out, nullptr, 0,
@@ -1067,7 +1130,7 @@ extern "C" int ductgpu_statistics_fou_dev(ductgpu_ctx ctx, const double *u, cons
     if (my < 16 || mz < 16)
         return set_error(ctx, DUCTGPU_EARG, "statistics_fou: my=%d mz=%d (the spectra points need 16 or more)", my, mz);
     cudaSetDevice(ctx->device);
-    DnsAux *a;
+    DnsAux *a = nullptr;
     if ((rc = aux_weights(ctx, my, mz, 1.0, &a))) return rc;
     const double *f[4] = {u, v, w, p};
     if ((rc = stats_issue(ctx, f, 3, a->wcc, nullptr, mean, ppb, a->partial, a->out, nullptr, 0, (long long)my * mz,
@@ -1121,6 +1184,11 @@ struct ductgpu_dns_s {
     int hist_cap = 0;
     int nstat = 0;
     double *divmax = nullptr;    // [3], one per substep
+    // time-step and slip checks of every step's first substep (order keys):
+    // [0] max(|u| hx, |v|/dy, |w|/dz) of the last step, [1] the largest wall
+    // velocity of the last step, [2] [0]'s maximum since the last read
+    unsigned long long *cfl = nullptr;
+    double *rdyz = nullptr;      // [2 my]: 1/dy, 1/dz
     // body force (src/main1.f90 (vi-b): forcings enter h like -grad p, h += (a + b) f)
     double *force = nullptr;     // 3 fields, owned
     bool forced = false;
@@ -1195,7 +1263,7 @@ static int dns_issue(ductgpu_dns d, int krk, bool stats)
     double **an = d->adv[krk % 2], **ao = d->adv[(krk - 1) % 2];
     double *u = d->vel[0], *v = d->vel[1], *w = d->vel[2], *p = d->p;
     const double *xd = d->xalp;
-    int rc;
+    int rc = DUCTGPU_OK;
     // (ii) adv(u^{k-1}); statistics_fou2 of the products with the statistics.
     // The statistics kernels only read u, v, w, p: on the side stream,
     // concurrent with the advection
@@ -1217,9 +1285,12 @@ static int dns_issue(ductgpu_dns d, int krk, bool stats)
         if (!rc) rc = check_cuda(ctx, cudaGetLastError(), "k_spectra");
         ctx->stream = mainst;
     }
+    if (!rc && krk == 1) rc = check_cuda(ctx, cudaMemsetAsync(d->cfl, 0, 2 * sizeof(unsigned long long), mainst),
+                                          "dns: cfl reset");
     if (!rc)
         rc = advection_issue(ctx, u, v, w, an[0], an[1], an[2], d->prod, my, my, M, d->mgalx, xd, asp,
-                             stats ? d->st_prod : nullptr, 1);
+                             stats ? d->st_prod : nullptr, 1, krk == 1 ? d->cfl : nullptr, d->rdyz,
+                             d->alp * d->mgalx / (2.0 * kPi));
     if (fork_stats) {
         const int rj = side_join(ctx, mainst);
         if (!rc) rc = rj;
@@ -1385,6 +1456,8 @@ static void dns_free(ductgpu_dns d)
     cudaFree(d->hist_om);
     cudaFree(d->hist_n);
     cudaFree(d->divmax);
+    cudaFree(d->cfl);
+    cudaFree(d->rdyz);
     cudaFree(d->force);
     cudaFree(d->dmat);
     cudaFree(d->adj);
@@ -1491,8 +1564,23 @@ extern "C" int ductgpu_dns_create(ductgpu_ctx ctx, int mgalx, double alp, double
     if (cudaMalloc(&d->hist, sizeof(double) * kStatVals * (hist_cap > 0 ? hist_cap : 1)) != cudaSuccess ||
         cudaMalloc(&d->hist_om, sizeof(double) * kOmgVals * (hist_cap > 0 ? hist_cap : 1)) != cudaSuccess ||
         cudaMalloc(&d->hist_n, sizeof(int)) != cudaSuccess || cudaMemset(d->hist_n, 0, sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&d->divmax, sizeof(double) * 3) != cudaSuccess)
+        cudaMalloc(&d->divmax, sizeof(double) * 3) != cudaSuccess ||
+        cudaMalloc(&d->cfl, sizeof(unsigned long long) * 3) != cudaSuccess ||
+        cudaMemset(d->cfl, 0, sizeof(unsigned long long) * 3) != cudaSuccess)
         return fail(check_cuda(ctx, cudaGetLastError(), "dns: history"));
+    {
+        // 1/dy, 1/dz of determine_step (the mesh sizes of src/ininewc.f90:102-112)
+        std::vector<double> dy, dz, r(2 * (size_t)my);
+        mesh_sizes(my, 1.0, dy);
+        mesh_sizes(my, aspect, dz);
+        for (int j = 0; j < my; ++j) {
+            r[j] = 1.0 / dy[j];
+            r[my + j] = 1.0 / dz[j];
+        }
+        if (cudaMalloc(&d->rdyz, sizeof(double) * r.size()) != cudaSuccess ||
+            cudaMemcpy(d->rdyz, r.data(), sizeof(double) * r.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(check_cuda(ctx, cudaGetLastError(), "dns: mesh sizes"));
+    }
     // the flow-rate forcing of CMASSFLOW: premassfu / premassf with alphak = beta_k
     if (d->cmassflow && (rc = ductgpu_precomp_mass_flow(ctx, dt, kBkk, 3, fnu, aspect, nullptr, nullptr)))
         return fail(rc);
@@ -1708,6 +1796,22 @@ extern "C" int ductgpu_dns_statistics(ductgpu_dns d, double *mean, double *prod,
     if (nstat) *nstat = d->nstat;
     if (nhist) *nhist = nh;
     if (divmax3) DUCT_CUDA(ctx, cudaMemcpy(divmax3, d->divmax, sizeof(double) * 3, cudaMemcpyDeviceToHost));
+    return DUCTGPU_OK;
+}
+
+extern "C" int ductgpu_dns_cfl(ductgpu_dns d, double *cfl, double *slip, double *cfl_max)
+{
+    if (!d) return DUCTGPU_EARG;
+    ductgpu_ctx ctx = d->ctx;
+    cudaSetDevice(ctx->device);
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    unsigned long long k[3];
+    DUCT_CUDA(ctx, cudaMemcpy(k, d->cfl, sizeof k, cudaMemcpyDeviceToHost));
+    DUCT_CUDA(ctx, cudaMemset(d->cfl + 2, 0, sizeof(unsigned long long)));
+    // before any step the keys are 0: nothing measured
+    if (cfl) *cfl = k[0] ? d->dt * order_key_value(k[0]) : 0.0;
+    if (slip) *slip = k[1] ? order_key_value(k[1]) : 0.0;
+    if (cfl_max) *cfl_max = k[2] ? d->dt * order_key_value(k[2]) : 0.0;
     return DUCTGPU_OK;
 }
 

@@ -505,6 +505,16 @@ int ductgpu_dns_steps(ductgpu_dns dns, int nsteps, int stats_every);
  * after each substep of the last step.  Synchronises.                    */
 int ductgpu_dns_statistics(ductgpu_dns dns, double *mean, double *prod, double *ppb, double *spec,
                            double *hist, int *nstat, int *nhist, double *divmax3);
+/* The time-step and slip checks that advection3d makes at the first
+ * substep of every step (determine_step, src/operators.F:608-672, and
+ * slip_velocity_3d, 2552-2608), taken by the x-FFT kernel on the physical
+ * velocities: cfl = dt max(|u| alp mgalx/(2 pi), |v|/dy, |w|/dz) of the
+ * last step (the CFL number of the fixed step; the reference stops above
+ * 100, src/main1.f90:426-434), slip = the largest velocity component on
+ * the walls of the last step, cfl_max = the largest cfl since the previous
+ * call (reset by the call).  0 before the first step.  NULL outputs are
+ * skipped.  Synchronises.                                                  */
+int ductgpu_dns_cfl(ductgpu_dns dns, double *cfl, double *slip, double *cfl_max);
 /* The vorticity diagnostics of the recorded steps (src/main1.f90:453-466):
  * om2 (my,my,3) the accumulators omx2, omy2, omz2 of statistics_omg2_fou
  * (src/operators.F:1859-1955); hist rows of 16 doubles per recorded step,

@@ -194,6 +194,7 @@ typedef struct {
     double *om2;        /* 3 my mz: omx2, omy2, omz2 (statistics_omg2_fou)   */
     double omg[16];     /* the step's energomx4[5], energomxb4[5], energy_fou
                            of om_x, om_y, om_z, the same with mode 0         */
+    double cfl2[2];     /* the step's remx (determine_step), slipmx          */
 } orc_dns_stats;
 
 void orc_fourx(double *fou, double *phys, int mx1, int mgalx, int my, int nz, int iopt);
@@ -209,6 +210,9 @@ void orc_vorticity(double *u, double *v, double *w, double *vort, double *tmp, i
 void orc_statistics_omg2_fou(const double *fou, int my, int mz, int M, double *om2);
 void orc_energy_fou_zero_sector(const double *u, int my, int mz, double aspect, double energy[5]);
 void orc_integral_abs_zero_sector(const double *u, int my, int mz, double aspect, double energy[5]);
+void orc_advection3d_ex(const double *u, const double *v, const double *w, double *adv1, double *adv2,
+                        double *adv3, int my, int mz, int M, int mgalx, const double *xalp, double aspect,
+                        double *stats2, double *cfl2);
 void orc_laplacian3d(double *u, double *flap, int my, int mz, int M, const double *xalp, double aspect,
                      double scal, char what);
 void orc_grad3d(double *u, double *dxu, double *dyu, double *dzu, int my, int mz, int M, const double *xalp,

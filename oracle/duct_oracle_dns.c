@@ -147,8 +147,21 @@ static void dphys(double *x, double *out, int my, int mz, int M, char cdir, int 
  * fields.  stats2 (6 my mz, or NULL): statistics_fou2 (src/operators.F:
  * 1957-2004) of the six products, the x-mean (mode-0 real part) added to
  * uub, vvb, wwb, uvb, uwb, vwb.                                             */
+static void cfl_slip(const double *ufis, const double *vfis, const double *wfis, int my, int mz, int mgalx,
+                     double alp, double aspect, double *cfl2);
+
 void orc_advection3d(const double *u, const double *v, const double *w, double *adv1, double *adv2, double *adv3,
                      int my, int mz, int M, int mgalx, const double *xalp, double aspect, double *stats2)
+{
+    orc_advection3d_ex(u, v, w, adv1, adv2, adv3, my, mz, M, mgalx, xalp, aspect, stats2, NULL);
+}
+
+/* advection3d with, when cfl2 is not NULL, its first-substep checks on the
+ * physical velocities (src/operators.F:71-75): cfl2[0] = the remx of
+ * determine_step, cfl2[1] = the slipmx of slip_velocity_3d. */
+void orc_advection3d_ex(const double *u, const double *v, const double *w, double *adv1, double *adv2, double *adv3,
+                        int my, int mz, int M, int mgalx, const double *xalp, double aspect, double *stats2,
+                        double *cfl2)
 {
     const size_t nf = 2 * (size_t)my * mz * M;        /* doubles of a fou field */
     const size_t ns = (size_t)(mgalx + 2) * my * mz;   /* doubles of a fis field */
@@ -169,6 +182,7 @@ void orc_advection3d(const double *u, const double *v, const double *w, double *
     orc_fourx(adv1, ufis, M - 1, mgalx, my, mz, 1);
     orc_fourx(adv2, vfis, M - 1, mgalx, my, mz, 1);
     orc_fourx(adv3, wfis, M - 1, mgalx, my, mz, 1);
+    if (cfl2) cfl_slip(ufis, vfis, wfis, my, mz, mgalx, M > 1 ? xalp[1] : 0.0, aspect, cfl2);
 #define STAT2(f, s)                                                                  \
     if (stats2)                                                                      \
         for (long q = 0; q < pl; ++q) stats2[(size_t)(s) * pl + q] += (f)[2 * q];
@@ -348,6 +362,39 @@ static void cgl_nodes(int n, double s, double *x)
 {
     const double pi = 4.0 * atan(1.0);
     for (int j = 0; j < n; ++j) x[j] = -s * cos(pi * (double)j / (double)(n - 1));
+}
+
+/* determine_step (src/operators.F:608-672): remx = max over the physical
+ * points of |u| alp mgalx/(2 pi), |v|/dy, |w|/dz; slip_velocity_3d
+ * (2552-2608): the largest u, v or w on the y = +-1 and z = +-aspect walls.
+ * Physical fields (mgalx+2, my, mz), points i < mgalx. */
+static void cfl_slip(const double *ufis, const double *vfis, const double *wfis, int my, int mz, int mgalx,
+                     double alp, double aspect, double *cfl2)
+{
+    const double pi = 4.0 * atan(1.0);
+    double *y = (double *)malloc(sizeof(double) * my), *z = (double *)malloc(sizeof(double) * mz);
+    double *dy = (double *)malloc(sizeof(double) * my), *dz = (double *)malloc(sizeof(double) * mz);
+    cgl_nodes(my, 1.0, y);
+    cgl_nodes(mz, aspect, z);
+    mesh_weights(y, my, dy);
+    mesh_weights(z, mz, dz);
+    const double hxalp = alp * (double)mgalx / (2.0 * pi);
+    double reig = 0.0, fmx = -1.0e308;
+    for (int k = 0; k < mz; ++k)
+        for (int j = 0; j < my; ++j) {
+            const size_t o = (size_t)(mgalx + 2) * (j + (size_t)my * k);
+            const int wall = (j == 0 || j == my - 1 || k == 0 || k == mz - 1);
+            for (int i = 0; i < mgalx; ++i) {
+                const double uu = ufis[o + i], vv = vfis[o + i], ww = wfis[o + i];
+                reig = fmax(reig, fabs(uu * hxalp));
+                reig = fmax(reig, fabs(vv / dy[j]));
+                reig = fmax(reig, fabs(ww / dz[k]));
+                if (wall) fmx = fmax(fmx, fmax(uu, fmax(vv, ww)));
+            }
+        }
+    cfl2[0] = reig;
+    cfl2[1] = fmx;
+    free(y); free(z); free(dy); free(dz);
 }
 
 /* energy_fou(u,energy,energy2), src/operators.F:907-973 (one rank):
@@ -537,8 +584,8 @@ double orc_dns_substep(double *u, double *v, double *w, double *p, double *adv1,
         }
     }
     /* (ii) adv(u^{k-1}) */
-    orc_advection3d(u, v, w, adv1, adv2, adv3, my, mz, M, mgalx, xalp, aspect,
-                    (stats && krk == 1) ? stats->prod : NULL);
+    orc_advection3d_ex(u, v, w, adv1, adv2, adv3, my, mz, M, mgalx, xalp, aspect,
+                       (stats && krk == 1) ? stats->prod : NULL, (stats && krk == 1) ? stats->cfl2 : NULL);
     if (stats && krk == 1) {
         orc_wallstressx(u, my, mz, aspect, stats->stress4);
         orc_energy_fou(u, my, mz, M, aspect, &stats->energy[0], &stats->energy2[0]);

@@ -352,7 +352,8 @@ _ = os
 class _DnsStats(C.Structure):
     _fields_ = [(n, C.POINTER(C.c_double)) for n in ("mean", "prod", "ppb", "spec")] + [
         ("stress4", C.c_double * 4), ("energy", C.c_double * 3), ("energy2", C.c_double * 3),
-        ("nstat", C.c_int), ("om2", C.POINTER(C.c_double)), ("omg", C.c_double * 16)]
+        ("nstat", C.c_int), ("om2", C.POINTER(C.c_double)), ("omg", C.c_double * 16),
+        ("cfl2", C.c_double * 2)]
 
 
 def _dns_sigs(L):
@@ -564,7 +565,8 @@ class Dns:
             self.nthreads, None if self.force is None else _p(self.force))
         if stats and krk == 1:
             self.history.append(dict(stress4=list(self._st.stress4), energy=list(self._st.energy),
-                                     energy2=list(self._st.energy2), omg=list(self._st.omg)))
+                                     energy2=list(self._st.energy2), omg=list(self._st.omg),
+                                     remx=self._st.cfl2[0], slip=self._st.cfl2[1]))
         return self.divmax
 
     def step(self, stats=False):

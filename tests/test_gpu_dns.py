@@ -256,6 +256,14 @@ def test_dns_steps_match_oracle(oracle, cmassflow):
             assert np.abs(st["hist"] - hist).max() < 1e-10 * np.abs(hist).max()
             assert st["divmax"][2] == pytest.approx(orc.divmax, rel=1e-6, abs=1e-13)
             assert st["divmax"].max() < 1e-11
+            # the first substep's time-step and slip checks (determine_step,
+            # slip_velocity_3d) on the physical velocities of the last step
+            cf = gpu.cfl()
+            dt = 1.0e-3
+            assert cf["cfl"] == pytest.approx(dt * orc.history[-1]["remx"], rel=1e-12)
+            assert cf["cfl_max"] == pytest.approx(dt * max(h["remx"] for h in orc.history), rel=1e-12)
+            assert abs(cf["slip"] - orc.history[-1]["slip"]) < 1e-12
+            assert gpu.cfl()["cfl_max"] == 0.0      # reset by the read, no step since
             # the vorticity diagnostics of the recorded steps
             om, oref = gpu.statistics_omg(), orc.statistics_omg()
             assert rel(om["om2"], oref["om2"]) < 1e-10
