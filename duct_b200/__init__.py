@@ -777,8 +777,9 @@ class Dns:
     def set_graphs(self, on):
         self.ctx._check(lib().ductgpu_dns_set_graphs(self.h, int(bool(on))))
 
-    def save_hdf5(self, filename, time=0.0, cfl=0.0, slip=0.0):
-        """The state as a uvwp_NNNN.h5 file (ductgpu_dns_save_hdf5)."""
+    def save_hdf5(self, filename, time=0.0, cfl=0.0, slip=float("nan")):
+        """The state as a uvwp_NNNN.h5 file (ductgpu_dns_save_hdf5); slip
+        NaN writes the wall slip measured at the last step."""
         self.ctx._check(lib().ductgpu_dns_save_hdf5(self.h, os.fsencode(filename), float(time), float(cfl),
                                                     float(slip)))
 

@@ -1663,9 +1663,13 @@ extern "C" int ductgpu_dns_save_hdf5(ductgpu_dns d, const char *filename, double
     h.cmassflow = d->cmassflow ? d->csum : 0.0;
     h.slip = slip;
     double dv[3];
+    unsigned long long key[2];
     DUCT_CUDA(ctx, cudaMemcpyAsync(dv, d->divmax, sizeof dv, cudaMemcpyDeviceToHost, ctx->stream));
+    DUCT_CUDA(ctx, cudaMemcpyAsync(key, d->cfl, sizeof key, cudaMemcpyDeviceToHost, ctx->stream));
     DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     h.divergence = dv[2];
+    // slip NaN: the wall slip slip_velocity_3d measured at the last step
+    if (slip != slip) h.slip = key[1] ? order_key_value(key[1]) : 0.0;
     return ductgpu_save_4fields_fou_hdf5_dev(ctx, filename, d->vel[0], d->vel[1], d->vel[2], d->p, &h);
 }
 

@@ -591,7 +591,8 @@ int ductgpu_read_4fields_fou_hdf5_dev(ductgpu_ctx ctx, const char *filename, dou
  * every nimag steps; irestart reads it back at start-up).  save: header
  * from the stepper (mgalx, my = mz, mx1 = modes - 1, alp, aspect, fnu,
  * dtfixed = dt, cmassflow = the held flow rate, DIVERGENCE = the last
- * substep's max_3din) plus the caller's time, cfl and slip.  load: the
+ * substep's max_3din) plus the caller's time, cfl and slip (NaN: the wall
+ * slip measured at the last step, as the reference saves).  load: the
  * fields as ductgpu_dns_set_fields takes them, the file's time to *time
  * (may be NULL); with cmassflow the file's cmassflow is the flow rate held
  * (that of the loaded u when the file's is 0), so a restart repeats the

@@ -134,9 +134,10 @@ def test_dns_save_and_restart_repeat_the_run(ctx, tmp_path):
     with D.Dns(ctx, mgalx, alp, fnu, dt, cmassflow=True) as dns:
         dns.set_fields(u, v, w, p)
         dns.steps(2)
-        dns.save_hdf5(path, time=2 * dt, cfl=0.25, slip=0.0)
+        dns.save_hdf5(path, time=2 * dt, cfl=0.25)
         saved = dns.fields()
         divmax = dns.statistics()["divmax"]
+        slip = dns.cfl()["slip"]
         dns.steps(2)
         after = dns.fields()
     ds = H.read(open(path, "rb").read())
@@ -146,6 +147,7 @@ def test_dns_save_and_restart_repeat_the_run(ctx, tmp_path):
     assert (h["mgalx"], h["my"], h["mz"], h["mx1"]) == (mgalx, m, m, saved[0].shape[2] - 1)
     assert h["dtfixed"] == dt and h["time"] == 2 * dt and h["cfl"] == 0.25 and h["alp"] == alp
     assert h["divergence"] == divmax[2]
+    assert h["slip"] == slip            # the measured wall slip of the last step
     # the restart holds the file's cmassflow, the run's own flow rate: the
     # run repeats bit for bit
     with D.Dns(ctx, mgalx, alp, fnu, dt, cmassflow=True) as dns:
