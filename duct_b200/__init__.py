@@ -49,6 +49,7 @@ EXPORTS = [
     "ductgpu_set_line_kernel", "ductgpu_uvwp_filename", "ductgpu_save_4fields_fou_hdf5_dev",
     "ductgpu_read_hdf5_header", "ductgpu_read_4fields_fou_hdf5_dev", "ductgpu_dns_save_hdf5",
     "ductgpu_dns_load_hdf5", "ductgpu_vorticity_dev", "ductgpu_dns_statistics_omg", "ductgpu_dns_cfl",
+    "ductgpu_dns_write_statistics_hdf5", "ductgpu_statistics_filename",
 ]
 SETUP_NO_EIGEN = 1
 (K_PASS_FP64, K_NEUMANN, K_WALLS, K_MIXED_GEMM, K_RESIDUAL, K_TRANSFORM, K_TRANSPOSE, K_OTHER, K_LINES,
@@ -195,6 +196,8 @@ def lib():
             "ductgpu_vorticity_dev": [P, P, P, P, P, I, I, I, P, D, I],
             "ductgpu_dns_statistics_omg": [P, P, P, C.POINTER(I)],
             "ductgpu_dns_cfl": [P, C.POINTER(D), C.POINTER(D), C.POINTER(D)],
+            "ductgpu_dns_write_statistics_hdf5": [P, C.c_char_p, D, D],
+            "ductgpu_statistics_filename": [C.c_char_p, C.c_char_p, I],
             "transpose_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
                                C.POINTER(C.c_size_t)],
             "mat_invdiag_gpu_": [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(C.c_size_t),
@@ -228,6 +231,16 @@ def uvwp_filename(fuvwpout, iimag):
     rc = lib().ductgpu_uvwp_filename(os.fsencode(fuvwpout), int(iimag), buf, 4096)
     if rc:
         raise DuctGPUError(rc, "uvwp_filename")
+    return buf.value.decode()
+
+
+def statistics_filename(fuvwpout):
+    """The reference's statistics file name: prefix + 'statistics_NNNN.h5'
+    with the first NNNN whose file does not exist yet."""
+    buf = C.create_string_buffer(4096)
+    rc = lib().ductgpu_statistics_filename(os.fsencode(fuvwpout), buf, 4096)
+    if rc:
+        raise DuctGPUError(rc, "statistics_filename")
     return buf.value.decode()
 
 
@@ -783,6 +796,11 @@ class Dns:
         self.ctx._check(lib().ductgpu_dns_save_hdf5(self.h, os.fsencode(filename), float(time), float(cfl),
                                                     float(slip)))
 
+    def write_statistics_hdf5(self, filename, time=0.0, timef=0.0):
+        """The accumulated statistics as a statistics_NNNN.h5 file."""
+        self.ctx._check(lib().ductgpu_dns_write_statistics_hdf5(self.h, os.fsencode(filename), float(time),
+                                                                float(timef)))
+
     def load_hdf5(self, filename):
         """Restart from a uvwp_NNNN.h5 file; returns the file's time."""
         t = C.c_double()
@@ -850,5 +868,5 @@ class Dns:
 
 
 __all__ = ["Context", "Dns", "DeviceArray", "DuctGPUError", "H5Header", "lib", "LIB_PATH", "EXPORTS",
-           "uvwp_filename", "read_hdf5_header",
+           "uvwp_filename", "statistics_filename", "read_hdf5_header",
            "PREC_FP64", "PREC_MIXED", "GAUGE_POINT", "GAUGE_MEAN"]

@@ -1673,6 +1673,36 @@ extern "C" int ductgpu_dns_save_hdf5(ductgpu_dns d, const char *filename, double
     return ductgpu_save_4fields_fou_hdf5_dev(ctx, filename, d->vel[0], d->vel[1], d->vel[2], d->p, &h);
 }
 
+extern "C" int ductgpu_dns_write_statistics_hdf5(ductgpu_dns d, const char *filename, double time, double timef)
+{
+    if (!d) return DUCTGPU_EARG;
+    ductgpu_ctx ctx = d->ctx;
+    if (!filename) return set_error(ctx, DUCTGPU_EARG, "write_statistics_hdf5: NULL file name");
+    cudaSetDevice(ctx->device);
+    DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const size_t P = d->P, M = d->M;
+    // mean, prod, ppb, spec, om2 are one contiguous block on the device
+    const size_t n = 4 * P + 6 * P + P + 4 * 7 * M + 3 * P;
+    std::vector<double> h(n);
+    DUCT_CUDA(ctx, cudaMemcpy(h.data(), d->st_mean, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    H5Stats st;
+    st.mgalx = d->mgalx;
+    st.my = st.mz = d->my;
+    st.nmodes = d->M;
+    st.nstat = d->nstat;
+    st.timef = timef;
+    st.time = time;
+    st.fnu = d->fnu;
+    st.alp = d->alp;
+    st.aspect = d->aspect;
+    st.mean = h.data();
+    st.prod = st.mean + 4 * P;
+    st.ppb = st.prod + 6 * P;
+    st.spec = st.ppb + P;
+    st.om2 = st.spec + 4 * 7 * M;
+    return h5_write_statistics(ctx, filename, st);
+}
+
 extern "C" int ductgpu_dns_load_hdf5(ductgpu_dns d, const char *filename, double *time)
 {
     if (!d) return DUCTGPU_EARG;

@@ -131,15 +131,25 @@ int device_pointer_check(ductgpu_ctx ctx, const void *p, const char *what)
 
 // ---------------------------------------------------------------- writer
 
-enum Kind { kI32, kF64, kField };
+enum Kind { kI32, kF64, kF64BE };   // 32-bit int (LE), IEEE double LE, IEEE double BE
 
+// One dataset of a file.  Its data is either given on the host (written
+// right after the metadata, 8-byte aligned) or streamed later (`stream`
+// >= 0: placed from the next 4 KiB boundary on, in stream order).
 struct Dset {
     std::string name;
     Kind kind;
-    int32_t i = 0;
-    double d = 0.0;
-    int field = -1;
+    int rank = 1;
+    uint64_t dims[4] = {1, 0, 0, 0};
+    const void *host = nullptr;
+    int stream = -1;
     uint64_t heap_off = 0, oh = 0, data = 0, bytes = 0;
+    uint64_t count() const
+    {
+        uint64_t n = 1;
+        for (int r = 0; r < rank; ++r) n *= dims[r];
+        return n;
+    }
 };
 
 struct Image {
@@ -161,15 +171,14 @@ struct Image {
 
 size_t dset_header_bytes(const Dset &d)
 {
-    const int rank = d.kind == kField ? 4 : 1;
-    return 16 + (8 + 8 + 8 * rank) + (8 + (d.kind == kI32 ? 16 : 24)) + (8 + 8) + (8 + 24);
+    return 16 + (8 + 8 + 8 * (size_t)d.rank) + (8 + (d.kind == kI32 ? 16 : 24)) + (8 + 8) + (8 + 24);
 }
 
 // The object header of one dataset: dataspace, datatype, fill value (none
 // defined, late allocation: libhdf5's defaults), contiguous layout.
-void put_dset_header(Image &im, const Dset &d, const uint64_t *dims)
+void put_dset_header(Image &im, const Dset &d)
 {
-    const int rank = d.kind == kField ? 4 : 1;
+    const int rank = d.rank;
     const size_t o = d.oh;
     im.u8(o, 1);                                          // object header version 1
     im.u16(o + 2, 4);                                     // messages
@@ -179,7 +188,7 @@ void put_dset_header(Image &im, const Dset &d, const uint64_t *dims)
     p = im.msg(p, 0x0001, 8 + 8 * rank, 0);               // dataspace, version 1, no maximum dims
     im.u8(p, 1);
     im.u8(p + 1, rank);
-    for (int r = 0; r < rank; ++r) im.u64(p + 8 + 8 * r, dims[r]);
+    for (int r = 0; r < rank; ++r) im.u64(p + 8 + 8 * r, d.dims[r]);
     p += 8 + 8 * rank;
     if (d.kind == kI32) {
         p = im.msg(p, 0x0003, 16, 1);                     // datatype: 32-bit signed little-endian
@@ -192,7 +201,7 @@ void put_dset_header(Image &im, const Dset &d, const uint64_t *dims)
     } else {
         p = im.msg(p, 0x0003, 24, 1);                     // datatype: IEEE double
         im.u8(p, 0x11);
-        im.u8(p + 1, d.kind == kField ? 0x21 : 0x20);     // implied mantissa msb; big-endian for the fields
+        im.u8(p + 1, d.kind == kF64BE ? 0x21 : 0x20);     // implied mantissa msb; byte order
         im.u8(p + 2, 63);                                 // sign bit
         im.u32(p + 4, 8);
         im.u16(p + 8, 0);                                 // bit offset
@@ -215,6 +224,120 @@ void put_dset_header(Image &im, const Dset &d, const uint64_t *dims)
     im.u8(p + 1, 1);
     im.u64(p + 2, d.data);
     im.u64(p + 10, d.bytes);
+}
+
+// A whole file but the streamed datasets' data: superblock, root group
+// header, local heap, B-tree, symbol table nodes, dataset headers, the host
+// datasets' data; the streamed datasets from the next 4 KiB boundary on.
+// Sorts ds by name and sets every dataset's address; returns the image and
+// the end-of-file address.
+void h5_build(std::vector<Dset> &ds, std::vector<uint8_t> &meta, uint64_t &eof)
+{
+    for (Dset &d : ds) d.bytes = d.count() * (d.kind == kI32 ? 4 : 8);
+    // link names in the order the symbol table nodes keep them
+    std::sort(ds.begin(), ds.end(), [](const Dset &a, const Dset &b) { return strcmp(a.name.c_str(), b.name.c_str()) < 0; });
+    size_t heap_bytes = 8;                                  // offset 0: the empty name
+    for (Dset &d : ds) {
+        d.heap_off = heap_bytes;
+        heap_bytes += pad8(d.name.size() + 1);
+    }
+    const size_t nsnod = (ds.size() + 2 * kLeafK - 1) / (2 * kLeafK);
+    uint64_t a = 96;
+    const uint64_t root_oh = a;
+    a += 40;
+    const uint64_t heap_hdr = a;
+    a += 32;
+    const uint64_t heap_data = a;
+    a += heap_bytes;
+    const uint64_t btree = a;
+    a += kTreeBytes;
+    std::vector<uint64_t> snod(nsnod);
+    for (size_t s = 0; s < nsnod; ++s) {
+        snod[s] = a;
+        a += kSnodBytes;
+    }
+    for (Dset &d : ds) {
+        d.oh = a;
+        a += dset_header_bytes(d);
+    }
+    for (Dset &d : ds)
+        if (d.stream < 0) {
+            d.data = a;
+            a += pad8(d.bytes);
+        }
+    const uint64_t meta_end = a;
+    a = (a + kFieldAlign - 1) / kFieldAlign * kFieldAlign;
+    std::vector<Dset *> streamed;
+    for (Dset &d : ds)
+        if (d.stream >= 0) streamed.push_back(&d);
+    std::sort(streamed.begin(), streamed.end(), [](const Dset *x, const Dset *y) { return x->stream < y->stream; });
+    for (Dset *d : streamed) {
+        d->data = a;
+        a += d->bytes;
+    }
+    eof = streamed.empty() ? meta_end : a;
+
+    Image im;
+    im.b.assign(meta_end, 0);
+    static const char sig[8] = {'\x89', 'H', 'D', 'F', '\r', '\n', '\x1a', '\n'};
+    im.str(0, sig, 8);
+    im.u8(13, 8);                                           // size of offsets
+    im.u8(14, 8);                                           // size of lengths
+    im.u16(16, kLeafK);
+    im.u16(18, kNodeK);
+    im.u64(24, 0);                                          // base address
+    im.u64(32, kUndef);                                     // free-space info
+    im.u64(40, eof);
+    im.u64(48, kUndef);                                     // driver information
+    im.u64(56, 0);                                          // root entry: name offset
+    im.u64(64, root_oh);
+    im.u32(72, 1);                                          // cache type 1: B-tree and heap cached
+    im.u64(80, btree);
+    im.u64(88, heap_hdr);
+    // root group object header: one symbol table message
+    im.u8(root_oh, 1);
+    im.u16(root_oh + 2, 1);
+    im.u32(root_oh + 4, 1);
+    im.u32(root_oh + 8, 24);
+    {
+        const size_t q = im.msg(root_oh + 16, 0x0011, 16, 0);
+        im.u64(q, btree);
+        im.u64(q + 8, heap_hdr);
+    }
+    // local heap of the link names (no free space)
+    im.str(heap_hdr, "HEAP", 4);
+    im.u64(heap_hdr + 8, heap_bytes);
+    im.u64(heap_hdr + 16, kHeapFreeNull);
+    im.u64(heap_hdr + 24, heap_data);
+    for (const Dset &d : ds) im.str(heap_data + d.heap_off, d.name.c_str(), d.name.size() + 1);
+    // one leaf B-tree node over the symbol table nodes; key i+1 is the last
+    // name of node i, key 0 the empty name
+    im.str(btree, "TREE", 4);
+    im.u16(btree + 6, (unsigned)nsnod);
+    im.u64(btree + 8, kUndef);
+    im.u64(btree + 16, kUndef);
+    im.u64(btree + 24, 0);
+    for (size_t s = 0; s < nsnod; ++s) {
+        const size_t last = std::min(ds.size(), (s + 1) * 2 * kLeafK) - 1;
+        im.u64(btree + 32 + 16 * s, snod[s]);
+        im.u64(btree + 40 + 16 * s, ds[last].heap_off);
+    }
+    for (size_t s = 0; s < nsnod; ++s) {
+        const size_t lo = s * 2 * kLeafK, hi = std::min(ds.size(), lo + 2 * kLeafK);
+        im.str(snod[s], "SNOD", 4);
+        im.u8(snod[s] + 4, 1);
+        im.u16(snod[s] + 6, (unsigned)(hi - lo));
+        for (size_t j = lo; j < hi; ++j) {
+            const size_t e = snod[s] + 8 + 40 * (j - lo);
+            im.u64(e, ds[j].heap_off);
+            im.u64(e + 8, ds[j].oh);
+        }
+    }
+    for (const Dset &d : ds) {
+        put_dset_header(im, d);
+        if (d.stream < 0 && d.host && d.bytes) memcpy(&im.b[d.data], d.host, d.bytes);
+    }
+    meta = std::move(im.b);
 }
 
 struct FileCloser {
@@ -564,151 +687,115 @@ int read_header(H5Reader &r, ductgpu_h5_header *h)
 // data -- and where the fields go.  Layout: superblock, root group header,
 // local heap, B-tree, symbol table nodes, dataset headers, the scalars'
 // data, then u, v, w, p from the next 4 KiB boundary on.
+// A file whose datasets all come from the host.
+int h5_write_host(ductgpu_ctx ctx, const char *filename, std::vector<Dset> &ds)
+{
+    std::vector<uint8_t> img;
+    uint64_t eof = 0;
+    h5_build(ds, img, eof);
+    FileCloser fc;
+    fc.fd = open(filename, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    if (fc.fd < 0) return set_error(ctx, DUCTGPU_EARG, "open %s: %s", filename, strerror(errno));
+    if (int rc = pwrite_all(ctx, fc.fd, img.data(), img.size(), 0, filename)) return rc;
+    const int fd = fc.fd;
+    fc.fd = -1;
+    if (close(fd) != 0) return set_error(ctx, DUCTGPU_EARG, "close %s: %s", filename, strerror(errno));
+    return DUCTGPU_OK;
+}
+
+// write_statistics_hdf5 (src/readwrite_hdf5.f90:388-648, one rank, no
+// temperature): the statistics accumulated over nstat recorded steps as the
+// reference names and shapes them.  Host arrays in the stepper's layout:
+// mean [4][P] (u, v, w, p), prod [6][P] (uu, vv, ww, uv, uw, vw), ppb [P],
+// spec [4][7][M], om2 [3][P]; P = my mz.
+int h5_write_statistics(ductgpu_ctx ctx, const char *filename, const H5Stats &st)
+{
+    const uint64_t P = (uint64_t)st.my * st.mz;
+    const int32_t iv[4] = {st.mgalx, st.my, st.mz, st.nstat};
+    const char *in[4] = {"mgalx", "my", "mz", "nstat"};
+    const double dv[5] = {st.timef, st.time, st.fnu, st.alp, st.aspect};
+    const char *dn[5] = {"timef", "time", "fnu", "alp", "aspect"};
+    // the seven spectra points of statistics_fou (src/operators.F:1680-1693), 1-based
+    const int32_t jinco[7] = {st.my / 16, st.my / 8, st.my / 4, st.my / 2, st.my / 16, st.my / 8, st.my / 4};
+    const int32_t kinco[7] = {st.mz / 2, st.mz / 2, st.mz / 2, st.mz / 2, st.mz / 16, st.mz / 8, st.mz / 4};
+    std::vector<Dset> ds;
+    auto scalar = [&](const char *n, Kind k, const void *v) {
+        Dset d{n, k};
+        d.host = v;
+        ds.push_back(d);
+    };
+    auto plane = [&](const char *n, const double *v) {    // Fortran (my, mz): HDF5 (mz, my)
+        Dset d{n, kF64};
+        d.rank = 2;
+        d.dims[0] = (uint64_t)st.mz;
+        d.dims[1] = (uint64_t)st.my;
+        d.host = v;
+        ds.push_back(d);
+    };
+    for (int i = 0; i < 4; ++i) scalar(in[i], kI32, &iv[i]);
+    for (int i = 0; i < 5; ++i) scalar(dn[i], kF64, &dv[i]);
+    const char *mn[4] = {"um", "vm", "wm", "pm"};
+    for (int c = 0; c < 4; ++c) plane(mn[c], st.mean + c * P);
+    const char *pn[6] = {"uub", "vvb", "wwb", "uvb", "uwb", "vwb"};
+    for (int c = 0; c < 6; ++c) plane(pn[c], st.prod + c * P);
+    plane("ppb", st.ppb);
+    const char *on[3] = {"ox2", "oy2", "oz2"};
+    for (int c = 0; c < 3; ++c) plane(on[c], st.om2 + c * P);
+    const char *sn[4] = {"uust", "vvst", "wwst", "ppst"};
+    for (int c = 0; c < 4; ++c) {                       // Fortran (0:mx1, nspec): HDF5 (nspec, mx1+1)
+        Dset d{sn[c], kF64};
+        d.rank = 2;
+        d.dims[0] = 7;
+        d.dims[1] = (uint64_t)st.nmodes;
+        d.host = st.spec + (size_t)c * 7 * st.nmodes;
+        ds.push_back(d);
+    }
+    for (int t = 0; t < 2; ++t) {
+        Dset d{t ? "kinco" : "jinco", kI32};
+        d.dims[0] = 7;
+        d.host = t ? kinco : jinco;
+        ds.push_back(d);
+    }
+    return h5_write_host(ctx, filename, ds);
+}
+
 void h5_layout(const ductgpu_h5_header *hdr, H5Layout &L)
 {
     const uint64_t nm = (uint64_t)hdr->mx1 + 1;
-    const uint64_t fbytes = nm * hdr->mz * hdr->my * 16;
-    const uint64_t fdims[4] = {nm, (uint64_t)hdr->mz, (uint64_t)hdr->my, 2};
-    const uint64_t sdims[1] = {1};
-
     // writeheader_hdf5's scalars (nparams 7: no temperature) and the fields
+    const int32_t iv[6] = {7, hdr->numerop > 0 ? hdr->numerop : 1, hdr->mgalx, hdr->my, hdr->mz, hdr->mx1};
+    const char *in[6] = {"nparams", "numerop", "mgalx", "my", "mz", "mx1"};
+    const double dv[9] = {hdr->alp, hdr->aspect, hdr->time, hdr->fnu, hdr->cfl, hdr->dtfixed, hdr->cmassflow,
+                          hdr->slip, hdr->divergence};
+    const char *dn[9] = {"alp", "aspect", "time", "fnu", "cfl", "dtfixed", "cmassflow", "SLIP-VELOCITY", "DIVERGENCE"};
     std::vector<Dset> ds;
-    auto add_i = [&](const char *n, int x) { Dset d{n, kI32}; d.i = x; d.bytes = 4; ds.push_back(d); };
-    auto add_d = [&](const char *n, double x) { Dset d{n, kF64}; d.d = x; d.bytes = 8; ds.push_back(d); };
-    add_i("nparams", 7);
-    add_i("numerop", hdr->numerop > 0 ? hdr->numerop : 1);
-    add_i("mgalx", hdr->mgalx);
-    add_i("my", hdr->my);
-    add_i("mz", hdr->mz);
-    add_i("mx1", hdr->mx1);
-    add_d("alp", hdr->alp);
-    add_d("aspect", hdr->aspect);
-    add_d("time", hdr->time);
-    add_d("fnu", hdr->fnu);
-    add_d("cfl", hdr->cfl);
-    add_d("dtfixed", hdr->dtfixed);
-    add_d("cmassflow", hdr->cmassflow);
-    add_d("SLIP-VELOCITY", hdr->slip);
-    add_d("DIVERGENCE", hdr->divergence);
-    const char *fname[4] = {"u", "v", "w", "p"};
-    for (int f = 0; f < 4; ++f) {
-        Dset d{fname[f], kField};
-        d.field = f;
-        d.bytes = fbytes;
+    for (int i = 0; i < 6; ++i) {
+        Dset d{in[i], kI32};
+        d.host = &iv[i];
         ds.push_back(d);
     }
-    // link names in the order the symbol table nodes keep them
-    std::sort(ds.begin(), ds.end(), [](const Dset &a, const Dset &b) { return strcmp(a.name.c_str(), b.name.c_str()) < 0; });
-
-    // file layout: superblock, root group header, local heap, B-tree,
-    // symbol table nodes, dataset headers, scalars, then the fields
-    size_t heap_bytes = 8;                                  // offset 0: the empty name
-    for (Dset &d : ds) {
-        d.heap_off = heap_bytes;
-        heap_bytes += pad8(d.name.size() + 1);
+    for (int i = 0; i < 9; ++i) {
+        Dset d{dn[i], kF64};
+        d.host = &dv[i];
+        ds.push_back(d);
     }
-    const size_t nsnod = (ds.size() + 2 * kLeafK - 1) / (2 * kLeafK);
-    uint64_t a = 96;
-    const uint64_t root_oh = a;
-    a += 40;
-    const uint64_t heap_hdr = a;
-    a += 32;
-    const uint64_t heap_data = a;
-    a += heap_bytes;
-    const uint64_t btree = a;
-    a += kTreeBytes;
-    std::vector<uint64_t> snod(nsnod);
-    for (size_t s = 0; s < nsnod; ++s) {
-        snod[s] = a;
-        a += kSnodBytes;
-    }
-    for (Dset &d : ds) {
-        d.oh = a;
-        a += dset_header_bytes(d);
-    }
-    for (Dset &d : ds)
-        if (d.kind != kField) {
-            d.data = a;
-            a += 8;
-        }
-    const uint64_t meta_end = a;
-    a = (a + kFieldAlign - 1) / kFieldAlign * kFieldAlign;
-    Dset *fd_of[4] = {};
-    for (int f = 0; f < 4; ++f)
-        for (Dset &d : ds)
-            if (d.field == f) fd_of[f] = &d;
+    const char *fname[4] = {"u", "v", "w", "p"};
     for (int f = 0; f < 4; ++f) {
-        fd_of[f]->data = a;
-        a += fbytes;
+        Dset d{fname[f], kF64BE};
+        d.rank = 4;
+        d.dims[0] = nm;
+        d.dims[1] = (uint64_t)hdr->mz;
+        d.dims[2] = (uint64_t)hdr->my;
+        d.dims[3] = 2;
+        d.stream = f;
+        ds.push_back(d);
     }
-    const uint64_t eof = a;
-    L.eof = eof;
-    L.field_bytes = fbytes;
-    for (int f = 0; f < 4; ++f) L.field_off[f] = fd_of[f]->data;
-
-    Image im;
-    im.b.assign(meta_end, 0);
-    static const char sig[8] = {'\x89', 'H', 'D', 'F', '\r', '\n', '\x1a', '\n'};
-    im.str(0, sig, 8);
-    im.u8(13, 8);                                           // size of offsets
-    im.u8(14, 8);                                           // size of lengths
-    im.u16(16, kLeafK);
-    im.u16(18, kNodeK);
-    im.u64(24, 0);                                          // base address
-    im.u64(32, kUndef);                                     // free-space info
-    im.u64(40, eof);
-    im.u64(48, kUndef);                                     // driver information
-    im.u64(56, 0);                                          // root entry: name offset
-    im.u64(64, root_oh);
-    im.u32(72, 1);                                          // cache type 1: B-tree and heap cached
-    im.u64(80, btree);
-    im.u64(88, heap_hdr);
-    // root group object header: one symbol table message
-    im.u8(root_oh, 1);
-    im.u16(root_oh + 2, 1);
-    im.u32(root_oh + 4, 1);
-    im.u32(root_oh + 8, 24);
-    {
-        const size_t q = im.msg(root_oh + 16, 0x0011, 16, 0);
-        im.u64(q, btree);
-        im.u64(q + 8, heap_hdr);
-    }
-    // local heap of the link names (no free space)
-    im.str(heap_hdr, "HEAP", 4);
-    im.u64(heap_hdr + 8, heap_bytes);
-    im.u64(heap_hdr + 16, kHeapFreeNull);
-    im.u64(heap_hdr + 24, heap_data);
-    for (const Dset &d : ds) im.str(heap_data + d.heap_off, d.name.c_str(), d.name.size() + 1);
-    // one leaf B-tree node over the symbol table nodes; key i+1 is the last
-    // name of node i, key 0 the empty name
-    im.str(btree, "TREE", 4);
-    im.u16(btree + 6, (unsigned)nsnod);
-    im.u64(btree + 8, kUndef);
-    im.u64(btree + 16, kUndef);
-    im.u64(btree + 24, 0);
-    for (size_t s = 0; s < nsnod; ++s) {
-        const size_t last = std::min(ds.size(), (s + 1) * 2 * kLeafK) - 1;
-        im.u64(btree + 32 + 16 * s, snod[s]);
-        im.u64(btree + 40 + 16 * s, ds[last].heap_off);
-    }
-    for (size_t s = 0; s < nsnod; ++s) {
-        const size_t lo = s * 2 * kLeafK, hi = std::min(ds.size(), lo + 2 * kLeafK);
-        im.str(snod[s], "SNOD", 4);
-        im.u8(snod[s] + 4, 1);
-        im.u16(snod[s] + 6, (unsigned)(hi - lo));
-        for (size_t j = lo; j < hi; ++j) {
-            const size_t e = snod[s] + 8 + 40 * (j - lo);
-            im.u64(e, ds[j].heap_off);
-            im.u64(e + 8, ds[j].oh);
+    h5_build(ds, L.meta, L.eof);
+    for (const Dset &d : ds)
+        if (d.stream >= 0) {
+            L.field_off[d.stream] = d.data;
+            L.field_bytes = d.bytes;
         }
-    }
-    for (const Dset &d : ds) {
-        put_dset_header(im, d, d.kind == kField ? fdims : sdims);
-        if (d.kind == kI32) im.u32(d.data, (uint32_t)d.i);
-        if (d.kind == kF64) memcpy(&im.b[d.data], &d.d, 8);
-    }
-
-    L.meta = std::move(im.b);
 }
 
 } // namespace duct
@@ -732,6 +819,27 @@ extern "C" int ductgpu_uvwp_filename(const char *fuvwpout, int iimag, char *out,
     if ((int)s.size() + 1 > cap) return DUCTGPU_EARG;
     memcpy(out, s.c_str(), s.size() + 1);
     return DUCTGPU_OK;
+}
+
+extern "C" int ductgpu_statistics_filename(const char *fuvwpout, char *out, int cap)
+{
+    if (!fuvwpout || !out || cap <= 0) return DUCTGPU_EARG;
+    // concatb(fuvwpout,'statistics_',11,ext,4,'.h5',3,filename) with ext the
+    // i4.4 of the first icf = 1, 2, ... whose file does not exist
+    // (src/readwrite_hdf5.f90:446-456, src/concat.F:33-45)
+    std::string head(fuvwpout);
+    const size_t sp = head.find(' ');
+    if (sp != std::string::npos) head.resize(sp);
+    for (int icf = 1; icf <= 9999; ++icf) {
+        char num[16];
+        snprintf(num, sizeof num, "%04d", icf);
+        const std::string s = head + "statistics_" + num + ".h5";
+        if (access(s.c_str(), F_OK) == 0) continue;
+        if ((int)s.size() + 1 > cap) return DUCTGPU_EARG;
+        memcpy(out, s.c_str(), s.size() + 1);
+        return DUCTGPU_OK;
+    }
+    return DUCTGPU_EARG;   // all 9999 taken (the reference would loop for ever)
 }
 
 extern "C" int ductgpu_save_4fields_fou_hdf5_dev(ductgpu_ctx ctx, const char *filename, const double *u,

@@ -202,6 +202,13 @@ struct H5Layout {
     uint64_t field_off[4] = {}, field_bytes = 0, eof = 0;
 };
 void h5_layout(const ductgpu_h5_header *hdr, H5Layout &L);
+// h5io.cu: a statistics_NNNN.h5 file from host copies of the accumulators
+struct H5Stats {
+    int mgalx = 0, my = 0, mz = 0, nmodes = 0, nstat = 0;
+    double timef = 0.0, time = 0.0, fnu = 0.0, alp = 0.0, aspect = 1.0;
+    const double *mean = nullptr, *prod = nullptr, *ppb = nullptr, *spec = nullptr, *om2 = nullptr;
+};
+int h5_write_statistics(ductgpu_ctx ctx, const char *filename, const H5Stats &st);
 
 // Brackets one kernel launch with profiling events when enabled and
 // counts it.  Use: { LaunchScope ls(ctx, DUCTGPU_K_...); kernel<<<>>>(); }

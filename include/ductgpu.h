@@ -598,6 +598,19 @@ int ductgpu_read_4fields_fou_hdf5_dev(ductgpu_ctx ctx, const char *filename, dou
  * (that of the loaded u when the file's is 0), so a restart repeats the
  * saved run bit for bit.                                                   */
 int ductgpu_dns_save_hdf5(ductgpu_dns dns, const char *filename, double time, double cfl, double slip);
+/* write_statistics_hdf5 (src/readwrite_hdf5.f90:388-648, one rank, no
+ * temperature): the stepper's accumulated statistics as the reference
+ * writes them -- mgalx, my, mz, nstat (32-bit ints), timef, time, fnu,
+ * alp, aspect (doubles), the (my, mz) sums um, vm, wm, pm, uub, uvb, uwb,
+ * vvb, vwb, wwb, ppb, ox2, oy2, oz2, the (mx1+1, nspec) spectra uust,
+ * vvst, wwst, ppst and the spectra points jinco, kinco (nspec = 7).
+ * timef: the reference's timef (the caller's value).  Synchronises.       */
+int ductgpu_dns_write_statistics_hdf5(ductgpu_dns dns, const char *filename, double time, double timef);
+/* The reference's statistics file name: the prefix (up to its first blank)
+ * + "statistics_NNNN.h5" with the first NNNN = 0001, 0002, ... that does
+ * not exist yet (src/readwrite_hdf5.f90:446-456).  DUCTGPU_EARG when all
+ * 9999 exist or cap is too small.                                          */
+int ductgpu_statistics_filename(const char *fuvwpout, char *out, int cap);
 int ductgpu_dns_load_hdf5(ductgpu_dns dns, const char *filename, double *time);
 
 /* ---- the reference's own GPU entry points (src/mytranspose_cuda.cu) --- */

@@ -67,30 +67,28 @@ def _header_values(hdr):
     return vals
 
 
-def write_4fields(fields, hdr, omit=()):
-    """The bytes of the file save_4fields_fou_hdf5 + writeheader_hdf5 give for
-    complex (my, mz, mx1+1) fields u, v, w, p (Fortran order) and the header
-    dict (my, mz, mx1, mgalx, numerop, alp, aspect, time, fnu, cfl, dtfixed,
-    cmassflow, slip, divergence).  omit: header scalars to leave out (an
-    older file's header)."""
-    my, mz, mx1 = int(hdr["my"]), int(hdr["mz"]), int(hdr["mx1"])
-    nm = mx1 + 1
-    vals = _header_values(hdr)
-    fbytes = nm * mz * my * 16
-    names = sorted([n for n in INT_NAMES + DBL_NAMES if n not in omit] + ["u", "v", "w", "p"],
-                   key=lambda s: s.encode())
-    kind = {n: ("i" if n in INT_NAMES else "d" if n in DBL_NAMES else "f") for n in names}
+def write_datasets(datasets):
+    """The bytes of an HDF5 file holding the given datasets in its root group,
+    laid out as the library lays it out: superblock, root group header, local
+    heap, B-tree, symbol table nodes, dataset headers (in strcmp order of
+    the names), the data of the non-streamed datasets (8-byte aligned), then
+    the streamed ones from the next 4 KiB boundary on, in stream order.
+    datasets: list of dict(name, kind 'i4' | 'f8' | '>f8', dims (HDF5
+    C-order shape), data (numpy array of that shape), stream None or int)."""
+    ds = sorted(datasets, key=lambda d: d["name"].encode())
+    item = {"i4": 4, "f8": 8, ">f8": 8}
+    nbytes = {d["name"]: int(np.prod(d["dims"])) * item[d["kind"]] for d in ds}
 
-    def oh_bytes(n):
-        rank = 4 if kind[n] == "f" else 1
-        return 16 + (8 + 8 + 8 * rank) + (8 + (16 if kind[n] == "i" else 24)) + 16 + 32
+    def oh_bytes(d):
+        rank = len(d["dims"])
+        return 16 + (8 + 8 + 8 * rank) + (8 + (16 if d["kind"] == "i4" else 24)) + 16 + 32
 
     heap_off, h = {}, 8
-    for n in names:
-        heap_off[n] = h
-        h += _pad8(len(n) + 1)
+    for d in ds:
+        heap_off[d["name"]] = h
+        h += _pad8(len(d["name"]) + 1)
     heap_bytes = h
-    nsnod = (len(names) + 2 * LEAF_K - 1) // (2 * LEAF_K)
+    nsnod = (len(ds) + 2 * LEAF_K - 1) // (2 * LEAF_K)
     a = 96
     root_oh = a
     a += 40
@@ -105,19 +103,21 @@ def write_4fields(fields, hdr, omit=()):
         snod.append(a)
         a += SNOD_BYTES
     oh = {}
-    for n in names:
-        oh[n] = a
-        a += oh_bytes(n)
+    for d in ds:
+        oh[d["name"]] = a
+        a += oh_bytes(d)
     data = {}
-    for n in names:
-        if kind[n] != "f":
-            data[n] = a
-            a += 8
+    for d in ds:
+        if d.get("stream") is None:
+            data[d["name"]] = a
+            a += _pad8(nbytes[d["name"]])
     meta_end = a
-    a = (a + FIELD_ALIGN - 1) // FIELD_ALIGN * FIELD_ALIGN
-    for n in ("u", "v", "w", "p"):
-        data[n] = a
-        a += fbytes
+    streamed = sorted([d for d in ds if d.get("stream") is not None], key=lambda d: d["stream"])
+    if streamed:
+        a = (a + FIELD_ALIGN - 1) // FIELD_ALIGN * FIELD_ALIGN
+        for d in streamed:
+            data[d["name"]] = a
+            a += nbytes[d["name"]]
     eof = a
 
     b = bytearray(eof)
@@ -135,56 +135,102 @@ def write_4fields(fields, hdr, omit=()):
     put(root_oh + 16, "HHB3xQQ", 0x0011, 16, 0, btree, heap_hdr)
     b[heap_hdr:heap_hdr + 4] = b"HEAP"
     put(heap_hdr + 8, "QQQ", heap_bytes, HEAP_FREE_NULL, heap_data)
-    for n in names:
-        nb = n.encode() + b"\0"
-        b[heap_data + heap_off[n]:heap_data + heap_off[n] + len(nb)] = nb
+    for d in ds:
+        nb = d["name"].encode() + b"\0"
+        o = heap_data + heap_off[d["name"]]
+        b[o:o + len(nb)] = nb
     b[btree:btree + 4] = b"TREE"
     put(btree + 4, "BBH", 0, 0, nsnod)
     put(btree + 8, "QQQ", UNDEF, UNDEF, 0)
     for s in range(nsnod):
-        last = names[min(len(names), (s + 1) * 2 * LEAF_K) - 1]
+        last = ds[min(len(ds), (s + 1) * 2 * LEAF_K) - 1]["name"]
         put(btree + 32 + 16 * s, "QQ", snod[s], heap_off[last])
     for s in range(nsnod):
-        group = names[s * 2 * LEAF_K:(s + 1) * 2 * LEAF_K]
+        group = ds[s * 2 * LEAF_K:(s + 1) * 2 * LEAF_K]
         b[snod[s]:snod[s] + 4] = b"SNOD"
         put(snod[s] + 4, "BBH", 1, 0, len(group))
-        for j, n in enumerate(group):
-            put(snod[s] + 8 + 40 * j, "QQII16x", heap_off[n], oh[n], 0, 0)
-    for n in names:
-        rank = 4 if kind[n] == "f" else 1
-        dims = (nm, mz, my, 2) if rank == 4 else (1,)
-        nbytes = fbytes if kind[n] == "f" else (4 if kind[n] == "i" else 8)
+        for j, d in enumerate(group):
+            put(snod[s] + 8 + 40 * j, "QQII16x", heap_off[d["name"]], oh[d["name"]], 0, 0)
+    for d in ds:
+        n, dims = d["name"], tuple(d["dims"])
+        rank = len(dims)
         o = oh[n]
-        put(o, "BBHII4x", 1, 0, 4, 1, oh_bytes(n) - 16)
+        put(o, "BBHII4x", 1, 0, 4, 1, oh_bytes(d) - 16)
         p = o + 16
         put(p, "HHB3x", 0x0001, 8 + 8 * rank, 0)
         put(p + 8, "BBBB4x", 1, rank, 0, 0)
         put(p + 16, "%dQ" % rank, *dims)
         p += 16 + 8 * rank
-        if kind[n] == "i":
+        if d["kind"] == "i4":
             put(p, "HHB3x", 0x0003, 16, 1)
             put(p + 8, "BBBBIHH4x", 0x10, 0x08, 0, 0, 4, 0, 32)
             p += 24
         else:
             put(p, "HHB3x", 0x0003, 24, 1)
-            put(p + 8, "BBBBIHHBBBBI4x", 0x11, 0x21 if kind[n] == "f" else 0x20, 63, 0, 8, 0, 64, 52, 11, 0, 52, 1023)
+            put(p + 8, "BBBBIHHBBBBI4x", 0x11, 0x21 if d["kind"] == ">f8" else 0x20, 63, 0, 8, 0, 64, 52, 11, 0, 52,
+                1023)
             p += 32
         put(p, "HHB3x", 0x0005, 8, 1)
         put(p + 8, "BBBB4x", 2, 2, 2, 0)
         p += 16
         put(p, "HHB3x", 0x0008, 24, 0)
-        put(p + 8, "BBQQ6x", 3, 1, data[n], nbytes)
-        if kind[n] == "i":
-            put(data[n], "i", vals[n])
-        elif kind[n] == "d":
-            put(data[n], "d", vals[n])
-    for n, f in zip(("u", "v", "w", "p"), fields):
+        put(p + 8, "BBQQ6x", 3, 1, data[n], nbytes[n])
+        raw = np.ascontiguousarray(d["data"], dtype={"i4": "<i4", "f8": "<f8", ">f8": ">f8"}[d["kind"]])
+        assert raw.size == int(np.prod(dims)), n
+        b[data[n]:data[n] + nbytes[n]] = raw.tobytes()
+    assert meta_end <= eof
+    return bytes(b)
+
+
+def write_4fields(fields, hdr, omit=()):
+    """The bytes of the file save_4fields_fou_hdf5 + writeheader_hdf5 give for
+    complex (my, mz, mx1+1) fields u, v, w, p (Fortran order) and the header
+    dict (my, mz, mx1, mgalx, numerop, alp, aspect, time, fnu, cfl, dtfixed,
+    cmassflow, slip, divergence).  omit: header scalars to leave out (an
+    older file's header)."""
+    my, mz, mx1 = int(hdr["my"]), int(hdr["mz"]), int(hdr["mx1"])
+    nm = mx1 + 1
+    vals = _header_values(hdr)
+    ds = [dict(name=n, kind="i4", dims=(1,), data=np.array([vals[n]])) for n in INT_NAMES if n not in omit]
+    ds += [dict(name=n, kind="f8", dims=(1,), data=np.array([vals[n]])) for n in DBL_NAMES if n not in omit]
+    for k, (n, f) in enumerate(zip(("u", "v", "w", "p"), fields)):
         f = np.asfortranarray(f, dtype=np.complex128)
         assert f.shape == (my, mz, nm), (f.shape, (my, mz, nm))
-        raw = f.reshape(-1, order="F").view(np.float64).astype(">f8").tobytes()
-        b[data[n]:data[n] + fbytes] = raw
-    assert meta_end <= data["u"]
-    return bytes(b)
+        ds.append(dict(name=n, kind=">f8", dims=(nm, mz, my, 2), stream=k,
+                       data=f.reshape(-1, order="F").view(np.float64)))
+    return write_datasets(ds)
+
+
+def write_statistics(st):
+    """The bytes of the file write_statistics_hdf5 (src/readwrite_hdf5.f90:
+    388-648, one rank, no temperature) gives: st = dict(mgalx, my, mz,
+    nstat, timef, time, fnu, alp, aspect, mean (4,my,mz), prod (6,my,mz) in
+    the order uu, vv, ww, uv, uw, vw, ppb (my,mz), spec (4,7,M), om2
+    (3,my,mz)) -- the layout of the stepper's statistics."""
+    my, mz = int(st["my"]), int(st["mz"])
+
+    def plane(a):   # Fortran (my, mz) -> HDF5 (mz, my)
+        return np.asarray(a, dtype=np.float64).T
+
+    ds = [dict(name=n, kind="i4", dims=(1,), data=np.array([int(st[n])])) for n in ("mgalx", "my", "mz", "nstat")]
+    ds += [dict(name=n, kind="f8", dims=(1,), data=np.array([float(st[n])]))
+           for n in ("timef", "time", "fnu", "alp", "aspect")]
+    for c, n in enumerate(("um", "vm", "wm", "pm")):
+        ds.append(dict(name=n, kind="f8", dims=(mz, my), data=plane(st["mean"][c])))
+    for c, n in enumerate(("uub", "vvb", "wwb", "uvb", "uwb", "vwb")):
+        ds.append(dict(name=n, kind="f8", dims=(mz, my), data=plane(st["prod"][c])))
+    ds.append(dict(name="ppb", kind="f8", dims=(mz, my), data=plane(st["ppb"])))
+    for c, n in enumerate(("ox2", "oy2", "oz2")):
+        ds.append(dict(name=n, kind="f8", dims=(mz, my), data=plane(st["om2"][c])))
+    M = np.asarray(st["spec"]).shape[2]
+    for c, n in enumerate(("uust", "vvst", "wwst", "ppst")):
+        ds.append(dict(name=n, kind="f8", dims=(7, M), data=np.asarray(st["spec"][c], dtype=np.float64)))
+    # the seven spectra points of statistics_fou (src/operators.F:1680-1693)
+    ds.append(dict(name="jinco", kind="i4", dims=(7,),
+                   data=np.array([my // 16, my // 8, my // 4, my // 2, my // 16, my // 8, my // 4])))
+    ds.append(dict(name="kinco", kind="i4", dims=(7,),
+                   data=np.array([mz // 2, mz // 2, mz // 2, mz // 2, mz // 16, mz // 8, mz // 4])))
+    return write_datasets(ds)
 
 
 class FormatError(ValueError):

@@ -157,3 +157,27 @@ def test_dns_save_and_restart_repeat_the_run(ctx, tmp_path):
         dns.steps(2)
         for a, b in zip(dns.fields(), after):
             assert np.array_equal(a, b)
+
+
+def test_dns_statistics_file_equals_oracle_file(ctx, tmp_path):
+    """write_statistics_hdf5 (src/readwrite_hdf5.f90:388-648): the stepper's
+    file equals the oracle's restatement of it, byte for byte, for the same
+    accumulated statistics."""
+    m, mgalx, alp, fnu, dt = 33, 64, 1.0, 1.0 / 2000.0, 1e-3
+    u, v, w, p, _ = synth.dns_initial(mgalx, m, alp, 0.1, seed=12)
+    ctx.pseudomat(m, m)
+    path = D.statistics_filename(str(tmp_path) + "/")
+    with D.Dns(ctx, mgalx, alp, fnu, dt, cmassflow=True) as dns:
+        dns.set_fields(u, v, w, p)
+        dns.steps(3, stats_every=1)
+        dns.write_statistics_hdf5(path, time=3 * dt, timef=0.0)
+        st = dns.statistics()
+        om = dns.statistics_omg()
+    assert path.endswith("statistics_0001.h5")
+    ref = H.write_statistics(dict(mgalx=mgalx, my=m, mz=m, nstat=st["nstat"], timef=0.0, time=3 * dt, fnu=fnu,
+                                  alp=alp, aspect=1.0, mean=st["mean"], prod=st["prod"], ppb=st["ppb"],
+                                  spec=st["spec"], om2=om["om2"]))
+    buf = open(path, "rb").read()
+    assert buf == ref
+    ds = H.read(buf)
+    assert int(ds["nstat"][0]) == 3 and np.array_equal(ds["ox2"], om["om2"][0].T)

@@ -1,10 +1,12 @@
-"""The field checkpoint file uvwp_NNNN.h5 on the CPU: the oracle's writer
-against its independent reader, the library's header reader and file name
-rule against the oracle (no GPU: the library's HDF5 reader of the header is
-host code), and the reader's refusals of damaged files.
+"""The field checkpoint file uvwp_NNNN.h5 and the statistics file
+statistics_NNNN.h5 on the CPU: the oracle's writers against its independent
+reader, the library's header reader and file name rules against the oracle
+(no GPU: the library's HDF5 reader of the header is host code), and the
+reader's refusals of damaged files.
 
-Reference: save_4fields_fou_hdf5 / writeheader_hdf5 / readheader_hdf5
-(src/readwrite_hdf5.f90:276-386, 799-920), concat5b (src/concat.F:74-87).
+Reference: save_4fields_fou_hdf5 / writeheader_hdf5 / readheader_hdf5 /
+write_statistics_hdf5 (src/readwrite_hdf5.f90:276-386, 388-648, 799-920),
+concat5b / concatb (src/concat.F:33-45, 74-87).
 """
 import numpy as np
 import pytest
@@ -119,3 +121,26 @@ def test_uvwp_filename_examples():
     assert D.uvwp_filename("run/", 12) == "run/uvwp_0012.h5"
     assert D.uvwp_filename("out   ", 3) == "outuvwp_0003.h5"
     assert D.uvwp_filename("x/", 12345) == "x/uvwp_****.h5"
+
+
+def test_statistics_filename_takes_the_first_free_number(tmp_path):
+    """concatb(fuvwpout,'statistics_',11,ext,4,'.h5',3,filename) with the first
+    icf whose file does not exist (src/readwrite_hdf5.f90:446-456)."""
+    prefix = str(tmp_path) + "/"
+    assert D.statistics_filename(prefix) == prefix + "statistics_0001.h5"
+    (tmp_path / "statistics_0001.h5").write_bytes(b"")
+    (tmp_path / "statistics_0002.h5").write_bytes(b"")
+    assert D.statistics_filename(prefix + " ignored") == prefix + "statistics_0003.h5"
+
+
+def test_oracle_statistics_file_decodes():
+    my, mz, M = 9, 9, 4
+    rng = np.random.default_rng(3)
+    st = dict(mgalx=12, my=my, mz=mz, nstat=5, timef=0.5, time=2.0, fnu=1e-3, alp=0.5, aspect=1.0,
+              mean=rng.standard_normal((4, my, mz)), prod=rng.standard_normal((6, my, mz)),
+              ppb=rng.standard_normal((my, mz)), spec=rng.standard_normal((4, 7, M)),
+              om2=rng.standard_normal((3, my, mz)))
+    ds = H.read(H.write_statistics(st))
+    assert np.array_equal(ds["um"], st["mean"][0].T) and np.array_equal(ds["ppst"], st["spec"][3])
+    assert np.array_equal(ds["uvb"], st["prod"][3].T) and np.array_equal(ds["oz2"], st["om2"][2].T)
+    assert int(ds["nstat"][0]) == 5 and list(ds["jinco"]) == [0, 1, 2, 4, 0, 1, 2]
