@@ -216,13 +216,13 @@ __global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)
 // One tile (field fi, the field's tile `local` = plane * nchunks + chunk)
 // of a flip-symmetric pass, by every thread of the CTA; smem as sized by
 // pass_smem_bytes for this MTW (with the eigenvalue staging).
-template <int MTW, int LINES>
+template <int MTW, int LINES, bool SINGLE = false>
 __device__ __forceinline__ void pass_s_tile(const PassParams &p, int fi, int local, double *smem)
 {
     constexpr int NLD = 2 * LINES + 4, NTW = LINES / 8;
     constexpr int a_chunk_max = (kKC / 16) * (4 * MTW) * 256;
     double *As = smem;
-    double *Bs = smem + 2 * a_chunk_max;
+    double *Bs = smem + (SINGLE ? 1 : 2) * a_chunk_max;
 
     const PassField &F = p.f[fi];
     const int plane = local / F.nchunks;
@@ -303,14 +303,19 @@ __device__ __forceinline__ void pass_s_tile(const PassParams &p, int fi, int loc
             for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
 
     for (int c = 0; c < nkc; ++c) {
-        if (c + 1 < nkc) {
+        if (SINGLE) {
+            // one operator buffer: chunk c is loaded once every warp is done
+            // with chunk c - 1 (the barrier closing the previous iteration)
+            if (c > 0) load_a(c, 0);
+            cp_async_wait<0>();
+        } else if (c + 1 < nkc) {
             load_a(c + 1, (c + 1) & 1);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
         }
         __syncthreads();
-        const double *Ab = As + (c & 1) * a_chunk_max;
+        const double *Ab = As + (SINGLE ? 0 : (c & 1) * a_chunk_max);
 #pragma unroll
         for (int ks = 0; ks < kKC / 16; ++ks) {
             const int kg = kb0 + c * kKC + ks * 16 + t;
@@ -424,13 +429,14 @@ __device__ __forceinline__ void pass_s_tile(const PassParams &p, int fi, int loc
     }
 }
 
-template <int MTW, int LINES>
-__global__ void __launch_bounds__(kThreads, LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)) k_pass_fp64s(const __grid_constant__ PassParams p)
+template <int MTW, int LINES, bool SINGLE = false>
+__global__ void __launch_bounds__(kThreads, SINGLE ? 4 : (LINES == 16 ? 3 : (MTW == 3 ? 1 : 2)))
+    k_pass_fp64s(const __grid_constant__ PassParams p)
 {
     extern __shared__ __align__(16) double smem[];
     int fi = 0;
     while (fi + 1 < p.nf && (int)blockIdx.x >= p.cta_start[fi + 1]) ++fi;
-    pass_s_tile<MTW, LINES>(p, fi, (int)blockIdx.x - p.cta_start[fi], smem);
+    pass_s_tile<MTW, LINES, SINGLE>(p, fi, (int)blockIdx.x - p.cta_start[fi], smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -834,13 +840,13 @@ static cudaError_t launch_pass_p(ductgpu_ctx ctx, const PassParams &pp, int ntil
     return cudaGetLastError();
 }
 
-static size_t pass_smem_bytes(int mtw, int kpad, int lines)
+static size_t pass_smem_bytes(int mtw, int kpad, int lines, int abuf = 2)
 {
     const size_t a_chunk = (size_t)(kKC / 16) * (4 * mtw) * 256;
-    return (2 * a_chunk + (size_t)kpad * (2 * lines + 4)) * sizeof(double);
+    return (abuf * a_chunk + (size_t)kpad * (2 * lines + 4)) * sizeof(double);
 }
 
-template <int MTW, int LINES>
+template <int MTW, int LINES, bool SINGLE = false>
 static cudaError_t launch_pass_s(ductgpu_ctx ctx, const PassParams &pp, int hpad_max)
 {
     // LINES-line tiles: re-cut the callers' 32-line grid
@@ -853,11 +859,13 @@ static cudaError_t launch_pass_s(ductgpu_ctx ctx, const PassParams &pp, int hpad
     }
     q.cta_start[q.nf] = grid;
     // + the eigenvalue staging of the divide epilogue (n <= 2 hpad rows, LINES lines)
-    const size_t smem = pass_smem_bytes(MTW, 2 * hpad_max, LINES) + (size_t)(2 * hpad_max + LINES) * sizeof(double);
-    cudaError_t e = cudaFuncSetAttribute(k_pass_fp64s<MTW, LINES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = pass_smem_bytes(MTW, 2 * hpad_max, LINES, SINGLE ? 1 : 2) +
+                        (size_t)(2 * hpad_max + LINES) * sizeof(double);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_pass_fp64s<MTW, LINES, SINGLE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     LaunchScope ls(ctx, DUCTGPU_K_PASS_FP64);
-    k_pass_fp64s<MTW, LINES><<<grid, kThreads, smem, ctx->stream>>>(q);
+    k_pass_fp64s<MTW, LINES, SINGLE><<<grid, kThreads, smem, ctx->stream>>>(q);
     return cudaGetLastError();
 }
 
@@ -1249,7 +1257,11 @@ int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid)
         switch (mtw) {
         case 1: e = launch_pass_s<1, kParityLines>(ctx, pp, kpad_max); break;
         case 2: e = launch_pass_s<2, kParityLines>(ctx, pp, kpad_max); break;
-        default: e = launch_pass_s<3, kParityLines>(ctx, pp, kpad_max); break;
+        // 96-row half blocks: 8 lines and one operator buffer, 57 KB, four
+        // CTAs per SM (the double-buffered 16-line tile takes 106 KB and
+        // fits twice): config-4 solves 2.99 -> 2.74 ms a step.  The same
+        // form at 32 / 64 rows was slower (config 2: 0.410 -> 0.473 ms).
+        default: e = launch_pass_s<3, 8, true>(ctx, pp, kpad_max); break;
         }
         return e == cudaSuccess ? DUCTGPU_OK : check_cuda(ctx, e, "k_pass_fp64s");
     }
