@@ -75,6 +75,35 @@ __global__ void k_h5_copy(const unsigned long long *__restrict__ src, unsigned l
         dst[i] = src[i];
 }
 
+// cheb_interp's sum (src/chebyshev.f90:750-761) for every point (i, j) of
+// every mode m: out = sum_{k<K} sum_{l<L} c(k, l, m) ty(i, k) tz(j, l), c the
+// old (myr, mzr) planes' Chebyshev coefficients, ty / tz the polynomials at
+// the new nodes; the reference's order of summation (k outer, l inner).
+__global__ void k_cheb_interp(const double2 *__restrict__ c, double2 *__restrict__ out, const double *__restrict__ ty,
+                              const double *__restrict__ tz, int myr, int mzr, int my, int mz, int K, int L, int M)
+{
+    const long long total = (long long)my * mz * M;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % my);
+        const long long r = t / my;
+        const int j = (int)(r % mz);
+        const long long m = r / mz;
+        const double2 *cm = c + (long long)myr * mzr * m;
+        double ax = 0.0, ay = 0.0;
+        for (int k = 0; k < K; ++k) {
+            const double a = ty[(long long)i * K + k];
+            for (int l = 0; l < L; ++l) {
+                const double2 v = cm[k + (long long)myr * l];
+                const double b = tz[(long long)j * L + l];
+                ax += v.x * a * b;
+                ay += v.y * a * b;
+            }
+        }
+        out[t] = make_double2(ax, ay);
+    }
+}
+
 int launch_swap(ductgpu_ctx ctx, const void *src, void *dst, size_t words, bool swap)
 {
     const size_t blocks = std::min<size_t>((words + 255) / 256, (size_t)ctx->num_sms * 8);
@@ -930,15 +959,22 @@ extern "C" int ductgpu_read_4fields_fou_hdf5_dev(ductgpu_ctx ctx, const char *fi
     if (int rc = r.open_root()) return rc;
     ductgpu_h5_header h;
     if (int rc = read_header(r, &h)) return rc;
-    if (h.my != my || h.mz != mz)
+    // read_4fields_fou_hdf5 (src/readwrite_hdf5.f90:129-136): another my AND
+    // mz re-interpolates every plane (cheb_interp); the reference's copy for
+    // one of them alone reads outside its array, so that is refused here
+    const bool interp = h.my != my || h.mz != mz;
+    if (interp && (h.my == my || h.mz == mz))
         return set_error(ctx, DUCTGPU_EARG,
-                         "%s holds my %d mz %d, asked for my %d mz %d (Chebyshev re-interpolation is not built)",
+                         "%s holds my %d mz %d, asked for my %d mz %d: only both sizes changed re-interpolate",
                          filename, h.my, h.mz, my, mz);
+    if (interp && (h.my < 2 || h.mz < 2 || h.my > 4097 || h.mz > 4097))
+        return set_error(ctx, DUCTGPU_EARG, "%s: my %d mz %d", filename, h.my, h.mz);
+    const int fy = interp ? h.my : my, fz = interp ? h.mz : mz;   // the file's planes
     const char *fname[4] = {"u", "v", "w", "p"};
-    const uint64_t plane = (uint64_t)my * mz * 16;
+    const uint64_t fplane = (uint64_t)fy * fz * 16;
     struct Piece {
-        char *dst;
-        uint64_t off, bytes;
+        int f;
+        uint64_t dst, off, bytes;
         bool swap;
     };
     std::vector<Piece> pieces;
@@ -947,23 +983,48 @@ extern "C" int ductgpu_read_4fields_fou_hdf5_dev(ductgpu_ctx ctx, const char *fi
         H5Reader::Info I;
         if (int rc = r.info(fname[f], I)) return rc;
         if (I.cls != 1 || I.tsize != 8) return set_error(ctx, DUCTGPU_EARG, "%s: %s is not double", filename, fname[f]);
-        if (I.rank != 4 || I.dims[1] != (uint64_t)mz || I.dims[2] != (uint64_t)my || I.dims[3] != 2)
-            return set_error(ctx, DUCTGPU_EARG, "%s: %s is not (modes, %d, %d, 2)", filename, fname[f], mz, my);
+        if (I.rank != 4 || I.dims[1] != (uint64_t)fz || I.dims[2] != (uint64_t)fy || I.dims[3] != 2)
+            return set_error(ctx, DUCTGPU_EARG, "%s: %s is not (modes, %d, %d, 2)", filename, fname[f], fz, fy);
         if (I.layout != 1 || I.addr == kUndef || I.bytes != I.count() * 8)
             return set_error(ctx, DUCTGPU_EARG, "%s: %s is not contiguous", filename, fname[f]);
         // h5load_parallel + the copy of read_4fields_fou_hdf5: the file's
         // modes beyond nmodes are dropped, missing ones are zero
-        const uint64_t keep = std::min<uint64_t>(I.dims[0], (uint64_t)nmodes) * plane;
+        const uint64_t keep = std::min<uint64_t>(I.dims[0], (uint64_t)nmodes) * fplane;
         if (r.base + I.addr > r.size || keep > r.size - (r.base + I.addr))
             return set_error(ctx, DUCTGPU_EARG, "%s: %s data outside the file", filename, fname[f]);
         for (uint64_t o = 0; o < keep; o += kChunkBytes)
-            pieces.push_back({(char *)fields[f] + o, r.base + I.addr + o, std::min<uint64_t>(kChunkBytes, keep - o), I.big != 0});
+            pieces.push_back({f, o, r.base + I.addr + o, std::min<uint64_t>(kChunkBytes, keep - o), I.big != 0});
         kept[f] = keep;
     }
+    const uint64_t kmodes = kept[0] / fplane;
+    for (int f = 1; f < 4; ++f)
+        if (kept[f] != kept[0]) return set_error(ctx, DUCTGPU_EARG, "%s: u, v, w, p differ in modes", filename);
+    // the file's planes go straight to the fields, or to a scratch array
+    // of the file's size when they are re-interpolated
+    struct Scratch {
+        void *p[3] = {};
+        ~Scratch()
+        {
+            for (void *q : p)
+                if (q) cudaFree(q);
+        }
+    } sc;
+    double *raw = nullptr;
+    const uint64_t fbytes = kmodes * fplane;
+    if (interp && fbytes) {
+        if (cudaMalloc(&sc.p[0], 4 * fbytes) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(ctx, DUCTGPU_EALLOC, "read_4fields_fou_hdf5: %.1f MB of re-interpolation scratch",
+                             4.0 * fbytes / 1e6);
+        }
+        raw = (double *)sc.p[0];
+    }
     // nothing is written to the fields before all four checked out
+    const uint64_t plane = (uint64_t)my * mz * 16;
+    const uint64_t done = interp ? 0 : kept[0];
     for (int f = 0; f < 4; ++f)
-        if (kept[f] < (uint64_t)nmodes * plane)
-            DUCT_CUDA(ctx, cudaMemsetAsync((char *)fields[f] + kept[f], 0, (uint64_t)nmodes * plane - kept[f], ctx->stream));
+        if (done < (uint64_t)nmodes * plane)
+            DUCT_CUDA(ctx, cudaMemsetAsync((char *)fields[f] + done, 0, (uint64_t)nmodes * plane - done, ctx->stream));
     Staging st;
     if (int rc = st.init(ctx)) return rc;
     for (size_t k = 0; k < pieces.size(); ++k) {
@@ -971,8 +1032,51 @@ extern "C" int ductgpu_read_4fields_fou_hdf5_dev(ductgpu_ctx ctx, const char *fi
         if (k >= 2) DUCT_CUDA(ctx, cudaEventSynchronize(st.ev[b]));   // the launch that read chunk b is done
         if (pread_all(r.fd, st.pin[b], pieces[k].bytes, pieces[k].off) != 0)
             return set_error(ctx, DUCTGPU_EARG, "read %s: %s", filename, strerror(errno));
-        if (int rc = launch_swap(ctx, st.dev[b], pieces[k].dst, pieces[k].bytes / 8, pieces[k].swap)) return rc;
+        char *base = interp ? (char *)raw + pieces[k].f * fbytes : (char *)fields[pieces[k].f];
+        if (int rc = launch_swap(ctx, st.dev[b], base + pieces[k].dst, pieces[k].bytes / 8, pieces[k].swap)) return rc;
         DUCT_CUDA(ctx, cudaEventRecord(st.ev[b], ctx->stream));
+    }
+    if (interp && kmodes) {
+        // cheb_interp (src/chebyshev.f90:725-765) of every plane: its
+        // Chebyshev coefficients (transyz_plane_fou -1), the first
+        // min(20, myr) x min(20, mzr) of them summed at the new nodes
+        for (int f = 0; f < 4; ++f) {
+            double *q = (double *)((char *)raw + f * fbytes);
+            if (int rc = transyz_dev(ctx, q, fy, fz, (int)kmodes, 'y', -1)) return rc;
+            if (int rc = transyz_dev(ctx, q, fy, fz, (int)kmodes, 'z', -1)) return rc;
+        }
+        const int K = std::min(20, fy), L = std::min(20, fz);
+        std::vector<double> t((size_t)my * K + (size_t)mz * L);
+        // cos(k acos(y2)) with y2 = -dglc(-1, 1, my) (src/chebyshev.f90:429-456)
+        const double pi = 4.0 * atan(1.0);
+        for (int i = 0; i < my; ++i) {
+            const double y2 = -(-cos((double)i * (pi / (double)(my - 1))));
+            for (int k = 0; k < K; ++k) t[(size_t)i * K + k] = cos((double)k * acos(y2));
+        }
+        for (int j = 0; j < mz; ++j) {
+            const double z2 = -(-cos((double)j * (pi / (double)(mz - 1))));
+            for (int l = 0; l < L; ++l) t[(size_t)my * K + (size_t)j * L + l] = cos((double)l * acos(z2));
+        }
+        if (cudaMalloc(&sc.p[1], t.size() * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(ctx, DUCTGPU_EALLOC, "read_4fields_fou_hdf5: interpolation tables");
+        }
+        const double *ty = (const double *)sc.p[1];
+        DUCT_CUDA(ctx, cudaMemcpyAsync(sc.p[1], t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                       ctx->stream));
+        for (int f = 0; f < 4; ++f) {
+            const long long total = (long long)my * mz * (long long)kmodes;
+            const int blocks = (int)std::min<long long>((total + 255) / 256, (long long)ctx->num_sms * 16);
+            {
+                LaunchScope ls(ctx, DUCTGPU_K_OTHER);
+                k_cheb_interp<<<blocks, 256, 0, ctx->stream>>>(
+                    reinterpret_cast<const double2 *>((char *)raw + f * fbytes), reinterpret_cast<double2 *>(fields[f]),
+                    ty, ty + (size_t)my * K, fy, fz, my, mz, K, L, (int)kmodes);
+            }
+            DUCT_CUDA(ctx, cudaGetLastError());
+        }
+        // the scratch is freed (and the tables) only after the kernels
+        DUCT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     }
     if (hdr_out) *hdr_out = h;
     return DUCTGPU_OK;

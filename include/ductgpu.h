@@ -581,9 +581,12 @@ int ductgpu_read_hdf5_header(ductgpu_ctx ctx, const char *filename, ductgpu_h5_h
 /* read_4fields_fou_hdf5(u,v,w,p,filename,'r8') (src/readwrite_hdf5.f90:5-197
  * with h5load_parallel :199-273) into DEVICE complex (my, mz, nmodes)
  * fields: the file's modes beyond nmodes are dropped and missing ones are
- * zero, as there; a file of another my or mz is refused (the reference
- * re-interpolates with cheb_interp, which is not built).  hdr_out (may be
- * NULL) receives the file's header.  Synchronises.                        */
+ * zero, as there; a file of another my AND mz is re-interpolated as the
+ * reference does (cheb_interp, src/chebyshev.f90:725-765: the first
+ * min(20, myr) x min(20, mzr) Chebyshev coefficients of each plane summed
+ * at the new nodes; myr - 1 and mzr - 1 of the form 2^a 3^b), a file with
+ * only one of them different is refused.  hdr_out (may be NULL) receives
+ * the file's header.  Synchronises.                                        */
 int ductgpu_read_4fields_fou_hdf5_dev(ductgpu_ctx ctx, const char *filename, double *u, double *v,
                                       double *w, double *p, int my, int mz, int nmodes,
                                       ductgpu_h5_header *hdr_out);

@@ -300,6 +300,26 @@ def transyz(f, cdir, iopt):
     return f
 
 
+def cheb_interp(f, my, mz):
+    """cheb_interp(myr,mzr,tmp1,my,mz,tmpo1), src/chebyshev.f90:725-765, on
+    every mode of a complex (myr, mzr, M) field: each plane's Chebyshev
+    coefficients (transyz_plane_fou -1), the first min(20, myr) x min(20,
+    mzr) of them summed at the nodes of the (my, mz) grid, T_k(y2) =
+    cos(k acos(y2)) with y2 = -dglc(-1, 1) (src/chebyshev.f90:429-456)."""
+    c = transyz(transyz(f, "y", -1), "z", -1)
+    myr, mzr, M = c.shape
+    K, L = min(20, myr), min(20, mzr)
+    pi = 4.0 * np.arctan(1.0)
+    y2 = -(-np.cos(np.arange(my) * (pi / (my - 1))))
+    z2 = -(-np.cos(np.arange(mz) * (pi / (mz - 1))))
+    ty = np.cos(np.outer(np.arccos(y2), np.arange(K)))      # (my, K)
+    tz = np.cos(np.outer(np.arccos(z2), np.arange(L)))      # (mz, L)
+    out = np.zeros((my, mz, M), dtype=np.complex128, order="F")
+    for m in range(M):
+        out[:, :, m] = ty @ c[:K, :L, m] @ tz.T
+    return out
+
+
 def transyz_plane(f, iopt):
     f = np.asfortranarray(f, dtype=np.float64).copy(order="F")
     my, mz = f.shape
@@ -343,7 +363,7 @@ def set_blas_threads(n):
     lib().orc_set_blas_threads(int(n))
 
 
-__all__ = ["Ops", "Dir", "Shen", "Pois", "solvepois", "precomp_mass_flow", "impose_mass_flow", "solveshen", "helm3d_shen", "helm3d_temp", "solvediag", "helm3d", "transyz", "transyz_plane", "derivyz",
+__all__ = ["Ops", "Dir", "Shen", "Pois", "solvepois", "cheb_interp", "precomp_mass_flow", "impose_mass_flow", "solveshen", "helm3d_shen", "helm3d_temp", "solvediag", "helm3d", "transyz", "transyz_plane", "derivyz",
            "cheb2_integral", "cxyz2yzx", "cyzx2xyz", "set_blas_threads", "lib"]
 _ = os
 

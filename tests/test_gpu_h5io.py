@@ -101,15 +101,15 @@ def test_read_oracle_file_with_fewer_and_more_modes(ctx, tmp_path):
                 a.free()
 
 
-def test_read_refuses_other_resolution_and_host_fields(ctx, tmp_path):
+def test_read_refuses_one_changed_size_and_host_fields(ctx, tmp_path):
     my, nm = 33, 5
     host = fields(my, my, nm, 6)
     path = tmp_path / "f.h5"
     path.write_bytes(H.write_4fields(host, header(my, my, nm)))
-    out = [ctx.device_array((65, 65, nm)) for _ in range(4)]
+    out = [ctx.device_array((65, 33, nm)) for _ in range(4)]
     try:
         before = out[0].download()
-        with pytest.raises(D.DuctGPUError, match="re-interpolation"):
+        with pytest.raises(D.DuctGPUError, match="re-interpolate"):
             ctx.read_4fields_fou_hdf5_dev(str(path), *out)
         assert np.array_equal(out[0].download(), before)    # nothing written
     finally:
@@ -181,3 +181,39 @@ def test_dns_statistics_file_equals_oracle_file(ctx, tmp_path):
     assert buf == ref
     ds = H.read(buf)
     assert int(ds["nstat"][0]) == 3 and np.array_equal(ds["ox2"], om["om2"][0].T)
+
+
+
+@pytest.mark.parametrize("src,dst,nm", [((65, 65), (97, 129), 6), ((129, 97), (33, 65), 4)])
+def test_read_reinterpolates_another_grid(ctx, oracle, tmp_path, src, dst, nm):
+    """read_4fields_fou_hdf5 with cheb_interp (src/chebyshev.f90:725-765):
+    against the oracle's restatement, and exact for fields that are
+    polynomials of degree < 20 in y and z."""
+    (myr, mzr), (my, mz) = src, dst
+    rng = np.random.default_rng(myr + my)
+    # polynomials of degree 12 in y and 9 in z at the old nodes (complex,
+    # every mode) -- cheb_interp reproduces them at the new nodes
+    yr, zr = -np.cos(np.arange(myr) * np.pi / (myr - 1)), -np.cos(np.arange(mzr) * np.pi / (mzr - 1))
+    y, z = -np.cos(np.arange(my) * np.pi / (my - 1)), -np.cos(np.arange(mz) * np.pi / (mz - 1))
+    A = rng.standard_normal((13, 10, nm, 4)) + 1j * rng.standard_normal((13, 10, nm, 4))
+
+    def poly(yy, zz):
+        P = np.polynomial.polynomial
+        return [np.asfortranarray(np.stack([P.polygrid2d(yy, zz, A[:, :, m, f])
+                                            for m in range(nm)], axis=2)) for f in range(4)]
+
+    host, exact = poly(yr, zr), poly(y, z)
+    path = tmp_path / "old.h5"
+    path.write_bytes(H.write_4fields(host, header(myr, mzr, nm)))
+    out = [ctx.device_array((my, mz, nm)) for _ in range(4)]
+    try:
+        h = ctx.read_4fields_fou_hdf5_dev(str(path), *out)
+        assert (h["my"], h["mz"]) == (myr, mzr)
+        for a, f, e in zip(out, host, exact):
+            g = a.download()
+            ref = oracle.cheb_interp(f, my, mz)
+            assert np.abs(g - ref).max() < 1e-12 * np.abs(ref).max()
+            assert np.abs(g - e).max() < 1e-11 * np.abs(e).max()
+    finally:
+        for a in out:
+            a.free()

@@ -144,3 +144,18 @@ def test_oracle_statistics_file_decodes():
     assert np.array_equal(ds["um"], st["mean"][0].T) and np.array_equal(ds["ppst"], st["spec"][3])
     assert np.array_equal(ds["uvb"], st["prod"][3].T) and np.array_equal(ds["oz2"], st["om2"][2].T)
     assert int(ds["nstat"][0]) == 5 and list(ds["jinco"]) == [0, 1, 2, 4, 0, 1, 2]
+
+
+@pytest.mark.parametrize("src,dst", [((65, 65), (97, 129)), ((129, 97), (33, 65))])
+def test_oracle_cheb_interp_is_exact_for_low_degree_polynomials(oracle, src, dst):
+    """cheb_interp (src/chebyshev.f90:725-765) keeps 20 x 20 Chebyshev
+    coefficients: a polynomial of degree 12 in y and 9 in z at the old nodes
+    comes out exactly at the new ones (pins the node and sign convention)."""
+    (myr, mzr), (my, mz) = src, dst
+    P = np.polynomial.polynomial
+    A = np.random.default_rng(0).standard_normal((13, 10))
+    nodes = lambda n: -np.cos(np.arange(n) * np.pi / (n - 1))
+    f = np.asfortranarray(P.polygrid2d(nodes(myr), nodes(mzr), A)[:, :, None].astype(complex))
+    e = P.polygrid2d(nodes(my), nodes(mz), A)
+    g = oracle.cheb_interp(f, my, mz)[:, :, 0]
+    assert np.abs(g - e).max() < 1e-13 * np.abs(e).max()
