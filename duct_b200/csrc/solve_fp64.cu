@@ -1260,7 +1260,8 @@ int fp64_pass(ductgpu_ctx ctx, const PassParams &pp, int grid)
         // 96-row half blocks: 8 lines and one operator buffer, 57 KB, four
         // CTAs per SM (the double-buffered 16-line tile takes 106 KB and
         // fits twice): config-4 solves 2.99 -> 2.74 ms a step.  The same
-        // form at 32 / 64 rows was slower (config 2: 0.410 -> 0.473 ms).
+        // form at 32 rows was slower (config 2: 0.410 -> 0.473 ms), at 64
+        // rows no faster (0.412 ms either way).
         default: e = launch_pass_s<3, 8, true>(ctx, pp, kpad_max); break;
         }
         return e == cudaSuccess ? DUCTGPU_OK : check_cuda(ctx, e, "k_pass_fp64s");
