@@ -472,10 +472,12 @@ struct H5Reader {
     };
     std::vector<Entry> entries;
     std::vector<uint8_t> heap;
+    int visits = 0;   // B-tree and symbol table nodes read (a bound for cyclic or huge trees)
 
     int tree(uint64_t addr, int depth)
     {
         if (depth > 16) return fail("group B-tree too deep");
+        if (++visits > 65536) return fail("group B-tree too large");
         uint8_t hdr[24];
         if (!get(addr, hdr, 24) || memcmp(hdr, "TREE", 4)) return fail("bad group B-tree node");
         if (hdr[4] != 0) return fail("group B-tree node of another type");
@@ -491,6 +493,7 @@ struct H5Reader {
                 continue;
             }
             uint8_t sh[8];
+            if (++visits > 65536) return fail("group B-tree too large");
             if (!get(child, sh, 8) || memcmp(sh, "SNOD", 4)) return fail("bad symbol table node");
             const unsigned n = (unsigned)le(sh + 6, 2);
             if (n > 4096) return fail("symbol table node too large");

@@ -315,9 +315,12 @@ def read(buf):
         return heap[off:end].decode()
 
     entries = []
+    visits = [0]
 
     def tree(addr, depth):
         _need(depth < 16, "B-tree too deep")
+        visits[0] += 1
+        _need(visits[0] <= 65536, "B-tree too large")
         node = get(addr, 24 + (2 * node_k) * 16 + 8)
         _need(node[:4] == b"TREE" and node[4] == 0, "group B-tree node")
         level, used = node[5], struct.unpack_from("<H", node, 6)[0]

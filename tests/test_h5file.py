@@ -82,10 +82,17 @@ def test_library_reads_file_behind_a_user_block(tmp_path):
     assert H.header_of(H.read(path.read_bytes()))["time"] == HDR["time"]
 
 
-@pytest.mark.parametrize("cut", ["truncated", "signature", "snod", "heap", "empty"])
+@pytest.mark.parametrize("cut", ["truncated", "signature", "snod", "heap", "empty", "cycle"])
 def test_library_refuses_damaged_files(tmp_path, cut):
     buf = bytearray(H.write_4fields(fields(9, 7, 5, 6), HDR))
-    if cut == "truncated":
+    if cut == "cycle":
+        # a level-1 B-tree node whose 32 children are itself: refused (a
+        # bound on the nodes visited), not walked 32^16 times
+        at = buf.find(b"TREE")
+        buf[at + 4:at + 8] = bytes([0, 1, 32, 0])
+        for i in range(32):
+            buf[at + 32 + 16 * i:at + 40 + 16 * i] = at.to_bytes(8, "little")
+    elif cut == "truncated":
         buf = buf[:len(buf) // 2]
     elif cut == "signature":
         buf[1:4] = b"XYZ"
