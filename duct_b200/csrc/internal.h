@@ -151,6 +151,7 @@ struct ductgpu_ctx_s {
     int tw_len[kTwTables] = {};
     void *tw_tab[kTwTables] = {};
     int *dev_err = nullptr;    // device error word (bounded waits)
+    int tma_tr_per_sm = 0;     // resident TMA-transpose CTAs per SM (0: not asked yet, -1: none)
     int *pq_ctr = nullptr;     // counters of the queued flip-symmetric passes
     size_t pq_cap = 0;
     // side streams of a rectangular batch's independent field groups
@@ -354,6 +355,8 @@ int transyz_dev(ductgpu_ctx ctx, double *f, int my, int mz, int nmodes, char cdi
 int derivyz_dev(ductgpu_ctx ctx, const double *u, double *du, int my, int mz, int nmodes, char cdir,
                 int ider, double scal, char what, double aspect);
 int transpose_dev(ductgpu_ctx ctx, const double *in, double *out, long long A, long long Q);
+// transpose_tma.cu: the same by TMA tile loads; -1 when not applicable
+int transpose_tma(ductgpu_ctx ctx, const double *in, double *out, long long A, long long Q);
 
 // cheb_lines.cu: fused Chebyshev derivative lines with a pointwise epilogue
 // (see the file's header).  One output:

@@ -718,6 +718,10 @@ int derivyz_dev(ductgpu_ctx ctx, const double *u, double *du, int my, int mz, in
 
 int transpose_dev(ductgpu_ctx ctx, const double *in, double *out, long long A, long long Q)
 {
+    // the TMA form where a tensor map describes the arrays, else 32 x 32
+    // tiles through shared memory
+    const int rt = transpose_tma(ctx, in, out, A, Q);
+    if (rt >= 0) return rt;
     dim3 grid((unsigned)((A + 31) / 32), (unsigned)((Q + 31) / 32));
     if (grid.y > 65535) return set_error(ctx, DUCTGPU_EARG, "transpose: %lld columns too many", Q);
     {

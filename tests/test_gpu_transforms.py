@@ -72,6 +72,24 @@ def test_pencil_transposes_bit_exact(gpu_ctx, oracle):
         d.free()
 
 
+@pytest.mark.parametrize("nm,my,nz", [(85, 193, 193), (1, 3, 5), (33, 7, 9), (8, 2, 2), (64, 129, 129), (5, 40, 3)])
+def test_pencil_transposes_bit_exact_sizes(gpu_ctx, oracle, nm, my, nz):
+    """The transposes at the config-4 field and at ragged sizes (tiles of 32
+    cut by the array's edges on both sides; tensor-map boxes beyond them)."""
+    L = D.lib()
+    phys = field(nm, my, nz, nm + my)
+    p_d = _dev(gpu_ctx, phys)
+    q_d = gpu_ctx.device_array((my, nz, nm))
+    gpu_ctx._check(L.ductgpu_cxyz2yzx_dev(gpu_ctx.h, C.c_void_p(p_d.ptr), C.c_void_p(q_d.ptr), nm, my, nz))
+    assert np.array_equal(q_d.download(), oracle.cxyz2yzx(phys))
+    r_d = gpu_ctx.device_array((nm, my, nz))
+    gpu_ctx._check(L.ductgpu_cyzx2xyz_dev(gpu_ctx.h, C.c_void_p(r_d.ptr), C.c_void_p(q_d.ptr), nm, my, nz))
+    assert np.array_equal(r_d.download(), phys)
+    gpu_ctx.synchronize()
+    for d in (p_d, q_d, r_d):
+        d.free()
+
+
 def test_chx2z_chz2x_round_trip(gpu_ctx, oracle):
     L = D.lib()
     my, mz, nm = 33, 33, 17
