@@ -20,7 +20,7 @@ difference of large derivative terms, so rounding-level differences of u*
 (1e-15) come back amplified by the Neumann operator's conditioning
 (measured 3e-12..1.2e-11 after one substep at my = 33, absolute 1e-14);
 any two FP64 implementations of the step differ this way.  Statistics at
-1e-10 (the north star's bar).
+1e-10 (the bar set for the flow statistics).
 
 The FFT line kernel (set_line_kernel(0)) computes the Chebyshev
 coefficients with a half-length DCT-I whose post-step is a scan over the

@@ -1,7 +1,7 @@
 """One RK3/CN step of the config-4 DNS (mgalx = 256: 85 Fourier modes, my =
 mz = 193, Lx = 4 pi, Re_b = 4400, dt = 2e-4, 10 % seeded divergence-free
 perturbation, CMASSFLOW, statistics recorded) on the GPU against the
-oracle's step from the same state -- the north star's full size.  The GPU
+oracle's step from the same state, at the full config-4 size.  The GPU
 runs as the drop-in does: its own eigen-decompositions, the tensor-core
 line kernel, graph-captured substeps; the kx = 0 pressure is pinned at the
 oracle's (LAPACK-order) point.
@@ -10,7 +10,7 @@ Tolerances: u, v, w 1e-12 relative (measured 2e-14 after two steps); p
 1e-10 (measured 2.9e-11: the Neumann solve's conditioning, as in
 test_gpu_dns.py); the statistics (means, products, x-mean of p^2, spectra),
 the wall-stress / energy history and the vorticity diagnostics (second
-moments, enstrophies, zero-mode sectors) 1e-10, the north star's bar for the
+moments, enstrophies, zero-mode sectors) 1e-10, the bar set for the
 flow statistics (measured at most 1.4e-11 and 3.9e-11).
 """
 import os
