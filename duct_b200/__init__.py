@@ -253,6 +253,41 @@ def read_hdf5_header(filename):
     return h.as_dict()
 
 
+def fortran_e15_8(x):
+    """A double as Fortran's e15.8 edit descriptor writes it
+    (" 0.12345678E+01"; the exponent in two digits up to 99)."""
+    import math
+    x = float(x)
+    if x == 0.0 or not math.isfinite(x):
+        return " 0.00000000E+00" if x == 0.0 else ("%15s" % x)
+    e = math.floor(math.log10(abs(x))) + 1
+    m = "%.8f" % (abs(x) / 10.0 ** e)
+    if m.startswith("1"):          # rounding reached 1.0: next decade
+        e += 1
+        m = "%.8f" % (abs(x) / 10.0 ** e)
+    if m.startswith("0.0"):        # below 0.1 after rounding down the power
+        e -= 1
+        m = "%.8f" % (abs(x) / 10.0 ** e)
+    exp = ("E+%02d" if e >= 0 else "E-%02d") % abs(e)
+    return ("-" if x < 0 else " ") + m + exp
+
+
+def ener_line(time, hist_row, omg_row):
+    """The reference's per-step log line (src/main1.f90:471-486, format 111:
+    'ENER: ', 38 values as e15.8 each followed by a blank) from one row of
+    Dns.statistics()['hist'] (stress4[4], energy of u, v, w, the same with
+    mode 0) and the matching row of Dns.statistics_omg()['hist'].  The
+    temperature columns and energi (not computed by the reference either)
+    are 0."""
+    st, en, en2 = list(hist_row[0:4]), list(hist_row[4:7]), list(hist_row[7:10])
+    ox4, oxb4, om, omb = list(omg_row[0:5]), list(omg_row[5:10]), list(omg_row[10:13]), list(omg_row[13:16])
+    import math
+    vals = ([time, sum(st), sum(en)] + en + [0.0, math.sqrt(sum(ox4))] + st + ox4[:4] + oxb4[:4] +
+            [ox4[4], oxb4[4], 0.0] + en2 + [0.0] + [0.0] * 4 + om + omb + [0.0])
+    assert len(vals) == 38
+    return "ENER: " + "".join(fortran_e15_8(v) + " " for v in vals)
+
+
 class DuctGPUError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__("ductgpu status %d: %s" % (code, msg))
@@ -759,6 +794,7 @@ class Dns:
                                             C.byref(h)))
         self.h = h
         self.my = ctx._my
+        self.dt = float(dt)
         self.M = (2 * (int(mgalx) // 3)) // 2
         self.hist_cap = int(hist_cap)
 
@@ -839,6 +875,14 @@ class Dns:
         self.ctx._check(lib().ductgpu_dns_cfl(self.h, C.byref(c), C.byref(s), C.byref(m)))
         return dict(cfl=c.value, slip=s.value, cfl_max=m.value)
 
+    def ener_lines(self, time0=0.0, interval=None):
+        """The reference's 'ENER:' log lines of the recorded steps (see
+        ener_line), the k-th at time time0 + k * interval (interval: the
+        time between recorded steps)."""
+        h, o = self.statistics()["hist"], self.statistics_omg()["hist"]
+        dt = self.dt if interval is None else float(interval)
+        return [ener_line(time0 + k * dt, h[k], o[k]) for k in range(min(len(h), len(o)))]
+
     def statistics_omg(self):
         """dict(om2 (3,my,my): omx2, omy2, omz2; hist (nhist,16): sector
         energies [5] and |Re| integrals [5] of om_x, energy_fou of om_x,
@@ -868,5 +912,5 @@ class Dns:
 
 
 __all__ = ["Context", "Dns", "DeviceArray", "DuctGPUError", "H5Header", "lib", "LIB_PATH", "EXPORTS",
-           "uvwp_filename", "statistics_filename", "read_hdf5_header",
+           "uvwp_filename", "statistics_filename", "read_hdf5_header", "ener_line", "fortran_e15_8",
            "PREC_FP64", "PREC_MIXED", "GAUGE_POINT", "GAUGE_MEAN"]

@@ -270,6 +270,12 @@ def test_dns_steps_match_oracle(oracle, cmassflow):
             assert om["hist"].shape == oref["hist"].shape == (3, 16)
             assert np.abs(om["hist"] - oref["hist"]).max() < 1e-10 * np.abs(oref["hist"]).max()
             assert np.all(oref["hist"][:, 10:] > 0)
+            # the reference's ENER log lines of the three recorded steps
+            lines = gpu.ener_lines()
+            assert len(lines) == 3 and all(len(ln.split()) == 39 for ln in lines)
+            ref13 = [D.fortran_e15_8(x) for x in oref["hist"][2, 0:4]]
+            assert lines[2].split()[13:17] == [r.strip() for r in ref13] or \
+                np.allclose([float(x) for x in lines[2].split()[13:17]], oref["hist"][2, 0:4], rtol=1e-7)
 
 
 def test_dns_graph_replay_equals_direct_launches(oracle):

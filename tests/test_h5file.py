@@ -166,3 +166,24 @@ def test_oracle_cheb_interp_is_exact_for_low_degree_polynomials(oracle, src, dst
     e = P.polygrid2d(nodes(my), nodes(mz), A)
     g = oracle.cheb_interp(f, my, mz)[:, :, 0]
     assert np.abs(g - e).max() < 1e-13 * np.abs(e).max()
+
+
+@pytest.mark.parametrize("x,want", [(1.0, " 0.10000000E+01"), (-2.5e-4, "-0.25000000E-03"), (0.0, " 0.00000000E+00"),
+                                    (123456789.0, " 0.12345679E+09"), (0.999999999, " 0.10000000E+01"),
+                                    (1.0e-10, " 0.10000000E-09"), (-7.0, "-0.70000000E+01")])
+def test_fortran_e15_8(x, want):
+    assert D.fortran_e15_8(x) == want
+
+
+def test_ener_line_columns_feed_the_reference_parser():
+    """utils/gen_tsd2hdf5.py:37-42 reads awk columns 14-17 of the ENER lines as
+    the om_x sector energies Sn, Sw, Ss, Se."""
+    hist = [1.0, 2.0, 3.0, 4.0, 0.1, 0.2, 0.3, 0.11, 0.21, 0.31]
+    omg = [5.0, 6.0, 7.0, 8.0, 9.0, 10.0, 11.0, 12.0, 13.0, 14.0, 0.5, 0.6, 0.7, 0.51, 0.61, 0.71]
+    line = D.ener_line(0.25, hist, omg)
+    cols = line.split()
+    assert cols[0] == "ENER:" and len(cols) == 39
+    assert [float(c) for c in cols[13:17]] == [5.0, 6.0, 7.0, 8.0]     # awk $14..$17
+    assert float(cols[1]) == 0.25 and float(cols[2]) == 10.0 and float(cols[3]) == pytest.approx(0.6)
+    assert float(cols[8]) == pytest.approx(35.0 ** 0.5)                  # sqrt of the five sector energies
+    assert [float(c) for c in cols[32:38]] == [0.5, 0.6, 0.7, 0.51, 0.61, 0.71]
