@@ -152,6 +152,17 @@ struct ductgpu_ctx_s {
     void *tw_tab[kTwTables] = {};
     int *dev_err = nullptr;    // device error word (bounded waits)
     int tma_tr_per_sm = 0;     // resident TMA-transpose CTAs per SM (0: not asked yet, -1: none)
+    // the last tensor maps of the TMA transpose (a map describes an address
+    // and sizes, not a context), encoded once: calls take ~16 us on a
+    // config-4 field, so per-call host work shows
+    struct TmaMap {
+        const void *in = nullptr;
+        long long A = 0, Q = 0;
+        alignas(64) unsigned char map[128];
+    };
+    static constexpr int kTmaMaps = 8;
+    TmaMap tma_maps[kTmaMaps];
+    int tma_next = 0;
     int *pq_ctr = nullptr;     // counters of the queued flip-symmetric passes
     size_t pq_cap = 0;
     // side streams of a rectangular batch's independent field groups

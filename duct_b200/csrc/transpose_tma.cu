@@ -17,6 +17,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <string.h>
 
 namespace duct {
 
@@ -142,15 +143,29 @@ int transpose_tma(ductgpu_ctx ctx, const double *in, double *out, long long A, l
     if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) return -1;
     // tensor coordinates are signed 32-bit: the last tile's must fit
     if (2 * A + 2 * kTile > 0x7fffffffll || Q + kTile > 0x7fffffffll || 16 * A >= (1ll << 40)) return -1;
+    static_assert(sizeof(CUtensorMap) == sizeof(ctx->tma_maps[0].map), "tensor map size");
     CUtensorMap map;
-    const cuuint64_t dims[2] = {(cuuint64_t)(2 * A), (cuuint64_t)Q};
-    const cuuint64_t strides[1] = {(cuuint64_t)(16 * A)};
-    const cuuint32_t box[2] = {(cuuint32_t)(2 * kBoxA), (cuuint32_t)kTile};
-    const cuuint32_t estr[2] = {1, 1};
-    if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(in), dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return -1;
+    int hit = -1;
+    for (int i = 0; i < ductgpu_ctx_s::kTmaMaps; ++i)
+        if (ctx->tma_maps[i].in == in && ctx->tma_maps[i].A == A && ctx->tma_maps[i].Q == Q) hit = i;
+    if (hit >= 0) {
+        memcpy(&map, ctx->tma_maps[hit].map, sizeof map);
+    } else {
+        const cuuint64_t dims[2] = {(cuuint64_t)(2 * A), (cuuint64_t)Q};
+        const cuuint64_t strides[1] = {(cuuint64_t)(16 * A)};
+        const cuuint32_t box[2] = {(cuuint32_t)(2 * kBoxA), (cuuint32_t)kTile};
+        const cuuint32_t estr[2] = {1, 1};
+        if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(in), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return -1;
+        ductgpu_ctx_s::TmaMap &slot = ctx->tma_maps[ctx->tma_next];
+        ctx->tma_next = (ctx->tma_next + 1) % ductgpu_ctx_s::kTmaMaps;
+        slot.in = in;
+        slot.A = A;
+        slot.Q = Q;
+        memcpy(slot.map, &map, sizeof map);
+    }
     const long long ta_n = (A + kTile - 1) / kTile, tiles = ta_n * ((Q + kTile - 1) / kTile);
     // resident CTAs per SM: asked once per context (a call is ~16 us of
     // device time at a config-4 field, so host work per call shows)
