@@ -972,6 +972,17 @@ extern "C" int ductgpu_read_4fields_fou_hdf5_dev(ductgpu_ctx ctx, const char *fi
                          filename, h.my, h.mz, my, mz);
     if (interp && (h.my < 2 || h.mz < 2 || h.my > 4097 || h.mz > 4097))
         return set_error(ctx, DUCTGPU_EARG, "%s: my %d mz %d", filename, h.my, h.mz);
+    // the old planes' Chebyshev transform needs n - 1 = 2^a 3^b (checked
+    // here, before anything is written to the fields)
+    auto dct_len_ok = [](int n) {
+        int m = n - 1;
+        while (m % 2 == 0) m /= 2;
+        while (m % 3 == 0) m /= 3;
+        return m == 1;
+    };
+    if (interp && (!dct_len_ok(h.my) || !dct_len_ok(h.mz)))
+        return set_error(ctx, DUCTGPU_EARG, "%s: my %d mz %d cannot be re-interpolated (n - 1 must be 2^a 3^b)",
+                         filename, h.my, h.mz);
     const int fy = interp ? h.my : my, fz = interp ? h.mz : mz;   // the file's planes
     const char *fname[4] = {"u", "v", "w", "p"};
     const uint64_t fplane = (uint64_t)fy * fz * 16;

@@ -101,6 +101,24 @@ def test_read_oracle_file_with_fewer_and_more_modes(ctx, tmp_path):
                 a.free()
 
 
+def test_read_refuses_an_old_grid_the_transform_cannot_take(ctx, tmp_path):
+    """my - 1 = 7^2: no Chebyshev transform of the old planes -- refused
+    before the fields are touched."""
+    host = fields(50, 50, 3, 9)
+    path = tmp_path / "odd.h5"
+    path.write_bytes(H.write_4fields(host, header(50, 50, 3)))
+    out = [ctx.device_array((33, 33, 3)) for _ in range(4)]
+    try:
+        for a in out:
+            a.upload(np.full((33, 33, 3), 2.0 + 1.0j))
+        with pytest.raises(D.DuctGPUError, match="re-interpolated"):
+            ctx.read_4fields_fou_hdf5_dev(str(path), *out)
+        assert np.all(out[0].download() == 2.0 + 1.0j)      # untouched
+    finally:
+        for a in out:
+            a.free()
+
+
 def test_read_refuses_one_changed_size_and_host_fields(ctx, tmp_path):
     my, nm = 33, 5
     host = fields(my, my, nm, 6)
