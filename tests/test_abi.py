@@ -47,3 +47,21 @@ def test_null_context_is_rejected():
     assert L.ductgpu_launch_count(None) == -1
     assert L.ductgpu_synchronize(None) == D.EARG
     assert L.ductgpu_selftest_wait_timeout(None, 16) == D.EARG
+
+
+@pytest.mark.parametrize("lang", ["c", "c++"])
+def test_header_compiles_for_c_and_cpp_hosts(tmp_path, lang):
+    """include/ductgpu.h is plain C (a Fortran host binds it through
+    ISO_C_BINDING; a C or C++ host includes it directly)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc" if lang == "c" else "g++")
+    if cc is None:
+        pytest.skip("no host compiler")
+    src = tmp_path / "use.c"
+    src.write_text('#include "ductgpu.h"\n'
+                   'int main(void) { ductgpu_h5_header h; h.my = 1; (void)h; return DUCTGPU_OK; }\n')
+    std = ["-std=c99", "-pedantic"] if lang == "c" else ["-std=c++11", "-x", "c++"]
+    r = subprocess.run([cc, *std, "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), "-c", str(src), "-o",
+                        str(tmp_path / "use.o")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
