@@ -65,3 +65,15 @@ def test_header_compiles_for_c_and_cpp_hosts(tmp_path, lang):
     r = subprocess.run([cc, *std, "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), "-c", str(src), "-o",
                         str(tmp_path / "use.o")], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_integration_interface_blocks_name_real_entries():
+    """Every bind(C, name=...) of the Fortran interface blocks in
+    INTEGRATION.md is declared in the header and exported by the library."""
+    import duct_b200 as D
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    bound = set(re.findall(r'bind\(C,\s*name="(\w+)"\)', text))
+    assert bound, "no interface blocks found"
+    L = D.lib()
+    assert bound <= declared(), sorted(bound - declared())
+    assert all(hasattr(L, n) for n in bound)
